@@ -1,0 +1,274 @@
+"""TEST INFRASTRUCTURE ONLY — ctypes access to the oracle.
+
+Two checkers, both CPU:
+
+* ``port``: oracle/lib/libkrige_oracle.so, this project's restatement of the
+  reference's kriging path (oracle/krige_oracle.cpp);
+* ``ref``:  oracle/_ref/libref_harness.so, the reference's own code compiled
+  from its sources by oracle/Makefile (present wherever it was built; the
+  product never loads either).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_PATH = os.path.join(HERE, "lib", "libkrige_oracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "libref_harness.so")
+REF_API_PATH = os.path.join(HERE, "_ref", "libhpgl.so")
+
+_i = C.POINTER(C.c_int)
+_d = C.POINTER(C.c_double)
+_f = C.POINTER(C.c_float)
+_u8 = C.POINTER(C.c_ubyte)
+_u32 = C.POINTER(C.c_uint)
+
+_libs = {}
+
+
+def _ptr(a, t):
+    if a is None:
+        return C.cast(None, t)
+    return a.ctypes.data_as(t)
+
+
+def _arr(v, dt):
+    return np.ascontiguousarray(np.asarray(v, dtype=dt))
+
+
+def load(which: str):
+    """Load 'port' or 'ref'; raises OSError when the library is absent."""
+    if which in _libs:
+        return _libs[which]
+    path = PORT_PATH if which == "port" else REF_PATH
+    lib = C.CDLL(path)
+    if which == "port":
+        lib.ko_krige_cont.argtypes = [C.c_int, _i, _f, _u8, C.c_int, _d, _d, C.c_double, C.c_double,
+                                      _i, C.c_int, C.c_double, _i, C.c_int, _i, _i, _u8, _d, _d,
+                                      _f, _i, C.c_int, C.c_int]
+        lib.ko_krige_ind.argtypes = [C.c_int, _i, _u8, _u8, C.c_int, C.c_int, _d, _d, C.c_double,
+                                     C.c_double, _i, C.c_int, C.c_double, _i, C.c_int, _i, _i, _u8,
+                                     _d, _d, _f, _i, C.c_int, C.c_int]
+        lib.ko_cont_grid.argtypes = [C.c_int, _i, _f, _u8, C.c_int, _d, _d, C.c_double, C.c_double,
+                                     _i, C.c_int, C.c_int, C.c_double, _f, _u8, _d, _d, _i, C.c_int]
+        lib.ko_indicator_grid.argtypes = [_i, _u8, _u8, C.c_int, _i, _d, _d, _d, _d, _i, _i, _d,
+                                          _u8, _u8, _f, C.c_int]
+        lib.ko_median_ik_grid.argtypes = [_i, _u8, _u8, C.c_int, _d, _d, C.c_double, C.c_double,
+                                          _i, C.c_int, _d, _u8, _u8, _d, _i, C.c_int]
+        lib.ko_template.argtypes = [C.c_int, C.c_int, _d, _d, C.c_double, C.c_double, _i, _i,
+                                    C.c_int, _i]
+        lib.ko_cov.argtypes = [C.c_int, C.c_int, _d, _d, C.c_double, C.c_double, _i, _i, _i]
+        lib.ko_cov.restype = C.c_double
+        lib.ko_transform.argtypes = [_d, _d, _d]
+        lib.ko_sk_weights.argtypes = [_d, _d, _d, _d, C.c_int, C.c_int, _d, _d, C.c_double,
+                                      C.c_double, _d, _d]
+        lib.ko_sort_check.argtypes = [_u32, C.c_int, _i, _i]
+        lib.ko_sort_check.restype = None
+    else:
+        lib.ref_krige_cont.argtypes = [C.c_int, _i, _f, _u8, C.c_int, _d, _d, C.c_double,
+                                       C.c_double, _i, C.c_int, C.c_double, _i, C.c_int, _i, _i,
+                                       _u8, _d, _d, _f, _i, C.c_int]
+        lib.ref_krige_ind.argtypes = [C.c_int, _i, _u8, _u8, C.c_int, C.c_int, _d, _d, C.c_double,
+                                      C.c_double, _i, C.c_int, C.c_double, _i, C.c_int, _i, _i,
+                                      _u8, _d, _d, _f, _i, C.c_int]
+        lib.ref_template.argtypes = [C.c_int, C.c_int, _d, _d, C.c_double, C.c_double, _i, _i,
+                                     C.c_int, _i]
+        lib.ref_cov.argtypes = [C.c_int, C.c_int, _d, _d, C.c_double, C.c_double, _i, _i, _i]
+        lib.ref_cov.restype = C.c_double
+        lib.ref_transform.argtypes = [_d, _d, _d]
+        lib.ref_sk_weights.argtypes = [_d, _d, _d, _d, C.c_int, C.c_int, _d, _d, C.c_double,
+                                       C.c_double, _d, _d]
+    _libs[which] = lib
+    return lib
+
+
+def available(which: str) -> bool:
+    try:
+        load(which)
+        return True
+    except OSError:
+        return False
+
+
+def krige_nodes(which, kind, dims, data, mask, cov, radiuses, k, mean=0.0, nodes=None,
+                ind_value: Optional[int] = None, precision=0, threads=0, want_idx=True):
+    """Per-node kriging at `nodes` (default: every uninformed cell).
+
+    kind 0 = OK (analytic covariance), 1 = SK / IK (truncated table),
+    2 = median-IK flavour (truncated field; same values as 1).
+    Returns a dict with idx (n,k; -1 padded), count, path (ref: template path
+    flag; port: same), est (f64), var (f64), est_f (f32), status.
+    """
+    lib = load(which)
+    dims_a = _arr(dims, np.int32)
+    mask = _arr(mask, np.uint8)
+    if nodes is None:
+        nodes = np.flatnonzero(mask == 0)
+    nodes = _arr(nodes, np.int32)
+    n = len(nodes)
+    out = {
+        "idx": np.full((n, k), -1, np.int32) if want_idx else None,
+        "count": np.zeros(n, np.int32),
+        "path": np.zeros(n, np.uint8),
+        "est": np.zeros(n, np.float64),
+        "var": np.zeros(n, np.float64),
+        "est_f": np.zeros(n, np.float32),
+        "status": np.zeros(n, np.int32),
+    }
+    ranges = _arr(cov.ranges, np.float64)
+    angles = _arr(cov.angles, np.float64)
+    rad = _arr(radiuses, np.int32)
+    common_tail = [_ptr(nodes, _i), n, _ptr(out["idx"], _i), _ptr(out["count"], _i),
+                   _ptr(out["path"], _u8), _ptr(out["est"], _d), _ptr(out["var"], _d),
+                   _ptr(out["est_f"], _f), _ptr(out["status"], _i)]
+    if ind_value is None:
+        data = _arr(data, np.float32)
+        head = [kind, _ptr(dims_a, _i), _ptr(data, _f), _ptr(mask, _u8), int(cov.cov_type),
+                _ptr(ranges, _d), _ptr(angles, _d), float(cov.sill), float(cov.nugget),
+                _ptr(rad, _i), int(k), float(mean)]
+        if which == "port":
+            rc = lib.ko_krige_cont(*head, *common_tail, int(precision), int(threads))
+        else:
+            rc = lib.ref_krige_cont(*head, *common_tail, int(threads))
+    else:
+        data = _arr(data, np.uint8)
+        head = [kind, _ptr(dims_a, _i), _ptr(data, _u8), _ptr(mask, _u8), int(ind_value),
+                int(cov.cov_type), _ptr(ranges, _d), _ptr(angles, _d), float(cov.sill),
+                float(cov.nugget), _ptr(rad, _i), int(k), float(mean)]
+        if which == "port":
+            rc = lib.ko_krige_ind(*head, *common_tail, int(precision), int(threads))
+        else:
+            rc = lib.ref_krige_ind(*head, *common_tail, int(threads))
+    if rc != 0:
+        raise RuntimeError(f"oracle {which} failed (rc={rc})")
+    out["nodes"] = nodes
+    return out
+
+
+def template(which, kind, cov, radiuses, cap=None):
+    lib = load(which)
+    ranges = _arr(cov.ranges, np.float64)
+    angles = _arr(cov.angles, np.float64)
+    rad = _arr(radiuses, np.int32)
+    if cap is None:
+        cap = int((2 * rad[0] + 1) * (2 * rad[1] + 1) * (2 * rad[2] + 1))
+    out = np.zeros((cap, 3), np.int32)
+    lim = C.c_int(0)
+    fn = lib.ko_template if which == "port" else lib.ref_template
+    n = fn(kind, int(cov.cov_type), _ptr(ranges, _d), _ptr(angles, _d), float(cov.sill),
+           float(cov.nugget), _ptr(rad, _i), _ptr(out, _i), cap, C.byref(lim))
+    if n < 0:
+        raise RuntimeError("template failed")
+    return out[:n].copy(), lim.value
+
+
+def transform(which, ranges, angles):
+    lib = load(which)
+    out = np.zeros(9, np.float64)
+    fn = lib.ko_transform if which == "port" else lib.ref_transform
+    rc = fn(_ptr(_arr(ranges, np.float64), _d), _ptr(_arr(angles, np.float64), _d), _ptr(out, _d))
+    if rc != 0:
+        raise ValueError("zero range")
+    return out
+
+
+def cov_point(which, kind, cov, radiuses, a, b):
+    lib = load(which)
+    fn = lib.ko_cov if which == "port" else lib.ref_cov
+    return fn(kind, int(cov.cov_type), _ptr(_arr(cov.ranges, np.float64), _d),
+              _ptr(_arr(cov.angles, np.float64), _d), float(cov.sill), float(cov.nugget),
+              _ptr(_arr(radiuses, np.int32), _i), _ptr(_arr(a, np.int32), _i),
+              _ptr(_arr(b, np.int32), _i))
+
+
+def sk_weights(which, center, xs, ys, zs, cov):
+    lib = load(which)
+    n = len(xs)
+    w = np.zeros(n, np.float64)
+    var = C.c_double(0)
+    fn = lib.ko_sk_weights if which == "port" else lib.ref_sk_weights
+    ok = fn(_ptr(_arr(center, np.float64), _d), _ptr(_arr(xs, np.float64), _d),
+            _ptr(_arr(ys, np.float64), _d), _ptr(_arr(zs, np.float64), _d), n, int(cov.cov_type),
+            _ptr(_arr(cov.ranges, np.float64), _d), _ptr(_arr(cov.angles, np.float64), _d),
+            float(cov.sill), float(cov.nugget), _ptr(w, _d), C.byref(var))
+    return (w, var.value) if ok else (None, None)
+
+
+def cont_grid(kind, dims, data, mask, cov, radiuses, k, mean=None, threads=0):
+    """Whole-grid OK (kind 0) / SK (kind 1) with the reference's output rules (port)."""
+    lib = load("port")
+    data = _arr(data, np.float32)
+    mask = _arr(mask, np.uint8)
+    out_d = data.copy()
+    out_m = mask.copy()
+    est = np.zeros(len(data), np.float64)
+    var = np.zeros(len(data), np.float64)
+    st = np.zeros(len(data), np.int32)
+    rc = lib.ko_cont_grid(kind, _ptr(_arr(dims, np.int32), _i), _ptr(data, _f), _ptr(mask, _u8),
+                          int(cov.cov_type), _ptr(_arr(cov.ranges, np.float64), _d),
+                          _ptr(_arr(cov.angles, np.float64), _d), float(cov.sill),
+                          float(cov.nugget), _ptr(_arr(radiuses, np.int32), _i), int(k),
+                          1 if mean is None else 0, 0.0 if mean is None else float(mean),
+                          _ptr(out_d, _f), _ptr(out_m, _u8), _ptr(est, _d), _ptr(var, _d),
+                          _ptr(st, _i), int(threads))
+    if rc:
+        raise RuntimeError("cont_grid failed")
+    return out_d, out_m, est, var, st
+
+
+def indicator_grid(dims, data, mask, covs, radiuses, ks, marginals, threads=0):
+    lib = load("port")
+    n_cat = len(covs)
+    data = _arr(data, np.uint8)
+    mask = _arr(mask, np.uint8)
+    out_d = data.copy()
+    out_m = mask.copy()
+    probs = np.zeros((len(data), n_cat), np.float32)
+    rc = lib.ko_indicator_grid(
+        _ptr(_arr(dims, np.int32), _i), _ptr(data, _u8), _ptr(mask, _u8), n_cat,
+        _ptr(_arr([c.cov_type for c in covs], np.int32), _i),
+        _ptr(_arr([c.ranges for c in covs], np.float64), _d),
+        _ptr(_arr([c.angles for c in covs], np.float64), _d),
+        _ptr(_arr([c.sill for c in covs], np.float64), _d),
+        _ptr(_arr([c.nugget for c in covs], np.float64), _d),
+        _ptr(_arr(radiuses, np.int32), _i), _ptr(_arr(ks, np.int32), _i),
+        _ptr(_arr(marginals, np.float64), _d), _ptr(out_d, _u8), _ptr(out_m, _u8),
+        _ptr(probs, _f), int(threads))
+    if rc:
+        raise RuntimeError("indicator_grid failed")
+    return out_d, out_m, probs
+
+
+def median_ik_grid(dims, data, mask, cov, radiuses, k, marginal_probs, threads=0):
+    lib = load("port")
+    data = _arr(data, np.uint8)
+    mask = _arr(mask, np.uint8)
+    out_d = data.copy()
+    out_m = mask.copy()
+    prob = np.zeros(len(data), np.float64)
+    st = np.zeros(len(data), np.int32)
+    rc = lib.ko_median_ik_grid(
+        _ptr(_arr(dims, np.int32), _i), _ptr(data, _u8), _ptr(mask, _u8), int(cov.cov_type),
+        _ptr(_arr(cov.ranges, np.float64), _d), _ptr(_arr(cov.angles, np.float64), _d),
+        float(cov.sill), float(cov.nugget), _ptr(_arr(radiuses, np.int32), _i), int(k),
+        _ptr(_arr(marginal_probs, np.float64), _d), _ptr(out_d, _u8), _ptr(out_m, _u8),
+        _ptr(prob, _d), _ptr(st, _i), int(threads))
+    if rc:
+        raise RuntimeError("median_ik_grid failed")
+    return out_d, out_m, prob, st
+
+
+def sort_check(keys):
+    lib = load("port")
+    keys = _arr(keys, np.uint32)
+    a = np.zeros(len(keys), np.int32)
+    b = np.zeros(len(keys), np.int32)
+    lib.ko_sort_check(_ptr(keys, _u32), len(keys), _ptr(a, _i), _ptr(b, _i))
+    return a, b
