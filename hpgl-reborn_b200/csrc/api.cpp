@@ -1,0 +1,391 @@
+// The C ABI declared in include/hpgl_b200.h. Reference-compatible entry
+// points keep HPGL's conventions (api.cpp:30-50): void returns, the message of
+// the last failure kept for hpgl_get_last_exception_message; nothing aborts.
+#include "../../include/hpgl_b200.h"
+#include "engine_api.h"
+#include "host_model.h"
+
+#include <climits>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace
+{
+std::mutex g_handler_mu;
+int (*g_output)(char *, void *) = nullptr;
+void *g_output_param = nullptr;
+int (*g_progress)(char *, int, void *) = nullptr;
+void *g_progress_param = nullptr;
+
+void emit(const std::string &s)
+{
+    std::lock_guard<std::mutex> lk(g_handler_mu);
+    if (g_output)
+    {
+        std::vector<char> buf(s.begin(), s.end());
+        buf.push_back(0);
+        g_output(buf.data(), g_output_param);
+    }
+    else
+    {
+        fputs(s.c_str(), stdout);
+        fflush(stdout);
+    }
+}
+
+void progress(const char *stage, int pct)
+{
+    std::lock_guard<std::mutex> lk(g_handler_mu);
+    if (g_progress)
+    {
+        std::string s(stage);
+        std::vector<char> buf(s.begin(), s.end());
+        buf.push_back(0);
+        g_progress(buf.data(), pct, g_progress_param);
+    }
+}
+
+// get_shape_volume (api_helpers.cpp:29-42)
+bool shape_dims(const hpgl_shape_t *sh, int *dims)
+{
+    if (!sh) return false;
+    long long v = 1;
+    for (int i = 0; i < 3; ++i)
+    {
+        dims[i] = sh->m_data[i];
+        v *= sh->m_data[i];
+    }
+    if (v > INT_MAX || v <= 0)
+    {
+        hb::set_error("get_shape_volume: grid volume exceeds INT_MAX");
+        return false;
+    }
+    return true;
+}
+
+hb::SkArgs sk_args_from(const hpgl_sk_params_t *p)
+{
+    hb::SkArgs a{};
+    a.cov_type = p->m_covariance_type;
+    for (int i = 0; i < 3; ++i)
+    {
+        a.ranges[i] = p->m_ranges[i];
+        a.angles[i] = p->m_angles[i];
+        a.radiuses[i] = p->m_radiuses[i];
+    }
+    a.sill = p->m_sill;
+    a.nugget = p->m_nugget;
+    a.max_nb = p->m_max_neighbours;
+    a.auto_mean = p->m_automatic_mean != 0;
+    a.mean = p->m_mean;
+    return a;
+}
+
+hb::SkArgs ok_args_from(const hpgl_ok_params_t *p)
+{
+    hb::SkArgs a{};
+    a.cov_type = p->m_covariance_type;
+    for (int i = 0; i < 3; ++i)
+    {
+        a.ranges[i] = p->m_ranges[i];
+        a.angles[i] = p->m_angles[i];
+        a.radiuses[i] = p->m_radiuses[i];
+    }
+    a.sill = p->m_sill;
+    a.nugget = p->m_nugget;
+    a.max_nb = p->m_max_neighbours;
+    a.auto_mean = false;
+    a.mean = 0;
+    return a;
+}
+
+hb::IkArgs ik_args_from(const hpgl_ik_params_t *p)
+{
+    hb::IkArgs a{};
+    a.cov_type = p->m_covariance_type;
+    for (int i = 0; i < 3; ++i)
+    {
+        a.ranges[i] = p->m_ranges[i];
+        a.angles[i] = p->m_angles[i];
+        a.radiuses[i] = p->m_radiuses[i];
+    }
+    a.sill = p->m_sill;
+    a.nugget = p->m_nugget;
+    a.max_nb = p->m_max_neighbours;
+    a.marginal = p->m_marginal_prob;
+    return a;
+}
+
+hb::Options options_from(const hpgl_b200_options_t *o)
+{
+    hb::Options r;
+    if (!o) return r;
+    r.precision = o->precision;
+    r.refine_steps = o->refine_steps;
+    r.flags = o->flags;
+    r.stream = o->stream;
+    r.estimate64 = o->estimate64;
+    r.variance = o->variance;
+    r.status = o->status;
+    r.ik_probs = o->ik_probs;
+    return r;
+}
+
+void report_done(const char *algo)
+{
+    hb::Stats s = hb::last_stats();
+    char buf[256];
+    double secs = s.total_ms / 1000.0;
+    snprintf(buf, sizeof(buf), "%s done on the GPU. Average speed: %.0f point/sec.\n", algo,
+             secs > 0 ? (double)s.kriged / secs : 0.0);
+    emit(buf);
+    progress(algo, 100);
+}
+} // namespace
+
+extern "C" {
+
+char *hpgl_get_last_exception_message(void) { return const_cast<char *>(hb::last_error()); }
+
+void hpgl_set_output_handler(int (*handler)(char *, void *), void *param)
+{
+    std::lock_guard<std::mutex> lk(g_handler_mu);
+    g_output = handler;
+    g_output_param = param;
+}
+
+void hpgl_set_progress_handler(int (*handler)(char *, int, void *), void *param)
+{
+    std::lock_guard<std::mutex> lk(g_handler_mu);
+    g_progress = handler;
+    g_progress_param = param;
+}
+
+void hpgl_set_thread_num(int n_threads) { hb::set_threads(n_threads); }
+int hpgl_get_thread_num(void) { return hb::get_threads(); }
+
+void hpgl_ordinary_kriging(hpgl_cont_masked_array_t *input_data, hpgl_ok_params_t *params,
+                           hpgl_cont_masked_array_t *output_data)
+{
+    if (!input_data || !params || !output_data)
+    {
+        hb::set_error("hpgl_ordinary_kriging: null argument");
+        return;
+    }
+    int dims[3];
+    if (!shape_dims(&input_data->m_shape, dims)) return;
+    hb::Options opt;
+    progress("Ordinary Kriging", 0);
+    if (hb::cont_kriging(0, dims, input_data->m_data, input_data->m_mask, ok_args_from(params), output_data->m_data,
+                         output_data->m_mask, opt) == 0)
+        report_done("Ordinary Kriging");
+}
+
+void hpgl_simple_kriging(float *input_data, unsigned char *input_mask, hpgl_shape_t *input_data_shape,
+                         hpgl_sk_params_t *params, float *output_data, unsigned char *output_mask,
+                         hpgl_shape_t *output_data_shape)
+{
+    (void)output_data_shape;
+    if (!params)
+    {
+        hb::set_error("hpgl_simple_kriging: null argument");
+        return;
+    }
+    int dims[3];
+    if (!shape_dims(input_data_shape, dims)) return;
+    hb::Options opt;
+    progress("Simple Kriging", 0);
+    if (hb::cont_kriging(1, dims, input_data, input_mask, sk_args_from(params), output_data, output_mask, opt) == 0)
+        report_done("Simple Kriging");
+}
+
+int hpgl_simple_kriging_weights(float *center_coords, float *neighbours_x, float *neighbours_y,
+                                float *neighbours_z, int neighbours_count, hpgl_cov_params_t *params,
+                                float *weights)
+{
+    if (!center_coords || !params || !weights || neighbours_count < 0)
+    {
+        hb::set_error("hpgl_simple_kriging_weights: bad argument");
+        return -1;
+    }
+    const int n = neighbours_count;
+    double c[3] = {center_coords[0], center_coords[1], center_coords[2]};
+    std::vector<double> xs(n), ys(n), zs(n), w(n);
+    for (int i = 0; i < n; ++i)
+    {
+        xs[i] = neighbours_x[i];
+        ys[i] = neighbours_y[i];
+        zs[i] = neighbours_z[i];
+    }
+    int rc = hb::sk_weights(c, xs.data(), ys.data(), zs.data(), n, params->m_covariance_type, params->m_ranges,
+                            params->m_angles, params->m_sill, params->m_nugget, w.data());
+    if (rc != 0) return -1;
+    for (int i = 0; i < n; ++i) weights[i] = (float)w[i];
+    return 0;
+}
+
+void hpgl_indicator_kriging(hpgl_ind_masked_array_t *in_data, hpgl_ind_masked_array_t *out_data,
+                            hpgl_ik_params_t *params, int indicator_count)
+{
+    if (!in_data || !out_data || !params || indicator_count <= 0)
+    {
+        hb::set_error("hpgl_indicator_kriging: bad argument");
+        return;
+    }
+    int dims[3], dims2[3];
+    if (!shape_dims(&in_data->m_shape, dims) || !shape_dims(&out_data->m_shape, dims2)) return;
+    if ((long long)dims[0] * dims[1] * dims[2] != (long long)dims2[0] * dims2[1] * dims2[2])
+    {
+        hb::set_error("hpgl_indicator_kriging: input and output size mismatch");
+        return;
+    }
+    std::vector<hb::IkArgs> cats;
+    for (int i = 0; i < indicator_count; ++i) cats.push_back(ik_args_from(params + i));
+    hb::Options opt;
+    progress("Indicator Kriging", 0);
+    if (hb::indicator_kriging(dims, in_data->m_data, in_data->m_mask, cats, out_data->m_data, out_data->m_mask,
+                              opt) == 0)
+        report_done("Indicator Kriging");
+}
+
+void hpgl_median_ik(hpgl_ind_masked_array_t *in_data, hpgl_median_ik_params_t *params,
+                    hpgl_ind_masked_array_t *out_data)
+{
+    if (!in_data || !out_data || !params)
+    {
+        hb::set_error("hpgl_median_ik: bad argument");
+        return;
+    }
+    int dims[3];
+    if (!shape_dims(&in_data->m_shape, dims)) return;
+    hb::IkArgs a{};
+    a.cov_type = params->m_covariance_type;
+    for (int i = 0; i < 3; ++i)
+    {
+        a.ranges[i] = params->m_ranges[i];
+        a.angles[i] = params->m_angles[i];
+        a.radiuses[i] = params->m_radiuses[i];
+    }
+    a.sill = params->m_sill;
+    a.nugget = params->m_nugget;
+    a.max_nb = params->m_max_neighbours;
+    a.marginal = params->m_marginal_probs[1];
+    hb::Options opt;
+    progress("Median IK", 0);
+    if (hb::median_ik(dims, in_data->m_data, in_data->m_mask, a, params->m_marginal_probs[1], out_data->m_data,
+                      out_data->m_mask, opt) == 0)
+        report_done("Median IK");
+}
+
+int hpgl_b200_cont_kriging_ex(int kind, const int *dims, const float *in_data, const unsigned char *in_mask,
+                              const hpgl_sk_params_t *params, float *out_data, unsigned char *out_mask,
+                              const hpgl_b200_options_t *opt)
+{
+    if (!params || (kind != 0 && kind != 1))
+    {
+        hb::set_error("hpgl_b200_cont_kriging_ex: bad argument");
+        return HPGL_B200_EINVAL;
+    }
+    return hb::cont_kriging(kind, dims, in_data, in_mask, sk_args_from(params), out_data, out_mask, options_from(opt));
+}
+
+int hpgl_b200_indicator_kriging_ex(const int *dims, const unsigned char *in_data, const unsigned char *in_mask,
+                                   const hpgl_ik_params_t *params, int indicator_count, unsigned char *out_data,
+                                   unsigned char *out_mask, const hpgl_b200_options_t *opt)
+{
+    if (!params || indicator_count <= 0)
+    {
+        hb::set_error("hpgl_b200_indicator_kriging_ex: bad argument");
+        return HPGL_B200_EINVAL;
+    }
+    std::vector<hb::IkArgs> cats;
+    for (int i = 0; i < indicator_count; ++i) cats.push_back(ik_args_from(params + i));
+    return hb::indicator_kriging(dims, in_data, in_mask, cats, out_data, out_mask, options_from(opt));
+}
+
+int hpgl_b200_median_ik_ex(const int *dims, const unsigned char *in_data, const unsigned char *in_mask,
+                           const hpgl_median_ik_params_t *params, unsigned char *out_data, unsigned char *out_mask,
+                           const hpgl_b200_options_t *opt)
+{
+    if (!params)
+    {
+        hb::set_error("hpgl_b200_median_ik_ex: bad argument");
+        return HPGL_B200_EINVAL;
+    }
+    hb::IkArgs a{};
+    a.cov_type = params->m_covariance_type;
+    for (int i = 0; i < 3; ++i)
+    {
+        a.ranges[i] = params->m_ranges[i];
+        a.angles[i] = params->m_angles[i];
+        a.radiuses[i] = params->m_radiuses[i];
+    }
+    a.sill = params->m_sill;
+    a.nugget = params->m_nugget;
+    a.max_nb = params->m_max_neighbours;
+    a.marginal = params->m_marginal_probs[1];
+    return hb::median_ik(dims, in_data, in_mask, a, params->m_marginal_probs[1], out_data, out_mask,
+                         options_from(opt));
+}
+
+int hpgl_b200_find_neighbours(int kind, const int *dims, const unsigned char *mask, const hpgl_sk_params_t *params,
+                              const int *nodes, int n_nodes, int *out_idx, int *out_count, unsigned char *out_path)
+{
+    if (!params || !dims || !mask || !nodes || !out_idx)
+    {
+        hb::set_error("hpgl_b200_find_neighbours: bad argument");
+        return HPGL_B200_EINVAL;
+    }
+    return hb::find_neighbours(kind, dims, mask, sk_args_from(params), nodes, n_nodes, out_idx, out_count, out_path);
+}
+
+int hpgl_b200_last_stats(double *out, int cap)
+{
+    hb::Stats s = hb::last_stats();
+    double v[9] = {s.total_ms, s.search_ms, s.solve_ms, (double)s.ties, (double)s.template_cells,
+                   (double)s.kriged, (double)s.launches, (double)s.h2d, (double)s.d2h};
+    int n = cap < 9 ? cap : 9;
+    for (int i = 0; i < n; ++i) out[i] = v[i];
+    return n;
+}
+
+void *hpgl_b200_host_alloc(size_t bytes) { return hb::host_alloc(bytes); }
+void hpgl_b200_host_free(void *p) { hb::host_free(p); }
+
+int hpgl_b200_transform(const double *ranges, const double *angles, double *out9)
+{
+    hb::CovModel m;
+    std::string err;
+    if (!hb::make_model(0, ranges, angles, 1.0, 0.0, m, err))
+    {
+        hb::set_error(err);
+        return HPGL_B200_EINVAL;
+    }
+    for (int i = 0; i < 9; ++i) out9[i] = m.T[i];
+    return 0;
+}
+
+int hpgl_b200_template(int kind, const hpgl_cov_params_t *cov, const int *radiuses, int *out, int cap,
+                       int *out_limit)
+{
+    if (!cov || !radiuses || (cap > 0 && !out))
+    {
+        hb::set_error("hpgl_b200_template: bad argument");
+        return HPGL_B200_EINVAL;
+    }
+    return hb::host_template(kind, cov->m_covariance_type, cov->m_ranges, cov->m_angles, cov->m_sill,
+                             cov->m_nugget, radiuses, out, cap, out_limit);
+}
+
+double hpgl_b200_covariance(int kind, const hpgl_cov_params_t *cov, const int *radiuses, const int *a, const int *b)
+{
+    return hb::host_covariance(kind, cov->m_covariance_type, cov->m_ranges, cov->m_angles, cov->m_sill,
+                               cov->m_nugget, radiuses, a, b);
+}
+
+const char *hpgl_b200_version(void) { return "hpgl_b200 0.1 (sm_100a)"; }
+
+} // extern "C"

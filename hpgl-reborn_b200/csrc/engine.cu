@@ -1,0 +1,872 @@
+// Engine: host orchestration of one kriging call on the GPU.
+//
+//   host  : validate, build the flavour's search template (std::sort, as the
+//           reference does), the selection-key table (exact double covariances
+//           and their dense descending ranks), geometry;
+//   device: upload, compact points, bin, search, resolve ties, bucket by
+//           neighbour count, solve per bucket, finalize; download.
+//
+// Device buffers are cached per engine (grow-only) so repeated calls do not
+// allocate. One engine per CUDA device, used under a mutex.
+#include "engine_api.h"
+#include "host_model.h"
+#include "kernels.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace hb
+{
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_last_error;
+static std::string g_last_error_global;
+static std::mutex g_err_mu;
+
+void set_error(const std::string &msg)
+{
+    g_last_error = msg;
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    g_last_error_global = msg;
+}
+const char *last_error()
+{
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    static std::string copy;
+    copy = g_last_error_global;
+    return copy.c_str();
+}
+
+struct CudaFail
+{
+    int code;
+    std::string msg;
+};
+
+#define HB_CK(expr)                                                                                            \
+    do                                                                                                         \
+    {                                                                                                          \
+        cudaError_t _e = (expr);                                                                               \
+        if (_e != cudaSuccess)                                                                                 \
+            throw CudaFail{_e == cudaErrorMemoryAllocation ? -3 : -2,                                          \
+                           std::string(#expr) + ": " + cudaGetErrorString(_e)};                                \
+    } while (0)
+
+// ------------------------------------------------------------------ buffers
+struct DevBuf
+{
+    void *p = nullptr;
+    size_t cap = 0;
+};
+
+class Engine
+{
+  public:
+    explicit Engine(int dev) : device_(dev)
+    {
+        HB_CK(cudaSetDevice(dev));
+        HB_CK(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking));
+        cudaDeviceProp prop;
+        HB_CK(cudaGetDeviceProperties(&prop, dev));
+        n_sm_ = prop.multiProcessorCount;
+        max_smem_ = (int)prop.sharedMemPerBlockOptin;
+        for (int i = 0; i < kNumEvents; ++i) HB_CK(cudaEventCreate(&ev_[i]));
+    }
+
+    template <typename T>
+    T *buf(const char *name, size_t count)
+    {
+        DevBuf &b = bufs_[name];
+        size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+        if (b.cap < bytes)
+        {
+            if (b.p) cudaFree(b.p);
+            b.p = nullptr;
+            b.cap = 0;
+            size_t want = bytes + bytes / 8;
+            HB_CK(cudaMalloc(&b.p, want));
+            b.cap = want;
+        }
+        return reinterpret_cast<T *>(b.p);
+    }
+
+    int n_sm() const { return n_sm_; }
+    int max_smem() const { return max_smem_; }
+    cudaStream_t stream(const void *user) const { return user ? (cudaStream_t)user : own_stream_; }
+    static constexpr int kNumEvents = 8;
+    cudaEvent_t ev_[kNumEvents];
+    Stats stats;
+
+  private:
+    int device_;
+    cudaStream_t own_stream_ = nullptr;
+    int n_sm_ = 148;
+    int max_smem_ = 227 * 1024;
+    std::map<std::string, DevBuf> bufs_;
+};
+
+static std::mutex g_engine_mu;
+static std::map<int, std::unique_ptr<Engine>> g_engines;
+static int g_threads = 0;
+
+void set_threads(int n) { g_threads = n; }
+int get_threads() { return clamp_threads(g_threads); }
+
+static Engine &engine_for_current_device()
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) throw CudaFail{-2, std::string("no usable CUDA device: ") + cudaGetErrorString(e)};
+    int n = 0;
+    e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) throw CudaFail{-2, "no usable CUDA device"};
+    auto it = g_engines.find(dev);
+    if (it == g_engines.end()) it = g_engines.emplace(dev, std::make_unique<Engine>(dev)).first;
+    return *it->second;
+}
+
+// ------------------------------------------------------------------ plan
+struct Plan
+{
+    Flavour f;
+    std::vector<Offset> tmpl;
+    KeyTable kt;
+    Geom g;
+    int rank_bits = 0;
+};
+
+static int bits_for(uint32_t max_value)
+{
+    int b = 0;
+    while (b < 32 && (max_value >> b) != 0) ++b;
+    return b;
+}
+
+static void check_model_args(int cov_type, const double *ranges, const double *angles, double sill, double nugget,
+                             const int *radiuses, int k)
+{
+    for (int i = 0; i < 3; ++i)
+    {
+        if (!std::isfinite(ranges[i]) || !std::isfinite(angles[i]))
+            throw CudaFail{-1, "ranges and angles must be finite"};
+        if (radiuses[i] <= 0)
+            throw CudaFail{-1, "search radiuses must be positive integers (a zero radius makes the reference's "
+                               "clusterizer index out of range)"};
+        if (radiuses[i] > 4096) throw CudaFail{-4, "search radius above 4096 is not supported"};
+    }
+    if (!std::isfinite(sill) || !std::isfinite(nugget)) throw CudaFail{-1, "sill and nugget must be finite"};
+    // a negative sill makes the strict C(0)/100 threshold negative, so zero
+    // (out-of-box) covariances would pass it; the reference's validation
+    // rejects it too (validation.py:397-430)
+    if (sill < 0) throw CudaFail{-1, "sill must be >= 0"};
+    if (k < 1) throw CudaFail{-1, "max_neighbours must be >= 1"};
+    if (k > 1024) throw CudaFail{-4, "max_neighbours above 1024 is not supported"};
+    if (cov_type < 0 || cov_type > 2) throw CudaFail{-1, "unknown covariance type"};
+}
+
+static long long check_dims(const int *dims)
+{
+    if (!dims) throw CudaFail{-1, "null dims"};
+    long long n = (long long)dims[0] * dims[1] * dims[2];
+    if (dims[0] <= 0 || dims[1] <= 0 || dims[2] <= 0 || n > 2147483647LL)
+        throw CudaFail{-1, "get_shape_volume: grid volume exceeds INT_MAX"};
+    if (dims[0] >= (1 << 21) || dims[1] >= (1 << 21) || dims[2] >= (1 << 21))
+        throw CudaFail{-4, "grid axis longer than 2^21 cells is not supported"};
+    return n;
+}
+
+static Plan make_plan(bool truncated, int cov_type, const double *ranges, const double *angles, double sill,
+                      double nugget, const int *radiuses, int k, const int *dims)
+{
+    check_model_args(cov_type, ranges, angles, sill, nugget, radiuses, k);
+    Plan pl;
+    std::string err;
+    if (!make_model(cov_type, ranges, angles, sill, nugget, pl.f.m, err)) throw CudaFail{-1, err};
+    pl.f.truncated = truncated;
+    for (int a = 0; a < 3; ++a) pl.f.r[a] = radiuses[a];
+    pl.tmpl = build_template(pl.f);
+    build_key_table(pl.f, pl.kt, g_threads);
+    pl.rank_bits = pl.kt.n_ranks > 1 ? bits_for(pl.kt.n_ranks - 1) : 0;
+
+    Geom &g = pl.g;
+    g.nx = dims[0];
+    g.ny = dims[1];
+    g.nz = dims[2];
+    g.n_cells = (long long)dims[0] * dims[1] * dims[2];
+    g.rx = radiuses[0];
+    g.ry = radiuses[1];
+    g.rz = radiuses[2];
+    // clusterizer.cpp:87-89: bins per axis = (int)(g / (double)r + 2)
+    g.bx = (int)(g.nx / (double)g.rx + 2);
+    g.by = (int)(g.ny / (double)g.ry + 2);
+    g.bz = (int)(g.nz / (double)g.rz + 2);
+    long long nb = (long long)g.bx * g.by * g.bz;
+    if (nb > (1LL << 30)) throw CudaFail{-4, "too many search bins"};
+    g.n_bins = (int)nb;
+    g.limit = (int)(pl.tmpl.size() / 250);
+    g.k = k;
+    g.khx = pl.kt.half[0];
+    g.khy = pl.kt.half[1];
+    g.khz = pl.kt.half[2];
+    g.knx = pl.kt.n[0];
+    g.kny = pl.kt.n[1];
+    int ph[3];
+    for (int a = 0; a < 3; ++a) ph[a] = truncated ? 2 * radiuses[a] : 4 * radiuses[a] - 2;
+    for (int a = 0; a < 3; ++a) ph[a] = std::max(ph[a], pl.kt.half[a]);
+    g.phx = ph[0];
+    g.phy = ph[1];
+    g.phz = ph[2];
+    g.pnx = 2 * ph[0] + 1;
+    g.pny = 2 * ph[1] + 1;
+    long long pn = (long long)g.pnx * g.pny * (2 * ph[2] + 1);
+    if (pn > (1LL << 31) - 1) throw CudaFail{-4, "covariance table too large for these radiuses"};
+    g.pair_center = ((long long)ph[2] * g.pny + ph[1]) * g.pnx + ph[0];
+    return pl;
+}
+
+static DevModel dev_model(const CovModel &m)
+{
+    DevModel d;
+    d.type = m.type;
+    d.r0 = m.ranges[0];
+    d.sill = m.sill;
+    d.nugget = m.nugget;
+    for (int i = 0; i < 9; ++i) d.T[i] = m.T[i];
+    return d;
+}
+
+// ------------------------------------------------------------------ stages
+struct DevPoints
+{
+    int *n_pts = nullptr; // device scalar
+    int m = 0;            // host copy
+    int *pts_node = nullptr;
+    unsigned long long *pts_xyz = nullptr;
+    float *pts_val = nullptr;
+    uint8_t *pts_cat = nullptr;
+    int *pid_of_node = nullptr;
+};
+
+static DevPoints compact_points(Engine &E, const Geom &g, const uint8_t *d_mask, const float *d_val_f,
+                                const uint8_t *d_val_u8, cudaStream_t st)
+{
+    DevPoints P;
+    long long n = g.n_cells;
+    int *pos = E.buf<int>("pos", (size_t)n);
+    int *tmp = E.buf<int>("scan_tmp", (size_t)scan_tmp_ints(n) + 4);
+    P.n_pts = E.buf<int>("n_pts", 1);
+    launch_flag_informed(d_mask, n, pos, st);
+    exclusive_scan(pos, n, tmp, P.n_pts, st);
+    HB_CK(cudaGetLastError());
+    HB_CK(cudaMemcpyAsync(&P.m, P.n_pts, sizeof(int), cudaMemcpyDeviceToHost, st));
+    HB_CK(cudaStreamSynchronize(st));
+    size_t m = std::max(P.m, 1);
+    P.pts_node = E.buf<int>("pts_node", m);
+    P.pts_xyz = E.buf<unsigned long long>("pts_xyz", m);
+    if (d_val_f) P.pts_val = E.buf<float>("pts_val", m);
+    if (d_val_u8) P.pts_cat = E.buf<uint8_t>("pts_cat", m);
+    P.pid_of_node = E.buf<int>("pid_of_node", (size_t)n);
+    launch_emit_points(d_mask, pos, g, d_val_f, d_val_u8, P.pts_node, P.pts_xyz, P.pts_val, P.pts_cat,
+                       P.pid_of_node, st);
+    HB_CK(cudaGetLastError());
+    return P;
+}
+
+struct DevSearch
+{
+    int *nb_pid = nullptr;
+    int *nb_n = nullptr;
+    uint8_t *bin_flag = nullptr;
+    double *search_vals = nullptr;
+    double *pair64 = nullptr;
+    float *pair32 = nullptr;
+    int ties = 0;
+    int template_cells = 0;
+};
+
+// Search for one flavour; `all_cells` selects every cell (IK) or only the
+// uninformed ones. Table slots are suffixed with `tag` so several flavours can
+// coexist (IK categories run one after another and reuse them).
+static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const uint8_t *d_mask, int all_cells,
+                            cudaStream_t st)
+{
+    const Geom &g = pl.g;
+    DevSearch S;
+    // tables
+    uint32_t *keytab = E.buf<uint32_t>("keytab", pl.kt.rank.size());
+    S.search_vals = E.buf<double>("search_vals", pl.kt.vals.size());
+    HB_CK(cudaMemcpyAsync(keytab, pl.kt.rank.data(), pl.kt.rank.size() * 4, cudaMemcpyHostToDevice, st));
+    HB_CK(cudaMemcpyAsync(S.search_vals, pl.kt.vals.data(), pl.kt.vals.size() * 8, cudaMemcpyHostToDevice, st));
+    std::vector<int4> t4(std::max<size_t>(pl.tmpl.size(), 1));
+    for (size_t i = 0; i < pl.tmpl.size(); ++i) t4[i] = make_int4(pl.tmpl[i].dx, pl.tmpl[i].dy, pl.tmpl[i].dz, 0);
+    int4 *tmpl = E.buf<int4>("tmpl", t4.size());
+    HB_CK(cudaMemcpyAsync(tmpl, t4.data(), t4.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+    long long pn = (long long)g.pnx * g.pny * (2 * g.phz + 1);
+    S.pair64 = E.buf<double>("pair64", (size_t)pn);
+    S.pair32 = E.buf<float>("pair32", (size_t)pn);
+    launch_build_pair(g, dev_model(pl.f.m), pl.f.truncated ? 1 : 0, S.search_vals, S.pair64, S.pair32, st);
+
+    // bins
+    int *bin_cnt = E.buf<int>("bin_cnt", g.n_bins);
+    int *bin_start = E.buf<int>("bin_start", g.n_bins);
+    int *bin_fill = E.buf<int>("bin_fill", g.n_bins);
+    S.bin_flag = E.buf<uint8_t>("bin_flag", g.n_bins);
+    int *bin_pts = E.buf<int>("bin_pts", std::max(P.m, 1));
+    int *scal = E.buf<int>("scalars", 8); // 0 total, 1 max_cand, 2 tmpl bins, 3 ties, 4 tmpl cells
+    int *tmp = E.buf<int>("scan_tmp2", (size_t)scan_tmp_ints(g.n_bins) + 4);
+    HB_CK(cudaMemsetAsync(bin_cnt, 0, sizeof(int) * g.n_bins, st));
+    HB_CK(cudaMemsetAsync(bin_fill, 0, sizeof(int) * g.n_bins, st));
+    HB_CK(cudaMemsetAsync(scal, 0, sizeof(int) * 8, st));
+    launch_bin_count(P.pts_xyz, P.n_pts, g, bin_cnt, st);
+    HB_CK(cudaMemcpyAsync(bin_start, bin_cnt, sizeof(int) * g.n_bins, cudaMemcpyDeviceToDevice, st));
+    exclusive_scan(bin_start, g.n_bins, tmp, scal + 0, st);
+    launch_bin_fill(P.pts_xyz, P.n_pts, g, bin_start, bin_fill, bin_pts, st);
+    launch_bin_sort(g, bin_start, bin_cnt, bin_pts, S.bin_flag, st);
+    launch_bin_region(g, S.bin_flag, bin_cnt, scal + 1, scal + 2, st);
+    HB_CK(cudaGetLastError());
+    int host_scal[8];
+    HB_CK(cudaMemcpyAsync(host_scal, scal, sizeof(host_scal), cudaMemcpyDeviceToHost, st));
+    HB_CK(cudaStreamSynchronize(st));
+    int max_cand = host_scal[1];
+
+    // search
+    int cand_cap = std::max(4, (max_cand + 3) / 4 * 4);
+    int warps = 8;
+    while (warps > 1 && search_smem_bytes(cand_cap, g.k, warps) > (size_t)E.max_smem()) --warps;
+    if (search_smem_bytes(cand_cap, g.k, warps) > (size_t)E.max_smem())
+        throw CudaFail{-4, "neighbour candidate list too long for shared memory (" + std::to_string(max_cand) +
+                               " candidates)"};
+    S.nb_pid = E.buf<int>("nb_pid", (size_t)g.n_cells * g.k);
+    S.nb_n = E.buf<int>("nb_n", (size_t)g.n_cells);
+    int *tie_cells = E.buf<int>("tie_cells", (size_t)g.n_cells);
+    HB_CK(cudaMemsetAsync(S.nb_n, 0, sizeof(int) * g.n_cells, st));
+    HB_CK(launch_search(g, d_mask, all_cells, bin_start, bin_cnt, S.bin_flag, bin_pts, P.pts_xyz, keytab,
+                        pl.rank_bits, tmpl, (int)pl.tmpl.size(), P.pid_of_node, cand_cap, warps, S.nb_pid, S.nb_n,
+                        tie_cells, scal + 3, scal + 4, st));
+    HB_CK(cudaMemcpyAsync(host_scal, scal, sizeof(host_scal), cudaMemcpyDeviceToHost, st));
+    HB_CK(cudaStreamSynchronize(st));
+    S.ties = host_scal[3];
+    S.template_cells = host_scal[4];
+    E.stats.launches += 8;
+
+    // tie groups straddling the k-th slot: exact std::sort permutation
+    if (S.ties > 0)
+    {
+        int cap = std::max(max_cand, 1);
+        size_t per = (size_t)cap * tie_entry_bytes();
+        size_t budget = (size_t)512 << 20;
+        int chunk = (int)std::max<size_t>(1, std::min<size_t>(budget / per, (size_t)S.ties));
+        void *scratch = E.buf<unsigned char>("tie_scratch", per * chunk);
+        for (int first = 0; first < S.ties; first += chunk)
+        {
+            launch_resolve_ties(g, tie_cells, scal + 3, first, chunk, bin_start, bin_cnt, bin_pts, P.pts_xyz,
+                                keytab, scratch, cap, S.nb_pid, st);
+            E.stats.launches += 1;
+        }
+        HB_CK(cudaGetLastError());
+    }
+    return S;
+}
+
+// Solve every bucket for one search result.
+static void run_solves(Engine &E, const Plan &pl, const DevPoints &P, const DevSearch &S, const uint8_t *d_mask,
+                       int all_cells, bool ordinary, int precision, int steps, double mean, int ind_value,
+                       signed char *d_status, const SolveOut &out, cudaStream_t st)
+{
+    const Geom &g = pl.g;
+    int *bucket_cnt = E.buf<int>("bucket_cnt", kBuckets);
+    int *bucket_off = E.buf<int>("bucket_off", kBuckets + 1);
+    int *bucket_fill = E.buf<int>("bucket_fill", kBuckets);
+    int *cells = E.buf<int>("cells", (size_t)g.n_cells);
+    launch_prepare(g, d_mask, all_cells, S.nb_n, d_status, bucket_cnt, bucket_off, bucket_fill, cells, st);
+    HB_CK(cudaGetLastError());
+    int cnt[kBuckets];
+    HB_CK(cudaMemcpyAsync(cnt, bucket_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, st));
+    HB_CK(cudaStreamSynchronize(st));
+    int off = 0;
+    const double c0 = pl.f.c0();
+    for (int b = 0; b < kBuckets; ++b)
+    {
+        if (cnt[b] > 0)
+        {
+            const int *bcells = cells + off;
+            // bucket item counts live in bucket_cnt[b]
+            if (b < 4)
+            {
+                HB_CK(launch_solve_bucket(kBucketNP[b], precision, ordinary, g, bcells, bucket_cnt + b, cnt[b],
+                                          S.nb_pid, S.nb_n, P.pts_xyz, P.pts_val, P.pts_cat, ind_value, S.pair64,
+                                          S.pair32, mean, c0, steps, out, E.n_sm(), st));
+            }
+            else
+            {
+                int blocks = std::min(cnt[b], E.n_sm() * 2);
+                double *scratch = E.buf<double>("large_scratch", large_scratch_doubles(g.k, blocks));
+                HB_CK(launch_solve_large(g, bcells, bucket_cnt + b, blocks, S.nb_pid, S.nb_n, P.pts_xyz, P.pts_val,
+                                         P.pts_cat, ind_value, S.pair64, ordinary, mean, c0, scratch, out, st));
+            }
+            E.stats.launches += 1;
+            E.stats.kriged += cnt[b];
+        }
+        off += cnt[b];
+    }
+    E.stats.launches += 3;
+}
+
+// ------------------------------------------------------------------ io helpers
+struct IoPlan
+{
+    bool device;
+    cudaStream_t st;
+};
+
+template <typename T>
+static T *to_device(Engine &E, const char *slot, const T *src, size_t n, const IoPlan &io)
+{
+    if (io.device) return const_cast<T *>(src);
+    T *d = E.buf<T>(slot, n);
+    HB_CK(cudaMemcpyAsync(d, src, n * sizeof(T), cudaMemcpyHostToDevice, io.st));
+    E.stats.h2d += n * sizeof(T);
+    return d;
+}
+
+template <typename T>
+static void to_host(Engine &E, T *dst, const T *dsrc, size_t n, const IoPlan &io)
+{
+    if (io.device || dst == dsrc) return;
+    HB_CK(cudaMemcpyAsync(dst, dsrc, n * sizeof(T), cudaMemcpyDeviceToHost, io.st));
+    E.stats.d2h += n * sizeof(T);
+}
+
+static void begin_call(Engine &E, cudaStream_t st)
+{
+    E.stats = Stats();
+    HB_CK(cudaEventRecord(E.ev_[0], st));
+}
+static void end_call(Engine &E, cudaStream_t st)
+{
+    HB_CK(cudaEventRecord(E.ev_[1], st));
+    HB_CK(cudaEventSynchronize(E.ev_[1]));
+    float ms = 0;
+    HB_CK(cudaEventElapsedTime(&ms, E.ev_[0], E.ev_[1]));
+    E.stats.total_ms = ms;
+}
+
+// ------------------------------------------------------------------ entry points
+int cont_kriging(int kind, const int *dims, const float *in_data, const unsigned char *in_mask,
+                 const SkArgs &a, float *out_data, unsigned char *out_mask, const Options &opt)
+{
+    std::lock_guard<std::mutex> lk(g_engine_mu);
+    try
+    {
+        if (!dims || !in_data || !in_mask || !out_data || !out_mask) throw CudaFail{-1, "null array argument"};
+        long long n = check_dims(dims);
+        const bool simple = kind == 1;
+        Plan pl = make_plan(simple, a.cov_type, a.ranges, a.angles, a.sill, a.nugget, a.radiuses, a.max_nb, dims);
+        Engine &E = engine_for_current_device();
+        cudaStream_t st = E.stream(opt.stream);
+        IoPlan io{(opt.flags & 1u) != 0, st};
+        begin_call(E, st);
+
+        const float *d_in = to_device(E, "in_data", in_data, (size_t)n, io);
+        const uint8_t *d_mask = to_device(E, "in_mask", in_mask, (size_t)n, io);
+        float *d_out = io.device ? out_data : E.buf<float>("out_data", (size_t)n);
+        uint8_t *d_omask = io.device ? out_mask : E.buf<uint8_t>("out_mask", (size_t)n);
+        if (!io.device)
+        {
+            if (opt.flags & 2u)
+            {
+                HB_CK(cudaMemcpyAsync(d_out, d_in, n * 4, cudaMemcpyDeviceToDevice, st));
+                HB_CK(cudaMemcpyAsync(d_omask, d_mask, n, cudaMemcpyDeviceToDevice, st));
+            }
+            else
+            {
+                HB_CK(cudaMemcpyAsync(d_out, out_data, n * 4, cudaMemcpyHostToDevice, st));
+                HB_CK(cudaMemcpyAsync(d_omask, out_mask, n, cudaMemcpyHostToDevice, st));
+                E.stats.h2d += n * 5;
+            }
+        }
+        double *d_est = nullptr, *d_var = nullptr;
+        signed char *d_status = nullptr;
+        if (opt.estimate64) d_est = io.device ? opt.estimate64 : E.buf<double>("est64", (size_t)n);
+        if (opt.variance) d_var = io.device ? opt.variance : E.buf<double>("var", (size_t)n);
+        d_status = (io.device && opt.status) ? opt.status : E.buf<signed char>("status", (size_t)n);
+
+        // SK mean: calc_mean over informed cells (calc_mean.cpp:6-30), on the host data
+        double mean = 0.0;
+        if (simple)
+        {
+            if (a.auto_mean)
+            {
+                std::vector<float> hv;
+                std::vector<uint8_t> hm;
+                const float *pv = in_data;
+                const uint8_t *pm = in_mask;
+                if (io.device)
+                {
+                    hv.resize(n);
+                    hm.resize(n);
+                    HB_CK(cudaMemcpyAsync(hv.data(), in_data, n * 4, cudaMemcpyDeviceToHost, st));
+                    HB_CK(cudaMemcpyAsync(hm.data(), in_mask, n, cudaMemcpyDeviceToHost, st));
+                    HB_CK(cudaStreamSynchronize(st));
+                    pv = hv.data();
+                    pm = hm.data();
+                }
+                double sum = 0;
+                long long cnt = 0;
+                for (long long i = 0; i < n; ++i)
+                    if (pm[i])
+                    {
+                        sum += pv[i];
+                        cnt += 1;
+                    }
+                mean = cnt ? sum / cnt : 0.0;
+            }
+            else
+                mean = a.mean;
+        }
+
+        HB_CK(cudaEventRecord(E.ev_[2], st));
+        DevPoints P = compact_points(E, pl.g, d_mask, d_in, nullptr, st);
+        DevSearch S = run_search(E, pl, P, d_mask, 0, st);
+        HB_CK(cudaEventRecord(E.ev_[3], st));
+        SolveOut so{};
+        so.out_data = d_out;
+        so.out_mask = d_omask;
+        so.est64 = d_est;
+        so.var = d_var;
+        so.status = d_status;
+        so.write_cont = 1;
+        int steps = opt.refine_steps > 0 ? opt.refine_steps : 2;
+        run_solves(E, pl, P, S, d_mask, 0, !simple, opt.precision, steps, mean, -1, d_status, so, st);
+        launch_finalize_cont(pl.g, d_in, d_status, simple ? 1 : 0, (float)mean, d_out, d_omask, d_est, d_var, st);
+        HB_CK(cudaGetLastError());
+        HB_CK(cudaEventRecord(E.ev_[4], st));
+
+        to_host(E, out_data, d_out, (size_t)n, io);
+        to_host(E, out_mask, d_omask, (size_t)n, io);
+        if (opt.estimate64) to_host(E, opt.estimate64, d_est, (size_t)n, io);
+        if (opt.variance) to_host(E, opt.variance, d_var, (size_t)n, io);
+        if (opt.status) to_host(E, opt.status, d_status, (size_t)n, io);
+        end_call(E, st);
+        float ms_search = 0, ms_solve = 0;
+        cudaEventElapsedTime(&ms_search, E.ev_[2], E.ev_[3]);
+        cudaEventElapsedTime(&ms_solve, E.ev_[3], E.ev_[4]);
+        E.stats.search_ms = ms_search;
+        E.stats.solve_ms = ms_solve;
+        E.stats.ties = S.ties;
+        E.stats.template_cells = S.template_cells;
+        return 0;
+    }
+    catch (const CudaFail &f)
+    {
+        set_error(f.msg);
+        return f.code;
+    }
+    catch (const std::exception &ex)
+    {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+int indicator_kriging(const int *dims, const unsigned char *in_data, const unsigned char *in_mask,
+                      const std::vector<IkArgs> &cats, unsigned char *out_data, unsigned char *out_mask,
+                      const Options &opt)
+{
+    std::lock_guard<std::mutex> lk(g_engine_mu);
+    try
+    {
+        if (!dims || !in_data || !in_mask || !out_data || !out_mask) throw CudaFail{-1, "null array argument"};
+        long long n = check_dims(dims);
+        const int m = (int)cats.size();
+        if (m < 1) throw CudaFail{-1, "indicator_count must be positive"};
+        Engine &E = engine_for_current_device();
+        cudaStream_t st = E.stream(opt.stream);
+        IoPlan io{(opt.flags & 1u) != 0, st};
+        begin_call(E, st);
+        const uint8_t *d_in = to_device(E, "in_u8", in_data, (size_t)n, io);
+        const uint8_t *d_mask = to_device(E, "in_mask", in_mask, (size_t)n, io);
+        uint8_t *d_out = io.device ? out_data : E.buf<uint8_t>("out_u8", (size_t)n);
+        uint8_t *d_omask = io.device ? out_mask : E.buf<uint8_t>("out_mask", (size_t)n);
+        float *d_probs = (io.device && opt.ik_probs) ? opt.ik_probs : E.buf<float>("ik_probs", (size_t)n * m);
+        signed char *d_status = E.buf<signed char>("status", (size_t)n);
+        HB_CK(cudaEventRecord(E.ev_[2], st));
+        Plan pl0 = make_plan(true, cats[0].cov_type, cats[0].ranges, cats[0].angles, cats[0].sill, cats[0].nugget,
+                             cats[0].radiuses, cats[0].max_nb, dims);
+        DevPoints P = compact_points(E, pl0.g, d_mask, nullptr, d_in, st);
+        float search_ms = 0, solve_ms = 0;
+        for (int c = 0; c < m; ++c)
+        {
+            const IkArgs &a = cats[c];
+            Plan pl = c == 0 ? pl0
+                             : make_plan(true, a.cov_type, a.ranges, a.angles, a.sill, a.nugget, a.radiuses, a.max_nb,
+                                         dims);
+            HB_CK(cudaEventRecord(E.ev_[5], st));
+            DevSearch S = run_search(E, pl, P, d_mask, 1, st);
+            HB_CK(cudaEventRecord(E.ev_[6], st));
+            SolveOut so{};
+            so.status = d_status;
+            so.prob = d_probs + c;
+            so.prob_stride = m;
+            // marginal stored as float (ik_params.h:20); the mean provider widens it back
+            const float mc = (float)a.marginal;
+            run_solves(E, pl, P, S, d_mask, 1, false, opt.precision, opt.refine_steps > 0 ? opt.refine_steps : 2,
+                       (double)mc, c, d_status, so, st);
+            launch_ik_fail_fill(pl.g, d_status, mc, c, m, d_probs, st);
+            HB_CK(cudaEventRecord(E.ev_[7], st));
+            HB_CK(cudaEventSynchronize(E.ev_[7]));
+            float a1 = 0, a2 = 0;
+            cudaEventElapsedTime(&a1, E.ev_[5], E.ev_[6]);
+            cudaEventElapsedTime(&a2, E.ev_[6], E.ev_[7]);
+            search_ms += a1;
+            solve_ms += a2;
+            E.stats.ties += S.ties;
+            E.stats.template_cells += S.template_cells;
+        }
+        launch_ik_finalize(n, m, d_probs, d_out, d_omask, st);
+        HB_CK(cudaGetLastError());
+        to_host(E, out_data, d_out, (size_t)n, io);
+        to_host(E, out_mask, d_omask, (size_t)n, io);
+        if (opt.ik_probs) to_host(E, opt.ik_probs, d_probs, (size_t)n * m, io);
+        end_call(E, st);
+        E.stats.search_ms = search_ms;
+        E.stats.solve_ms = solve_ms;
+        return 0;
+    }
+    catch (const CudaFail &f)
+    {
+        set_error(f.msg);
+        return f.code;
+    }
+    catch (const std::exception &ex)
+    {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+int median_ik(const int *dims, const unsigned char *in_data, const unsigned char *in_mask, const IkArgs &a,
+              double marginal1, unsigned char *out_data, unsigned char *out_mask, const Options &opt)
+{
+    std::lock_guard<std::mutex> lk(g_engine_mu);
+    try
+    {
+        if (!dims || !in_data || !in_mask || !out_data || !out_mask) throw CudaFail{-1, "null array argument"};
+        long long n = check_dims(dims);
+        Plan pl = make_plan(true, a.cov_type, a.ranges, a.angles, a.sill, a.nugget, a.radiuses, a.max_nb, dims);
+        Engine &E = engine_for_current_device();
+        cudaStream_t st = E.stream(opt.stream);
+        IoPlan io{(opt.flags & 1u) != 0, st};
+        begin_call(E, st);
+        const uint8_t *d_in = to_device(E, "in_u8", in_data, (size_t)n, io);
+        const uint8_t *d_mask = to_device(E, "in_mask", in_mask, (size_t)n, io);
+        uint8_t *d_out = io.device ? out_data : E.buf<uint8_t>("out_u8", (size_t)n);
+        uint8_t *d_omask = io.device ? out_mask : E.buf<uint8_t>("out_mask", (size_t)n);
+        signed char *d_status = E.buf<signed char>("status", (size_t)n);
+        double *d_est = E.buf<double>("est64", (size_t)n);
+        float *d_prob = opt.ik_probs ? ((io.device) ? opt.ik_probs : E.buf<float>("ik_probs", (size_t)n)) : nullptr;
+        HB_CK(cudaEventRecord(E.ev_[2], st));
+        DevPoints P = compact_points(E, pl.g, d_mask, nullptr, d_in, st);
+        DevSearch S = run_search(E, pl, P, d_mask, 1, st);
+        HB_CK(cudaEventRecord(E.ev_[3], st));
+        SolveOut so{};
+        so.status = d_status;
+        so.est64 = d_est;
+        run_solves(E, pl, P, S, d_mask, 1, false, opt.precision, opt.refine_steps > 0 ? opt.refine_steps : 2,
+                   marginal1, 1, d_status, so, st);
+        launch_mik_finalize(n, d_status, d_est, marginal1, d_out, d_omask, d_prob, st);
+        HB_CK(cudaGetLastError());
+        HB_CK(cudaEventRecord(E.ev_[4], st));
+        to_host(E, out_data, d_out, (size_t)n, io);
+        to_host(E, out_mask, d_omask, (size_t)n, io);
+        if (opt.ik_probs) to_host(E, opt.ik_probs, d_prob, (size_t)n, io);
+        end_call(E, st);
+        float a1 = 0, a2 = 0;
+        cudaEventElapsedTime(&a1, E.ev_[2], E.ev_[3]);
+        cudaEventElapsedTime(&a2, E.ev_[3], E.ev_[4]);
+        E.stats.search_ms = a1;
+        E.stats.solve_ms = a2;
+        E.stats.ties = S.ties;
+        E.stats.template_cells = S.template_cells;
+        return 0;
+    }
+    catch (const CudaFail &f)
+    {
+        set_error(f.msg);
+        return f.code;
+    }
+    catch (const std::exception &ex)
+    {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+int find_neighbours(int kind, const int *dims, const unsigned char *mask, const SkArgs &a, const int *nodes,
+                    int n_nodes, int *out_idx, int *out_count, unsigned char *out_path)
+{
+    std::lock_guard<std::mutex> lk(g_engine_mu);
+    try
+    {
+        long long n = check_dims(dims);
+        Plan pl = make_plan(kind != 0, a.cov_type, a.ranges, a.angles, a.sill, a.nugget, a.radiuses, a.max_nb, dims);
+        Engine &E = engine_for_current_device();
+        cudaStream_t st = E.stream(nullptr);
+        IoPlan io{false, st};
+        begin_call(E, st);
+        const uint8_t *d_mask = to_device(E, "in_mask", mask, (size_t)n, io);
+        DevPoints P = compact_points(E, pl.g, d_mask, nullptr, nullptr, st);
+        DevSearch S = run_search(E, pl, P, d_mask, 1, st);
+        std::vector<int> nb_n(n), pts(std::max(P.m, 1));
+        std::vector<uint8_t> flags(pl.g.n_bins);
+        HB_CK(cudaMemcpyAsync(nb_n.data(), S.nb_n, n * 4, cudaMemcpyDeviceToHost, st));
+        HB_CK(cudaMemcpyAsync(pts.data(), P.pts_node, pts.size() * 4, cudaMemcpyDeviceToHost, st));
+        HB_CK(cudaMemcpyAsync(flags.data(), S.bin_flag, flags.size(), cudaMemcpyDeviceToHost, st));
+        std::vector<int> lst((size_t)pl.g.k);
+        for (int t = 0; t < n_nodes; ++t)
+        {
+            int node = nodes[t];
+            if (node < 0 || node >= n) throw CudaFail{-1, "node index out of range"};
+            HB_CK(cudaMemcpyAsync(lst.data(), S.nb_pid + (size_t)node * pl.g.k, pl.g.k * 4, cudaMemcpyDeviceToHost,
+                                  st));
+            HB_CK(cudaStreamSynchronize(st));
+            int cnt = nb_n[node];
+            if (out_count) out_count[t] = cnt;
+            for (int i = 0; i < pl.g.k; ++i) out_idx[(size_t)t * pl.g.k + i] = i < cnt ? pts[lst[i]] : -1;
+            if (out_path)
+            {
+                int x = node % dims[0], y = node % (dims[0] * dims[1]) / dims[0], z = node / (dims[0] * dims[1]);
+                int b = ((z / pl.g.rz) * pl.g.by + (y / pl.g.ry)) * pl.g.bx + (x / pl.g.rx);
+                out_path[t] = (flags[b] & 2) ? 1 : 0;
+            }
+        }
+        end_call(E, st);
+        return 0;
+    }
+    catch (const CudaFail &f)
+    {
+        set_error(f.msg);
+        return f.code;
+    }
+    catch (const std::exception &ex)
+    {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+Stats last_stats()
+{
+    std::lock_guard<std::mutex> lk(g_engine_mu);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return Stats();
+    auto it = g_engines.find(dev);
+    return it == g_engines.end() ? Stats() : it->second->stats;
+}
+
+int host_template(int kind, int cov_type, const double *ranges, const double *angles, double sill, double nugget,
+                  const int *radiuses, int *out, int cap, int *out_limit)
+{
+    try
+    {
+        check_model_args(cov_type, ranges, angles, sill, nugget, radiuses, 1);
+        Flavour f;
+        std::string err;
+        if (!make_model(cov_type, ranges, angles, sill, nugget, f.m, err)) throw CudaFail{-1, err};
+        f.truncated = kind != 0;
+        for (int a = 0; a < 3; ++a) f.r[a] = radiuses[a];
+        std::vector<Offset> t = build_template(f);
+        for (int i = 0; i < (int)t.size() && i < cap; ++i)
+        {
+            out[3 * i] = t[i].dx;
+            out[3 * i + 1] = t[i].dy;
+            out[3 * i + 2] = t[i].dz;
+        }
+        if (out_limit) *out_limit = (int)(t.size() / 250);
+        return (int)t.size();
+    }
+    catch (const CudaFail &f)
+    {
+        set_error(f.msg);
+        return f.code;
+    }
+}
+
+double host_covariance(int kind, int cov_type, const double *ranges, const double *angles, double sill,
+                       double nugget, const int *radiuses, const int *a, const int *b)
+{
+    Flavour f;
+    std::string err;
+    if (!make_model(cov_type, ranges, angles, sill, nugget, f.m, err))
+    {
+        set_error(err);
+        return NAN;
+    }
+    f.truncated = kind != 0;
+    for (int i = 0; i < 3; ++i) f.r[i] = radiuses ? radiuses[i] : 1;
+    return f.at_offset(b[0] - a[0], b[1] - a[1], b[2] - a[2]);
+}
+} // namespace hb
+
+namespace hb
+{
+int sk_weights(const double *center, const double *xs, const double *ys, const double *zs, int n, int cov_type,
+               const double *ranges, const double *angles, double sill, double nugget, double *out_w)
+{
+    std::lock_guard<std::mutex> lk(g_engine_mu);
+    try
+    {
+        if (n <= 0) throw CudaFail{-1, "sk_kriging_weights: no neighbours"};
+        CovModel m;
+        std::string err;
+        if (!make_model(cov_type, ranges, angles, sill, nugget, m, err)) throw CudaFail{-1, err};
+        Engine &E = engine_for_current_device();
+        cudaStream_t st = E.stream(nullptr);
+        std::vector<double> h(3 + 3 * (size_t)n);
+        h[0] = center[0];
+        h[1] = center[1];
+        h[2] = center[2];
+        for (int i = 0; i < n; ++i)
+        {
+            h[3 + i] = xs[i];
+            h[3 + n + i] = ys[i];
+            h[3 + 2 * n + i] = zs[i];
+        }
+        double *d_pts = E.buf<double>("skw_pts", h.size());
+        double *d_A = E.buf<double>("skw_A", (size_t)n * n);
+        double *d_w = E.buf<double>("skw_w", (size_t)n);
+        int *d_st = E.buf<int>("skw_status", 1);
+        HB_CK(cudaMemcpyAsync(d_pts, h.data(), h.size() * 8, cudaMemcpyHostToDevice, st));
+        launch_sk_weights(dev_model(m), d_pts, n, d_A, d_w, d_st, st);
+        HB_CK(cudaGetLastError());
+        int ok = 0;
+        HB_CK(cudaMemcpyAsync(out_w, d_w, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
+        HB_CK(cudaMemcpyAsync(&ok, d_st, 4, cudaMemcpyDeviceToHost, st));
+        HB_CK(cudaStreamSynchronize(st));
+        if (!ok) throw CudaFail{-1, "sk_kriging_weights: covariance matrix is not positive definite"};
+        return 0;
+    }
+    catch (const CudaFail &f)
+    {
+        set_error(f.msg);
+        return f.code;
+    }
+}
+
+void *host_alloc(size_t bytes)
+{
+    void *p = nullptr;
+    if (cudaHostAlloc(&p, bytes, cudaHostAllocPortable) != cudaSuccess) return nullptr;
+    return p;
+}
+void host_free(void *p)
+{
+    if (p) cudaFreeHost(p);
+}
+} // namespace hb

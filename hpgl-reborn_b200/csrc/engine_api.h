@@ -1,0 +1,74 @@
+// Internal interface between the C ABI (api.cpp) and the engine (engine.cu).
+#pragma once
+#include <cstddef>
+#include <string>
+#include <vector>
+
+namespace hb
+{
+struct SkArgs
+{
+    int cov_type;
+    double ranges[3];
+    double angles[3];
+    double sill, nugget;
+    int radiuses[3];
+    int max_nb;
+    bool auto_mean;
+    double mean;
+};
+
+struct IkArgs
+{
+    int cov_type;
+    double ranges[3];
+    double angles[3];
+    double sill, nugget;
+    int radiuses[3];
+    int max_nb;
+    double marginal;
+};
+
+struct Options
+{
+    int precision = 0;
+    int refine_steps = 0;
+    unsigned flags = 0;
+    void *stream = nullptr;
+    double *estimate64 = nullptr;
+    double *variance = nullptr;
+    signed char *status = nullptr;
+    float *ik_probs = nullptr;
+};
+
+struct Stats
+{
+    double total_ms = 0, search_ms = 0, solve_ms = 0;
+    long long ties = 0, template_cells = 0, kriged = 0, launches = 0;
+    long long h2d = 0, d2h = 0;
+};
+
+void set_error(const std::string &msg);
+const char *last_error();
+void set_threads(int n);
+int get_threads();
+
+int cont_kriging(int kind, const int *dims, const float *in_data, const unsigned char *in_mask, const SkArgs &a,
+                 float *out_data, unsigned char *out_mask, const Options &opt);
+int indicator_kriging(const int *dims, const unsigned char *in_data, const unsigned char *in_mask,
+                      const std::vector<IkArgs> &cats, unsigned char *out_data, unsigned char *out_mask,
+                      const Options &opt);
+int median_ik(const int *dims, const unsigned char *in_data, const unsigned char *in_mask, const IkArgs &a,
+              double marginal1, unsigned char *out_data, unsigned char *out_mask, const Options &opt);
+int find_neighbours(int kind, const int *dims, const unsigned char *mask, const SkArgs &a, const int *nodes,
+                    int n_nodes, int *out_idx, int *out_count, unsigned char *out_path);
+Stats last_stats();
+int host_template(int kind, int cov_type, const double *ranges, const double *angles, double sill, double nugget,
+                  const int *radiuses, int *out, int cap, int *out_limit);
+double host_covariance(int kind, int cov_type, const double *ranges, const double *angles, double sill,
+                       double nugget, const int *radiuses, const int *a, const int *b);
+int sk_weights(const double *center, const double *xs, const double *ys, const double *zs, int n, int cov_type,
+               const double *ranges, const double *angles, double sill, double nugget, double *out_w);
+void *host_alloc(size_t bytes);
+void host_free(void *p);
+} // namespace hb

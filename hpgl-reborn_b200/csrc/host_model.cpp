@@ -1,0 +1,185 @@
+// See host_model.h. Built with the host compiler at -O3 without -march,
+// -mfma or -ffast-math (plain SSE2 double, no contraction).
+#include "host_model.h"
+
+#include <algorithm>
+#include <cmath>
+#include <thread>
+
+namespace hb
+{
+static double deg2rad(double deg) { return (deg * 3.14159265358979323846264338327950288419) / 180; }
+
+// c = a * b for 3x3 row-major, summing k ascending from 0 (tnt_cmat.h:525-538)
+static void mul3(const double *a, const double *b, double *c)
+{
+    for (int i = 0; i < 3; ++i)
+        for (int k = 0; k < 3; ++k)
+        {
+            double s = 0;
+            for (int j = 0; j < 3; ++j) s += a[3 * i + j] * b[3 * j + k];
+            c[3 * i + k] = s;
+        }
+}
+
+bool make_transform(const double *ranges, const double *angles, double *T)
+{
+    for (int i = 0; i < 3; ++i)
+        if (ranges[i] == 0) return false;
+    double S[9] = {0}, Z[9] = {0}, Y[9] = {0}, X[9] = {0};
+    S[0] = 1.0;
+    S[4] = ranges[0] / ranges[1];
+    S[8] = ranges[0] / ranges[2];
+    const double a0 = deg2rad(angles[0]), a1 = deg2rad(angles[1]), a2 = deg2rad(angles[2]);
+    Z[0] = cos(a0); Z[4] = cos(a0); Z[1] = sin(a0); Z[3] = -sin(a0); Z[8] = 1;
+    Y[0] = cos(a1); Y[8] = cos(a1); Y[2] = -sin(a1); Y[6] = sin(a1); Y[4] = 1;
+    X[4] = cos(a2); X[8] = cos(a2); X[5] = sin(a2); X[7] = -sin(a2); X[0] = 1;
+    double xy[9], xyz[9];
+    mul3(X, Y, xy);
+    mul3(xy, Z, xyz);
+    mul3(S, xyz, T);
+    return true;
+}
+
+double CovModel::h_of(double v0, double v1, double v2) const
+{
+    double acc = 0.0;
+    for (int i = 0; i < 3; ++i)
+    {
+        double d = 0.0;
+        d += v0 * T[3 * i + 0];
+        d += v1 * T[3 * i + 1];
+        d += v2 * T[3 * i + 2];
+        acc += d * d;
+    }
+    return sqrt(acc);
+}
+
+double CovModel::of_h(double h) const
+{
+    const double r0 = ranges[0];
+    if (h < 0.0001) return sill;
+    switch (type)
+    {
+    case COV_GAUSSIAN:
+        return (sill - nugget) * exp(-3 * pow(h / r0, 2));
+    case COV_EXPONENTIAL:
+        return (sill - nugget) * exp(-3 * h / r0);
+    default:
+        if (h > r0) return 0;
+        return (sill - nugget) * (1 - 1.5 * h / r0 + 0.5 * pow(h / r0, 3));
+    }
+}
+
+bool make_model(int type, const double *ranges, const double *angles, double sill, double nugget,
+                CovModel &m, std::string &err)
+{
+    if (type < 0 || type > 2)
+    {
+        err = "unknown covariance type " + std::to_string(type);
+        return false;
+    }
+    m.type = type;
+    for (int i = 0; i < 3; ++i)
+    {
+        m.ranges[i] = ranges[i];
+        m.angles[i] = angles[i];
+    }
+    m.sill = sill;
+    m.nugget = nugget;
+    if (!make_transform(ranges, angles, m.T))
+    {
+        err = "create_transform: All covariance ranges should be non-zero";
+        return false;
+    }
+    return true;
+}
+
+double Flavour::at_offset(int dx, int dy, int dz) const
+{
+    if (truncated)
+    {
+        // precalculated_covariance.h:249-264: the table entry of offset
+        // c2 - c1 = d, built as cov((0,0,0), d) from doubles (v = 0 - d)
+        if (dx < -r[0] || dx > r[0] || dy < -r[1] || dy > r[1] || dz < -r[2] || dz > r[2]) return 0;
+        return m.of_h(m.h_of(0.0 - (double)dx, 0.0 - (double)dy, 0.0 - (double)dz));
+    }
+    // cov_model_t on integer points: v = center - (center + d) in int
+    return m.of_h(m.h_of((double)(0 - dx), (double)(0 - dy), (double)(0 - dz)));
+}
+
+std::vector<Offset> build_template(const Flavour &f)
+{
+    struct Ent
+    {
+        Offset o;
+        double key;
+    };
+    std::vector<Ent> v;
+    const double thr = f.threshold();
+    for (int z = -f.r[2]; z <= f.r[2]; ++z)
+        for (int y = -f.r[1]; y <= f.r[1]; ++y)
+            for (int x = -f.r[0]; x <= f.r[0]; ++x)
+            {
+                if (f.at_offset(x, y, z) > thr)
+                {
+                    Offset o = {0 - x, 0 - y, 0 - z};
+                    v.push_back({o, f.at_offset(o.dx, o.dy, o.dz)});
+                }
+            }
+    // covariance descending, libstdc++ std::sort as in covariance_field.h:359
+    std::sort(v.begin(), v.end(), [](const Ent &a, const Ent &b) { return a.key > b.key; });
+    std::vector<Offset> out;
+    out.reserve(v.size());
+    for (const Ent &e : v) out.push_back(e.o);
+    return out;
+}
+
+int clamp_threads(int n)
+{
+    int hw = (int)std::thread::hardware_concurrency();
+    if (hw <= 0) hw = 1;
+    if (n <= 0) n = hw;
+    return std::min(n, 64);
+}
+
+void build_key_table(const Flavour &f, KeyTable &kt, int n_threads)
+{
+    for (int a = 0; a < 3; ++a)
+    {
+        kt.half[a] = 2 * f.r[a] - 1;
+        kt.n[a] = 2 * kt.half[a] + 1;
+    }
+    const long total = (long)kt.n[0] * kt.n[1] * kt.n[2];
+    kt.vals.assign(total, 0.0);
+    kt.rank.assign(total, KEY_EXCLUDED);
+    const double thr = f.threshold();
+    const int nt = clamp_threads(n_threads);
+    const int nz = kt.n[2];
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nt; ++t)
+        pool.emplace_back([&, t]() {
+            for (int iz = t; iz < nz; iz += nt)
+                for (int iy = 0; iy < kt.n[1]; ++iy)
+                    for (int ix = 0; ix < kt.n[0]; ++ix)
+                    {
+                        long i = ((long)iz * kt.n[1] + iy) * kt.n[0] + ix;
+                        kt.vals[i] = f.at_offset(ix - kt.half[0], iy - kt.half[1], iz - kt.half[2]);
+                    }
+        });
+    for (auto &th : pool) th.join();
+    // dense descending ranks of the kept values
+    std::vector<std::pair<double, long>> kept;
+    for (long i = 0; i < total; ++i)
+        if (kt.vals[i] > thr) kept.push_back({kt.vals[i], i});
+    std::sort(kept.begin(), kept.end(),
+              [](const std::pair<double, long> &a, const std::pair<double, long> &b) { return a.first > b.first; });
+    uint32_t r = 0;
+    for (size_t j = 0; j < kept.size(); ++j)
+    {
+        if (j > 0 && kept[j].first != kept[j - 1].first) ++r;
+        kt.rank[kept[j].second] = r;
+    }
+    kt.n_ranks = kept.empty() ? 0 : r + 1;
+}
+} // namespace hb

@@ -1,0 +1,88 @@
+// Launchers of the device kernels (search.cu, solve.cu, misc.cu).
+#pragma once
+#include "engine.cuh"
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace hb
+{
+constexpr int kBuckets = 5; // neighbour counts 1-8, 9-16, 17-32, 33-64, >64
+constexpr int kBucketNP[4] = {8, 16, 32, 64};
+
+struct DevModel
+{
+    int type;
+    double r0, sill, nugget;
+    double T[9];
+};
+
+struct SolveOut
+{
+    float *out_data;     // continuous estimate (float) per cell
+    uint8_t *out_mask;   // set to 1 where out_data is written
+    double *est64;       // optional FP64 estimate per cell
+    double *var;         // optional kriging variance per cell
+    signed char *status; // per-cell status (0 success, 2 singular)
+    float *prob;         // optional: indicator probability of one category (float result)
+    int prob_stride;     // distance between cells in `prob` (the category count)
+    int write_cont;      // write out_data / out_mask
+};
+
+// scan / points / bins (search.cu)
+long long scan_tmp_ints(long long n);
+void exclusive_scan(int *v, long long n, int *tmp, int *total, cudaStream_t st);
+void launch_flag_informed(const uint8_t *mask, long long n, int *flag, cudaStream_t st);
+void launch_emit_points(const uint8_t *mask, const int *pos, const Geom &g, const float *val_f,
+                        const uint8_t *val_u8, int *pts_node, unsigned long long *pts_xyz, float *pts_val,
+                        uint8_t *pts_cat, int *pid_of_node, cudaStream_t st);
+void launch_bin_count(const unsigned long long *pts_xyz, const int *n_pts, const Geom &g, int *bin_cnt,
+                      cudaStream_t st);
+void launch_bin_fill(const unsigned long long *pts_xyz, const int *n_pts, const Geom &g, const int *bin_start,
+                     int *bin_fill, int *bin_pts, cudaStream_t st);
+void launch_bin_sort(const Geom &g, const int *bin_start, const int *bin_cnt, int *bin_pts, uint8_t *bin_flag,
+                     cudaStream_t st);
+void launch_bin_region(const Geom &g, uint8_t *bin_flag, const int *bin_cnt, int *max_cand, int *n_tmpl_bins,
+                       cudaStream_t st);
+size_t search_smem_bytes(int cand_cap, int k, int warps);
+cudaError_t launch_search(const Geom &g, const uint8_t *mask, int all_cells, const int *bin_start,
+                          const int *bin_cnt, const uint8_t *bin_flag, const int *bin_pts,
+                          const unsigned long long *pts_xyz, const uint32_t *keytab, int rank_bits,
+                          const int4 *tmpl, int n_tmpl, const int *pid_of_node, int cand_cap, int warps,
+                          int *nb_pid, int *nb_n, int *tie_cells, int *tie_count, int *n_template_cells,
+                          cudaStream_t st);
+void launch_resolve_ties(const Geom &g, const int *tie_cells, const int *tie_count, int first, int chunk,
+                         const int *bin_start, const int *bin_cnt, const int *bin_pts,
+                         const unsigned long long *pts_xyz, const uint32_t *keytab, void *scratch, int cap,
+                         int *nb_pid, cudaStream_t st);
+size_t tie_entry_bytes();
+
+// solves (solve.cu, misc.cu)
+cudaError_t launch_solve_bucket(int np, int precision, bool ordinary, const Geom &g, const int *cells,
+                                const int *n_items, int max_items, const int *nb_pid, const int *nb_n,
+                                const unsigned long long *pts_xyz, const float *pts_val, const uint8_t *pts_cat,
+                                int ind_value, const double *pair64, const float *pair32, double mean, double c0,
+                                int steps, const SolveOut &out, int n_sm, cudaStream_t st);
+size_t large_scratch_doubles(int k, int blocks);
+cudaError_t launch_solve_large(const Geom &g, const int *cells, const int *n_items, int blocks, const int *nb_pid,
+                               const int *nb_n, const unsigned long long *pts_xyz, const float *pts_val,
+                               const uint8_t *pts_cat, int ind_value, const double *pair64, bool ordinary,
+                               double mean, double c0, double *scratch, const SolveOut &out, cudaStream_t st);
+
+// misc (misc.cu)
+void launch_build_pair(const Geom &g, const DevModel &m, int truncated, const double *search_vals, double *pair64,
+                       float *pair32, cudaStream_t st);
+void launch_prepare(const Geom &g, const uint8_t *mask, int all_cells, const int *nb_n, signed char *status,
+                    int *bucket_cnt, int *bucket_off, int *bucket_fill, int *cells, cudaStream_t st);
+void launch_finalize_cont(const Geom &g, const float *in_data, signed char *status, int simple, float mean_f,
+                          float *out_data, uint8_t *out_mask, double *est64, double *var, cudaStream_t st);
+void launch_ik_fail_fill(const Geom &g, const signed char *status, float marginal, int c, int m, float *probs,
+                         cudaStream_t st);
+void launch_ik_finalize(long long n_cells, int m, float *probs, uint8_t *out_data, uint8_t *out_mask,
+                        cudaStream_t st);
+void launch_sk_weights(const DevModel &m, const double *pts, int n, double *A, double *w, int *status,
+                       cudaStream_t st);
+void launch_mik_finalize(long long n_cells, const signed char *status, const double *est64, double marginal1,
+                         uint8_t *out_data, uint8_t *out_mask, float *prob_out, cudaStream_t st);
+} // namespace hb

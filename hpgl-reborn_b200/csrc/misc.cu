@@ -1,0 +1,491 @@
+// Supporting kernels of the kriging pipeline: pair-covariance tables, work
+// buckets, failure handling, indicator order relations, and the solver for
+// neighbour counts above 64.
+#include "engine.cuh"
+#include "kernels.h"
+
+#include <cstdint>
+
+namespace hb
+{
+// ------------------------------------------------------------- pair tables
+// Device evaluation of the covariance model for displacements outside the
+// exactly tabulated search block: same formulas as cov_model.h:146-183, the
+// transform sum without contraction (explicit round-to-nearest ops).
+__device__ double cov_model_dev(const DevModel &m, int dx, int dy, int dz)
+{
+    double v0 = (double)dx, v1 = (double)dy, v2 = (double)dz;
+    double acc = 0.0;
+    for (int i = 0; i < 3; ++i)
+    {
+        double d = 0.0;
+        d = __dadd_rn(d, __dmul_rn(v0, m.T[3 * i + 0]));
+        d = __dadd_rn(d, __dmul_rn(v1, m.T[3 * i + 1]));
+        d = __dadd_rn(d, __dmul_rn(v2, m.T[3 * i + 2]));
+        acc = __dadd_rn(acc, __dmul_rn(d, d));
+    }
+    double h = sqrt(acc);
+    if (h < 0.0001) return m.sill;
+    double u = h / m.r0;
+    if (m.type == 2) return (m.sill - m.nugget) * exp(-3.0 * (u * u));
+    if (m.type == 1) return (m.sill - m.nugget) * exp((-3.0 * h) / m.r0);
+    if (h > m.r0) return 0.0;
+    return (m.sill - m.nugget) * (1.0 - (1.5 * h) / m.r0 + 0.5 * (u * u * u));
+}
+
+// pair[i] for displacement d: the host's exact value inside the search
+// block, else (analytic flavour) the device model, else (truncated) 0.
+__global__ void k_build_pair(const Geom g, DevModel m, int truncated, const double *__restrict__ search_vals,
+                             double *__restrict__ pair64, float *__restrict__ pair32)
+{
+    long long total = (long long)g.pnx * g.pny * (2 * g.phz + 1);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x)
+    {
+        int ix = (int)(i % g.pnx);
+        int iy = (int)((i / g.pnx) % g.pny);
+        int iz = (int)(i / ((long long)g.pnx * g.pny));
+        int dx = ix - g.phx, dy = iy - g.phy, dz = iz - g.phz;
+        double v;
+        if (key_in_block(g, dx, dy, dz))
+            v = search_vals[key_index(g, dx, dy, dz)];
+        else if (truncated)
+            v = 0.0;
+        else
+            v = cov_model_dev(m, dx, dy, dz);
+        pair64[i] = v;
+        pair32[i] = (float)v;
+    }
+}
+
+void launch_build_pair(const Geom &g, const DevModel &m, int truncated, const double *search_vals, double *pair64,
+                       float *pair32, cudaStream_t st)
+{
+    k_build_pair<<<2368, 256, 0, st>>>(g, m, truncated, search_vals, pair64, pair32);
+}
+
+// ------------------------------------------------------------- buckets
+__device__ __forceinline__ int bucket_of(int n)
+{
+    if (n <= 0) return -1;
+    if (n <= 8) return 0;
+    if (n <= 16) return 1;
+    if (n <= 32) return 2;
+    if (n <= 64) return 3;
+    return 4;
+}
+
+// Per-cell status before the solve: -1 informed (continuous kriging only),
+// 1 no neighbours, 3 pending (to be solved).
+__global__ void k_prepare(const Geom g, const uint8_t *__restrict__ mask, int all_cells, const int *__restrict__ nb_n,
+                          signed char *__restrict__ status, int *__restrict__ bucket_cnt)
+{
+    __shared__ int s_cnt[kBuckets];
+    if (threadIdx.x < kBuckets) s_cnt[threadIdx.x] = 0;
+    __syncthreads();
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < g.n_cells;
+         c += (long long)gridDim.x * blockDim.x)
+    {
+        if (!all_cells && mask[c])
+        {
+            status[c] = -1;
+            continue;
+        }
+        int n = nb_n[c];
+        int b = bucket_of(n);
+        status[c] = b < 0 ? 1 : 3;
+        if (b >= 0) atomicAdd(&s_cnt[b], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < kBuckets && s_cnt[threadIdx.x]) atomicAdd(&bucket_cnt[threadIdx.x], s_cnt[threadIdx.x]);
+}
+
+__global__ void k_bucket_offsets(const int *__restrict__ cnt, int *__restrict__ off, int *__restrict__ fill)
+{
+    if (threadIdx.x == 0)
+    {
+        int run = 0;
+        for (int b = 0; b < kBuckets; ++b)
+        {
+            off[b] = run;
+            fill[b] = 0;
+            run += cnt[b];
+        }
+        off[kBuckets] = run;
+    }
+}
+
+__global__ void k_bucket_fill(const Geom g, const signed char *__restrict__ status, const int *__restrict__ nb_n,
+                              const int *__restrict__ off, int *__restrict__ fill, int *__restrict__ cells)
+{
+    const int lane = threadIdx.x & 31;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < g.n_cells;
+         base += (long long)gridDim.x * blockDim.x)
+    {
+        long long c = base + threadIdx.x;
+        int b = -1;
+        if (c < g.n_cells && status[c] == 3) b = bucket_of(nb_n[c]);
+        // warp-aggregated append per bucket
+        for (int q = 0; q < kBuckets; ++q)
+        {
+            unsigned m = __ballot_sync(0xffffffffu, b == q);
+            if (!m) continue;
+            int leader = __ffs(m) - 1;
+            int start = 0;
+            if (lane == leader) start = atomicAdd(&fill[q], __popc(m));
+            start = __shfl_sync(0xffffffffu, start, leader);
+            if (b == q)
+            {
+                unsigned lt;
+                asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+                cells[off[q] + start + __popc(m & lt)] = (int)c;
+            }
+        }
+    }
+}
+
+void launch_prepare(const Geom &g, const uint8_t *mask, int all_cells, const int *nb_n, signed char *status,
+                    int *bucket_cnt, int *bucket_off, int *bucket_fill, int *cells, cudaStream_t st)
+{
+    cudaMemsetAsync(bucket_cnt, 0, sizeof(int) * kBuckets, st);
+    k_prepare<<<1184, 256, 0, st>>>(g, mask, all_cells, nb_n, status, bucket_cnt);
+    k_bucket_offsets<<<1, 32, 0, st>>>(bucket_cnt, bucket_off, bucket_fill);
+    k_bucket_fill<<<1184, 256, 0, st>>>(g, status, nb_n, bucket_off, bucket_fill, cells);
+}
+
+// ------------------------------------------------------------- finalize
+// Continuous kriging outputs for cells the solver did not write
+// (cont_kriging.h:80-110): informed cells are copied, failures of SK get the
+// mean, failures of OK are left alone.
+__global__ void k_finalize_cont(const Geom g, const float *__restrict__ in_data, signed char *__restrict__ status,
+                                int simple, float mean_f, float *__restrict__ out_data, uint8_t *__restrict__ out_mask,
+                                double *__restrict__ est64, double *__restrict__ var)
+{
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < g.n_cells;
+         c += (long long)gridDim.x * blockDim.x)
+    {
+        signed char s = status[c];
+        if (s == -1)
+        {
+            out_data[c] = in_data[c];
+            out_mask[c] = 1;
+            if (est64) est64[c] = (double)in_data[c];
+            if (var) var[c] = 0.0;
+        }
+        else if (s == 1 || s == 2 || s == 3)
+        {
+            if (s == 3) status[c] = 2; // not written by any solver: treat as singular
+            if (simple)
+            {
+                out_data[c] = mean_f;
+                out_mask[c] = 1;
+            }
+            if (est64) est64[c] = __longlong_as_double(0x7ff8000000000000LL);
+            if (var) var[c] = -1.0;
+        }
+    }
+}
+
+void launch_finalize_cont(const Geom &g, const float *in_data, signed char *status, int simple, float mean_f,
+                          float *out_data, uint8_t *out_mask, double *est64, double *var, cudaStream_t st)
+{
+    k_finalize_cont<<<1184, 256, 0, st>>>(g, in_data, status, simple, mean_f, out_data, out_mask, est64, var);
+}
+
+// Indicator category c: cells whose solve failed (or had no neighbours) take
+// the marginal probability (indicator_kriging.h:137-140).
+__global__ void k_ik_fail_fill(const Geom g, const signed char *__restrict__ status, float marginal, int c, int m,
+                               float *__restrict__ probs)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.n_cells;
+         i += (long long)gridDim.x * blockDim.x)
+        if (status[i] != 0) probs[i * m + c] = marginal;
+}
+
+void launch_ik_fail_fill(const Geom &g, const signed char *status, float marginal, int c, int m, float *probs,
+                         cudaStream_t st)
+{
+    k_ik_fail_fill<<<1184, 256, 0, st>>>(g, status, marginal, c, m, probs);
+}
+
+// Order relations (indicator_kriging.h:34-59) and the first-maximum argmax
+// (cdf_utils.cpp:11-27).
+__global__ void k_ik_finalize(long long n_cells, int m, float *__restrict__ probs, uint8_t *__restrict__ out_data,
+                              uint8_t *__restrict__ out_mask)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_cells;
+         i += (long long)gridDim.x * blockDim.x)
+    {
+        float *p = probs + i * m;
+        for (int c = 0; c < m; ++c)
+        {
+            float v = p[c];
+            if (v < 0.0f) v = 0.0f;
+            else if (v > 1.0f) v = 1.0f;
+            p[c] = v;
+        }
+        for (int c = 0; c + 1 < m; ++c)
+            if (p[c] > p[c + 1])
+            {
+                float s = __fadd_rn(p[c], p[c + 1]);
+                float avg = (float)((double)s / 2.0);
+                p[c] = avg;
+                p[c + 1] = avg;
+            }
+        double best = p[0];
+        int arg = 0;
+        for (int c = 1; c < m; ++c)
+            if ((double)p[c] > best)
+            {
+                best = p[c];
+                arg = c;
+            }
+        out_data[i] = (uint8_t)arg;
+        out_mask[i] = 1;
+    }
+}
+
+void launch_ik_finalize(long long n_cells, int m, float *probs, uint8_t *out_data, uint8_t *out_mask, cudaStream_t st)
+{
+    k_ik_finalize<<<1184, 256, 0, st>>>(n_cells, m, probs, out_data, out_mask);
+}
+
+// Median IK decision (median_ik.cpp:15-21 through a float); failures use the
+// marginal (the reference leaves this case undefined).
+__global__ void k_mik_finalize(long long n_cells, const signed char *__restrict__ status,
+                               const double *__restrict__ est64, double marginal1, uint8_t *__restrict__ out_data,
+                               uint8_t *__restrict__ out_mask, float *__restrict__ prob_out)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_cells;
+         i += (long long)gridDim.x * blockDim.x)
+    {
+        double p = status[i] == 0 ? est64[i] : (double)(float)marginal1;
+        float pf = (float)p;
+        out_data[i] = pf <= 0.5f ? 0 : 1;
+        out_mask[i] = 1;
+        if (prob_out) prob_out[i] = pf;
+    }
+}
+
+void launch_mik_finalize(long long n_cells, const signed char *status, const double *est64, double marginal1,
+                         uint8_t *out_data, uint8_t *out_mask, float *prob_out, cudaStream_t st)
+{
+    k_mik_finalize<<<1184, 256, 0, st>>>(n_cells, status, est64, marginal1, out_data, out_mask, prob_out);
+}
+
+// ------------------------------------------------------------- large systems
+// Neighbour counts above 64: one CTA per system, matrix in global scratch,
+// double precision, right-looking Cholesky with block barriers.
+__global__ void __launch_bounds__(256) k_solve_large(const Geom g, const int *__restrict__ cells,
+                                                     const int *__restrict__ n_items_ptr, const int *__restrict__ nb_pid,
+                                                     const int *__restrict__ nb_n,
+                                                     const unsigned long long *__restrict__ pts_xyz,
+                                                     const float *__restrict__ pts_val,
+                                                     const uint8_t *__restrict__ pts_cat, int ind_value,
+                                                     const double *__restrict__ pair64, int ordinary, double mean,
+                                                     double c0, double *__restrict__ scratch, SolveOut out)
+{
+    const int n_items = *n_items_ptr;
+    const int kmax = g.k;
+    double *A = scratch + (size_t)blockIdx.x * ((size_t)kmax * kmax + 4 * kmax);
+    double *rhs = A + (size_t)kmax * kmax; // b, ones, x(b), x(1)
+    const long long pc = g.pair_center;
+    for (int item = blockIdx.x; item < n_items; item += gridDim.x)
+    {
+        const int cell = cells[item];
+        const int n = nb_n[cell];
+        const int cxg = cell % g.nx, cyg = cell % (g.nx * g.ny) / g.nx, czg = cell / (g.nx * g.ny);
+        // assemble A, b
+        for (int e = threadIdx.x; e < n * n; e += blockDim.x)
+        {
+            int i = e / n, j = e % n;
+            int pi = nb_pid[(long long)cell * kmax + i], pj = nb_pid[(long long)cell * kmax + j];
+            int xi, yi, zi, xj, yj, zj;
+            unpack_xyz(pts_xyz[pi], xi, yi, zi);
+            unpack_xyz(pts_xyz[pj], xj, yj, zj);
+            A[(size_t)i * n + j] = pair64[pc + pair_lin(g, xi - xj, yi - yj, zi - zj)];
+        }
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+        {
+            int pi = nb_pid[(long long)cell * kmax + i];
+            int xi, yi, zi;
+            unpack_xyz(pts_xyz[pi], xi, yi, zi);
+            rhs[i] = pair64[pc + pair_lin(g, xi - cxg, yi - cyg, zi - czg)];
+            rhs[kmax + i] = 1.0;
+        }
+        __syncthreads();
+        // factor (lower triangle, row-major)
+        bool fail = false;
+        for (int j = 0; j < n; ++j)
+        {
+            double d = A[(size_t)j * n + j];
+            if (!(d > 0.0)) fail = true;
+            double ljj = sqrt(d);
+            __syncthreads();
+            for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) A[(size_t)i * n + j] /= ljj;
+            if (threadIdx.x == 0) A[(size_t)j * n + j] = ljj;
+            __syncthreads();
+            for (int e = threadIdx.x; e < (n - j - 1) * (n - j - 1); e += blockDim.x)
+            {
+                int i = j + 1 + e / (n - j - 1), c = j + 1 + e % (n - j - 1);
+                if (c <= i) A[(size_t)i * n + c] -= A[(size_t)i * n + j] * A[(size_t)c * n + j];
+            }
+            __syncthreads();
+        }
+        // two right-hand sides solved by one thread each (n is small enough)
+        if (threadIdx.x < 2)
+        {
+            double *x = rhs + (threadIdx.x == 0 ? 2 * kmax : 3 * kmax);
+            const double *src = rhs + (threadIdx.x == 0 ? 0 : kmax);
+            for (int i = 0; i < n; ++i)
+            {
+                double s = src[i];
+                for (int c = 0; c < i; ++c) s -= A[(size_t)i * n + c] * x[c];
+                x[i] = s / A[(size_t)i * n + i];
+            }
+            for (int i = n - 1; i >= 0; --i)
+            {
+                double s = x[i];
+                for (int c = i + 1; c < n; ++c) s -= A[(size_t)c * n + i] * x[c];
+                x[i] = s / A[(size_t)i * n + i];
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            const double *x = rhs + 2 * kmax, *y = rhs + 3 * kmax;
+            double mu = 0.0;
+            double sx = 0, sy = 0;
+            for (int i = 0; i < n; ++i)
+            {
+                sx += x[i];
+                sy += y[i];
+            }
+            if (ordinary)
+            {
+                if (fabs(sy) < 1e-15) fail = true;
+                mu = (sx - 1.0) / sy;
+            }
+            const float mf = (float)mean;
+            double est = (double)mf, var = c0 - mu;
+            for (int i = 0; i < n; ++i)
+            {
+                double w = ordinary ? x[i] - mu * y[i] : x[i];
+                int p = nb_pid[(long long)cell * kmax + i];
+                double v = pts_val ? (double)pts_val[p] : (pts_cat[p] == ind_value ? 1.0 : 0.0);
+                est += w * (double)((float)v - mf);
+                var -= w * rhs[i];
+            }
+            if (var < 0) var = 0;
+            if (!fail)
+            {
+                if (out.write_cont)
+                {
+                    out.out_data[cell] = (float)est;
+                    out.out_mask[cell] = 1;
+                }
+                if (out.prob) out.prob[(long long)cell * out.prob_stride] = (float)est;
+                if (out.est64) out.est64[cell] = est;
+                if (out.var) out.var[cell] = var;
+                if (out.status) out.status[cell] = 0;
+            }
+            else if (out.status)
+                out.status[cell] = 2;
+        }
+        __syncthreads();
+    }
+}
+
+size_t large_scratch_doubles(int k, int blocks) { return (size_t)blocks * ((size_t)k * k + 4 * (size_t)k); }
+
+cudaError_t launch_solve_large(const Geom &g, const int *cells, const int *n_items, int blocks, const int *nb_pid,
+                               const int *nb_n, const unsigned long long *pts_xyz, const float *pts_val,
+                               const uint8_t *pts_cat, int ind_value, const double *pair64, bool ordinary,
+                               double mean, double c0, double *scratch, const SolveOut &out, cudaStream_t st)
+{
+    k_solve_large<<<blocks, 256, 0, st>>>(g, cells, n_items, nb_pid, nb_n, pts_xyz, pts_val, pts_cat, ind_value,
+                                          pair64, ordinary ? 1 : 0, mean, c0, scratch, out);
+    return cudaGetLastError();
+}
+} // namespace hb
+
+namespace hb
+{
+// ------------------------------------------------------------- single system
+// SK weights for arbitrary real coordinates with the analytic model
+// (simple_kriging.cpp:67-87 via sk_kriging_weights_3 on real_location_t):
+// one CTA, matrix in global memory, FP64. status[0] = 1 on success.
+__device__ double cov_real_dev(const DevModel &m, double v0, double v1, double v2)
+{
+    double acc = 0.0;
+    for (int i = 0; i < 3; ++i)
+    {
+        double d = 0.0;
+        d = __dadd_rn(d, __dmul_rn(v0, m.T[3 * i + 0]));
+        d = __dadd_rn(d, __dmul_rn(v1, m.T[3 * i + 1]));
+        d = __dadd_rn(d, __dmul_rn(v2, m.T[3 * i + 2]));
+        acc = __dadd_rn(acc, __dmul_rn(d, d));
+    }
+    double h = sqrt(acc);
+    if (h < 0.0001) return m.sill;
+    double u = h / m.r0;
+    if (m.type == 2) return (m.sill - m.nugget) * exp(-3.0 * (u * u));
+    if (m.type == 1) return (m.sill - m.nugget) * exp((-3.0 * h) / m.r0);
+    if (h > m.r0) return 0.0;
+    return (m.sill - m.nugget) * (1.0 - (1.5 * h) / m.r0 + 0.5 * (u * u * u));
+}
+
+__global__ void k_sk_weights(DevModel m, const double *__restrict__ pts, int n, double *__restrict__ A,
+                             double *__restrict__ w, int *__restrict__ status)
+{
+    const double cx = pts[0], cy = pts[1], cz = pts[2];
+    const double *xs = pts + 3, *ys = xs + n, *zs = ys + n;
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x)
+    {
+        int i = e / n, j = e % n;
+        A[e] = cov_real_dev(m, xs[i] - xs[j], ys[i] - ys[j], zs[i] - zs[j]);
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) w[i] = cov_real_dev(m, xs[i] - cx, ys[i] - cy, zs[i] - cz);
+    __syncthreads();
+    bool fail = false;
+    for (int j = 0; j < n; ++j)
+    {
+        double d = A[(size_t)j * n + j];
+        if (!(d > 0.0)) fail = true;
+        double ljj = sqrt(d);
+        __syncthreads();
+        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) A[(size_t)i * n + j] /= ljj;
+        if (threadIdx.x == 0) A[(size_t)j * n + j] = ljj;
+        __syncthreads();
+        int span = n - j - 1;
+        for (int e = threadIdx.x; e < span * span; e += blockDim.x)
+        {
+            int i = j + 1 + e / span, c = j + 1 + e % span;
+            if (c <= i) A[(size_t)i * n + c] -= A[(size_t)i * n + j] * A[(size_t)c * n + j];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+    {
+        for (int i = 0; i < n; ++i)
+        {
+            double s = w[i];
+            for (int c = 0; c < i; ++c) s -= A[(size_t)i * n + c] * w[c];
+            w[i] = s / A[(size_t)i * n + i];
+        }
+        for (int i = n - 1; i >= 0; --i)
+        {
+            double s = w[i];
+            for (int c = i + 1; c < n; ++c) s -= A[(size_t)c * n + i] * w[c];
+            w[i] = s / A[(size_t)i * n + i];
+        }
+        status[0] = fail ? 0 : 1;
+    }
+}
+
+void launch_sk_weights(const DevModel &m, const double *pts, int n, double *A, double *w, int *status,
+                       cudaStream_t st)
+{
+    k_sk_weights<<<1, 256, 0, st>>>(m, pts, n, A, w, status);
+}
+} // namespace hb

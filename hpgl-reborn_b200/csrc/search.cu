@@ -1,0 +1,633 @@
+// Neighbour search on the GPU, bit-exact with the reference's
+// indexed_neighbour_lookup_t::find (sugarbox_indexed_neighbour_lookup.h:67-124).
+//
+// Stages (all on one stream, no host round trip in between):
+//   1. compact the informed cells into points, ascending node order;
+//   2. bin the points (clusterizer.cpp:74-188): per-bin counts, offsets and
+//      ascending-node lists; a bin holding more than `limit` points is exceeded;
+//   3. per bin, decide the path of its cells: template scan when any of the 27
+//      surrounding bins is exceeded (clusterizer.cpp:169-188), else the bins;
+//   4. k_search: one CTA per bin. Cluster path: the CTA stages the candidate
+//      list of the 27 bins (z, y, x nested, ascending nodes inside a bin) in
+//      shared memory; each warp takes one cell, looks up every candidate's
+//      selection key (dense covariance rank, host-built with the reference's
+//      own double arithmetic), finds the k-th smallest key by radix select,
+//      and keeps the k best. If a run of equal keys straddles the k-th slot the
+//      reference's choice depends on std::sort's permutation; such cells are
+//      queued for stage 5. Template path: one warp per cell walks the sorted
+//      template 32 offsets at a time with a ballot on the mask.
+//   5. k_resolve_ties: one thread per queued cell rebuilds the filtered
+//      candidate list and runs the introsort restatement (gnu_introsort.h),
+//      which reproduces std::sort's permutation, then takes the first k.
+#include "engine.cuh"
+#include "gnu_introsort.h"
+#include "kernels.h"
+
+#include <cstdint>
+
+namespace hb
+{
+// ------------------------------------------------------------------ scan
+// Exclusive scan of n ints in place, in three passes; tile = 1024 per block.
+constexpr int kScanTile = 1024;
+
+__global__ void k_scan_tiles(int *v, long long n, int *tile_sums)
+{
+    __shared__ int warp_sums[32];
+    long long base = (long long)blockIdx.x * kScanTile;
+    int t = threadIdx.x; // 256 threads, 4 items each
+    int a[4];
+    int s = 0;
+    for (int i = 0; i < 4; ++i)
+    {
+        long long idx = base + t * 4 + i;
+        a[i] = idx < n ? v[idx] : 0;
+        s += a[i];
+    }
+    int lane = t & 31, w = t >> 5;
+    int incl = s;
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) warp_sums[w] = incl;
+    __syncthreads();
+    if (w == 0)
+    {
+        int ws = lane < 8 ? warp_sums[lane] : 0;
+        int wi = ws;
+        for (int o = 1; o < 8; o <<= 1)
+        {
+            int y = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += y;
+        }
+        if (lane < 8) warp_sums[lane] = wi - ws;
+        if (lane == 7) tile_sums[blockIdx.x] = wi;
+    }
+    __syncthreads();
+    int run = warp_sums[w] + incl - s;
+    for (int i = 0; i < 4; ++i)
+    {
+        long long idx = base + t * 4 + i;
+        if (idx < n) v[idx] = run;
+        run += a[i];
+    }
+}
+
+__global__ void k_scan_add(int *v, long long n, const int *tile_offsets)
+{
+    long long idx = (long long)blockIdx.x * kScanTile + threadIdx.x;
+    int add = tile_offsets[blockIdx.x];
+    for (int i = 0; i < kScanTile; i += blockDim.x)
+        if (idx + i < n) v[idx + i] += add;
+}
+
+// Exclusive scan; `total` (device int) receives the sum. `tmp` needs
+// scan_tmp_ints(n) ints.
+long long scan_tmp_ints(long long n)
+{
+    long long t = (n + kScanTile - 1) / kScanTile;
+    long long need = t + 1;
+    if (t > 1) need += scan_tmp_ints(t);
+    return need;
+}
+
+void exclusive_scan(int *v, long long n, int *tmp, int *total, cudaStream_t st)
+{
+    long long tiles = (n + kScanTile - 1) / kScanTile;
+    if (tiles <= 0)
+    {
+        cudaMemsetAsync(total, 0, sizeof(int), st);
+        return;
+    }
+    int *sums = tmp;
+    k_scan_tiles<<<(unsigned)tiles, 256, 0, st>>>(v, n, sums);
+    if (tiles == 1)
+    {
+        cudaMemcpyAsync(total, sums, sizeof(int), cudaMemcpyDeviceToDevice, st);
+        return;
+    }
+    exclusive_scan(sums, tiles, tmp + tiles + 1, total, st);
+    k_scan_add<<<(unsigned)tiles, 256, 0, st>>>(v, n, sums);
+}
+
+// ------------------------------------------------------------------ points
+// flag[i] = 1 for informed cells (mask != 0, property_array.h:53-58)
+__global__ void k_flag_informed(const uint8_t *__restrict__ mask, long long n, int *__restrict__ flag)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        flag[i] = mask[i] != 0;
+}
+
+// after the exclusive scan, pos[i] is the point id of informed cell i
+__global__ void k_emit_points(const uint8_t *__restrict__ mask, const int *__restrict__ pos, Geom g,
+                              const float *__restrict__ val_f, const uint8_t *__restrict__ val_u8,
+                              int *__restrict__ pts_node, unsigned long long *__restrict__ pts_xyz,
+                              float *__restrict__ pts_val, uint8_t *__restrict__ pts_cat,
+                              int *__restrict__ pid_of_node)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.n_cells;
+         i += (long long)gridDim.x * blockDim.x)
+    {
+        if (!mask[i])
+        {
+            if (pid_of_node) pid_of_node[i] = -1;
+            continue;
+        }
+        int p = pos[i];
+        int node = (int)i;
+        int x = node % g.nx, y = node % (g.nx * g.ny) / g.nx, z = node / (g.nx * g.ny);
+        pts_node[p] = node;
+        pts_xyz[p] = pack_xyz(x, y, z);
+        if (val_f) pts_val[p] = val_f[i];
+        if (val_u8) pts_cat[p] = val_u8[i];
+        if (pid_of_node) pid_of_node[i] = p;
+    }
+}
+
+// ------------------------------------------------------------------ bins
+__device__ __forceinline__ int bin_of(const Geom &g, int x, int y, int z)
+{
+    int cx = x / g.rx, cy = y / g.ry, cz = z / g.rz;
+    return (cz * g.by + cy) * g.bx + cx;
+}
+
+__global__ void k_bin_count(const unsigned long long *__restrict__ pts_xyz, const int *__restrict__ n_pts,
+                            Geom g, int *__restrict__ bin_cnt)
+{
+    int m = *n_pts;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < m; p += gridDim.x * blockDim.x)
+    {
+        int x, y, z;
+        unpack_xyz(pts_xyz[p], x, y, z);
+        atomicAdd(&bin_cnt[bin_of(g, x, y, z)], 1);
+    }
+}
+
+__global__ void k_bin_fill(const unsigned long long *__restrict__ pts_xyz, const int *__restrict__ n_pts,
+                           Geom g, const int *__restrict__ bin_start, int *__restrict__ bin_fill,
+                           int *__restrict__ bin_pts)
+{
+    int m = *n_pts;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < m; p += gridDim.x * blockDim.x)
+    {
+        int x, y, z;
+        unpack_xyz(pts_xyz[p], x, y, z);
+        int b = bin_of(g, x, y, z);
+        int s = atomicAdd(&bin_fill[b], 1);
+        bin_pts[bin_start[b] + s] = p;
+    }
+}
+
+// Restores ascending point order inside each non-exceeded bin (insertion sort;
+// bins hold at most `limit` points) and records per-bin flags:
+//   bit 0: exceeded (count > limit)
+__global__ void k_bin_sort(Geom g, const int *__restrict__ bin_start, const int *__restrict__ bin_cnt,
+                           int *__restrict__ bin_pts, uint8_t *__restrict__ bin_flag)
+{
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < g.n_bins; b += gridDim.x * blockDim.x)
+    {
+        int c = bin_cnt[b];
+        bool exceeded = c > g.limit;
+        bin_flag[b] = exceeded ? 1 : 0;
+        if (exceeded) continue;
+        int *a = bin_pts + bin_start[b];
+        for (int i = 1; i < c; ++i)
+        {
+            int v = a[i];
+            int j = i - 1;
+            while (j >= 0 && a[j] > v)
+            {
+                a[j + 1] = a[j];
+                --j;
+            }
+            a[j + 1] = v;
+        }
+    }
+}
+
+// bit 1: the cells of this bin take the template path
+__global__ void k_bin_region(Geom g, uint8_t *__restrict__ bin_flag, const int *__restrict__ bin_cnt,
+                             int *__restrict__ max_cand, int *__restrict__ n_template_bins)
+{
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < g.n_bins; b += gridDim.x * blockDim.x)
+    {
+        int cx = b % g.bx, cy = (b / g.bx) % g.by, cz = b / (g.bx * g.by);
+        bool tmpl = false;
+        int cand = 0;
+        for (int k = cz - 1; k <= cz + 1; ++k)
+            for (int j = cy - 1; j <= cy + 1; ++j)
+                for (int i = cx - 1; i <= cx + 1; ++i)
+                {
+                    if (i < 0 || j < 0 || k < 0 || i >= g.bx || j >= g.by || k >= g.bz) continue;
+                    int nb = (k * g.by + j) * g.bx + i;
+                    if (bin_flag[nb] & 1) tmpl = true;
+                    cand += bin_cnt[nb];
+                }
+        if (tmpl)
+        {
+            bin_flag[b] |= 2;
+            atomicAdd(n_template_bins, 1);
+        }
+        else
+            atomicMax(max_cand, cand);
+    }
+}
+
+// ------------------------------------------------------------------ search
+struct SearchSmem
+{
+    // layout computed at launch: [cand_x | cand_y | cand_z | cand_pid] (C_cap ints each),
+    // then per warp: keys[C_cap] u32, hist[256] u32, sel[k_cap] u64
+};
+
+__device__ __forceinline__ unsigned lanemask_lt()
+{
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Selects, for the cell at (x, y, z), the up-to-k candidates with the
+// smallest keys. Returns the number selected (written to `out` as point ids,
+// keys ascending, ties in candidate order) or -1 when a run of equal keys
+// straddles the k-th slot.
+__device__ int select_cell(const Geom &g, int x, int y, int z, int C, const int *cx, const int *cy,
+                           const int *cz, const int *cpid, const uint32_t *__restrict__ keytab,
+                           uint32_t *keys, uint32_t *hist, unsigned long long *sel, int rank_bits,
+                           int lane, int *out)
+{
+    const int k = g.k;
+    int kept = 0;
+    for (int i = lane; i < C; i += 32)
+    {
+        int dx = cx[i] - x, dy = cy[i] - y, dz = cz[i] - z;
+        uint32_t key = keytab[key_index(g, dx, dy, dz)];
+        keys[i] = key;
+        kept += key != kKeyExcluded;
+    }
+    for (int o = 16; o > 0; o >>= 1) kept += __shfl_xor_sync(0xffffffffu, kept, o);
+    __syncwarp();
+
+    uint32_t kstar = kKeyExcluded; // select every kept candidate when kept <= k
+    if (kept > k)
+    {
+        // radix select of the k-th smallest key, 8 bits per pass from the top
+        int passes = (rank_bits + 7) / 8;
+        uint32_t prefix = 0;
+        int remaining = k; // 1-based rank still to locate inside the prefix class
+        for (int p = passes - 1; p >= 0; --p)
+        {
+            int shift = 8 * p;
+            for (int b = lane; b < 256; b += 32) hist[b] = 0;
+            __syncwarp();
+            for (int i = lane; i < C; i += 32)
+            {
+                uint32_t key = keys[i];
+                if (key == kKeyExcluded) continue;
+                if (p + 1 < passes && (key >> (shift + 8)) != prefix) continue;
+                atomicAdd(&hist[(key >> shift) & 255u], 1u);
+            }
+            __syncwarp();
+            // locate the digit holding the remaining-th key
+            uint32_t h[8];
+            uint32_t s = 0;
+            for (int q = 0; q < 8; ++q)
+            {
+                h[q] = hist[lane * 8 + q];
+                s += h[q];
+            }
+            uint32_t incl = s;
+            for (int o = 1; o < 32; o <<= 1)
+            {
+                uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            uint32_t excl = incl - s;
+            int digit = -1;
+            uint32_t below = 0;
+            if ((int)excl < remaining && (int)incl >= remaining)
+            {
+                uint32_t run = excl;
+                for (int q = 0; q < 8; ++q)
+                {
+                    if ((int)(run + h[q]) >= remaining)
+                    {
+                        digit = lane * 8 + q;
+                        below = run;
+                        break;
+                    }
+                    run += h[q];
+                }
+            }
+            unsigned who = __ballot_sync(0xffffffffu, digit >= 0);
+            int src = __ffs(who) - 1;
+            digit = __shfl_sync(0xffffffffu, digit, src);
+            below = __shfl_sync(0xffffffffu, below, src);
+            prefix = (prefix << 8) | (uint32_t)digit;
+            remaining -= (int)below;
+            __syncwarp();
+        }
+        kstar = prefix;
+    }
+
+    // compact the selection in candidate order: keys < kstar, then keys == kstar
+    int n_less = 0, n_eq = 0;
+    for (int base = 0; base < C; base += 32)
+    {
+        int i = base + lane;
+        uint32_t key = i < C ? keys[i] : kKeyExcluded;
+        bool less = (kept > k) ? key < kstar : key != kKeyExcluded;
+        bool eq = (kept > k) && key == kstar;
+        unsigned bl = __ballot_sync(0xffffffffu, less);
+        unsigned be = __ballot_sync(0xffffffffu, eq);
+        if (less)
+        {
+            int slot = n_less + __popc(bl & lanemask_lt());
+            if (slot < k) sel[slot] = ((unsigned long long)key << 32) | (unsigned)i;
+        }
+        n_less += __popc(bl);
+        n_eq += __popc(be);
+    }
+    int n_sel;
+    if (kept <= k)
+        n_sel = kept;
+    else
+    {
+        int need = k - n_less;
+        if (n_eq != need) return -1; // tie group straddles the k-th slot
+        // append the whole tie group (it fits exactly)
+        int w = n_less;
+        for (int base = 0; base < C; base += 32)
+        {
+            int i = base + lane;
+            bool eq = i < C && keys[i] == kstar;
+            unsigned be = __ballot_sync(0xffffffffu, eq);
+            if (eq) sel[w + __popc(be & lanemask_lt())] = ((unsigned long long)kstar << 32) | (unsigned)i;
+            w += __popc(be);
+        }
+        n_sel = k;
+    }
+    __syncwarp();
+    // order by (key, candidate position): rank of each entry among the selection
+    for (int e = lane; e < n_sel; e += 32)
+    {
+        unsigned long long me = sel[e];
+        int rank = 0;
+        for (int f = 0; f < n_sel; ++f) rank += sel[f] < me;
+        out[rank] = cpid[(int)(me & 0xFFFFFFFFu)];
+    }
+    __syncwarp();
+    return n_sel;
+}
+
+__global__ void __launch_bounds__(256) k_search(
+    const Geom g, const uint8_t *__restrict__ mask, int all_cells, const int *__restrict__ bin_start,
+    const int *__restrict__ bin_cnt, const uint8_t *__restrict__ bin_flag, const int *__restrict__ bin_pts,
+    const unsigned long long *__restrict__ pts_xyz, const uint32_t *__restrict__ keytab, int rank_bits,
+    const int4 *__restrict__ tmpl, int n_tmpl, const int *__restrict__ pid_of_node, int cand_cap,
+    int *__restrict__ nb_pid, int *__restrict__ nb_n, int *__restrict__ tie_cells, int *__restrict__ tie_count,
+    int *__restrict__ n_template_cells)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int b = blockIdx.x;
+    const int bxi = b % g.bx, byi = (b / g.bx) % g.by, bzi = b / (g.bx * g.by);
+    const int x0 = bxi * g.rx, y0 = byi * g.ry, z0 = bzi * g.rz;
+    if (x0 >= g.nx || y0 >= g.ny || z0 >= g.nz) return; // bin past the grid: no cells
+    const int x1 = min(x0 + g.rx, g.nx), y1 = min(y0 + g.ry, g.ny), z1 = min(z0 + g.rz, g.nz);
+    const int wx = x1 - x0, wy = y1 - y0, wz = z1 - z0;
+    const int n_cells_bin = wx * wy * wz;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int k = g.k;
+
+    if (bin_flag[b] & 2)
+    {
+        // ---------------- template path: warp per cell
+        int counted = 0;
+        for (int c = warp; c < n_cells_bin; c += nwarps)
+        {
+            int x = x0 + c % wx, y = y0 + (c / wx) % wy, z = z0 + c / (wx * wy);
+            long long cell = ((long long)z * g.ny + y) * g.nx + x;
+            if (!all_cells && mask[cell]) continue;
+            ++counted;
+            int *out = nb_pid + cell * k;
+            int found = 0;
+            for (int base = 0; base < n_tmpl && found < k; base += 32)
+            {
+                int t = base + lane;
+                bool ok = false;
+                long long node = -1;
+                if (t < n_tmpl)
+                {
+                    int4 o = tmpl[t];
+                    int px = x + o.x, py = y + o.y, pz = z + o.z;
+                    if ((unsigned)px < (unsigned)g.nx && (unsigned)py < (unsigned)g.ny &&
+                        (unsigned)pz < (unsigned)g.nz)
+                    {
+                        node = ((long long)pz * g.ny + py) * g.nx + px;
+                        ok = mask[node] != 0;
+                    }
+                }
+                unsigned bl = __ballot_sync(0xffffffffu, ok);
+                int slot = found + __popc(bl & lanemask_lt());
+                if (ok && slot < k) out[slot] = pid_of_node[node];
+                found += __popc(bl);
+            }
+            if (lane == 0) nb_n[cell] = min(found, k);
+        }
+        if (lane == 0 && counted) atomicAdd(n_template_cells, counted);
+        return;
+    }
+
+    // ---------------- cluster path
+    int *cx = reinterpret_cast<int *>(smem);
+    int *cy = cx + cand_cap;
+    int *cz = cy + cand_cap;
+    int *cpid = cz + cand_cap;
+    unsigned char *wbase = reinterpret_cast<unsigned char *>(cpid + cand_cap);
+    const size_t per_warp = (size_t)cand_cap * 4 + 256 * 4 + (size_t)k * 8;
+    uint32_t *keys = reinterpret_cast<uint32_t *>(wbase + per_warp * warp);
+    uint32_t *hist = keys + cand_cap;
+    unsigned long long *sel = reinterpret_cast<unsigned long long *>(hist + 256);
+
+    // stage the 27-bin candidate list in the reference's order
+    __shared__ int s_off[28];
+    if (threadIdx.x == 0)
+    {
+        int run = 0, q = 0;
+        for (int kk = bzi - 1; kk <= bzi + 1; ++kk)
+            for (int jj = byi - 1; jj <= byi + 1; ++jj)
+                for (int ii = bxi - 1; ii <= bxi + 1; ++ii)
+                {
+                    s_off[q] = run;
+                    if (ii >= 0 && jj >= 0 && kk >= 0 && ii < g.bx && jj < g.by && kk < g.bz)
+                        run += bin_cnt[(kk * g.by + jj) * g.bx + ii];
+                    ++q;
+                }
+        s_off[27] = run;
+    }
+    __syncthreads();
+    const int C = s_off[27];
+    for (int q = 0; q < 27; ++q)
+    {
+        int kk = bzi - 1 + q / 9, jj = byi - 1 + (q / 3) % 3, ii = bxi - 1 + q % 3;
+        if (ii < 0 || jj < 0 || kk < 0 || ii >= g.bx || jj >= g.by || kk >= g.bz) continue;
+        int nb = (kk * g.by + jj) * g.bx + ii;
+        int s = bin_start[nb], cnt = s_off[q + 1] - s_off[q];
+        for (int i = threadIdx.x; i < cnt; i += blockDim.x)
+        {
+            int p = bin_pts[s + i];
+            int px, py, pz;
+            unpack_xyz(pts_xyz[p], px, py, pz);
+            int d = s_off[q] + i;
+            cx[d] = px;
+            cy[d] = py;
+            cz[d] = pz;
+            cpid[d] = p;
+        }
+    }
+    __syncthreads();
+
+    for (int c = warp; c < n_cells_bin; c += nwarps)
+    {
+        int x = x0 + c % wx, y = y0 + (c / wx) % wy, z = z0 + c / (wx * wy);
+        long long cell = ((long long)z * g.ny + y) * g.nx + x;
+        if (!all_cells && mask[cell]) continue;
+        int n = select_cell(g, x, y, z, C, cx, cy, cz, cpid, keytab, keys, hist, sel, rank_bits, lane,
+                            nb_pid + cell * k);
+        if (lane == 0)
+        {
+            if (n < 0)
+            {
+                nb_n[cell] = k; // list filled by k_resolve_ties
+                int slot = atomicAdd(tie_count, 1);
+                tie_cells[slot] = (int)cell;
+            }
+            else
+                nb_n[cell] = n;
+        }
+    }
+}
+
+// One thread per tie-straddling cell: rebuild the threshold-filtered candidate
+// list in the reference's order, sort it with the std::sort restatement and
+// keep the first k. `scratch` holds cap entries per thread.
+struct KeyPid
+{
+    uint32_t key;
+    int pid;
+};
+struct KeyLess
+{
+    __device__ bool operator()(const KeyPid &a, const KeyPid &b) const { return a.key < b.key; }
+};
+
+__global__ void k_resolve_ties(const Geom g, const int *__restrict__ tie_cells, const int *__restrict__ tie_count,
+                               int first, int chunk, const int *__restrict__ bin_start,
+                               const int *__restrict__ bin_cnt, const int *__restrict__ bin_pts,
+                               const unsigned long long *__restrict__ pts_xyz,
+                               const uint32_t *__restrict__ keytab, KeyPid *__restrict__ scratch, int cap,
+                               int *__restrict__ nb_pid)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int idx = first + t;
+    if (t >= chunk || idx >= *tie_count) return;
+    int cell = tie_cells[idx];
+    int x = cell % g.nx, y = cell % (g.nx * g.ny) / g.nx, z = cell / (g.nx * g.ny);
+    int bxi = x / g.rx, byi = y / g.ry, bzi = z / g.rz;
+    KeyPid *a = scratch + (size_t)t * cap;
+    int n = 0;
+    for (int kk = bzi - 1; kk <= bzi + 1; ++kk)
+        for (int jj = byi - 1; jj <= byi + 1; ++jj)
+            for (int ii = bxi - 1; ii <= bxi + 1; ++ii)
+            {
+                if (ii < 0 || jj < 0 || kk < 0 || ii >= g.bx || jj >= g.by || kk >= g.bz) continue;
+                int nb = (kk * g.by + jj) * g.bx + ii;
+                int s = bin_start[nb], cnt = bin_cnt[nb];
+                for (int i = 0; i < cnt; ++i)
+                {
+                    int p = bin_pts[s + i];
+                    int px, py, pz;
+                    unpack_xyz(pts_xyz[p], px, py, pz);
+                    uint32_t key = keytab[key_index(g, px - x, py - y, pz - z)];
+                    if (key != kKeyExcluded && n < cap) a[n++] = KeyPid{key, p};
+                }
+            }
+    gis::sort(a, (long)n, KeyLess());
+    int *out = nb_pid + (long long)cell * g.k;
+    int m = n < g.k ? n : g.k;
+    for (int i = 0; i < m; ++i) out[i] = a[i].pid;
+}
+
+// ------------------------------------------------------------------ launchers
+void launch_flag_informed(const uint8_t *mask, long long n, int *flag, cudaStream_t st)
+{
+    k_flag_informed<<<1184, 256, 0, st>>>(mask, n, flag);
+}
+void launch_emit_points(const uint8_t *mask, const int *pos, const Geom &g, const float *val_f,
+                        const uint8_t *val_u8, int *pts_node, unsigned long long *pts_xyz, float *pts_val,
+                        uint8_t *pts_cat, int *pid_of_node, cudaStream_t st)
+{
+    k_emit_points<<<1184, 256, 0, st>>>(mask, pos, g, val_f, val_u8, pts_node, pts_xyz, pts_val, pts_cat,
+                                        pid_of_node);
+}
+void launch_bin_count(const unsigned long long *pts_xyz, const int *n_pts, const Geom &g, int *bin_cnt,
+                      cudaStream_t st)
+{
+    k_bin_count<<<592, 256, 0, st>>>(pts_xyz, n_pts, g, bin_cnt);
+}
+void launch_bin_fill(const unsigned long long *pts_xyz, const int *n_pts, const Geom &g, const int *bin_start,
+                     int *bin_fill, int *bin_pts, cudaStream_t st)
+{
+    k_bin_fill<<<592, 256, 0, st>>>(pts_xyz, n_pts, g, bin_start, bin_fill, bin_pts);
+}
+void launch_bin_sort(const Geom &g, const int *bin_start, const int *bin_cnt, int *bin_pts, uint8_t *bin_flag,
+                     cudaStream_t st)
+{
+    int blocks = (g.n_bins + 255) / 256;
+    k_bin_sort<<<blocks, 256, 0, st>>>(g, bin_start, bin_cnt, bin_pts, bin_flag);
+}
+void launch_bin_region(const Geom &g, uint8_t *bin_flag, const int *bin_cnt, int *max_cand, int *n_tmpl_bins,
+                       cudaStream_t st)
+{
+    int blocks = (g.n_bins + 255) / 256;
+    k_bin_region<<<blocks, 256, 0, st>>>(g, bin_flag, bin_cnt, max_cand, n_tmpl_bins);
+}
+
+size_t search_smem_bytes(int cand_cap, int k, int warps)
+{
+    return (size_t)cand_cap * 16 + (size_t)warps * ((size_t)cand_cap * 4 + 256 * 4 + (size_t)k * 8);
+}
+
+cudaError_t launch_search(const Geom &g, const uint8_t *mask, int all_cells, const int *bin_start,
+                          const int *bin_cnt, const uint8_t *bin_flag, const int *bin_pts,
+                          const unsigned long long *pts_xyz, const uint32_t *keytab, int rank_bits,
+                          const int4 *tmpl, int n_tmpl, const int *pid_of_node, int cand_cap, int warps,
+                          int *nb_pid, int *nb_n, int *tie_cells, int *tie_count, int *n_template_cells,
+                          cudaStream_t st)
+{
+    size_t smem = search_smem_bytes(cand_cap, g.k, warps);
+    cudaError_t e = cudaFuncSetAttribute(k_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_search<<<g.n_bins, warps * 32, smem, st>>>(g, mask, all_cells, bin_start, bin_cnt, bin_flag, bin_pts,
+                                                  pts_xyz, keytab, rank_bits, tmpl, n_tmpl, pid_of_node,
+                                                  cand_cap, nb_pid, nb_n, tie_cells, tie_count,
+                                                  n_template_cells);
+    return cudaGetLastError();
+}
+
+void launch_resolve_ties(const Geom &g, const int *tie_cells, const int *tie_count, int first, int chunk,
+                         const int *bin_start, const int *bin_cnt, const int *bin_pts,
+                         const unsigned long long *pts_xyz, const uint32_t *keytab, void *scratch, int cap,
+                         int *nb_pid, cudaStream_t st)
+{
+    int threads = 64;
+    int blocks = (chunk + threads - 1) / threads;
+    k_resolve_ties<<<blocks, threads, 0, st>>>(g, tie_cells, tie_count, first, chunk, bin_start, bin_cnt,
+                                               bin_pts, pts_xyz, keytab, reinterpret_cast<KeyPid *>(scratch),
+                                               cap, nb_pid);
+}
+size_t tie_entry_bytes() { return sizeof(KeyPid); }
+} // namespace hb

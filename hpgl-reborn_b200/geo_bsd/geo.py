@@ -1,0 +1,359 @@
+"""geo_bsd's kriging API on the B200 engine.
+
+Signatures, argument validation and output conventions follow HPGL's
+src/geo_bsd/geo.py: ordinary_kriging (:573-607), simple_kriging (:610-649),
+median_ik (:699-738), indicator_kriging (:759-801, two categories dispatch to
+median IK with data[0]'s model, :785-793), simple_kriging_weights (:897-935),
+the property/grid/model classes (:215-299) and the handler setters (:947-966).
+The output property is a clone of the input that the library fills in place.
+
+Additions (keyword-only, defaults keep the reference's behaviour):
+  precision="fp64" | "fp32_refined"   FP64 solve, or FP32 factorisation with
+                                      FP64-residual refinement
+  refine_steps=2                      refinement steps for fp32_refined
+  return_variance=False               also return the kriging variance (float64)
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy
+
+from . import hpgl_wrap as W
+from .validation import (CriticalValidationError, GridValidator, ParameterValidator, ValidationError,
+                         ValidationWarning)
+
+_hpgl_so = W._hpgl_so
+
+_PRECISIONS = {"fp64": W.FP64_PLAIN, "fp64_plain": W.FP64_PLAIN, "fp32_refined": W.FP32_REFINED,
+               "fp32": W.FP32_REFINED}
+_default_precision = "fp64"
+
+
+def set_precision(name: str) -> None:
+    """Default precision mode for calls that do not pass `precision=`."""
+    global _default_precision
+    if name not in _PRECISIONS:
+        raise ValueError(f"unknown precision {name!r}; one of {sorted(_PRECISIONS)}")
+    _default_precision = name
+
+
+def checkFWA(a):
+    assert a.flags["F"] and a.flags["W"] and a.flags["A"]
+
+
+class ContProperty:
+    def __init__(self, data, mask):
+        self.data = numpy.require(data, "float32", "F")
+        self.mask = numpy.require(mask, "uint8", "F")
+
+    def validate(self):
+        checkFWA(self.data)
+        checkFWA(self.mask)
+        assert self.data.shape == self.mask.shape
+
+    def fix_shape(self, grid):
+        if self.data.ndim != 3 and self.data.size == grid.x * grid.y * grid.z:
+            self.data = self.data.reshape((grid.x, grid.y, grid.z), order="F")
+        if self.mask.ndim != 3 and self.mask.size == grid.x * grid.y * grid.z:
+            self.mask = self.mask.reshape((grid.x, grid.y, grid.z), order="F")
+
+    def __getitem__(self, idx):
+        if idx == 0:
+            return self.data
+        if idx == 1:
+            return self.mask
+        raise RuntimeError("Index out of range.")
+
+
+class IndProperty:
+    def __init__(self, data, mask, indicator_count):
+        self.data = numpy.require(data, "uint8", "F")
+        self.mask = numpy.require(mask, "uint8", "F")
+        self.indicator_count = indicator_count
+        if numpy.sum(numpy.bitwise_and(numpy.asarray(mask) > 0, numpy.asarray(data) >= indicator_count)) > 0:
+            raise RuntimeError("Property contains some indicators outside of [0..%s] range." % (indicator_count - 1))
+        assert numpy.shape(data) == numpy.shape(mask)
+
+    def validate(self):
+        checkFWA(self.data)
+        checkFWA(self.mask)
+        assert self.data.shape == self.mask.shape
+
+    def __getitem__(self, idx):
+        if idx == 0:
+            return self.data
+        if idx == 1:
+            return self.mask
+        if idx == 2:
+            return self.indicator_count
+        raise RuntimeError("Index out of range.")
+
+
+class covariance:
+    spherical = 0
+    exponential = 1
+    gaussian = 2
+
+
+class SugarboxGrid:
+    def __init__(self, x, y, z):
+        GridValidator.validate_grid_dimensions(x, y, z)
+        self.x = x
+        self.y = y
+        self.z = z
+
+
+class CovarianceModel:
+    def __init__(self, type=0, ranges=(0, 0, 0), angles=(0.0, 0.0, 0.0), sill=1.0, nugget=0.0):
+        self.type = type
+        self.ranges = ranges
+        self.angles = angles
+        self.sill = sill
+        self.nugget = nugget
+        ParameterValidator.validate_covariance_parameters(sill, nugget, ranges, angles)
+
+
+def _to_prop(t):
+    if isinstance(t, tuple):
+        if len(t) == 3:
+            return IndProperty(*t)
+        if len(t) == 2:
+            return ContProperty(*t)
+        raise AssertionError("property tuple must have 2 or 3 items")
+    assert isinstance(t, (ContProperty, IndProperty))
+    return t
+
+
+def _clone_prop(prop):
+    data2 = prop.data.copy("F")
+    mask2 = prop.mask.copy("F")
+    if isinstance(prop, IndProperty):
+        return IndProperty(data2, mask2, prop.indicator_count)
+    return ContProperty(data2, mask2)
+
+
+def _dims(grid, prop):
+    n = grid.x * grid.y * grid.z
+    if prop.data.size != n:
+        raise RuntimeError("Invalid data size. Size of data = %s. Size of grid = %s" % (prop.data.size, n))
+    return (C.c_int * 3)(grid.x, grid.y, grid.z)
+
+
+def _flat(a):
+    # Fortran-order flattening is the node order x + nx*y + nx*ny*z
+    return a.reshape(-1, order="F")
+
+
+def _int_radiuses(r):
+    return tuple(int(round(v)) for v in r)
+
+
+def _options(precision, refine_steps, estimate64=None, variance=None, status=None, probs=None):
+    o = W._HPGL_B200_OPTIONS()
+    o.precision = _PRECISIONS[precision or _default_precision]
+    o.refine_steps = int(refine_steps)
+    o.flags = W.FLAG_OUT_IS_CLONE
+    o.estimate64 = estimate64.ctypes.data if estimate64 is not None else None
+    o.variance = variance.ctypes.data if variance is not None else None
+    o.status = status.ctypes.data if status is not None else None
+    o.ik_probs = probs.ctypes.data if probs is not None else None
+    return o
+
+
+def _cont_kriging(kind, prop, grid, radiuses, max_neighbours, cov_model, mean, precision, refine_steps,
+                  return_variance):
+    prop = _to_prop(prop)
+    GridValidator.validate_grid_dimensions(grid.x, grid.y, grid.z)
+    valid_radiuses = ParameterValidator.validate_radius(radiuses, "radiuses")
+    ParameterValidator.validate_max_neighbors(max_neighbours)
+    ParameterValidator.validate_covariance_parameters(cov_model.sill, cov_model.nugget, cov_model.ranges,
+                                                      cov_model.angles)
+    out_prop = _clone_prop(prop)
+    dims = _dims(grid, prop)
+    p = W._HPGL_SK_PARAMS(covariance_type=cov_model.type, ranges=tuple(cov_model.ranges),
+                          angles=tuple(cov_model.angles), sill=cov_model.sill, nugget=cov_model.nugget,
+                          radiuses=_int_radiuses(valid_radiuses), max_neighbours=max_neighbours,
+                          automatic_mean=(mean is None), mean=(mean if mean is not None else 0))
+    var = numpy.empty(prop.data.size, numpy.float64) if return_variance else None
+    opt = _options(precision, refine_steps, variance=var)
+    d_in = _flat(prop.data)
+    m_in = _flat(prop.mask)
+    d_out = _flat(out_prop.data)
+    m_out = _flat(out_prop.mask)
+    rc = _hpgl_so.hpgl_b200_cont_kriging_ex(kind, dims, d_in.ctypes.data, m_in.ctypes.data, C.byref(p),
+                                            d_out.ctypes.data, m_out.ctypes.data, C.byref(opt))
+    W.check(rc, "ordinary_kriging" if kind == 0 else "simple_kriging")
+    if return_variance:
+        return out_prop, var.reshape(prop.data.shape, order="F")
+    return out_prop
+
+
+def ordinary_kriging(prop, grid, radiuses, max_neighbours, cov_model, *, precision: Optional[str] = None,
+                     refine_steps: int = 2, return_variance: bool = False):
+    return _cont_kriging(0, prop, grid, radiuses, max_neighbours, cov_model, None, precision, refine_steps,
+                         return_variance)
+
+
+def simple_kriging(prop, grid, radiuses, max_neighbours, cov_model, mean=None, *, precision: Optional[str] = None,
+                   refine_steps: int = 2, return_variance: bool = False):
+    return _cont_kriging(1, prop, grid, radiuses, max_neighbours, cov_model, mean, precision, refine_steps,
+                         return_variance)
+
+
+def median_ik(prop, grid, marginal_probs, radiuses, max_neighbours, cov_model, *, precision: Optional[str] = None,
+              refine_steps: int = 2):
+    prop = _to_prop(prop)
+    GridValidator.validate_grid_dimensions(grid.x, grid.y, grid.z)
+    valid_radiuses = ParameterValidator.validate_radius(radiuses, "radiuses")
+    ParameterValidator.validate_max_neighbors(max_neighbours)
+    ParameterValidator.validate_covariance_parameters(cov_model.sill, cov_model.nugget, cov_model.ranges,
+                                                      cov_model.angles)
+    if len(marginal_probs) != 2:
+        raise ValueError("median_ik: marginal_probs must have exactly 2 elements")
+    for i, pr in enumerate(marginal_probs):
+        ParameterValidator.validate_probability(pr, f"marginal_probs[{i}]")
+    out_prop = _clone_prop(prop)
+    dims = _dims(grid, prop)
+    p = W._HPGL_MEDIAN_IK_PARAMS(covariance_type=cov_model.type, ranges=tuple(cov_model.ranges),
+                                 angles=tuple(cov_model.angles), sill=cov_model.sill, nugget=cov_model.nugget,
+                                 radiuses=_int_radiuses(valid_radiuses), max_neighbours=max_neighbours,
+                                 marginal_probs=tuple(marginal_probs))
+    opt = _options(precision, refine_steps)
+    rc = _hpgl_so.hpgl_b200_median_ik_ex(dims, _flat(prop.data).ctypes.data, _flat(prop.mask).ctypes.data,
+                                         C.byref(p), _flat(out_prop.data).ctypes.data,
+                                         _flat(out_prop.mask).ctypes.data, C.byref(opt))
+    W.check(rc, "median_ik")
+    return out_prop
+
+
+def indicator_kriging(prop, grid, data, marginal_probs, *, precision: Optional[str] = None, refine_steps: int = 2,
+                      return_probabilities: bool = False):
+    prop = _to_prop(prop)
+    GridValidator.validate_grid_dimensions(grid.x, grid.y, grid.z)
+    ParameterValidator.validate_indicator_count(len(data))
+    if len(marginal_probs) != len(data):
+        raise ValueError(f"indicator_kriging: marginal_probs length ({len(marginal_probs)}) must match data length "
+                         f"({len(data)})")
+    for i, pr in enumerate(marginal_probs):
+        ParameterValidator.validate_probability(pr, f"marginal_probs[{i}]")
+    for i, ikd in enumerate(data):
+        ParameterValidator.validate_radius(ikd["radiuses"], f"data[{i}].radiuses")
+        ParameterValidator.validate_max_neighbors(ikd["max_neighbours"])
+        cm = ikd["cov_model"]
+        ParameterValidator.validate_covariance_parameters(cm.sill, cm.nugget, cm.ranges, cm.angles)
+    for i in range(len(data)):
+        data[i]["marginal_prob"] = marginal_probs[i]
+    if len(data) == 2:
+        return median_ik(prop, grid, (data[0]["marginal_prob"], 1 - data[0]["marginal_prob"]),
+                         data[0]["radiuses"], data[0]["max_neighbours"], data[0]["cov_model"], precision=precision,
+                         refine_steps=refine_steps)
+    out_prop = _clone_prop(prop)
+    dims = _dims(grid, prop)
+    m = len(data)
+    params = (W._HPGL_IK_PARAMS * m)()
+    for i, ikd in enumerate(data):
+        cm = ikd["cov_model"]
+        params[i] = W._HPGL_IK_PARAMS(covariance_type=cm.type, ranges=tuple(cm.ranges), angles=tuple(cm.angles),
+                                      sill=cm.sill, nugget=cm.nugget, radiuses=_int_radiuses(ikd["radiuses"]),
+                                      max_neighbours=ikd["max_neighbours"], marginal_prob=marginal_probs[i])
+    probs = numpy.empty((prop.data.size, m), numpy.float32) if return_probabilities else None
+    opt = _options(precision, refine_steps, probs=probs)
+    rc = _hpgl_so.hpgl_b200_indicator_kriging_ex(dims, _flat(prop.data).ctypes.data, _flat(prop.mask).ctypes.data,
+                                                 params, m, _flat(out_prop.data).ctypes.data,
+                                                 _flat(out_prop.mask).ctypes.data, C.byref(opt))
+    W.check(rc, "indicator_kriging")
+    if return_probabilities:
+        return out_prop, probs
+    return out_prop
+
+
+def simple_kriging_weights(center_point, n_x, n_y, n_z, ranges=(100000, 100000, 100000), sill=1,
+                           cov_type=covariance.exponential, nugget=None, angles=None):
+    if angles is None:
+        angles = (0, 0, 0)
+    if nugget is None:
+        nugget = 0
+    ParameterValidator.validate_covariance_parameters(sill, nugget, ranges, angles)
+    if len(n_x) != len(n_y) or len(n_x) != len(n_z):
+        raise RuntimeError("Invalid pointset. %s,%s,%s." % (len(n_x), len(n_y), len(n_z)))
+    for name, arr in (("n_x", n_x), ("n_y", n_y), ("n_z", n_z)):
+        a = numpy.asarray(arr, dtype="float32")
+        if numpy.any(numpy.isnan(a)) or numpy.any(numpy.isinf(a)):
+            raise ValueError(f"simple_kriging_weights: {name} contains NaN or infinite values")
+    covp = W._HPGL_COV_PARAMS(covariance_type=cov_type, ranges=tuple(ranges), angles=tuple(angles), sill=sill,
+                              nugget=nugget)
+    weights = numpy.zeros(len(n_x), dtype="float32")
+    centre = (C.c_float * 3)(*center_point)
+    _hpgl_so.hpgl_simple_kriging_weights(centre, numpy.array(n_x, dtype="float32"),
+                                         numpy.array(n_y, dtype="float32"), numpy.array(n_z, dtype="float32"),
+                                         len(n_x), C.byref(covp), weights)
+    return weights
+
+
+def calc_mean(prop):
+    prop = _to_prop(prop)
+    sel = prop.mask.reshape(-1) == 1
+    if not numpy.any(sel):
+        raise ValueError("calc_mean: no informed values (all masked)")
+    return float(numpy.sum(prop.data.reshape(-1)[sel].astype(numpy.float64)) / numpy.count_nonzero(sel))
+
+
+def set_thread_num(num):
+    _hpgl_so.hpgl_set_thread_num(num)
+
+
+def get_thread_num():
+    return _hpgl_so.hpgl_get_thread_num()
+
+
+_handlers = {}
+
+
+def set_output_handler(handler, param):
+    if handler is None:
+        _hpgl_so.hpgl_set_output_handler(C.cast(None, W.hpgl_output_handler), None)
+        _handlers.pop("out", None)
+    else:
+        h = W.hpgl_output_handler(handler)
+        _handlers["out"] = h
+        _hpgl_so.hpgl_set_output_handler(h, param)
+
+
+def set_progress_handler(handler, param):
+    if handler is None:
+        _hpgl_so.hpgl_set_progress_handler(C.cast(None, W.hpgl_progress_handler), None)
+        _handlers.pop("progress", None)
+    else:
+        h = W.hpgl_progress_handler(handler)
+        _handlers["progress"] = h
+        _hpgl_so.hpgl_set_progress_handler(h, param)
+
+
+def find_neighbours(prop, grid, radiuses, max_neighbours, cov_model, nodes, kind=0):
+    """Neighbour node indices per node, as the reference's lookup returns them.
+
+    kind 0 = OK (analytic covariance), 1 = SK / IK (box-truncated). Returns
+    (idx[n, k] -1-padded, count[n], template_path[n])."""
+    prop = _to_prop(prop)
+    dims = _dims(grid, prop)
+    nodes = numpy.ascontiguousarray(nodes, dtype=numpy.int32)
+    k = int(max_neighbours)
+    idx = numpy.full((len(nodes), k), -1, numpy.int32)
+    cnt = numpy.zeros(len(nodes), numpy.int32)
+    path = numpy.zeros(len(nodes), numpy.uint8)
+    p = W._HPGL_SK_PARAMS(covariance_type=cov_model.type, ranges=tuple(cov_model.ranges),
+                          angles=tuple(cov_model.angles), sill=cov_model.sill, nugget=cov_model.nugget,
+                          radiuses=_int_radiuses(radiuses), max_neighbours=k, automatic_mean=1, mean=0)
+    rc = _hpgl_so.hpgl_b200_find_neighbours(kind, dims, _flat(prop.mask).ctypes.data, C.byref(p),
+                                            nodes.ctypes.data, len(nodes), idx.ctypes.data, cnt.ctypes.data,
+                                            path.ctypes.data)
+    W.check(rc, "find_neighbours")
+    return idx, cnt, path
+
+
+__all__ = ["ContProperty", "IndProperty", "SugarboxGrid", "CovarianceModel", "covariance", "ordinary_kriging",
+           "simple_kriging", "median_ik", "indicator_kriging", "simple_kriging_weights", "calc_mean",
+           "set_thread_num", "get_thread_num", "set_output_handler", "set_progress_handler", "set_precision",
+           "find_neighbours", "ValidationError", "CriticalValidationError", "ValidationWarning"]

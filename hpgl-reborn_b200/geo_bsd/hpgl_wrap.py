@@ -1,0 +1,172 @@
+"""ctypes binding of libhpgl_b200.so (include/hpgl_b200.h).
+
+Struct layouts are those of the reference's binding (src/geo_bsd/hpgl_wrap.py:44-165)
+so code written against HPGL's ctypes structs keeps working. The library is
+loaded from this package's directory; there is no CPU fallback: a missing or
+unloadable library raises ImportError at import time.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+from numpy.ctypeslib import ndpointer
+
+hpgl_output_handler = C.CFUNCTYPE(C.c_int, C.c_char_p, C.py_object)
+hpgl_progress_handler = C.CFUNCTYPE(C.c_int, C.c_char_p, C.c_int, C.py_object)
+
+
+class _HPGL_SHAPE(C.Structure):
+    _fields_ = [("data", C.c_int * 3), ("strides", C.c_int * 3)]
+
+
+class _HPGL_CONT_MASKED_ARRAY(C.Structure):
+    _fields_ = [("data", C.POINTER(C.c_float)), ("mask", C.POINTER(C.c_ubyte)), ("shape", _HPGL_SHAPE)]
+
+
+class _HPGL_IND_MASKED_ARRAY(C.Structure):
+    _fields_ = [("data", C.POINTER(C.c_ubyte)), ("mask", C.POINTER(C.c_ubyte)), ("shape", _HPGL_SHAPE),
+                ("indicator_count", C.c_int)]
+
+
+class _HPGL_OK_PARAMS(C.Structure):
+    _fields_ = [("covariance_type", C.c_int), ("ranges", C.c_double * 3), ("angles", C.c_double * 3),
+                ("sill", C.c_double), ("nugget", C.c_double), ("radiuses", C.c_int * 3),
+                ("max_neighbours", C.c_int)]
+
+
+class _HPGL_SK_PARAMS(C.Structure):
+    _fields_ = [("covariance_type", C.c_int), ("ranges", C.c_double * 3), ("angles", C.c_double * 3),
+                ("sill", C.c_double), ("nugget", C.c_double), ("radiuses", C.c_int * 3),
+                ("max_neighbours", C.c_int), ("automatic_mean", C.c_ubyte), ("mean", C.c_double)]
+
+
+class _HPGL_MEDIAN_IK_PARAMS(C.Structure):
+    _fields_ = [("covariance_type", C.c_int), ("ranges", C.c_double * 3), ("angles", C.c_double * 3),
+                ("sill", C.c_double), ("nugget", C.c_double), ("radiuses", C.c_int * 3),
+                ("max_neighbours", C.c_int), ("marginal_probs", C.c_double * 2)]
+
+
+class _HPGL_IK_PARAMS(C.Structure):
+    _fields_ = [("covariance_type", C.c_int), ("ranges", C.c_double * 3), ("angles", C.c_double * 3),
+                ("sill", C.c_double), ("nugget", C.c_double), ("radiuses", C.c_int * 3),
+                ("max_neighbours", C.c_int), ("marginal_prob", C.c_double)]
+
+
+class __hpgl_cov_params_t(C.Structure):
+    _fields_ = [("covariance_type", C.c_int), ("ranges", C.c_double * 3), ("angles", C.c_double * 3),
+                ("sill", C.c_double), ("nugget", C.c_double)]
+
+
+_HPGL_COV_PARAMS = __hpgl_cov_params_t
+
+
+class _HPGL_B200_OPTIONS(C.Structure):
+    _fields_ = [("precision", C.c_int), ("refine_steps", C.c_int), ("flags", C.c_uint),
+                ("stream", C.c_void_p), ("estimate64", C.c_void_p), ("variance", C.c_void_p),
+                ("status", C.c_void_p), ("ik_probs", C.c_void_p)]
+
+
+FP64_PLAIN = 0
+FP32_REFINED = 1
+FLAG_DEVICE_POINTERS = 1
+FLAG_OUT_IS_CLONE = 2
+
+LIB_NAME = "libhpgl_b200.so"
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
+
+# Exported symbols of include/hpgl_b200.h (checked by the test suite).
+EXPORTS = [
+    "hpgl_get_last_exception_message", "hpgl_set_output_handler", "hpgl_set_progress_handler",
+    "hpgl_set_thread_num", "hpgl_get_thread_num", "hpgl_ordinary_kriging", "hpgl_simple_kriging",
+    "hpgl_simple_kriging_weights", "hpgl_indicator_kriging", "hpgl_median_ik",
+    "hpgl_b200_cont_kriging_ex", "hpgl_b200_indicator_kriging_ex", "hpgl_b200_median_ik_ex",
+    "hpgl_b200_find_neighbours", "hpgl_b200_last_stats", "hpgl_b200_host_alloc", "hpgl_b200_host_free",
+    "hpgl_b200_transform", "hpgl_b200_template", "hpgl_b200_covariance", "hpgl_b200_version",
+]
+
+
+def _load():
+    if not os.path.isfile(LIB_PATH):
+        raise ImportError(
+            f"{LIB_NAME} is not built (expected at {LIB_PATH}); run `make -C hpgl-reborn_b200` "
+            "or __graft_entry__.build()")
+    lib = C.CDLL(LIB_PATH)
+    _f32 = ndpointer(dtype="float32", flags="C")
+    _u8 = ndpointer(dtype="uint8", flags="C")
+    _f32F = ndpointer(dtype="float32", flags=("F", "W", "A"))
+    _u8F = ndpointer(dtype="uint8", flags=("F", "W", "A"))
+    i_p = C.POINTER(C.c_int)
+    lib.hpgl_get_last_exception_message.restype = C.c_char_p
+    lib.hpgl_get_last_exception_message.argtypes = []
+    lib.hpgl_set_output_handler.restype = None
+    lib.hpgl_set_output_handler.argtypes = [hpgl_output_handler, C.py_object]
+    lib.hpgl_set_progress_handler.restype = None
+    lib.hpgl_set_progress_handler.argtypes = [hpgl_progress_handler, C.py_object]
+    lib.hpgl_set_thread_num.restype = None
+    lib.hpgl_set_thread_num.argtypes = [C.c_int]
+    lib.hpgl_get_thread_num.restype = C.c_int
+    lib.hpgl_ordinary_kriging.restype = None
+    lib.hpgl_ordinary_kriging.argtypes = [C.POINTER(_HPGL_CONT_MASKED_ARRAY), C.POINTER(_HPGL_OK_PARAMS),
+                                          C.POINTER(_HPGL_CONT_MASKED_ARRAY)]
+    lib.hpgl_simple_kriging.restype = None
+    lib.hpgl_simple_kriging.argtypes = [_f32F, _u8F, C.POINTER(_HPGL_SHAPE), C.POINTER(_HPGL_SK_PARAMS),
+                                        _f32F, _u8F, C.POINTER(_HPGL_SHAPE)]
+    lib.hpgl_simple_kriging_weights.restype = C.c_int
+    lib.hpgl_simple_kriging_weights.argtypes = [C.POINTER(C.c_float), _f32, _f32, _f32, C.c_int,
+                                                C.POINTER(_HPGL_COV_PARAMS), _f32]
+    lib.hpgl_indicator_kriging.restype = None
+    lib.hpgl_indicator_kriging.argtypes = [C.POINTER(_HPGL_IND_MASKED_ARRAY), C.POINTER(_HPGL_IND_MASKED_ARRAY),
+                                           C.POINTER(_HPGL_IK_PARAMS), C.c_int]
+    lib.hpgl_median_ik.restype = None
+    lib.hpgl_median_ik.argtypes = [C.POINTER(_HPGL_IND_MASKED_ARRAY), C.POINTER(_HPGL_MEDIAN_IK_PARAMS),
+                                   C.POINTER(_HPGL_IND_MASKED_ARRAY)]
+    vp = C.c_void_p
+    lib.hpgl_b200_cont_kriging_ex.restype = C.c_int
+    lib.hpgl_b200_cont_kriging_ex.argtypes = [C.c_int, i_p, vp, vp, C.POINTER(_HPGL_SK_PARAMS), vp, vp,
+                                              C.POINTER(_HPGL_B200_OPTIONS)]
+    lib.hpgl_b200_indicator_kriging_ex.restype = C.c_int
+    lib.hpgl_b200_indicator_kriging_ex.argtypes = [i_p, vp, vp, C.POINTER(_HPGL_IK_PARAMS), C.c_int, vp, vp,
+                                                   C.POINTER(_HPGL_B200_OPTIONS)]
+    lib.hpgl_b200_median_ik_ex.restype = C.c_int
+    lib.hpgl_b200_median_ik_ex.argtypes = [i_p, vp, vp, C.POINTER(_HPGL_MEDIAN_IK_PARAMS), vp, vp,
+                                           C.POINTER(_HPGL_B200_OPTIONS)]
+    lib.hpgl_b200_find_neighbours.restype = C.c_int
+    lib.hpgl_b200_find_neighbours.argtypes = [C.c_int, i_p, vp, C.POINTER(_HPGL_SK_PARAMS), vp, C.c_int, vp, vp,
+                                              vp]
+    lib.hpgl_b200_last_stats.restype = C.c_int
+    lib.hpgl_b200_last_stats.argtypes = [C.POINTER(C.c_double), C.c_int]
+    lib.hpgl_b200_host_alloc.restype = C.c_void_p
+    lib.hpgl_b200_host_alloc.argtypes = [C.c_size_t]
+    lib.hpgl_b200_host_free.restype = None
+    lib.hpgl_b200_host_free.argtypes = [C.c_void_p]
+    lib.hpgl_b200_transform.restype = C.c_int
+    lib.hpgl_b200_transform.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    lib.hpgl_b200_template.restype = C.c_int
+    lib.hpgl_b200_template.argtypes = [C.c_int, C.POINTER(_HPGL_COV_PARAMS), i_p, vp, C.c_int, i_p]
+    lib.hpgl_b200_covariance.restype = C.c_double
+    lib.hpgl_b200_covariance.argtypes = [C.c_int, C.POINTER(_HPGL_COV_PARAMS), i_p, i_p, i_p]
+    lib.hpgl_b200_version.restype = C.c_char_p
+    return lib
+
+
+_hpgl_so = _load()
+
+
+def last_error() -> str:
+    msg = _hpgl_so.hpgl_get_last_exception_message()
+    return msg.decode("utf-8", errors="replace") if msg else ""
+
+
+def check(rc: int, what: str) -> None:
+    if rc != 0:
+        raise RuntimeError(f"{what} failed ({rc}): {last_error()}")
+
+
+def last_stats() -> dict:
+    buf = (C.c_double * 9)()
+    _hpgl_so.hpgl_b200_last_stats(buf, 9)
+    keys = ["total_ms", "search_ms", "solve_ms", "tie_cells", "template_cells", "kriged_cells",
+            "kernel_launches", "h2d_bytes", "d2h_bytes"]
+    return {k: float(buf[i]) for i, k in enumerate(keys)}

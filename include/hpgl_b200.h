@@ -1,0 +1,175 @@
+/*
+ * hpgl_b200 — C ABI of the B200 kriging engine.
+ *
+ * Drop-in for the kriging entry points of HPGL's C API
+ * (itohnobue/hpgl-reborn, src/geo_bsd/hpgl/api.h). The structs below are
+ * laid out exactly as api.h:18-153 lays them out (same members, same order,
+ * natural alignment), so the reference's ctypes bindings
+ * (src/geo_bsd/hpgl_wrap.py:44-165) bind to this library unchanged.
+ *
+ * Ownership: every buffer belongs to the caller. Kriging entry points read
+ * and write HOST memory (pinned or pageable) unless the `_ex` flag
+ * HPGL_B200_DEVICE_POINTERS says the pointers are CUDA device pointers.
+ * Nothing the caller can see is allocated by the library.
+ *
+ * Errors: the reference-compatible entry points return void (or 0/-1 where
+ * the reference does) and keep the message of the last failure for
+ * hpgl_get_last_exception_message (api.cpp:30-50). The `_ex` entry points
+ * return 0 or a negative HPGL_B200_E* code and never abort.
+ */
+#ifndef HPGL_B200_H
+#define HPGL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ structs */
+/* api.h:18-22 */
+struct hpgl_shape_t { int m_data[3]; int m_strides[3]; };
+/* api.h:24-29 */
+struct hpgl_cont_masked_array_t { float *m_data; unsigned char *m_mask; struct hpgl_shape_t m_shape; };
+/* api.h:31-37 */
+struct hpgl_ind_masked_array_t { unsigned char *m_data; unsigned char *m_mask; struct hpgl_shape_t m_shape; int m_indicator_count; };
+/* api.h:51-60 */
+struct hpgl_ok_params_t {
+    int m_covariance_type; double m_ranges[3]; double m_angles[3]; double m_sill; double m_nugget;
+    int m_radiuses[3]; int m_max_neighbours;
+};
+/* api.h:62-73 */
+struct hpgl_sk_params_t {
+    int m_covariance_type; double m_ranges[3]; double m_angles[3]; double m_sill; double m_nugget;
+    int m_radiuses[3]; int m_max_neighbours; unsigned char m_automatic_mean; double m_mean;
+};
+/* api.h:75-82 */
+struct hpgl_cov_params_t { int m_covariance_type; double m_ranges[3]; double m_angles[3]; double m_sill; double m_nugget; };
+/* api.h:98-108 */
+struct hpgl_median_ik_params_t {
+    int m_covariance_type; double m_ranges[3]; double m_angles[3]; double m_sill; double m_nugget;
+    int m_radiuses[3]; int m_max_neighbours; double m_marginal_probs[2];
+};
+/* api.h:110-120 */
+struct hpgl_ik_params_t {
+    int m_covariance_type; double m_ranges[3]; double m_angles[3]; double m_sill; double m_nugget;
+    int m_radiuses[3]; int m_max_neighbours; double m_marginal_prob;
+};
+
+/* -------------------------------------------------- reference-compatible ABI */
+/* Replaces api.h:159-160 / api.cpp:38-41. */
+char *hpgl_get_last_exception_message(void);
+/* Replaces api.h:162-166 / output.cpp:58-68. Handlers run on the calling host
+ * thread only, never from a CUDA callback. */
+void hpgl_set_output_handler(int (*handler)(char *str, void *param), void *param);
+void hpgl_set_progress_handler(int (*handler)(char *stage, int percentage, void *param), void *param);
+/* Replaces api.h:168-169 / set_thread_num.cpp:22-33: the host-side worker
+ * count used to build covariance tables (the kriging itself runs on the GPU). */
+void hpgl_set_thread_num(int n_threads);
+int hpgl_get_thread_num(void);
+
+/* Replaces api.h:218-221 / api.cpp:253-293 (ordinary_kriging.cpp:14-48). */
+void hpgl_ordinary_kriging(struct hpgl_cont_masked_array_t *input_data, struct hpgl_ok_params_t *params,
+                           struct hpgl_cont_masked_array_t *output_data);
+/* Replaces api.h:223-230 / api.cpp:323-354 (simple_kriging.cpp:89-124). */
+void hpgl_simple_kriging(float *input_data, unsigned char *input_mask, struct hpgl_shape_t *input_data_shape,
+                         struct hpgl_sk_params_t *params, float *output_data, unsigned char *output_mask,
+                         struct hpgl_shape_t *output_data_shape);
+/* Replaces api.h:232-240 / api.cpp:356-410 (simple_kriging.cpp:67-87). */
+int hpgl_simple_kriging_weights(float *center_coords, float *neighbours_x, float *neighbours_y,
+                                float *neighbours_z, int neighbours_count, struct hpgl_cov_params_t *params,
+                                float *weights);
+/* Replaces api.h:267-272 / api.cpp:457-482 (indicator_kriging.h:88-161). */
+void hpgl_indicator_kriging(struct hpgl_ind_masked_array_t *in_data, struct hpgl_ind_masked_array_t *out_data,
+                            struct hpgl_ik_params_t *params, int indicator_count);
+/* Replaces api.h:274-277 / api.cpp:552-601 (median_ik.cpp:24-89). */
+void hpgl_median_ik(struct hpgl_ind_masked_array_t *in_data, struct hpgl_median_ik_params_t *params,
+                    struct hpgl_ind_masked_array_t *out_data);
+
+/* ------------------------------------------------------------ _ex extensions */
+/* status codes */
+#define HPGL_B200_OK 0
+#define HPGL_B200_EINVAL -1     /* bad argument (message says which) */
+#define HPGL_B200_ECUDA -2      /* CUDA error, or no usable device */
+#define HPGL_B200_ENOMEM -3     /* device memory exhausted */
+#define HPGL_B200_ELIMIT -4     /* a size beyond what the engine supports */
+
+/* precision modes */
+#define HPGL_B200_FP64_PLAIN 0      /* FP64 assembly, factorisation and solve */
+#define HPGL_B200_FP32_REFINED 1    /* FP32 assembly + factorisation, FP64-residual refinement */
+
+/* flags */
+#define HPGL_B200_DEVICE_POINTERS 1u   /* data/mask/outputs are device pointers */
+#define HPGL_B200_OUT_IS_CLONE 2u      /* output arrays already hold a copy of the input */
+
+/* per-cell status codes (written to `status` when non-null) */
+#define HPGL_B200_CELL_INFORMED -1     /* conditioning cell, copied */
+#define HPGL_B200_CELL_SUCCESS 0       /* kriged (KI_SUCCESS, kriging_interpolation.h:199-204) */
+#define HPGL_B200_CELL_NO_NEIGHBOURS 1 /* KI_NO_NEIGHBOURS */
+#define HPGL_B200_CELL_SINGULAR 2      /* KI_SINGULARITY: non-SPD factor or OK sum(A^-1 1) ~ 0 */
+
+struct hpgl_b200_options_t {
+    int precision;           /* HPGL_B200_FP64_PLAIN or HPGL_B200_FP32_REFINED */
+    int refine_steps;        /* FP64-residual refinement steps for FP32_REFINED (1..4; 0 -> 2) */
+    unsigned flags;          /* HPGL_B200_* flags */
+    void *stream;            /* cudaStream_t to run on; NULL -> the engine's own stream */
+    double *estimate64;      /* optional: FP64 estimate per cell (NaN where not kriged) */
+    double *variance;        /* optional: kriging variance per cell (-1 where not kriged) */
+    signed char *status;     /* optional: per-cell status (HPGL_B200_CELL_*) */
+    float *ik_probs;         /* optional (IK): corrected probabilities, cell-major [cell][category] */
+};
+
+/* OK / SK over a whole grid with options; dims = (nx, ny, nz), Fortran order.
+ * kind 0 = ordinary (params from ok), 1 = simple (sk). The output arrays
+ * follow the reference's rules (cont_kriging.h:63-117). */
+int hpgl_b200_cont_kriging_ex(int kind, const int *dims, const float *in_data, const unsigned char *in_mask,
+                              const struct hpgl_sk_params_t *params, float *out_data, unsigned char *out_mask,
+                              const struct hpgl_b200_options_t *opt);
+/* Full IK (indicator_count > 2 categories, per-category models) or, with one
+ * params entry and indicator_count == 2, median IK (median_ik.cpp:24-89). */
+int hpgl_b200_indicator_kriging_ex(const int *dims, const unsigned char *in_data, const unsigned char *in_mask,
+                                   const struct hpgl_ik_params_t *params, int indicator_count,
+                                   unsigned char *out_data, unsigned char *out_mask,
+                                   const struct hpgl_b200_options_t *opt);
+int hpgl_b200_median_ik_ex(const int *dims, const unsigned char *in_data, const unsigned char *in_mask,
+                           const struct hpgl_median_ik_params_t *params, unsigned char *out_data,
+                           unsigned char *out_mask, const struct hpgl_b200_options_t *opt);
+
+/* Neighbour lists exactly as indexed_neighbour_lookup_t::find returns them
+ * (sugarbox_indexed_neighbour_lookup.h:67-124) for the listed nodes: node
+ * indices, -1 padded to max_neighbours; `path` gets 1 where the template scan
+ * ran. kind 0 = analytic covariance (OK), 1 = truncated table (SK / IK /
+ * median IK). Host pointers. */
+int hpgl_b200_find_neighbours(int kind, const int *dims, const unsigned char *mask,
+                              const struct hpgl_sk_params_t *params, const int *nodes, int n_nodes,
+                              int *out_idx, int *out_count, unsigned char *out_path);
+
+/* Timing of the last call on this thread's engine: device milliseconds of
+ * the whole pipeline and of each stage, and counters. Returns the number of
+ * doubles written (<= cap): [total_ms, search_ms, solve_ms, straddle_cells,
+ * template_cells, kriged_cells, kernel_launches, h2d_bytes, d2h_bytes]. */
+int hpgl_b200_last_stats(double *out, int cap);
+
+/* Page-locked host buffers for fast copies (cudaHostAlloc / cudaFreeHost). */
+void *hpgl_b200_host_alloc(size_t bytes);
+void hpgl_b200_host_free(void *p);
+
+/* Host-side pieces, callable without a GPU. */
+/* The anisotropy transform of cov_model.h:16-61 (row-major, 9 doubles). */
+int hpgl_b200_transform(const double *ranges, const double *angles, double *out9);
+/* The sorted search template of calc_cov_field (covariance_field.h:62-106):
+ * up to `cap` (dx,dy,dz) triples; returns its length, limit = length / 250
+ * (sugarbox_indexed_neighbour_lookup.h:59). kind as for find_neighbours. */
+int hpgl_b200_template(int kind, const struct hpgl_cov_params_t *cov, const int *radiuses, int *out, int cap,
+                       int *out_limit);
+/* Covariance between two integer points for a flavour (kind as above). */
+double hpgl_b200_covariance(int kind, const struct hpgl_cov_params_t *cov, const int *radiuses, const int *a,
+                            const int *b);
+/* Library version string. */
+const char *hpgl_b200_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HPGL_B200_H */
