@@ -1,0 +1,382 @@
+"""Benchmark: kriged cells/s on one B200 — FP32-refined (headline) vs FP64 plain.
+
+Workload (default): ordinary kriging on the 256x256x128 grid (8.4M cells), 1%
+seeded conditioning cells with lognormal(0, 0.5) values, exponential model
+ranges (30,15,6) azimuth 30, nugget 0.05, radiuses (30,15,6), max_neighbours 32
+(geo_bsd.workloads.sk_ok_large; synthetic, no dataset).
+
+A step is one whole-grid kriging call through the engine's C ABI
+(hpgl_b200_cont_kriging_ex): neighbour search + per-cell solves + estimate and
+variance for every uninformed cell. `value` has the inputs resident in HBM
+(device pointers, CUDA events on the launching stream); `e2e` repeats the call
+with pinned HOST buffers, so each step includes the host->device copy of data
+and mask and the device->host copy of estimate, mask and variance.
+
+Usage:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+For N > 1 the driver runs it under torchrun; every rank runs its own replica
+(the path needs no collective) and rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "hpgl-reborn_b200"))
+
+METRIC = "kriged cells/s, 1 B200: FP32-refined vs FP64 plain at <=1e-6 rel err"
+UNIT = "cells/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", default="sk_ok_large")
+    ap.add_argument("--kind", choices=["ok", "sk"], default="ok")
+    ap.add_argument("--skip-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--profile-case", type=float, default=0.0, metavar="SCALE",
+                    help="run one FP32-refined device call on the workload shrunk by SCALE and exit "
+                         "(the case profiled with ncu)")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def load_workload(name):
+    from geo_bsd import workloads as WL
+    return WL.ALL[name](1.0)
+
+
+# ---------------------------------------------------------------- CPU baseline
+def cpu_reference(wl, kind, target_seconds, threads):
+    """Reference CPU path (oracle/_ref, the reference's own code) on a sample of
+    uninformed cells; falls back to the CPU restatement if the reference build
+    is absent. Returns (cells/s, dict)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    which = "ref" if O.available("ref") else "port"
+    unk = np.flatnonzero(wl.mask == 0)
+    rng = np.random.default_rng(123)
+    k = 0 if kind == "ok" else 1
+    mean = float(wl.data[wl.mask == 1].astype(np.float64).mean()) if kind == "sk" else 0.0
+
+    def timed(nodes):
+        t0 = time.perf_counter()
+        O.krige_nodes(which, k, wl.dims, wl.data, wl.mask, wl.cov, wl.radiuses, wl.max_neighbours, mean=mean,
+                      nodes=nodes, threads=threads, want_idx=False)
+        return time.perf_counter() - t0
+
+    setup = timed(np.zeros(0, np.int32))  # template + clusterizer construction only
+    probe = np.sort(rng.choice(unk, min(4000, len(unk)), replace=False)).astype(np.int32)
+    t_probe = max(timed(probe) - setup, 1e-3)
+    rate = len(probe) / t_probe
+    n = int(min(len(unk), max(len(probe), rate * target_seconds)))
+    sample = np.sort(rng.choice(unk, n, replace=False)).astype(np.int32)
+    t = timed(sample) - setup
+    return n / t, {"which": which, "sample_cells": n, "seconds": t, "setup_seconds": setup, "threads": threads}
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+        self.thread = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------- engine runs
+def peak_table():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peaks = {}
+    if os.path.exists(path):
+        with open(path) as f:
+            peaks = json.load(f)
+    mhz = peaks.get("sm_max_mhz", 1965.0)
+    src = "measured sm_max_mhz" if "sm_max_mhz" in peaks else "fallback 1965 MHz"
+    # CUDA-core peaks: 148 SMs x (128 FP32 | 64 FP64) lanes x 2 flop/FMA x clock
+    return {"fp32": 148 * 128 * 2 * mhz * 1e6 / 1e12, "fp64": 148 * 64 * 2 * mhz * 1e6 / 1e12,
+            "hbm_gbs": peaks.get("hbm_gbs", 6650.0), "source": src}
+
+
+def traffic_per_cell():
+    """DRAM bytes per kriged cell of the dominant solve kernel from the committed
+    ncu summary (profiles/solve_kernel_traffic.json), or None."""
+    path = os.path.join(ROOT, "profiles", "solve_kernel_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    return d.get("dram_bytes_per_cell")
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    import torch
+
+    if args.impl == "reference":
+        if rank == 0:
+            wl = load_workload(args.workload)
+            threads = os.cpu_count() or 1
+            vals = []
+            info = None
+            for i in range(args.warmup + args.steps):
+                v, info = cpu_reference(wl, args.kind, min(args.cpu_seconds, 8.0), threads)
+                if i >= args.warmup:
+                    vals.append(v)
+            value = float(np.median(vals))
+            line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+                    "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                    "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, geo_bsd.workloads)",
+                    "config": {"workload": f"{args.workload} {args.kind.upper()} (256x256x128, k=32)",
+                               "sample": f"{info['sample_cells']} random uninformed cells per step"},
+                    "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
+                                     "kind": "reference" if info["which"] == "ref" else "port",
+                                     "sample": f"{info['sample_cells']} random uninformed cells, lookup built once"},
+                    "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            print(json.dumps(line), flush=True)
+        return
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist_mod
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+        dist = dist_mod
+    from geo_bsd import hpgl_wrap as W
+
+    if args.profile_case > 0:
+        from geo_bsd import workloads as WL
+        wl = WL.ALL[args.workload](args.profile_case)
+    else:
+        wl = load_workload(args.workload)
+    kind = 0 if args.kind == "ok" else 1
+    n = wl.n_cells
+    dev = torch.device("cuda", local)
+    d_data = torch.from_numpy(np.ascontiguousarray(wl.data)).to(dev)
+    d_mask = torch.from_numpy(np.ascontiguousarray(wl.mask)).to(dev)
+    d_out = d_data.clone()
+    d_omask = d_mask.clone()
+    d_var = torch.empty(n, dtype=torch.float64, device=dev)
+    d_est = torch.empty(n, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+    dims = (C.c_int * 3)(*wl.dims)
+    p = W._HPGL_SK_PARAMS(covariance_type=wl.cov.cov_type, ranges=wl.cov.ranges, angles=wl.cov.angles,
+                          sill=wl.cov.sill, nugget=wl.cov.nugget, radiuses=wl.radiuses,
+                          max_neighbours=wl.max_neighbours, automatic_mean=1, mean=0.0)
+
+    def dev_call(precision, est=False):
+        o = W._HPGL_B200_OPTIONS(precision=precision, refine_steps=3,
+                                 flags=W.FLAG_DEVICE_POINTERS | W.FLAG_OUT_IS_CLONE, stream=stream.cuda_stream,
+                                 estimate64=d_est.data_ptr() if est else None, variance=d_var.data_ptr(),
+                                 status=None, ik_probs=None)
+        rc = W._hpgl_so.hpgl_b200_cont_kriging_ex(kind, dims, d_data.data_ptr(), d_mask.data_ptr(), C.byref(p),
+                                                  d_out.data_ptr(), d_omask.data_ptr(), C.byref(o))
+        W.check(rc, "cont_kriging_ex")
+        return W.last_stats()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed_device(precision):
+        for _ in range(args.warmup):
+            dev_call(precision)
+        times, stats = [], []
+        for _ in range(args.steps):
+            flush.zero_()  # L2 flush between steps (outside the timed region)
+            barrier()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st = dev_call(precision)
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+            stats.append(st)
+        barrier()
+        return times, stats
+
+    if args.profile_case > 0:
+        st = dev_call(1)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_case": wl.dims, "stats": st}), flush=True)
+        return
+
+    # accuracy of the FP32-refined estimate against the FP64 plain one, same grid
+    dev_call(0, est=True)
+    est64 = d_est.clone()
+    dev_call(1, est=True)
+    kriged = torch.isfinite(est64) & (d_mask == 0)
+    diff = (d_est - est64)[kriged].abs().max().item()
+    scale = est64[kriged].abs().max().item()
+    rel_err = diff / scale if scale > 0 else 0.0
+
+    t64, s64 = timed_device(0)
+    with ClockSampler(local) as clk:
+        t32, s32 = timed_device(1)
+    ms32 = max_over_ranks(float(np.mean(t32)))
+    ms64 = max_over_ranks(float(np.mean(t64)))
+    cells = s32[-1]["kriged_cells"]
+    value = cells * world / (ms32 / 1e3)
+    value64 = s64[-1]["kriged_cells"] * world / (ms64 / 1e3)
+    launches = int(sum(s["kernel_launches"] for s in s32))
+
+    # roofline of the dominant kernel (the solve bucket with the largest time)
+    last = s32[-1]
+    b = int(np.argmax([last[f"bucket_ms_{i}"] for i in range(5)])) if "bucket_ms_0" in last else 2
+    pk = peak_table()
+    b_ms = float(np.mean([s[f"bucket_ms_{b}"] for s in s32]))
+    b_flops = last[f"bucket_flops_{b}"]
+    achieved = b_flops / (b_ms / 1e3) / 1e12
+    tpc = traffic_per_cell()
+    roofline = {"bound": "fp32", "kernel": f"k_solve<NP={[8, 16, 32, 64, 'large'][b]}, float, refined>",
+                "achieved": achieved, "peak": pk["fp32"], "unit": "TFLOP/s", "frac": achieved / pk["fp32"],
+                "traffic": (tpc * last[f"bucket_items_{b}"]) if tpc else None,
+                "peak_source": f"CUDA-core FP32 peak 148 SM x 128 lanes x 2 x {pk['source']}",
+                "algorithmic_flops_per_launch": b_flops, "kernel_ms": b_ms}
+    s64b = s64[-1]
+    b64 = int(np.argmax([s64b[f"bucket_ms_{i}"] for i in range(5)]))
+    fp64_kernel_tflops = s64b[f"bucket_flops_{b64}"] / (np.mean([s[f"bucket_ms_{b64}"] for s in s64]) / 1e3) / 1e12
+
+    # end to end through the C ABI with pinned host buffers
+    lib = W._hpgl_so
+    nbytes = n * 4
+    h_ptrs = [lib.hpgl_b200_host_alloc(sz) for sz in (nbytes, n, nbytes, n, n * 8)]
+    h_data, h_mask, h_out, h_omask, h_var = h_ptrs
+    C.memmove(h_data, np.ascontiguousarray(wl.data).ctypes.data, nbytes)
+    C.memmove(h_mask, np.ascontiguousarray(wl.mask).ctypes.data, n)
+    C.memmove(h_out, h_data, nbytes)
+    C.memmove(h_omask, h_mask, n)
+
+    def host_call():
+        o = W._HPGL_B200_OPTIONS(precision=1, refine_steps=3, flags=W.FLAG_OUT_IS_CLONE, stream=None,
+                                 estimate64=None, variance=h_var, status=None, ik_probs=None)
+        rc = lib.hpgl_b200_cont_kriging_ex(kind, dims, h_data, h_mask, C.byref(p), h_out, h_omask, C.byref(o))
+        W.check(rc, "cont_kriging_ex (host)")
+        return W.last_stats()
+
+    for _ in range(args.warmup):
+        host_call()
+    e2e_t = []
+    st = None
+    for _ in range(args.steps):
+        barrier()
+        t0 = time.perf_counter()
+        st = host_call()
+        e2e_t.append(time.perf_counter() - t0)
+    barrier()
+    e2e_s = max_over_ranks(float(np.mean(e2e_t)))
+    e2e_value = st["kriged_cells"] * world / e2e_s
+    for ptr in h_ptrs:
+        lib.hpgl_b200_host_free(ptr)
+
+    cpu = None
+    if rank == 0 and not args.skip_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, info = cpu_reference(wl, args.kind, args.cpu_seconds, threads)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "reference" if info["which"] == "ref" else "port",
+               "sample": f"{info['sample_cells']} random uninformed cells of the same grid; the reference's own "
+                         f"per-node code (kriging_interpolation) over OpenMP, lookup construction excluded "
+                         f"({info['setup_seconds']:.2f}s)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (FP64-refined residuals)", "data": "synthetic (seeded, geo_bsd.workloads)",
+            "config": {"workload": f"{'ordinary' if kind == 0 else 'simple'} kriging {wl.dims[0]}x{wl.dims[1]}x"
+                                   f"{wl.dims[2]}, 1% lognormal conditioning, exponential (30,15,6) az 30, "
+                                   f"k={wl.max_neighbours}", "precision": "fp32_refined",
+                       "l2": "flushed between timed steps (256 MB write)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "fp64_plain": {"value": value64, "ms_per_step": ms64, "kernel_tflops": fp64_kernel_tflops,
+                           "kernel_frac_of_fp64_peak": fp64_kernel_tflops / pk["fp64"]},
+            "fp32_refined_over_fp64_plain": value / value64,
+            "rel_err_fp32_refined_vs_fp64": rel_err,
+            "escalated_cells": last["escalated_cells"],
+            "stages_ms": {k[len("stage_"):-len("_ms")]: round(v, 3) for k, v in last.items() if k.startswith("stage_")},
+            "tie_resolved_cells": last["tie_cells"],
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(st["h2d_bytes"]),
+                    "d2h_bytes_per_step": int(st["d2h_bytes"]), "timing": "wall clock per call (host tables, "
+                                                                         "copies and kernels)"},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -131,6 +131,7 @@ hb::Options options_from(const hpgl_b200_options_t *o)
     r.variance = o->variance;
     r.status = o->status;
     r.ik_probs = o->ik_probs;
+    r.tolerance = o->tolerance;
     return r;
 }
 
@@ -345,9 +346,17 @@ int hpgl_b200_find_neighbours(int kind, const int *dims, const unsigned char *ma
 int hpgl_b200_last_stats(double *out, int cap)
 {
     hb::Stats s = hb::last_stats();
-    double v[9] = {s.total_ms, s.search_ms, s.solve_ms, (double)s.ties, (double)s.template_cells,
-                   (double)s.kriged, (double)s.launches, (double)s.h2d, (double)s.d2h};
-    int n = cap < 9 ? cap : 9;
+    double v[HPGL_B200_STATS_LEN] = {s.total_ms, s.search_ms, s.solve_ms, (double)s.ties, (double)s.template_cells,
+                                     (double)s.kriged, (double)s.launches, (double)s.h2d, (double)s.d2h,
+                                     (double)s.escalated, s.search_kernel_ms};
+    for (int b = 0; b < 5; ++b)
+    {
+        v[11 + b] = (double)s.bucket_items[b];
+        v[16 + b] = s.bucket_ms[b];
+        v[21 + b] = s.bucket_flops[b];
+    }
+    for (int i = 0; i < hb::kStages; ++i) v[26 + i] = s.stage_ms[i];
+    int n = cap < HPGL_B200_STATS_LEN ? cap : HPGL_B200_STATS_LEN;
     for (int i = 0; i < n; ++i) out[i] = v[i];
     return n;
 }

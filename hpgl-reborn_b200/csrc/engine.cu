@@ -77,6 +77,8 @@ class Engine
         n_sm_ = prop.multiProcessorCount;
         max_smem_ = (int)prop.sharedMemPerBlockOptin;
         for (int i = 0; i < kNumEvents; ++i) HB_CK(cudaEventCreate(&ev_[i]));
+        for (int i = 0; i < 64; ++i) HB_CK(cudaEventCreate(&stage_ev_[i]));
+        HB_CK(cudaEventCreate(&stage_start_));
     }
 
     template <typename T>
@@ -96,14 +98,42 @@ class Engine
         return reinterpret_cast<T *>(b.p);
     }
 
+    // Stage timing: mark(id) records the end of stage `id` on the stream; the
+    // stage lasts from the previous mark (or the call start).
+    void mark(int id, cudaStream_t st)
+    {
+        if (id < 0 || id >= kStages) return;
+        HB_CK(cudaEventRecord(stage_ev_[n_marks_ % 64], st));
+        mark_id_[n_marks_ % 64] = id;
+        ++n_marks_;
+    }
+    void reset_marks(cudaStream_t st)
+    {
+        n_marks_ = 0;
+        HB_CK(cudaEventRecord(stage_start_, st));
+    }
+    void collect_marks()
+    {
+        cudaEvent_t prev = stage_start_;
+        for (int i = 0; i < n_marks_ && i < 64; ++i)
+        {
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, prev, stage_ev_[i]) == cudaSuccess) stats.stage_ms[mark_id_[i]] += ms;
+            prev = stage_ev_[i];
+        }
+    }
     int n_sm() const { return n_sm_; }
     int max_smem() const { return max_smem_; }
     cudaStream_t stream(const void *user) const { return user ? (cudaStream_t)user : own_stream_; }
-    static constexpr int kNumEvents = 8;
+    static constexpr int kNumEvents = 32;
     cudaEvent_t ev_[kNumEvents];
     Stats stats;
 
   private:
+    cudaEvent_t stage_ev_[64];
+    cudaEvent_t stage_start_;
+    int mark_id_[64];
+    int n_marks_ = 0;
     int device_;
     cudaStream_t own_stream_ = nullptr;
     int n_sm_ = 148;
@@ -261,6 +291,7 @@ static DevPoints compact_points(Engine &E, const Geom &g, const uint8_t *d_mask,
     int *pos = E.buf<int>("pos", (size_t)n);
     int *tmp = E.buf<int>("scan_tmp", (size_t)scan_tmp_ints(n) + 4);
     P.n_pts = E.buf<int>("n_pts", 1);
+    E.mark(STAGE_UPLOAD, st);
     launch_flag_informed(d_mask, n, pos, st);
     exclusive_scan(pos, n, tmp, P.n_pts, st);
     HB_CK(cudaGetLastError());
@@ -269,17 +300,19 @@ static DevPoints compact_points(Engine &E, const Geom &g, const uint8_t *d_mask,
     size_t m = std::max(P.m, 1);
     P.pts_node = E.buf<int>("pts_node", m);
     P.pts_xyz = E.buf<unsigned long long>("pts_xyz", m);
-    if (d_val_f) P.pts_val = E.buf<float>("pts_val", m);
+    P.pts_val = E.buf<float>("pts_val", m);
     if (d_val_u8) P.pts_cat = E.buf<uint8_t>("pts_cat", m);
     P.pid_of_node = E.buf<int>("pid_of_node", (size_t)n);
     launch_emit_points(d_mask, pos, g, d_val_f, d_val_u8, P.pts_node, P.pts_xyz, P.pts_val, P.pts_cat,
                        P.pid_of_node, st);
     HB_CK(cudaGetLastError());
+    E.mark(STAGE_COMPACT, st);
     return P;
 }
 
 struct DevSearch
 {
+    int2 *nb_rec = nullptr;
     int *nb_pid = nullptr;
     int *nb_n = nullptr;
     uint8_t *bin_flag = nullptr;
@@ -294,7 +327,7 @@ struct DevSearch
 // uninformed ones. Table slots are suffixed with `tag` so several flavours can
 // coexist (IK categories run one after another and reuse them).
 static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const uint8_t *d_mask, int all_cells,
-                            cudaStream_t st)
+                            cudaStream_t st, bool want_pids = false)
 {
     const Geom &g = pl.g;
     DevSearch S;
@@ -306,11 +339,24 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
     std::vector<int4> t4(std::max<size_t>(pl.tmpl.size(), 1));
     for (size_t i = 0; i < pl.tmpl.size(); ++i) t4[i] = make_int4(pl.tmpl[i].dx, pl.tmpl[i].dy, pl.tmpl[i].dz, 0);
     int4 *tmpl = E.buf<int4>("tmpl", t4.size());
+    // 16-bit ranks for the fast selection path when the rank space allows it
+    const bool fast_keys = g.k <= 64 && pl.kt.n_ranks <= 0xFFFE;
+    uint16_t *keytab16 = nullptr;
+    if (fast_keys)
+    {
+        std::vector<uint16_t> k16(pl.kt.rank.size());
+        for (size_t i = 0; i < k16.size(); ++i)
+            k16[i] = pl.kt.rank[i] == KEY_EXCLUDED ? (uint16_t)0xFFFF : (uint16_t)pl.kt.rank[i];
+        keytab16 = E.buf<uint16_t>("keytab16", k16.size());
+        HB_CK(cudaMemcpyAsync(keytab16, k16.data(), k16.size() * 2, cudaMemcpyHostToDevice, st));
+        HB_CK(cudaStreamSynchronize(st)); // k16 is a temporary
+    }
     HB_CK(cudaMemcpyAsync(tmpl, t4.data(), t4.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
     long long pn = (long long)g.pnx * g.pny * (2 * g.phz + 1);
     S.pair64 = E.buf<double>("pair64", (size_t)pn);
     S.pair32 = E.buf<float>("pair32", (size_t)pn);
     launch_build_pair(g, dev_model(pl.f.m), pl.f.truncated ? 1 : 0, S.search_vals, S.pair64, S.pair32, st);
+    E.mark(STAGE_TABLES, st);
 
     // bins
     int *bin_cnt = E.buf<int>("bin_cnt", g.n_bins);
@@ -333,89 +379,163 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
     int host_scal[8];
     HB_CK(cudaMemcpyAsync(host_scal, scal, sizeof(host_scal), cudaMemcpyDeviceToHost, st));
     HB_CK(cudaStreamSynchronize(st));
+    E.mark(STAGE_BINS, st);
     int max_cand = host_scal[1];
 
     // search
     int cand_cap = std::max(4, (max_cand + 3) / 4 * 4);
+    const bool fast = fast_keys && cand_cap <= 65536;
+    auto smem_need = [&](int w) {
+        return fast ? search_fast_smem_bytes(cand_cap, g.k, w) : search_smem_bytes(cand_cap, g.k, w);
+    };
     int warps = 8;
-    while (warps > 1 && search_smem_bytes(cand_cap, g.k, warps) > (size_t)E.max_smem()) --warps;
-    if (search_smem_bytes(cand_cap, g.k, warps) > (size_t)E.max_smem())
+    while (warps > 1 && smem_need(warps) > (size_t)E.max_smem()) --warps;
+    if (smem_need(warps) > (size_t)E.max_smem())
         throw CudaFail{-4, "neighbour candidate list too long for shared memory (" + std::to_string(max_cand) +
                                " candidates)"};
-    S.nb_pid = E.buf<int>("nb_pid", (size_t)g.n_cells * g.k);
+    S.nb_rec = E.buf<int2>("nb_rec", (size_t)g.n_cells * g.k);
+    S.nb_pid = want_pids ? E.buf<int>("nb_pid", (size_t)g.n_cells * g.k) : nullptr;
     S.nb_n = E.buf<int>("nb_n", (size_t)g.n_cells);
     int *tie_cells = E.buf<int>("tie_cells", (size_t)g.n_cells);
     HB_CK(cudaMemsetAsync(S.nb_n, 0, sizeof(int) * g.n_cells, st));
-    HB_CK(launch_search(g, d_mask, all_cells, bin_start, bin_cnt, S.bin_flag, bin_pts, P.pts_xyz, keytab,
-                        pl.rank_bits, tmpl, (int)pl.tmpl.size(), P.pid_of_node, cand_cap, warps, S.nb_pid, S.nb_n,
-                        tie_cells, scal + 3, scal + 4, st));
+    HB_CK(cudaEventRecord(E.ev_[8], st));
+    if (fast)
+        HB_CK(launch_search_fast(g, d_mask, all_cells, bin_start, bin_cnt, S.bin_flag, bin_pts, P.pts_xyz, P.pts_val,
+                                 keytab16, tmpl, (int)pl.tmpl.size(), P.pid_of_node, cand_cap, warps, S.nb_pid,
+                                 S.nb_rec, S.nb_n, tie_cells, scal + 3, scal + 4, st));
+    else
+        HB_CK(launch_search(g, d_mask, all_cells, bin_start, bin_cnt, S.bin_flag, bin_pts, P.pts_xyz, P.pts_val,
+                            keytab, pl.rank_bits, tmpl, (int)pl.tmpl.size(), P.pid_of_node, cand_cap, warps,
+                            S.nb_pid, S.nb_rec, S.nb_n, tie_cells, scal + 3, scal + 4, st));
+    HB_CK(cudaEventRecord(E.ev_[9], st));
     HB_CK(cudaMemcpyAsync(host_scal, scal, sizeof(host_scal), cudaMemcpyDeviceToHost, st));
     HB_CK(cudaStreamSynchronize(st));
     S.ties = host_scal[3];
     S.template_cells = host_scal[4];
-    E.stats.launches += 8;
+    E.mark(STAGE_SEARCH, st);
+    {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, E.ev_[8], E.ev_[9]);
+        E.stats.search_kernel_ms += ms;
+    }
+    // flag, scan tiles (+add), emit, pair table, bin count, bin scan, fill, sort, region, search
+    E.stats.launches += 10 + (g.n_cells > 1024 ? 2 : 0);
 
-    // tie groups straddling the k-th slot: exact std::sort permutation
+    // tie groups straddling the k-th slot: std::sort's choice, replayed
     if (S.ties > 0)
     {
         int cap = std::max(max_cand, 1);
-        size_t per = (size_t)cap * tie_entry_bytes();
-        size_t budget = (size_t)512 << 20;
-        int chunk = (int)std::max<size_t>(1, std::min<size_t>(budget / per, (size_t)S.ties));
-        void *scratch = E.buf<unsigned char>("tie_scratch", per * chunk);
-        for (int first = 0; first < S.ties; first += chunk)
+        if (fast && resolve_ties_fast_smem(cap, 4) <= (size_t)E.max_smem())
         {
-            launch_resolve_ties(g, tie_cells, scal + 3, first, chunk, bin_start, bin_cnt, bin_pts, P.pts_xyz,
-                                keytab, scratch, cap, S.nb_pid, st);
+            HB_CK(launch_resolve_ties_fast(g, tie_cells, scal + 3, S.ties, bin_start, bin_cnt, bin_pts, P.pts_xyz,
+                                           P.pts_val, keytab16, cap, S.nb_pid, S.nb_rec, E.n_sm(), st));
             E.stats.launches += 1;
+        }
+        else
+        {
+            size_t per = (size_t)cap * tie_entry_bytes();
+            size_t budget = (size_t)512 << 20;
+            int chunk = (int)std::max<size_t>(1, std::min<size_t>(budget / per, (size_t)S.ties));
+            void *scratch = E.buf<unsigned char>("tie_scratch", per * chunk);
+            for (int first = 0; first < S.ties; first += chunk)
+            {
+                launch_resolve_ties(g, tie_cells, scal + 3, first, chunk, bin_start, bin_cnt, bin_pts, P.pts_xyz,
+                                    P.pts_val, keytab, scratch, cap, S.nb_pid, S.nb_rec, st);
+                E.stats.launches += 1;
+            }
         }
         HB_CK(cudaGetLastError());
     }
+    E.mark(STAGE_TIES, st);
     return S;
 }
 
-// Solve every bucket for one search result.
+// Solve every bucket for one search result. FP32-refined systems that do not
+// converge (or whose float factor breaks down) are re-solved in FP64.
 static void run_solves(Engine &E, const Plan &pl, const DevPoints &P, const DevSearch &S, const uint8_t *d_mask,
-                       int all_cells, bool ordinary, int precision, int steps, double mean, int ind_value,
-                       signed char *d_status, const SolveOut &out, cudaStream_t st)
+                       int all_cells, bool ordinary, int precision, int steps, double tol, double mean,
+                       int ind_value, signed char *d_status, const SolveOut &out, cudaStream_t st)
 {
+    if (!(tol > 0.0)) tol = 1e-9;
+    (void)P;
     const Geom &g = pl.g;
     int *bucket_cnt = E.buf<int>("bucket_cnt", kBuckets);
     int *bucket_off = E.buf<int>("bucket_off", kBuckets + 1);
     int *bucket_fill = E.buf<int>("bucket_fill", kBuckets);
     int *cells = E.buf<int>("cells", (size_t)g.n_cells);
-    launch_prepare(g, d_mask, all_cells, S.nb_n, d_status, bucket_cnt, bucket_off, bucket_fill, cells, st);
+    unsigned long long *moments = E.buf<unsigned long long>("moments", kBuckets * 3);
+    int *esc_cnt = E.buf<int>("esc_cnt", kBuckets);
+    int *esc_cells = precision ? E.buf<int>("esc_cells", (size_t)g.n_cells) : nullptr;
+    launch_prepare(g, d_mask, all_cells, S.nb_n, d_status, bucket_cnt, bucket_off, bucket_fill, cells, moments, st);
+    HB_CK(cudaMemsetAsync(esc_cnt, 0, sizeof(int) * kBuckets, st));
     HB_CK(cudaGetLastError());
+    E.stats.launches += 3;
     int cnt[kBuckets];
+    unsigned long long mom[kBuckets * 3];
     HB_CK(cudaMemcpyAsync(cnt, bucket_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, st));
+    HB_CK(cudaMemcpyAsync(mom, moments, sizeof(mom), cudaMemcpyDeviceToHost, st));
     HB_CK(cudaStreamSynchronize(st));
+    E.mark(STAGE_PREPARE, st);
     int off = 0;
     const double c0 = pl.f.c0();
+    const double rhs = ordinary ? 2.0 : 1.0;
+    int esc_off[kBuckets];
     for (int b = 0; b < kBuckets; ++b)
     {
+        esc_off[b] = off;
         if (cnt[b] > 0)
         {
             const int *bcells = cells + off;
-            // bucket item counts live in bucket_cnt[b]
+            HB_CK(cudaEventRecord(E.ev_[10 + 2 * b], st));
             if (b < 4)
             {
                 HB_CK(launch_solve_bucket(kBucketNP[b], precision, ordinary, g, bcells, bucket_cnt + b, cnt[b],
-                                          S.nb_pid, S.nb_n, P.pts_xyz, P.pts_val, P.pts_cat, ind_value, S.pair64,
-                                          S.pair32, mean, c0, steps, out, E.n_sm(), st));
+                                          S.nb_rec, S.nb_n, ind_value, S.pair64, S.pair32, mean, c0, steps, tol, out,
+                                          esc_cells ? esc_cells + off : nullptr, esc_cnt + b, E.n_sm(), st));
             }
             else
             {
                 int blocks = std::min(cnt[b], E.n_sm() * 2);
                 double *scratch = E.buf<double>("large_scratch", large_scratch_doubles(g.k, blocks));
-                HB_CK(launch_solve_large(g, bcells, bucket_cnt + b, blocks, S.nb_pid, S.nb_n, P.pts_xyz, P.pts_val,
-                                         P.pts_cat, ind_value, S.pair64, ordinary, mean, c0, scratch, out, st));
+                HB_CK(launch_solve_large(g, bcells, bucket_cnt + b, blocks, S.nb_rec, S.nb_n, ind_value, S.pair64,
+                                         ordinary, mean, c0, scratch, out, st));
             }
+            HB_CK(cudaEventRecord(E.ev_[11 + 2 * b], st));
             E.stats.launches += 1;
             E.stats.kriged += cnt[b];
+            E.stats.bucket_items[b] += cnt[b];
+            const double s1 = (double)mom[3 * b], s2 = (double)mom[3 * b + 1], s3 = (double)mom[3 * b + 2];
+            // F(n, r) = n^3/3 + n^2/2 + 2 r n^2 + 30 (n(n+1)/2 + n) + 2 r n, summed over the bucket
+            E.stats.bucket_flops[b] += s3 / 3.0 + s2 * (0.5 + 2.0 * rhs + 15.0) + s1 * (45.0 + 2.0 * rhs);
         }
         off += cnt[b];
     }
-    E.stats.launches += 3;
+    if (precision)
+    {
+        // FP64 re-solve of escalated systems, one persistent launch per bucket
+        for (int b = 0; b < 4; ++b)
+        {
+            if (cnt[b] == 0) continue;
+            HB_CK(launch_solve_bucket(kBucketNP[b], 0, ordinary, g, esc_cells + esc_off[b], esc_cnt + b,
+                                      std::min(cnt[b], E.n_sm() * 8), S.nb_rec, S.nb_n, ind_value, S.pair64,
+                                      S.pair32, mean, c0, 0, tol, out, nullptr, nullptr, E.n_sm(), st));
+            E.stats.launches += 1;
+        }
+        int esc[kBuckets];
+        HB_CK(cudaMemcpyAsync(esc, esc_cnt, sizeof(esc), cudaMemcpyDeviceToHost, st));
+        HB_CK(cudaStreamSynchronize(st));
+        for (int b = 0; b < kBuckets; ++b) E.stats.escalated += esc[b];
+    }
+    else
+        HB_CK(cudaStreamSynchronize(st));
+    E.mark(STAGE_SOLVE, st);
+    for (int b = 0; b < kBuckets; ++b)
+        if (cnt[b] > 0)
+        {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, E.ev_[10 + 2 * b], E.ev_[11 + 2 * b]);
+            E.stats.bucket_ms[b] += ms;
+        }
 }
 
 // ------------------------------------------------------------------ io helpers
@@ -447,6 +567,7 @@ static void begin_call(Engine &E, cudaStream_t st)
 {
     E.stats = Stats();
     HB_CK(cudaEventRecord(E.ev_[0], st));
+    E.reset_marks(st);
 }
 static void end_call(Engine &E, cudaStream_t st)
 {
@@ -455,6 +576,7 @@ static void end_call(Engine &E, cudaStream_t st)
     float ms = 0;
     HB_CK(cudaEventElapsedTime(&ms, E.ev_[0], E.ev_[1]));
     E.stats.total_ms = ms;
+    E.collect_marks();
 }
 
 // ------------------------------------------------------------------ entry points
@@ -543,16 +665,19 @@ int cont_kriging(int kind, const int *dims, const float *in_data, const unsigned
         so.status = d_status;
         so.write_cont = 1;
         int steps = opt.refine_steps > 0 ? opt.refine_steps : 2;
-        run_solves(E, pl, P, S, d_mask, 0, !simple, opt.precision, steps, mean, -1, d_status, so, st);
+        run_solves(E, pl, P, S, d_mask, 0, !simple, opt.precision, steps, opt.tolerance, mean, -1, d_status, so, st);
         launch_finalize_cont(pl.g, d_in, d_status, simple ? 1 : 0, (float)mean, d_out, d_omask, d_est, d_var, st);
         HB_CK(cudaGetLastError());
+        E.stats.launches += 1;
         HB_CK(cudaEventRecord(E.ev_[4], st));
+        E.mark(STAGE_FINALIZE, st);
 
         to_host(E, out_data, d_out, (size_t)n, io);
         to_host(E, out_mask, d_omask, (size_t)n, io);
         if (opt.estimate64) to_host(E, opt.estimate64, d_est, (size_t)n, io);
         if (opt.variance) to_host(E, opt.variance, d_var, (size_t)n, io);
         if (opt.status) to_host(E, opt.status, d_status, (size_t)n, io);
+        E.mark(STAGE_DOWNLOAD, st);
         end_call(E, st);
         float ms_search = 0, ms_solve = 0;
         cudaEventElapsedTime(&ms_search, E.ev_[2], E.ev_[3]);
@@ -617,7 +742,7 @@ int indicator_kriging(const int *dims, const unsigned char *in_data, const unsig
             // marginal stored as float (ik_params.h:20); the mean provider widens it back
             const float mc = (float)a.marginal;
             run_solves(E, pl, P, S, d_mask, 1, false, opt.precision, opt.refine_steps > 0 ? opt.refine_steps : 2,
-                       (double)mc, c, d_status, so, st);
+                       opt.tolerance, (double)mc, c, d_status, so, st);
             launch_ik_fail_fill(pl.g, d_status, mc, c, m, d_probs, st);
             HB_CK(cudaEventRecord(E.ev_[7], st));
             HB_CK(cudaEventSynchronize(E.ev_[7]));
@@ -679,7 +804,7 @@ int median_ik(const int *dims, const unsigned char *in_data, const unsigned char
         so.status = d_status;
         so.est64 = d_est;
         run_solves(E, pl, P, S, d_mask, 1, false, opt.precision, opt.refine_steps > 0 ? opt.refine_steps : 2,
-                   marginal1, 1, d_status, so, st);
+                   opt.tolerance, marginal1, 1, d_status, so, st);
         launch_mik_finalize(n, d_status, d_est, marginal1, d_out, d_omask, d_prob, st);
         HB_CK(cudaGetLastError());
         HB_CK(cudaEventRecord(E.ev_[4], st));
@@ -722,7 +847,7 @@ int find_neighbours(int kind, const int *dims, const unsigned char *mask, const 
         begin_call(E, st);
         const uint8_t *d_mask = to_device(E, "in_mask", mask, (size_t)n, io);
         DevPoints P = compact_points(E, pl.g, d_mask, nullptr, nullptr, st);
-        DevSearch S = run_search(E, pl, P, d_mask, 1, st);
+        DevSearch S = run_search(E, pl, P, d_mask, 1, st, true);
         std::vector<int> nb_n(n), pts(std::max(P.m, 1));
         std::vector<uint8_t> flags(pl.g.n_bins);
         HB_CK(cudaMemcpyAsync(nb_n.data(), S.nb_n, n * 4, cudaMemcpyDeviceToHost, st));

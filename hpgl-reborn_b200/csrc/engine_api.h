@@ -39,13 +39,33 @@ struct Options
     double *variance = nullptr;
     signed char *status = nullptr;
     float *ik_probs = nullptr;
+    double tolerance = 0.0;
+};
+
+enum Stage
+{
+    STAGE_UPLOAD = 0,   // host->device copies of the inputs
+    STAGE_COMPACT,      // informed cells -> points (scan + readback of the count)
+    STAGE_TABLES,       // key/value/template uploads and the pair-covariance tables
+    STAGE_BINS,         // binning, per-bin path decision (and readback)
+    STAGE_SEARCH,       // neighbour search kernel
+    STAGE_TIES,         // tie-straddle resolution
+    STAGE_PREPARE,      // status + work buckets (and readback)
+    STAGE_SOLVE,        // per-bucket solves and FP64 re-solves
+    STAGE_FINALIZE,     // outputs of cells not written by a solver
+    STAGE_DOWNLOAD,     // device->host copies of the outputs
+    kStages
 };
 
 struct Stats
 {
-    double total_ms = 0, search_ms = 0, solve_ms = 0;
+    double stage_ms[kStages] = {0};
+    double total_ms = 0, search_ms = 0, solve_ms = 0, search_kernel_ms = 0;
     long long ties = 0, template_cells = 0, kriged = 0, launches = 0;
-    long long h2d = 0, d2h = 0;
+    long long h2d = 0, d2h = 0, escalated = 0;
+    long long bucket_items[5] = {0, 0, 0, 0, 0};
+    double bucket_ms[5] = {0, 0, 0, 0, 0};
+    double bucket_flops[5] = {0, 0, 0, 0, 0};
 };
 
 void set_error(const std::string &msg);

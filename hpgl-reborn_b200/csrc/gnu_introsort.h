@@ -218,4 +218,38 @@ GIS_HD void sort(E *a, long n, Less less)
         insertion_sort_guarded(a, 0, n, less);
     }
 }
+// Rearranges a[0 .. n) so that a[0 .. k) holds exactly the elements that
+// sort() (std::sort) places at positions 0 .. k-1; they are not put in order.
+// Only the partitions of the ranges containing the boundary between positions
+// k-1 and k are replayed: a partition leaves every element left of its cut not
+// greater than every element right of it, later steps on a range only permute
+// inside it, and the closing insertion sort is stable and never moves an
+// element out of its final chunk of <= 16, so the chunk straddling the
+// boundary is the only one whose internal order decides the split.
+template <typename E, typename Less>
+GIS_HD void select_first_k(E *a, long n, long k, Less less)
+{
+    const long kThreshold = 16;
+    if (n <= 0 || k <= 0 || k >= n) return;
+    long lo = 0, hi = n;
+    int depth = 2 * floor_log2(n);
+    while (hi - lo > kThreshold)
+    {
+        if (depth == 0)
+        {
+            heap_sort_range(a, lo, hi, less);
+            return;
+        }
+        --depth;
+        long mid = lo + (hi - lo) / 2;
+        median_to_front(a, lo, lo + 1, mid, hi - 1, less);
+        long cut = partition_around_front(a, lo, hi, less);
+        if (cut == k) return;
+        if (cut > k)
+            hi = cut;
+        else
+            lo = cut;
+    }
+    insertion_sort_guarded(a, lo, hi, less);
+}
 } // namespace gis

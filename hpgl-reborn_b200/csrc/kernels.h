@@ -48,33 +48,45 @@ void launch_bin_region(const Geom &g, uint8_t *bin_flag, const int *bin_cnt, int
 size_t search_smem_bytes(int cand_cap, int k, int warps);
 cudaError_t launch_search(const Geom &g, const uint8_t *mask, int all_cells, const int *bin_start,
                           const int *bin_cnt, const uint8_t *bin_flag, const int *bin_pts,
-                          const unsigned long long *pts_xyz, const uint32_t *keytab, int rank_bits,
-                          const int4 *tmpl, int n_tmpl, const int *pid_of_node, int cand_cap, int warps,
-                          int *nb_pid, int *nb_n, int *tie_cells, int *tie_count, int *n_template_cells,
-                          cudaStream_t st);
+                          const unsigned long long *pts_xyz, const float *pts_vf, const uint32_t *keytab,
+                          int rank_bits, const int4 *tmpl, int n_tmpl, const int *pid_of_node, int cand_cap,
+                          int warps, int *nb_pid, int2 *nb_rec, int *nb_n, int *tie_cells, int *tie_count,
+                          int *n_template_cells, cudaStream_t st);
+size_t search_fast_smem_bytes(int cand_cap, int k, int warps);
+cudaError_t launch_search_fast(const Geom &g, const uint8_t *mask, int all_cells, const int *bin_start,
+                               const int *bin_cnt, const uint8_t *bin_flag, const int *bin_pts,
+                               const unsigned long long *pts_xyz, const float *pts_vf, const uint16_t *keytab16,
+                               const int4 *tmpl, int n_tmpl, const int *pid_of_node, int cand_cap, int warps,
+                               int *nb_pid, int2 *nb_rec, int *nb_n, int *tie_cells, int *tie_count,
+                               int *n_template_cells, cudaStream_t st);
 void launch_resolve_ties(const Geom &g, const int *tie_cells, const int *tie_count, int first, int chunk,
                          const int *bin_start, const int *bin_cnt, const int *bin_pts,
-                         const unsigned long long *pts_xyz, const uint32_t *keytab, void *scratch, int cap,
-                         int *nb_pid, cudaStream_t st);
+                         const unsigned long long *pts_xyz, const float *pts_vf, const uint32_t *keytab,
+                         void *scratch, int cap, int *nb_pid, int2 *nb_rec, cudaStream_t st);
 size_t tie_entry_bytes();
+size_t resolve_ties_fast_smem(int cap, int warps);
+cudaError_t launch_resolve_ties_fast(const Geom &g, const int *tie_cells, const int *tie_count, int n_ties,
+                                     const int *bin_start, const int *bin_cnt, const int *bin_pts,
+                                     const unsigned long long *pts_xyz, const float *pts_vf, const uint16_t *keytab16,
+                                     int cap, int *nb_pid, int2 *nb_rec, int n_sm, cudaStream_t st);
 
 // solves (solve.cu, misc.cu)
 cudaError_t launch_solve_bucket(int np, int precision, bool ordinary, const Geom &g, const int *cells,
-                                const int *n_items, int max_items, const int *nb_pid, const int *nb_n,
-                                const unsigned long long *pts_xyz, const float *pts_val, const uint8_t *pts_cat,
-                                int ind_value, const double *pair64, const float *pair32, double mean, double c0,
-                                int steps, const SolveOut &out, int n_sm, cudaStream_t st);
+                                const int *n_items, int max_items, const int2 *nb_rec, const int *nb_n, int ind_value,
+                                const double *pair64, const float *pair32, double mean, double c0, int steps,
+                                double tol, const SolveOut &out, int *esc_cells, int *esc_count, int n_sm,
+                                cudaStream_t st);
 size_t large_scratch_doubles(int k, int blocks);
-cudaError_t launch_solve_large(const Geom &g, const int *cells, const int *n_items, int blocks, const int *nb_pid,
-                               const int *nb_n, const unsigned long long *pts_xyz, const float *pts_val,
-                               const uint8_t *pts_cat, int ind_value, const double *pair64, bool ordinary,
-                               double mean, double c0, double *scratch, const SolveOut &out, cudaStream_t st);
+cudaError_t launch_solve_large(const Geom &g, const int *cells, const int *n_items, int blocks, const int2 *nb_rec,
+                               const int *nb_n, int ind_value, const double *pair64, bool ordinary, double mean,
+                               double c0, double *scratch, const SolveOut &out, cudaStream_t st);
 
 // misc (misc.cu)
 void launch_build_pair(const Geom &g, const DevModel &m, int truncated, const double *search_vals, double *pair64,
                        float *pair32, cudaStream_t st);
 void launch_prepare(const Geom &g, const uint8_t *mask, int all_cells, const int *nb_n, signed char *status,
-                    int *bucket_cnt, int *bucket_off, int *bucket_fill, int *cells, cudaStream_t st);
+                    int *bucket_cnt, int *bucket_off, int *bucket_fill, int *cells,
+                    unsigned long long *moments, cudaStream_t st);
 void launch_finalize_cont(const Geom &g, const float *in_data, signed char *status, int simple, float mean_f,
                           float *out_data, uint8_t *out_mask, double *est64, double *var, cudaStream_t st);
 void launch_ik_fail_fill(const Geom &g, const signed char *status, float marginal, int c, int m, float *probs,

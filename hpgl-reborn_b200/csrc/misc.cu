@@ -78,10 +78,13 @@ __device__ __forceinline__ int bucket_of(int n)
 // Per-cell status before the solve: -1 informed (continuous kriging only),
 // 1 no neighbours, 3 pending (to be solved).
 __global__ void k_prepare(const Geom g, const uint8_t *__restrict__ mask, int all_cells, const int *__restrict__ nb_n,
-                          signed char *__restrict__ status, int *__restrict__ bucket_cnt)
+                          signed char *__restrict__ status, int *__restrict__ bucket_cnt,
+                          unsigned long long *__restrict__ moments)
 {
     __shared__ int s_cnt[kBuckets];
+    __shared__ unsigned long long s_mom[kBuckets * 3];
     if (threadIdx.x < kBuckets) s_cnt[threadIdx.x] = 0;
+    if (threadIdx.x < kBuckets * 3) s_mom[threadIdx.x] = 0;
     __syncthreads();
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < g.n_cells;
          c += (long long)gridDim.x * blockDim.x)
@@ -94,10 +97,19 @@ __global__ void k_prepare(const Geom g, const uint8_t *__restrict__ mask, int al
         int n = nb_n[c];
         int b = bucket_of(n);
         status[c] = b < 0 ? 1 : 3;
-        if (b >= 0) atomicAdd(&s_cnt[b], 1);
+        if (b >= 0)
+        {
+            atomicAdd(&s_cnt[b], 1);
+            // sum n, n^2, n^3 per bucket: the algorithmic flop count is a cubic in n
+            unsigned long long nn = (unsigned long long)n;
+            atomicAdd(&s_mom[3 * b + 0], nn);
+            atomicAdd(&s_mom[3 * b + 1], nn * nn);
+            atomicAdd(&s_mom[3 * b + 2], nn * nn * nn);
+        }
     }
     __syncthreads();
     if (threadIdx.x < kBuckets && s_cnt[threadIdx.x]) atomicAdd(&bucket_cnt[threadIdx.x], s_cnt[threadIdx.x]);
+    if (threadIdx.x < kBuckets * 3 && s_mom[threadIdx.x]) atomicAdd(&moments[threadIdx.x], s_mom[threadIdx.x]);
 }
 
 __global__ void k_bucket_offsets(const int *__restrict__ cnt, int *__restrict__ off, int *__restrict__ fill)
@@ -145,10 +157,12 @@ __global__ void k_bucket_fill(const Geom g, const signed char *__restrict__ stat
 }
 
 void launch_prepare(const Geom &g, const uint8_t *mask, int all_cells, const int *nb_n, signed char *status,
-                    int *bucket_cnt, int *bucket_off, int *bucket_fill, int *cells, cudaStream_t st)
+                    int *bucket_cnt, int *bucket_off, int *bucket_fill, int *cells,
+                    unsigned long long *moments, cudaStream_t st)
 {
     cudaMemsetAsync(bucket_cnt, 0, sizeof(int) * kBuckets, st);
-    k_prepare<<<1184, 256, 0, st>>>(g, mask, all_cells, nb_n, status, bucket_cnt);
+    cudaMemsetAsync(moments, 0, sizeof(unsigned long long) * kBuckets * 3, st);
+    k_prepare<<<1184, 256, 0, st>>>(g, mask, all_cells, nb_n, status, bucket_cnt, moments);
     k_bucket_offsets<<<1, 32, 0, st>>>(bucket_cnt, bucket_off, bucket_fill);
     k_bucket_fill<<<1184, 256, 0, st>>>(g, status, nb_n, bucket_off, bucket_fill, cells);
 }
@@ -172,9 +186,9 @@ __global__ void k_finalize_cont(const Geom g, const float *__restrict__ in_data,
             if (est64) est64[c] = (double)in_data[c];
             if (var) var[c] = 0.0;
         }
-        else if (s == 1 || s == 2 || s == 3)
+        else if (s >= 1)
         {
-            if (s == 3) status[c] = 2; // not written by any solver: treat as singular
+            if (s >= 3) status[c] = 2; // not written by any solver: treat as singular
             if (simple)
             {
                 out_data[c] = mean_f;
@@ -277,11 +291,8 @@ void launch_mik_finalize(long long n_cells, const signed char *status, const dou
 // Neighbour counts above 64: one CTA per system, matrix in global scratch,
 // double precision, right-looking Cholesky with block barriers.
 __global__ void __launch_bounds__(256) k_solve_large(const Geom g, const int *__restrict__ cells,
-                                                     const int *__restrict__ n_items_ptr, const int *__restrict__ nb_pid,
-                                                     const int *__restrict__ nb_n,
-                                                     const unsigned long long *__restrict__ pts_xyz,
-                                                     const float *__restrict__ pts_val,
-                                                     const uint8_t *__restrict__ pts_cat, int ind_value,
+                                                     const int *__restrict__ n_items_ptr, const int2 *__restrict__ nb_rec,
+                                                     const int *__restrict__ nb_n, int ind_value,
                                                      const double *__restrict__ pair64, int ordinary, double mean,
                                                      double c0, double *__restrict__ scratch, SolveOut out)
 {
@@ -294,27 +305,18 @@ __global__ void __launch_bounds__(256) k_solve_large(const Geom g, const int *__
     {
         const int cell = cells[item];
         const int n = nb_n[cell];
-        const int cxg = cell % g.nx, cyg = cell % (g.nx * g.ny) / g.nx, czg = cell / (g.nx * g.ny);
-        // assemble A, b
+        const int2 *rec = nb_rec + (long long)cell * kmax;
         for (int e = threadIdx.x; e < n * n; e += blockDim.x)
         {
             int i = e / n, j = e % n;
-            int pi = nb_pid[(long long)cell * kmax + i], pj = nb_pid[(long long)cell * kmax + j];
-            int xi, yi, zi, xj, yj, zj;
-            unpack_xyz(pts_xyz[pi], xi, yi, zi);
-            unpack_xyz(pts_xyz[pj], xj, yj, zj);
-            A[(size_t)i * n + j] = pair64[pc + pair_lin(g, xi - xj, yi - yj, zi - zj)];
+            A[(size_t)i * n + j] = pair64[pc + rec[i].x - rec[j].x];
         }
         for (int i = threadIdx.x; i < n; i += blockDim.x)
         {
-            int pi = nb_pid[(long long)cell * kmax + i];
-            int xi, yi, zi;
-            unpack_xyz(pts_xyz[pi], xi, yi, zi);
-            rhs[i] = pair64[pc + pair_lin(g, xi - cxg, yi - cyg, zi - czg)];
+            rhs[i] = pair64[pc + rec[i].x];
             rhs[kmax + i] = 1.0;
         }
         __syncthreads();
-        // factor (lower triangle, row-major)
         bool fail = false;
         for (int j = 0; j < n; ++j)
         {
@@ -325,14 +327,14 @@ __global__ void __launch_bounds__(256) k_solve_large(const Geom g, const int *__
             for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) A[(size_t)i * n + j] /= ljj;
             if (threadIdx.x == 0) A[(size_t)j * n + j] = ljj;
             __syncthreads();
-            for (int e = threadIdx.x; e < (n - j - 1) * (n - j - 1); e += blockDim.x)
+            int span = n - j - 1;
+            for (int e = threadIdx.x; e < span * span; e += blockDim.x)
             {
-                int i = j + 1 + e / (n - j - 1), c = j + 1 + e % (n - j - 1);
+                int i = j + 1 + e / span, c = j + 1 + e % span;
                 if (c <= i) A[(size_t)i * n + c] -= A[(size_t)i * n + j] * A[(size_t)c * n + j];
             }
             __syncthreads();
         }
-        // two right-hand sides solved by one thread each (n is small enough)
         if (threadIdx.x < 2)
         {
             double *x = rhs + (threadIdx.x == 0 ? 2 * kmax : 3 * kmax);
@@ -354,8 +356,7 @@ __global__ void __launch_bounds__(256) k_solve_large(const Geom g, const int *__
         if (threadIdx.x == 0)
         {
             const double *x = rhs + 2 * kmax, *y = rhs + 3 * kmax;
-            double mu = 0.0;
-            double sx = 0, sy = 0;
+            double mu = 0.0, sx = 0, sy = 0;
             for (int i = 0; i < n; ++i)
             {
                 sx += x[i];
@@ -371,8 +372,8 @@ __global__ void __launch_bounds__(256) k_solve_large(const Geom g, const int *__
             for (int i = 0; i < n; ++i)
             {
                 double w = ordinary ? x[i] - mu * y[i] : x[i];
-                int p = nb_pid[(long long)cell * kmax + i];
-                double v = pts_val ? (double)pts_val[p] : (pts_cat[p] == ind_value ? 1.0 : 0.0);
+                float vr = __int_as_float(rec[i].y);
+                double v = ind_value >= 0 ? (vr == (float)ind_value ? 1.0 : 0.0) : (double)vr;
                 est += w * (double)((float)v - mf);
                 var -= w * rhs[i];
             }
@@ -398,13 +399,12 @@ __global__ void __launch_bounds__(256) k_solve_large(const Geom g, const int *__
 
 size_t large_scratch_doubles(int k, int blocks) { return (size_t)blocks * ((size_t)k * k + 4 * (size_t)k); }
 
-cudaError_t launch_solve_large(const Geom &g, const int *cells, const int *n_items, int blocks, const int *nb_pid,
-                               const int *nb_n, const unsigned long long *pts_xyz, const float *pts_val,
-                               const uint8_t *pts_cat, int ind_value, const double *pair64, bool ordinary,
-                               double mean, double c0, double *scratch, const SolveOut &out, cudaStream_t st)
+cudaError_t launch_solve_large(const Geom &g, const int *cells, const int *n_items, int blocks, const int2 *nb_rec,
+                               const int *nb_n, int ind_value, const double *pair64, bool ordinary, double mean,
+                               double c0, double *scratch, const SolveOut &out, cudaStream_t st)
 {
-    k_solve_large<<<blocks, 256, 0, st>>>(g, cells, n_items, nb_pid, nb_n, pts_xyz, pts_val, pts_cat, ind_value,
-                                          pair64, ordinary ? 1 : 0, mean, c0, scratch, out);
+    k_solve_large<<<blocks, 256, 0, st>>>(g, cells, n_items, nb_rec, nb_n, ind_value, pair64, ordinary ? 1 : 0, mean,
+                                          c0, scratch, out);
     return cudaGetLastError();
 }
 } // namespace hb

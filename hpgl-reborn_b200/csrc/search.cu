@@ -141,8 +141,9 @@ __global__ void k_emit_points(const uint8_t *__restrict__ mask, const int *__res
         int x = node % g.nx, y = node % (g.nx * g.ny) / g.nx, z = node / (g.nx * g.ny);
         pts_node[p] = node;
         pts_xyz[p] = pack_xyz(x, y, z);
-        if (val_f) pts_val[p] = val_f[i];
-        if (val_u8) pts_cat[p] = val_u8[i];
+        // continuous value, or the category as a float (indicator kriging)
+        pts_val[p] = val_f ? val_f[i] : (val_u8 ? (float)val_u8[i] : 0.0f);
+        if (val_u8 && pts_cat) pts_cat[p] = val_u8[i];
         if (pid_of_node) pid_of_node[i] = p;
     }
 }
@@ -255,9 +256,9 @@ __device__ __forceinline__ unsigned lanemask_lt()
 // keys ascending, ties in candidate order) or -1 when a run of equal keys
 // straddles the k-th slot.
 __device__ int select_cell(const Geom &g, int x, int y, int z, int C, const int *cx, const int *cy,
-                           const int *cz, const int *cpid, const uint32_t *__restrict__ keytab,
-                           uint32_t *keys, uint32_t *hist, unsigned long long *sel, int rank_bits,
-                           int lane, int *out)
+                           const int *cz, const int *cpid, const float *cval,
+                           const uint32_t *__restrict__ keytab, uint32_t *keys, uint32_t *hist,
+                           unsigned long long *sel, int rank_bits, int lane, int *out_pid, int2 *out_rec)
 {
     const int k = g.k;
     int kept = 0;
@@ -377,19 +378,69 @@ __device__ int select_cell(const Geom &g, int x, int y, int z, int C, const int 
         unsigned long long me = sel[e];
         int rank = 0;
         for (int f = 0; f < n_sel; ++f) rank += sel[f] < me;
-        out[rank] = cpid[(int)(me & 0xFFFFFFFFu)];
+        const int pos = (int)(me & 0xFFFFFFFFu);
+        if (out_pid) out_pid[rank] = cpid[pos];
+        if (out_rec) out_rec[rank] = make_int2(pair_lin(g, cx[pos] - x, cy[pos] - y, cz[pos] - z), __float_as_int(cval[pos]));
     }
     __syncwarp();
     return n_sel;
 }
 
+// Template path (sugarbox_neighbour_lookup.h:171-197): one warp per cell walks the
+// sorted template 32 offsets at a time and keeps the first k informed nodes.
+__device__ void template_cells(const Geom &g, const uint8_t *__restrict__ mask, int all_cells, int x0, int y0, int z0,
+                               int wx, int wy, int n_cells_bin, int warp, int nwarps, int lane,
+                               const float *__restrict__ pts_vf, const int4 *__restrict__ tmpl, int n_tmpl,
+                               const int *__restrict__ pid_of_node, int *__restrict__ nb_pid,
+                               int2 *__restrict__ nb_rec, int *__restrict__ nb_n, int *__restrict__ n_template_cells)
+{
+    const int k = g.k;
+    int counted = 0;
+    for (int c = warp; c < n_cells_bin; c += nwarps)
+    {
+        int x = x0 + c % wx, y = y0 + (c / wx) % wy, z = z0 + c / (wx * wy);
+        long long cell = ((long long)z * g.ny + y) * g.nx + x;
+        if (!all_cells && mask[cell]) continue;
+        ++counted;
+        int found = 0;
+        for (int base = 0; base < n_tmpl && found < k; base += 32)
+        {
+            int t = base + lane;
+            bool ok = false;
+            long long node = -1;
+            int4 o = make_int4(0, 0, 0, 0);
+            if (t < n_tmpl)
+            {
+                o = tmpl[t];
+                int px = x + o.x, py = y + o.y, pz = z + o.z;
+                if ((unsigned)px < (unsigned)g.nx && (unsigned)py < (unsigned)g.ny && (unsigned)pz < (unsigned)g.nz)
+                {
+                    node = ((long long)pz * g.ny + py) * g.nx + px;
+                    ok = mask[node] != 0;
+                }
+            }
+            unsigned bl = __ballot_sync(0xffffffffu, ok);
+            int slot = found + __popc(bl & lanemask_lt());
+            if (ok && slot < k)
+            {
+                const int p = pid_of_node[node];
+                if (nb_pid) nb_pid[cell * k + slot] = p;
+                if (nb_rec) nb_rec[cell * k + slot] = make_int2(pair_lin(g, o.x, o.y, o.z), __float_as_int(pts_vf[p]));
+            }
+            found += __popc(bl);
+        }
+        if (lane == 0) nb_n[cell] = min(found, k);
+    }
+    if (lane == 0 && counted) atomicAdd(n_template_cells, counted);
+}
+
 __global__ void __launch_bounds__(256) k_search(
     const Geom g, const uint8_t *__restrict__ mask, int all_cells, const int *__restrict__ bin_start,
     const int *__restrict__ bin_cnt, const uint8_t *__restrict__ bin_flag, const int *__restrict__ bin_pts,
-    const unsigned long long *__restrict__ pts_xyz, const uint32_t *__restrict__ keytab, int rank_bits,
-    const int4 *__restrict__ tmpl, int n_tmpl, const int *__restrict__ pid_of_node, int cand_cap,
-    int *__restrict__ nb_pid, int *__restrict__ nb_n, int *__restrict__ tie_cells, int *__restrict__ tie_count,
-    int *__restrict__ n_template_cells)
+    const unsigned long long *__restrict__ pts_xyz, const float *__restrict__ pts_vf, const uint32_t *__restrict__ keytab,
+    int rank_bits, const int4 *__restrict__ tmpl, int n_tmpl, const int *__restrict__ pid_of_node, int cand_cap,
+    int *__restrict__ nb_pid, int2 *__restrict__ nb_rec, int *__restrict__ nb_n, int *__restrict__ tie_cells,
+    int *__restrict__ tie_count, int *__restrict__ n_template_cells)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int b = blockIdx.x;
@@ -404,40 +455,8 @@ __global__ void __launch_bounds__(256) k_search(
 
     if (bin_flag[b] & 2)
     {
-        // ---------------- template path: warp per cell
-        int counted = 0;
-        for (int c = warp; c < n_cells_bin; c += nwarps)
-        {
-            int x = x0 + c % wx, y = y0 + (c / wx) % wy, z = z0 + c / (wx * wy);
-            long long cell = ((long long)z * g.ny + y) * g.nx + x;
-            if (!all_cells && mask[cell]) continue;
-            ++counted;
-            int *out = nb_pid + cell * k;
-            int found = 0;
-            for (int base = 0; base < n_tmpl && found < k; base += 32)
-            {
-                int t = base + lane;
-                bool ok = false;
-                long long node = -1;
-                if (t < n_tmpl)
-                {
-                    int4 o = tmpl[t];
-                    int px = x + o.x, py = y + o.y, pz = z + o.z;
-                    if ((unsigned)px < (unsigned)g.nx && (unsigned)py < (unsigned)g.ny &&
-                        (unsigned)pz < (unsigned)g.nz)
-                    {
-                        node = ((long long)pz * g.ny + py) * g.nx + px;
-                        ok = mask[node] != 0;
-                    }
-                }
-                unsigned bl = __ballot_sync(0xffffffffu, ok);
-                int slot = found + __popc(bl & lanemask_lt());
-                if (ok && slot < k) out[slot] = pid_of_node[node];
-                found += __popc(bl);
-            }
-            if (lane == 0) nb_n[cell] = min(found, k);
-        }
-        if (lane == 0 && counted) atomicAdd(n_template_cells, counted);
+        template_cells(g, mask, all_cells, x0, y0, z0, wx, wy, n_cells_bin, warp, nwarps, lane, pts_vf, tmpl, n_tmpl,
+                       pid_of_node, nb_pid, nb_rec, nb_n, n_template_cells);
         return;
     }
 
@@ -446,7 +465,8 @@ __global__ void __launch_bounds__(256) k_search(
     int *cy = cx + cand_cap;
     int *cz = cy + cand_cap;
     int *cpid = cz + cand_cap;
-    unsigned char *wbase = reinterpret_cast<unsigned char *>(cpid + cand_cap);
+    float *cval = reinterpret_cast<float *>(cpid + cand_cap);
+    unsigned char *wbase = reinterpret_cast<unsigned char *>(cval + cand_cap);
     const size_t per_warp = (size_t)cand_cap * 4 + 256 * 4 + (size_t)k * 8;
     uint32_t *keys = reinterpret_cast<uint32_t *>(wbase + per_warp * warp);
     uint32_t *hist = keys + cand_cap;
@@ -486,6 +506,7 @@ __global__ void __launch_bounds__(256) k_search(
             cy[d] = py;
             cz[d] = pz;
             cpid[d] = p;
+            cval[d] = pts_vf[p];
         }
     }
     __syncthreads();
@@ -495,8 +516,8 @@ __global__ void __launch_bounds__(256) k_search(
         int x = x0 + c % wx, y = y0 + (c / wx) % wy, z = z0 + c / (wx * wy);
         long long cell = ((long long)z * g.ny + y) * g.nx + x;
         if (!all_cells && mask[cell]) continue;
-        int n = select_cell(g, x, y, z, C, cx, cy, cz, cpid, keytab, keys, hist, sel, rank_bits, lane,
-                            nb_pid + cell * k);
+        int n = select_cell(g, x, y, z, C, cx, cy, cz, cpid, cval, keytab, keys, hist, sel, rank_bits, lane,
+                            nb_pid ? nb_pid + cell * k : nullptr, nb_rec ? nb_rec + cell * k : nullptr);
         if (lane == 0)
         {
             if (n < 0)
@@ -509,6 +530,309 @@ __global__ void __launch_bounds__(256) k_search(
                 nb_n[cell] = n;
         }
     }
+}
+
+// ---------------------------------------------------------------- fast path
+// Cluster-path selection for k <= 64 with 16-bit ranks: each candidate's key
+// is (rank << 16) | candidate position (unique, ordered like (covariance desc,
+// position)). A count-based search for a rank threshold T with
+// k <= #(rank <= T) <= CAP (seeded by the k-th rank of this warp's previous
+// cell) leaves at most CAP survivors, which are compacted in candidate order
+// and sorted in registers (bitonic network over the warp). The k-th key then
+// decides exactness: if the (k+1)-th survivor has the same rank the tie group
+// straddles the k-th slot and the cell goes to k_resolve_ties.
+template <int E>
+__device__ __forceinline__ void warp_bitonic_sort(uint32_t (&v)[E], int lane)
+{
+    // element index i = e * 32 + lane; ascending over 32 * E elements
+#pragma unroll
+    for (int size = 2; size <= 32 * E; size <<= 1)
+    {
+#pragma unroll
+        for (int j = size >> 1; j > 0; j >>= 1)
+        {
+            if (j >= 32)
+            {
+#pragma unroll
+                for (int e = 0; e < E; ++e)
+                {
+                    const int pe = e ^ (j >> 5);
+                    if (pe > e)
+                    {
+                        const bool up = (((e * 32 + lane) & size) == 0);
+                        const uint32_t a = v[e], b = v[pe];
+                        const bool sw = up ? (a > b) : (a < b);
+                        v[e] = sw ? b : a;
+                        v[pe] = sw ? a : b;
+                    }
+                }
+            }
+            else
+            {
+#pragma unroll
+                for (int e = 0; e < E; ++e)
+                {
+                    const bool up = (((e * 32 + lane) & size) == 0);
+                    const uint32_t p = __shfl_xor_sync(0xffffffffu, v[e], j);
+                    const bool lower = (lane & j) == 0;
+                    v[e] = (lower == up) ? min(v[e], p) : max(v[e], p);
+                }
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ int warp_count_le(const uint32_t *keys, int C, uint32_t rank_t, int lane)
+{
+    int c = 0;
+    for (int i = lane; i < C; i += 32) c += (keys[i] >> 16) <= rank_t;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    return c;
+}
+
+template <int E>
+__device__ int select_fast(const Geom &g, int C, const int *cklin, const int *cplin, const int *cpid,
+                           const float *cval, int kc0, int klin_c, int plin_c,
+                           const uint16_t *__restrict__ keytab, uint32_t *keys, uint32_t *sel, int lane,
+                           int &kguess, int *out_pid, int2 *out_rec)
+{
+    constexpr int CAP = 32 * E;
+    const int k = g.k;
+    int kept = 0;
+    for (int i = lane; i < C; i += 32)
+    {
+        const uint32_t r16 = keytab[kc0 + cklin[i] - klin_c];
+        const uint32_t comp = r16 == 0xFFFFu ? 0xFFFFFFFFu : ((r16 << 16) | (uint32_t)i);
+        keys[i] = comp;
+        kept += r16 != 0xFFFFu;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) kept += __shfl_xor_sync(0xffffffffu, kept, o);
+    __syncwarp();
+
+    uint32_t T = 0xFFFEu; // keep every kept candidate
+    if (kept > CAP)
+    {
+        // invariant: #(rank <= tlo) < k (tlo = -1 means none), #(rank <= thi) >= k
+        int tlo = -1, thi = 0xFFFE;
+        bool thi_tight = false; // thi known to give more than CAP survivors
+        int t = kguess >= 0 ? min(kguess + (kguess >> 2) + 8, 0xFFFE) : 64;
+        for (int it = 0; it < 40; ++it)
+        {
+            const int c = warp_count_le(keys, C, (uint32_t)t, lane);
+            if (c < k)
+            {
+                tlo = t;
+                t = thi_tight ? tlo + (thi - tlo + 1) / 2 : min(2 * t + 16, thi);
+                if (t <= tlo) t = tlo + 1;
+            }
+            else if (c > CAP)
+            {
+                thi = t;
+                thi_tight = true;
+                if (t == tlo + 1)
+                {
+                    // the tie group at rank t holds more than CAP - #(rank < t) keys:
+                    // it straddles the k-th slot
+                    kguess = t;
+                    return -1;
+                }
+                t = tlo + (t - tlo) / 2;
+            }
+            else
+            {
+                T = (uint32_t)t;
+                break;
+            }
+        }
+        if (T == 0xFFFEu) return -1; // no threshold found: leave the cell to the exact resolver
+    }
+    // compact survivors (rank <= T) in candidate order
+    int cnt = 0;
+    for (int base = 0; base < C; base += 32)
+    {
+        const int i = base + lane;
+        const uint32_t key = i < C ? keys[i] : 0xFFFFFFFFu;
+        const bool in = (key >> 16) <= T && key != 0xFFFFFFFFu;
+        const unsigned bl = __ballot_sync(0xffffffffu, in);
+        if (in)
+        {
+            const int slot = cnt + __popc(bl & lanemask_lt());
+            if (slot < CAP) sel[slot] = key;
+        }
+        cnt += __popc(bl);
+    }
+    __syncwarp();
+    if (cnt > CAP) cnt = CAP; // cannot happen: T bounds the survivors
+    uint32_t v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+    {
+        const int i = e * 32 + lane;
+        v[e] = i < cnt ? sel[i] : 0xFFFFFFFFu;
+    }
+    warp_bitonic_sort<E>(v, lane);
+    // sorted element i sits in v[i / 32] of lane i % 32
+    const int n_sel = cnt < k ? cnt : k;
+    if (n_sel <= 0) return 0;
+    const uint32_t kth = __shfl_sync(0xffffffffu, v[(n_sel - 1) >> 5], (n_sel - 1) & 31);
+    if (cnt > k)
+    {
+        const uint32_t nxt = __shfl_sync(0xffffffffu, v[k >> 5], k & 31);
+        if ((nxt >> 16) == (kth >> 16))
+        {
+            kguess = (int)(kth >> 16);
+            return -1;
+        }
+    }
+    kguess = (int)(kth >> 16);
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+    {
+        const int i = e * 32 + lane;
+        if (i < n_sel)
+        {
+            const int pos = (int)(v[e] & 0xFFFFu);
+            if (out_pid) out_pid[i] = cpid[pos];
+            if (out_rec) out_rec[i] = make_int2(cplin[pos] - plin_c, __float_as_int(cval[pos]));
+        }
+    }
+    return n_sel;
+}
+
+template <int E>
+__global__ void __launch_bounds__(256) k_search_fast(
+    const Geom g, const uint8_t *__restrict__ mask, int all_cells, const int *__restrict__ bin_start,
+    const int *__restrict__ bin_cnt, const uint8_t *__restrict__ bin_flag, const int *__restrict__ bin_pts,
+    const unsigned long long *__restrict__ pts_xyz, const float *__restrict__ pts_vf,
+    const uint16_t *__restrict__ keytab16, const int4 *__restrict__ tmpl, int n_tmpl,
+    const int *__restrict__ pid_of_node, int cand_cap, int *__restrict__ nb_pid, int2 *__restrict__ nb_rec,
+    int *__restrict__ nb_n, int *__restrict__ tie_cells, int *__restrict__ tie_count,
+    int *__restrict__ n_template_cells)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int b = blockIdx.x;
+    const int bxi = b % g.bx, byi = (b / g.bx) % g.by, bzi = b / (g.bx * g.by);
+    const int x0 = bxi * g.rx, y0 = byi * g.ry, z0 = bzi * g.rz;
+    if (x0 >= g.nx || y0 >= g.ny || z0 >= g.nz) return;
+    const int x1 = min(x0 + g.rx, g.nx), y1 = min(y0 + g.ry, g.ny), z1 = min(z0 + g.rz, g.nz);
+    const int wx = x1 - x0, wy = y1 - y0, wz = z1 - z0;
+    const int n_cells_bin = wx * wy * wz;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int k = g.k;
+
+    if (bin_flag[b] & 2)
+    {
+        template_cells(g, mask, all_cells, x0, y0, z0, wx, wy, n_cells_bin, warp, nwarps, lane, pts_vf, tmpl,
+                       n_tmpl, pid_of_node, nb_pid, nb_rec, nb_n, n_template_cells);
+        return;
+    }
+
+    int *cklin = reinterpret_cast<int *>(smem);
+    int *cplin = cklin + cand_cap;
+    int *cpid = cplin + cand_cap;
+    float *cval = reinterpret_cast<float *>(cpid + cand_cap);
+    uint32_t *wbase = reinterpret_cast<uint32_t *>(cval + cand_cap);
+    uint32_t *keys = wbase + (size_t)warp * (cand_cap + 32 * E);
+    uint32_t *sel = keys + cand_cap;
+
+    __shared__ int s_off[28];
+    if (threadIdx.x == 0)
+    {
+        int run = 0, q = 0;
+        for (int kk = bzi - 1; kk <= bzi + 1; ++kk)
+            for (int jj = byi - 1; jj <= byi + 1; ++jj)
+                for (int ii = bxi - 1; ii <= bxi + 1; ++ii)
+                {
+                    s_off[q] = run;
+                    if (ii >= 0 && jj >= 0 && kk >= 0 && ii < g.bx && jj < g.by && kk < g.bz)
+                        run += bin_cnt[(kk * g.by + jj) * g.bx + ii];
+                    ++q;
+                }
+        s_off[27] = run;
+    }
+    __syncthreads();
+    const int C = s_off[27];
+    for (int q = 0; q < 27; ++q)
+    {
+        int kk = bzi - 1 + q / 9, jj = byi - 1 + (q / 3) % 3, ii = bxi - 1 + q % 3;
+        if (ii < 0 || jj < 0 || kk < 0 || ii >= g.bx || jj >= g.by || kk >= g.bz) continue;
+        int nb = (kk * g.by + jj) * g.bx + ii;
+        int s = bin_start[nb], cnt = s_off[q + 1] - s_off[q];
+        for (int i = threadIdx.x; i < cnt; i += blockDim.x)
+        {
+            int p = bin_pts[s + i];
+            int px, py, pz;
+            unpack_xyz(pts_xyz[p], px, py, pz);
+            int d = s_off[q] + i;
+            // linear offsets relative to the bin corner: key and pair table indices
+            // of a displacement are differences of these
+            cklin[d] = ((pz - z0) * g.kny + (py - y0)) * g.knx + (px - x0);
+            cplin[d] = ((pz - z0) * g.pny + (py - y0)) * g.pnx + (px - x0);
+            cpid[d] = p;
+            cval[d] = pts_vf[p];
+        }
+    }
+    __syncthreads();
+    const int kc0 = (g.khz * g.kny + g.khy) * g.knx + g.khx;
+    int kguess = -1;
+    for (int c = warp; c < n_cells_bin; c += nwarps)
+    {
+        const int cxr = c % wx, cyr = (c / wx) % wy, czr = c / (wx * wy);
+        const long long cell = ((long long)(z0 + czr) * g.ny + (y0 + cyr)) * g.nx + (x0 + cxr);
+        if (!all_cells && mask[cell]) continue;
+        const int klin_c = (czr * g.kny + cyr) * g.knx + cxr;
+        const int plin_c = (czr * g.pny + cyr) * g.pnx + cxr;
+        const int n = select_fast<E>(g, C, cklin, cplin, cpid, cval, kc0, klin_c, plin_c, keytab16, keys, sel, lane,
+                                     kguess, nb_pid ? nb_pid + cell * k : nullptr, nb_rec ? nb_rec + cell * k : nullptr);
+        if (lane == 0)
+        {
+            if (n < 0)
+            {
+                nb_n[cell] = k;
+                int slot = atomicAdd(tie_count, 1);
+                tie_cells[slot] = (int)cell;
+            }
+            else
+                nb_n[cell] = n;
+        }
+    }
+}
+
+size_t search_fast_smem_bytes(int cand_cap, int k, int warps)
+{
+    const int E = k <= 32 ? 2 : 4;
+    return (size_t)cand_cap * 16 + (size_t)warps * ((size_t)cand_cap + 32 * E) * 4;
+}
+
+cudaError_t launch_search_fast(const Geom &g, const uint8_t *mask, int all_cells, const int *bin_start,
+                               const int *bin_cnt, const uint8_t *bin_flag, const int *bin_pts,
+                               const unsigned long long *pts_xyz, const float *pts_vf, const uint16_t *keytab16,
+                               const int4 *tmpl, int n_tmpl, const int *pid_of_node, int cand_cap, int warps,
+                               int *nb_pid, int2 *nb_rec, int *nb_n, int *tie_cells, int *tie_count,
+                               int *n_template_cells, cudaStream_t st)
+{
+    size_t smem = search_fast_smem_bytes(cand_cap, g.k, warps);
+    if (g.k <= 32)
+    {
+        cudaError_t e = cudaFuncSetAttribute(k_search_fast<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        k_search_fast<2><<<g.n_bins, warps * 32, smem, st>>>(g, mask, all_cells, bin_start, bin_cnt, bin_flag, bin_pts,
+                                                            pts_xyz, pts_vf, keytab16, tmpl, n_tmpl, pid_of_node,
+                                                            cand_cap, nb_pid, nb_rec, nb_n, tie_cells, tie_count,
+                                                            n_template_cells);
+    }
+    else
+    {
+        cudaError_t e = cudaFuncSetAttribute(k_search_fast<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        k_search_fast<4><<<g.n_bins, warps * 32, smem, st>>>(g, mask, all_cells, bin_start, bin_cnt, bin_flag, bin_pts,
+                                                            pts_xyz, pts_vf, keytab16, tmpl, n_tmpl, pid_of_node,
+                                                            cand_cap, nb_pid, nb_rec, nb_n, tie_cells, tie_count,
+                                                            n_template_cells);
+    }
+    return cudaGetLastError();
 }
 
 // One thread per tie-straddling cell: rebuild the threshold-filtered candidate
@@ -528,8 +852,9 @@ __global__ void k_resolve_ties(const Geom g, const int *__restrict__ tie_cells, 
                                int first, int chunk, const int *__restrict__ bin_start,
                                const int *__restrict__ bin_cnt, const int *__restrict__ bin_pts,
                                const unsigned long long *__restrict__ pts_xyz,
-                               const uint32_t *__restrict__ keytab, KeyPid *__restrict__ scratch, int cap,
-                               int *__restrict__ nb_pid)
+                               const float *__restrict__ pts_vf, const uint32_t *__restrict__ keytab,
+                               KeyPid *__restrict__ scratch, int cap, int *__restrict__ nb_pid,
+                               int2 *__restrict__ nb_rec)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     int idx = first + t;
@@ -556,9 +881,143 @@ __global__ void k_resolve_ties(const Geom g, const int *__restrict__ tie_cells, 
                 }
             }
     gis::sort(a, (long)n, KeyLess());
-    int *out = nb_pid + (long long)cell * g.k;
+    const long long base = (long long)cell * g.k;
     int m = n < g.k ? n : g.k;
-    for (int i = 0; i < m; ++i) out[i] = a[i].pid;
+    for (int i = 0; i < m; ++i)
+    {
+        const int p = a[i].pid;
+        if (nb_pid) nb_pid[base + i] = p;
+        if (nb_rec)
+        {
+            int px, py, pz;
+            unpack_xyz(pts_xyz[p], px, py, pz);
+            nb_rec[base + i] = make_int2(pair_lin(g, px - x, py - y, pz - z), __float_as_int(pts_vf[p]));
+        }
+    }
+}
+
+// One warp per tie-straddling cell, 16-bit ranks: the warp rebuilds the
+// threshold-filtered candidate list in the reference's order in shared memory,
+// one lane replays introsort's partitions along the k-th slot
+// (gis::select_first_k, the same set std::sort leaves in front), and the warp
+// orders the selected k by (rank, position) for output.
+struct RankLess
+{
+    __device__ bool operator()(uint32_t a, uint32_t b) const { return (a >> 16) < (b >> 16); }
+};
+
+template <int E>
+__global__ void __launch_bounds__(128) k_resolve_ties_fast(
+    const Geom g, const int *__restrict__ tie_cells, const int *__restrict__ tie_count,
+    const int *__restrict__ bin_start, const int *__restrict__ bin_cnt, const int *__restrict__ bin_pts,
+    const unsigned long long *__restrict__ pts_xyz, const float *__restrict__ pts_vf,
+    const uint16_t *__restrict__ keytab, int cap, int *__restrict__ nb_pid, int2 *__restrict__ nb_rec)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    uint32_t *arr = reinterpret_cast<uint32_t *>(smem) + (size_t)warp * 2 * cap;
+    int *pid = reinterpret_cast<int *>(arr + cap);
+    const int n_ties = *tie_count;
+    for (int t = blockIdx.x * nwarps + warp; t < n_ties; t += gridDim.x * nwarps)
+    {
+        const int cell = tie_cells[t];
+        const int x = cell % g.nx, y = cell % (g.nx * g.ny) / g.nx, z = cell / (g.nx * g.ny);
+        const int bxi = x / g.rx, byi = y / g.ry, bzi = z / g.rz;
+        int n = 0;
+        for (int kk = bzi - 1; kk <= bzi + 1; ++kk)
+            for (int jj = byi - 1; jj <= byi + 1; ++jj)
+                for (int ii = bxi - 1; ii <= bxi + 1; ++ii)
+                {
+                    if (ii < 0 || jj < 0 || kk < 0 || ii >= g.bx || jj >= g.by || kk >= g.bz) continue;
+                    const int nb = (kk * g.by + jj) * g.bx + ii;
+                    const int s = bin_start[nb], cnt = bin_cnt[nb];
+                    for (int base = 0; base < cnt; base += 32)
+                    {
+                        const int i = base + lane;
+                        uint32_t key = 0xFFFFu;
+                        int p = 0;
+                        if (i < cnt)
+                        {
+                            p = bin_pts[s + i];
+                            int px, py, pz;
+                            unpack_xyz(pts_xyz[p], px, py, pz);
+                            key = keytab[key_index(g, px - x, py - y, pz - z)];
+                        }
+                        const bool keep = key != 0xFFFFu;
+                        const unsigned bl = __ballot_sync(0xffffffffu, keep);
+                        const int slot = n + __popc(bl & lanemask_lt());
+                        if (keep && slot < cap)
+                        {
+                            arr[slot] = (key << 16) | (uint32_t)slot;
+                            pid[slot] = p;
+                        }
+                        n += __popc(bl);
+                    }
+                }
+        if (n > cap) n = cap; // cannot happen: cap bounds every candidate list
+        __syncwarp();
+        if (lane == 0) gis::select_first_k(arr, (long)n, (long)g.k, RankLess());
+        __syncwarp();
+        const int m = n < g.k ? n : g.k;
+        uint32_t v[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+        {
+            const int i = e * 32 + lane;
+            v[e] = i < m ? arr[i] : 0xFFFFFFFFu;
+        }
+        warp_bitonic_sort<E>(v, lane);
+        const long long base = (long long)cell * g.k;
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+        {
+            const int i = e * 32 + lane;
+            if (i < m)
+            {
+                const int j = (int)(v[e] & 0xFFFFu);
+                const int p = pid[j];
+                if (nb_pid) nb_pid[base + i] = p;
+                if (nb_rec)
+                {
+                    int px, py, pz;
+                    unpack_xyz(pts_xyz[p], px, py, pz);
+                    nb_rec[base + i] = make_int2(pair_lin(g, px - x, py - y, pz - z), __float_as_int(pts_vf[p]));
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+size_t resolve_ties_fast_smem(int cap, int warps) { return (size_t)warps * 2 * cap * 4; }
+
+cudaError_t launch_resolve_ties_fast(const Geom &g, const int *tie_cells, const int *tie_count, int n_ties,
+                                     const int *bin_start, const int *bin_cnt, const int *bin_pts,
+                                     const unsigned long long *pts_xyz, const float *pts_vf, const uint16_t *keytab16,
+                                     int cap, int *nb_pid, int2 *nb_rec, int n_sm, cudaStream_t st)
+{
+    const int warps = 4;
+    const size_t smem = resolve_ties_fast_smem(cap, warps);
+    int blocks = (n_ties + warps - 1) / warps;
+    if (blocks > n_sm * 16) blocks = n_sm * 16;
+    if (blocks < 1) blocks = 1;
+    if (g.k <= 32)
+    {
+        cudaError_t e = cudaFuncSetAttribute(k_resolve_ties_fast<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        k_resolve_ties_fast<2><<<blocks, warps * 32, smem, st>>>(g, tie_cells, tie_count, bin_start, bin_cnt, bin_pts,
+                                                                 pts_xyz, pts_vf, keytab16, cap, nb_pid, nb_rec);
+    }
+    else
+    {
+        cudaError_t e = cudaFuncSetAttribute(k_resolve_ties_fast<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        k_resolve_ties_fast<4><<<blocks, warps * 32, smem, st>>>(g, tie_cells, tie_count, bin_start, bin_cnt, bin_pts,
+                                                                 pts_xyz, pts_vf, keytab16, cap, nb_pid, nb_rec);
+    }
+    return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------ launchers
@@ -598,36 +1057,36 @@ void launch_bin_region(const Geom &g, uint8_t *bin_flag, const int *bin_cnt, int
 
 size_t search_smem_bytes(int cand_cap, int k, int warps)
 {
-    return (size_t)cand_cap * 16 + (size_t)warps * ((size_t)cand_cap * 4 + 256 * 4 + (size_t)k * 8);
+    return (size_t)cand_cap * 20 + (size_t)warps * ((size_t)cand_cap * 4 + 256 * 4 + (size_t)k * 8);
 }
 
 cudaError_t launch_search(const Geom &g, const uint8_t *mask, int all_cells, const int *bin_start,
                           const int *bin_cnt, const uint8_t *bin_flag, const int *bin_pts,
-                          const unsigned long long *pts_xyz, const uint32_t *keytab, int rank_bits,
-                          const int4 *tmpl, int n_tmpl, const int *pid_of_node, int cand_cap, int warps,
-                          int *nb_pid, int *nb_n, int *tie_cells, int *tie_count, int *n_template_cells,
-                          cudaStream_t st)
+                          const unsigned long long *pts_xyz, const float *pts_vf, const uint32_t *keytab,
+                          int rank_bits, const int4 *tmpl, int n_tmpl, const int *pid_of_node, int cand_cap,
+                          int warps, int *nb_pid, int2 *nb_rec, int *nb_n, int *tie_cells, int *tie_count,
+                          int *n_template_cells, cudaStream_t st)
 {
     size_t smem = search_smem_bytes(cand_cap, g.k, warps);
     cudaError_t e = cudaFuncSetAttribute(k_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k_search<<<g.n_bins, warps * 32, smem, st>>>(g, mask, all_cells, bin_start, bin_cnt, bin_flag, bin_pts,
-                                                  pts_xyz, keytab, rank_bits, tmpl, n_tmpl, pid_of_node,
-                                                  cand_cap, nb_pid, nb_n, tie_cells, tie_count,
+                                                  pts_xyz, pts_vf, keytab, rank_bits, tmpl, n_tmpl, pid_of_node,
+                                                  cand_cap, nb_pid, nb_rec, nb_n, tie_cells, tie_count,
                                                   n_template_cells);
     return cudaGetLastError();
 }
 
 void launch_resolve_ties(const Geom &g, const int *tie_cells, const int *tie_count, int first, int chunk,
                          const int *bin_start, const int *bin_cnt, const int *bin_pts,
-                         const unsigned long long *pts_xyz, const uint32_t *keytab, void *scratch, int cap,
-                         int *nb_pid, cudaStream_t st)
+                         const unsigned long long *pts_xyz, const float *pts_vf, const uint32_t *keytab,
+                         void *scratch, int cap, int *nb_pid, int2 *nb_rec, cudaStream_t st)
 {
     int threads = 64;
     int blocks = (chunk + threads - 1) / threads;
     k_resolve_ties<<<blocks, threads, 0, st>>>(g, tie_cells, tie_count, first, chunk, bin_start, bin_cnt,
-                                               bin_pts, pts_xyz, keytab, reinterpret_cast<KeyPid *>(scratch),
-                                               cap, nb_pid);
+                                               bin_pts, pts_xyz, pts_vf, keytab,
+                                               reinterpret_cast<KeyPid *>(scratch), cap, nb_pid, nb_rec);
 }
 size_t tie_entry_bytes() { return sizeof(KeyPid); }
 } // namespace hb

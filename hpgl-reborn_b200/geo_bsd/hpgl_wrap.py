@@ -65,7 +65,7 @@ _HPGL_COV_PARAMS = __hpgl_cov_params_t
 class _HPGL_B200_OPTIONS(C.Structure):
     _fields_ = [("precision", C.c_int), ("refine_steps", C.c_int), ("flags", C.c_uint),
                 ("stream", C.c_void_p), ("estimate64", C.c_void_p), ("variance", C.c_void_p),
-                ("status", C.c_void_p), ("ik_probs", C.c_void_p)]
+                ("status", C.c_void_p), ("ik_probs", C.c_void_p), ("tolerance", C.c_double)]
 
 
 FP64_PLAIN = 0
@@ -164,9 +164,16 @@ def check(rc: int, what: str) -> None:
         raise RuntimeError(f"{what} failed ({rc}): {last_error()}")
 
 
+STATS_KEYS = (["total_ms", "search_ms", "solve_ms", "tie_cells", "template_cells", "kriged_cells",
+               "kernel_launches", "h2d_bytes", "d2h_bytes", "escalated_cells", "search_kernel_ms"]
+              + [f"bucket_items_{i}" for i in range(5)] + [f"bucket_ms_{i}" for i in range(5)]
+              + [f"bucket_flops_{i}" for i in range(5)]
+              + ["stage_" + s + "_ms" for s in ("upload", "compact", "tables", "bins", "search", "ties", "prepare",
+                                              "solve", "finalize", "download")])
+
+
 def last_stats() -> dict:
-    buf = (C.c_double * 9)()
-    _hpgl_so.hpgl_b200_last_stats(buf, 9)
-    keys = ["total_ms", "search_ms", "solve_ms", "tie_cells", "template_cells", "kriged_cells",
-            "kernel_launches", "h2d_bytes", "d2h_bytes"]
-    return {k: float(buf[i]) for i, k in enumerate(keys)}
+    """Timing and counters of the last engine call (hpgl_b200_last_stats)."""
+    buf = (C.c_double * len(STATS_KEYS))()
+    n = _hpgl_so.hpgl_b200_last_stats(buf, len(STATS_KEYS))
+    return {k: float(buf[i]) for i, k in enumerate(STATS_KEYS[:n])}

@@ -118,6 +118,9 @@ struct hpgl_b200_options_t {
     double *variance;        /* optional: kriging variance per cell (-1 where not kriged) */
     signed char *status;     /* optional: per-cell status (HPGL_B200_CELL_*) */
     float *ik_probs;         /* optional (IK): corrected probabilities, cell-major [cell][category] */
+    double tolerance;        /* FP32_REFINED: accepted estimate of the remaining relative error of the
+                                estimate/variance forms (0 -> 1e-9); systems above it are refined
+                                further, then re-solved in FP64 */
 };
 
 /* OK / SK over a whole grid with options; dims = (nx, ny, nz), Fortran order.
@@ -145,10 +148,20 @@ int hpgl_b200_find_neighbours(int kind, const int *dims, const unsigned char *ma
                               const struct hpgl_sk_params_t *params, const int *nodes, int n_nodes,
                               int *out_idx, int *out_count, unsigned char *out_path);
 
-/* Timing of the last call on this thread's engine: device milliseconds of
- * the whole pipeline and of each stage, and counters. Returns the number of
- * doubles written (<= cap): [total_ms, search_ms, solve_ms, straddle_cells,
- * template_cells, kriged_cells, kernel_launches, h2d_bytes, d2h_bytes]. */
+/* Timing and counters of the last call on the current device's engine.
+ * Writes up to `cap` doubles, returns how many:
+ *   [0] total_ms (device, whole call)   [1] search_ms (stage)   [2] solve_ms (stage)
+ *   [3] tie-resolved cells   [4] template-path cells   [5] kriged cells
+ *   [6] kernel launches      [7] h2d bytes   [8] d2h bytes
+ *   [9] cells re-solved in FP64 after FP32 refinement did not converge
+ *   [10] neighbour-search kernel ms
+ *   [11..15] cells per solve bucket (n <= 8, 16, 32, 64, > 64)
+ *   [16..20] solve kernel ms per bucket
+ *   [21..25] algorithmic flops per bucket, sum of F(n, r) =
+ *            n^3/3 + n^2/2 + 2 r n^2 + 30 (n(n+1)/2 + n) + 2 r n (r = 2 OK, 1 SK)
+ *   [26..35] ms per stage: upload, compaction, tables, binning, search, tie
+ *            resolution, bucketing, solves, finalize, download */
+#define HPGL_B200_STATS_LEN 36
 int hpgl_b200_last_stats(double *out, int cap);
 
 /* Page-locked host buffers for fast copies (cudaHostAlloc / cudaFreeHost). */

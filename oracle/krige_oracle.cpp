@@ -818,4 +818,30 @@ void ko_sort_check(const unsigned *keys, int n, int *perm_std, int *perm_gis)
     }
 }
 
+// Checks select_first_k (gnu_introsort.h) against std::sort: writes 1 to
+// *same_set when the first k elements of both hold the same positions.
+void ko_select_check(const unsigned *keys, int n, int k, int *same_set)
+{
+    struct E
+    {
+        unsigned key;
+        int pos;
+    };
+    std::vector<E> a(n);
+    for (int i = 0; i < n; ++i) a[i] = {keys[i], i};
+    std::vector<E> b = a;
+    std::sort(a.begin(), a.end(), [](const E &x, const E &y) { return x.key < y.key; });
+    gis::select_first_k(b.data(), (long)n, (long)k, [](const E &x, const E &y) { return x.key < y.key; });
+    int m = k < n ? k : n;
+    std::vector<int> sa(m), sb(m);
+    for (int i = 0; i < m; ++i)
+    {
+        sa[i] = a[i].pos;
+        sb[i] = b[i].pos;
+    }
+    std::sort(sa.begin(), sa.end());
+    std::sort(sb.begin(), sb.end());
+    *same_set = sa == sb ? 1 : 0;
+}
+
 } // extern "C"

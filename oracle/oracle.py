@@ -71,6 +71,8 @@ def load(which: str):
                                       C.c_double, _d, _d]
         lib.ko_sort_check.argtypes = [_u32, C.c_int, _i, _i]
         lib.ko_sort_check.restype = None
+        lib.ko_select_check.argtypes = [_u32, C.c_int, C.c_int, _i]
+        lib.ko_select_check.restype = None
     else:
         lib.ref_krige_cont.argtypes = [C.c_int, _i, _f, _u8, C.c_int, _d, _d, C.c_double,
                                        C.c_double, _i, C.c_int, C.c_double, _i, C.c_int, _i, _i,
@@ -272,3 +274,11 @@ def sort_check(keys):
     b = np.zeros(len(keys), np.int32)
     lib.ko_sort_check(_ptr(keys, _u32), len(keys), _ptr(a, _i), _ptr(b, _i))
     return a, b
+
+
+def select_check(keys, k):
+    lib = load("port")
+    keys = _arr(keys, np.uint32)
+    out = C.c_int(0)
+    lib.ko_select_check(_ptr(keys, _u32), len(keys), int(k), C.byref(out))
+    return bool(out.value)

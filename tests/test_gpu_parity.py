@@ -1,0 +1,183 @@
+"""GPU parity: the engine (through its C ABI) against the reference's golden
+vectors and the oracle.
+
+Bars: neighbour sets bit-exact (node indices; order exact wherever the
+reference's order is fixed by distinct keys or by its std::sort permutation on
+tie-straddling cells); FP64-plain estimates and variances within 1e-10
+relative of the reference's FP64 path; FP32-refined within 1e-6; per-cell
+status identical; the float grid the reference's public API writes reproduced
+to float rounding; indicator categories identical.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import golden_io as G
+import helpers as H
+import oracle as O
+from geo_bsd import hpgl_wrap as W
+from geo_bsd import workloads as WL
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-10
+FP32_TOL = 1e-6
+
+
+def _sets_equal(a, b):
+    return all(set(x[x >= 0].tolist()) == set(y[y >= 0].tolist()) for x, y in zip(a, b))
+
+
+@pytest.mark.parametrize("case", G.CONT_CASES)
+@pytest.mark.parametrize("tag,kind", [("ok", 0), ("sk", 1)])
+def test_neighbours_match_reference(case, tag, kind):
+    g = G.load(case)
+    wl = G.as_workload(g, case)
+    idx, cnt, path = H.engine_neighbours(kind, wl, g["nodes"])
+    np.testing.assert_array_equal(cnt, g[f"{tag}_count"])
+    np.testing.assert_array_equal(path, g[f"{tag}_path"])
+    assert _sets_equal(idx, g[f"{tag}_idx"])
+
+
+@pytest.mark.parametrize("case", G.CONT_CASES)
+@pytest.mark.parametrize("tag,kind", [("ok", 0), ("sk", 1)])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_estimates_match_reference(case, tag, kind, precision):
+    g = G.load(case)
+    wl = G.as_workload(g, case)
+    e = H.engine_cont(kind, wl, precision=precision, mean=None)
+    nodes = g["nodes"]
+    st = e["status"][nodes]
+    np.testing.assert_array_equal(st, g[f"{tag}_status"].astype(np.int8))
+    ok = st == 0
+    tol = FP64_TOL if precision == 0 else FP32_TOL
+    if case.startswith("clustered"):
+        tol = max(tol, 1e-8)  # nugget 1e-3 Gaussian: cond(A) * eps of the reference's own LAPACK path
+    assert H.rel_err(e["est"][nodes][ok], g[f"{tag}_est"][ok]) <= tol
+    assert H.rel_err(e["var"][nodes][ok], g[f"{tag}_var"][ok]) <= tol
+
+
+@pytest.mark.parametrize("case", ["ok_small_s030", "gauss_cv_s020"])
+@pytest.mark.parametrize("tag,kind", [("ok", 0), ("sk", 1)])
+def test_grid_output_matches_reference_api(case, tag, kind):
+    """The float grid and mask that the reference's hpgl_ordinary_kriging /
+    hpgl_simple_kriging write, reproduced through the engine's compatible entry points."""
+    g = G.load(case)
+    wl = G.as_workload(g, case)
+    n = wl.n_cells
+    data = np.ascontiguousarray(wl.data)
+    mask = np.ascontiguousarray(wl.mask)
+    out_d, out_m = data.copy(), mask.copy()
+    sh = W._HPGL_SHAPE(data=wl.dims, strides=(1, wl.dims[0], wl.dims[0] * wl.dims[1]))
+    fp = C.POINTER(C.c_float)
+    up = C.POINTER(C.c_ubyte)
+    if kind == 0:
+        p = W._HPGL_OK_PARAMS(covariance_type=wl.cov.cov_type, ranges=wl.cov.ranges, angles=wl.cov.angles,
+                              sill=wl.cov.sill, nugget=wl.cov.nugget, radiuses=wl.radiuses,
+                              max_neighbours=wl.max_neighbours)
+        a = W._HPGL_CONT_MASKED_ARRAY(data.ctypes.data_as(fp), mask.ctypes.data_as(up), sh)
+        b = W._HPGL_CONT_MASKED_ARRAY(out_d.ctypes.data_as(fp), out_m.ctypes.data_as(up), sh)
+        W._hpgl_so.hpgl_ordinary_kriging(C.byref(a), C.byref(p), C.byref(b))
+    else:
+        p = W._HPGL_SK_PARAMS(covariance_type=wl.cov.cov_type, ranges=wl.cov.ranges, angles=wl.cov.angles,
+                              sill=wl.cov.sill, nugget=wl.cov.nugget, radiuses=wl.radiuses,
+                              max_neighbours=wl.max_neighbours, automatic_mean=1, mean=0.0)
+        d3 = data.reshape(wl.dims, order="F")
+        m3 = mask.reshape(wl.dims, order="F")
+        o3 = out_d.reshape(wl.dims, order="F")
+        om3 = out_m.reshape(wl.dims, order="F")
+        W._hpgl_so.hpgl_simple_kriging(d3, m3, C.byref(sh), C.byref(p), o3, om3, C.byref(sh))
+    assert W.last_error() == "" or W.last_stats()["kriged_cells"] > 0
+    np.testing.assert_array_equal(out_m, g[f"{tag}_grid_mask"])
+    ref = g[f"{tag}_grid_data"]
+    assert np.abs(out_d - ref).max() <= 1e-6 * max(np.abs(ref).max(), 1.0)
+    assert n == len(ref)
+
+
+def test_indicator_kriging_matches_reference():
+    g = G.load("indicator_s015")
+    dims, data, mask = G.grid_inputs(g, dtype=np.uint8)
+    wl = WL.Workload("ik", dims, data, mask, None, None, 24)
+    covs, rads, ks = [], [], []
+    for c in range(5):
+        cov, rad, k = G.cov_of(g, f"c{c}_")
+        covs.append(cov)
+        rads.append(rad)
+        ks.append(k)
+    out_d, out_m, probs = H.engine_indicator(wl, covs, rads, ks, list(g["marginals"]))
+    np.testing.assert_array_equal(out_d, g["ik_grid"])
+    assert np.all(out_m == 1)
+    for c in range(5):
+        nodes = g["nodes"]
+        idx, cnt, path = H.engine_neighbours(1, wl, nodes, cov=covs[c], radiuses=rads[c], k=ks[c])
+        assert _sets_equal(idx, g[f"c{c}_idx"])
+        np.testing.assert_array_equal(path, g[f"c{c}_path"])
+
+
+def test_median_ik_matches_reference():
+    g = G.load("indicator_s015")
+    dims, data, mask = G.grid_inputs(g, "mik_values", dtype=np.uint8)
+    wl = WL.Workload("mik", dims, data, mask, None, None, 24)
+    cov, rad, _ = G.cov_of(g, "c2_")
+    out_d, out_m, prob = H.engine_median_ik(wl, cov, rad, 24, list(g["mik_marginals"]))
+    # cells where the reference's kriging failed hold an uninitialised decision there
+    _, _, _, st = O.median_ik_grid(dims, data, mask, cov, rad, 24, list(g["mik_marginals"]))
+    ok = st == 0
+    np.testing.assert_array_equal(out_d[ok], g["mik_grid"][ok])
+
+
+def test_known_answers():
+    """Constant field 42 -> 42 and zeros -> 0 (reference test_edge_cases.py:368-392, 487-511)."""
+    g = dict(np.load(G.GOLDEN + "/known_answers.npz"))
+    for name, val in (("const42", 42.0), ("zeros", 0.0)):
+        wl = WL.Workload(name, (10, 10, 5), g[f"{name}_data"], g[f"{name}_mask"],
+                         WL.CovSpec(WL.SPHERICAL, (10.0, 10.0, 10.0), (0.0, 0.0, 0.0), 1.0, 0.0), (5, 5, 5), 12)
+        for precision in (0, 1):
+            e = H.engine_cont(0, wl, precision=precision)
+            np.testing.assert_array_equal(e["mask"], g[f"{name}_outmask"])
+            assert np.abs(e["data"] - g[f"{name}_out"]).max() <= 1e-4
+            assert np.abs(e["data"][e["mask"] == 1] - val).max() <= 0.1
+
+
+@pytest.mark.parametrize("name,scale", [("ok_small", 0.6), ("sk_ok_large", 0.3), ("gauss_cv", 0.35),
+                                        ("clustered", 0.2)])
+@pytest.mark.parametrize("kind", [0, 1])
+def test_larger_grids_against_oracle(name, scale, kind):
+    wl = WL.ALL[name](scale)
+    od, om, oest, ovar, ost = O.cont_grid(kind, wl.dims, wl.data, wl.mask, wl.cov, wl.radiuses, wl.max_neighbours)
+    unk = wl.mask == 0
+    for precision in (0, 1):
+        e = H.engine_cont(kind, wl, precision=precision)
+        np.testing.assert_array_equal(e["status"][unk], ost[unk].astype(np.int8))
+        np.testing.assert_array_equal(e["mask"], om)
+        ok = unk & (ost == 0)
+        tol = FP64_TOL if precision == 0 else FP32_TOL
+        if name == "clustered":
+            tol = max(tol, 1e-8)
+        assert H.rel_err(e["est"][ok], oest[ok]) <= tol, (precision, H.rel_err(e["est"][ok], oest[ok]))
+        assert H.rel_err(e["var"][ok], ovar[ok]) <= tol
+    rng = np.random.default_rng(1)
+    nodes = np.sort(rng.choice(np.flatnonzero(unk), 2000, replace=False))
+    idx, cnt, path = H.engine_neighbours(kind, wl, nodes)
+    r = O.krige_nodes("port", kind, wl.dims, wl.data, wl.mask, wl.cov, wl.radiuses, wl.max_neighbours,
+                      nodes=nodes)
+    np.testing.assert_array_equal(cnt, r["count"])
+    np.testing.assert_array_equal(path, r["path"])
+    assert _sets_equal(idx, r["idx"])
+
+
+def test_simple_kriging_weights_entry():
+    rng = np.random.default_rng(4)
+    for cov in (WL.CovSpec(WL.EXPONENTIAL, (10.0, 10.0, 10.0), (0.0, 0.0, 0.0), 1.0, 0.0),
+                WL.CovSpec(WL.GAUSSIAN, (20.0, 10.0, 5.0), (30.0, 0.0, 0.0), 1.0, 0.1)):
+        xs, ys, zs = (rng.uniform(0, 10, 12).astype(np.float32) for _ in range(3))
+        centre = np.array([5.0, 5.0, 5.0], np.float32)
+        covp = W._HPGL_COV_PARAMS(covariance_type=cov.cov_type, ranges=cov.ranges, angles=cov.angles,
+                                  sill=cov.sill, nugget=cov.nugget)
+        w = np.zeros(12, np.float32)
+        rc = W._hpgl_so.hpgl_simple_kriging_weights((C.c_float * 3)(*centre), xs, ys, zs, 12, C.byref(covp), w)
+        assert rc == 0
+        ref, _ = O.sk_weights("port", centre.astype(np.float64), xs.astype(np.float64), ys.astype(np.float64),
+                              zs.astype(np.float64), cov)
+        assert np.abs(w - ref).max() <= 1e-5 * max(1.0, np.abs(ref).max())

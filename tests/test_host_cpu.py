@@ -1,0 +1,134 @@
+"""Host-side pieces of the engine, runnable without a GPU: the C ABI library
+loads and exports every entry point of include/hpgl_b200.h, its struct layouts
+agree with the header, and its covariance / template / transform code is
+bit-identical to the oracle (and so to the reference)."""
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+import oracle as O
+from geo_bsd import hpgl_wrap as W
+from geo_bsd import workloads as WL
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "hpgl_b200.h")
+
+MODELS = [
+    WL.CovSpec(WL.SPHERICAL, (10.0, 10.0, 5.0), (0.0, 0.0, 0.0), 1.0, 0.1),
+    WL.CovSpec(WL.EXPONENTIAL, (30.0, 15.0, 6.0), (30.0, 0.0, 0.0), 1.0, 0.05),
+    WL.CovSpec(WL.GAUSSIAN, (18.0, 18.0, 6.0), (0.0, 0.0, 0.0), 1.0, 0.05),
+    WL.CovSpec(WL.GAUSSIAN, (12.0, 7.0, 3.0), (45.0, 10.0, 5.0), 2.5, 0.3),
+    WL.CovSpec(WL.SPHERICAL, (8.0, 5.0, 4.0), (120.0, 30.0, 60.0), 1.0, 0.0),
+]
+RADII = [(10, 10, 5), (30, 15, 6), (18, 18, 6), (9, 6, 3), (6, 4, 3)]
+
+
+def header_functions():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(hpgl_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_exports_every_header_function():
+    names = header_functions()
+    assert len(names) >= 20
+    for name in names:
+        assert hasattr(W._hpgl_so, name), name
+    assert set(W.EXPORTS) <= set(names)
+
+
+def test_struct_layouts_match_header():
+    fields = {
+        "hpgl_shape_t": (W._HPGL_SHAPE, ["m_data", "m_strides"]),
+        "hpgl_cont_masked_array_t": (W._HPGL_CONT_MASKED_ARRAY, ["m_data", "m_mask", "m_shape"]),
+        "hpgl_ind_masked_array_t": (W._HPGL_IND_MASKED_ARRAY, ["m_data", "m_mask", "m_shape", "m_indicator_count"]),
+        "hpgl_ok_params_t": (W._HPGL_OK_PARAMS, ["m_covariance_type", "m_ranges", "m_angles", "m_sill", "m_nugget",
+                                                 "m_radiuses", "m_max_neighbours"]),
+        "hpgl_sk_params_t": (W._HPGL_SK_PARAMS, ["m_covariance_type", "m_ranges", "m_angles", "m_sill", "m_nugget",
+                                                 "m_radiuses", "m_max_neighbours", "m_automatic_mean", "m_mean"]),
+        "hpgl_cov_params_t": (W._HPGL_COV_PARAMS, ["m_covariance_type", "m_ranges", "m_angles", "m_sill",
+                                                   "m_nugget"]),
+        "hpgl_median_ik_params_t": (W._HPGL_MEDIAN_IK_PARAMS, ["m_covariance_type", "m_ranges", "m_angles", "m_sill",
+                                                               "m_nugget", "m_radiuses", "m_max_neighbours",
+                                                               "m_marginal_probs"]),
+        "hpgl_ik_params_t": (W._HPGL_IK_PARAMS, ["m_covariance_type", "m_ranges", "m_angles", "m_sill", "m_nugget",
+                                                 "m_radiuses", "m_max_neighbours", "m_marginal_prob"]),
+        "hpgl_b200_options_t": (W._HPGL_B200_OPTIONS, ["precision", "refine_steps", "flags", "stream", "estimate64",
+                                                       "variance", "status", "ik_probs", "tolerance"]),
+    }
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
+    for s, (_, fl) in fields.items():
+        lines.append(f'printf("{s} %zu\\n", sizeof(struct {s}));')
+        for f in fl:
+            lines.append(f'printf("{s}.{f} %zu\\n", offsetof(struct {s}, {f}));')
+    lines.append("return 0;}")
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "layout.c")
+        exe = os.path.join(d, "layout")
+        open(src, "w").write("\n".join(lines))
+        subprocess.run(["/usr/bin/gcc", src, "-o", exe], check=True)
+        out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = dict(l.split() for l in out if l.strip())
+    for s, (ct, fl) in fields.items():
+        assert int(got[s]) == C.sizeof(ct), s
+        for f, (cname, _) in zip(fl, ct._fields_):
+            assert int(got[f"{s}.{f}"]) == getattr(ct, cname).offset, f"{s}.{f}"
+
+
+def _covp(cov):
+    return W._HPGL_COV_PARAMS(covariance_type=cov.cov_type, ranges=cov.ranges, angles=cov.angles, sill=cov.sill,
+                              nugget=cov.nugget)
+
+
+@pytest.mark.parametrize("mi", range(len(MODELS)))
+def test_transform_template_and_covariance_bit_identical(mi):
+    cov, rad = MODELS[mi], RADII[mi]
+    lib = W._hpgl_so
+    t = (C.c_double * 9)()
+    assert lib.hpgl_b200_transform((C.c_double * 3)(*cov.ranges), (C.c_double * 3)(*cov.angles), t) == 0
+    np.testing.assert_array_equal(np.array(list(t)), O.transform("port", cov.ranges, cov.angles))
+    cap = (2 * rad[0] + 1) * (2 * rad[1] + 1) * (2 * rad[2] + 1)
+    for kind in (0, 1):
+        out = np.zeros((cap, 3), np.int32)
+        lim = C.c_int(0)
+        n = lib.hpgl_b200_template(kind, C.byref(_covp(cov)), (C.c_int * 3)(*rad), out.ctypes.data, cap,
+                                   C.byref(lim))
+        ref, rlim = O.template("port", kind, cov, rad)
+        assert n == len(ref) and lim.value == rlim
+        np.testing.assert_array_equal(out[:n], ref)
+    rng = np.random.default_rng(mi)
+    for _ in range(300):
+        a = rng.integers(0, 60, 3).astype(np.int32)
+        b = (a + rng.integers(-2 * max(rad), 2 * max(rad) + 1, 3)).astype(np.int32)
+        for kind in (0, 1):
+            v = lib.hpgl_b200_covariance(kind, C.byref(_covp(cov)), (C.c_int * 3)(*rad), (C.c_int * 3)(*a),
+                                         (C.c_int * 3)(*b))
+            assert v == O.cov_point("port", kind, cov, rad, a, b)
+
+
+def test_zero_range_is_an_error_not_an_abort():
+    lib = W._hpgl_so
+    out = (C.c_double * 9)()
+    assert lib.hpgl_b200_transform((C.c_double * 3)(10, 0, 5), (C.c_double * 3)(0, 0, 0), out) != 0
+    assert "non-zero" in W.last_error()
+
+
+def test_kriging_without_gpu_reports_an_error():
+    """On a machine without a usable GPU the C ABI returns an error code (never a CPU fallback)."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    wl = WL.ok_small(0.2)
+    dims = (C.c_int * 3)(*wl.dims)
+    p = W._HPGL_SK_PARAMS(covariance_type=0, ranges=wl.cov.ranges, angles=wl.cov.angles, sill=1.0, nugget=0.1,
+                          radiuses=wl.radiuses, max_neighbours=12, automatic_mean=1, mean=0.0)
+    out = wl.data.copy()
+    om = wl.mask.copy()
+    rc = W._hpgl_so.hpgl_b200_cont_kriging_ex(0, dims, wl.data.ctypes.data, wl.mask.ctypes.data, C.byref(p),
+                                              out.ctypes.data, om.ctypes.data, None)
+    assert rc == -2
+    np.testing.assert_array_equal(out, wl.data)

@@ -1,0 +1,98 @@
+"""The oracle (CPU restatement, oracle/krige_oracle.cpp) against golden vectors
+produced by the reference itself (tests/golden/make_golden.py)."""
+import numpy as np
+import pytest
+
+import golden_io as G
+import oracle as O
+
+
+@pytest.mark.parametrize("case", G.CONT_CASES)
+@pytest.mark.parametrize("tag,kind", [("ok", 0), ("sk", 1)])
+def test_oracle_matches_reference_per_node(case, tag, kind):
+    g = G.load(case)
+    wl = G.as_workload(g, case)
+    r = O.krige_nodes("port", kind, wl.dims, wl.data, wl.mask, wl.cov, wl.radiuses, wl.max_neighbours,
+                      mean=float(g["sk_mean"]), nodes=g["nodes"], threads=4)
+    # neighbour indices: identical, in the reference's order
+    np.testing.assert_array_equal(r["idx"], g[f"{tag}_idx"])
+    np.testing.assert_array_equal(r["count"], g[f"{tag}_count"])
+    np.testing.assert_array_equal(r["path"], g[f"{tag}_path"])
+    np.testing.assert_array_equal(r["status"], g[f"{tag}_status"])
+    ok = g[f"{tag}_status"] == 0
+    tol = 1e-8 if case.startswith("clustered") else 1e-12  # LAPACK vs own Cholesky, cond(A) * eps
+    scale = max(np.abs(g[f"{tag}_est"][ok]).max(), 1.0)
+    assert np.abs(r["est"][ok] - g[f"{tag}_est"][ok]).max() <= tol * scale
+    assert np.abs(r["var"][ok] - g[f"{tag}_var"][ok]).max() <= tol * max(np.abs(g[f"{tag}_var"][ok]).max(), 1.0)
+    # float estimate the drivers store: same float accumulation, at most a few ulp apart
+    assert np.abs(r["est_f"][ok] - g[f"{tag}_est_f"][ok]).max() <= 4e-7 * scale
+
+
+@pytest.mark.parametrize("case", ["ok_small_s030", "gauss_cv_s020"])
+@pytest.mark.parametrize("tag,kind", [("ok", 0), ("sk", 1)])
+def test_oracle_whole_grid_matches_reference_api(case, tag, kind):
+    g = G.load(case)
+    wl = G.as_workload(g, case)
+    od, om, _, _, _ = O.cont_grid(kind, wl.dims, wl.data, wl.mask, wl.cov, wl.radiuses, wl.max_neighbours, threads=4)
+    np.testing.assert_array_equal(om, g[f"{tag}_grid_mask"])
+    ref = g[f"{tag}_grid_data"]
+    assert np.abs(od - ref).max() <= 4e-7 * max(np.abs(ref).max(), 1.0)
+
+
+def test_oracle_indicator_matches_reference():
+    g = G.load("indicator_s015")
+    dims, data, mask = G.grid_inputs(g, dtype=np.uint8)
+    covs, rads, ks = [], [], []
+    for c in range(5):
+        cov, rad, k = G.cov_of(g, f"c{c}_")
+        covs.append(cov)
+        rads.append(rad)
+        ks.append(k)
+        r = O.krige_nodes("port", 1, dims, data, mask, cov, rad, k, mean=float(np.float32(g["marginals"][c])),
+                          nodes=g["nodes"], ind_value=c, threads=4)
+        np.testing.assert_array_equal(r["idx"], g[f"c{c}_idx"])
+        np.testing.assert_array_equal(r["path"], g[f"c{c}_path"])
+        ok = g[f"c{c}_status"] == 0
+        assert np.abs(r["est_f"][ok] - g[f"c{c}_est_f"][ok]).max() <= 4e-7
+    od, om, probs = O.indicator_grid(dims, data, mask, covs, rads, ks, list(g["marginals"]), threads=4)
+    np.testing.assert_array_equal(od, g["ik_grid"])
+    dims, mdata, mask = G.grid_inputs(g, "mik_values", dtype=np.uint8)
+    cov, rad, _ = G.cov_of(g, "c2_")
+    od, om, prob, st = O.median_ik_grid(dims, mdata, mask, cov, rad, 24, list(g["mik_marginals"]), threads=4)
+    defined = st == 0  # the reference leaves failed cells undefined (median_ik.cpp:65-76)
+    np.testing.assert_array_equal(od[defined], g["mik_grid"][defined])
+
+
+def test_oracle_known_answers():
+    """Constant field -> OK returns the constant; zeros -> 0 (reference test_edge_cases.py:368-392, 487-511)."""
+    g = dict(np.load(G.GOLDEN + "/known_answers.npz"))
+    from geo_bsd import workloads as WL
+    cov = WL.CovSpec(WL.SPHERICAL, (10.0, 10.0, 10.0), (0.0, 0.0, 0.0), 1.0, 0.0)
+    for name, val in (("const42", 42.0), ("zeros", 0.0)):
+        od, om, _, _, _ = O.cont_grid(0, (10, 10, 5), g[f"{name}_data"], g[f"{name}_mask"], cov, (5, 5, 5), 12)
+        np.testing.assert_array_equal(om, g[f"{name}_outmask"])
+        assert np.abs(od - g[f"{name}_out"]).max() <= 1e-4
+        assert np.abs(od[om == 1] - val).max() <= 0.1
+
+
+def test_introsort_restatement_matches_std_sort():
+    rng = np.random.default_rng(5)
+    for trial in range(400):
+        n = int(rng.integers(0, 3000 if trial % 10 == 0 else 200))
+        distinct = int(rng.integers(1, 50))
+        keys = rng.integers(0, distinct, n).astype(np.uint32)
+        a, b = O.sort_check(keys)
+        np.testing.assert_array_equal(a, b)
+
+
+def test_introselect_matches_std_sort_first_k():
+    """The O(n) tie resolver used for straddling cells picks the same first-k set as std::sort."""
+    rng = np.random.default_rng(8)
+    for trial in range(600):
+        n = int(rng.integers(1, 3000 if trial % 7 == 0 else 300))
+        distinct = int(rng.integers(1, 40))
+        keys = rng.integers(0, distinct, n).astype(np.uint32)
+        if trial % 5 == 0:
+            keys = np.sort(keys)[::-1].copy()  # descending runs
+        k = int(rng.integers(1, n + 1))
+        assert O.select_check(keys, k), (n, k, distinct)
