@@ -84,6 +84,7 @@ EXPORTS = [
     "hpgl_b200_cont_kriging_ex", "hpgl_b200_indicator_kriging_ex", "hpgl_b200_median_ik_ex",
     "hpgl_b200_find_neighbours", "hpgl_b200_last_stats", "hpgl_b200_host_alloc", "hpgl_b200_host_free",
     "hpgl_b200_transform", "hpgl_b200_template", "hpgl_b200_covariance", "hpgl_b200_version",
+    "hpgl_b200_sk_weights_noalloc",
 ]
 
 
@@ -148,6 +149,9 @@ def _load():
     lib.hpgl_b200_covariance.restype = C.c_double
     lib.hpgl_b200_covariance.argtypes = [C.c_int, C.POINTER(_HPGL_COV_PARAMS), i_p, i_p, i_p]
     lib.hpgl_b200_version.restype = C.c_char_p
+    lib.hpgl_b200_sk_weights_noalloc.restype = C.c_int
+    lib.hpgl_b200_sk_weights_noalloc.argtypes = [C.POINTER(C.c_float), _f32, _f32, _f32, C.c_int,
+                                                 C.POINTER(_HPGL_COV_PARAMS), _f32, C.c_void_p]
     return lib
 
 

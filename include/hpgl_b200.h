@@ -164,6 +164,22 @@ int hpgl_b200_find_neighbours(int kind, const int *dims, const unsigned char *ma
 #define HPGL_B200_STATS_LEN 36
 int hpgl_b200_last_stats(double *out, int cap);
 
+/* No counterpart in the reference. The same SK weights as
+ * hpgl_simple_kriging_weights for callers that cannot allocate device memory
+ * while they run (device memory owned by another allocator, or a fixed budget
+ * reserved up front): the system is solved in a fixed file-scope device array
+ * (about 135 KB, held by every GPU that loads the library until exit), so the
+ * call never allocates or frees device memory. At most 128 neighbours
+ * (HPGL_B200_ELIMIT beyond). Calls share the array: calls that overlap on the
+ * GPU race and must be serialised by the caller. The first call on a device
+ * looks the array's address up (cudaGetSymbolAddress); make it before any
+ * stream capture. Host pointers; `stream` may be NULL (the legacy stream).
+ * Returns 0, or a negative HPGL_B200_E* code with the message kept for
+ * hpgl_get_last_exception_message. */
+int hpgl_b200_sk_weights_noalloc(const float *center_coords, const float *neighbours_x, const float *neighbours_y,
+                                 const float *neighbours_z, int neighbours_count,
+                                 const struct hpgl_cov_params_t *params, float *weights, void *stream);
+
 /* Page-locked host buffers for fast copies (cudaHostAlloc / cudaFreeHost). */
 void *hpgl_b200_host_alloc(size_t bytes);
 void hpgl_b200_host_free(void *p);
