@@ -462,10 +462,10 @@ static void run_solves(Engine &E, const Plan &pl, const DevPoints &P, const DevS
     int *bucket_cnt = E.buf<int>("bucket_cnt", kBuckets);
     int *bucket_off = E.buf<int>("bucket_off", kBuckets + 1);
     int *bucket_fill = E.buf<int>("bucket_fill", kBuckets);
-    int *cells = E.buf<int>("cells", (size_t)g.n_cells);
+    int2 *cells = E.buf<int2>("cells", (size_t)g.n_cells);
     unsigned long long *moments = E.buf<unsigned long long>("moments", kBuckets * 3);
     int *esc_cnt = E.buf<int>("esc_cnt", kBuckets);
-    int *esc_cells = precision ? E.buf<int>("esc_cells", (size_t)g.n_cells) : nullptr;
+    int2 *esc_cells = precision ? E.buf<int2>("esc_cells", (size_t)g.n_cells) : nullptr;
     launch_prepare(g, d_mask, all_cells, S.nb_n, d_status, bucket_cnt, bucket_off, bucket_fill, cells, moments, st);
     HB_CK(cudaMemsetAsync(esc_cnt, 0, sizeof(int) * kBuckets, st));
     HB_CK(cudaGetLastError());
@@ -485,7 +485,7 @@ static void run_solves(Engine &E, const Plan &pl, const DevPoints &P, const DevS
         esc_off[b] = off;
         if (cnt[b] > 0)
         {
-            const int *bcells = cells + off;
+            const int2 *bcells = cells + off;
             HB_CK(cudaEventRecord(E.ev_[10 + 2 * b], st));
             if (b < 4)
             {

@@ -71,13 +71,13 @@ cudaError_t launch_resolve_ties_fast(const Geom &g, const int *tie_cells, const 
                                      int cap, int *nb_pid, int2 *nb_rec, int n_sm, cudaStream_t st);
 
 // solves (solve.cu, misc.cu)
-cudaError_t launch_solve_bucket(int np, int precision, bool ordinary, const Geom &g, const int *cells,
+cudaError_t launch_solve_bucket(int np, int precision, bool ordinary, const Geom &g, const int2 *cells,
                                 const int *n_items, int max_items, const int2 *nb_rec, const int *nb_n, int ind_value,
                                 const double *pair64, const float *pair32, double mean, double c0, int steps,
-                                double tol, const SolveOut &out, int *esc_cells, int *esc_count, int n_sm,
+                                double tol, const SolveOut &out, int2 *esc_cells, int *esc_count, int n_sm,
                                 cudaStream_t st);
 size_t large_scratch_doubles(int k, int blocks);
-cudaError_t launch_solve_large(const Geom &g, const int *cells, const int *n_items, int blocks, const int2 *nb_rec,
+cudaError_t launch_solve_large(const Geom &g, const int2 *cells, const int *n_items, int blocks, const int2 *nb_rec,
                                const int *nb_n, int ind_value, const double *pair64, bool ordinary, double mean,
                                double c0, double *scratch, const SolveOut &out, cudaStream_t st);
 
@@ -85,7 +85,7 @@ cudaError_t launch_solve_large(const Geom &g, const int *cells, const int *n_ite
 void launch_build_pair(const Geom &g, const DevModel &m, int truncated, const double *search_vals, double *pair64,
                        float *pair32, cudaStream_t st);
 void launch_prepare(const Geom &g, const uint8_t *mask, int all_cells, const int *nb_n, signed char *status,
-                    int *bucket_cnt, int *bucket_off, int *bucket_fill, int *cells,
+                    int *bucket_cnt, int *bucket_off, int *bucket_fill, int2 *cells,
                     unsigned long long *moments, cudaStream_t st);
 void launch_finalize_cont(const Geom &g, const float *in_data, signed char *status, int simple, float mean_f,
                           float *out_data, uint8_t *out_mask, double *est64, double *var, cudaStream_t st);

@@ -128,15 +128,19 @@ __global__ void k_bucket_offsets(const int *__restrict__ cnt, int *__restrict__ 
 }
 
 __global__ void k_bucket_fill(const Geom g, const signed char *__restrict__ status, const int *__restrict__ nb_n,
-                              const int *__restrict__ off, int *__restrict__ fill, int *__restrict__ cells)
+                              const int *__restrict__ off, int *__restrict__ fill, int2 *__restrict__ cells)
 {
     const int lane = threadIdx.x & 31;
     for (long long base = (long long)blockIdx.x * blockDim.x; base < g.n_cells;
          base += (long long)gridDim.x * blockDim.x)
     {
         long long c = base + threadIdx.x;
-        int b = -1;
-        if (c < g.n_cells && status[c] == 3) b = bucket_of(nb_n[c]);
+        int b = -1, nn = 0;
+        if (c < g.n_cells && status[c] == 3)
+        {
+            nn = nb_n[c];
+            b = bucket_of(nn);
+        }
         // warp-aggregated append per bucket
         for (int q = 0; q < kBuckets; ++q)
         {
@@ -150,14 +154,14 @@ __global__ void k_bucket_fill(const Geom g, const signed char *__restrict__ stat
             {
                 unsigned lt;
                 asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
-                cells[off[q] + start + __popc(m & lt)] = (int)c;
+                cells[off[q] + start + __popc(m & lt)] = make_int2((int)c, nn);
             }
         }
     }
 }
 
 void launch_prepare(const Geom &g, const uint8_t *mask, int all_cells, const int *nb_n, signed char *status,
-                    int *bucket_cnt, int *bucket_off, int *bucket_fill, int *cells,
+                    int *bucket_cnt, int *bucket_off, int *bucket_fill, int2 *cells,
                     unsigned long long *moments, cudaStream_t st)
 {
     cudaMemsetAsync(bucket_cnt, 0, sizeof(int) * kBuckets, st);
@@ -290,7 +294,7 @@ void launch_mik_finalize(long long n_cells, const signed char *status, const dou
 // ------------------------------------------------------------- large systems
 // Neighbour counts above 64: one CTA per system, matrix in global scratch,
 // double precision, right-looking Cholesky with block barriers.
-__global__ void __launch_bounds__(256) k_solve_large(const Geom g, const int *__restrict__ cells,
+__global__ void __launch_bounds__(256) k_solve_large(const Geom g, const int2 *__restrict__ cells,
                                                      const int *__restrict__ n_items_ptr, const int2 *__restrict__ nb_rec,
                                                      const int *__restrict__ nb_n, int ind_value,
                                                      const double *__restrict__ pair64, int ordinary, double mean,
@@ -303,8 +307,8 @@ __global__ void __launch_bounds__(256) k_solve_large(const Geom g, const int *__
     const long long pc = g.pair_center;
     for (int item = blockIdx.x; item < n_items; item += gridDim.x)
     {
-        const int cell = cells[item];
-        const int n = nb_n[cell];
+        const int cell = cells[item].x;
+        const int n = cells[item].y;
         const int2 *rec = nb_rec + (long long)cell * kmax;
         for (int e = threadIdx.x; e < n * n; e += blockDim.x)
         {
@@ -399,7 +403,7 @@ __global__ void __launch_bounds__(256) k_solve_large(const Geom g, const int *__
 
 size_t large_scratch_doubles(int k, int blocks) { return (size_t)blocks * ((size_t)k * k + 4 * (size_t)k); }
 
-cudaError_t launch_solve_large(const Geom &g, const int *cells, const int *n_items, int blocks, const int2 *nb_rec,
+cudaError_t launch_solve_large(const Geom &g, const int2 *cells, const int *n_items, int blocks, const int2 *nb_rec,
                                const int *nb_n, int ind_value, const double *pair64, bool ordinary, double mean,
                                double c0, double *scratch, const SolveOut &out, cudaStream_t st)
 {

@@ -272,13 +272,19 @@ __device__ __forceinline__ void residuals_fp64(const Grp<NP> &grp, const double 
     grp.sync();
 }
 
+// Minimum resident 256-thread blocks per SM requested for the FP32 kernels
+// (caps their registers at 65536 / (256 * blocks)).
+#ifndef HB_SOLVE_MIN_BLOCKS_F32
+#define HB_SOLVE_MIN_BLOCKS_F32 3
+#endif
+
 template <int NP, typename TF, bool ORDINARY, bool REFINE>
-__global__ void __launch_bounds__(256) k_solve(const Geom g, const int *__restrict__ cells,
+__global__ void __launch_bounds__(256, sizeof(TF) == 4 ? HB_SOLVE_MIN_BLOCKS_F32 : 1) k_solve(const Geom g, const int2 *__restrict__ cells,
                                                const int *__restrict__ n_items_ptr, const int2 *__restrict__ nb_rec,
                                                const int *__restrict__ nb_n, int ind_value,
                                                const double *__restrict__ pair64, const float *__restrict__ pair32,
                                                double mean, double c0, int steps, double tol, SolveOut out,
-                                               int *__restrict__ esc_cells, int *__restrict__ esc_count)
+                                               int2 *__restrict__ esc_cells, int *__restrict__ esc_count)
 {
     typedef SolveSmem<NP, TF> SM;
     constexpr int LD = SM::LD;
@@ -313,31 +319,22 @@ __global__ void __launch_bounds__(256) k_solve(const Geom g, const int *__restri
     const long long pc = g.pair_center;
     const int stride = gridDim.x * groups_per_block;
     const float mf = (float)mean; // mean_t is float (typedefs.h:122)
+    // Work items are {cell, n}. The record of item i+1 and the work entry of
+    // item i+2 are loaded while item i is solved, so no load the solve waits on
+    // depends on another load issued in the same iteration.
     int item = blockIdx.x * groups_per_block + gi;
-    int cell = 0, n = 0;
-    int2 rec = make_int2(0, 0);
-    if (item < n_items)
-    {
-        cell = cells[item];
-        n = nb_n[cell];
-        if (r < n) rec = nb_rec[(long long)cell * g.k + r];
-    }
+    int2 w_cur = item < n_items ? cells[item] : make_int2(0, 0);
+    int2 w_nxt = item + stride < n_items ? cells[item + stride] : make_int2(0, 0);
+    int2 rec = (item < n_items && r < w_cur.y) ? nb_rec[(long long)w_cur.x * g.k + r] : make_int2(0, 0);
     for (; item < n_items; item += stride)
     {
-        const int my_cell = cell, my_n = n;
+        const int my_cell = w_cur.x, my_n = w_cur.y;
         const int lin = rec.x;
         const bool live = r < my_n;
         const float vraw = __int_as_float(rec.y);
-        {
-            // issue the next item's record loads; they complete during this solve
-            int nxt = item + stride;
-            if (nxt < n_items)
-            {
-                cell = cells[nxt];
-                n = nb_n[cell];
-                rec = r < n ? nb_rec[(long long)cell * g.k + r] : make_int2(0, 0);
-            }
-        }
+        rec = (item + stride < n_items && r < w_nxt.y) ? nb_rec[(long long)w_nxt.x * g.k + r] : make_int2(0, 0);
+        w_cur = w_nxt;
+        w_nxt = item + 2 * stride < n_items ? cells[item + 2 * stride] : make_int2(0, 0);
         // neighbour value centred on the (float) mean as combine() does (combiner.h:19-24)
         float v = 0.0f;
         if (live) v = ind_value >= 0 ? (vraw == (float)ind_value ? 1.0f : 0.0f) : vraw;
@@ -507,7 +504,7 @@ __global__ void __launch_bounds__(256) k_solve(const Geom g, const int *__restri
             if (r == 0)
             {
                 int slot = atomicAdd(esc_count, 1);
-                esc_cells[slot] = my_cell;
+                esc_cells[slot] = make_int2(my_cell, my_n);
                 if (out.status) out.status[my_cell] = 4;
             }
             grp.sync();
@@ -554,9 +551,9 @@ __global__ void __launch_bounds__(256) k_solve(const Geom g, const int *__restri
 }
 
 template <int NP, typename TF, bool ORD, bool REF>
-static cudaError_t launch_one(const Geom &g, const int *cells, const int *n_items, int max_items, const int2 *nb_rec,
+static cudaError_t launch_one(const Geom &g, const int2 *cells, const int *n_items, int max_items, const int2 *nb_rec,
                               const int *nb_n, int ind_value, const double *pair64, const float *pair32, double mean,
-                              double c0, int steps, double tol, const SolveOut &out, int *esc_cells, int *esc_count,
+                              double c0, int steps, double tol, const SolveOut &out, int2 *esc_cells, int *esc_count,
                               int n_sm, cudaStream_t st)
 {
     constexpr int threads = 256;
@@ -579,10 +576,10 @@ static cudaError_t launch_one(const Geom &g, const int *cells, const int *n_item
 }
 
 template <int NP>
-static cudaError_t launch_np(int precision, bool ordinary, const Geom &g, const int *cells, const int *n_items,
+static cudaError_t launch_np(int precision, bool ordinary, const Geom &g, const int2 *cells, const int *n_items,
                              int max_items, const int2 *nb_rec, const int *nb_n, int ind_value, const double *pair64,
                              const float *pair32, double mean, double c0, int steps, double tol, const SolveOut &out,
-                             int *esc_cells, int *esc_count, int n_sm, cudaStream_t st)
+                             int2 *esc_cells, int *esc_count, int n_sm, cudaStream_t st)
 {
 #define HB_ARGS g, cells, n_items, max_items, nb_rec, nb_n, ind_value, pair64, pair32, mean, c0, steps, tol, out, esc_cells, esc_count, n_sm, st
     if (precision == 0)
@@ -591,10 +588,10 @@ static cudaError_t launch_np(int precision, bool ordinary, const Geom &g, const 
 #undef HB_ARGS
 }
 
-cudaError_t launch_solve_bucket(int np, int precision, bool ordinary, const Geom &g, const int *cells,
+cudaError_t launch_solve_bucket(int np, int precision, bool ordinary, const Geom &g, const int2 *cells,
                                 const int *n_items, int max_items, const int2 *nb_rec, const int *nb_n, int ind_value,
                                 const double *pair64, const float *pair32, double mean, double c0, int steps,
-                                double tol, const SolveOut &out, int *esc_cells, int *esc_count, int n_sm,
+                                double tol, const SolveOut &out, int2 *esc_cells, int *esc_count, int n_sm,
                                 cudaStream_t st)
 {
     switch (np)
