@@ -167,6 +167,7 @@ struct Plan
     Flavour f;
     std::vector<Offset> tmpl;
     KeyTable kt;
+    Surrogate sg;
     Geom g;
     int rank_bits = 0;
 };
@@ -222,6 +223,7 @@ static Plan make_plan(bool truncated, int cov_type, const double *ranges, const 
     for (int a = 0; a < 3; ++a) pl.f.r[a] = radiuses[a];
     pl.tmpl = build_template(pl.f);
     build_key_table(pl.f, pl.kt, g_threads);
+    if (k <= 64 && pl.kt.n_ranks <= 0xFFFE) build_surrogate(pl.f, pl.kt, pl.sg);
     pl.rank_bits = pl.kt.n_ranks > 1 ? bits_for(pl.kt.n_ranks - 1) : 0;
 
     Geom &g = pl.g;
@@ -327,7 +329,7 @@ struct DevSearch
 // uninformed ones. Table slots are suffixed with `tag` so several flavours can
 // coexist (IK categories run one after another and reuse them).
 static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const uint8_t *d_mask, int all_cells,
-                            cudaStream_t st, bool want_pids = false)
+                            cudaStream_t st, bool want_pids = false, bool exact_search = false)
 {
     const Geom &g = pl.g;
     DevSearch S;
@@ -351,6 +353,18 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
         HB_CK(cudaMemcpyAsync(keytab16, k16.data(), k16.size() * 2, cudaMemcpyHostToDevice, st));
         HB_CK(cudaStreamSynchronize(st)); // k16 is a temporary
     }
+    SurrDev sd = {};
+    if (fast_keys && pl.sg.ok && !exact_search)
+    {
+        double *h2r = E.buf<double>("h2_rank", pl.sg.h2_rank.size());
+        HB_CK(cudaMemcpyAsync(h2r, pl.sg.h2_rank.data(), pl.sg.h2_rank.size() * 8, cudaMemcpyHostToDevice, st));
+        sd.on = 1;
+        for (int i = 0; i < 9; ++i) sd.T[i] = pl.sg.T[i];
+        for (int a = 0; a < 3; ++a) sd.step[a] = pl.sg.step[a];
+        sd.e3 = pl.sg.e3;
+        sd.h2_cut = pl.sg.h2_cut;
+        sd.h2_rank = h2r;
+    }
     HB_CK(cudaMemcpyAsync(tmpl, t4.data(), t4.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
     long long pn = (long long)g.pnx * g.pny * (2 * g.phz + 1);
     S.pair64 = E.buf<double>("pair64", (size_t)pn);
@@ -364,7 +378,7 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
     int *bin_fill = E.buf<int>("bin_fill", g.n_bins);
     S.bin_flag = E.buf<uint8_t>("bin_flag", g.n_bins);
     int *bin_pts = E.buf<int>("bin_pts", std::max(P.m, 1));
-    int *scal = E.buf<int>("scalars", 8); // 0 total, 1 max_cand, 2 tmpl bins, 3 ties, 4 tmpl cells
+    int *scal = E.buf<int>("scalars", 8); // 0 total, 1 max_cand, 2 tmpl bins, 3 ties, 4 tmpl cells, 5 exact cells
     int *tmp = E.buf<int>("scan_tmp2", (size_t)scan_tmp_ints(g.n_bins) + 4);
     HB_CK(cudaMemsetAsync(bin_cnt, 0, sizeof(int) * g.n_bins, st));
     HB_CK(cudaMemsetAsync(bin_fill, 0, sizeof(int) * g.n_bins, st));
@@ -401,8 +415,8 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
     HB_CK(cudaEventRecord(E.ev_[8], st));
     if (fast)
         HB_CK(launch_search_fast(g, d_mask, all_cells, bin_start, bin_cnt, S.bin_flag, bin_pts, P.pts_xyz, P.pts_val,
-                                 keytab16, tmpl, (int)pl.tmpl.size(), P.pid_of_node, cand_cap, warps, S.nb_pid,
-                                 S.nb_rec, S.nb_n, tie_cells, scal + 3, scal + 4, st));
+                                 keytab16, sd, tmpl, (int)pl.tmpl.size(), P.pid_of_node, cand_cap, warps, S.nb_pid,
+                                 S.nb_rec, S.nb_n, tie_cells, scal + 3, scal + 4, scal + 5, st));
     else
         HB_CK(launch_search(g, d_mask, all_cells, bin_start, bin_cnt, S.bin_flag, bin_pts, P.pts_xyz, P.pts_val,
                             keytab, pl.rank_bits, tmpl, (int)pl.tmpl.size(), P.pid_of_node, cand_cap, warps,
@@ -412,6 +426,8 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
     HB_CK(cudaStreamSynchronize(st));
     S.ties = host_scal[3];
     S.template_cells = host_scal[4];
+    E.stats.exact_cells += host_scal[5];
+    E.stats.prefilter = E.stats.prefilter || (fast && sd.on);
     E.mark(STAGE_SEARCH, st);
     {
         float ms = 0;
@@ -655,7 +671,7 @@ int cont_kriging(int kind, const int *dims, const float *in_data, const unsigned
 
         HB_CK(cudaEventRecord(E.ev_[2], st));
         DevPoints P = compact_points(E, pl.g, d_mask, d_in, nullptr, st);
-        DevSearch S = run_search(E, pl, P, d_mask, 0, st);
+        DevSearch S = run_search(E, pl, P, d_mask, 0, st, false, (opt.flags & 4u) != 0);
         HB_CK(cudaEventRecord(E.ev_[3], st));
         SolveOut so{};
         so.out_data = d_out;
@@ -733,7 +749,7 @@ int indicator_kriging(const int *dims, const unsigned char *in_data, const unsig
                              : make_plan(true, a.cov_type, a.ranges, a.angles, a.sill, a.nugget, a.radiuses, a.max_nb,
                                          dims);
             HB_CK(cudaEventRecord(E.ev_[5], st));
-            DevSearch S = run_search(E, pl, P, d_mask, 1, st);
+            DevSearch S = run_search(E, pl, P, d_mask, 1, st, false, (opt.flags & 4u) != 0);
             HB_CK(cudaEventRecord(E.ev_[6], st));
             SolveOut so{};
             so.status = d_status;
@@ -798,7 +814,7 @@ int median_ik(const int *dims, const unsigned char *in_data, const unsigned char
         float *d_prob = opt.ik_probs ? ((io.device) ? opt.ik_probs : E.buf<float>("ik_probs", (size_t)n)) : nullptr;
         HB_CK(cudaEventRecord(E.ev_[2], st));
         DevPoints P = compact_points(E, pl.g, d_mask, nullptr, d_in, st);
-        DevSearch S = run_search(E, pl, P, d_mask, 1, st);
+        DevSearch S = run_search(E, pl, P, d_mask, 1, st, false, (opt.flags & 4u) != 0);
         HB_CK(cudaEventRecord(E.ev_[3], st));
         SolveOut so{};
         so.status = d_status;

@@ -66,6 +66,8 @@ struct Stats
     long long bucket_items[5] = {0, 0, 0, 0, 0};
     double bucket_ms[5] = {0, 0, 0, 0, 0};
     double bucket_flops[5] = {0, 0, 0, 0, 0};
+    long long exact_cells = 0; // cells the float prefilter left to the exact rank path
+    bool prefilter = false;
 };
 
 void set_error(const std::string &msg);

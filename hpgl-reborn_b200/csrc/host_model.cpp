@@ -182,4 +182,70 @@ void build_key_table(const Flavour &f, KeyTable &kt, int n_threads)
     }
     kt.n_ranks = kept.empty() ? 0 : r + 1;
 }
+void build_surrogate(const Flavour &f, const KeyTable &kt, Surrogate &sg)
+{
+    sg.ok = false;
+    sg.h2_rank.clear();
+    for (int i = 0; i < 9; ++i) sg.T[i] = (float)f.m.T[i];
+    struct Ent
+    {
+        double h2;
+        uint32_t rank;
+    };
+    std::vector<Ent> kept;
+    for (int iz = 0; iz < kt.n[2]; ++iz)
+        for (int iy = 0; iy < kt.n[1]; ++iy)
+            for (int ix = 0; ix < kt.n[0]; ++ix)
+            {
+                const long i = ((long)iz * kt.n[1] + iy) * kt.n[0] + ix;
+                if (kt.rank[i] == KEY_EXCLUDED) continue;
+                const double v[3] = {(double)(0 - (ix - kt.half[0])), (double)(0 - (iy - kt.half[1])),
+                                     (double)(0 - (iz - kt.half[2]))};
+                double acc = 0.0;
+                for (int r = 0; r < 3; ++r)
+                {
+                    double d = 0.0;
+                    d += v[0] * f.m.T[3 * r + 0];
+                    d += v[1] * f.m.T[3 * r + 1];
+                    d += v[2] * f.m.T[3 * r + 2];
+                    acc += d * d;
+                }
+                kept.push_back({acc, kt.rank[i]});
+            }
+    if (kept.empty()) return;
+    std::sort(kept.begin(), kept.end(), [](const Ent &a, const Ent &b) {
+        return a.h2 < b.h2 || (a.h2 == b.h2 && a.rank < b.rank);
+    });
+    // offsets whose h2 agree mathematically can differ in the last bit and still
+    // share a covariance value (one rank, several h2): keep the largest h2 per rank
+    sg.h2_rank.assign(kt.n_ranks, 0.0);
+    for (size_t j = 0; j < kept.size(); ++j)
+    {
+        if (j > 0 && kept[j].rank < kept[j - 1].rank) return; // not monotone
+        if (kept[j].rank >= kt.n_ranks) return;
+        sg.h2_rank[kept[j].rank] = kept[j].h2; // ascending h2: the last one is the largest
+    }
+    sg.h2_cut = kept.back().h2;
+    // A transformed coordinate is formed in float as fma(T2, z, fma(T1, y, T0 * x))
+    // for the cell and for the candidate, both relative to the bin corner, then
+    // subtracted: with |T' - T| <= u |T| and four roundings, each component is off
+    // by at most 5.02 u sum_j |T_ij| (|p_j| + |c_j|), where |p_j| <= 2 r_j and
+    // |c_j| < r_j. 16 u sum_j |T_ij| r_j bounds that with room to spare.
+    const double u = 1.0 / 16777216.0;
+    double E = 0.0;
+    for (int r = 0; r < 3; ++r)
+    {
+        double s = 0.0;
+        for (int c = 0; c < 3; ++c) s += std::fabs(f.m.T[3 * r + c]) * (double)f.r[c];
+        E = std::max(E, 16.0 * u * s);
+    }
+    sg.e3 = 1.7320508075688774 * E + 1e-30;
+    for (int a = 0; a < 3; ++a)
+    {
+        double s = 0.0;
+        for (int r = 0; r < 3; ++r) s += f.m.T[3 * r + a] * f.m.T[3 * r + a];
+        sg.step[a] = (float)(std::sqrt(s) * (1.0 + 1e-6));
+    }
+    sg.ok = true;
+}
 } // namespace hb

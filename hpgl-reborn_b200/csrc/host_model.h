@@ -82,5 +82,25 @@ struct KeyTable
 };
 void build_key_table(const Flavour &f, KeyTable &kt, int n_threads);
 
+// Float surrogate of the selection key. Over the kept offsets of the key
+// block the dense rank must be a non-decreasing function of the reference's
+// squared anisotropic distance h2 = sum_i (sum_j T_ij v_j)^2 (the quantity
+// whose square root transfrom_and_norm returns, cov_model.h:63-77).
+// build_surrogate checks that on the exact doubles and records, per rank, the
+// largest h2 carrying it; when the check holds (ok == true) any candidate whose
+// true h2 exceeds that value for the k-th selected rank ranks strictly after
+// it, so a float h2 with a bounded error can discard far candidates without
+// reading their ranks.
+struct Surrogate
+{
+    bool ok = false;
+    float T[9];                 // the transform rounded to float
+    double h2_cut = 0;          // largest h2 of a kept offset
+    double e3 = 0;              // bound on || float(T d) - T d ||_2 for the packed offsets
+    float step[3] = {0, 0, 0};  // ||T e_a||: a bound on how far the k-th distance moves per unit step
+    std::vector<double> h2_rank; // largest h2 of each rank
+};
+void build_surrogate(const Flavour &f, const KeyTable &kt, Surrogate &sg);
+
 int clamp_threads(int n);
 } // namespace hb

@@ -52,13 +52,26 @@ cudaError_t launch_search(const Geom &g, const uint8_t *mask, int all_cells, con
                           int rank_bits, const int4 *tmpl, int n_tmpl, const int *pid_of_node, int cand_cap,
                           int warps, int *nb_pid, int2 *nb_rec, int *nb_n, int *tie_cells, int *tie_count,
                           int *n_template_cells, cudaStream_t st);
+// Float-distance prefilter of the fast selection (host_model.h, Surrogate):
+// on == 0 runs the exact rank path for every cell.
+struct SurrDev
+{
+    int on;
+    float T[9];
+    float step[3];
+    double e3;
+    double h2_cut;
+    const double *h2_rank;
+};
+
 size_t search_fast_smem_bytes(int cand_cap, int k, int warps);
+// exact_cells (may be null) counts cells the float prefilter left to the exact path
 cudaError_t launch_search_fast(const Geom &g, const uint8_t *mask, int all_cells, const int *bin_start,
                                const int *bin_cnt, const uint8_t *bin_flag, const int *bin_pts,
                                const unsigned long long *pts_xyz, const float *pts_vf, const uint16_t *keytab16,
-                               const int4 *tmpl, int n_tmpl, const int *pid_of_node, int cand_cap, int warps,
-                               int *nb_pid, int2 *nb_rec, int *nb_n, int *tie_cells, int *tie_count,
-                               int *n_template_cells, cudaStream_t st);
+                               const SurrDev &sd, const int4 *tmpl, int n_tmpl, const int *pid_of_node, int cand_cap,
+                               int warps, int *nb_pid, int2 *nb_rec, int *nb_n, int *tie_cells, int *tie_count,
+                               int *n_template_cells, int *exact_cells, cudaStream_t st);
 void launch_resolve_ties(const Geom &g, const int *tie_cells, const int *tie_count, int first, int chunk,
                          const int *bin_start, const int *bin_cnt, const int *bin_pts,
                          const unsigned long long *pts_xyz, const float *pts_vf, const uint32_t *keytab,

@@ -701,15 +701,119 @@ __device__ int select_fast(const Geom &g, int C, const int *cklin, const int *cp
     return n_sel;
 }
 
+// Float prefilter of select_fast. One sweep forms every candidate's squared
+// transformed distance h2f in float (no table reads) and keeps those with
+// h2f <= Tg; only these (at most CAP) read their exact ranks, which are sorted
+// as in select_fast. A candidate left out has h2f > Tg, so its true h2 exceeds
+// lo = (sqrt(Tg / (1 + 4u)) - e3)^2 (three roundings in h2f, e3 the bound on the
+// coordinate error). With the ranks non-decreasing in h2, lo above the largest
+// h2 carrying the k-th kept rank (or above every kept offset's h2 when fewer
+// than k are kept) means every candidate left out ranks strictly after the
+// k-th, so the outcome equals the exact path's. Returns n_sel, -1 for a tie group straddling
+// the k-th slot, or -2 when the prefilter cannot decide (the caller then runs
+// select_fast). On success or -1, H receives that bound.
+template <int E>
+__device__ int select_surr(const Geom &g, const SurrDev &sd, int C, const float4 *ctp, const int *cklin,
+                           const int *cplin, const int *cpid, const float *cval, int kc0, int klin_c, int plin_c,
+                           const uint16_t *__restrict__ keytab, uint32_t *sel, int lane, float tcx, float tcy,
+                           float tcz, float Tg, double &H, int &kguess, int *out_pid, int2 *out_rec)
+{
+    constexpr int CAP = 32 * E;
+    const int k = g.k;
+    int cnt = 0;
+    __syncwarp(); // the previous cell's reads of sel are done
+    for (int base = 0; base < C; base += 32)
+    {
+        const int i = base + lane;
+        bool in = false;
+        if (i < C)
+        {
+            const float4 t = ctp[i];
+            const float qx = t.x - tcx, qy = t.y - tcy, qz = t.z - tcz;
+            in = fmaf(qz, qz, fmaf(qy, qy, qx * qx)) <= Tg;
+        }
+        const unsigned bl = __ballot_sync(0xffffffffu, in);
+        if (in)
+        {
+            const int slot = cnt + __popc(bl & lanemask_lt());
+            if (slot < CAP) sel[slot] = (uint32_t)i;
+        }
+        cnt += __popc(bl);
+        if (cnt > CAP) return -2;
+    }
+    __syncwarp();
+    uint32_t v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+    {
+        const int i = e * 32 + lane;
+        v[e] = 0xFFFFFFFFu;
+        if (i < cnt)
+        {
+            const uint32_t pos = sel[i];
+            const uint32_t r16 = keytab[kc0 + cklin[pos] - klin_c];
+            if (r16 != 0xFFFFu) v[e] = (r16 << 16) | pos;
+        }
+    }
+    __syncwarp();
+    warp_bitonic_sort<E>(v, lane);
+    int nk = 0;
+#pragma unroll
+    for (int e = 0; e < E; ++e) nk += __popc(__ballot_sync(0xffffffffu, v[e] != 0xFFFFFFFFu));
+    uint32_t kth = 0;
+    if (nk >= k)
+    {
+        kth = __shfl_sync(0xffffffffu, v[(k - 1) >> 5], (k - 1) & 31);
+        H = sd.h2_rank[kth >> 16];
+    }
+    else
+        H = sd.h2_cut;
+    const double s = sqrt((double)Tg / (1.0 + 4.0 / 16777216.0)) - sd.e3;
+    const double lo = s > 0.0 ? s * s * (1.0 - 1e-12) : 0.0;
+    if (!(lo > H)) return -2;
+    const int n_sel = nk < k ? nk : k;
+    if (nk > k)
+    {
+        const uint32_t nxt = __shfl_sync(0xffffffffu, v[k >> 5], k & 31);
+        if ((nxt >> 16) == (kth >> 16))
+        {
+            kguess = (int)(kth >> 16);
+            return -1;
+        }
+    }
+    if (n_sel > 0) kguess = (int)(__shfl_sync(0xffffffffu, v[(n_sel - 1) >> 5], (n_sel - 1) & 31) >> 16);
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+    {
+        const int i = e * 32 + lane;
+        if (i < n_sel)
+        {
+            const int pos = (int)(v[e] & 0xFFFFu);
+            if (out_pid) out_pid[i] = cpid[pos];
+            if (out_rec) out_rec[i] = make_int2(cplin[pos] - plin_c, __float_as_int(cval[pos]));
+        }
+    }
+    return n_sel;
+}
+
+// transformed coordinates of an offset from the bin corner, in float
+__device__ __forceinline__ float4 surr_coords(const SurrDev &sd, int x, int y, int z)
+{
+    const float fx = (float)x, fy = (float)y, fz = (float)z;
+    return make_float4(fmaf(sd.T[2], fz, fmaf(sd.T[1], fy, sd.T[0] * fx)),
+                       fmaf(sd.T[5], fz, fmaf(sd.T[4], fy, sd.T[3] * fx)),
+                       fmaf(sd.T[8], fz, fmaf(sd.T[7], fy, sd.T[6] * fx)), 0.0f);
+}
+
 template <int E>
 __global__ void __launch_bounds__(256) k_search_fast(
     const Geom g, const uint8_t *__restrict__ mask, int all_cells, const int *__restrict__ bin_start,
     const int *__restrict__ bin_cnt, const uint8_t *__restrict__ bin_flag, const int *__restrict__ bin_pts,
     const unsigned long long *__restrict__ pts_xyz, const float *__restrict__ pts_vf,
-    const uint16_t *__restrict__ keytab16, const int4 *__restrict__ tmpl, int n_tmpl,
+    const uint16_t *__restrict__ keytab16, const SurrDev sd, const int4 *__restrict__ tmpl, int n_tmpl,
     const int *__restrict__ pid_of_node, int cand_cap, int *__restrict__ nb_pid, int2 *__restrict__ nb_rec,
     int *__restrict__ nb_n, int *__restrict__ tie_cells, int *__restrict__ tie_count,
-    int *__restrict__ n_template_cells)
+    int *__restrict__ n_template_cells, int *__restrict__ exact_cells)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int b = blockIdx.x;
@@ -729,7 +833,8 @@ __global__ void __launch_bounds__(256) k_search_fast(
         return;
     }
 
-    int *cklin = reinterpret_cast<int *>(smem);
+    float4 *ctp = reinterpret_cast<float4 *>(smem);
+    int *cklin = reinterpret_cast<int *>(ctp + cand_cap);
     int *cplin = cklin + cand_cap;
     int *cpid = cplin + cand_cap;
     float *cval = reinterpret_cast<float *>(cpid + cand_cap);
@@ -772,20 +877,58 @@ __global__ void __launch_bounds__(256) k_search_fast(
             cplin[d] = ((pz - z0) * g.pny + (py - y0)) * g.pnx + (px - x0);
             cpid[d] = p;
             cval[d] = pts_vf[p];
+            ctp[d] = surr_coords(sd, px - x0, py - y0, pz - z0);
         }
     }
     __syncthreads();
     const int kc0 = (g.khz * g.kny + g.khy) * g.knx + g.khx;
+    // Each warp walks a contiguous run of the bin's cells in snake order (x
+    // alternating direction per row, y per layer), so consecutive cells are
+    // unit steps apart and the k-th distance moves by at most the step norm.
+    const int run_len = (n_cells_bin + nwarps - 1) / nwarps;
+    const int c0 = warp * run_len, c1 = min(c0 + run_len, n_cells_bin);
     int kguess = -1;
-    for (int c = warp; c < n_cells_bin; c += nwarps)
+    bool have_h = false;
+    double h_prev = 0.0;
+    float path = 0.0f;
+    int n_exact = 0;
+    for (int c = c0; c < c1; ++c)
     {
-        const int cxr = c % wx, cyr = (c / wx) % wy, czr = c / (wx * wy);
+        if (c > c0) path += (c % wx) ? sd.step[0] : ((c / wx) % wy ? sd.step[1] : sd.step[2]);
+        const int row = c / wx;
+        int cxr = c - row * wx;
+        if (row & 1) cxr = wx - 1 - cxr;
+        const int czr = row / wy;
+        int cyr = row - czr * wy;
+        if (czr & 1) cyr = wy - 1 - cyr;
         const long long cell = ((long long)(z0 + czr) * g.ny + (y0 + cyr)) * g.nx + (x0 + cxr);
         if (!all_cells && mask[cell]) continue;
         const int klin_c = (czr * g.kny + cyr) * g.knx + cxr;
         const int plin_c = (czr * g.pny + cyr) * g.pnx + cxr;
-        const int n = select_fast<E>(g, C, cklin, cplin, cpid, cval, kc0, klin_c, plin_c, keytab16, keys, sel, lane,
-                                     kguess, nb_pid ? nb_pid + cell * k : nullptr, nb_rec ? nb_rec + cell * k : nullptr);
+        int *o_pid = nb_pid ? nb_pid + cell * k : nullptr;
+        int2 *o_rec = nb_rec ? nb_rec + cell * k : nullptr;
+        int n = -2;
+        double h = 0.0;
+        if (sd.on && have_h)
+        {
+            const double rt = sqrt(h_prev) + (double)path + 2.0 * sd.e3;
+            const float Tg = __double2float_ru(rt * rt * (1.0 + 1e-6));
+            const float4 tc = surr_coords(sd, cxr, cyr, czr);
+            n = select_surr<E>(g, sd, C, ctp, cklin, cplin, cpid, cval, kc0, klin_c, plin_c, keytab16, sel, lane,
+                               tc.x, tc.y, tc.z, Tg, h, kguess, o_pid, o_rec);
+        }
+        if (n == -2)
+        {
+            n = select_fast<E>(g, C, cklin, cplin, cpid, cval, kc0, klin_c, plin_c, keytab16, keys, sel, lane,
+                               kguess, o_pid, o_rec);
+            n_exact += sd.on;
+            h = (sd.on && kguess >= 0) ? sd.h2_rank[kguess] : 0.0;
+            have_h = sd.on && kguess >= 0 && n != 0;
+        }
+        else
+            have_h = n != 0;
+        h_prev = h;
+        path = 0.0f;
         if (lane == 0)
         {
             if (n < 0)
@@ -798,20 +941,21 @@ __global__ void __launch_bounds__(256) k_search_fast(
                 nb_n[cell] = n;
         }
     }
+    if (exact_cells && lane == 0 && n_exact) atomicAdd(exact_cells, n_exact);
 }
 
 size_t search_fast_smem_bytes(int cand_cap, int k, int warps)
 {
     const int E = k <= 32 ? 2 : 4;
-    return (size_t)cand_cap * 16 + (size_t)warps * ((size_t)cand_cap + 32 * E) * 4;
+    return (size_t)cand_cap * 32 + (size_t)warps * ((size_t)cand_cap + 32 * E) * 4;
 }
 
 cudaError_t launch_search_fast(const Geom &g, const uint8_t *mask, int all_cells, const int *bin_start,
                                const int *bin_cnt, const uint8_t *bin_flag, const int *bin_pts,
                                const unsigned long long *pts_xyz, const float *pts_vf, const uint16_t *keytab16,
-                               const int4 *tmpl, int n_tmpl, const int *pid_of_node, int cand_cap, int warps,
-                               int *nb_pid, int2 *nb_rec, int *nb_n, int *tie_cells, int *tie_count,
-                               int *n_template_cells, cudaStream_t st)
+                               const SurrDev &sd, const int4 *tmpl, int n_tmpl, const int *pid_of_node, int cand_cap,
+                               int warps, int *nb_pid, int2 *nb_rec, int *nb_n, int *tie_cells, int *tie_count,
+                               int *n_template_cells, int *exact_cells, cudaStream_t st)
 {
     size_t smem = search_fast_smem_bytes(cand_cap, g.k, warps);
     if (g.k <= 32)
@@ -819,18 +963,18 @@ cudaError_t launch_search_fast(const Geom &g, const uint8_t *mask, int all_cells
         cudaError_t e = cudaFuncSetAttribute(k_search_fast<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         k_search_fast<2><<<g.n_bins, warps * 32, smem, st>>>(g, mask, all_cells, bin_start, bin_cnt, bin_flag, bin_pts,
-                                                            pts_xyz, pts_vf, keytab16, tmpl, n_tmpl, pid_of_node,
+                                                            pts_xyz, pts_vf, keytab16, sd, tmpl, n_tmpl, pid_of_node,
                                                             cand_cap, nb_pid, nb_rec, nb_n, tie_cells, tie_count,
-                                                            n_template_cells);
+                                                            n_template_cells, exact_cells);
     }
     else
     {
         cudaError_t e = cudaFuncSetAttribute(k_search_fast<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         k_search_fast<4><<<g.n_bins, warps * 32, smem, st>>>(g, mask, all_cells, bin_start, bin_cnt, bin_flag, bin_pts,
-                                                            pts_xyz, pts_vf, keytab16, tmpl, n_tmpl, pid_of_node,
+                                                            pts_xyz, pts_vf, keytab16, sd, tmpl, n_tmpl, pid_of_node,
                                                             cand_cap, nb_pid, nb_rec, nb_n, tie_cells, tie_count,
-                                                            n_template_cells);
+                                                            n_template_cells, exact_cells);
     }
     return cudaGetLastError();
 }

@@ -72,6 +72,7 @@ FP64_PLAIN = 0
 FP32_REFINED = 1
 FLAG_DEVICE_POINTERS = 1
 FLAG_OUT_IS_CLONE = 2
+FLAG_EXACT_SEARCH = 4
 
 LIB_NAME = "libhpgl_b200.so"
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
@@ -173,7 +174,8 @@ STATS_KEYS = (["total_ms", "search_ms", "solve_ms", "tie_cells", "template_cells
               + [f"bucket_items_{i}" for i in range(5)] + [f"bucket_ms_{i}" for i in range(5)]
               + [f"bucket_flops_{i}" for i in range(5)]
               + ["stage_" + s + "_ms" for s in ("upload", "compact", "tables", "bins", "search", "ties", "prepare",
-                                              "solve", "finalize", "download")])
+                                              "solve", "finalize", "download")]
+              + ["prefilter_exact_cells", "prefilter_active"])
 
 
 def last_stats() -> dict:

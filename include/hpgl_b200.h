@@ -102,6 +102,8 @@ void hpgl_median_ik(struct hpgl_ind_masked_array_t *in_data, struct hpgl_median_
 /* flags */
 #define HPGL_B200_DEVICE_POINTERS 1u   /* data/mask/outputs are device pointers */
 #define HPGL_B200_OUT_IS_CLONE 2u      /* output arrays already hold a copy of the input */
+#define HPGL_B200_EXACT_SEARCH 4u      /* select neighbours by exact ranks only (no float
+                                          distance prefilter); same neighbours, slower */
 
 /* per-cell status codes (written to `status` when non-null) */
 #define HPGL_B200_CELL_INFORMED -1     /* conditioning cell, copied */
@@ -160,8 +162,11 @@ int hpgl_b200_find_neighbours(int kind, const int *dims, const unsigned char *ma
  *   [21..25] algorithmic flops per bucket, sum of F(n, r) =
  *            n^3/3 + n^2/2 + 2 r n^2 + 30 (n(n+1)/2 + n) + 2 r n (r = 2 OK, 1 SK)
  *   [26..35] ms per stage: upload, compaction, tables, binning, search, tie
- *            resolution, bucketing, solves, finalize, download */
-#define HPGL_B200_STATS_LEN 36
+ *            resolution, bucketing, solves, finalize, download
+ *   [36] cells whose neighbours the float distance prefilter could not
+ *        decide (selected by exact ranks over every candidate instead)
+ *   [37] 1 when the float distance prefilter was active in the last search */
+#define HPGL_B200_STATS_LEN 38
 int hpgl_b200_last_stats(double *out, int cap);
 
 /* No counterpart in the reference. The same SK weights as

@@ -13,7 +13,7 @@ def sk_params(cov, radiuses, k, mean=None):
                              mean=0.0 if mean is None else float(mean))
 
 
-def engine_cont(kind, wl, precision=0, refine_steps=2, mean=None, cov=None, radiuses=None, k=None):
+def engine_cont(kind, wl, precision=0, refine_steps=2, mean=None, cov=None, radiuses=None, k=None, flags=0):
     """Whole-grid OK (kind 0) / SK (kind 1) through hpgl_b200_cont_kriging_ex with host buffers."""
     cov = cov or wl.cov
     radiuses = radiuses or wl.radiuses
@@ -27,7 +27,7 @@ def engine_cont(kind, wl, precision=0, refine_steps=2, mean=None, cov=None, radi
     est = np.full(n, np.nan)
     var = np.full(n, np.nan)
     st = np.zeros(n, np.int8)
-    opt = W._HPGL_B200_OPTIONS(precision=precision, refine_steps=refine_steps, flags=W.FLAG_OUT_IS_CLONE,
+    opt = W._HPGL_B200_OPTIONS(precision=precision, refine_steps=refine_steps, flags=W.FLAG_OUT_IS_CLONE | flags,
                                stream=None, estimate64=est.ctypes.data, variance=var.ctypes.data,
                                status=st.ctypes.data, ik_probs=None)
     p = sk_params(cov, radiuses, k, mean)

@@ -167,6 +167,26 @@ def test_larger_grids_against_oracle(name, scale, kind):
     assert _sets_equal(idx, r["idx"])
 
 
+@pytest.mark.parametrize("name,scale,kind", [("sk_ok_large", 1.0, 0), ("sk_ok_large", 0.5, 1),
+                                             ("gauss_cv", 0.5, 0), ("clustered", 0.35, 1), ("ok_small", 1.0, 0)])
+def test_float_prefilter_selects_the_exact_neighbours(name, scale, kind):
+    """The float distance prefilter changes no neighbour set: FP64 estimates and variances
+    are bit-identical to a search by exact ranks over every candidate, at full size."""
+    wl = WL.ALL[name](scale)
+    a = H.engine_cont(kind, wl, precision=0)
+    b = H.engine_cont(kind, wl, precision=0, flags=W.FLAG_EXACT_SEARCH)
+    assert b["stats"]["prefilter_active"] == 0.0
+    np.testing.assert_array_equal(a["status"], b["status"])
+    np.testing.assert_array_equal(a["est"], b["est"])
+    np.testing.assert_array_equal(a["var"], b["var"])
+    np.testing.assert_array_equal(a["data"], b["data"])
+    assert a["stats"]["tie_cells"] == b["stats"]["tie_cells"]
+    if name == "sk_ok_large" and kind == 0:
+        # the benchmark model passes the host monotonicity check; most cells are decided in float
+        assert a["stats"]["prefilter_active"] == 1.0
+        assert a["stats"]["prefilter_exact_cells"] <= 0.25 * a["stats"]["kriged_cells"]
+
+
 def test_simple_kriging_weights_entry():
     rng = np.random.default_rng(4)
     for cov in (WL.CovSpec(WL.EXPONENTIAL, (10.0, 10.0, 10.0), (0.0, 0.0, 0.0), 1.0, 0.0),
