@@ -16,30 +16,37 @@
 // cov(c_i, c_j) = pair[centre + lin_i - lin_j] and cov(c_i, centre) =
 // pair[centre + lin_i]: assembly is one subtraction and one gather per entry.
 //
-// Factorisation: right-looking Cholesky. Step j: every thread stores its
-// current A[r][j] in row j of the group's shared matrix M (rows padded to 16
-// bytes), then reads row j back with 16-byte broadcast loads and updates
-// A[r][c] -= A[r][j] * M[j][c] / M[j][j] (c > j), and scales A[r][j] by
-// 1/sqrt(M[j][j]). Afterwards thread r holds row r of L in registers and row r
-// of M holds column r of L (times sqrt(M[r][r])), so both triangular solves
-// are one broadcast and one FMA per step.
+// Factorisation: right-looking Cholesky with the forward substitution fused in.
+// Step j: every thread stores its current A[r][j] in row j of the group's shared
+// matrix M and thread j appends its current right-hand sides; the row is read
+// back with 16-byte broadcast loads, and each thread r > j updates
+// A[r][c] -= A[r][j] * M[j][c] / M[j][j] (c > j) and rhs_r -= A[r][j] * rhs_j /
+// M[j][j]; thread j scales its row by 1/sqrt(M[j][j]) and keeps y_j = rhs_j /
+// sqrt(M[j][j]), the forward solution. Afterwards thread r holds row r of L in
+// registers and row r of M holds column r of L (times sqrt(M[r][r])), which the
+// back substitution reads with 16-byte loads of the thread's own row.
 //
 // Precision modes:
-//   FP64 plain   : T = double throughout.
-//   FP32 refined : A assembled from the float pair table, factored and solved
-//                  in float for b, (OK) the ones vector and the centred values
-//                  v - mean. The estimate and the variance are bilinear forms
-//                  u^T A^-1 w; each is corrected with one FP64 residual,
+//   FP64 plain   : T = double throughout. Every kriging quantity is a bilinear
+//                  form u^T A^-1 w = (L^-1 u) . (L^-1 w), so the forward
+//                  solutions of b, (OK) the ones vector and v - mean suffice:
+//                  no back substitution.
+//   FP32 refined : the matrix is gathered once from the double pair table and
+//                  kept in shared memory (packed lower triangle, groups of up to
+//                  32 threads; larger groups gather it again); its float
+//                  rounding is factored and solved in float for b, (OK) the
+//                  ones vector and the centred values v - mean. Each bilinear
+//                  form is corrected with one FP64 residual,
 //                    u^T A^-1 w = u^T x_w + x_u^T (w - A64 x_w) + O(|e_u| |e_w|),
-//                  (x_w = A32^-1 w), so one residual pass in double against the
-//                  double pair table gives quadratically small errors without a
-//                  second triangular solve. The relative size of the first-order
-//                  correction bounds what remains (its square); above `tol` the
-//                  group falls back to classic refinement x += A32^-1 (b - A64 x)
-//                  (up to `steps` rounds, each with an FP64 residual), and a
-//                  system that still does not converge, or whose float factor
-//                  breaks down, is queued for the FP64 kernel (status 4) instead
-//                  of being reported singular.
+//                  (x_w = A32^-1 w), so one residual pass in double gives
+//                  quadratically small errors without a second triangular solve.
+//                  The relative size of the first-order correction bounds what
+//                  remains (its square); above `tol` the group falls back to
+//                  classic refinement x += A32^-1 (b - A64 x) (up to `steps`
+//                  rounds, each with an FP64 residual), and a system that still
+//                  does not converge, or whose float factor breaks down, is
+//                  queued for the FP64 kernel (status 4) instead of being
+//                  reported singular.
 #include "engine.cuh"
 #include "kernels.h"
 
@@ -190,11 +197,16 @@ __device__ __forceinline__ void forward_solve(const Grp<NP> &g, const T (&row)[N
     if constexpr (NP > 32) g.sync(); // slots are reused by the next solve
 }
 
-// Back substitution L^T x = y; row r of M holds column r of L times sqrt(M[r][r]).
+// Back substitution L^T x = y; row r of M holds column r of L times
+// sqrt(M[r][r]). Thread r reads its own row four (float) or two (double)
+// entries at a time; with rows NP + V entries apart the 16-byte loads of eight
+// consecutive threads fall on distinct bank groups.
 template <int NP, typename T, int R, int LD>
 __device__ __forceinline__ void back_solve(const Grp<NP> &g, const T *M, T (&yv)[R], T my_inv, T *slots,
                                            T (&x)[R])
 {
+    typedef typename Vec<T>::type VT;
+    constexpr int V = Vec<T>::n;
     T acc[R];
 #pragma unroll
     for (int q = 0; q < R; ++q)
@@ -202,10 +214,12 @@ __device__ __forceinline__ void back_solve(const Grp<NP> &g, const T *M, T (&yv)
         acc[q] = yv[q];
         x[q] = 0;
     }
-    const T *Mr = M + g.r * LD;
+    const VT *Mr = reinterpret_cast<const VT *>(M + g.r * LD);
+    T mc[V];
 #pragma unroll
     for (int i = NP - 1; i >= 0; --i)
     {
+        if (i % V == V - 1) Vec<T>::unpack(Mr[i / V], mc);
         if (g.r == i)
         {
 #pragma unroll
@@ -216,7 +230,7 @@ __device__ __forceinline__ void back_solve(const Grp<NP> &g, const T *M, T (&yv)
         for (int q = 0; q < R; ++q) xi[q] = group_bcast<NP, T>(g, x[q], i, slots + (NP <= 32 ? 0 : (q * NP + i)));
         if (g.r < i)
         {
-            const T l = Mr[i] * my_inv;
+            const T l = mc[i % V] * my_inv;
 #pragma unroll
             for (int q = 0; q < R; ++q) acc[q] -= l * xi[q];
         }
@@ -224,17 +238,21 @@ __device__ __forceinline__ void back_solve(const Grp<NP> &g, const T *M, T (&yv)
     if constexpr (NP > 32) g.sync();
 }
 
-template <int NP, typename TF>
+// Per-group shared memory of k_solve. M: NP rows of NP matrix entries plus RP
+// right-hand side slots (R padded to 16 bytes).
+template <int NP, typename TF, bool REFINE, int R>
 struct SolveSmem
 {
     static constexpr int V = 16 / (int)sizeof(TF);
-    static constexpr int LD = NP + V;
-    // M (NP x LD of TF), LIN (NP int), X (2 NP double), slots (3 NP TF), scratch (4 double)
+    static constexpr int RP = (R + V - 1) / V * V;
+    static constexpr int LD = NP + RP;
     static constexpr size_t m_bytes = (size_t)NP * LD * sizeof(TF);
-    static constexpr size_t lin_off = m_bytes;
+    static constexpr size_t lin_off = (m_bytes + 15) / 16 * 16;
     static constexpr size_t x_off = (lin_off + NP * sizeof(int) + 15) / 16 * 16;
-    static constexpr size_t slot_off = x_off + 2 * NP * sizeof(double);
-    static constexpr size_t scr_off = (slot_off + 3 * NP * sizeof(TF) + 15) / 16 * 16;
+    static constexpr size_t x_bytes = REFINE ? 2 * NP * sizeof(double) : 0;
+    static constexpr size_t slot_off = x_off + x_bytes;
+    static constexpr size_t slot_bytes = NP > 32 ? 3 * NP * sizeof(TF) : 0;
+    static constexpr size_t scr_off = (slot_off + slot_bytes + 15) / 16 * 16;
     static constexpr size_t bytes = (scr_off + 4 * sizeof(double) + 15) / 16 * 16;
 };
 
@@ -272,30 +290,303 @@ __device__ __forceinline__ void residuals_fp64(const Grp<NP> &grp, const double 
     grp.sync();
 }
 
-// Minimum resident 256-thread blocks per SM requested for the FP32 kernels
-// (caps their registers at 65536 / (256 * blocks)).
-#ifndef HB_SOLVE_MIN_BLOCKS_F32
-#define HB_SOLVE_MIN_BLOCKS_F32 3
-#endif
-
-template <int NP, typename TF, bool ORDINARY, bool REFINE>
-__global__ void __launch_bounds__(256, sizeof(TF) == 4 ? HB_SOLVE_MIN_BLOCKS_F32 : 1) k_solve(const Geom g, const int2 *__restrict__ cells,
-                                               const int *__restrict__ n_items_ptr, const int2 *__restrict__ nb_rec,
-                                               const int *__restrict__ nb_n, int ind_value,
-                                               const double *__restrict__ pair64, const float *__restrict__ pair32,
-                                               double mean, double c0, int steps, double tol, SolveOut out,
-                                               int2 *__restrict__ esc_cells, int *__restrict__ esc_count)
+// Per-group view of the shared memory and the launch-wide parameters.
+template <int NP, typename TF>
+struct GroupMem
 {
-    typedef SolveSmem<NP, TF> SM;
-    constexpr int LD = SM::LD;
-    constexpr int V = SM::V;
-    // right-hand sides: b, (OK) the ones vector, and the centred values v - mean
+    TF *M;
+    int *LIN;
+    double *X;
+    TF *slots;
+    double *scr;
+};
+
+struct SolveParams
+{
+    const double *pair64;
+    long long pc;
+    float mf;
+    double c0;
+    int steps;
+    double tol;
+    SolveOut out;
+    int2 *esc_cells;
+    int *esc_count;
+};
+
+// Factorisation, solves, FP64 correction and outputs of one system whose
+// (float or double) matrix row r is in `row` (lower triangle, padding rows
+// identity) and whose b_r is b64.
+template <int NP, typename TF, bool ORDINARY, bool REFINE>
+__device__ __forceinline__ void solve_one(const Grp<NP> &grp, const GroupMem<NP, TF> &gm, const SolveParams &P,
+                                          TF (&row)[NP], double b64, double vc, bool live, int lin, int my_cell,
+                                          int my_n)
+{
     constexpr int QB = ORDINARY ? 2 : 1; // b and 1: the systems the weights come from
     constexpr int R = QB + 1;            // plus v: the adjoint system of the estimate
+    typedef SolveSmem<NP, TF, REFINE, R> SM;
+    constexpr int LD = SM::LD;
+    constexpr int V = SM::V;
     typedef typename Vec<TF>::type VT;
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int groups_per_block = blockDim.x / NP;
-    const int gi = threadIdx.x / NP;
+    const int r = grp.r;
+    TF *M = gm.M;
+    double *scr = gm.scr;
+
+    // ---- factorisation with the forward substitution of b, 1 and v - mean
+    TF rhs[R], yv[R];
+    rhs[0] = live ? (TF)b64 : (TF)0;
+    if constexpr (ORDINARY) rhs[1] = live ? (TF)1 : (TF)0;
+    rhs[R - 1] = (TF)vc;
+#pragma unroll
+    for (int q = 0; q < R; ++q) yv[q] = (TF)0;
+    bool fail = false;
+    TF my_inv = 0;
+#pragma unroll
+    for (int j = 0; j < NP; ++j)
+    {
+        M[j * LD + r] = row[j];
+        if (r == j)
+        {
+#pragma unroll
+            for (int q = 0; q < R; ++q) M[j * LD + NP + q] = rhs[q];
+        }
+        grp.sync();
+        TF mj[LD];
+        const VT *mv = reinterpret_cast<const VT *>(M + j * LD);
+#pragma unroll
+        for (int q = j / V; q < LD / V; ++q) Vec<TF>::unpack(mv[q], mj + q * V);
+        const TF d = mj[j];
+        fail |= !(d > (TF)0);
+        const TF inv_s = rsqrt_t<TF>(d);
+        const TF s = row[j] * (inv_s * inv_s);
+#pragma unroll
+        for (int c = j + 1; c < NP; ++c) row[c] -= s * mj[c];
+        if (r > j)
+        {
+#pragma unroll
+            for (int q = 0; q < R; ++q) rhs[q] -= s * mj[NP + q];
+        }
+        row[j] *= inv_s;
+        if (r == j)
+        {
+            my_inv = inv_s;
+#pragma unroll
+            for (int q = 0; q < R; ++q) yv[q] = rhs[q] * inv_s;
+        }
+    }
+    const double one = live ? 1.0 : 0.0;
+
+    // Bilinear forms u^T A^-1 w of the estimate and variance.
+    double f_vb, f_bb, f_1b = 0.0, f_v1 = 0.0, f_11 = 0.0;
+    bool escalate = false;
+    double x[R];
+    double corr_vb = 0.0, corr_bb = 0.0;
+    if constexpr (!REFINE)
+    {
+        // (L^-1 u) . (L^-1 w): the forward solutions are all that is needed
+        const double yb = (double)yv[0], yvv = (double)yv[R - 1];
+        f_vb = yvv * yb;
+        f_bb = yb * yb;
+        if constexpr (ORDINARY)
+        {
+            const double y1 = (double)yv[1];
+            f_1b = y1 * yb;
+            f_v1 = yvv * y1;
+            f_11 = y1 * y1;
+        }
+    }
+    else
+    {
+        TF xs[R];
+        back_solve<NP, TF, R, LD>(grp, M, yv, my_inv, gm.slots, xs);
+#pragma unroll
+        for (int q = 0; q < R; ++q) x[q] = (double)xs[q];
+        // With FP32 solutions each form gets the dual-weighted residual correction
+        //   u^T A^-1 w = u^T x_w + x_u^T (w - A64 x_w) + O(|e_u| |e_w|),
+        // x_w = A32^-1 w, x_u = A32^-1 u, the residual in FP64.
+        f_vb = vc * x[0];
+        f_bb = b64 * x[0];
+        if constexpr (ORDINARY)
+        {
+            f_1b = one * x[0];
+            f_v1 = vc * x[1];
+            f_11 = one * x[1];
+        }
+        escalate = fail;
+        double rhs64[QB], res[QB];
+        rhs64[0] = b64;
+        if constexpr (ORDINARY) rhs64[1] = one;
+        residuals_fp64<NP, QB, R>(grp, P.pair64, P.pc, lin, gm.LIN, gm.X, my_n, live, x, rhs64, res);
+        corr_vb = x[R - 1] * res[0];
+        corr_bb = x[0] * res[0];
+        f_vb += corr_vb;
+        f_bb += corr_bb;
+        if constexpr (ORDINARY)
+        {
+            f_1b += x[1] * res[0];
+            f_v1 += x[R - 1] * res[1];
+            f_11 += x[1] * res[1];
+        }
+    }
+    double s_vb = group_sum<NP, double>(grp, f_vb, scr);
+    double s_bb = group_sum<NP, double>(grp, f_bb, scr);
+    double s_1b = 0.0, s_v1 = 0.0, s_11 = 0.0;
+    if constexpr (ORDINARY)
+    {
+        s_1b = group_sum<NP, double>(grp, f_1b, scr);
+        s_v1 = group_sum<NP, double>(grp, f_v1, scr);
+        s_11 = group_sum<NP, double>(grp, f_11, scr);
+    }
+    if constexpr (REFINE)
+    {
+        // a-posteriori check: the first-order correction of each form relative
+        // to the form's scale; what remains after it is about its square
+        const double abs_vb = group_sum<NP, double>(grp, fabs(vc * x[0]), scr) + 1e-300;
+        const double abs_bb = group_sum<NP, double>(grp, fabs(b64 * x[0]), scr) + 1e-300;
+        const double c1 = fabs(group_sum<NP, double>(grp, corr_vb, scr)) / abs_vb;
+        const double c2 = fabs(group_sum<NP, double>(grp, corr_bb, scr)) / abs_bb;
+        const double d = fmax(c1, c2);
+        if (!(d * d <= P.tol)) escalate = true;
+        if (!(s_vb == s_vb) || !(s_bb == s_bb)) escalate = true;
+        if (escalate && P.steps > 0 && !fail)
+        {
+            // classic refinement of x (and y): x += A32^-1 (b - A64 x) until the
+            // correction stops mattering, then the forms without correction
+            double prev = 0.0;
+            bool done = false;
+            for (int it = 0; it < P.steps && !done; ++it)
+            {
+                double rq[QB], rr64[QB], xq[QB];
+#pragma unroll
+                for (int q = 0; q < QB; ++q)
+                {
+                    rq[q] = q == 0 ? b64 : one;
+                    xq[q] = x[q];
+                }
+                residuals_fp64<NP, QB, QB>(grp, P.pair64, P.pc, lin, gm.LIN, gm.X, my_n, live, xq, rq, rr64);
+                TF rr[QB], yy[QB], dd[QB];
+#pragma unroll
+                for (int q = 0; q < QB; ++q) rr[q] = (TF)rr64[q];
+                forward_solve<NP, TF, QB>(grp, row, rr, my_inv, gm.slots, yy);
+                back_solve<NP, TF, QB, LD>(grp, M, yy, my_inv, gm.slots, dd);
+                double dmax = 0.0, xmax = 0.0;
+#pragma unroll
+                for (int q = 0; q < QB; ++q)
+                {
+                    x[q] += (double)dd[q];
+                    dmax = fmax(dmax, fabs((double)dd[q]));
+                    xmax = fmax(xmax, fabs(x[q]));
+                }
+                dmax = group_max<NP, double>(grp, dmax, scr);
+                xmax = group_max<NP, double>(grp, xmax, scr);
+                const double delta = xmax > 0.0 ? dmax / xmax : 0.0;
+                double err;
+                if (it == 0)
+                    err = delta * delta;
+                else
+                {
+                    const double rho = prev > 0.0 ? delta / prev : 0.0;
+                    err = rho < 0.5 ? delta * rho / (1.0 - rho) : 1.0;
+                }
+                if (!(delta == delta)) err = 1.0;
+                prev = delta;
+                done = err <= P.tol;
+            }
+            if (done)
+            {
+                escalate = false;
+                s_vb = group_sum<NP, double>(grp, vc * x[0], scr);
+                s_bb = group_sum<NP, double>(grp, b64 * x[0], scr);
+                if constexpr (ORDINARY)
+                {
+                    s_1b = group_sum<NP, double>(grp, one * x[0], scr);
+                    s_v1 = group_sum<NP, double>(grp, vc * x[1], scr);
+                    s_11 = group_sum<NP, double>(grp, one * x[1], scr);
+                }
+            }
+        }
+    }
+
+    if (escalate)
+    {
+        if (r == 0)
+        {
+            int slot = atomicAdd(P.esc_count, 1);
+            P.esc_cells[slot] = make_int2(my_cell, my_n);
+            if (P.out.status) P.out.status[my_cell] = 4;
+        }
+        grp.sync();
+        return;
+    }
+
+    // ---- estimate and variance from the forms
+    //   SK: est = mean + (v-m)^T A^-1 b,        var = C0 - b^T A^-1 b
+    //   OK: mu = (1^T A^-1 b - 1) / 1^T A^-1 1,  est = v^T A^-1 b - mu v^T A^-1 1,
+    //       var = C0 - b^T A^-1 b + mu 1^T A^-1 b - mu   (my_kriging_weights.h:312-357)
+    double est, var;
+    if constexpr (ORDINARY)
+    {
+        if (fabs(s_11) < 1e-15) fail = true;
+        const double mu = (s_1b - 1.0) / s_11;
+        est = s_vb - mu * s_v1;
+        var = P.c0 - s_bb + mu * s_1b - mu;
+    }
+    else
+    {
+        est = (double)P.mf + s_vb;
+        var = P.c0 - s_bb;
+    }
+    if (var < 0) var = 0;
+    if (r == 0)
+    {
+        const SolveOut &out = P.out;
+        if (!fail)
+        {
+            if (out.write_cont)
+            {
+                out.out_data[my_cell] = (float)est;
+                out.out_mask[my_cell] = 1;
+            }
+            if (out.prob) out.prob[(long long)my_cell * out.prob_stride] = (float)est;
+            if (out.est64) out.est64[my_cell] = est;
+            if (out.var) out.var[my_cell] = var;
+            if (out.status) out.status[my_cell] = 0;
+        }
+        else if (out.status)
+            out.status[my_cell] = 2;
+    }
+    grp.sync();
+}
+
+// Work items are {cell, n}, listed in ascending cell order. Each block takes a
+// contiguous run of them and its groups interleave inside it, so the systems a
+// block has in flight belong to neighbouring cells, which share most of their
+// neighbour pairs: their pair-table gathers hit the same lines.
+struct WorkRun
+{
+    int first, end, stride;
+};
+__device__ __forceinline__ WorkRun work_run(int n_items, int groups_per_block, int gi)
+{
+    const int per_block = (n_items + gridDim.x - 1) / gridDim.x;
+    WorkRun w;
+    w.first = blockIdx.x * per_block + gi;
+    w.end = min(n_items, (blockIdx.x + 1) * per_block);
+    w.stride = groups_per_block;
+    return w;
+}
+
+// neighbour value centred on the (float) mean as combine() does (combiner.h:19-24)
+__device__ __forceinline__ double centred_value(bool live, float vraw, int ind_value, float mf)
+{
+    float v = 0.0f;
+    if (live) v = ind_value >= 0 ? (vraw == (float)ind_value ? 1.0f : 0.0f) : vraw;
+    return live ? (double)(v - mf) : 0.0;
+}
+
+template <int NP>
+__device__ __forceinline__ Grp<NP> make_group(int gi)
+{
     Grp<NP> grp;
     grp.r = threadIdx.x % NP;
     if constexpr (NP <= 32)
@@ -306,40 +597,50 @@ __global__ void __launch_bounds__(256, sizeof(TF) == 4 ? HB_SOLVE_MIN_BLOCKS_F32
     else
         grp.mask = 0xffffffffu;
     grp.bar = 1 + gi;
+    return grp;
+}
+
+// One system per group of NP threads, thread r owning row r (the FP64 kernel
+// and FP32-refined systems of 33 to 64 neighbours).
+template <int NP, typename TF, bool ORDINARY, bool REFINE>
+__global__ void __launch_bounds__(256, 1)
+    k_solve(const Geom g, const int2 *__restrict__ cells, const int *__restrict__ n_items_ptr,
+            const int2 *__restrict__ nb_rec, int ind_value, const float *__restrict__ pair32, SolveParams P)
+{
+    constexpr int R = (ORDINARY ? 2 : 1) + 1;
+    typedef SolveSmem<NP, TF, REFINE, R> SM;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int groups_per_block = blockDim.x / NP;
+    const int gi = threadIdx.x / NP;
+    const Grp<NP> grp = make_group<NP>(gi);
     const int r = grp.r;
-
     unsigned char *gb = smem + SM::bytes * gi;
-    TF *M = reinterpret_cast<TF *>(gb);
-    int *LIN = reinterpret_cast<int *>(gb + SM::lin_off);
-    double *X = reinterpret_cast<double *>(gb + SM::x_off);
-    TF *slots = reinterpret_cast<TF *>(gb + SM::slot_off);
-    double *scr = reinterpret_cast<double *>(gb + SM::scr_off);
+    GroupMem<NP, TF> gm;
+    gm.M = reinterpret_cast<TF *>(gb);
+    gm.LIN = reinterpret_cast<int *>(gb + SM::lin_off);
+    gm.X = reinterpret_cast<double *>(gb + SM::x_off);
+    gm.slots = reinterpret_cast<TF *>(gb + SM::slot_off);
+    gm.scr = reinterpret_cast<double *>(gb + SM::scr_off);
+    const long long pc = P.pc;
 
-    const int n_items = *n_items_ptr;
-    const long long pc = g.pair_center;
-    const int stride = gridDim.x * groups_per_block;
-    const float mf = (float)mean; // mean_t is float (typedefs.h:122)
-    // Work items are {cell, n}. The record of item i+1 and the work entry of
-    // item i+2 are loaded while item i is solved, so no load the solve waits on
-    // depends on another load issued in the same iteration.
-    int item = blockIdx.x * groups_per_block + gi;
-    int2 w_cur = item < n_items ? cells[item] : make_int2(0, 0);
-    int2 w_nxt = item + stride < n_items ? cells[item + stride] : make_int2(0, 0);
-    int2 rec = (item < n_items && r < w_cur.y) ? nb_rec[(long long)w_cur.x * g.k + r] : make_int2(0, 0);
-    for (; item < n_items; item += stride)
+    // The record of item i+1 and the work entry of item i+2 are loaded while
+    // item i is solved.
+    const WorkRun wr = work_run(*n_items_ptr, groups_per_block, gi);
+    const int stride = wr.stride, run_end = wr.end;
+    int item = wr.first;
+    int2 w_cur = item < run_end ? cells[item] : make_int2(0, 0);
+    int2 w_nxt = item + stride < run_end ? cells[item + stride] : make_int2(0, 0);
+    int2 rec = (item < run_end && r < w_cur.y) ? nb_rec[(long long)w_cur.x * g.k + r] : make_int2(0, 0);
+    for (; item < run_end; item += stride)
     {
         const int my_cell = w_cur.x, my_n = w_cur.y;
         const int lin = rec.x;
         const bool live = r < my_n;
-        const float vraw = __int_as_float(rec.y);
-        rec = (item + stride < n_items && r < w_nxt.y) ? nb_rec[(long long)w_nxt.x * g.k + r] : make_int2(0, 0);
+        const double vc = centred_value(live, __int_as_float(rec.y), ind_value, P.mf);
+        rec = (item + stride < run_end && r < w_nxt.y) ? nb_rec[(long long)w_nxt.x * g.k + r] : make_int2(0, 0);
         w_cur = w_nxt;
-        w_nxt = item + 2 * stride < n_items ? cells[item + 2 * stride] : make_int2(0, 0);
-        // neighbour value centred on the (float) mean as combine() does (combiner.h:19-24)
-        float v = 0.0f;
-        if (live) v = ind_value >= 0 ? (vraw == (float)ind_value ? 1.0f : 0.0f) : vraw;
-        const double vc = live ? (double)(v - mf) : 0.0;
-        LIN[r] = live ? lin : 0;
+        w_nxt = item + 2 * stride < run_end ? cells[item + 2 * stride] : make_int2(0, 0);
+        gm.LIN[r] = live ? lin : 0;
         grp.sync();
 
         // ---- assembly (lower triangle of row r; padding rows are identity)
@@ -348,218 +649,567 @@ __global__ void __launch_bounds__(256, sizeof(TF) == 4 ? HB_SOLVE_MIN_BLOCKS_F32
         for (int c = 0; c < NP; ++c)
         {
             TF a = (TF)0;
-            if (live && c <= r) a = pair_get<TF>(pair32, pair64, pc + lin - LIN[c]);
+            if (live && c <= r) a = pair_get<TF>(pair32, P.pair64, pc + lin - gm.LIN[c]);
             if (!live && c == r) a = (TF)1;
             row[c] = a;
         }
-        const double b64 = live ? __ldg(pair64 + pc + lin) : 0.0;
-
-        // ---- factorisation
-        bool fail = false;
-        TF my_inv = 0;
-#pragma unroll
-        for (int j = 0; j < NP; ++j)
-        {
-            M[j * LD + r] = row[j];
-            grp.sync();
-            TF mj[NP + V];
-            const VT *mv = reinterpret_cast<const VT *>(M + j * LD);
-#pragma unroll
-            for (int q = j / V; q < NP / V; ++q) Vec<TF>::unpack(mv[q], mj + q * V);
-            const TF d = mj[j];
-            fail |= !(d > (TF)0);
-            const TF inv_s = rsqrt_t<TF>(d);
-            const TF s = row[j] * (inv_s * inv_s);
-#pragma unroll
-            for (int c = j + 1; c < NP; ++c) row[c] -= s * mj[c];
-            row[j] *= inv_s;
-            if (r == j) my_inv = inv_s;
-        }
-
-        // ---- solves: x = A^-1 b, (OK) y = A^-1 1, and lambda = A^-1 (v - mean)
-        TF rhs[R], ytmp[R], xs[R];
-        rhs[0] = live ? (TF)b64 : (TF)0;
-        if constexpr (ORDINARY) rhs[1] = live ? (TF)1 : (TF)0;
-        rhs[R - 1] = (TF)vc;
-        forward_solve<NP, TF, R>(grp, row, rhs, my_inv, slots, ytmp);
-        back_solve<NP, TF, R, LD>(grp, M, ytmp, my_inv, slots, xs);
-        double x[R];
-#pragma unroll
-        for (int q = 0; q < R; ++q) x[q] = (double)xs[q];
-        const double one = live ? 1.0 : 0.0;
-
-        // Bilinear forms u^T A^-1 w of the estimate and variance. With FP32
-        // solutions each form gets the dual-weighted residual correction
-        //   u^T A^-1 w = u^T x_w + x_u^T (w - A64 x_w) + O(|e_u| |e_w|),
-        // x_w = A32^-1 w, x_u = A32^-1 u, the residual in FP64: one residual
-        // pass gives quadratically accurate forms without another solve.
-        double f_vb = vc * x[0], f_bb = b64 * x[0], f_1b = 0.0, f_v1 = 0.0, f_11 = 0.0;
-        if constexpr (ORDINARY)
-        {
-            f_1b = one * x[0];
-            f_v1 = vc * x[1];
-            f_11 = one * x[1];
-        }
-        bool escalate = false;
-        double corr_vb = 0.0, corr_bb = 0.0;
-        if constexpr (REFINE)
-        {
-            escalate = fail;
-            double rhs64[QB], res[QB];
-            rhs64[0] = b64;
-            if constexpr (ORDINARY) rhs64[1] = one;
-            residuals_fp64<NP, QB, R>(grp, pair64, pc, lin, LIN, X, my_n, live, x, rhs64, res);
-            corr_vb = x[R - 1] * res[0];
-            corr_bb = x[0] * res[0];
-            f_vb += corr_vb;
-            f_bb += corr_bb;
-            if constexpr (ORDINARY)
-            {
-                f_1b += x[1] * res[0];
-                f_v1 += x[R - 1] * res[1];
-                f_11 += x[1] * res[1];
-            }
-        }
-        double s_vb = group_sum<NP, double>(grp, f_vb, scr);
-        double s_bb = group_sum<NP, double>(grp, f_bb, scr);
-        double s_1b = 0.0, s_v1 = 0.0, s_11 = 0.0;
-        if constexpr (ORDINARY)
-        {
-            s_1b = group_sum<NP, double>(grp, f_1b, scr);
-            s_v1 = group_sum<NP, double>(grp, f_v1, scr);
-            s_11 = group_sum<NP, double>(grp, f_11, scr);
-        }
-        if constexpr (REFINE)
-        {
-            // a-posteriori check: the first-order correction of each form relative
-            // to the form's scale; what remains after it is about its square
-            const double abs_vb = group_sum<NP, double>(grp, fabs(vc * x[0]), scr) + 1e-300;
-            const double abs_bb = group_sum<NP, double>(grp, fabs(b64 * x[0]), scr) + 1e-300;
-            const double c1 = fabs(group_sum<NP, double>(grp, corr_vb, scr)) / abs_vb;
-            const double c2 = fabs(group_sum<NP, double>(grp, corr_bb, scr)) / abs_bb;
-            const double d = fmax(c1, c2);
-            if (!(d * d <= tol)) escalate = true;
-            if (!(s_vb == s_vb) || !(s_bb == s_bb)) escalate = true;
-            if (escalate && steps > 0 && !fail)
-            {
-                // classic refinement of x (and y): x += A32^-1 (b - A64 x) until the
-                // correction stops mattering, then the forms without correction
-                double prev = 0.0;
-                bool done = false;
-                for (int it = 0; it < steps && !done; ++it)
-                {
-                    double rq[QB], rr64[QB], xq[QB];
-#pragma unroll
-                    for (int q = 0; q < QB; ++q)
-                    {
-                        rq[q] = q == 0 ? b64 : one;
-                        xq[q] = x[q];
-                    }
-                    residuals_fp64<NP, QB, QB>(grp, pair64, pc, lin, LIN, X, my_n, live, xq, rq, rr64);
-                    TF rr[QB], yy[QB], dd[QB];
-#pragma unroll
-                    for (int q = 0; q < QB; ++q) rr[q] = (TF)rr64[q];
-                    forward_solve<NP, TF, QB>(grp, row, rr, my_inv, slots, yy);
-                    back_solve<NP, TF, QB, LD>(grp, M, yy, my_inv, slots, dd);
-                    double dmax = 0.0, xmax = 0.0;
-#pragma unroll
-                    for (int q = 0; q < QB; ++q)
-                    {
-                        x[q] += (double)dd[q];
-                        dmax = fmax(dmax, fabs((double)dd[q]));
-                        xmax = fmax(xmax, fabs(x[q]));
-                    }
-                    dmax = group_max<NP, double>(grp, dmax, scr);
-                    xmax = group_max<NP, double>(grp, xmax, scr);
-                    const double delta = xmax > 0.0 ? dmax / xmax : 0.0;
-                    double err;
-                    if (it == 0)
-                        err = delta * delta;
-                    else
-                    {
-                        const double rho = prev > 0.0 ? delta / prev : 0.0;
-                        err = rho < 0.5 ? delta * rho / (1.0 - rho) : 1.0;
-                    }
-                    if (!(delta == delta)) err = 1.0;
-                    prev = delta;
-                    done = err <= tol;
-                }
-                if (done)
-                {
-                    escalate = false;
-                    s_vb = group_sum<NP, double>(grp, vc * x[0], scr);
-                    s_bb = group_sum<NP, double>(grp, b64 * x[0], scr);
-                    if constexpr (ORDINARY)
-                    {
-                        s_1b = group_sum<NP, double>(grp, one * x[0], scr);
-                        s_v1 = group_sum<NP, double>(grp, vc * x[1], scr);
-                        s_11 = group_sum<NP, double>(grp, one * x[1], scr);
-                    }
-                }
-            }
-        }
-
-        if (escalate)
-        {
-            if (r == 0)
-            {
-                int slot = atomicAdd(esc_count, 1);
-                esc_cells[slot] = make_int2(my_cell, my_n);
-                if (out.status) out.status[my_cell] = 4;
-            }
-            grp.sync();
-            continue;
-        }
-
-        // ---- estimate and variance from the forms
-        //   SK: est = mean + (v-m)^T A^-1 b,        var = C0 - b^T A^-1 b
-        //   OK: mu = (1^T A^-1 b - 1) / 1^T A^-1 1,  est = v^T A^-1 b - mu v^T A^-1 1,
-        //       var = C0 - b^T A^-1 b + mu 1^T A^-1 b - mu   (my_kriging_weights.h:312-357)
-        double est, var;
-        if constexpr (ORDINARY)
-        {
-            if (fabs(s_11) < 1e-15) fail = true;
-            const double mu = (s_1b - 1.0) / s_11;
-            est = s_vb - mu * s_v1;
-            var = c0 - s_bb + mu * s_1b - mu;
-        }
-        else
-        {
-            est = (double)mf + s_vb;
-            var = c0 - s_bb;
-        }
-        if (var < 0) var = 0;
-        if (r == 0)
-        {
-            if (!fail)
-            {
-                if (out.write_cont)
-                {
-                    out.out_data[my_cell] = (float)est;
-                    out.out_mask[my_cell] = 1;
-                }
-                if (out.prob) out.prob[(long long)my_cell * out.prob_stride] = (float)est;
-                if (out.est64) out.est64[my_cell] = est;
-                if (out.var) out.var[my_cell] = var;
-                if (out.status) out.status[my_cell] = 0;
-            }
-            else if (out.status)
-                out.status[my_cell] = 2;
-        }
-        grp.sync();
+        const double b64 = live ? __ldg(P.pair64 + pc + lin) : 0.0;
+        solve_one<NP, TF, ORDINARY, REFINE>(grp, gm, P, row, b64, vc, live, lin, my_cell, my_n);
     }
 }
 
-template <int NP, typename TF, bool ORD, bool REF>
-static cudaError_t launch_one(const Geom &g, const int2 *cells, const int *n_items, int max_items, const int2 *nb_rec,
-                              const int *nb_n, int ind_value, const double *pair64, const float *pair32, double mean,
-                              double c0, int steps, double tol, const SolveOut &out, int2 *esc_cells, int *esc_count,
-                              int n_sm, cudaStream_t st)
+// ------------------------------------------------------------------ folded
+// FP32-refined systems of up to 32 neighbours, folded: a system is solved by
+// G = NP / 2 lanes and lane t owns rows t ("row a", columns 0..t) and
+// NP - 1 - t ("row b", columns 0..NP-1-t), so every lane holds NP + 1 entries
+// of the lower triangle and a warp solves 32 / G systems at once. Each step of
+// the factorisation updates row a over columns j+1..G-1 and row b over
+// j+1..NP-1: about 5/8 of the multiply-adds of one row per lane, with the
+// shared-memory broadcast, the rsqrt and the synchronisation of a step serving
+// two rows. The arithmetic (right-looking Cholesky with the forward
+// substitution fused in, FP32 back substitution, dual-weighted FP64 residual
+// correction, classic refinement and FP64 escalation) is that of solve_one.
+template <int NP, int R>
+struct FoldSmem
+{
+    static constexpr int LD = NP + 4; // NP entries, then up to 4 right-hand sides
+    static constexpr size_t m_bytes = (size_t)NP * LD * sizeof(float);
+    static constexpr size_t lin_off = m_bytes;
+    static constexpr size_t x_off = (lin_off + NP * sizeof(int) + 15) / 16 * 16;
+    static constexpr size_t bytes = x_off + 2 * NP * sizeof(double);
+};
+
+template <int G>
+struct FoldGrp
+{
+    unsigned mask; // the system's lanes
+    __device__ __forceinline__ void sync() const { __syncwarp(mask); }
+    template <typename T>
+    __device__ __forceinline__ T bcast(T v, int src) const
+    {
+        return __shfl_sync(mask, v, src, G);
+    }
+    template <typename T>
+    __device__ __forceinline__ T sum(T v) const
+    {
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, G);
+        return v;
+    }
+    template <typename T>
+    __device__ __forceinline__ T max(T v) const
+    {
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(mask, v, o, G));
+        return v;
+    }
+};
+
+// Back substitution L^T x = y for both rows of the lane; row r of M holds
+// column r of L times sqrt(d_r), read with 16-byte loads of the lane's rows.
+template <int NP, int Q>
+__device__ __forceinline__ void fold_back(const FoldGrp<NP / 2> &fg, const float *M, int t, const float (&ya)[Q],
+                                          const float (&yb)[Q], float inv_a, float inv_b, float (&xa)[Q],
+                                          float (&xb)[Q])
+{
+    constexpr int G = NP / 2, LD = FoldSmem<NP, 3>::LD;
+    const int rb = NP - 1 - t;
+    float acc_a[Q], acc_b[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+    {
+        acc_a[q] = ya[q];
+        acc_b[q] = yb[q];
+        xa[q] = 0.0f;
+        xb[q] = 0.0f;
+    }
+    const float4 *Ma = reinterpret_cast<const float4 *>(M + t * LD);
+    const float4 *Mb = reinterpret_cast<const float4 *>(M + rb * LD);
+    float4 ma = make_float4(0, 0, 0, 0), mb = ma;
+#pragma unroll
+    for (int i = NP - 1; i >= 0; --i)
+    {
+        if (i % 4 == 3)
+        {
+            ma = Ma[i / 4];
+            mb = Mb[i / 4];
+        }
+        const float ea = (i % 4 == 0) ? ma.x : (i % 4 == 1) ? ma.y : (i % 4 == 2) ? ma.z : ma.w;
+        const float eb = (i % 4 == 0) ? mb.x : (i % 4 == 1) ? mb.y : (i % 4 == 2) ? mb.z : mb.w;
+        float xi[Q];
+        if (i < G)
+        {
+            if (t == i)
+            {
+#pragma unroll
+                for (int q = 0; q < Q; ++q) xa[q] = acc_a[q] * inv_a;
+            }
+#pragma unroll
+            for (int q = 0; q < Q; ++q) xi[q] = fg.bcast(xa[q], i);
+        }
+        else
+        {
+            if (rb == i)
+            {
+#pragma unroll
+                for (int q = 0; q < Q; ++q) xb[q] = acc_b[q] * inv_b;
+            }
+#pragma unroll
+            for (int q = 0; q < Q; ++q) xi[q] = fg.bcast(xb[q], NP - 1 - i);
+        }
+        if (t < i)
+        {
+            const float l = ea * inv_a;
+#pragma unroll
+            for (int q = 0; q < Q; ++q) acc_a[q] -= l * xi[q];
+        }
+        if (rb < i)
+        {
+            const float l = eb * inv_b;
+#pragma unroll
+            for (int q = 0; q < Q; ++q) acc_b[q] -= l * xi[q];
+        }
+    }
+}
+
+// Forward substitution L y = rhs from the factor kept in M (the refinement
+// fallback): L[r][j] = M[j][r] / sqrt(M[j][j]).
+template <int NP, int Q>
+__device__ __forceinline__ void fold_forward(const FoldGrp<NP / 2> &fg, const float *M, int t, const float (&ra)[Q],
+                                             const float (&rb_rhs)[Q], float (&ya)[Q], float (&yb)[Q])
+{
+    constexpr int G = NP / 2, LD = FoldSmem<NP, 3>::LD;
+    const int rb = NP - 1 - t;
+    float acc_a[Q], acc_b[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+    {
+        acc_a[q] = ra[q];
+        acc_b[q] = rb_rhs[q];
+        ya[q] = 0.0f;
+        yb[q] = 0.0f;
+    }
+#pragma unroll
+    for (int j = 0; j < NP; ++j)
+    {
+        const float inv_j = rsqrtf(M[j * LD + j]);
+        float yj[Q];
+        if (j < G)
+        {
+            if (t == j)
+            {
+#pragma unroll
+                for (int q = 0; q < Q; ++q) ya[q] = acc_a[q] * inv_j;
+            }
+#pragma unroll
+            for (int q = 0; q < Q; ++q) yj[q] = fg.bcast(ya[q], j);
+        }
+        else
+        {
+            if (rb == j)
+            {
+#pragma unroll
+                for (int q = 0; q < Q; ++q) yb[q] = acc_b[q] * inv_j;
+            }
+#pragma unroll
+            for (int q = 0; q < Q; ++q) yj[q] = fg.bcast(yb[q], NP - 1 - j);
+        }
+        if (j < G && t > j)
+        {
+            const float l = M[j * LD + t] * inv_j;
+#pragma unroll
+            for (int q = 0; q < Q; ++q) acc_a[q] -= l * yj[q];
+        }
+        if (rb > j)
+        {
+            const float l = M[j * LD + rb] * inv_j;
+#pragma unroll
+            for (int q = 0; q < Q; ++q) acc_b[q] -= l * yj[q];
+        }
+    }
+}
+
+// FP64 residuals of both rows: res = rhs - A64 x, A64 rows gathered from the
+// double pair table, X the solutions of all rows.
+template <int NP, int Q>
+__device__ __forceinline__ void fold_residuals(const FoldGrp<NP / 2> &fg, const double *__restrict__ pair64,
+                                               long long pc, const int *LIN, double *X, int n, int t, int lin_a,
+                                               int lin_b, bool live_a, bool live_b, const double (&xa)[Q],
+                                               const double (&xb)[Q], const double (&rhs_a)[Q],
+                                               const double (&rhs_b)[Q], double (&res_a)[Q], double (&res_b)[Q])
+{
+    const int rb = NP - 1 - t;
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+    {
+        X[q * NP + t] = xa[q];
+        X[q * NP + rb] = xb[q];
+        res_a[q] = rhs_a[q];
+        res_b[q] = rhs_b[q];
+    }
+    fg.sync();
+    const double *base_a = pair64 + pc + lin_a, *base_b = pair64 + pc + lin_b;
+#pragma unroll
+    for (int c = 0; c < NP; ++c)
+    {
+        if (c < n)
+        {
+            const int l = LIN[c];
+            double xc[Q];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) xc[q] = X[q * NP + c];
+            if (live_a)
+            {
+                const double a = __ldg(base_a - l);
+#pragma unroll
+                for (int q = 0; q < Q; ++q) res_a[q] -= a * xc[q];
+            }
+            if (live_b)
+            {
+                const double b = __ldg(base_b - l);
+#pragma unroll
+                for (int q = 0; q < Q; ++q) res_b[q] -= b * xc[q];
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+    {
+        if (!live_a) res_a[q] = -xa[q];
+        if (!live_b) res_b[q] = -xb[q];
+    }
+    fg.sync();
+}
+
+template <int NP, bool ORDINARY>
+__global__ void __launch_bounds__(256, 2)
+    k_solve_fold(const Geom g, const int2 *__restrict__ cells, const int *__restrict__ n_items_ptr,
+                 const int2 *__restrict__ nb_rec, int ind_value, const float *__restrict__ pair32, SolveParams P)
+{
+    constexpr int G = NP / 2;   // lanes per system
+    constexpr int SPW = 32 / G; // systems per warp
+    constexpr int QB = ORDINARY ? 2 : 1;
+    constexpr int R = QB + 1;
+    typedef FoldSmem<NP, R> SM;
+    constexpr int LD = SM::LD;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int h = lane / G; // the warp's system slot
+    const int t = lane % G;
+    const int rb = NP - 1 - t;
+    FoldGrp<G> fg;
+    fg.mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (h * G));
+    unsigned char *gb = smem + SM::bytes * (warp * SPW + h);
+    float *M = reinterpret_cast<float *>(gb);
+    int *LIN = reinterpret_cast<int *>(gb + SM::lin_off);
+    double *X = reinterpret_cast<double *>(gb + SM::x_off);
+    const long long pc = P.pc;
+    const double *pair64 = P.pair64;
+
+    // The block's contiguous run of items; the warps take SPW consecutive items
+    // at a time, so every lane of a warp runs the same number of iterations (a
+    // slot past the end solves an empty system and writes nothing).
+    const int n_items = *n_items_ptr;
+    const int per_block = (n_items + gridDim.x - 1) / gridDim.x;
+    const int run_first = blockIdx.x * per_block;
+    const int run_end = min(n_items, run_first + per_block);
+    const int wstride = nwarps * SPW;
+    int base = run_first + warp * SPW;
+    auto work_at = [&](int it) { return it < run_end ? cells[it] : make_int2(0, 0); };
+    int2 w_cur = work_at(base + h);
+    int2 w_nxt = work_at(base + wstride + h);
+    int2 rec_a = t < w_cur.y ? nb_rec[(long long)w_cur.x * g.k + t] : make_int2(0, 0);
+    int2 rec_b = rb < w_cur.y ? nb_rec[(long long)w_cur.x * g.k + rb] : make_int2(0, 0);
+    for (; base < run_end; base += wstride)
+    {
+        const bool valid = base + h < run_end;
+        const int my_cell = w_cur.x, my_n = w_cur.y;
+        const bool live_a = t < my_n, live_b = rb < my_n;
+        const int lin_a = rec_a.x, lin_b = rec_b.x;
+        const double vc_a = centred_value(live_a, __int_as_float(rec_a.y), ind_value, P.mf);
+        const double vc_b = centred_value(live_b, __int_as_float(rec_b.y), ind_value, P.mf);
+        // records of the next iteration
+        rec_a = t < w_nxt.y ? nb_rec[(long long)w_nxt.x * g.k + t] : make_int2(0, 0);
+        rec_b = rb < w_nxt.y ? nb_rec[(long long)w_nxt.x * g.k + rb] : make_int2(0, 0);
+        w_cur = w_nxt;
+        w_nxt = work_at(base + 2 * wstride + h);
+        LIN[t] = live_a ? lin_a : 0;
+        LIN[rb] = live_b ? lin_b : 0;
+        fg.sync();
+
+        // ---- assembly: lower triangles of rows a and b; padding rows are identity
+        float ra[G], rbv[NP];
+#pragma unroll
+        for (int c = 0; c < G; ++c)
+        {
+            float a = 0.0f;
+            if (live_a && c <= t) a = __ldg(pair32 + pc + lin_a - LIN[c]);
+            if (!live_a && c == t) a = 1.0f;
+            ra[c] = a;
+        }
+#pragma unroll
+        for (int c = 0; c < NP; ++c)
+        {
+            float a = 0.0f;
+            if (live_b && c <= rb) a = __ldg(pair32 + pc + lin_b - LIN[c]);
+            if (!live_b && c == rb) a = 1.0f;
+            rbv[c] = a;
+        }
+        const double b64_a = live_a ? __ldg(pair64 + pc + lin_a) : 0.0;
+        const double b64_b = live_b ? __ldg(pair64 + pc + lin_b) : 0.0;
+
+        // ---- factorisation with the forward substitution of b, 1 and v - mean
+        float rhs_a[R], rhs_b[R], ya[R], yb[R];
+        rhs_a[0] = (float)b64_a;
+        rhs_b[0] = (float)b64_b;
+        if constexpr (ORDINARY)
+        {
+            rhs_a[1] = live_a ? 1.0f : 0.0f;
+            rhs_b[1] = live_b ? 1.0f : 0.0f;
+        }
+        rhs_a[R - 1] = (float)vc_a;
+        rhs_b[R - 1] = (float)vc_b;
+#pragma unroll
+        for (int q = 0; q < R; ++q)
+        {
+            ya[q] = 0.0f;
+            yb[q] = 0.0f;
+        }
+        bool fail = false;
+        float inv_a = 0.0f, inv_b = 0.0f;
+#pragma unroll
+        for (int j = 0; j < NP; ++j)
+        {
+            if (j < G)
+            {
+                M[j * LD + t] = ra[j];
+                if (t == j)
+                {
+#pragma unroll
+                    for (int q = 0; q < R; ++q) M[j * LD + NP + q] = rhs_a[q];
+                }
+            }
+            M[j * LD + rb] = rbv[j];
+            if (j >= G && rb == j)
+            {
+#pragma unroll
+                for (int q = 0; q < R; ++q) M[j * LD + NP + q] = rhs_b[q];
+            }
+            fg.sync();
+            float mj[LD];
+            const float4 *mv = reinterpret_cast<const float4 *>(M + j * LD);
+#pragma unroll
+            for (int q = j / 4; q < LD / 4; ++q)
+            {
+                const float4 v4 = mv[q];
+                mj[4 * q] = v4.x;
+                mj[4 * q + 1] = v4.y;
+                mj[4 * q + 2] = v4.z;
+                mj[4 * q + 3] = v4.w;
+            }
+            const float d = mj[j];
+            fail |= !(d > 0.0f);
+            const float inv_s = rsqrtf(d);
+            const float inv2 = inv_s * inv_s;
+            if (j < G)
+            {
+                const float s = ra[j] * inv2;
+#pragma unroll
+                for (int c = j + 1; c < G; ++c) ra[c] -= s * mj[c];
+                if (t > j)
+                {
+#pragma unroll
+                    for (int q = 0; q < R; ++q) rhs_a[q] -= s * mj[NP + q];
+                }
+                ra[j] *= inv_s;
+                if (t == j)
+                {
+                    inv_a = inv_s;
+#pragma unroll
+                    for (int q = 0; q < R; ++q) ya[q] = rhs_a[q] * inv_s;
+                }
+            }
+            {
+                const float s = rbv[j] * inv2;
+#pragma unroll
+                for (int c = j + 1; c < NP; ++c) rbv[c] -= s * mj[c];
+                if (rb > j)
+                {
+#pragma unroll
+                    for (int q = 0; q < R; ++q) rhs_b[q] -= s * mj[NP + q];
+                }
+                rbv[j] *= inv_s;
+                if (rb == j)
+                {
+                    inv_b = inv_s;
+#pragma unroll
+                    for (int q = 0; q < R; ++q) yb[q] = rhs_b[q] * inv_s;
+                }
+            }
+        }
+
+        // ---- back substitution and the dual-weighted FP64 correction of the forms
+        float xsa[R], xsb[R];
+        fold_back<NP, R>(fg, M, t, ya, yb, inv_a, inv_b, xsa, xsb);
+        double xa[R], xb[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q)
+        {
+            xa[q] = (double)xsa[q];
+            xb[q] = (double)xsb[q];
+        }
+        const double one_a = live_a ? 1.0 : 0.0, one_b = live_b ? 1.0 : 0.0;
+        double r64a[QB], r64b[QB], resa[QB], resb[QB], xqa[QB], xqb[QB];
+#pragma unroll
+        for (int q = 0; q < QB; ++q)
+        {
+            r64a[q] = q == 0 ? b64_a : one_a;
+            r64b[q] = q == 0 ? b64_b : one_b;
+            xqa[q] = xa[q];
+            xqb[q] = xb[q];
+        }
+        fold_residuals<NP, QB>(fg, pair64, pc, LIN, X, my_n, t, lin_a, lin_b, live_a, live_b, xqa, xqb, r64a, r64b,
+                               resa, resb);
+        // u^T A^-1 w = u^T x_w + x_u^T (w - A64 x_w) + O(|e_u| |e_w|)
+        const double corr_vb = xa[R - 1] * resa[0] + xb[R - 1] * resb[0];
+        const double corr_bb = xa[0] * resa[0] + xb[0] * resb[0];
+        double f_vb = vc_a * xa[0] + vc_b * xb[0] + corr_vb;
+        double f_bb = b64_a * xa[0] + b64_b * xb[0] + corr_bb;
+        double f_1b = 0.0, f_v1 = 0.0, f_11 = 0.0;
+        if constexpr (ORDINARY)
+        {
+            f_1b = one_a * xa[0] + one_b * xb[0] + xa[1] * resa[0] + xb[1] * resb[0];
+            f_v1 = vc_a * xa[1] + vc_b * xb[1] + xa[R - 1] * resa[1] + xb[R - 1] * resb[1];
+            f_11 = one_a * xa[1] + one_b * xb[1] + xa[1] * resa[1] + xb[1] * resb[1];
+        }
+        double s_vb = fg.sum(f_vb), s_bb = fg.sum(f_bb);
+        double s_1b = 0.0, s_v1 = 0.0, s_11 = 0.0;
+        if constexpr (ORDINARY)
+        {
+            s_1b = fg.sum(f_1b);
+            s_v1 = fg.sum(f_v1);
+            s_11 = fg.sum(f_11);
+        }
+        // a-posteriori check: the first-order correction of each form relative
+        // to the form's scale; what remains after it is about its square
+        const double abs_vb = fg.sum(fabs(vc_a * xa[0]) + fabs(vc_b * xb[0])) + 1e-300;
+        const double abs_bb = fg.sum(fabs(b64_a * xa[0]) + fabs(b64_b * xb[0])) + 1e-300;
+        const double c1 = fabs(fg.sum(corr_vb)) / abs_vb;
+        const double c2 = fabs(fg.sum(corr_bb)) / abs_bb;
+        const double dd = fmax(c1, c2);
+        bool escalate = fail || !(dd * dd <= P.tol) || !(s_vb == s_vb) || !(s_bb == s_bb);
+        if (escalate && P.steps > 0 && !fail)
+        {
+            // classic refinement x += A32^-1 (b - A64 x) of b (and 1), then the forms uncorrected
+            double prev = 0.0;
+            bool done = false;
+            for (int it = 0; it < P.steps && !done; ++it)
+            {
+#pragma unroll
+                for (int q = 0; q < QB; ++q)
+                {
+                    xqa[q] = xa[q];
+                    xqb[q] = xb[q];
+                }
+                fold_residuals<NP, QB>(fg, pair64, pc, LIN, X, my_n, t, lin_a, lin_b, live_a, live_b, xqa, xqb, r64a,
+                                       r64b, resa, resb);
+                float rfa[QB], rfb[QB], yya[QB], yyb[QB], dda[QB], ddb[QB];
+#pragma unroll
+                for (int q = 0; q < QB; ++q)
+                {
+                    rfa[q] = (float)resa[q];
+                    rfb[q] = (float)resb[q];
+                }
+                fold_forward<NP, QB>(fg, M, t, rfa, rfb, yya, yyb);
+                fold_back<NP, QB>(fg, M, t, yya, yyb, inv_a, inv_b, dda, ddb);
+                double dmax = 0.0, xmax = 0.0;
+#pragma unroll
+                for (int q = 0; q < QB; ++q)
+                {
+                    xa[q] += (double)dda[q];
+                    xb[q] += (double)ddb[q];
+                    dmax = fmax(dmax, fmax(fabs((double)dda[q]), fabs((double)ddb[q])));
+                    xmax = fmax(xmax, fmax(fabs(xa[q]), fabs(xb[q])));
+                }
+                dmax = fg.max(dmax);
+                xmax = fg.max(xmax);
+                const double delta = xmax > 0.0 ? dmax / xmax : 0.0;
+                double err;
+                if (it == 0)
+                    err = delta * delta;
+                else
+                {
+                    const double rho = prev > 0.0 ? delta / prev : 0.0;
+                    err = rho < 0.5 ? delta * rho / (1.0 - rho) : 1.0;
+                }
+                if (!(delta == delta)) err = 1.0;
+                prev = delta;
+                done = err <= P.tol;
+            }
+            if (done)
+            {
+                escalate = false;
+                s_vb = fg.sum(vc_a * xa[0] + vc_b * xb[0]);
+                s_bb = fg.sum(b64_a * xa[0] + b64_b * xb[0]);
+                if constexpr (ORDINARY)
+                {
+                    s_1b = fg.sum(one_a * xa[0] + one_b * xb[0]);
+                    s_v1 = fg.sum(vc_a * xa[1] + vc_b * xb[1]);
+                    s_11 = fg.sum(one_a * xa[1] + one_b * xb[1]);
+                }
+            }
+        }
+        if (valid && t == 0)
+        {
+            const SolveOut &out = P.out;
+            if (escalate)
+            {
+                int slot = atomicAdd(P.esc_count, 1);
+                P.esc_cells[slot] = make_int2(my_cell, my_n);
+                if (out.status) out.status[my_cell] = 4;
+            }
+            else
+            {
+                // forms -> estimate and variance (my_kriging_weights.h:312-357)
+                double est, var;
+                bool bad = fail;
+                if constexpr (ORDINARY)
+                {
+                    if (fabs(s_11) < 1e-15) bad = true;
+                    const double mu = (s_1b - 1.0) / s_11;
+                    est = s_vb - mu * s_v1;
+                    var = P.c0 - s_bb + mu * s_1b - mu;
+                }
+                else
+                {
+                    est = (double)P.mf + s_vb;
+                    var = P.c0 - s_bb;
+                }
+                if (var < 0) var = 0;
+                if (!bad)
+                {
+                    if (out.write_cont)
+                    {
+                        out.out_data[my_cell] = (float)est;
+                        out.out_mask[my_cell] = 1;
+                    }
+                    if (out.prob) out.prob[(long long)my_cell * out.prob_stride] = (float)est;
+                    if (out.est64) out.est64[my_cell] = est;
+                    if (out.var) out.var[my_cell] = var;
+                    if (out.status) out.status[my_cell] = 0;
+                }
+                else if (out.status)
+                    out.status[my_cell] = 2;
+            }
+        }
+        fg.sync();
+    }
+}
+
+template <typename K>
+static cudaError_t launch_kernel(K kern, size_t smem, int max_items, int gpb, int n_sm, cudaStream_t st, int &blocks_out)
 {
     constexpr int threads = 256;
-    constexpr int gpb = threads / NP;
-    const size_t smem = SolveSmem<NP, TF>::bytes * gpb;
-    auto kern = k_solve<NP, TF, ORD, REF>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
@@ -570,18 +1220,44 @@ static cudaError_t launch_one(const Geom &g, const int2 *cells, const int *n_ite
     long long blocks = (long long)n_sm * per_sm;
     if (want < blocks) blocks = want;
     if (blocks < 1) blocks = 1;
-    kern<<<(unsigned)blocks, threads, smem, st>>>(g, cells, n_items, nb_rec, nb_n, ind_value, pair64, pair32, mean, c0,
-                                                  steps, tol, out, esc_cells, esc_count);
+    blocks_out = (int)blocks;
+    return cudaSuccess;
+}
+
+template <int NP, typename TF, bool ORD, bool REF>
+static cudaError_t launch_one(const Geom &g, const int2 *cells, const int *n_items, int max_items, const int2 *nb_rec,
+                              int ind_value, const float *pair32, const SolveParams &P, int n_sm, cudaStream_t st)
+{
+    constexpr int threads = 256;
+    constexpr int gpb = threads / NP;
+    constexpr bool FOLD = REF && NP <= 32;
+    int blocks = 0;
+    if constexpr (FOLD)
+    {
+        constexpr int spb = threads / (NP / 2); // systems per block
+        const size_t smem = FoldSmem<NP, ORD ? 3 : 2>::bytes * spb;
+        auto kern = k_solve_fold<NP, ORD>;
+        cudaError_t e = launch_kernel(kern, smem, max_items, spb, n_sm, st, blocks);
+        if (e != cudaSuccess) return e;
+        kern<<<(unsigned)blocks, threads, smem, st>>>(g, cells, n_items, nb_rec, ind_value, pair32, P);
+    }
+    else
+    {
+        const size_t smem = SolveSmem<NP, TF, REF, ORD ? 3 : 2>::bytes * gpb;
+        auto kern = k_solve<NP, TF, ORD, REF>;
+        cudaError_t e = launch_kernel(kern, smem, max_items, gpb, n_sm, st, blocks);
+        if (e != cudaSuccess) return e;
+        kern<<<(unsigned)blocks, threads, smem, st>>>(g, cells, n_items, nb_rec, ind_value, pair32, P);
+    }
     return cudaGetLastError();
 }
 
 template <int NP>
 static cudaError_t launch_np(int precision, bool ordinary, const Geom &g, const int2 *cells, const int *n_items,
-                             int max_items, const int2 *nb_rec, const int *nb_n, int ind_value, const double *pair64,
-                             const float *pair32, double mean, double c0, int steps, double tol, const SolveOut &out,
-                             int2 *esc_cells, int *esc_count, int n_sm, cudaStream_t st)
+                             int max_items, const int2 *nb_rec, int ind_value, const float *pair32,
+                             const SolveParams &P, int n_sm, cudaStream_t st)
 {
-#define HB_ARGS g, cells, n_items, max_items, nb_rec, nb_n, ind_value, pair64, pair32, mean, c0, steps, tol, out, esc_cells, esc_count, n_sm, st
+#define HB_ARGS g, cells, n_items, max_items, nb_rec, ind_value, pair32, P, n_sm, st
     if (precision == 0)
         return ordinary ? launch_one<NP, double, true, false>(HB_ARGS) : launch_one<NP, double, false, false>(HB_ARGS);
     return ordinary ? launch_one<NP, float, true, true>(HB_ARGS) : launch_one<NP, float, false, true>(HB_ARGS);
@@ -594,20 +1270,27 @@ cudaError_t launch_solve_bucket(int np, int precision, bool ordinary, const Geom
                                 double tol, const SolveOut &out, int2 *esc_cells, int *esc_count, int n_sm,
                                 cudaStream_t st)
 {
+    (void)nb_n;
+    SolveParams P;
+    P.pair64 = pair64;
+    P.pc = g.pair_center;
+    P.mf = (float)mean; // mean_t is float (typedefs.h:122)
+    P.c0 = c0;
+    P.steps = steps;
+    P.tol = tol;
+    P.out = out;
+    P.esc_cells = esc_cells;
+    P.esc_count = esc_count;
     switch (np)
     {
     case 8:
-        return launch_np<8>(precision, ordinary, g, cells, n_items, max_items, nb_rec, nb_n, ind_value, pair64,
-                            pair32, mean, c0, steps, tol, out, esc_cells, esc_count, n_sm, st);
+        return launch_np<8>(precision, ordinary, g, cells, n_items, max_items, nb_rec, ind_value, pair32, P, n_sm, st);
     case 16:
-        return launch_np<16>(precision, ordinary, g, cells, n_items, max_items, nb_rec, nb_n, ind_value, pair64,
-                             pair32, mean, c0, steps, tol, out, esc_cells, esc_count, n_sm, st);
+        return launch_np<16>(precision, ordinary, g, cells, n_items, max_items, nb_rec, ind_value, pair32, P, n_sm, st);
     case 32:
-        return launch_np<32>(precision, ordinary, g, cells, n_items, max_items, nb_rec, nb_n, ind_value, pair64,
-                             pair32, mean, c0, steps, tol, out, esc_cells, esc_count, n_sm, st);
+        return launch_np<32>(precision, ordinary, g, cells, n_items, max_items, nb_rec, ind_value, pair32, P, n_sm, st);
     case 64:
-        return launch_np<64>(precision, ordinary, g, cells, n_items, max_items, nb_rec, nb_n, ind_value, pair64,
-                             pair32, mean, c0, steps, tol, out, esc_cells, esc_count, n_sm, st);
+        return launch_np<64>(precision, ordinary, g, cells, n_items, max_items, nb_rec, ind_value, pair32, P, n_sm, st);
     default:
         return cudaErrorInvalidValue;
     }
