@@ -297,7 +297,9 @@ def main():
     b_flops = last[f"bucket_flops_{b}"]
     achieved = b_flops / (b_ms / 1e3) / 1e12
     tpc = traffic_per_cell()
-    roofline = {"bound": "fp32", "kernel": f"k_solve<NP={[8, 16, 32, 64, 'large'][b]}, float, refined>",
+    kname = (f"k_solve_fold<NP={[8, 16, 32][b]}, ordinary> (FP32 refined, NP/2 lanes per system)" if b < 3
+             else "k_solve<NP=64, float, ordinary, refined>" if b == 3 else "k_solve_large")
+    roofline = {"bound": "fp32", "kernel": kname,
                 "achieved": achieved, "peak": pk["fp32"], "unit": "TFLOP/s", "frac": achieved / pk["fp32"],
                 "traffic": (tpc * last[f"bucket_items_{b}"]) if tpc else None,
                 "peak_source": f"CUDA-core FP32 peak 148 SM x 128 lanes x 2 x {pk['source']}",
