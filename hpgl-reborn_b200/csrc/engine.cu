@@ -16,10 +16,13 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <exception>
+#include <future>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace hb
@@ -165,7 +168,7 @@ static Engine &engine_for_current_device()
 struct Plan
 {
     Flavour f;
-    std::vector<Offset> tmpl;
+    long tmpl_count = 0; // length of the search template (built only when a bin needs it)
     KeyTable kt;
     Surrogate sg;
     Geom g;
@@ -221,8 +224,8 @@ static Plan make_plan(bool truncated, int cov_type, const double *ranges, const 
     if (!make_model(cov_type, ranges, angles, sill, nugget, pl.f.m, err)) throw CudaFail{-1, err};
     pl.f.truncated = truncated;
     for (int a = 0; a < 3; ++a) pl.f.r[a] = radiuses[a];
-    pl.tmpl = build_template(pl.f);
     build_key_table(pl.f, pl.kt, g_threads);
+    pl.tmpl_count = template_size(pl.f, pl.kt);
     if (k <= 64 && pl.kt.n_ranks <= 0xFFFE) build_surrogate(pl.f, pl.kt, pl.sg);
     pl.rank_bits = pl.kt.n_ranks > 1 ? bits_for(pl.kt.n_ranks - 1) : 0;
 
@@ -241,7 +244,7 @@ static Plan make_plan(bool truncated, int cov_type, const double *ranges, const 
     long long nb = (long long)g.bx * g.by * g.bz;
     if (nb > (1LL << 30)) throw CudaFail{-4, "too many search bins"};
     g.n_bins = (int)nb;
-    g.limit = (int)(pl.tmpl.size() / 250);
+    g.limit = (int)(pl.tmpl_count / 250);
     g.k = k;
     g.khx = pl.kt.half[0];
     g.khy = pl.kt.half[1];
@@ -260,6 +263,17 @@ static Plan make_plan(bool truncated, int cov_type, const double *ranges, const 
     if (pn > (1LL << 31) - 1) throw CudaFail{-4, "covariance table too large for these radiuses"};
     g.pair_center = ((long long)ph[2] * g.pny + ph[1]) * g.pnx + ph[0];
     return pl;
+}
+
+// Geometry of the grid alone: what the upload and point compaction read.
+static Geom grid_geom(const int *dims)
+{
+    Geom g = {};
+    g.nx = dims[0];
+    g.ny = dims[1];
+    g.nz = dims[2];
+    g.n_cells = (long long)dims[0] * dims[1] * dims[2];
+    return g;
 }
 
 static DevModel dev_model(const CovModel &m)
@@ -338,9 +352,6 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
     S.search_vals = E.buf<double>("search_vals", pl.kt.vals.size());
     HB_CK(cudaMemcpyAsync(keytab, pl.kt.rank.data(), pl.kt.rank.size() * 4, cudaMemcpyHostToDevice, st));
     HB_CK(cudaMemcpyAsync(S.search_vals, pl.kt.vals.data(), pl.kt.vals.size() * 8, cudaMemcpyHostToDevice, st));
-    std::vector<int4> t4(std::max<size_t>(pl.tmpl.size(), 1));
-    for (size_t i = 0; i < pl.tmpl.size(); ++i) t4[i] = make_int4(pl.tmpl[i].dx, pl.tmpl[i].dy, pl.tmpl[i].dz, 0);
-    int4 *tmpl = E.buf<int4>("tmpl", t4.size());
     // 16-bit ranks for the fast selection path when the rank space allows it
     const bool fast_keys = g.k <= 64 && pl.kt.n_ranks <= 0xFFFE;
     uint16_t *keytab16 = nullptr;
@@ -365,7 +376,6 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
         sd.h2_cut = pl.sg.h2_cut;
         sd.h2_rank = h2r;
     }
-    HB_CK(cudaMemcpyAsync(tmpl, t4.data(), t4.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
     long long pn = (long long)g.pnx * g.pny * (2 * g.phz + 1);
     S.pair64 = E.buf<double>("pair64", (size_t)pn);
     S.pair32 = E.buf<float>("pair32", (size_t)pn);
@@ -395,6 +405,18 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
     HB_CK(cudaStreamSynchronize(st));
     E.mark(STAGE_BINS, st);
     int max_cand = host_scal[1];
+    // the sorted template, only when some bin takes the template path
+    int n_tmpl = 0;
+    int4 *tmpl = E.buf<int4>("tmpl", std::max<long>(pl.tmpl_count, 1));
+    if (host_scal[2] > 0 && pl.tmpl_count > 0)
+    {
+        const std::vector<Offset> tv = build_template(pl.f, pl.kt);
+        std::vector<int4> t4(tv.size());
+        for (size_t i = 0; i < tv.size(); ++i) t4[i] = make_int4(tv[i].dx, tv[i].dy, tv[i].dz, 0);
+        HB_CK(cudaMemcpyAsync(tmpl, t4.data(), t4.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+        HB_CK(cudaStreamSynchronize(st)); // t4 is a temporary
+        n_tmpl = (int)tv.size();
+    }
 
     // search
     int cand_cap = std::max(4, (max_cand + 3) / 4 * 4);
@@ -415,11 +437,11 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
     HB_CK(cudaEventRecord(E.ev_[8], st));
     if (fast)
         HB_CK(launch_search_fast(g, d_mask, all_cells, bin_start, bin_cnt, S.bin_flag, bin_pts, P.pts_xyz, P.pts_val,
-                                 keytab16, sd, tmpl, (int)pl.tmpl.size(), P.pid_of_node, cand_cap, warps, S.nb_pid,
+                                 keytab16, sd, tmpl, n_tmpl, P.pid_of_node, cand_cap, warps, S.nb_pid,
                                  S.nb_rec, S.nb_n, tie_cells, scal + 3, scal + 4, scal + 5, st));
     else
         HB_CK(launch_search(g, d_mask, all_cells, bin_start, bin_cnt, S.bin_flag, bin_pts, P.pts_xyz, P.pts_val,
-                            keytab, pl.rank_bits, tmpl, (int)pl.tmpl.size(), P.pid_of_node, cand_cap, warps,
+                            keytab, pl.rank_bits, tmpl, n_tmpl, P.pid_of_node, cand_cap, warps,
                             S.nb_pid, S.nb_rec, S.nb_n, tie_cells, scal + 3, scal + 4, st));
     HB_CK(cudaEventRecord(E.ev_[9], st));
     HB_CK(cudaMemcpyAsync(host_scal, scal, sizeof(host_scal), cudaMemcpyDeviceToHost, st));
@@ -605,7 +627,11 @@ int cont_kriging(int kind, const int *dims, const float *in_data, const unsigned
         if (!dims || !in_data || !in_mask || !out_data || !out_mask) throw CudaFail{-1, "null array argument"};
         long long n = check_dims(dims);
         const bool simple = kind == 1;
-        Plan pl = make_plan(simple, a.cov_type, a.ranges, a.angles, a.sill, a.nugget, a.radiuses, a.max_nb, dims);
+        check_model_args(a.cov_type, a.ranges, a.angles, a.sill, a.nugget, a.radiuses, a.max_nb);
+        // the host tables are built while the grid is uploaded and compacted
+        auto plan_f = std::async(std::launch::async, [&]() {
+            return make_plan(simple, a.cov_type, a.ranges, a.angles, a.sill, a.nugget, a.radiuses, a.max_nb, dims);
+        });
         Engine &E = engine_for_current_device();
         cudaStream_t st = E.stream(opt.stream);
         IoPlan io{(opt.flags & 1u) != 0, st};
@@ -670,7 +696,8 @@ int cont_kriging(int kind, const int *dims, const float *in_data, const unsigned
         }
 
         HB_CK(cudaEventRecord(E.ev_[2], st));
-        DevPoints P = compact_points(E, pl.g, d_mask, d_in, nullptr, st);
+        DevPoints P = compact_points(E, grid_geom(dims), d_mask, d_in, nullptr, st);
+        const Plan pl = plan_f.get();
         DevSearch S = run_search(E, pl, P, d_mask, 0, st, false, (opt.flags & 4u) != 0);
         HB_CK(cudaEventRecord(E.ev_[3], st));
         SolveOut so{};
@@ -800,7 +827,10 @@ int median_ik(const int *dims, const unsigned char *in_data, const unsigned char
     {
         if (!dims || !in_data || !in_mask || !out_data || !out_mask) throw CudaFail{-1, "null array argument"};
         long long n = check_dims(dims);
-        Plan pl = make_plan(true, a.cov_type, a.ranges, a.angles, a.sill, a.nugget, a.radiuses, a.max_nb, dims);
+        check_model_args(a.cov_type, a.ranges, a.angles, a.sill, a.nugget, a.radiuses, a.max_nb);
+        auto plan_f = std::async(std::launch::async, [&]() {
+            return make_plan(true, a.cov_type, a.ranges, a.angles, a.sill, a.nugget, a.radiuses, a.max_nb, dims);
+        });
         Engine &E = engine_for_current_device();
         cudaStream_t st = E.stream(opt.stream);
         IoPlan io{(opt.flags & 1u) != 0, st};
@@ -813,7 +843,8 @@ int median_ik(const int *dims, const unsigned char *in_data, const unsigned char
         double *d_est = E.buf<double>("est64", (size_t)n);
         float *d_prob = opt.ik_probs ? ((io.device) ? opt.ik_probs : E.buf<float>("ik_probs", (size_t)n)) : nullptr;
         HB_CK(cudaEventRecord(E.ev_[2], st));
-        DevPoints P = compact_points(E, pl.g, d_mask, nullptr, d_in, st);
+        DevPoints P = compact_points(E, grid_geom(dims), d_mask, nullptr, d_in, st);
+        const Plan pl = plan_f.get();
         DevSearch S = run_search(E, pl, P, d_mask, 1, st, false, (opt.flags & 4u) != 0);
         HB_CK(cudaEventRecord(E.ev_[3], st));
         SolveOut so{};
@@ -922,7 +953,9 @@ int host_template(int kind, int cov_type, const double *ranges, const double *an
         if (!make_model(cov_type, ranges, angles, sill, nugget, f.m, err)) throw CudaFail{-1, err};
         f.truncated = kind != 0;
         for (int a = 0; a < 3; ++a) f.r[a] = radiuses[a];
-        std::vector<Offset> t = build_template(f);
+        KeyTable kt;
+        build_key_table(f, kt, g_threads);
+        std::vector<Offset> t = build_template(f, kt);
         for (int i = 0; i < (int)t.size() && i < cap; ++i)
         {
             out[3 * i] = t[i].dx;

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <thread>
 
 namespace hb
@@ -135,6 +136,37 @@ std::vector<Offset> build_template(const Flavour &f)
     return out;
 }
 
+std::vector<Offset> build_template(const Flavour &f, const KeyTable &kt)
+{
+    // the same sequence of (offset, key) as build_template(f), read from the key
+    // table (the +-r box lies inside the key block, and kt.vals holds at_offset)
+    struct Ent
+    {
+        Offset o;
+        double key;
+    };
+    auto val = [&](int dx, int dy, int dz) {
+        return kt.vals[((long)(dz + kt.half[2]) * kt.n[1] + (dy + kt.half[1])) * kt.n[0] + (dx + kt.half[0])];
+    };
+    std::vector<Ent> v;
+    const double thr = f.threshold();
+    for (int z = -f.r[2]; z <= f.r[2]; ++z)
+        for (int y = -f.r[1]; y <= f.r[1]; ++y)
+            for (int x = -f.r[0]; x <= f.r[0]; ++x)
+            {
+                if (val(x, y, z) > thr)
+                {
+                    Offset o = {0 - x, 0 - y, 0 - z};
+                    v.push_back({o, val(o.dx, o.dy, o.dz)});
+                }
+            }
+    std::sort(v.begin(), v.end(), [](const Ent &a, const Ent &b) { return a.key > b.key; });
+    std::vector<Offset> out;
+    out.reserve(v.size());
+    for (const Ent &e : v) out.push_back(e.o);
+    return out;
+}
+
 int clamp_threads(int n)
 {
     int hw = (int)std::thread::hardware_concurrency();
@@ -168,37 +200,78 @@ void build_key_table(const Flavour &f, KeyTable &kt, int n_threads)
                     }
         });
     for (auto &th : pool) th.join();
-    // dense descending ranks of the kept values
-    std::vector<std::pair<double, long>> kept;
-    for (long i = 0; i < total; ++i)
-        if (kt.vals[i] > thr) kept.push_back({kt.vals[i], i});
-    std::sort(kept.begin(), kept.end(),
-              [](const std::pair<double, long> &a, const std::pair<double, long> &b) { return a.first > b.first; });
-    uint32_t r = 0;
-    for (size_t j = 0; j < kept.size(); ++j)
+    // dense descending ranks of the kept values. The kept (value, index) pairs
+    // are sorted by the value's bit pattern, which orders positive doubles like
+    // their values (least-significant-digit radix sort, 11-bit digits, digits
+    // that every key shares skipped), then ranked walking down from the top.
+    struct KI
     {
-        if (j > 0 && kept[j].first != kept[j - 1].first) ++r;
-        kt.rank[kept[j].second] = r;
+        uint64_t key;
+        uint32_t idx;
+    };
+    std::vector<KI> a, b;
+    a.reserve(total / 4);
+    for (long i = 0; i < total; ++i)
+        if (kt.vals[i] > thr)
+        {
+            uint64_t bits;
+            std::memcpy(&bits, &kt.vals[i], 8);
+            a.push_back({bits, (uint32_t)i});
+        }
+    b.resize(a.size());
+    for (int shift = 0; shift < 64; shift += 11)
+    {
+        size_t cnt[2048] = {0};
+        for (const KI &e : a) ++cnt[(e.key >> shift) & 2047];
+        if (!a.empty() && cnt[(a[0].key >> shift) & 2047] == a.size()) continue; // one digit value: order kept
+        size_t pos = 0;
+        for (int d = 0; d < 2048; ++d)
+        {
+            const size_t c = cnt[d];
+            cnt[d] = pos;
+            pos += c;
+        }
+        for (const KI &e : a) b[cnt[(e.key >> shift) & 2047]++] = e;
+        a.swap(b);
     }
-    kt.n_ranks = kept.empty() ? 0 : r + 1;
+    uint32_t r = 0;
+    for (size_t j = a.size(); j-- > 0;)
+    {
+        if (j + 1 < a.size() && a[j].key != a[j + 1].key) ++r;
+        kt.rank[a[j].idx] = r;
+    }
+    kt.n_ranks = a.empty() ? 0 : r + 1;
 }
+
+long template_size(const Flavour &f, const KeyTable &kt)
+{
+    const double thr = f.threshold();
+    long n = 0;
+    for (int z = -f.r[2]; z <= f.r[2]; ++z)
+        for (int y = -f.r[1]; y <= f.r[1]; ++y)
+        {
+            const double *row = &kt.vals[((long)(z + kt.half[2]) * kt.n[1] + (y + kt.half[1])) * kt.n[0] + kt.half[0]];
+            for (int x = -f.r[0]; x <= f.r[0]; ++x) n += row[x] > thr;
+        }
+    return n;
+}
+
 void build_surrogate(const Flavour &f, const KeyTable &kt, Surrogate &sg)
 {
     sg.ok = false;
     sg.h2_rank.clear();
     for (int i = 0; i < 9; ++i) sg.T[i] = (float)f.m.T[i];
-    struct Ent
-    {
-        double h2;
-        uint32_t rank;
-    };
-    std::vector<Ent> kept;
+    if (kt.n_ranks == 0) return;
+    // per rank the smallest and largest h2 carrying it (offsets whose h2 agree
+    // mathematically can differ in the last bit and still share a covariance)
+    std::vector<double> lo(kt.n_ranks, 1e308), hi(kt.n_ranks, -1.0);
     for (int iz = 0; iz < kt.n[2]; ++iz)
         for (int iy = 0; iy < kt.n[1]; ++iy)
             for (int ix = 0; ix < kt.n[0]; ++ix)
             {
                 const long i = ((long)iz * kt.n[1] + iy) * kt.n[0] + ix;
-                if (kt.rank[i] == KEY_EXCLUDED) continue;
+                const uint32_t rk = kt.rank[i];
+                if (rk == KEY_EXCLUDED) continue;
                 const double v[3] = {(double)(0 - (ix - kt.half[0])), (double)(0 - (iy - kt.half[1])),
                                      (double)(0 - (iz - kt.half[2]))};
                 double acc = 0.0;
@@ -210,22 +283,14 @@ void build_surrogate(const Flavour &f, const KeyTable &kt, Surrogate &sg)
                     d += v[2] * f.m.T[3 * r + 2];
                     acc += d * d;
                 }
-                kept.push_back({acc, kt.rank[i]});
+                lo[rk] = std::min(lo[rk], acc);
+                hi[rk] = std::max(hi[rk], acc);
             }
-    if (kept.empty()) return;
-    std::sort(kept.begin(), kept.end(), [](const Ent &a, const Ent &b) {
-        return a.h2 < b.h2 || (a.h2 == b.h2 && a.rank < b.rank);
-    });
-    // offsets whose h2 agree mathematically can differ in the last bit and still
-    // share a covariance value (one rank, several h2): keep the largest h2 per rank
-    sg.h2_rank.assign(kt.n_ranks, 0.0);
-    for (size_t j = 0; j < kept.size(); ++j)
-    {
-        if (j > 0 && kept[j].rank < kept[j - 1].rank) return; // not monotone
-        if (kept[j].rank >= kt.n_ranks) return;
-        sg.h2_rank[kept[j].rank] = kept[j].h2; // ascending h2: the last one is the largest
-    }
-    sg.h2_cut = kept.back().h2;
+    // ranks increase with h2: every h2 of rank r lies below every h2 of rank r + 1
+    for (uint32_t r = 0; r + 1 < kt.n_ranks; ++r)
+        if (!(hi[r] < lo[r + 1])) return;
+    sg.h2_rank = hi;
+    sg.h2_cut = hi[kt.n_ranks - 1];
     // A transformed coordinate is formed in float as fma(T2, z, fma(T1, y, T0 * x))
     // for the cell and for the candidate, both relative to the bin corner, then
     // subtracted: with |T' - T| <= u |T| and four roundings, each component is off

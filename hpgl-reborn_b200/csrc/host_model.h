@@ -81,6 +81,10 @@ struct KeyTable
     uint32_t n_ranks = 0; // distinct kept values
 };
 void build_key_table(const Flavour &f, KeyTable &kt, int n_threads);
+// The same template as build_template(f), its covariances read from kt.
+std::vector<Offset> build_template(const Flavour &f, const KeyTable &kt);
+// Its length alone (the clusterizer's limit is length / 250), without the sort.
+long template_size(const Flavour &f, const KeyTable &kt);
 
 // Float surrogate of the selection key. Over the kept offsets of the key
 // block the dense rank must be a non-decreasing function of the reference's

@@ -676,7 +676,9 @@ struct FoldSmem
     static constexpr size_t m_bytes = (size_t)NP * LD * sizeof(float);
     static constexpr size_t lin_off = m_bytes;
     static constexpr size_t x_off = (lin_off + NP * sizeof(int) + 15) / 16 * 16;
-    static constexpr size_t bytes = x_off + 2 * NP * sizeof(double);
+    // Systems sharing a warp sit 4 G bytes apart modulo 128, so the G words each
+    // writes per step, and the rows they broadcast, fall on disjoint banks.
+    static constexpr size_t bytes = (x_off + 2 * NP * sizeof(double) + 127) / 128 * 128 + 4 * (NP / 2);
 };
 
 template <int G>
