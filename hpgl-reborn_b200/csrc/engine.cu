@@ -499,12 +499,15 @@ static void run_solves(Engine &E, const Plan &pl, const DevPoints &P, const DevS
     const Geom &g = pl.g;
     int *bucket_cnt = E.buf<int>("bucket_cnt", kBuckets);
     int *bucket_off = E.buf<int>("bucket_off", kBuckets + 1);
-    int *bucket_fill = E.buf<int>("bucket_fill", kBuckets);
+    const size_t n_tiles = (size_t)prepare_tiles(g.n_cells);
+    int *tile_cnt = E.buf<int>("tile_cnt", n_tiles * kBuckets);
+    unsigned long long *tile_mom = E.buf<unsigned long long>("tile_mom", n_tiles * kBuckets * 3);
     int2 *cells = E.buf<int2>("cells", (size_t)g.n_cells);
     unsigned long long *moments = E.buf<unsigned long long>("moments", kBuckets * 3);
     int *esc_cnt = E.buf<int>("esc_cnt", kBuckets);
     int2 *esc_cells = precision ? E.buf<int2>("esc_cells", (size_t)g.n_cells) : nullptr;
-    launch_prepare(g, d_mask, all_cells, S.nb_n, d_status, bucket_cnt, bucket_off, bucket_fill, cells, moments, st);
+    launch_prepare(g, d_mask, all_cells, S.nb_n, d_status, bucket_cnt, bucket_off, tile_cnt, tile_mom, cells, moments,
+                   st);
     HB_CK(cudaMemsetAsync(esc_cnt, 0, sizeof(int) * kBuckets, st));
     HB_CK(cudaGetLastError());
     E.stats.launches += 3;

@@ -97,8 +97,11 @@ cudaError_t launch_solve_large(const Geom &g, const int2 *cells, const int *n_it
 // misc (misc.cu)
 void launch_build_pair(const Geom &g, const DevModel &m, int truncated, const double *search_vals, double *pair64,
                        float *pair32, cudaStream_t st);
+// tiles of the stable bucket partition; tile_cnt holds kBuckets ints and tile_mom
+// 3 kBuckets values per tile
+long long prepare_tiles(long long n_cells);
 void launch_prepare(const Geom &g, const uint8_t *mask, int all_cells, const int *nb_n, signed char *status,
-                    int *bucket_cnt, int *bucket_off, int *bucket_fill, int2 *cells,
+                    int *bucket_cnt, int *bucket_off, int *tile_cnt, unsigned long long *tile_mom, int2 *cells,
                     unsigned long long *moments, cudaStream_t st);
 void launch_finalize_cont(const Geom &g, const float *in_data, signed char *status, int simple, float mean_f,
                           float *out_data, uint8_t *out_mask, double *est64, double *var, cudaStream_t st);

@@ -77,98 +77,209 @@ __device__ __forceinline__ int bucket_of(int n)
 
 // Per-cell status before the solve: -1 informed (continuous kriging only),
 // 1 no neighbours, 3 pending (to be solved).
-__global__ void k_prepare(const Geom g, const uint8_t *__restrict__ mask, int all_cells, const int *__restrict__ nb_n,
-                          signed char *__restrict__ status, int *__restrict__ bucket_cnt,
-                          unsigned long long *__restrict__ moments)
+// Per-cell status and the solve work lists, as a stable partition by bucket:
+// the list of every bucket holds its cells in ascending cell order, so the
+// solver's blocks, which take contiguous runs of a list, work on neighbouring
+// cells. Three passes over tiles of kTile cells: counts (and the moments of n
+// per bucket, for the flop count), a one-block scan, and the ordered fill.
+constexpr int kTileThreads = 256, kTileIters = 8, kTile = kTileThreads * kTileIters;
+
+long long prepare_tiles(long long n_cells) { return (n_cells + kTile - 1) / kTile; }
+
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
 {
-    __shared__ int s_cnt[kBuckets];
-    __shared__ unsigned long long s_mom[kBuckets * 3];
-    if (threadIdx.x < kBuckets) s_cnt[threadIdx.x] = 0;
-    if (threadIdx.x < kBuckets * 3) s_mom[threadIdx.x] = 0;
-    __syncthreads();
-    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < g.n_cells;
-         c += (long long)gridDim.x * blockDim.x)
-    {
-        if (!all_cells && mask[c])
-        {
-            status[c] = -1;
-            continue;
-        }
-        int n = nb_n[c];
-        int b = bucket_of(n);
-        status[c] = b < 0 ? 1 : 3;
-        if (b >= 0)
-        {
-            atomicAdd(&s_cnt[b], 1);
-            // sum n, n^2, n^3 per bucket: the algorithmic flop count is a cubic in n
-            unsigned long long nn = (unsigned long long)n;
-            atomicAdd(&s_mom[3 * b + 0], nn);
-            atomicAdd(&s_mom[3 * b + 1], nn * nn);
-            atomicAdd(&s_mom[3 * b + 2], nn * nn * nn);
-        }
-    }
-    __syncthreads();
-    if (threadIdx.x < kBuckets && s_cnt[threadIdx.x]) atomicAdd(&bucket_cnt[threadIdx.x], s_cnt[threadIdx.x]);
-    if (threadIdx.x < kBuckets * 3 && s_mom[threadIdx.x]) atomicAdd(&moments[threadIdx.x], s_mom[threadIdx.x]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
 }
 
-__global__ void k_bucket_offsets(const int *__restrict__ cnt, int *__restrict__ off, int *__restrict__ fill)
+// status: -1 informed (not kriged), 1 no neighbours, 3 queued for a solve.
+// tile_cnt[q * T + tile] = cells of bucket q in the tile; tile_mom[(3q + e) * T + tile]
+// = sum of n^(e+1) over them.
+__global__ void __launch_bounds__(kTileThreads) k_prepare(const Geom g, const uint8_t *__restrict__ mask, int all_cells,
+                                                          const int *__restrict__ nb_n, signed char *__restrict__ status,
+                                                          int *__restrict__ tile_cnt,
+                                                          unsigned long long *__restrict__ tile_mom)
 {
+    const int T = gridDim.x;
+    const long long base = (long long)blockIdx.x * kTile;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int cnt[kBuckets];
+    unsigned long long mom[kBuckets * 3];
+#pragma unroll
+    for (int q = 0; q < kBuckets; ++q) cnt[q] = 0;
+#pragma unroll
+    for (int q = 0; q < kBuckets * 3; ++q) mom[q] = 0;
+    for (int it = 0; it < kTileIters; ++it)
+    {
+        const long long c = base + it * kTileThreads + threadIdx.x;
+        int b = -1, n = 0;
+        if (c < g.n_cells)
+        {
+            if (!all_cells && mask[c])
+                status[c] = -1;
+            else
+            {
+                n = nb_n[c];
+                b = bucket_of(n);
+                status[c] = b < 0 ? 1 : 3;
+            }
+        }
+        const unsigned long long nn = (unsigned long long)n;
+#pragma unroll
+        for (int q = 0; q < kBuckets; ++q)
+        {
+            cnt[q] += __popc(__ballot_sync(0xffffffffu, b == q));
+            if (b == q)
+            {
+                mom[3 * q] += nn;
+                mom[3 * q + 1] += nn * nn;
+                mom[3 * q + 2] += nn * nn * nn;
+            }
+        }
+    }
+    __shared__ int s_cnt[kTileThreads / 32][kBuckets];
+    __shared__ unsigned long long s_mom[kTileThreads / 32][kBuckets * 3];
+#pragma unroll
+    for (int q = 0; q < kBuckets * 3; ++q)
+    {
+        const unsigned long long v = warp_sum_u64(mom[q]);
+        if (lane == 0) s_mom[warp][q] = v;
+    }
+    if (lane == 0)
+    {
+#pragma unroll
+        for (int q = 0; q < kBuckets; ++q) s_cnt[warp][q] = cnt[q];
+    }
+    __syncthreads();
+    if (threadIdx.x < kBuckets)
+    {
+        int v = 0;
+        for (int w = 0; w < kTileThreads / 32; ++w) v += s_cnt[w][threadIdx.x];
+        tile_cnt[threadIdx.x * T + blockIdx.x] = v;
+    }
+    else if (threadIdx.x >= 32 && threadIdx.x < 32 + kBuckets * 3)
+    {
+        const int q = threadIdx.x - 32;
+        unsigned long long v = 0;
+        for (int w = 0; w < kTileThreads / 32; ++w) v += s_mom[w][q];
+        tile_mom[q * T + blockIdx.x] = v;
+    }
+}
+
+// One block: exclusive scan of every bucket's tile counts (in place, as offsets
+// into the whole list), bucket totals and offsets, and the moments.
+__global__ void __launch_bounds__(1024) k_prepare_scan(int T, int *__restrict__ tile_cnt,
+                                                       const unsigned long long *__restrict__ tile_mom,
+                                                       int *__restrict__ bucket_cnt, int *__restrict__ bucket_off,
+                                                       unsigned long long *__restrict__ moments)
+{
+    __shared__ int s_part[1024];
+    __shared__ int s_total[kBuckets];
+    const int per = (T + blockDim.x - 1) / blockDim.x;
+    const int t0 = threadIdx.x * per, t1 = min(T, t0 + per);
+    for (int q = 0; q < kBuckets; ++q)
+    {
+        int *tc = tile_cnt + (long long)q * T;
+        int local = 0;
+        for (int t = t0; t < t1; ++t) local += tc[t];
+        s_part[threadIdx.x] = local;
+        __syncthreads();
+        // Hillis-Steele inclusive scan of the per-thread sums
+        for (int o = 1; o < (int)blockDim.x; o <<= 1)
+        {
+            const int v = threadIdx.x >= o ? s_part[threadIdx.x - o] : 0;
+            __syncthreads();
+            s_part[threadIdx.x] += v;
+            __syncthreads();
+        }
+        int run = s_part[threadIdx.x] - local;
+        for (int t = t0; t < t1; ++t)
+        {
+            const int c = tc[t];
+            tc[t] = run;
+            run += c;
+        }
+        if (threadIdx.x == blockDim.x - 1) s_total[q] = s_part[threadIdx.x];
+        __syncthreads();
+    }
     if (threadIdx.x == 0)
     {
         int run = 0;
-        for (int b = 0; b < kBuckets; ++b)
+        for (int q = 0; q < kBuckets; ++q)
         {
-            off[b] = run;
-            fill[b] = 0;
-            run += cnt[b];
+            bucket_cnt[q] = s_total[q];
+            bucket_off[q] = run;
+            run += s_total[q];
         }
-        off[kBuckets] = run;
+        bucket_off[kBuckets] = run;
+    }
+    if (threadIdx.x < kBuckets * 3)
+    {
+        unsigned long long v = 0;
+        for (int t = 0; t < T; ++t) v += tile_mom[(long long)threadIdx.x * T + t];
+        moments[threadIdx.x] = v;
     }
 }
 
-__global__ void k_bucket_fill(const Geom g, const signed char *__restrict__ status, const int *__restrict__ nb_n,
-                              const int *__restrict__ off, int *__restrict__ fill, int2 *__restrict__ cells)
+__global__ void __launch_bounds__(kTileThreads) k_bucket_fill(const Geom g, const signed char *__restrict__ status,
+                                                              const int *__restrict__ nb_n,
+                                                              const int *__restrict__ tile_off,
+                                                              const int *__restrict__ bucket_off,
+                                                              int2 *__restrict__ cells)
 {
-    const int lane = threadIdx.x & 31;
-    for (long long base = (long long)blockIdx.x * blockDim.x; base < g.n_cells;
-         base += (long long)gridDim.x * blockDim.x)
+    const int T = gridDim.x;
+    const long long base = (long long)blockIdx.x * kTile;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int W = kTileThreads / 32;
+    __shared__ int s_wc[W][kBuckets];
+    __shared__ int s_run[kBuckets];
+    if (threadIdx.x < kBuckets) s_run[threadIdx.x] = bucket_off[threadIdx.x] + tile_off[threadIdx.x * T + blockIdx.x];
+    unsigned lt;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+    for (int it = 0; it < kTileIters; ++it)
     {
-        long long c = base + threadIdx.x;
-        int b = -1, nn = 0;
+        const long long c = base + it * kTileThreads + threadIdx.x;
+        int b = -1, n = 0;
         if (c < g.n_cells && status[c] == 3)
         {
-            nn = nb_n[c];
-            b = bucket_of(nn);
+            n = nb_n[c];
+            b = bucket_of(n);
         }
-        // warp-aggregated append per bucket
+        unsigned my_bl = 0;
+#pragma unroll
         for (int q = 0; q < kBuckets; ++q)
         {
-            unsigned m = __ballot_sync(0xffffffffu, b == q);
-            if (!m) continue;
-            int leader = __ffs(m) - 1;
-            int start = 0;
-            if (lane == leader) start = atomicAdd(&fill[q], __popc(m));
-            start = __shfl_sync(0xffffffffu, start, leader);
-            if (b == q)
-            {
-                unsigned lt;
-                asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
-                cells[off[q] + start + __popc(m & lt)] = make_int2((int)c, nn);
-            }
+            const unsigned bl = __ballot_sync(0xffffffffu, b == q);
+            if (b == q) my_bl = bl;
+            if (lane == 0) s_wc[warp][q] = __popc(bl);
         }
+        __syncthreads();
+        if (b >= 0)
+        {
+            int off = s_run[b];
+            for (int w = 0; w < warp; ++w) off += s_wc[w][b];
+            cells[off + __popc(my_bl & lt)] = make_int2((int)c, n);
+        }
+        __syncthreads();
+        if (threadIdx.x < kBuckets)
+        {
+            int v = 0;
+            for (int w = 0; w < W; ++w) v += s_wc[w][threadIdx.x];
+            s_run[threadIdx.x] += v;
+        }
+        __syncthreads();
     }
 }
 
 void launch_prepare(const Geom &g, const uint8_t *mask, int all_cells, const int *nb_n, signed char *status,
-                    int *bucket_cnt, int *bucket_off, int *bucket_fill, int2 *cells,
+                    int *bucket_cnt, int *bucket_off, int *tile_cnt, unsigned long long *tile_mom, int2 *cells,
                     unsigned long long *moments, cudaStream_t st)
 {
-    cudaMemsetAsync(bucket_cnt, 0, sizeof(int) * kBuckets, st);
-    cudaMemsetAsync(moments, 0, sizeof(unsigned long long) * kBuckets * 3, st);
-    k_prepare<<<1184, 256, 0, st>>>(g, mask, all_cells, nb_n, status, bucket_cnt, moments);
-    k_bucket_offsets<<<1, 32, 0, st>>>(bucket_cnt, bucket_off, bucket_fill);
-    k_bucket_fill<<<1184, 256, 0, st>>>(g, status, nb_n, bucket_off, bucket_fill, cells);
+    const int T = (int)prepare_tiles(g.n_cells);
+    k_prepare<<<T, kTileThreads, 0, st>>>(g, mask, all_cells, nb_n, status, tile_cnt, tile_mom);
+    k_prepare_scan<<<1, 1024, 0, st>>>(T, tile_cnt, tile_mom, bucket_cnt, bucket_off, moments);
+    k_bucket_fill<<<T, kTileThreads, 0, st>>>(g, status, nb_n, tile_cnt, bucket_off, cells);
 }
 
 // ------------------------------------------------------------- finalize
