@@ -678,7 +678,7 @@ struct FoldSmem
     static constexpr size_t x_off = (lin_off + NP * sizeof(int) + 15) / 16 * 16;
     // Systems sharing a warp sit 4 G bytes apart modulo 128, so the G words each
     // writes per step, and the rows they broadcast, fall on disjoint banks.
-    static constexpr size_t bytes = (x_off + 2 * NP * sizeof(double) + 127) / 128 * 128 + 4 * (NP / 2);
+    static constexpr size_t bytes = (x_off + (size_t)R * NP * sizeof(double) + 127) / 128 * 128 + 4 * (NP / 2);
 };
 
 template <int G>
@@ -883,8 +883,80 @@ __device__ __forceinline__ void fold_residuals(const FoldGrp<NP / 2> &fg, const 
     fg.sync();
 }
 
+// The bilinear forms x_u^T A64 x_w of the dual-weighted correction, from the
+// lower triangle only: for symmetric A,
+//   x_u^T A x_w = sum_r ( A_rr u_r w_r + u_r P_w(r) + w_r P_u(r) ),
+//   P_w(r) = sum_{c<r} A_rc w_c,
+// so each lane gathers the entries of its two rows left of the diagonal (P)
+// and the diagonal (D) from the double pair table: one gather per entry of the
+// triangle instead of one per entry of the matrix. X receives the R solution
+// vectors of all rows.
+template <int NP, int R>
+__device__ __forceinline__ void fold_bilinear(const FoldGrp<NP / 2> &fg, const double *__restrict__ pair64,
+                                              long long pc, const int *LIN, double *X, int n, int t, int lin_a,
+                                              int lin_b, bool live_a, bool live_b, const double (&xa)[R],
+                                              const double (&xb)[R], double (&Pa)[R], double (&Pb)[R], double &Da,
+                                              double &Db)
+{
+    constexpr int G = NP / 2;
+    const int rb = NP - 1 - t;
+#pragma unroll
+    for (int q = 0; q < R; ++q)
+    {
+        X[q * NP + t] = xa[q];
+        X[q * NP + rb] = xb[q];
+        Pa[q] = 0.0;
+        Pb[q] = 0.0;
+    }
+    Da = 0.0;
+    Db = 0.0;
+    fg.sync();
+    const double *base_a = pair64 + pc + lin_a, *base_b = pair64 + pc + lin_b;
+#pragma unroll
+    for (int c = 0; c < NP; ++c)
+    {
+        if (c < n)
+        {
+            const int l = LIN[c];
+            double xc[R];
+#pragma unroll
+            for (int q = 0; q < R; ++q) xc[q] = X[q * NP + c];
+            if (c < G && live_a && c <= t)
+            {
+                const double p = __ldg(base_a - l);
+                if (c < t)
+                {
+#pragma unroll
+                    for (int q = 0; q < R; ++q) Pa[q] += p * xc[q];
+                }
+                else
+                    Da = p;
+            }
+            if (live_b && c <= rb)
+            {
+                const double p = __ldg(base_b - l);
+                if (c < rb)
+                {
+#pragma unroll
+                    for (int q = 0; q < R; ++q) Pb[q] += p * xc[q];
+                }
+                else
+                    Db = p;
+            }
+        }
+    }
+    fg.sync();
+}
+
+// Threads per block of the folded kernel: one block of 512 per SM (registers
+// capped at 128), so all the systems in flight on an SM come from one run of
+// neighbouring cells.
+#ifndef HB_FOLD_THREADS
+#define HB_FOLD_THREADS 512
+#endif
+
 template <int NP, bool ORDINARY>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(HB_FOLD_THREADS, 512 / HB_FOLD_THREADS)
     k_solve_fold(const Geom g, const int2 *__restrict__ cells, const int *__restrict__ n_items_ptr,
                  const int2 *__restrict__ nb_rec, int ind_value, const float *__restrict__ pair32, SolveParams P)
 {
@@ -917,9 +989,8 @@ __global__ void __launch_bounds__(256, 2)
     const int run_end = min(n_items, run_first + per_block);
     const int wstride = nwarps * SPW;
     int base = run_first + warp * SPW;
-    auto work_at = [&](int it) { return it < run_end ? cells[it] : make_int2(0, 0); };
-    int2 w_cur = work_at(base + h);
-    int2 w_nxt = work_at(base + wstride + h);
+    int2 w_cur = base + h < run_end ? cells[base + h] : make_int2(0, 0);
+    int2 w_nxt = base + wstride + h < run_end ? cells[base + wstride + h] : make_int2(0, 0);
     int2 rec_a = t < w_cur.y ? nb_rec[(long long)w_cur.x * g.k + t] : make_int2(0, 0);
     int2 rec_b = rb < w_cur.y ? nb_rec[(long long)w_cur.x * g.k + rb] : make_int2(0, 0);
     for (; base < run_end; base += wstride)
@@ -934,7 +1005,7 @@ __global__ void __launch_bounds__(256, 2)
         rec_a = t < w_nxt.y ? nb_rec[(long long)w_nxt.x * g.k + t] : make_int2(0, 0);
         rec_b = rb < w_nxt.y ? nb_rec[(long long)w_nxt.x * g.k + rb] : make_int2(0, 0);
         w_cur = w_nxt;
-        w_nxt = work_at(base + 2 * wstride + h);
+        w_nxt = base + 2 * wstride + h < run_end ? cells[base + 2 * wstride + h] : make_int2(0, 0);
         LIN[t] = live_a ? lin_a : 0;
         LIN[rb] = live_b ? lin_b : 0;
         fg.sync();
@@ -1070,19 +1141,25 @@ __global__ void __launch_bounds__(256, 2)
             xqa[q] = xa[q];
             xqb[q] = xb[q];
         }
-        fold_residuals<NP, QB>(fg, pair64, pc, LIN, X, my_n, t, lin_a, lin_b, live_a, live_b, xqa, xqb, r64a, r64b,
-                               resa, resb);
-        // u^T A^-1 w = u^T x_w + x_u^T (w - A64 x_w) + O(|e_u| |e_w|)
-        const double corr_vb = xa[R - 1] * resa[0] + xb[R - 1] * resb[0];
-        const double corr_bb = xa[0] * resa[0] + xb[0] * resb[0];
+        // u^T A^-1 w = u^T x_w + x_u^T w - x_u^T A64 x_w + O(|e_u| |e_w|); solution
+        // q: 0 = x_b, 1 = x_1 (OK), R-1 = x_v
+        double Pa[R], Pb[R], Da, Db;
+        fold_bilinear<NP, R>(fg, pair64, pc, LIN, X, my_n, t, lin_a, lin_b, live_a, live_b, xa, xb, Pa, Pb, Da, Db);
+        auto bil = [&](int u, int w) {
+            return Da * xa[u] * xa[w] + xa[u] * Pa[w] + xa[w] * Pa[u] + Db * xb[u] * xb[w] + xb[u] * Pb[w] +
+                   xb[w] * Pb[u];
+        };
+        constexpr int V = R - 1;
+        const double corr_vb = xa[V] * b64_a + xb[V] * b64_b - bil(V, 0);
+        const double corr_bb = xa[0] * b64_a + xb[0] * b64_b - bil(0, 0);
         double f_vb = vc_a * xa[0] + vc_b * xb[0] + corr_vb;
         double f_bb = b64_a * xa[0] + b64_b * xb[0] + corr_bb;
         double f_1b = 0.0, f_v1 = 0.0, f_11 = 0.0;
         if constexpr (ORDINARY)
         {
-            f_1b = one_a * xa[0] + one_b * xb[0] + xa[1] * resa[0] + xb[1] * resb[0];
-            f_v1 = vc_a * xa[1] + vc_b * xb[1] + xa[R - 1] * resa[1] + xb[R - 1] * resb[1];
-            f_11 = one_a * xa[1] + one_b * xb[1] + xa[1] * resa[1] + xb[1] * resb[1];
+            f_1b = one_a * xa[0] + one_b * xb[0] + xa[1] * b64_a + xb[1] * b64_b - bil(1, 0);
+            f_v1 = vc_a * xa[1] + vc_b * xb[1] + xa[V] * one_a + xb[V] * one_b - bil(V, 1);
+            f_11 = one_a * xa[1] + one_b * xb[1] + xa[1] * one_a + xb[1] * one_b - bil(1, 1);
         }
         double s_vb = fg.sum(f_vb), s_bb = fg.sum(f_bb);
         double s_1b = 0.0, s_v1 = 0.0, s_11 = 0.0;
@@ -1209,9 +1286,8 @@ __global__ void __launch_bounds__(256, 2)
 }
 
 template <typename K>
-static cudaError_t launch_kernel(K kern, size_t smem, int max_items, int gpb, int n_sm, cudaStream_t st, int &blocks_out)
+static cudaError_t launch_kernel(K kern, int threads, size_t smem, int max_items, int gpb, int n_sm, int &blocks_out)
 {
-    constexpr int threads = 256;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
@@ -1236,18 +1312,19 @@ static cudaError_t launch_one(const Geom &g, const int2 *cells, const int *n_ite
     int blocks = 0;
     if constexpr (FOLD)
     {
-        constexpr int spb = threads / (NP / 2); // systems per block
+        constexpr int fthreads = HB_FOLD_THREADS;
+        constexpr int spb = fthreads / (NP / 2); // systems per block
         const size_t smem = FoldSmem<NP, ORD ? 3 : 2>::bytes * spb;
         auto kern = k_solve_fold<NP, ORD>;
-        cudaError_t e = launch_kernel(kern, smem, max_items, spb, n_sm, st, blocks);
+        cudaError_t e = launch_kernel(kern, fthreads, smem, max_items, spb, n_sm, blocks);
         if (e != cudaSuccess) return e;
-        kern<<<(unsigned)blocks, threads, smem, st>>>(g, cells, n_items, nb_rec, ind_value, pair32, P);
+        kern<<<(unsigned)blocks, fthreads, smem, st>>>(g, cells, n_items, nb_rec, ind_value, pair32, P);
     }
     else
     {
         const size_t smem = SolveSmem<NP, TF, REF, ORD ? 3 : 2>::bytes * gpb;
         auto kern = k_solve<NP, TF, ORD, REF>;
-        cudaError_t e = launch_kernel(kern, smem, max_items, gpb, n_sm, st, blocks);
+        cudaError_t e = launch_kernel(kern, threads, smem, max_items, gpb, n_sm, blocks);
         if (e != cudaSuccess) return e;
         kern<<<(unsigned)blocks, threads, smem, st>>>(g, cells, n_items, nb_rec, ind_value, pair32, P);
     }
