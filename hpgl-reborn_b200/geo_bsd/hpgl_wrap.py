@@ -77,6 +77,9 @@ FLAG_EXACT_SEARCH = 4
 LIB_NAME = "libhpgl_b200.so"
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 
+# Status codes of the _ex / b200 entry points (include/hpgl_b200.h)
+OK, EINVAL, ECUDA, ENOMEM, ELIMIT = 0, -1, -2, -3, -4
+
 # Exported symbols of include/hpgl_b200.h (checked by the test suite).
 EXPORTS = [
     "hpgl_get_last_exception_message", "hpgl_set_output_handler", "hpgl_set_progress_handler",
@@ -85,7 +88,7 @@ EXPORTS = [
     "hpgl_b200_cont_kriging_ex", "hpgl_b200_indicator_kriging_ex", "hpgl_b200_median_ik_ex",
     "hpgl_b200_find_neighbours", "hpgl_b200_last_stats", "hpgl_b200_host_alloc", "hpgl_b200_host_free",
     "hpgl_b200_transform", "hpgl_b200_template", "hpgl_b200_covariance", "hpgl_b200_version",
-    "hpgl_b200_sk_weights_noalloc",
+    "hpgl_b200_sk_weights_noalloc", "hpgl_b200_loo_ok", "hpgl_b200_loo_ok_adjoint",
 ]
 
 
@@ -153,6 +156,13 @@ def _load():
     lib.hpgl_b200_sk_weights_noalloc.restype = C.c_int
     lib.hpgl_b200_sk_weights_noalloc.argtypes = [C.POINTER(C.c_float), _f32, _f32, _f32, C.c_int,
                                                  C.POINTER(_HPGL_COV_PARAMS), _f32, C.c_void_p]
+    vp = C.c_void_p
+    d9 = C.POINTER(C.c_double)
+    loo_common = [vp, vp, C.c_int, vp, vp, vp, C.c_int, C.c_int, C.c_int, d9, C.c_double, C.c_double, C.c_double]
+    lib.hpgl_b200_loo_ok.restype = C.c_int
+    lib.hpgl_b200_loo_ok.argtypes = loo_common + [vp, vp, vp]
+    lib.hpgl_b200_loo_ok_adjoint.restype = C.c_int
+    lib.hpgl_b200_loo_ok_adjoint.argtypes = loo_common + [vp, vp, vp, vp]
     return lib
 
 

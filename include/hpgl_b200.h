@@ -185,6 +185,30 @@ int hpgl_b200_sk_weights_noalloc(const float *center_coords, const float *neighb
                                  const float *neighbours_z, int neighbours_count,
                                  const struct hpgl_cov_params_t *params, float *weights, void *stream);
 
+/* Leave-one-out ordinary kriging of conditioning points, and its adjoint. No
+ * counterpart in the reference (HPGL has no cross-validation and computes no
+ * gradients); the system of each target is the reference's OK system
+ * (ok_kriging_weights_3, my_kriging_weights.h:198-361) in FP64, its covariance
+ * evaluated from M = diag(1/r0, 1/r1, 1/r2) Rx Ry Rz, the anisotropy transform of
+ * cov_model.h:16-61 divided by ranges[0] (row-major, host pointer to 9 doubles),
+ * with C = sill where r0 |M v| < 1e-4 (cov_model.h:146-183).
+ *   pts_xyz  [n_pts][3] int grid coordinates, values [n_pts] (device)
+ *   targets  [n_targets] point ids; nb_idx [n_targets][k] neighbour point ids
+ *            (the target itself excluded), nb_cnt [n_targets] (device); k <= 32
+ *   zhat     [n_targets] estimates; status (optional) 0 kriged, 1 no
+ *            neighbours, 2 singular (estimate 0)
+ * The adjoint takes dL/dzhat and ADDS dL/dvalues to grad_values [n_pts] and
+ * dL/dM (9, row-major), dL/dsill, dL/dnugget to grad_params [11]; it recomputes
+ * the factors, and targets with status != 0 contribute nothing. Device
+ * pointers, work queued on `stream`. */
+int hpgl_b200_loo_ok(const int *pts_xyz, const double *values, int n_pts, const int *targets, const int *nb_idx,
+                     const int *nb_cnt, int n_targets, int k, int cov_type, const double *M, double r0, double sill,
+                     double nugget, double *zhat, signed char *status, void *stream);
+int hpgl_b200_loo_ok_adjoint(const int *pts_xyz, const double *values, int n_pts, const int *targets,
+                             const int *nb_idx, const int *nb_cnt, int n_targets, int k, int cov_type,
+                             const double *M, double r0, double sill, double nugget, const double *grad_zhat,
+                             double *grad_values, double *grad_params, void *stream);
+
 /* Page-locked host buffers for fast copies (cudaHostAlloc / cudaFreeHost). */
 void *hpgl_b200_host_alloc(size_t bytes);
 void hpgl_b200_host_free(void *p);
