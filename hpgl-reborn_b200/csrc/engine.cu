@@ -388,6 +388,7 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
     int *bin_fill = E.buf<int>("bin_fill", g.n_bins);
     S.bin_flag = E.buf<uint8_t>("bin_flag", g.n_bins);
     int *bin_pts = E.buf<int>("bin_pts", std::max(P.m, 1));
+    int *tmpl_bins = E.buf<int>("tmpl_bins", g.n_bins);
     int *scal = E.buf<int>("scalars", 8); // 0 total, 1 max_cand, 2 tmpl bins, 3 ties, 4 tmpl cells, 5 exact cells
     int *tmp = E.buf<int>("scan_tmp2", (size_t)scan_tmp_ints(g.n_bins) + 4);
     HB_CK(cudaMemsetAsync(bin_cnt, 0, sizeof(int) * g.n_bins, st));
@@ -398,13 +399,14 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
     exclusive_scan(bin_start, g.n_bins, tmp, scal + 0, st);
     launch_bin_fill(P.pts_xyz, P.n_pts, g, bin_start, bin_fill, bin_pts, st);
     launch_bin_sort(g, bin_start, bin_cnt, bin_pts, S.bin_flag, st);
-    launch_bin_region(g, S.bin_flag, bin_cnt, scal + 1, scal + 2, st);
+    launch_bin_region(g, S.bin_flag, bin_cnt, scal + 1, scal + 2, tmpl_bins, st);
     HB_CK(cudaGetLastError());
     int host_scal[8];
     HB_CK(cudaMemcpyAsync(host_scal, scal, sizeof(host_scal), cudaMemcpyDeviceToHost, st));
     HB_CK(cudaStreamSynchronize(st));
     E.mark(STAGE_BINS, st);
     int max_cand = host_scal[1];
+    const int n_tmpl_bins = host_scal[2];
     // the sorted template, only when some bin takes the template path
     int n_tmpl = 0;
     int4 *tmpl = E.buf<int4>("tmpl", std::max<long>(pl.tmpl_count, 1));
@@ -443,6 +445,8 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
         HB_CK(launch_search(g, d_mask, all_cells, bin_start, bin_cnt, S.bin_flag, bin_pts, P.pts_xyz, P.pts_val,
                             keytab, pl.rank_bits, tmpl, n_tmpl, P.pid_of_node, cand_cap, warps,
                             S.nb_pid, S.nb_rec, S.nb_n, tie_cells, scal + 3, scal + 4, st));
+    HB_CK(launch_search_template(g, d_mask, all_cells, tmpl_bins, n_tmpl_bins, P.pts_val, tmpl, n_tmpl,
+                                 P.pid_of_node, S.nb_pid, S.nb_rec, S.nb_n, scal + 4, E.n_sm(), st));
     HB_CK(cudaEventRecord(E.ev_[9], st));
     HB_CK(cudaMemcpyAsync(host_scal, scal, sizeof(host_scal), cudaMemcpyDeviceToHost, st));
     HB_CK(cudaStreamSynchronize(st));
@@ -457,7 +461,7 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
         E.stats.search_kernel_ms += ms;
     }
     // flag, scan tiles (+add), emit, pair table, bin count, bin scan, fill, sort, region, search
-    E.stats.launches += 10 + (g.n_cells > 1024 ? 2 : 0);
+    E.stats.launches += 10 + (g.n_cells > 1024 ? 2 : 0) + (n_tmpl_bins > 0 ? 1 : 0);
 
     // tie groups straddling the k-th slot: std::sort's choice, replayed
     if (S.ties > 0)

@@ -44,7 +44,11 @@ void launch_bin_fill(const unsigned long long *pts_xyz, const int *n_pts, const 
 void launch_bin_sort(const Geom &g, const int *bin_start, const int *bin_cnt, int *bin_pts, uint8_t *bin_flag,
                      cudaStream_t st);
 void launch_bin_region(const Geom &g, uint8_t *bin_flag, const int *bin_cnt, int *max_cand, int *n_tmpl_bins,
-                       cudaStream_t st);
+                       int *tmpl_bins, cudaStream_t st);
+cudaError_t launch_search_template(const Geom &g, const uint8_t *mask, int all_cells, const int *tmpl_bins,
+                                   int n_tmpl_bins, const float *pts_vf, const int4 *tmpl, int n_tmpl,
+                                   const int *pid_of_node, int *nb_pid, int2 *nb_rec, int *nb_n,
+                                   int *n_template_cells, int n_sm, cudaStream_t st);
 size_t search_smem_bytes(int cand_cap, int k, int warps);
 cudaError_t launch_search(const Geom &g, const uint8_t *mask, int all_cells, const int *bin_start,
                           const int *bin_cnt, const uint8_t *bin_flag, const int *bin_pts,

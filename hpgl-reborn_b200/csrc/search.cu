@@ -19,6 +19,8 @@
 //   5. k_resolve_ties: one thread per queued cell rebuilds the filtered
 //      candidate list and runs the introsort restatement (gnu_introsort.h),
 //      which reproduces std::sort's permutation, then takes the first k.
+#include <algorithm>
+
 #include "engine.cuh"
 #include "gnu_introsort.h"
 #include "kernels.h"
@@ -211,7 +213,8 @@ __global__ void k_bin_sort(Geom g, const int *__restrict__ bin_start, const int 
 
 // bit 1: the cells of this bin take the template path
 __global__ void k_bin_region(Geom g, uint8_t *__restrict__ bin_flag, const int *__restrict__ bin_cnt,
-                             int *__restrict__ max_cand, int *__restrict__ n_template_bins)
+                             int *__restrict__ max_cand, int *__restrict__ n_template_bins,
+                             int *__restrict__ template_bins)
 {
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < g.n_bins; b += gridDim.x * blockDim.x)
     {
@@ -230,7 +233,7 @@ __global__ void k_bin_region(Geom g, uint8_t *__restrict__ bin_flag, const int *
         if (tmpl)
         {
             bin_flag[b] |= 2;
-            atomicAdd(n_template_bins, 1);
+            template_bins[atomicAdd(n_template_bins, 1)] = b;
         }
         else
             atomicMax(max_cand, cand);
@@ -453,12 +456,7 @@ __global__ void __launch_bounds__(256) k_search(
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const int k = g.k;
 
-    if (bin_flag[b] & 2)
-    {
-        template_cells(g, mask, all_cells, x0, y0, z0, wx, wy, n_cells_bin, warp, nwarps, lane, pts_vf, tmpl, n_tmpl,
-                       pid_of_node, nb_pid, nb_rec, nb_n, n_template_cells);
-        return;
-    }
+    if (bin_flag[b] & 2) return; // k_search_template
 
     // ---------------- cluster path
     int *cx = reinterpret_cast<int *>(smem);
@@ -826,12 +824,7 @@ __global__ void __launch_bounds__(256) k_search_fast(
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const int k = g.k;
 
-    if (bin_flag[b] & 2)
-    {
-        template_cells(g, mask, all_cells, x0, y0, z0, wx, wy, n_cells_bin, warp, nwarps, lane, pts_vf, tmpl,
-                       n_tmpl, pid_of_node, nb_pid, nb_rec, nb_n, n_template_cells);
-        return;
-    }
+    if (bin_flag[b] & 2) return; // k_search_template
 
     float4 *ctp = reinterpret_cast<float4 *>(smem);
     int *cklin = reinterpret_cast<int *>(ctp + cand_cap);
@@ -1193,10 +1186,47 @@ void launch_bin_sort(const Geom &g, const int *bin_start, const int *bin_cnt, in
     k_bin_sort<<<blocks, 256, 0, st>>>(g, bin_start, bin_cnt, bin_pts, bin_flag);
 }
 void launch_bin_region(const Geom &g, uint8_t *bin_flag, const int *bin_cnt, int *max_cand, int *n_tmpl_bins,
-                       cudaStream_t st)
+                       int *tmpl_bins, cudaStream_t st)
 {
     int blocks = (g.n_bins + 255) / 256;
-    k_bin_region<<<blocks, 256, 0, st>>>(g, bin_flag, bin_cnt, max_cand, n_tmpl_bins);
+    k_bin_region<<<blocks, 256, 0, st>>>(g, bin_flag, bin_cnt, max_cand, n_tmpl_bins, tmpl_bins);
+}
+
+// Template-path cells (k_search and k_search_fast leave their bins alone): a
+// grid of (template bins) x (slices), each warp scanning the sorted template
+// for one cell at a time, so the few bins that take this path (those around an
+// overflowing bin) are spread over the whole GPU.
+__global__ void __launch_bounds__(256) k_search_template(
+    const Geom g, const uint8_t *__restrict__ mask, int all_cells, const int *__restrict__ template_bins,
+    const float *__restrict__ pts_vf, const int4 *__restrict__ tmpl, int n_tmpl, const int *__restrict__ pid_of_node,
+    int *__restrict__ nb_pid, int2 *__restrict__ nb_rec, int *__restrict__ nb_n, int *__restrict__ n_template_cells)
+{
+    const int b = template_bins[blockIdx.x];
+    const int bxi = b % g.bx, byi = (b / g.bx) % g.by, bzi = b / (g.bx * g.by);
+    const int x0 = bxi * g.rx, y0 = byi * g.ry, z0 = bzi * g.rz;
+    if (x0 >= g.nx || y0 >= g.ny || z0 >= g.nz) return;
+    const int wx = min(x0 + g.rx, g.nx) - x0, wy = min(y0 + g.ry, g.ny) - y0, wz = min(z0 + g.rz, g.nz) - z0;
+    const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    const int warp = blockIdx.y * nwarps + (threadIdx.x >> 5);
+    template_cells(g, mask, all_cells, x0, y0, z0, wx, wy, wx * wy * wz, warp, nwarps * gridDim.y, lane, pts_vf, tmpl,
+                   n_tmpl, pid_of_node, nb_pid, nb_rec, nb_n, n_template_cells);
+}
+
+cudaError_t launch_search_template(const Geom &g, const uint8_t *mask, int all_cells, const int *tmpl_bins,
+                                   int n_tmpl_bins, const float *pts_vf, const int4 *tmpl, int n_tmpl,
+                                   const int *pid_of_node, int *nb_pid, int2 *nb_rec, int *nb_n,
+                                   int *n_template_cells, int n_sm, cudaStream_t st)
+{
+    if (n_tmpl_bins <= 0) return cudaSuccess;
+    // about four waves of 256-thread blocks, at most one warp per 32 cells of a bin
+    const long long cells = (long long)g.rx * g.ry * g.rz;
+    long long split = ((long long)4 * n_sm * 8 + n_tmpl_bins - 1) / n_tmpl_bins;
+    split = std::min(split, std::max(1LL, cells / (8 * 32)));
+    split = std::max(1LL, std::min(split, 65535LL));
+    dim3 grid((unsigned)n_tmpl_bins, (unsigned)split);
+    k_search_template<<<grid, 256, 0, st>>>(g, mask, all_cells, tmpl_bins, pts_vf, tmpl, n_tmpl, pid_of_node, nb_pid,
+                                            nb_rec, nb_n, n_template_cells);
+    return cudaGetLastError();
 }
 
 size_t search_smem_bytes(int cand_cap, int k, int warps)
