@@ -659,7 +659,7 @@ __global__ void __launch_bounds__(256, 1)
 }
 
 // ------------------------------------------------------------------ folded
-// FP32-refined systems of up to 32 neighbours, folded: a system is solved by
+// FP32-refined systems of up to 64 neighbours, folded: a system is solved by
 // G = NP / 2 lanes and lane t owns rows t ("row a", columns 0..t) and
 // NP - 1 - t ("row b", columns 0..NP-1-t), so every lane holds NP + 1 entries
 // of the lower triangle and a warp solves 32 / G systems at once. Each step of
@@ -955,8 +955,21 @@ __device__ __forceinline__ void fold_bilinear(const FoldGrp<NP / 2> &fg, const d
 #define HB_FOLD_THREADS 512
 #endif
 
+// Systems of 33 to 64 neighbours fold onto one warp each (two rows of up to 64
+// entries per lane): 256-thread blocks, up to 255 registers.
+template <int NP>
+constexpr int fold_threads()
+{
+    return NP <= 32 ? HB_FOLD_THREADS : 256;
+}
+template <int NP>
+constexpr int fold_min_blocks()
+{
+    return NP <= 32 ? 512 / HB_FOLD_THREADS : 1;
+}
+
 template <int NP, bool ORDINARY>
-__global__ void __launch_bounds__(HB_FOLD_THREADS, 512 / HB_FOLD_THREADS)
+__global__ void __launch_bounds__(fold_threads<NP>(), fold_min_blocks<NP>())
     k_solve_fold(const Geom g, const int2 *__restrict__ cells, const int *__restrict__ n_items_ptr,
                  const int2 *__restrict__ nb_rec, int ind_value, const float *__restrict__ pair32, SolveParams P)
 {
@@ -1308,11 +1321,11 @@ static cudaError_t launch_one(const Geom &g, const int2 *cells, const int *n_ite
 {
     constexpr int threads = 256;
     constexpr int gpb = threads / NP;
-    constexpr bool FOLD = REF && NP <= 32;
+    constexpr bool FOLD = REF;
     int blocks = 0;
     if constexpr (FOLD)
     {
-        constexpr int fthreads = HB_FOLD_THREADS;
+        constexpr int fthreads = fold_threads<NP>();
         constexpr int spb = fthreads / (NP / 2); // systems per block
         const size_t smem = FoldSmem<NP, ORD ? 3 : 2>::bytes * spb;
         auto kern = k_solve_fold<NP, ORD>;
