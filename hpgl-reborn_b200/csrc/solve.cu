@@ -1298,6 +1298,228 @@ __global__ void __launch_bounds__(fold_threads<NP>(), fold_min_blocks<NP>())
     }
 }
 
+// FP64-plain systems of up to 32 neighbours, folded like k_solve_fold (G = NP/2
+// lanes per system, lane t owning rows t and NP-1-t). FP64 plain needs only the
+// forward substitution: every kriging quantity is a bilinear form
+// u^T A^-1 w = (L^-1 u) . (L^-1 w) of b, (OK) the ones vector and v - mean, so the
+// forward solutions that ride in the factorisation's broadcast rows are summed
+// directly; there is no back substitution and no residual.
+template <int NP>
+struct Fold64Smem
+{
+    static constexpr int LD = NP + 4; // doubles: NP entries, then up to 4 right-hand sides
+    static constexpr size_t m_bytes = (size_t)NP * LD * sizeof(double);
+    static constexpr size_t lin_off = m_bytes;
+    // systems sharing a warp 16 bytes apart modulo 128: their broadcast rows on different banks
+    static constexpr size_t bytes = (lin_off + NP * sizeof(int) + 127) / 128 * 128 + 16;
+};
+
+template <int NP, bool ORDINARY>
+__global__ void __launch_bounds__(256, 1)
+    k_solve_fold64(const Geom g, const int2 *__restrict__ cells, const int *__restrict__ n_items_ptr,
+                   const int2 *__restrict__ nb_rec, int ind_value, SolveParams P)
+{
+    constexpr int G = NP / 2;
+    constexpr int SPW = 32 / G;
+    constexpr int QB = ORDINARY ? 2 : 1;
+    constexpr int R = QB + 1;
+    typedef Fold64Smem<NP> SM;
+    constexpr int LD = SM::LD;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int h = lane / G;
+    const int t = lane % G;
+    const int rb = NP - 1 - t;
+    FoldGrp<G> fg;
+    fg.mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (h * G));
+    unsigned char *gb = smem + SM::bytes * (warp * SPW + h);
+    double *M = reinterpret_cast<double *>(gb);
+    int *LIN = reinterpret_cast<int *>(gb + SM::lin_off);
+    const long long pc = P.pc;
+    const double *pair64 = P.pair64;
+
+    const int n_items = *n_items_ptr;
+    const int per_block = (n_items + gridDim.x - 1) / gridDim.x;
+    const int run_first = blockIdx.x * per_block;
+    const int run_end = min(n_items, run_first + per_block);
+    const int wstride = nwarps * SPW;
+    int base = run_first + warp * SPW;
+    int2 w_cur = base + h < run_end ? cells[base + h] : make_int2(0, 0);
+    int2 w_nxt = base + wstride + h < run_end ? cells[base + wstride + h] : make_int2(0, 0);
+    int2 rec_a = t < w_cur.y ? nb_rec[(long long)w_cur.x * g.k + t] : make_int2(0, 0);
+    int2 rec_b = rb < w_cur.y ? nb_rec[(long long)w_cur.x * g.k + rb] : make_int2(0, 0);
+    for (; base < run_end; base += wstride)
+    {
+        const bool valid = base + h < run_end;
+        const int my_cell = w_cur.x, my_n = w_cur.y;
+        const bool live_a = t < my_n, live_b = rb < my_n;
+        const int lin_a = rec_a.x, lin_b = rec_b.x;
+        const double vc_a = centred_value(live_a, __int_as_float(rec_a.y), ind_value, P.mf);
+        const double vc_b = centred_value(live_b, __int_as_float(rec_b.y), ind_value, P.mf);
+        rec_a = t < w_nxt.y ? nb_rec[(long long)w_nxt.x * g.k + t] : make_int2(0, 0);
+        rec_b = rb < w_nxt.y ? nb_rec[(long long)w_nxt.x * g.k + rb] : make_int2(0, 0);
+        w_cur = w_nxt;
+        w_nxt = base + 2 * wstride + h < run_end ? cells[base + 2 * wstride + h] : make_int2(0, 0);
+        LIN[t] = live_a ? lin_a : 0;
+        LIN[rb] = live_b ? lin_b : 0;
+        fg.sync();
+
+        // ---- assembly (lower triangles of rows a and b; padding rows identity)
+        double ra[G], rbv[NP];
+        const double *base_a = pair64 + pc + lin_a, *base_b = pair64 + pc + lin_b;
+#pragma unroll
+        for (int c = 0; c < G; ++c)
+        {
+            double a = 0.0;
+            if (live_a && c <= t) a = __ldg(base_a - LIN[c]);
+            if (!live_a && c == t) a = 1.0;
+            ra[c] = a;
+        }
+#pragma unroll
+        for (int c = 0; c < NP; ++c)
+        {
+            double a = 0.0;
+            if (live_b && c <= rb) a = __ldg(base_b - LIN[c]);
+            if (!live_b && c == rb) a = 1.0;
+            rbv[c] = a;
+        }
+        const double b64_a = live_a ? __ldg(base_a) : 0.0;
+        const double b64_b = live_b ? __ldg(base_b) : 0.0;
+
+        // ---- factorisation with the forward substitution of b, 1 and v - mean
+        double rhs_a[R], rhs_b[R], ya[R], yb[R];
+        rhs_a[0] = b64_a;
+        rhs_b[0] = b64_b;
+        if constexpr (ORDINARY)
+        {
+            rhs_a[1] = live_a ? 1.0 : 0.0;
+            rhs_b[1] = live_b ? 1.0 : 0.0;
+        }
+        rhs_a[R - 1] = vc_a;
+        rhs_b[R - 1] = vc_b;
+#pragma unroll
+        for (int q = 0; q < R; ++q)
+        {
+            ya[q] = 0.0;
+            yb[q] = 0.0;
+        }
+        bool fail = false;
+#pragma unroll
+        for (int j = 0; j < NP; ++j)
+        {
+            if (j < G)
+            {
+                M[j * LD + t] = ra[j];
+                if (t == j)
+                {
+#pragma unroll
+                    for (int q = 0; q < R; ++q) M[j * LD + NP + q] = rhs_a[q];
+                }
+            }
+            M[j * LD + rb] = rbv[j];
+            if (j >= G && rb == j)
+            {
+#pragma unroll
+                for (int q = 0; q < R; ++q) M[j * LD + NP + q] = rhs_b[q];
+            }
+            fg.sync();
+            double mj[LD];
+            const double2 *mv = reinterpret_cast<const double2 *>(M + j * LD);
+#pragma unroll
+            for (int q = j / 2; q < LD / 2; ++q)
+            {
+                const double2 v2 = mv[q];
+                mj[2 * q] = v2.x;
+                mj[2 * q + 1] = v2.y;
+            }
+            const double d = mj[j];
+            fail |= !(d > 0.0);
+            const double inv_s = rsqrt(d);
+            const double inv2 = inv_s * inv_s;
+            if (j < G)
+            {
+                const double s = ra[j] * inv2;
+#pragma unroll
+                for (int c = j + 1; c < G; ++c) ra[c] -= s * mj[c];
+                if (t > j)
+                {
+#pragma unroll
+                    for (int q = 0; q < R; ++q) rhs_a[q] -= s * mj[NP + q];
+                }
+                ra[j] *= inv_s;
+                if (t == j)
+                {
+#pragma unroll
+                    for (int q = 0; q < R; ++q) ya[q] = rhs_a[q] * inv_s;
+                }
+            }
+            {
+                const double s = rbv[j] * inv2;
+#pragma unroll
+                for (int c = j + 1; c < NP; ++c) rbv[c] -= s * mj[c];
+                if (rb > j)
+                {
+#pragma unroll
+                    for (int q = 0; q < R; ++q) rhs_b[q] -= s * mj[NP + q];
+                }
+                rbv[j] *= inv_s;
+                if (rb == j)
+                {
+#pragma unroll
+                    for (int q = 0; q < R; ++q) yb[q] = rhs_b[q] * inv_s;
+                }
+            }
+        }
+
+        // ---- forms (L^-1 u) . (L^-1 w); q: 0 = b, 1 = ones (OK), R-1 = v - mean
+        constexpr int V = R - 1;
+        const double s_vb = fg.sum(ya[V] * ya[0] + yb[V] * yb[0]);
+        const double s_bb = fg.sum(ya[0] * ya[0] + yb[0] * yb[0]);
+        double s_1b = 0.0, s_v1 = 0.0, s_11 = 0.0;
+        if constexpr (ORDINARY)
+        {
+            s_1b = fg.sum(ya[1] * ya[0] + yb[1] * yb[0]);
+            s_v1 = fg.sum(ya[V] * ya[1] + yb[V] * yb[1]);
+            s_11 = fg.sum(ya[1] * ya[1] + yb[1] * yb[1]);
+        }
+        if (valid && t == 0)
+        {
+            // forms -> estimate and variance (my_kriging_weights.h:312-357)
+            const SolveOut &out = P.out;
+            double est, var;
+            bool bad = fail;
+            if constexpr (ORDINARY)
+            {
+                if (fabs(s_11) < 1e-15) bad = true;
+                const double mu = (s_1b - 1.0) / s_11;
+                est = s_vb - mu * s_v1;
+                var = P.c0 - s_bb + mu * s_1b - mu;
+            }
+            else
+            {
+                est = (double)P.mf + s_vb;
+                var = P.c0 - s_bb;
+            }
+            if (var < 0) var = 0;
+            if (!bad)
+            {
+                if (out.write_cont)
+                {
+                    out.out_data[my_cell] = (float)est;
+                    out.out_mask[my_cell] = 1;
+                }
+                if (out.prob) out.prob[(long long)my_cell * out.prob_stride] = (float)est;
+                if (out.est64) out.est64[my_cell] = est;
+                if (out.var) out.var[my_cell] = var;
+                if (out.status) out.status[my_cell] = 0;
+            }
+            else if (out.status)
+                out.status[my_cell] = 2;
+        }
+        fg.sync();
+    }
+}
+
 template <typename K>
 static cudaError_t launch_kernel(K kern, int threads, size_t smem, int max_items, int gpb, int n_sm, int &blocks_out)
 {
@@ -1332,6 +1554,15 @@ static cudaError_t launch_one(const Geom &g, const int2 *cells, const int *n_ite
         cudaError_t e = launch_kernel(kern, fthreads, smem, max_items, spb, n_sm, blocks);
         if (e != cudaSuccess) return e;
         kern<<<(unsigned)blocks, fthreads, smem, st>>>(g, cells, n_items, nb_rec, ind_value, pair32, P);
+    }
+    else if constexpr (!REF && NP <= 32)
+    {
+        constexpr int spb = 256 / (NP / 2); // systems per block
+        const size_t smem = Fold64Smem<NP>::bytes * spb;
+        auto kern = k_solve_fold64<NP, ORD>;
+        cudaError_t e = launch_kernel(kern, 256, smem, max_items, spb, n_sm, blocks);
+        if (e != cudaSuccess) return e;
+        kern<<<(unsigned)blocks, 256, smem, st>>>(g, cells, n_items, nb_rec, ind_value, P);
     }
     else
     {
