@@ -412,9 +412,15 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
     int4 *tmpl = E.buf<int4>("tmpl", std::max<long>(pl.tmpl_count, 1));
     if (host_scal[2] > 0 && pl.tmpl_count > 0)
     {
+        // the template probes a bitmap of the grid padded by the radiuses; its
+        // linear offsets are 32-bit
+        const long long PX = g.nx + 2LL * g.rx, PY = g.ny + 2LL * g.ry;
+        if ((long long)g.rz * PY * PX + (long long)g.ry * PX + g.rx > 2147483647LL)
+            throw CudaFail{-4, "grid too large for the template search path at these radiuses"};
         const std::vector<Offset> tv = build_template(pl.f, pl.kt);
         std::vector<int4> t4(tv.size());
-        for (size_t i = 0; i < tv.size(); ++i) t4[i] = make_int4(tv[i].dx, tv[i].dy, tv[i].dz, 0);
+        for (size_t i = 0; i < tv.size(); ++i)
+            t4[i] = make_int4(tv[i].dx, tv[i].dy, tv[i].dz, template_padded_offset(g, tv[i].dx, tv[i].dy, tv[i].dz));
         HB_CK(cudaMemcpyAsync(tmpl, t4.data(), t4.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
         HB_CK(cudaStreamSynchronize(st)); // t4 is a temporary
         n_tmpl = (int)tv.size();
@@ -445,8 +451,10 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
         HB_CK(launch_search(g, d_mask, all_cells, bin_start, bin_cnt, S.bin_flag, bin_pts, P.pts_xyz, P.pts_val,
                             keytab, pl.rank_bits, tmpl, n_tmpl, P.pid_of_node, cand_cap, warps,
                             S.nb_pid, S.nb_rec, S.nb_n, tie_cells, scal + 3, scal + 4, st));
-    HB_CK(launch_search_template(g, d_mask, all_cells, tmpl_bins, n_tmpl_bins, P.pts_val, tmpl, n_tmpl,
-                                 P.pid_of_node, S.nb_pid, S.nb_rec, S.nb_n, scal + 4, E.n_sm(), st));
+    if (n_tmpl_bins > 0)
+        HB_CK(launch_search_template(g, d_mask, E.buf<uint32_t>("mask_bits", (size_t)(template_padded_cells(g) + 31) / 32), all_cells,
+                                     tmpl_bins, n_tmpl_bins, P.pts_val, tmpl, n_tmpl, P.pid_of_node, S.nb_pid,
+                                     S.nb_rec, S.nb_n, scal + 4, E.n_sm(), st));
     HB_CK(cudaEventRecord(E.ev_[9], st));
     HB_CK(cudaMemcpyAsync(host_scal, scal, sizeof(host_scal), cudaMemcpyDeviceToHost, st));
     HB_CK(cudaStreamSynchronize(st));
@@ -461,7 +469,7 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
         E.stats.search_kernel_ms += ms;
     }
     // flag, scan tiles (+add), emit, pair table, bin count, bin scan, fill, sort, region, search
-    E.stats.launches += 10 + (g.n_cells > 1024 ? 2 : 0) + (n_tmpl_bins > 0 ? 1 : 0);
+    E.stats.launches += 10 + (g.n_cells > 1024 ? 2 : 0) + (n_tmpl_bins > 0 ? 2 : 0);
 
     // tie groups straddling the k-th slot: std::sort's choice, replayed
     if (S.ties > 0)

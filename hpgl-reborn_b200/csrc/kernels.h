@@ -45,9 +45,14 @@ void launch_bin_sort(const Geom &g, const int *bin_start, const int *bin_cnt, in
                      cudaStream_t st);
 void launch_bin_region(const Geom &g, uint8_t *bin_flag, const int *bin_cnt, int *max_cand, int *n_tmpl_bins,
                        int *tmpl_bins, cudaStream_t st);
-cudaError_t launch_search_template(const Geom &g, const uint8_t *mask, int all_cells, const int *tmpl_bins,
-                                   int n_tmpl_bins, const float *pts_vf, const int4 *tmpl, int n_tmpl,
-                                   const int *pid_of_node, int *nb_pid, int2 *nb_rec, int *nb_n,
+// Template-path search over a bitmap of the grid padded by the radiuses:
+// `bits` is scratch of (template_padded_cells + 31) / 32 words; template entries
+// carry template_padded_offset(dx, dy, dz) in .w.
+long long template_padded_cells(const Geom &g);
+int template_padded_offset(const Geom &g, int dx, int dy, int dz);
+cudaError_t launch_search_template(const Geom &g, const uint8_t *mask, uint32_t *bits, int all_cells,
+                                   const int *tmpl_bins, int n_tmpl_bins, const float *pts_vf, const int4 *tmpl,
+                                   int n_tmpl, const int *pid_of_node, int *nb_pid, int2 *nb_rec, int *nb_n,
                                    int *n_template_cells, int n_sm, cudaStream_t st);
 size_t search_smem_bytes(int cand_cap, int k, int warps);
 cudaError_t launch_search(const Geom &g, const uint8_t *mask, int all_cells, const int *bin_start,

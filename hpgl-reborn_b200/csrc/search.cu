@@ -391,13 +391,46 @@ __device__ int select_cell(const Geom &g, int x, int y, int z, int C, const int 
 
 // Template path (sugarbox_neighbour_lookup.h:171-197): one warp per cell walks the
 // sorted template 32 offsets at a time and keeps the first k informed nodes.
-__device__ void template_cells(const Geom &g, const uint8_t *__restrict__ mask, int all_cells, int x0, int y0, int z0,
-                               int wx, int wy, int n_cells_bin, int warp, int nwarps, int lane,
+// The informed cells as a bitmap over the grid padded by (hx, hy, hz) cells on
+// every side (padding bits 0): bit (q & 31) of word q >> 5 for the padded index
+// q = ((z + hz) PY + (y + hy)) PX + (x + hx), PX = nx + 2 hx, PY = ny + 2 hy.
+__global__ void k_mask_bits_padded(const Geom g, const uint8_t *__restrict__ mask, int hx, int hy, int hz,
+                                   long long n_padded, uint32_t *__restrict__ bits)
+{
+    const int lane = threadIdx.x & 31;
+    const long long PX = g.nx + 2LL * hx, PY = g.ny + 2LL * hy;
+    for (long long base = ((long long)blockIdx.x * blockDim.x + threadIdx.x) & ~31LL; base < n_padded;
+         base += (long long)gridDim.x * blockDim.x)
+    {
+        const long long q = base + lane;
+        bool inf = false;
+        if (q < n_padded)
+        {
+            const long long x = q % PX - hx, y = (q / PX) % PY - hy, z = q / (PX * PY) - hz;
+            if (x >= 0 && y >= 0 && z >= 0 && x < g.nx && y < g.ny && z < g.nz)
+                inf = mask[(z * g.ny + y) * g.nx + x] != 0;
+        }
+        const unsigned w = __ballot_sync(0xffffffffu, inf);
+        if (lane == 0) bits[base >> 5] = w;
+    }
+}
+
+// Template path (sugarbox_neighbour_lookup.h:171-197): walk the sorted template
+// and take the first k informed nodes. Template entries are {dx, dy, dz, padded
+// linear offset}; with the padded bitmap a probe needs no bounds check (offsets
+// reaching out of the grid land on padding). A warp tests 4 x 32 offsets per
+// round: the entries and bits of all four steps are loaded before the first is
+// consumed, then the steps are taken in order (the same first-k as the serial walk).
+__device__ void template_cells(const Geom &g, const uint32_t *__restrict__ bits, int hx, int hy, int hz,
+                               const uint8_t *__restrict__ mask, int all_cells, int x0, int y0, int z0, int wx,
+                               int wy, int n_cells_bin, int warp, int nwarps, int lane,
                                const float *__restrict__ pts_vf, const int4 *__restrict__ tmpl, int n_tmpl,
                                const int *__restrict__ pid_of_node, int *__restrict__ nb_pid,
                                int2 *__restrict__ nb_rec, int *__restrict__ nb_n, int *__restrict__ n_template_cells)
 {
+    constexpr int U = 4;
     const int k = g.k;
+    const long long PX = g.nx + 2LL * hx, PY = g.ny + 2LL * hy;
     int counted = 0;
     for (int c = warp; c < n_cells_bin; c += nwarps)
     {
@@ -405,32 +438,40 @@ __device__ void template_cells(const Geom &g, const uint8_t *__restrict__ mask, 
         long long cell = ((long long)z * g.ny + y) * g.nx + x;
         if (!all_cells && mask[cell]) continue;
         ++counted;
+        const long long qc = ((long long)(z + hz) * PY + (y + hy)) * PX + (x + hx);
         int found = 0;
-        for (int base = 0; base < n_tmpl && found < k; base += 32)
+        for (int base = 0; base < n_tmpl && found < k; base += 32 * U)
         {
-            int t = base + lane;
-            bool ok = false;
-            long long node = -1;
-            int4 o = make_int4(0, 0, 0, 0);
-            if (t < n_tmpl)
+            bool ok[U];
+            int t_of[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
             {
-                o = tmpl[t];
-                int px = x + o.x, py = y + o.y, pz = z + o.z;
-                if ((unsigned)px < (unsigned)g.nx && (unsigned)py < (unsigned)g.ny && (unsigned)pz < (unsigned)g.nz)
+                const int t = base + 32 * u + lane;
+                t_of[u] = t;
+                ok[u] = false;
+                if (t < n_tmpl)
                 {
-                    node = ((long long)pz * g.ny + py) * g.nx + px;
-                    ok = mask[node] != 0;
+                    const long long q = qc + tmpl[t].w;
+                    ok[u] = (bits[q >> 5] >> (q & 31)) & 1u;
                 }
             }
-            unsigned bl = __ballot_sync(0xffffffffu, ok);
-            int slot = found + __popc(bl & lanemask_lt());
-            if (ok && slot < k)
+#pragma unroll
+            for (int u = 0; u < U; ++u)
             {
-                const int p = pid_of_node[node];
-                if (nb_pid) nb_pid[cell * k + slot] = p;
-                if (nb_rec) nb_rec[cell * k + slot] = make_int2(pair_lin(g, o.x, o.y, o.z), __float_as_int(pts_vf[p]));
+                if (found >= k) break; // warp-uniform
+                const unsigned bl = __ballot_sync(0xffffffffu, ok[u]);
+                const int slot = found + __popc(bl & lanemask_lt());
+                if (ok[u] && slot < k)
+                {
+                    const int4 o = tmpl[t_of[u]];
+                    const long long node = ((long long)(z + o.z) * g.ny + (y + o.y)) * g.nx + (x + o.x);
+                    const int p = pid_of_node[node];
+                    if (nb_pid) nb_pid[cell * k + slot] = p;
+                    if (nb_rec) nb_rec[cell * k + slot] = make_int2(pair_lin(g, o.x, o.y, o.z), __float_as_int(pts_vf[p]));
+                }
+                found += __popc(bl);
             }
-            found += __popc(bl);
         }
         if (lane == 0) nb_n[cell] = min(found, k);
     }
@@ -1197,7 +1238,8 @@ void launch_bin_region(const Geom &g, uint8_t *bin_flag, const int *bin_cnt, int
 // for one cell at a time, so the few bins that take this path (those around an
 // overflowing bin) are spread over the whole GPU.
 __global__ void __launch_bounds__(256) k_search_template(
-    const Geom g, const uint8_t *__restrict__ mask, int all_cells, const int *__restrict__ template_bins,
+    const Geom g, const uint32_t *__restrict__ bits, int hx, int hy, int hz, const uint8_t *__restrict__ mask,
+    int all_cells, const int *__restrict__ template_bins,
     const float *__restrict__ pts_vf, const int4 *__restrict__ tmpl, int n_tmpl, const int *__restrict__ pid_of_node,
     int *__restrict__ nb_pid, int2 *__restrict__ nb_rec, int *__restrict__ nb_n, int *__restrict__ n_template_cells)
 {
@@ -1208,24 +1250,41 @@ __global__ void __launch_bounds__(256) k_search_template(
     const int wx = min(x0 + g.rx, g.nx) - x0, wy = min(y0 + g.ry, g.ny) - y0, wz = min(z0 + g.rz, g.nz) - z0;
     const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
     const int warp = blockIdx.y * nwarps + (threadIdx.x >> 5);
-    template_cells(g, mask, all_cells, x0, y0, z0, wx, wy, wx * wy * wz, warp, nwarps * gridDim.y, lane, pts_vf, tmpl,
+    template_cells(g, bits, hx, hy, hz, mask, all_cells, x0, y0, z0, wx, wy, wx * wy * wz, warp, nwarps * gridDim.y, lane,
+                   pts_vf, tmpl,
                    n_tmpl, pid_of_node, nb_pid, nb_rec, nb_n, n_template_cells);
 }
 
-cudaError_t launch_search_template(const Geom &g, const uint8_t *mask, int all_cells, const int *tmpl_bins,
-                                   int n_tmpl_bins, const float *pts_vf, const int4 *tmpl, int n_tmpl,
-                                   const int *pid_of_node, int *nb_pid, int2 *nb_rec, int *nb_n,
+long long template_padded_cells(const Geom &g)
+{
+    return ((long long)g.nx + 2LL * g.rx) * ((long long)g.ny + 2LL * g.ry) * ((long long)g.nz + 2LL * g.rz);
+}
+
+int template_padded_offset(const Geom &g, int dx, int dy, int dz)
+{
+    const long long PX = g.nx + 2LL * g.rx, PY = g.ny + 2LL * g.ry;
+    return (int)(((long long)dz * PY + dy) * PX + dx);
+}
+
+cudaError_t launch_search_template(const Geom &g, const uint8_t *mask, uint32_t *bits, int all_cells,
+                                   const int *tmpl_bins, int n_tmpl_bins, const float *pts_vf, const int4 *tmpl,
+                                   int n_tmpl, const int *pid_of_node, int *nb_pid, int2 *nb_rec, int *nb_n,
                                    int *n_template_cells, int n_sm, cudaStream_t st)
 {
     if (n_tmpl_bins <= 0) return cudaSuccess;
+    {
+        const long long n_padded = template_padded_cells(g);
+        const int blocks = (int)std::min<long long>((n_padded + 255) / 256, (long long)n_sm * 16);
+        k_mask_bits_padded<<<blocks, 256, 0, st>>>(g, mask, g.rx, g.ry, g.rz, n_padded, bits);
+    }
     // about four waves of 256-thread blocks, at most one warp per 32 cells of a bin
     const long long cells = (long long)g.rx * g.ry * g.rz;
     long long split = ((long long)4 * n_sm * 8 + n_tmpl_bins - 1) / n_tmpl_bins;
     split = std::min(split, std::max(1LL, cells / (8 * 32)));
     split = std::max(1LL, std::min(split, 65535LL));
     dim3 grid((unsigned)n_tmpl_bins, (unsigned)split);
-    k_search_template<<<grid, 256, 0, st>>>(g, mask, all_cells, tmpl_bins, pts_vf, tmpl, n_tmpl, pid_of_node, nb_pid,
-                                            nb_rec, nb_n, n_template_cells);
+    k_search_template<<<grid, 256, 0, st>>>(g, bits, g.rx, g.ry, g.rz, mask, all_cells, tmpl_bins, pts_vf, tmpl,
+                                            n_tmpl, pid_of_node, nb_pid, nb_rec, nb_n, n_template_cells);
     return cudaGetLastError();
 }
 
