@@ -358,6 +358,7 @@ int hpgl_b200_last_stats(double *out, int cap)
     for (int i = 0; i < hb::kStages; ++i) v[26 + i] = s.stage_ms[i];
     v[36] = (double)s.exact_cells;
     v[37] = s.prefilter ? 1.0 : 0.0;
+    v[38] = s.plan_ms;
     int n = cap < HPGL_B200_STATS_LEN ? cap : HPGL_B200_STATS_LEN;
     for (int i = 0; i < n; ++i) out[i] = v[i];
     return n;

@@ -125,6 +125,22 @@ class Engine
             prev = stage_ev_[i];
         }
     }
+    // Page-locked host staging for table uploads. The contents must not be
+    // rewritten before the copies issued from them have completed (the engine
+    // synchronises its stream between the uses).
+    unsigned char *staging(size_t bytes)
+    {
+        if (stage_cap_ < bytes)
+        {
+            if (stage_) cudaFreeHost(stage_);
+            stage_ = nullptr;
+            stage_cap_ = 0;
+            const size_t want = bytes + bytes / 4;
+            HB_CK(cudaHostAlloc(reinterpret_cast<void **>(&stage_), want, cudaHostAllocDefault));
+            stage_cap_ = want;
+        }
+        return stage_;
+    }
     int n_sm() const { return n_sm_; }
     int max_smem() const { return max_smem_; }
     cudaStream_t stream(const void *user) const { return user ? (cudaStream_t)user : own_stream_; }
@@ -142,6 +158,8 @@ class Engine
     int n_sm_ = 148;
     int max_smem_ = 227 * 1024;
     std::map<std::string, DevBuf> bufs_;
+    unsigned char *stage_ = nullptr;
+    size_t stage_cap_ = 0;
 };
 
 static std::mutex g_engine_mu;
@@ -347,28 +365,42 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
 {
     const Geom &g = pl.g;
     DevSearch S;
-    // tables
-    uint32_t *keytab = E.buf<uint32_t>("keytab", pl.kt.rank.size());
-    S.search_vals = E.buf<double>("search_vals", pl.kt.vals.size());
-    HB_CK(cudaMemcpyAsync(keytab, pl.kt.rank.data(), pl.kt.rank.size() * 4, cudaMemcpyHostToDevice, st));
-    HB_CK(cudaMemcpyAsync(S.search_vals, pl.kt.vals.data(), pl.kt.vals.size() * 8, cudaMemcpyHostToDevice, st));
-    // 16-bit ranks for the fast selection path when the rank space allows it
+    // tables: the exact covariances of the key block (for the pair tables), the
+    // 16-bit ranks of the fast selection and the prefilter's per-rank h2, staged
+    // through page-locked memory; the 32-bit ranks only when a slow path needs them
+    const size_t nk = pl.kt.rank.size();
     const bool fast_keys = g.k <= 64 && pl.kt.n_ranks <= 0xFFFE;
+    const bool use_sd = fast_keys && pl.sg.ok && !exact_search;
+    const size_t nh = use_sd ? pl.sg.h2_rank.size() : 0;
+    const size_t off_k16 = nk * 8, off_h2 = (off_k16 + (fast_keys ? nk * 2 : 0) + 15) / 16 * 16;
+    unsigned char *stg = E.staging(off_h2 + nh * 8);
+    std::memcpy(stg, pl.kt.vals.data(), nk * 8);
+    S.search_vals = E.buf<double>("search_vals", nk);
+    HB_CK(cudaMemcpyAsync(S.search_vals, stg, nk * 8, cudaMemcpyHostToDevice, st));
     uint16_t *keytab16 = nullptr;
     if (fast_keys)
     {
-        std::vector<uint16_t> k16(pl.kt.rank.size());
-        for (size_t i = 0; i < k16.size(); ++i)
+        uint16_t *k16 = reinterpret_cast<uint16_t *>(stg + off_k16);
+        for (size_t i = 0; i < nk; ++i)
             k16[i] = pl.kt.rank[i] == KEY_EXCLUDED ? (uint16_t)0xFFFF : (uint16_t)pl.kt.rank[i];
-        keytab16 = E.buf<uint16_t>("keytab16", k16.size());
-        HB_CK(cudaMemcpyAsync(keytab16, k16.data(), k16.size() * 2, cudaMemcpyHostToDevice, st));
-        HB_CK(cudaStreamSynchronize(st)); // k16 is a temporary
+        keytab16 = E.buf<uint16_t>("keytab16", nk);
+        HB_CK(cudaMemcpyAsync(keytab16, k16, nk * 2, cudaMemcpyHostToDevice, st));
     }
+    uint32_t *keytab32 = nullptr;
+    auto keytab = [&]() {
+        if (!keytab32)
+        {
+            keytab32 = E.buf<uint32_t>("keytab", nk);
+            HB_CK(cudaMemcpyAsync(keytab32, pl.kt.rank.data(), nk * 4, cudaMemcpyHostToDevice, st));
+        }
+        return keytab32;
+    };
     SurrDev sd = {};
-    if (fast_keys && pl.sg.ok && !exact_search)
+    if (use_sd)
     {
-        double *h2r = E.buf<double>("h2_rank", pl.sg.h2_rank.size());
-        HB_CK(cudaMemcpyAsync(h2r, pl.sg.h2_rank.data(), pl.sg.h2_rank.size() * 8, cudaMemcpyHostToDevice, st));
+        std::memcpy(stg + off_h2, pl.sg.h2_rank.data(), nh * 8);
+        double *h2r = E.buf<double>("h2_rank", nh);
+        HB_CK(cudaMemcpyAsync(h2r, stg + off_h2, nh * 8, cudaMemcpyHostToDevice, st));
         sd.on = 1;
         for (int i = 0; i < 9; ++i) sd.T[i] = pl.sg.T[i];
         for (int a = 0; a < 3; ++a) sd.step[a] = pl.sg.step[a];
@@ -449,7 +481,7 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
                                  S.nb_rec, S.nb_n, tie_cells, scal + 3, scal + 4, scal + 5, st));
     else
         HB_CK(launch_search(g, d_mask, all_cells, bin_start, bin_cnt, S.bin_flag, bin_pts, P.pts_xyz, P.pts_val,
-                            keytab, pl.rank_bits, tmpl, n_tmpl, P.pid_of_node, cand_cap, warps,
+                            keytab(), pl.rank_bits, tmpl, n_tmpl, P.pid_of_node, cand_cap, warps,
                             S.nb_pid, S.nb_rec, S.nb_n, tie_cells, scal + 3, scal + 4, st));
     if (n_tmpl_bins > 0)
         HB_CK(launch_search_template(g, d_mask, E.buf<uint32_t>("mask_bits", (size_t)(template_padded_cells(g) + 31) / 32), all_cells,
@@ -490,7 +522,7 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
             for (int first = 0; first < S.ties; first += chunk)
             {
                 launch_resolve_ties(g, tie_cells, scal + 3, first, chunk, bin_start, bin_cnt, bin_pts, P.pts_xyz,
-                                    P.pts_val, keytab, scratch, cap, S.nb_pid, S.nb_rec, st);
+                                    P.pts_val, keytab(), scratch, cap, S.nb_pid, S.nb_rec, st);
                 E.stats.launches += 1;
             }
         }
@@ -644,8 +676,12 @@ int cont_kriging(int kind, const int *dims, const float *in_data, const unsigned
         const bool simple = kind == 1;
         check_model_args(a.cov_type, a.ranges, a.angles, a.sill, a.nugget, a.radiuses, a.max_nb);
         // the host tables are built while the grid is uploaded and compacted
+        double plan_ms = 0.0;
         auto plan_f = std::async(std::launch::async, [&]() {
-            return make_plan(simple, a.cov_type, a.ranges, a.angles, a.sill, a.nugget, a.radiuses, a.max_nb, dims);
+            const auto t0 = std::chrono::steady_clock::now();
+            Plan p = make_plan(simple, a.cov_type, a.ranges, a.angles, a.sill, a.nugget, a.radiuses, a.max_nb, dims);
+            plan_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            return p;
         });
         Engine &E = engine_for_current_device();
         cudaStream_t st = E.stream(opt.stream);
@@ -713,6 +749,7 @@ int cont_kriging(int kind, const int *dims, const float *in_data, const unsigned
         HB_CK(cudaEventRecord(E.ev_[2], st));
         DevPoints P = compact_points(E, grid_geom(dims), d_mask, d_in, nullptr, st);
         const Plan pl = plan_f.get();
+        E.stats.plan_ms = plan_ms;
         DevSearch S = run_search(E, pl, P, d_mask, 0, st, false, (opt.flags & 4u) != 0);
         HB_CK(cudaEventRecord(E.ev_[3], st));
         SolveOut so{};

@@ -68,6 +68,7 @@ struct Stats
     double bucket_flops[5] = {0, 0, 0, 0, 0};
     long long exact_cells = 0; // cells the float prefilter left to the exact rank path
     bool prefilter = false;
+    double plan_ms = 0;        // host time building the covariance tables (overlapped with upload/compaction)
 };
 
 void set_error(const std::string &msg);

@@ -165,8 +165,9 @@ int hpgl_b200_find_neighbours(int kind, const int *dims, const unsigned char *ma
  *            resolution, bucketing, solves, finalize, download
  *   [36] cells whose neighbours the float distance prefilter could not
  *        decide (selected by exact ranks over every candidate instead)
- *   [37] 1 when the float distance prefilter was active in the last search */
-#define HPGL_B200_STATS_LEN 38
+ *   [37] 1 when the float distance prefilter was active in the last search
+ *   [38] host ms building the covariance tables (overlapped with the upload) */
+#define HPGL_B200_STATS_LEN 39
 int hpgl_b200_last_stats(double *out, int cap);
 
 /* No counterpart in the reference. The same SK weights as
