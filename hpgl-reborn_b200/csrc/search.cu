@@ -755,18 +755,23 @@ template <int E>
 __device__ int select_surr(const Geom &g, const SurrDev &sd, int C, const float4 *ctp, const int *cklin,
                            const int *cplin, const int *cpid, const float *cval, int kc0, int klin_c, int plin_c,
                            const uint16_t *__restrict__ keytab, uint32_t *sel, int lane, float tcx, float tcy,
-                           float tcz, float Tg, double &H, int &kguess, int *out_pid, int2 *out_rec)
+                           float tcz, float Tg, const uint32_t *sub, int n_sub, double &H, int &kguess,
+                           int *out_pid, int2 *out_rec)
 {
     constexpr int CAP = 32 * E;
     const int k = g.k;
     int cnt = 0;
     __syncwarp(); // the previous cell's reads of sel are done
-    for (int base = 0; base < C; base += 32)
+    // candidates scanned: the sublist `sub` (n_sub entries) when given, else all C
+    const int n_scan = sub ? n_sub : C;
+    for (int base = 0; base < n_scan; base += 32)
     {
-        const int i = base + lane;
+        const int j = base + lane;
         bool in = false;
-        if (i < C)
+        int i = 0;
+        if (j < n_scan)
         {
+            i = sub ? (int)sub[j] : j;
             const float4 t = ctp[i];
             const float qx = t.x - tcx, qy = t.y - tcy, qz = t.z - tcz;
             in = fmaf(qz, qz, fmaf(qy, qy, qx * qx)) <= Tg;
@@ -926,15 +931,79 @@ __global__ void __launch_bounds__(256) k_search_fast(
     double h_prev = 0.0;
     float path = 0.0f;
     int n_exact = 0;
+    // Chunks of kChunk consecutive cells share a sublist of the candidates within
+    // R of the chunk's centre (transformed coordinates), kept in `keys`. A cell scans
+    // it instead of all C when sqrt(Tg) + |cell - centre| + slack <= R: every
+    // candidate left out of the sublist is then farther than sqrt(Tg) from the cell
+    // (true distance), so it lies beyond the prefilter's threshold like any other
+    // candidate the prefilter drops. select_fast reuses `keys`, invalidating the sublist.
+    constexpr int kChunk = 12;
+    int ch_left = 0, n_sub = 0;
+    bool sl_ok = false;
+    float ccx = 0.f, ccy = 0.f, ccz = 0.f, Rcov = 0.f;
+    const float slack = (float)(2.0 * sd.e3) + 1e-3f;
+    auto snake = [&](int cc, int &sx, int &sy, int &sz) {
+        const int row = cc / wx;
+        sx = cc - row * wx;
+        if (row & 1) sx = wx - 1 - sx;
+        sz = row / wy;
+        sy = row - sz * wy;
+        if (sz & 1) sy = wy - 1 - sy;
+    };
     for (int c = c0; c < c1; ++c)
     {
         if (c > c0) path += (c % wx) ? sd.step[0] : ((c / wx) % wy ? sd.step[1] : sd.step[2]);
-        const int row = c / wx;
-        int cxr = c - row * wx;
-        if (row & 1) cxr = wx - 1 - cxr;
-        const int czr = row / wy;
-        int cyr = row - czr * wy;
-        if (czr & 1) cyr = wy - 1 - cyr;
+        int cxr, cyr, czr;
+        snake(c, cxr, cyr, czr);
+        if (ch_left == 0)
+        {
+            ch_left = min(kChunk, c1 - c);
+            sl_ok = false;
+            if (sd.on && have_h)
+            {
+                // centre and radius of the chunk's cells in transformed coordinates
+                int sx, sy, sz;
+                snake(c + min(lane, ch_left - 1), sx, sy, sz);
+                const float4 q = surr_coords(sd, sx, sy, sz);
+                float lo_x = q.x, hi_x = q.x, lo_y = q.y, hi_y = q.y, lo_z = q.z, hi_z = q.z;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1)
+                {
+                    lo_x = fminf(lo_x, __shfl_xor_sync(0xffffffffu, lo_x, o));
+                    hi_x = fmaxf(hi_x, __shfl_xor_sync(0xffffffffu, hi_x, o));
+                    lo_y = fminf(lo_y, __shfl_xor_sync(0xffffffffu, lo_y, o));
+                    hi_y = fmaxf(hi_y, __shfl_xor_sync(0xffffffffu, hi_y, o));
+                    lo_z = fminf(lo_z, __shfl_xor_sync(0xffffffffu, lo_z, o));
+                    hi_z = fmaxf(hi_z, __shfl_xor_sync(0xffffffffu, hi_z, o));
+                }
+                ccx = 0.5f * (lo_x + hi_x);
+                ccy = 0.5f * (lo_y + hi_y);
+                ccz = 0.5f * (lo_z + hi_z);
+                const float ex = hi_x - ccx, ey = hi_y - ccy, ez = hi_z - ccz;
+                const float rho = sqrtf(ex * ex + ey * ey + ez * ez);
+                Rcov = (float)sqrt(h_prev) + 2.0f * rho + 1.5f;
+                const float R2 = Rcov * Rcov;
+                __syncwarp();
+                n_sub = 0;
+                for (int base = 0; base < C; base += 32)
+                {
+                    const int i = base + lane;
+                    bool in = false;
+                    if (i < C)
+                    {
+                        const float4 t = ctp[i];
+                        const float dx = t.x - ccx, dy = t.y - ccy, dz = t.z - ccz;
+                        in = fmaf(dz, dz, fmaf(dy, dy, dx * dx)) <= R2;
+                    }
+                    const unsigned bl = __ballot_sync(0xffffffffu, in);
+                    if (in) keys[n_sub + __popc(bl & lanemask_lt())] = (uint32_t)i;
+                    n_sub += __popc(bl);
+                }
+                __syncwarp();
+                sl_ok = true;
+            }
+        }
+        --ch_left;
         const long long cell = ((long long)(z0 + czr) * g.ny + (y0 + cyr)) * g.nx + (x0 + cxr);
         if (!all_cells && mask[cell]) continue;
         const int klin_c = (czr * g.kny + cyr) * g.knx + cxr;
@@ -948,13 +1017,24 @@ __global__ void __launch_bounds__(256) k_search_fast(
             const double rt = sqrt(h_prev) + (double)path + 2.0 * sd.e3;
             const float Tg = __double2float_ru(rt * rt * (1.0 + 1e-6));
             const float4 tc = surr_coords(sd, cxr, cyr, czr);
+            bool use_sub = false;
+            if (sl_ok)
+            {
+                const float dx = tc.x - ccx, dy = tc.y - ccy, dz = tc.z - ccz;
+                const float dc = sqrtf(fmaf(dz, dz, fmaf(dy, dy, dx * dx)));
+                // R excludes candidates at float distance > R from the centre: true
+                // distance > R - e3 - rounding; the cell is within dc + e3 of the
+                // centre; slack covers both errors and the roundings of dc and sqrt(Tg)
+                use_sub = sqrtf(Tg) * (1.0f + 1e-6f) + dc * (1.0f + 1e-6f) + slack + 1e-5f * Rcov <= Rcov;
+            }
             n = select_surr<E>(g, sd, C, ctp, cklin, cplin, cpid, cval, kc0, klin_c, plin_c, keytab16, sel, lane,
-                               tc.x, tc.y, tc.z, Tg, h, kguess, o_pid, o_rec);
+                               tc.x, tc.y, tc.z, Tg, use_sub ? keys : nullptr, n_sub, h, kguess, o_pid, o_rec);
         }
         if (n == -2)
         {
             n = select_fast<E>(g, C, cklin, cplin, cpid, cval, kc0, klin_c, plin_c, keytab16, keys, sel, lane,
                                kguess, o_pid, o_rec);
+            sl_ok = false; // keys[] now holds select_fast's keys
             n_exact += sd.on;
             h = (sd.on && kguess >= 0) ? sd.h2_rank[kguess] : 0.0;
             have_h = sd.on && kguess >= 0 && n != 0;
