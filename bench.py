@@ -47,8 +47,10 @@ def parse():
     ap.add_argument("--skip-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--profile-case", type=float, default=0.0, metavar="SCALE",
-                    help="run one FP32-refined device call on the workload shrunk by SCALE and exit "
+                    help="run one device call on the workload shrunk by SCALE and exit "
                          "(the case profiled with ncu)")
+    ap.add_argument("--profile-precision", choices=["fp32_refined", "fp64"], default="fp32_refined",
+                    help="precision of the --profile-case call")
     return ap.parse_args()
 
 
@@ -265,7 +267,7 @@ def main():
         return times, stats
 
     if args.profile_case > 0:
-        st = dev_call(1)
+        st = dev_call(1 if args.profile_precision == "fp32_refined" else 0)
         torch.cuda.synchronize()
         print(json.dumps({"profile_case": wl.dims, "stats": st}), flush=True)
         return
