@@ -214,11 +214,24 @@ __global__ void __launch_bounds__(1024) k_prepare_scan(int T, int *__restrict__ 
         }
         bucket_off[kBuckets] = run;
     }
-    if (threadIdx.x < kBuckets * 3)
+    // moments: every thread sums a strided share of each of the 3 kBuckets rows
+    __shared__ unsigned long long s_m[32];
+    for (int q = 0; q < kBuckets * 3; ++q)
     {
         unsigned long long v = 0;
-        for (int t = 0; t < T; ++t) v += tile_mom[(long long)threadIdx.x * T + t];
-        moments[threadIdx.x] = v;
+        for (int t = threadIdx.x; t < T; t += blockDim.x) v += tile_mom[(long long)q * T + t];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) s_m[threadIdx.x >> 5] = v;
+        __syncthreads();
+        if (threadIdx.x < 32)
+        {
+            unsigned long long w = threadIdx.x < (blockDim.x >> 5) ? s_m[threadIdx.x] : 0ULL;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+            if (threadIdx.x == 0) moments[q] = w;
+        }
+        __syncthreads();
     }
 }
 

@@ -631,7 +631,7 @@ __device__ __forceinline__ int warp_count_le(const uint32_t *keys, int C, uint32
 }
 
 template <int E>
-__device__ int select_fast(const Geom &g, int C, const int *cklin, const int *cplin, const int *cpid,
+__device__ __forceinline__ int select_fast(const Geom &g, int C, const int *cklin, const int *cplin, const int *cpid,
                            const float *cval, int kc0, int klin_c, int plin_c,
                            const uint16_t *__restrict__ keytab, uint32_t *keys, uint32_t *sel, int lane,
                            int &kguess, int *out_pid, int2 *out_rec)
@@ -752,7 +752,7 @@ __device__ int select_fast(const Geom &g, int C, const int *cklin, const int *cp
 // the k-th slot, or -2 when the prefilter cannot decide (the caller then runs
 // select_fast). On success or -1, H receives that bound.
 template <int E>
-__device__ int select_surr(const Geom &g, const SurrDev &sd, int C, const float4 *ctp, const int *cklin,
+__device__ __forceinline__ int select_surr(const Geom &g, const SurrDev &sd, int C, const float4 *ctp, const int *cklin,
                            const int *cplin, const int *cpid, const float *cval, int kc0, int klin_c, int plin_c,
                            const uint16_t *__restrict__ keytab, uint32_t *sel, int lane, float tcx, float tcy,
                            float tcz, float Tg, const uint32_t *sub, int n_sub, double &H, int &kguess,

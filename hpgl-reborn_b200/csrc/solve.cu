@@ -1314,8 +1314,13 @@ struct Fold64Smem
     static constexpr size_t bytes = (lin_off + NP * sizeof(int) + 127) / 128 * 128 + 16;
 };
 
+// Threads per block of the FP64 folded kernel (one block per SM).
+#ifndef HB_FOLD64_THREADS
+#define HB_FOLD64_THREADS 256
+#endif
+
 template <int NP, bool ORDINARY>
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(HB_FOLD64_THREADS, 1)
     k_solve_fold64(const Geom g, const int2 *__restrict__ cells, const int *__restrict__ n_items_ptr,
                    const int2 *__restrict__ nb_rec, int ind_value, SolveParams P)
 {
@@ -1557,12 +1562,13 @@ static cudaError_t launch_one(const Geom &g, const int2 *cells, const int *n_ite
     }
     else if constexpr (!REF && NP <= 32)
     {
-        constexpr int spb = 256 / (NP / 2); // systems per block
+        constexpr int fthreads = HB_FOLD64_THREADS;
+        constexpr int spb = fthreads / (NP / 2); // systems per block
         const size_t smem = Fold64Smem<NP>::bytes * spb;
         auto kern = k_solve_fold64<NP, ORD>;
-        cudaError_t e = launch_kernel(kern, 256, smem, max_items, spb, n_sm, blocks);
+        cudaError_t e = launch_kernel(kern, fthreads, smem, max_items, spb, n_sm, blocks);
         if (e != cudaSuccess) return e;
-        kern<<<(unsigned)blocks, 256, smem, st>>>(g, cells, n_items, nb_rec, ind_value, P);
+        kern<<<(unsigned)blocks, fthreads, smem, st>>>(g, cells, n_items, nb_rec, ind_value, P);
     }
     else
     {
