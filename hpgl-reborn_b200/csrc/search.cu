@@ -1156,13 +1156,101 @@ __global__ void k_resolve_ties(const Geom g, const int *__restrict__ tie_cells, 
 
 // One warp per tie-straddling cell, 16-bit ranks: the warp rebuilds the
 // threshold-filtered candidate list in the reference's order in shared memory,
-// one lane replays introsort's partitions along the k-th slot
-// (gis::select_first_k, the same set std::sort leaves in front), and the warp
+// replays introsort's partitions along the k-th slot (warp_select_first_k, the
+// same set std::sort leaves in front), and the warp
 // orders the selected k by (rank, position) for output.
 struct RankLess
 {
     __device__ bool operator()(uint32_t a, uint32_t b) const { return (a >> 16) < (b >> 16); }
 };
+
+// partition_around_front (libstdc++'s unguarded partition with the pivot at lo)
+// by a warp. On the array as it stands, let L be the positions in (lo, hi) that
+// stop the left scan (not less than the pivot), ascending, and R those in
+// [lo, hi) that stop the right scan (pivot not less than them), descending.
+// The serial loop swaps a[L[m]] and a[R[m]] while L[m] < R[m]; every such L
+// lies below every such R, so the swaps are disjoint and independent, and the
+// loop returns min(L[M], R[M-1]) for the first M with L[M] >= R[M] (an exhausted
+// L counts as +inf, R[-1] as +inf). lstop / rstop hold hi - lo ints each.
+template <typename Less>
+__device__ int warp_partition_around_front(uint32_t *a, int lo, int hi, Less less, int *lstop, int *rstop, int lane)
+{
+    const uint32_t pivot = a[lo];
+    int nr = 0;
+    for (int top = hi - 1; top >= lo; top -= 32)
+    {
+        const int j = top - lane;
+        const bool st = j >= lo && !less(pivot, a[j]);
+        const unsigned bl = __ballot_sync(0xffffffffu, st);
+        if (st) rstop[nr + __popc(bl & lanemask_lt())] = j;
+        nr += __popc(bl);
+    }
+    __syncwarp();
+    int nl = 0, M = -1, LM = 0x7fffffff;
+    for (int base = lo + 1; base < hi; base += 32)
+    {
+        const int i = base + lane;
+        const bool st = i < hi && !less(a[i], pivot);
+        const unsigned bl = __ballot_sync(0xffffffffu, st);
+        const int m = nl + __popc(bl & lanemask_lt());
+        const bool cross = st && (m >= nr || i >= rstop[m]);
+        if (st && !cross) lstop[m] = i;
+        const unsigned cb = __ballot_sync(0xffffffffu, cross);
+        if (cb)
+        {
+            const int src = __ffs(cb) - 1;
+            M = __shfl_sync(0xffffffffu, m, src);
+            LM = __shfl_sync(0xffffffffu, i, src);
+            break;
+        }
+        nl += __popc(bl);
+    }
+    if (M < 0) M = nl;
+    __syncwarp();
+    for (int m = lane; m < M; m += 32)
+    {
+        const int x = lstop[m], y = rstop[m];
+        const uint32_t t = a[x];
+        a[x] = a[y];
+        a[y] = t;
+    }
+    __syncwarp();
+    const int rm1 = M > 0 ? rstop[M - 1] : 0x7fffffff;
+    return LM < rm1 ? LM : rm1;
+}
+
+// gis::select_first_k with the partitions done by the warp (median choice,
+// heapsort fallback and the final short insertion sort by lane 0): the same
+// first-k set std::sort leaves in front.
+template <typename Less>
+__device__ void warp_select_first_k(uint32_t *a, int n, int k, Less less, int *lstop, int *rstop, int lane)
+{
+    const int kThreshold = 16;
+    if (n <= 0 || k <= 0 || k >= n) return;
+    int lo = 0, hi = n;
+    int depth = 2 * gis::floor_log2(n);
+    while (hi - lo > kThreshold)
+    {
+        if (depth == 0)
+        {
+            if (lane == 0) gis::heap_sort_range(a, (long)lo, (long)hi, less);
+            __syncwarp();
+            return;
+        }
+        --depth;
+        const int mid = lo + (hi - lo) / 2;
+        if (lane == 0) gis::median_to_front(a, (long)lo, (long)lo + 1, (long)mid, (long)hi - 1, less);
+        __syncwarp();
+        const int cut = warp_partition_around_front(a, lo, hi, less, lstop, rstop, lane);
+        if (cut == k) return;
+        if (cut > k)
+            hi = cut;
+        else
+            lo = cut;
+    }
+    if (lane == 0) gis::insertion_sort_guarded(a, (long)lo, (long)hi, less);
+    __syncwarp();
+}
 
 template <int E>
 __global__ void __launch_bounds__(128) k_resolve_ties_fast(
@@ -1173,8 +1261,9 @@ __global__ void __launch_bounds__(128) k_resolve_ties_fast(
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    uint32_t *arr = reinterpret_cast<uint32_t *>(smem) + (size_t)warp * 2 * cap;
+    uint32_t *arr = reinterpret_cast<uint32_t *>(smem) + (size_t)warp * 4 * cap;
     int *pid = reinterpret_cast<int *>(arr + cap);
+    int *lstop = pid + cap, *rstop = lstop + cap;
     const int n_ties = *tie_count;
     for (int t = blockIdx.x * nwarps + warp; t < n_ties; t += gridDim.x * nwarps)
     {
@@ -1214,8 +1303,7 @@ __global__ void __launch_bounds__(128) k_resolve_ties_fast(
                 }
         if (n > cap) n = cap; // cannot happen: cap bounds every candidate list
         __syncwarp();
-        if (lane == 0) gis::select_first_k(arr, (long)n, (long)g.k, RankLess());
-        __syncwarp();
+        warp_select_first_k(arr, n, g.k, RankLess(), lstop, rstop, lane);
         const int m = n < g.k ? n : g.k;
         uint32_t v[E];
 #pragma unroll
@@ -1247,7 +1335,7 @@ __global__ void __launch_bounds__(128) k_resolve_ties_fast(
     }
 }
 
-size_t resolve_ties_fast_smem(int cap, int warps) { return (size_t)warps * 2 * cap * 4; }
+size_t resolve_ties_fast_smem(int cap, int warps) { return (size_t)warps * 4 * cap * 4; }
 
 cudaError_t launch_resolve_ties_fast(const Geom &g, const int *tie_cells, const int *tie_count, int n_ties,
                                      const int *bin_start, const int *bin_cnt, const int *bin_pts,
