@@ -203,6 +203,34 @@ void hpgl_simple_kriging(float *input_data, unsigned char *input_mask, hpgl_shap
         report_done("Simple Kriging");
 }
 
+void hpgl_lvm_kriging(float *input_data, unsigned char *input_mask, hpgl_shape_t *input_data_shape,
+                      float *mean_data, hpgl_shape_t *mean_data_shape, hpgl_ok_params_t *params, float *output_data,
+                      unsigned char *output_mask, hpgl_shape_t *output_data_shape)
+{
+    (void)output_data_shape;
+    if (!params || !mean_data)
+    {
+        hb::set_error("hpgl_lvm_kriging: null argument");
+        return;
+    }
+    int dims[3], mdims[3];
+    if (!shape_dims(input_data_shape, dims)) return;
+    if (mean_data_shape)
+    {
+        if (!shape_dims(mean_data_shape, mdims)) return;
+        if ((long long)mdims[0] * mdims[1] * mdims[2] != (long long)dims[0] * dims[1] * dims[2])
+        {
+            hb::set_error("hpgl_lvm_kriging: mean and input size mismatch");
+            return;
+        }
+    }
+    hb::Options opt;
+    progress("LVM Kriging", 0);
+    if (hb::cont_kriging(2, dims, input_data, input_mask, ok_args_from(params), output_data, output_mask, opt,
+                         mean_data) == 0)
+        report_done("LVM Kriging");
+}
+
 int hpgl_simple_kriging_weights(float *center_coords, float *neighbours_x, float *neighbours_y,
                                 float *neighbours_z, int neighbours_count, hpgl_cov_params_t *params,
                                 float *weights)
@@ -291,6 +319,19 @@ int hpgl_b200_cont_kriging_ex(int kind, const int *dims, const float *in_data, c
         return HPGL_B200_EINVAL;
     }
     return hb::cont_kriging(kind, dims, in_data, in_mask, sk_args_from(params), out_data, out_mask, options_from(opt));
+}
+
+int hpgl_b200_lvm_kriging_ex(const int *dims, const float *in_data, const unsigned char *in_mask,
+                             const float *mean_data, const hpgl_ok_params_t *params, float *out_data,
+                             unsigned char *out_mask, const hpgl_b200_options_t *opt)
+{
+    if (!params || !mean_data)
+    {
+        hb::set_error("hpgl_b200_lvm_kriging_ex: bad argument");
+        return HPGL_B200_EINVAL;
+    }
+    return hb::cont_kriging(2, dims, in_data, in_mask, ok_args_from(params), out_data, out_mask, options_from(opt),
+                            mean_data);
 }
 
 int hpgl_b200_indicator_kriging_ex(const int *dims, const unsigned char *in_data, const unsigned char *in_mask,

@@ -318,7 +318,7 @@ struct DevPoints
 };
 
 static DevPoints compact_points(Engine &E, const Geom &g, const uint8_t *d_mask, const float *d_val_f,
-                                const uint8_t *d_val_u8, cudaStream_t st)
+                                const uint8_t *d_val_u8, cudaStream_t st, const float *d_mean = nullptr)
 {
     DevPoints P;
     long long n = g.n_cells;
@@ -337,7 +337,7 @@ static DevPoints compact_points(Engine &E, const Geom &g, const uint8_t *d_mask,
     P.pts_val = E.buf<float>("pts_val", m);
     if (d_val_u8) P.pts_cat = E.buf<uint8_t>("pts_cat", m);
     P.pid_of_node = E.buf<int>("pid_of_node", (size_t)n);
-    launch_emit_points(d_mask, pos, g, d_val_f, d_val_u8, P.pts_node, P.pts_xyz, P.pts_val, P.pts_cat,
+    launch_emit_points(d_mask, pos, g, d_val_f, d_mean, d_val_u8, P.pts_node, P.pts_xyz, P.pts_val, P.pts_cat,
                        P.pid_of_node, st);
     HB_CK(cudaGetLastError());
     E.mark(STAGE_COMPACT, st);
@@ -666,14 +666,17 @@ static void end_call(Engine &E, cudaStream_t st)
 
 // ------------------------------------------------------------------ entry points
 int cont_kriging(int kind, const int *dims, const float *in_data, const unsigned char *in_mask,
-                 const SkArgs &a, float *out_data, unsigned char *out_mask, const Options &opt)
+                 const SkArgs &a, float *out_data, unsigned char *out_mask, const Options &opt, const float *means)
 {
     std::lock_guard<std::mutex> lk(g_engine_mu);
     try
     {
         if (!dims || !in_data || !in_mask || !out_data || !out_mask) throw CudaFail{-1, "null array argument"};
+        if (kind < 0 || kind > 2) throw CudaFail{-1, "unknown kriging kind"};
+        const bool lvm = kind == 2;
+        if (lvm && !means) throw CudaFail{-1, "LVM kriging needs the mean array"};
         long long n = check_dims(dims);
-        const bool simple = kind == 1;
+        const bool simple = kind != 0; // SK and LVM share the truncated covariance and SK weights
         check_model_args(a.cov_type, a.ranges, a.angles, a.sill, a.nugget, a.radiuses, a.max_nb);
         // the host tables are built while the grid is uploaded and compacted
         double plan_ms = 0.0;
@@ -690,6 +693,7 @@ int cont_kriging(int kind, const int *dims, const float *in_data, const unsigned
 
         const float *d_in = to_device(E, "in_data", in_data, (size_t)n, io);
         const uint8_t *d_mask = to_device(E, "in_mask", in_mask, (size_t)n, io);
+        const float *d_means = lvm ? to_device(E, "in_means", means, (size_t)n, io) : nullptr;
         float *d_out = io.device ? out_data : E.buf<float>("out_data", (size_t)n);
         uint8_t *d_omask = io.device ? out_mask : E.buf<uint8_t>("out_mask", (size_t)n);
         if (!io.device)
@@ -712,9 +716,11 @@ int cont_kriging(int kind, const int *dims, const float *in_data, const unsigned
         if (opt.variance) d_var = io.device ? opt.variance : E.buf<double>("var", (size_t)n);
         d_status = (io.device && opt.status) ? opt.status : E.buf<signed char>("status", (size_t)n);
 
-        // SK mean: calc_mean over informed cells (calc_mean.cpp:6-30), on the host data
+        // SK mean: calc_mean over informed cells (calc_mean.cpp:6-30), on the host
+        // data. LVM centres the values on their own means as they are compacted,
+        // so the uniform mean stays 0 there.
         double mean = 0.0;
-        if (simple)
+        if (kind == 1)
         {
             if (a.auto_mean)
             {
@@ -747,7 +753,7 @@ int cont_kriging(int kind, const int *dims, const float *in_data, const unsigned
         }
 
         HB_CK(cudaEventRecord(E.ev_[2], st));
-        DevPoints P = compact_points(E, grid_geom(dims), d_mask, d_in, nullptr, st);
+        DevPoints P = compact_points(E, grid_geom(dims), d_mask, d_in, nullptr, st, d_means);
         const Plan pl = plan_f.get();
         E.stats.plan_ms = plan_ms;
         DevSearch S = run_search(E, pl, P, d_mask, 0, st, false, (opt.flags & 4u) != 0);
@@ -759,9 +765,11 @@ int cont_kriging(int kind, const int *dims, const float *in_data, const unsigned
         so.var = d_var;
         so.status = d_status;
         so.write_cont = 1;
+        so.cell_mean = d_means;
         int steps = opt.refine_steps > 0 ? opt.refine_steps : 2;
         run_solves(E, pl, P, S, d_mask, 0, !simple, opt.precision, steps, opt.tolerance, mean, -1, d_status, so, st);
-        launch_finalize_cont(pl.g, d_in, d_status, simple ? 1 : 0, (float)mean, d_out, d_omask, d_est, d_var, st);
+        launch_finalize_cont(pl.g, d_in, d_status, simple ? 1 : 0, (float)mean, d_means, d_out, d_omask, d_est, d_var,
+                             st);
         HB_CK(cudaGetLastError());
         E.stats.launches += 1;
         HB_CK(cudaEventRecord(E.ev_[4], st));

@@ -76,8 +76,10 @@ const char *last_error();
 void set_threads(int n);
 int get_threads();
 
+// kind 0 OK, 1 SK, 2 LVM (SK weights around the per-cell `means`, which kind 2
+// requires; lvm_kriging.cpp:16-39)
 int cont_kriging(int kind, const int *dims, const float *in_data, const unsigned char *in_mask, const SkArgs &a,
-                 float *out_data, unsigned char *out_mask, const Options &opt);
+                 float *out_data, unsigned char *out_mask, const Options &opt, const float *means = nullptr);
 int indicator_kriging(const int *dims, const unsigned char *in_data, const unsigned char *in_mask,
                       const std::vector<IkArgs> &cats, unsigned char *out_data, unsigned char *out_mask,
                       const Options &opt);

@@ -28,15 +28,17 @@ struct SolveOut
     float *prob;         // optional: indicator probability of one category (float result)
     int prob_stride;     // distance between cells in `prob` (the category count)
     int write_cont;      // write out_data / out_mask
+    const float *cell_mean; // LVM: per-cell mean, added at the centre instead of the SK mean
 };
 
 // scan / points / bins (search.cu)
 long long scan_tmp_ints(long long n);
 void exclusive_scan(int *v, long long n, int *tmp, int *total, cudaStream_t st);
 void launch_flag_informed(const uint8_t *mask, long long n, int *flag, cudaStream_t st);
+// `mean_f` (LVM) centres each continuous value on its own cell's mean, in float
 void launch_emit_points(const uint8_t *mask, const int *pos, const Geom &g, const float *val_f,
-                        const uint8_t *val_u8, int *pts_node, unsigned long long *pts_xyz, float *pts_val,
-                        uint8_t *pts_cat, int *pid_of_node, cudaStream_t st);
+                        const float *mean_f, const uint8_t *val_u8, int *pts_node, unsigned long long *pts_xyz,
+                        float *pts_val, uint8_t *pts_cat, int *pid_of_node, cudaStream_t st);
 void launch_bin_count(const unsigned long long *pts_xyz, const int *n_pts, const Geom &g, int *bin_cnt,
                       cudaStream_t st);
 void launch_bin_fill(const unsigned long long *pts_xyz, const int *n_pts, const Geom &g, const int *bin_start,
@@ -113,7 +115,8 @@ void launch_prepare(const Geom &g, const uint8_t *mask, int all_cells, const int
                     int *bucket_cnt, int *bucket_off, int *tile_cnt, unsigned long long *tile_mom, int2 *cells,
                     unsigned long long *moments, cudaStream_t st);
 void launch_finalize_cont(const Geom &g, const float *in_data, signed char *status, int simple, float mean_f,
-                          float *out_data, uint8_t *out_mask, double *est64, double *var, cudaStream_t st);
+                          const float *cell_mean, float *out_data, uint8_t *out_mask, double *est64, double *var,
+                          cudaStream_t st);
 void launch_ik_fail_fill(const Geom &g, const signed char *status, float marginal, int c, int m, float *probs,
                          cudaStream_t st);
 void launch_ik_finalize(long long n_cells, int m, float *probs, uint8_t *out_data, uint8_t *out_mask,

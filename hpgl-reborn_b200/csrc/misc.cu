@@ -298,9 +298,11 @@ void launch_prepare(const Geom &g, const uint8_t *mask, int all_cells, const int
 // ------------------------------------------------------------- finalize
 // Continuous kriging outputs for cells the solver did not write
 // (cont_kriging.h:80-110): informed cells are copied, failures of SK get the
-// mean, failures of OK are left alone.
+// mean (LVM: the cell's own mean, lvm_kriging.cpp:33), failures of OK are left
+// alone.
 __global__ void k_finalize_cont(const Geom g, const float *__restrict__ in_data, signed char *__restrict__ status,
-                                int simple, float mean_f, float *__restrict__ out_data, uint8_t *__restrict__ out_mask,
+                                int simple, float mean_f, const float *__restrict__ cell_mean,
+                                float *__restrict__ out_data, uint8_t *__restrict__ out_mask,
                                 double *__restrict__ est64, double *__restrict__ var)
 {
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < g.n_cells;
@@ -319,7 +321,7 @@ __global__ void k_finalize_cont(const Geom g, const float *__restrict__ in_data,
             if (s >= 3) status[c] = 2; // not written by any solver: treat as singular
             if (simple)
             {
-                out_data[c] = mean_f;
+                out_data[c] = cell_mean ? cell_mean[c] : mean_f;
                 out_mask[c] = 1;
             }
             if (est64) est64[c] = __longlong_as_double(0x7ff8000000000000LL);
@@ -329,9 +331,11 @@ __global__ void k_finalize_cont(const Geom g, const float *__restrict__ in_data,
 }
 
 void launch_finalize_cont(const Geom &g, const float *in_data, signed char *status, int simple, float mean_f,
-                          float *out_data, uint8_t *out_mask, double *est64, double *var, cudaStream_t st)
+                          const float *cell_mean, float *out_data, uint8_t *out_mask, double *est64, double *var,
+                          cudaStream_t st)
 {
-    k_finalize_cont<<<1184, 256, 0, st>>>(g, in_data, status, simple, mean_f, out_data, out_mask, est64, var);
+    k_finalize_cont<<<1184, 256, 0, st>>>(g, in_data, status, simple, mean_f, cell_mean, out_data, out_mask, est64,
+                                          var);
 }
 
 // Indicator category c: cells whose solve failed (or had no neighbours) take
@@ -496,7 +500,7 @@ __global__ void __launch_bounds__(256) k_solve_large(const Geom g, const int2 *_
                 mu = (sx - 1.0) / sy;
             }
             const float mf = (float)mean;
-            double est = (double)mf, var = c0 - mu;
+            double est = out.cell_mean ? (double)out.cell_mean[cell] : (double)mf, var = c0 - mu;
             for (int i = 0; i < n; ++i)
             {
                 double w = ordinary ? x[i] - mu * y[i] : x[i];

@@ -125,7 +125,8 @@ __global__ void k_flag_informed(const uint8_t *__restrict__ mask, long long n, i
 
 // after the exclusive scan, pos[i] is the point id of informed cell i
 __global__ void k_emit_points(const uint8_t *__restrict__ mask, const int *__restrict__ pos, Geom g,
-                              const float *__restrict__ val_f, const uint8_t *__restrict__ val_u8,
+                              const float *__restrict__ val_f, const float *__restrict__ mean_f,
+                              const uint8_t *__restrict__ val_u8,
                               int *__restrict__ pts_node, unsigned long long *__restrict__ pts_xyz,
                               float *__restrict__ pts_val, uint8_t *__restrict__ pts_cat,
                               int *__restrict__ pid_of_node)
@@ -143,8 +144,9 @@ __global__ void k_emit_points(const uint8_t *__restrict__ mask, const int *__res
         int x = node % g.nx, y = node % (g.nx * g.ny) / g.nx, z = node / (g.nx * g.ny);
         pts_node[p] = node;
         pts_xyz[p] = pack_xyz(x, y, z);
-        // continuous value, or the category as a float (indicator kriging)
-        pts_val[p] = val_f ? val_f[i] : (val_u8 ? (float)val_u8[i] : 0.0f);
+        // continuous value (LVM: minus its cell's mean, the float subtraction of
+        // combiner.h:19-24), or the category as a float (indicator kriging)
+        pts_val[p] = val_f ? (mean_f ? val_f[i] - mean_f[i] : val_f[i]) : (val_u8 ? (float)val_u8[i] : 0.0f);
         if (val_u8 && pts_cat) pts_cat[p] = val_u8[i];
         if (pid_of_node) pid_of_node[i] = p;
     }
@@ -1372,10 +1374,10 @@ void launch_flag_informed(const uint8_t *mask, long long n, int *flag, cudaStrea
     k_flag_informed<<<1184, 256, 0, st>>>(mask, n, flag);
 }
 void launch_emit_points(const uint8_t *mask, const int *pos, const Geom &g, const float *val_f,
-                        const uint8_t *val_u8, int *pts_node, unsigned long long *pts_xyz, float *pts_val,
-                        uint8_t *pts_cat, int *pid_of_node, cudaStream_t st)
+                        const float *mean_f, const uint8_t *val_u8, int *pts_node, unsigned long long *pts_xyz,
+                        float *pts_val, uint8_t *pts_cat, int *pid_of_node, cudaStream_t st)
 {
-    k_emit_points<<<1184, 256, 0, st>>>(mask, pos, g, val_f, val_u8, pts_node, pts_xyz, pts_val, pts_cat,
+    k_emit_points<<<1184, 256, 0, st>>>(mask, pos, g, val_f, mean_f, val_u8, pts_node, pts_xyz, pts_val, pts_cat,
                                         pid_of_node);
 }
 void launch_bin_count(const unsigned long long *pts_xyz, const int *n_pts, const Geom &g, int *bin_cnt,

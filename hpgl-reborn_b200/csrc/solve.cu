@@ -533,7 +533,7 @@ __device__ __forceinline__ void solve_one(const Grp<NP> &grp, const GroupMem<NP,
     }
     else
     {
-        est = (double)P.mf + s_vb;
+        est = (double)(P.out.cell_mean ? P.out.cell_mean[my_cell] : P.mf) + s_vb;
         var = P.c0 - s_bb;
     }
     if (var < 0) var = 0;
@@ -1274,7 +1274,7 @@ __global__ void __launch_bounds__(fold_threads<NP>(), fold_min_blocks<NP>())
                 }
                 else
                 {
-                    est = (double)P.mf + s_vb;
+                    est = (double)(out.cell_mean ? out.cell_mean[my_cell] : P.mf) + s_vb;
                     var = P.c0 - s_bb;
                 }
                 if (var < 0) var = 0;
@@ -1502,7 +1502,7 @@ __global__ void __launch_bounds__(HB_FOLD64_THREADS, 1)
             }
             else
             {
-                est = (double)P.mf + s_vb;
+                est = (double)(out.cell_mean ? out.cell_mean[my_cell] : P.mf) + s_vb;
                 var = P.c0 - s_bb;
             }
             if (var < 0) var = 0;

@@ -2,7 +2,7 @@
 
 Signatures, argument validation and output conventions follow HPGL's
 src/geo_bsd/geo.py: ordinary_kriging (:573-607), simple_kriging (:610-649),
-median_ik (:699-738), indicator_kriging (:759-801, two categories dispatch to
+lvm_kriging (:651-696), median_ik (:699-738), indicator_kriging (:759-801, two categories dispatch to
 median IK with data[0]'s model, :785-793), simple_kriging_weights (:897-935),
 the property/grid/model classes (:215-299) and the handler setters (:947-966).
 The output property is a clone of the input that the library fills in place.
@@ -202,6 +202,45 @@ def simple_kriging(prop, grid, radiuses, max_neighbours, cov_model, mean=None, *
                          return_variance)
 
 
+def lvm_kriging(prop, grid, mean_data, radiuses, max_neighbours, cov_model, *, precision: Optional[str] = None,
+                refine_steps: int = 2, return_variance: bool = False):
+    """Kriging with a locally varying mean: SK weights, each neighbour centred
+    on its own cell's mean and the cell's mean added back; failed cells take
+    their mean. mean_data holds one value per grid cell (Fortran order, as
+    the reference's ndpointer(flags='F') argument requires)."""
+    prop = _to_prop(prop)
+    GridValidator.validate_grid_dimensions(grid.x, grid.y, grid.z)
+    valid_radiuses = ParameterValidator.validate_radius(radiuses, "radiuses")
+    ParameterValidator.validate_max_neighbors(max_neighbours)
+    ParameterValidator.validate_covariance_parameters(cov_model.sill, cov_model.nugget, cov_model.ranges,
+                                                      cov_model.angles)
+    if not isinstance(mean_data, numpy.ndarray):
+        raise ValueError("lvm_kriging: mean_data must be a numpy array")
+    if mean_data.dtype != numpy.float32:
+        mean_data = numpy.require(mean_data, dtype="float32")
+    out_prop = _clone_prop(prop)
+    dims = _dims(grid, prop)
+    if mean_data.size != prop.data.size:
+        raise RuntimeError("lvm_kriging: mean_data has %d values, the grid %d" % (mean_data.size, prop.data.size))
+    flags = mean_data.flags
+    if not (flags.f_contiguous and flags.writeable and flags.aligned):
+        # the reference binds mean_data as ndpointer(float32, flags=['F', 'W', 'A'])
+        raise C.ArgumentError("argument 4: TypeError: array must have flags ['F_CONTIGUOUS', 'WRITEABLE', "
+                              "'ALIGNED']")
+    p = W._HPGL_OK_PARAMS(covariance_type=cov_model.type, ranges=tuple(cov_model.ranges),
+                          angles=tuple(cov_model.angles), sill=cov_model.sill, nugget=cov_model.nugget,
+                          radiuses=_int_radiuses(valid_radiuses), max_neighbours=max_neighbours)
+    var = numpy.empty(prop.data.size, numpy.float64) if return_variance else None
+    opt = _options(precision, refine_steps, variance=var)
+    rc = _hpgl_so.hpgl_b200_lvm_kriging_ex(dims, _flat(prop.data).ctypes.data, _flat(prop.mask).ctypes.data,
+                                           mean_data.ctypes.data, C.byref(p), _flat(out_prop.data).ctypes.data,
+                                           _flat(out_prop.mask).ctypes.data, C.byref(opt))
+    W.check(rc, "lvm_kriging")
+    if return_variance:
+        return out_prop, var.reshape(prop.data.shape, order="F")
+    return out_prop
+
+
 def median_ik(prop, grid, marginal_probs, radiuses, max_neighbours, cov_model, *, precision: Optional[str] = None,
               refine_steps: int = 2):
     prop = _to_prop(prop)
@@ -354,6 +393,6 @@ def find_neighbours(prop, grid, radiuses, max_neighbours, cov_model, nodes, kind
 
 
 __all__ = ["ContProperty", "IndProperty", "SugarboxGrid", "CovarianceModel", "covariance", "ordinary_kriging",
-           "simple_kriging", "median_ik", "indicator_kriging", "simple_kriging_weights", "calc_mean",
+           "simple_kriging", "lvm_kriging", "median_ik", "indicator_kriging", "simple_kriging_weights", "calc_mean",
            "set_thread_num", "get_thread_num", "set_output_handler", "set_progress_handler", "set_precision",
            "find_neighbours", "ValidationError", "CriticalValidationError", "ValidationWarning"]

@@ -84,8 +84,8 @@ OK, EINVAL, ECUDA, ENOMEM, ELIMIT = 0, -1, -2, -3, -4
 EXPORTS = [
     "hpgl_get_last_exception_message", "hpgl_set_output_handler", "hpgl_set_progress_handler",
     "hpgl_set_thread_num", "hpgl_get_thread_num", "hpgl_ordinary_kriging", "hpgl_simple_kriging",
-    "hpgl_simple_kriging_weights", "hpgl_indicator_kriging", "hpgl_median_ik",
-    "hpgl_b200_cont_kriging_ex", "hpgl_b200_indicator_kriging_ex", "hpgl_b200_median_ik_ex",
+    "hpgl_simple_kriging_weights", "hpgl_indicator_kriging", "hpgl_median_ik", "hpgl_lvm_kriging",
+    "hpgl_b200_cont_kriging_ex", "hpgl_b200_lvm_kriging_ex", "hpgl_b200_indicator_kriging_ex", "hpgl_b200_median_ik_ex",
     "hpgl_b200_find_neighbours", "hpgl_b200_last_stats", "hpgl_b200_host_alloc", "hpgl_b200_host_free",
     "hpgl_b200_transform", "hpgl_b200_template", "hpgl_b200_covariance", "hpgl_b200_version",
     "hpgl_b200_sk_weights_noalloc", "hpgl_b200_loo_ok", "hpgl_b200_loo_ok_adjoint",
@@ -131,6 +131,12 @@ def _load():
     lib.hpgl_b200_cont_kriging_ex.restype = C.c_int
     lib.hpgl_b200_cont_kriging_ex.argtypes = [C.c_int, i_p, vp, vp, C.POINTER(_HPGL_SK_PARAMS), vp, vp,
                                               C.POINTER(_HPGL_B200_OPTIONS)]
+    lib.hpgl_lvm_kriging.restype = None
+    lib.hpgl_lvm_kriging.argtypes = [_f32F, _u8F, C.POINTER(_HPGL_SHAPE), _f32F, C.POINTER(_HPGL_SHAPE),
+                                     C.POINTER(_HPGL_OK_PARAMS), _f32F, _u8F, C.POINTER(_HPGL_SHAPE)]
+    lib.hpgl_b200_lvm_kriging_ex.restype = C.c_int
+    lib.hpgl_b200_lvm_kriging_ex.argtypes = [i_p, vp, vp, vp, C.POINTER(_HPGL_OK_PARAMS), vp, vp,
+                                             C.POINTER(_HPGL_B200_OPTIONS)]
     lib.hpgl_b200_indicator_kriging_ex.restype = C.c_int
     lib.hpgl_b200_indicator_kriging_ex.argtypes = [i_p, vp, vp, C.POINTER(_HPGL_IK_PARAMS), C.c_int, vp, vp,
                                                    C.POINTER(_HPGL_B200_OPTIONS)]

@@ -195,5 +195,17 @@ def clustered(scale: float = 1.0) -> Workload:
                     (40, 40, 8), 64)
 
 
+def lvm_means(dims, seed: int = 5) -> np.ndarray:
+    """A smooth locally varying mean over the grid (flat, Fortran order): a
+    plane plus a long-wavelength sine, the shape of the trend fields LVM
+    kriging is run with."""
+    nx, ny, nz = dims
+    x, y, z = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    rng = np.random.default_rng(seed)
+    a, b, c = rng.uniform(-0.02, 0.02, 3)
+    m = 0.3 + a * x + b * y + c * z + 0.4 * np.sin(2 * np.pi * x / max(nx, 2)) * np.cos(2 * np.pi * y / max(ny, 2))
+    return m.reshape(-1, order="F").astype(np.float32)
+
+
 ALL = {"ok_small": ok_small, "sk_ok_large": sk_ok_large, "indicator": indicator,
        "gauss_cv": gauss_cv, "clustered": clustered}

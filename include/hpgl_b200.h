@@ -80,6 +80,13 @@ void hpgl_simple_kriging(float *input_data, unsigned char *input_mask, struct hp
 int hpgl_simple_kriging_weights(float *center_coords, float *neighbours_x, float *neighbours_y,
                                 float *neighbours_z, int neighbours_count, struct hpgl_cov_params_t *params,
                                 float *weights);
+/* Replaces api.h:242-251 / api.cpp:412-455 (lvm_kriging.cpp:16-39): SK weights
+ * around a locally varying mean, one float per grid cell; failures take the
+ * cell's mean. mean_data_shape, when given, must have the input's volume (the
+ * reference does not check it). */
+void hpgl_lvm_kriging(float *input_data, unsigned char *input_mask, struct hpgl_shape_t *input_data_shape,
+                      float *mean_data, struct hpgl_shape_t *mean_data_shape, struct hpgl_ok_params_t *params,
+                      float *output_data, unsigned char *output_mask, struct hpgl_shape_t *output_data_shape);
 /* Replaces api.h:267-272 / api.cpp:457-482 (indicator_kriging.h:88-161). */
 void hpgl_indicator_kriging(struct hpgl_ind_masked_array_t *in_data, struct hpgl_ind_masked_array_t *out_data,
                             struct hpgl_ik_params_t *params, int indicator_count);
@@ -131,6 +138,11 @@ struct hpgl_b200_options_t {
 int hpgl_b200_cont_kriging_ex(int kind, const int *dims, const float *in_data, const unsigned char *in_mask,
                               const struct hpgl_sk_params_t *params, float *out_data, unsigned char *out_mask,
                               const struct hpgl_b200_options_t *opt);
+/* LVM kriging with options (hpgl_lvm_kriging's rules); mean_data holds one
+ * float per cell, on the device when opt->flags has HPGL_B200_DEVICE_POINTERS. */
+int hpgl_b200_lvm_kriging_ex(const int *dims, const float *in_data, const unsigned char *in_mask,
+                             const float *mean_data, const struct hpgl_ok_params_t *params, float *out_data,
+                             unsigned char *out_mask, const struct hpgl_b200_options_t *opt);
 /* Full IK (indicator_count > 2 categories, per-category models) or, with one
  * params entry and indicator_count == 2, median IK (median_ik.cpp:24-89). */
 int hpgl_b200_indicator_kriging_ex(const int *dims, const unsigned char *in_data, const unsigned char *in_mask,

@@ -452,10 +452,12 @@ enum
 // kriging_interpolation (kriging_interpolation.h:230-315) + combine
 // (combiner.h:10-25). `value_of(i)` gives the neighbour value as the float the
 // reference subtracts the (float) mean from. est_d accumulates in double,
-// est_f in float exactly as cont_kriging's float result does.
+// est_f in float exactly as cont_kriging's float result does. `means` (LVM,
+// lvm_kriging.cpp:16-39) gives a mean per node instead of the single `mean`.
 template <typename R, typename ValueOf>
-static int krige_node(const Search &s, bool ordinary, double mean, int node, ValueOf value_of,
-                      std::vector<int> &idx, int &path, double &est_d, double &var, float &est_f)
+static int krige_node(const Search &s, bool ordinary, double mean, const float *means, int node,
+                      ValueOf value_of, std::vector<int> &idx, int &path, double &est_d, double &var,
+                      float &est_f)
 {
     path = s.find(node, idx);
     if (idx.empty()) return KI_NO_NEIGHBOURS;
@@ -466,12 +468,12 @@ static int krige_node(const Search &s, bool ordinary, double mean, int node, Val
     s.g.coord(node, cx, cy, cz);
     std::vector<double> w;
     if (!weights<R>(s.f, ordinary, cx, cy, cz, xs, ys, zs, w, var)) return KI_SINGULARITY;
-    float m = (float)mean; // mean_t is float (typedefs.h:122)
+    float m = means ? means[node] : (float)mean; // mean_t is float (typedefs.h:122)
     est_d = (double)m;
     est_f = m;
     for (int i = 0; i < n; ++i)
     {
-        float d = value_of(idx[i]) - m;
+        float d = value_of(idx[i]) - (means ? means[idx[i]] : m);
         est_d += w[i] * (double)d;
         est_f += (float)(w[i] * d);
     }
@@ -552,10 +554,10 @@ int ko_template(int kind, int cov_type, const double *ranges, const double *angl
 static int krige_nodes(int kind, const int *dims, const float *data_f, const unsigned char *data_u8,
                        int ind_value, const unsigned char *mask, int cov_type,
                        const double *ranges, const double *angles, double sill, double nugget,
-                       const int *radiuses, int max_nb, double mean, const int *nodes,
-                       int n_nodes, int *out_idx, int *out_count, unsigned char *out_path,
-                       double *out_est, double *out_var, float *out_est_f, int *out_status,
-                       int precision, int n_threads)
+                       const int *radiuses, int max_nb, double mean, const float *means,
+                       const int *nodes, int n_nodes, int *out_idx, int *out_count,
+                       unsigned char *out_path, double *out_est, double *out_var, float *out_est_f,
+                       int *out_status, int precision, int n_threads)
 {
     Grid g = {dims[0], dims[1], dims[2]};
     Flavour f;
@@ -565,6 +567,7 @@ static int krige_nodes(int kind, const int *dims, const float *data_f, const uns
     s.init(g, f, max_nb, mask);
     bool ordinary = (kind == 0);
     if (ordinary) mean = 0.0; // OK combines with no_mean_t (ordinary_kriging.cpp:31, mean_provider.h:8-15)
+    if (ordinary) means = nullptr;
     if (n_threads > 0) omp_set_num_threads(n_threads);
 #pragma omp parallel for schedule(dynamic, 64)
     for (int t = 0; t < n_nodes; ++t)
@@ -577,14 +580,14 @@ static int krige_nodes(int kind, const int *dims, const float *data_f, const uns
         if (data_u8)
         {
             auto vo = [&](int i) -> float { return data_u8[i] == ind_value ? 1.0f : 0.0f; };
-            st = precision ? krige_node<long double>(s, ordinary, mean, nodes[t], vo, idx, path, est, var, est_f)
-                           : krige_node<double>(s, ordinary, mean, nodes[t], vo, idx, path, est, var, est_f);
+            st = precision ? krige_node<long double>(s, ordinary, mean, means, nodes[t], vo, idx, path, est, var, est_f)
+                           : krige_node<double>(s, ordinary, mean, means, nodes[t], vo, idx, path, est, var, est_f);
         }
         else
         {
             auto vo = [&](int i) -> float { return data_f[i]; };
-            st = precision ? krige_node<long double>(s, ordinary, mean, nodes[t], vo, idx, path, est, var, est_f)
-                           : krige_node<double>(s, ordinary, mean, nodes[t], vo, idx, path, est, var, est_f);
+            st = precision ? krige_node<long double>(s, ordinary, mean, means, nodes[t], vo, idx, path, est, var, est_f)
+                           : krige_node<double>(s, ordinary, mean, means, nodes[t], vo, idx, path, est, var, est_f);
         }
         if (out_idx)
             for (int i = 0; i < max_nb; ++i)
@@ -607,7 +610,7 @@ int ko_krige_cont(int kind, const int *dims, const float *data, const unsigned c
                   int precision, int n_threads)
 {
     return krige_nodes(kind, dims, data, nullptr, -1, mask, cov_type, ranges, angles, sill, nugget,
-                       radiuses, max_nb, mean, nodes, n_nodes, out_idx, out_count, out_path,
+                       radiuses, max_nb, mean, nullptr, nodes, n_nodes, out_idx, out_count, out_path,
                        out_est, out_var, out_est_f, out_status, precision, n_threads);
 }
 
@@ -619,7 +622,7 @@ int ko_krige_ind(int kind, const int *dims, const unsigned char *data, const uns
                  int *out_status, int precision, int n_threads)
 {
     return krige_nodes(kind, dims, nullptr, data, ind_value, mask, cov_type, ranges, angles, sill,
-                       nugget, radiuses, max_nb, mean, nodes, n_nodes, out_idx, out_count,
+                       nugget, radiuses, max_nb, mean, nullptr, nodes, n_nodes, out_idx, out_count,
                        out_path, out_est, out_var, out_est_f, out_status, precision, n_threads);
 }
 
@@ -685,6 +688,47 @@ int ko_cont_grid(int kind, const int *dims, const float *data, const unsigned ch
             out_data[i] = (float)mean;
             out_mask[i] = 1;
         }
+    }
+    return 0;
+}
+
+// LVM kriging (lvm_kriging.cpp:16-39): cont_kriging with the box-truncated
+// covariance table, SK weights and the per-node mean array as the mean
+// provider (combine centres each neighbour on its own mean and adds the
+// node's); failures get the node's mean (mean_on_failure).
+int ko_lvm_grid(const int *dims, const float *data, const unsigned char *mask, const float *means,
+                int cov_type, const double *ranges, const double *angles, double sill, double nugget,
+                const int *radiuses, int max_nb, float *out_data, unsigned char *out_mask, double *out_est,
+                double *out_var, int *out_status, int n_threads)
+{
+    long size = (long)dims[0] * dims[1] * dims[2];
+    std::vector<int> nodes;
+    for (long i = 0; i < size; ++i)
+        if (!mask[i]) nodes.push_back((int)i);
+    std::vector<float> ef(nodes.size());
+    std::vector<double> ed(nodes.size()), vd(nodes.size());
+    std::vector<int> st(nodes.size());
+    int rc = krige_nodes(1, dims, data, nullptr, -1, mask, cov_type, ranges, angles, sill, nugget, radiuses,
+                         max_nb, 0.0, means, nodes.data(), (int)nodes.size(), nullptr, nullptr, nullptr,
+                         ed.data(), vd.data(), ef.data(), st.data(), 0, n_threads);
+    if (rc) return rc;
+    for (long i = 0; i < size; ++i)
+        if (mask[i])
+        {
+            out_data[i] = data[i];
+            out_mask[i] = 1;
+            if (out_est) out_est[i] = data[i];
+            if (out_var) out_var[i] = 0;
+            if (out_status) out_status[i] = -1;
+        }
+    for (size_t t = 0; t < nodes.size(); ++t)
+    {
+        int i = nodes[t];
+        if (out_est) out_est[i] = ed[t];
+        if (out_var) out_var[i] = vd[t];
+        if (out_status) out_status[i] = st[t];
+        out_data[i] = st[t] == KI_SUCCESS ? ef[t] : means[i];
+        out_mask[i] = 1;
     }
     return 0;
 }

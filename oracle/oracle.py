@@ -58,6 +58,8 @@ def load(which: str):
                                      _d, _d, _f, _i, C.c_int, C.c_int]
         lib.ko_cont_grid.argtypes = [C.c_int, _i, _f, _u8, C.c_int, _d, _d, C.c_double, C.c_double,
                                      _i, C.c_int, C.c_int, C.c_double, _f, _u8, _d, _d, _i, C.c_int]
+        lib.ko_lvm_grid.argtypes = [_i, _f, _u8, _f, C.c_int, _d, _d, C.c_double, C.c_double, _i,
+                                    C.c_int, _f, _u8, _d, _d, _i, C.c_int]
         lib.ko_indicator_grid.argtypes = [_i, _u8, _u8, C.c_int, _i, _d, _d, _d, _d, _i, _i, _d,
                                           _u8, _u8, _f, C.c_int]
         lib.ko_median_ik_grid.argtypes = [_i, _u8, _u8, C.c_int, _d, _d, C.c_double, C.c_double,
@@ -222,6 +224,27 @@ def cont_grid(kind, dims, data, mask, cov, radiuses, k, mean=None, threads=0):
                           _ptr(st, _i), int(threads))
     if rc:
         raise RuntimeError("cont_grid failed")
+    return out_d, out_m, est, var, st
+
+
+def lvm_grid(dims, data, mask, means, cov, radiuses, k, threads=0):
+    """Whole-grid LVM kriging with the reference's output rules (port)."""
+    lib = load("port")
+    data = _arr(data, np.float32)
+    mask = _arr(mask, np.uint8)
+    means = _arr(means, np.float32)
+    out_d = data.copy()
+    out_m = mask.copy()
+    est = np.zeros(len(data), np.float64)
+    var = np.zeros(len(data), np.float64)
+    st = np.zeros(len(data), np.int32)
+    rc = lib.ko_lvm_grid(_ptr(_arr(dims, np.int32), _i), _ptr(data, _f), _ptr(mask, _u8), _ptr(means, _f),
+                         int(cov.cov_type), _ptr(_arr(cov.ranges, np.float64), _d),
+                         _ptr(_arr(cov.angles, np.float64), _d), float(cov.sill), float(cov.nugget),
+                         _ptr(_arr(radiuses, np.int32), _i), int(k), _ptr(out_d, _f), _ptr(out_m, _u8),
+                         _ptr(est, _d), _ptr(var, _d), _ptr(st, _i), int(threads))
+    if rc:
+        raise RuntimeError("lvm_grid failed")
     return out_d, out_m, est, var, st
 
 

@@ -4,7 +4,8 @@ Run here, where the reference sources are present and oracle/Makefile has built
 oracle/_ref/ (the reference's unmodified library, libhpgl.so, and the white-box
 harness libref_harness.so around its own templates):
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle && python tests/golden/make_golden.py        (all fixtures)
+                      python tests/golden/make_golden.py lvm    (lvm.npz only)
 
 Inputs are the seeded workloads of geo_bsd.workloads at reduced scale (the
 conditioning cells are stored in each file, so the fixtures do not depend on
@@ -12,8 +13,8 @@ the generator). Outputs per sampled node: the reference's neighbour indices in
 its own order, the search path taken, the FP64 estimate and variance of
 kriging_interpolation with result_t = double, the float estimate the drivers
 store, and the status code. Whole-grid outputs of the reference's public C API
-(hpgl_ordinary_kriging, hpgl_simple_kriging, hpgl_indicator_kriging,
-hpgl_median_ik) are stored for the small grids, plus the known-answer cases
+(hpgl_ordinary_kriging, hpgl_simple_kriging, hpgl_lvm_kriging,
+hpgl_indicator_kriging, hpgl_median_ik) are stored for the small grids, plus the known-answer cases
 of the reference's test suite (constant field 42, all zeros).
 """
 import ctypes as C
@@ -98,6 +99,21 @@ def api_cont(lib, kind, dims, data, mask, cov, rad, k, mean=None):
     return od, om
 
 
+def api_lvm(lib, dims, data, mask, means, cov, rad, k):
+    data = np.ascontiguousarray(data, np.float32)
+    mask = np.ascontiguousarray(mask, np.uint8)
+    means = np.ascontiguousarray(means, np.float32)
+    od, om = data.copy(), mask.copy()
+    fp = C.POINTER(C.c_float)
+    up = C.POINTER(C.c_ubyte)
+    p = OkP(cov.cov_type, (C.c_double * 3)(*cov.ranges), (C.c_double * 3)(*cov.angles), cov.sill, cov.nugget,
+            (C.c_int * 3)(*rad), k)
+    sh = _shape(dims)
+    lib.hpgl_lvm_kriging(data.ctypes.data_as(fp), mask.ctypes.data_as(up), C.byref(sh), means.ctypes.data_as(fp),
+                         C.byref(sh), C.byref(p), od.ctypes.data_as(fp), om.ctypes.data_as(up), C.byref(sh))
+    return od, om
+
+
 def api_ik(lib, dims, data, mask, covs, rads, ks, marginals):
     data = np.ascontiguousarray(data, np.uint8)
     mask = np.ascontiguousarray(mask, np.uint8)
@@ -157,8 +173,26 @@ def cont_case(lib, wl, name, kinds=(0, 1), sample=SAMPLE, grid_api=False):
     print("wrote", name, {k: v.shape for k, v in out.items() if hasattr(v, "shape") and v.size > 3})
 
 
-def main():
+def lvm_cases(lib):
+    """LVM kriging (hpgl_lvm_kriging) on the small grids with a smooth trend as
+    the mean; the inputs are those of the OK/SK fixtures of the same names."""
+    out = {}
+    for name, wl in (("ok_small_s030", WL.ok_small(0.3)), ("gauss_cv_s020", WL.gauss_cv(0.2))):
+        m = WL.lvm_means(wl.dims)
+        od, om = api_lvm(lib, wl.dims, wl.data, wl.mask, m, wl.cov, wl.radiuses, wl.max_neighbours)
+        out[f"{name}_means"] = m
+        out[f"{name}_grid_data"] = od
+        out[f"{name}_grid_mask"] = om
+    np.savez_compressed(os.path.join(HERE, "lvm.npz"), **out)
+    print("wrote lvm")
+
+
+def main(only=None):
     lib = _api()
+    if only == "lvm":
+        lvm_cases(lib)
+        return
+    lvm_cases(lib)
     cont_case(lib, WL.ok_small(0.3), "ok_small_s030", grid_api=True)
     cont_case(lib, WL.sk_ok_large(0.16), "sk_ok_large_s016")
     cont_case(lib, WL.gauss_cv(0.2), "gauss_cv_s020", grid_api=True)
@@ -212,4 +246,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1] if len(sys.argv) > 1 else None)

@@ -37,6 +37,34 @@ def engine_cont(kind, wl, precision=0, refine_steps=2, mean=None, cov=None, radi
     return {"data": out_d, "mask": out_m, "est": est, "var": var, "status": st, "stats": W.last_stats()}
 
 
+def ok_params(cov, radiuses, k):
+    return W._HPGL_OK_PARAMS(covariance_type=cov.cov_type, ranges=tuple(cov.ranges), angles=tuple(cov.angles),
+                             sill=cov.sill, nugget=cov.nugget, radiuses=tuple(int(r) for r in radiuses),
+                             max_neighbours=int(k))
+
+
+def engine_lvm(wl, means, precision=0, refine_steps=2, flags=0):
+    """Whole-grid LVM kriging through hpgl_b200_lvm_kriging_ex with host buffers."""
+    n = wl.n_cells
+    dims = (C.c_int * 3)(*wl.dims)
+    data = np.ascontiguousarray(wl.data, np.float32)
+    mask = np.ascontiguousarray(wl.mask, np.uint8)
+    means = np.ascontiguousarray(means, np.float32)
+    out_d = data.copy()
+    out_m = mask.copy()
+    est = np.full(n, np.nan)
+    var = np.full(n, np.nan)
+    st = np.zeros(n, np.int8)
+    opt = W._HPGL_B200_OPTIONS(precision=precision, refine_steps=refine_steps, flags=W.FLAG_OUT_IS_CLONE | flags,
+                               stream=None, estimate64=est.ctypes.data, variance=var.ctypes.data,
+                               status=st.ctypes.data, ik_probs=None)
+    p = ok_params(wl.cov, wl.radiuses, wl.max_neighbours)
+    rc = W._hpgl_so.hpgl_b200_lvm_kriging_ex(dims, data.ctypes.data, mask.ctypes.data, means.ctypes.data, C.byref(p),
+                                             out_d.ctypes.data, out_m.ctypes.data, C.byref(opt))
+    W.check(rc, "lvm_kriging_ex")
+    return {"data": out_d, "mask": out_m, "est": est, "var": var, "status": st, "stats": W.last_stats()}
+
+
 def engine_neighbours(kind, wl, nodes, cov=None, radiuses=None, k=None, mask=None):
     cov = cov or wl.cov
     radiuses = radiuses or wl.radiuses

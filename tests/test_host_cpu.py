@@ -132,3 +132,24 @@ def test_kriging_without_gpu_reports_an_error():
                                               out.ctypes.data, om.ctypes.data, None)
     assert rc == -2
     np.testing.assert_array_equal(out, wl.data)
+
+
+def test_lvm_entry_argument_checks():
+    """LVM: a missing mean array is EINVAL before any device work; without a GPU the
+    call returns ECUDA and leaves the output untouched."""
+    wl = WL.ok_small(0.2)
+    dims = (C.c_int * 3)(*wl.dims)
+    p = W._HPGL_OK_PARAMS(covariance_type=0, ranges=wl.cov.ranges, angles=wl.cov.angles, sill=1.0, nugget=0.1,
+                          radiuses=wl.radiuses, max_neighbours=12)
+    out = wl.data.copy()
+    om = wl.mask.copy()
+    fn = W._hpgl_so.hpgl_b200_lvm_kriging_ex
+    assert fn(dims, wl.data.ctypes.data, wl.mask.ctypes.data, None, C.byref(p), out.ctypes.data, om.ctypes.data,
+              None) == W.EINVAL
+    import torch
+    if torch.cuda.is_available():
+        return
+    means = WL.lvm_means(wl.dims)
+    assert fn(dims, wl.data.ctypes.data, wl.mask.ctypes.data, means.ctypes.data, C.byref(p), out.ctypes.data,
+              om.ctypes.data, None) == W.ECUDA
+    np.testing.assert_array_equal(out, wl.data)

@@ -39,6 +39,22 @@ def test_oracle_whole_grid_matches_reference_api(case, tag, kind):
     assert np.abs(od - ref).max() <= 4e-7 * max(np.abs(ref).max(), 1.0)
 
 
+@pytest.mark.parametrize("case", ["ok_small_s030", "gauss_cv_s020"])
+def test_oracle_lvm_matches_reference_api(case):
+    """LVM kriging: the restatement's grid against hpgl_lvm_kriging's output."""
+    g = G.load(case)
+    lv = G.load("lvm")
+    wl = G.as_workload(g, case)
+    means = lv[f"{case}_means"]
+    od, om, _, _, st = O.lvm_grid(wl.dims, wl.data, wl.mask, means, wl.cov, wl.radiuses, wl.max_neighbours,
+                                  threads=4)
+    np.testing.assert_array_equal(om, lv[f"{case}_grid_mask"])
+    ref = lv[f"{case}_grid_data"]
+    assert np.abs(od - ref).max() <= 4e-7 * max(np.abs(ref).max(), 1.0)
+    failed = (wl.mask == 0) & (st != 0)
+    np.testing.assert_array_equal(ref[failed], means[failed])  # mean_on_failure
+
+
 def test_oracle_indicator_matches_reference():
     g = G.load("indicator_s015")
     dims, data, mask = G.grid_inputs(g, dtype=np.uint8)
