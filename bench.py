@@ -12,6 +12,9 @@ variance for every uninformed cell. `value` has the inputs resident in HBM
 with pinned HOST buffers, so each step includes the host->device copy of data
 and mask and the device->host copy of estimate, mask and variance.
 
+`--kind sk|lvm` runs simple kriging or kriging with a locally varying mean
+(a smooth trend, geo_bsd.workloads.lvm_means) on the same grid instead.
+
 Usage:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 For N > 1 the driver runs it under torchrun; every rank runs its own replica
 (the path needs no collective) and rank 0 prints one JSON line.
@@ -43,7 +46,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--workload", default="sk_ok_large")
-    ap.add_argument("--kind", choices=["ok", "sk"], default="ok")
+    ap.add_argument("--kind", choices=["ok", "sk", "lvm"], default="ok")
     ap.add_argument("--skip-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--profile-case", type=float, default=0.0, metavar="SCALE",
@@ -66,6 +69,14 @@ def load_workload(name):
     return WL.ALL[name](1.0)
 
 
+def lvm_means(wl):
+    from geo_bsd import workloads as WL
+    return WL.lvm_means(wl.dims)
+
+
+KIND_NAMES = {"ok": "ordinary kriging", "sk": "simple kriging", "lvm": "LVM kriging (smooth trend mean)"}
+
+
 # ---------------------------------------------------------------- CPU baseline
 def cpu_reference(wl, kind, target_seconds, threads):
     """Reference CPU path (oracle/_ref, the reference's own code) on a sample of
@@ -78,11 +89,12 @@ def cpu_reference(wl, kind, target_seconds, threads):
     rng = np.random.default_rng(123)
     k = 0 if kind == "ok" else 1
     mean = float(wl.data[wl.mask == 1].astype(np.float64).mean()) if kind == "sk" else 0.0
+    means = lvm_means(wl) if kind == "lvm" else None
 
     def timed(nodes):
         t0 = time.perf_counter()
         O.krige_nodes(which, k, wl.dims, wl.data, wl.mask, wl.cov, wl.radiuses, wl.max_neighbours, mean=mean,
-                      nodes=nodes, threads=threads, want_idx=False)
+                      nodes=nodes, threads=threads, want_idx=False, means=means)
         return time.perf_counter() - t0
 
     setup = timed(np.zeros(0, np.int32))  # template + clusterizer construction only
@@ -211,6 +223,7 @@ def main():
     else:
         wl = load_workload(args.workload)
     kind = 0 if args.kind == "ok" else 1
+    lvm = args.kind == "lvm"
     n = wl.n_cells
     dev = torch.device("cuda", local)
     d_data = torch.from_numpy(np.ascontiguousarray(wl.data)).to(dev)
@@ -225,15 +238,26 @@ def main():
     p = W._HPGL_SK_PARAMS(covariance_type=wl.cov.cov_type, ranges=wl.cov.ranges, angles=wl.cov.angles,
                           sill=wl.cov.sill, nugget=wl.cov.nugget, radiuses=wl.radiuses,
                           max_neighbours=wl.max_neighbours, automatic_mean=1, mean=0.0)
+    p_ok = W._HPGL_OK_PARAMS(covariance_type=wl.cov.cov_type, ranges=wl.cov.ranges, angles=wl.cov.angles,
+                             sill=wl.cov.sill, nugget=wl.cov.nugget, radiuses=wl.radiuses,
+                             max_neighbours=wl.max_neighbours)
+    h_means = lvm_means(wl) if lvm else None
+    d_means = torch.from_numpy(h_means).to(dev) if lvm else None
+
+    def krige(data, mask, means, out, omask, o):
+        if lvm:
+            return W._hpgl_so.hpgl_b200_lvm_kriging_ex(dims, data, mask, means, C.byref(p_ok), out, omask,
+                                                       C.byref(o))
+        return W._hpgl_so.hpgl_b200_cont_kriging_ex(kind, dims, data, mask, C.byref(p), out, omask, C.byref(o))
 
     def dev_call(precision, est=False):
         o = W._HPGL_B200_OPTIONS(precision=precision, refine_steps=3,
                                  flags=W.FLAG_DEVICE_POINTERS | W.FLAG_OUT_IS_CLONE, stream=stream.cuda_stream,
                                  estimate64=d_est.data_ptr() if est else None, variance=d_var.data_ptr(),
                                  status=None, ik_probs=None)
-        rc = W._hpgl_so.hpgl_b200_cont_kriging_ex(kind, dims, d_data.data_ptr(), d_mask.data_ptr(), C.byref(p),
-                                                  d_out.data_ptr(), d_omask.data_ptr(), C.byref(o))
-        W.check(rc, "cont_kriging_ex")
+        rc = krige(d_data.data_ptr(), d_mask.data_ptr(), d_means.data_ptr() if lvm else None, d_out.data_ptr(),
+                   d_omask.data_ptr(), o)
+        W.check(rc, "kriging_ex")
         return W.last_stats()
 
     def barrier():
@@ -299,8 +323,9 @@ def main():
     b_flops = last[f"bucket_flops_{b}"]
     achieved = b_flops / (b_ms / 1e3) / 1e12
     tpc = traffic_per_cell()
-    kname = (f"k_solve_fold<NP={[8, 16, 32][b]}, ordinary> (FP32 refined, NP/2 lanes per system)" if b < 3
-             else "k_solve<NP=64, float, ordinary, refined>" if b == 3 else "k_solve_large")
+    ordn = "ordinary" if kind == 0 and not lvm else "simple"
+    kname = (f"k_solve_fold<NP={[8, 16, 32][b]}, {ordn}> (FP32 refined, NP/2 lanes per system)" if b < 3
+             else f"k_solve_fold<NP=64, {ordn}> (FP32 refined)" if b == 3 else "k_solve_large")
     roofline = {"bound": "fp32", "kernel": kname,
                 "achieved": achieved, "peak": pk["fp32"], "unit": "TFLOP/s", "frac": achieved / pk["fp32"],
                 "traffic": (tpc * last[f"bucket_items_{b}"]) if tpc else None,
@@ -313,8 +338,10 @@ def main():
     # end to end through the C ABI with pinned host buffers
     lib = W._hpgl_so
     nbytes = n * 4
-    h_ptrs = [lib.hpgl_b200_host_alloc(sz) for sz in (nbytes, n, nbytes, n, n * 8)]
-    h_data, h_mask, h_out, h_omask, h_var = h_ptrs
+    h_ptrs = [lib.hpgl_b200_host_alloc(sz) for sz in (nbytes, n, nbytes, n, n * 8, nbytes)]
+    h_data, h_mask, h_out, h_omask, h_var, h_mean = h_ptrs
+    if lvm:
+        C.memmove(h_mean, h_means.ctypes.data, nbytes)
     C.memmove(h_data, np.ascontiguousarray(wl.data).ctypes.data, nbytes)
     C.memmove(h_mask, np.ascontiguousarray(wl.mask).ctypes.data, n)
     C.memmove(h_out, h_data, nbytes)
@@ -323,8 +350,8 @@ def main():
     def host_call():
         o = W._HPGL_B200_OPTIONS(precision=1, refine_steps=3, flags=W.FLAG_OUT_IS_CLONE, stream=None,
                                  estimate64=None, variance=h_var, status=None, ik_probs=None)
-        rc = lib.hpgl_b200_cont_kriging_ex(kind, dims, h_data, h_mask, C.byref(p), h_out, h_omask, C.byref(o))
-        W.check(rc, "cont_kriging_ex (host)")
+        rc = krige(h_data, h_mask, h_mean if lvm else None, h_out, h_omask, o)
+        W.check(rc, "kriging_ex (host)")
         return W.last_stats()
 
     for _ in range(args.warmup):
@@ -356,7 +383,7 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (FP64-refined residuals)", "data": "synthetic (seeded, geo_bsd.workloads)",
-            "config": {"workload": f"{'ordinary' if kind == 0 else 'simple'} kriging {wl.dims[0]}x{wl.dims[1]}x"
+            "config": {"workload": f"{KIND_NAMES[args.kind]} {wl.dims[0]}x{wl.dims[1]}x"
                                    f"{wl.dims[2]}, 1% lognormal conditioning, exponential (30,15,6) az 30, "
                                    f"k={wl.max_neighbours}", "precision": "fp32_refined",
                        "l2": "flushed between timed steps (256 MB write)",

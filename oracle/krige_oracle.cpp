@@ -614,6 +614,18 @@ int ko_krige_cont(int kind, const int *dims, const float *data, const unsigned c
                        out_est, out_var, out_est_f, out_status, precision, n_threads);
 }
 
+// LVM at the listed nodes: the SK flavour with a mean per node (lvm_kriging.cpp:28-34).
+int ko_krige_lvm(const int *dims, const float *data, const unsigned char *mask, const float *means,
+                 int cov_type, const double *ranges, const double *angles, double sill, double nugget,
+                 const int *radiuses, int max_nb, const int *nodes, int n_nodes, int *out_idx,
+                 int *out_count, unsigned char *out_path, double *out_est, double *out_var,
+                 float *out_est_f, int *out_status, int precision, int n_threads)
+{
+    return krige_nodes(1, dims, data, nullptr, -1, mask, cov_type, ranges, angles, sill, nugget, radiuses,
+                       max_nb, 0.0, means, nodes, n_nodes, out_idx, out_count, out_path, out_est, out_var,
+                       out_est_f, out_status, precision, n_threads);
+}
+
 int ko_krige_ind(int kind, const int *dims, const unsigned char *data, const unsigned char *mask,
                  int ind_value, int cov_type, const double *ranges, const double *angles,
                  double sill, double nugget, const int *radiuses, int max_nb, double mean,

@@ -53,6 +53,8 @@ def load(which: str):
         lib.ko_krige_cont.argtypes = [C.c_int, _i, _f, _u8, C.c_int, _d, _d, C.c_double, C.c_double,
                                       _i, C.c_int, C.c_double, _i, C.c_int, _i, _i, _u8, _d, _d,
                                       _f, _i, C.c_int, C.c_int]
+        lib.ko_krige_lvm.argtypes = [_i, _f, _u8, _f, C.c_int, _d, _d, C.c_double, C.c_double, _i, C.c_int,
+                                     _i, C.c_int, _i, _i, _u8, _d, _d, _f, _i, C.c_int, C.c_int]
         lib.ko_krige_ind.argtypes = [C.c_int, _i, _u8, _u8, C.c_int, C.c_int, _d, _d, C.c_double,
                                      C.c_double, _i, C.c_int, C.c_double, _i, C.c_int, _i, _i, _u8,
                                      _d, _d, _f, _i, C.c_int, C.c_int]
@@ -82,6 +84,8 @@ def load(which: str):
         lib.ref_krige_ind.argtypes = [C.c_int, _i, _u8, _u8, C.c_int, C.c_int, _d, _d, C.c_double,
                                       C.c_double, _i, C.c_int, C.c_double, _i, C.c_int, _i, _i,
                                       _u8, _d, _d, _f, _i, C.c_int]
+        lib.ref_krige_lvm.argtypes = [_i, _f, _u8, _f, C.c_int, _d, _d, C.c_double, C.c_double, _i, C.c_int,
+                                      _i, C.c_int, _i, _i, _u8, _d, _d, _f, _i, C.c_int]
         lib.ref_template.argtypes = [C.c_int, C.c_int, _d, _d, C.c_double, C.c_double, _i, _i,
                                      C.c_int, _i]
         lib.ref_cov.argtypes = [C.c_int, C.c_int, _d, _d, C.c_double, C.c_double, _i, _i, _i]
@@ -102,11 +106,12 @@ def available(which: str) -> bool:
 
 
 def krige_nodes(which, kind, dims, data, mask, cov, radiuses, k, mean=0.0, nodes=None,
-                ind_value: Optional[int] = None, precision=0, threads=0, want_idx=True):
+                ind_value: Optional[int] = None, precision=0, threads=0, want_idx=True, means=None):
     """Per-node kriging at `nodes` (default: every uninformed cell).
 
     kind 0 = OK (analytic covariance), 1 = SK / IK (truncated table),
-    2 = median-IK flavour (truncated field; same values as 1).
+    2 = median-IK flavour (truncated field; same values as 1). `means` (one
+    float per grid cell) makes it LVM kriging (kind and mean are then unused).
     Returns a dict with idx (n,k; -1 padded), count, path (ref: template path
     flag; port: same), est (f64), var (f64), est_f (f32), status.
     """
@@ -132,7 +137,16 @@ def krige_nodes(which, kind, dims, data, mask, cov, radiuses, k, mean=0.0, nodes
     common_tail = [_ptr(nodes, _i), n, _ptr(out["idx"], _i), _ptr(out["count"], _i),
                    _ptr(out["path"], _u8), _ptr(out["est"], _d), _ptr(out["var"], _d),
                    _ptr(out["est_f"], _f), _ptr(out["status"], _i)]
-    if ind_value is None:
+    if means is not None:
+        data = _arr(data, np.float32)
+        means = _arr(means, np.float32)
+        head = [_ptr(dims_a, _i), _ptr(data, _f), _ptr(mask, _u8), _ptr(means, _f), int(cov.cov_type),
+                _ptr(ranges, _d), _ptr(angles, _d), float(cov.sill), float(cov.nugget), _ptr(rad, _i), int(k)]
+        if which == "port":
+            rc = lib.ko_krige_lvm(*head, *common_tail, int(precision), int(threads))
+        else:
+            rc = lib.ref_krige_lvm(*head, *common_tail, int(threads))
+    elif ind_value is None:
         data = _arr(data, np.float32)
         head = [kind, _ptr(dims_a, _i), _ptr(data, _f), _ptr(mask, _u8), int(cov.cov_type),
                 _ptr(ranges, _d), _ptr(angles, _d), float(cov.sill), float(cov.nugget),

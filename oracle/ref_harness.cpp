@@ -176,6 +176,36 @@ int ref_krige_cont(int kind, const int *dims, const float *data, const unsigned 
     }
 }
 
+// LVM kriging at the listed nodes, instantiated as lvm_kriging does
+// (lvm_kriging.cpp:28-34): truncated covariances, SK weights and the per-cell
+// mean array itself as the mean provider.
+int ref_krige_lvm(const int *dims, const float *data, const unsigned char *mask, const float *means,
+                  int cov_type, const double *ranges, const double *angles, double sill, double nugget,
+                  const int *radiuses, int max_nb, const int *nodes, int n_nodes, int *out_idx,
+                  int *out_count, unsigned char *out_path, double *out_est, double *out_var,
+                  float *out_est_f, int *out_status, int n_threads)
+{
+    try
+    {
+        sugarbox_grid_t grid;
+        grid.init(dims[0], dims[1], dims[2]);
+        int size = dims[0] * dims[1] * dims[2];
+        cont_property_array_t prop(const_cast<float *>(data), const_cast<unsigned char *>(mask), size);
+        covariance_param_t cp = make_cov(cov_type, ranges, angles, sill, nugget);
+        neighbourhood_param_t nb = make_nb(radiuses, max_nb);
+        precalculated_covariances_t cov(cov_model_t(cp), nb.m_radiuses);
+        const mean_t *mp = means;
+        run_nodes(grid, cov, nb, prop, prop, mp, sk_weight_calculator_t(), nodes, n_nodes, max_nb, out_idx,
+                  out_count, out_path, out_est, out_var, out_est_f, out_status, n_threads);
+        if (out_path) run_paths(grid, cov, nb, prop, nodes, n_nodes, out_path, 0, 0);
+        return 0;
+    }
+    catch (const std::exception &)
+    {
+        return -1;
+    }
+}
+
 // Indicator SK at the listed nodes for indicator value `ind_value`: IK per
 // category (kind == 1, precalculated covariances, indicator_kriging.h:135) or
 // median IK (kind == 2, covariance_field_t, median_ik.cpp:258-264).

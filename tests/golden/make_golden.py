@@ -174,8 +174,10 @@ def cont_case(lib, wl, name, kinds=(0, 1), sample=SAMPLE, grid_api=False):
 
 
 def lvm_cases(lib):
-    """LVM kriging (hpgl_lvm_kriging) on the small grids with a smooth trend as
-    the mean; the inputs are those of the OK/SK fixtures of the same names."""
+    """LVM kriging on the small grids with a smooth trend as the mean: the whole
+    grid through hpgl_lvm_kriging and per-node results of the reference's
+    templates instantiated as lvm_kriging does; the inputs are those of the
+    OK/SK fixtures of the same names."""
     out = {}
     for name, wl in (("ok_small_s030", WL.ok_small(0.3)), ("gauss_cv_s020", WL.gauss_cv(0.2))):
         m = WL.lvm_means(wl.dims)
@@ -183,6 +185,14 @@ def lvm_cases(lib):
         out[f"{name}_means"] = m
         out[f"{name}_grid_data"] = od
         out[f"{name}_grid_mask"] = om
+        rng = np.random.default_rng(7)
+        unk = np.flatnonzero(wl.mask == 0)
+        nodes = np.sort(rng.choice(unk, min(SAMPLE, len(unk)), replace=False)).astype(np.int32)
+        r = O.krige_nodes("ref", 1, wl.dims, wl.data, wl.mask, wl.cov, wl.radiuses, wl.max_neighbours, nodes=nodes,
+                          threads=8, means=m)
+        out[f"{name}_nodes"] = nodes
+        for key in ("idx", "count", "path", "est", "var", "est_f", "status"):
+            out[f"{name}_{key}"] = r[key]
     np.savez_compressed(os.path.join(HERE, "lvm.npz"), **out)
     print("wrote lvm")
 

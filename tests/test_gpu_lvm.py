@@ -45,6 +45,23 @@ def test_lvm_grid_matches_reference_api(case):
     assert np.abs(out_d.reshape(-1, order="F") - ref).max() <= 1e-6 * max(np.abs(ref).max(), 1.0)
 
 
+@pytest.mark.parametrize("case", ["ok_small_s030", "gauss_cv_s020"])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_lvm_estimates_match_reference_per_node(case, precision):
+    """FP64 estimates and variances of the reference's own LVM instantiation."""
+    g = G.load(case)
+    lv = G.load("lvm")
+    wl = G.as_workload(g, case)
+    e = H.engine_lvm(wl, lv[f"{case}_means"], precision=precision)
+    nodes = lv[f"{case}_nodes"]
+    st = e["status"][nodes]
+    np.testing.assert_array_equal(st, lv[f"{case}_status"].astype(np.int8))
+    ok = st == 0
+    tol = FP64_TOL if precision == 0 else FP32_TOL
+    assert H.rel_err(e["est"][nodes][ok], lv[f"{case}_est"][ok]) <= tol
+    assert H.rel_err(e["var"][nodes][ok], lv[f"{case}_var"][ok]) <= tol
+
+
 @pytest.mark.parametrize("name,scale", [("ok_small", 0.6), ("sk_ok_large", 0.3), ("gauss_cv", 0.35),
                                         ("clustered", 0.2)])
 def test_lvm_against_oracle(name, scale):

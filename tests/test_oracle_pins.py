@@ -55,6 +55,22 @@ def test_oracle_lvm_matches_reference_api(case):
     np.testing.assert_array_equal(ref[failed], means[failed])  # mean_on_failure
 
 
+@pytest.mark.parametrize("case", ["ok_small_s030", "gauss_cv_s020"])
+def test_oracle_lvm_matches_reference_per_node(case):
+    g = G.load(case)
+    lv = G.load("lvm")
+    wl = G.as_workload(g, case)
+    r = O.krige_nodes("port", 1, wl.dims, wl.data, wl.mask, wl.cov, wl.radiuses, wl.max_neighbours,
+                      nodes=lv[f"{case}_nodes"], threads=4, means=lv[f"{case}_means"])
+    for key in ("idx", "count", "path", "status"):
+        np.testing.assert_array_equal(r[key], lv[f"{case}_{key}"])
+    ok = lv[f"{case}_status"] == 0
+    ref = lv[f"{case}_est"][ok]
+    assert np.abs(r["est"][ok] - ref).max() <= 1e-12 * max(np.abs(ref).max(), 1.0)
+    assert np.abs(r["var"][ok] - lv[f"{case}_var"][ok]).max() <= 1e-12
+    assert np.abs(r["est_f"][ok] - lv[f"{case}_est_f"][ok]).max() <= 4e-7 * max(np.abs(ref).max(), 1.0)
+
+
 def test_oracle_indicator_matches_reference():
     g = G.load("indicator_s015")
     dims, data, mask = G.grid_inputs(g, dtype=np.uint8)
