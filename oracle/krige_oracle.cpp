@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <random>
 #include <vector>
 #include <omp.h>
 
@@ -510,6 +511,116 @@ static int argmax_first(const std::vector<float> &p)
         }
     return k;
 }
+
+// ---------------------------------------------------------------- SGS
+// path_random_generator.cpp:24-67. A linear congruential walk R <- (A R + C)
+// mod size over every node, started at seed % size: A = 1 + the product of the
+// primes dividing size (doubled when 4 divides size), C = the largest prime not
+// above size / 3 that does not divide size (2 when there is none). The primes
+// are walked in ascending order as the reference walks its prime table.
+struct PathLcg
+{
+    long long A = 1, C = 2, M = 1, R = 0;
+    bool init(long long size, long long seed)
+    {
+        if (size <= 0 || size > 10000000) return false;
+        std::vector<int> primes; // ascending, up to the first prime above size
+        {
+            long long lim = size + 64;
+            std::vector<char> comp((size_t)lim + 1, 0);
+            for (long long i = 2; i <= lim; ++i)
+            {
+                if (comp[(size_t)i]) continue;
+                primes.push_back((int)i);
+                if (i > size) break;
+                for (long long j = i * i; j <= lim; j += i) comp[(size_t)j] = 1;
+            }
+        }
+        M = size;
+        A = 1;
+        size_t idx = 0;
+        for (; idx < primes.size(); ++idx)
+        {
+            if (primes[idx] > size) break;
+            if (size % primes[idx] == 0) A *= primes[idx];
+        }
+        if (M % 4 == 0) A *= 2;
+        A += 1;
+        idx = 0;
+        while (idx + 1 < primes.size() && primes[idx + 1] <= size / 3) ++idx;
+        for (long long k = (long long)idx; k >= 0; --k)
+        {
+            C = primes[(size_t)k];
+            if (std::floor(double(size) / double(C)) != double(size) / double(C)) break;
+        }
+        R = seed % size;
+        return R >= 0;
+    }
+    int next()
+    {
+        int r = (int)R;
+        R = (A * R + C) % M;
+        return r;
+    }
+};
+
+// gaussian_cdf_t (gaussian_distribution.h): the cumulative distribution by
+// Abramowitz & Stegun 26.2.17 and its inverse by the Odeh & Evans rational
+// approximation, with the reference's expression shapes and guards.
+static double gauss_cdf(double x, double mean, double var)
+{
+    const double p = 0.2316419;
+    const double b[] = {0.319381530, -0.356563782, 1.781477937, -1.821255978, 1.330274429};
+    double sx = (x - mean) / sqrt(var);
+    bool neg = sx < 0;
+    if (neg) sx = -sx;
+    double t = 1 / (1 + p * sx);
+    double zx = 1 / sqrt(2 * 3.14159265358) * exp(-sx * sx / 2);
+    double r = 1 - zx * ((((b[4] * t + b[3]) * t + b[2]) * t + b[1]) * t + b[0]) * t;
+    if (neg) r = 1 - r;
+    return r;
+}
+
+static double gauss_inverse(double pr, double mean, double var)
+{
+    if (pr <= 0.0 || pr >= 1.0) return mean;
+    const double ps[] = {-0.322232431088, -1.0, -0.342242088547, -0.0204231210245, -0.453642210148e-4};
+    const double qs[] = {0.0993484626060, 0.588581570495, 0.531103462366, 0.103537752850, 0.38560700634e-2};
+    double p2 = pr > 0.5 ? 1 - pr : pr;
+    if (p2 < 1e-150) p2 = 1e-150;
+    double y = sqrt(log(1 / (p2 * p2)));
+    double xp = y + ((((ps[4] * y + ps[3]) * y + ps[2]) * y + ps[1]) * y + ps[0]) /
+                        ((((qs[4] * y + qs[3]) * y + qs[2]) * y + qs[1]) * y + qs[0]);
+    if (pr < 0.5) xp = -xp;
+    return xp * sqrt(var) + mean;
+}
+
+// non_parametric_cdf_2_t (non_parametric_cdf.h:189-270): piecewise-linear in
+// float between the table's points, clamped at both ends.
+struct NpCdf
+{
+    const float *v = nullptr, *p = nullptr;
+    long long n = 0;
+    float prob(float x) const
+    {
+        const float *it = std::lower_bound(v, v + n, x);
+        if (it == v + n) return p[n - 1];
+        if (it == v) return p[0];
+        long long i2 = it - v, i1 = i2 - 1;
+        float x1 = v[i1], x2 = v[i2], y1 = p[i1], y2 = p[i2];
+        return y1 + (y2 - y1) / (x2 - x1) * (x - x1);
+    }
+    float inverse(float q) const
+    {
+        if (n <= 0) return 0;
+        const float *it = std::lower_bound(p, p + n, q);
+        if (it == p) return v[0];
+        if (it == p + n) return v[n - 1];
+        long long i2 = it - p, i1 = i2 - 1;
+        float x1 = v[i1], x2 = v[i2], y1 = p[i1], y2 = p[i2];
+        return x1 + (x2 - x1) / (y2 - y1) * (q - y1);
+    }
+};
 } // namespace ko
 
 using namespace ko;
@@ -898,6 +1009,131 @@ void ko_select_check(const unsigned *keys, int n, int k, int *same_set)
     std::sort(sa.begin(), sa.end());
     std::sort(sb.begin(), sb.end());
     *same_set = sa == sb ? 1 : 0;
+}
+
+// Sequential Gaussian simulation, do_sequential_gausian_simulation
+// (sequential_simulation.h:51-118) as sequential_gaussian_simulation(_lvm)
+// instantiates it (sequential_gaussian_simulation.cpp:18-131): the optional
+// forward CDF transform of the informed cells (and of the LVM means), then
+// every node in the path order that is not informed and whose simulation mask
+// is 1 is kriged from the first max_nb informed cells of the template (the
+// template-only lookup, sugarbox_neighbour_lookup.h:39-63) with the truncated
+// covariances, SK with mean 0 / OK / SK around the LVM means, and set to a
+// draw from N(mean, variance) (N(0, 1) on failure) by inverting one
+// std::uniform_real_distribution<double> draw of a std::mt19937 seeded with
+// `seed`; then the back transform of every informed cell. `data`/`mask` are
+// updated in place; out_status (optional) gets the kriging status of each
+// simulated node (-1 elsewhere). Returns 0, -1 on bad arguments, -4 when the
+// grid exceeds the path generator's 10,000,000-node limit.
+int ko_sgs(const int *dims, float *data, unsigned char *mask, const unsigned char *sim_mask,
+           const float *cdf_values, const float *cdf_probs, long long cdf_size, const float *means,
+           int kind, int cov_type, const double *ranges, const double *angles, double sill, double nugget,
+           const int *radiuses, int max_nb, long long seed, int *out_status)
+{
+    Grid g = {dims[0], dims[1], dims[2]};
+    const long size = g.size();
+    if (size > 10000000) return -4;
+    Flavour f;
+    if (!make_flavour(f, true, cov_type, ranges, angles, sill, nugget, radiuses)) return -1;
+    PathLcg path;
+    if (!path.init(size, seed)) return -1;
+    NpCdf cdf;
+    const bool use_cdf = cdf_values != nullptr && cdf_probs != nullptr;
+    if (use_cdf)
+    {
+        cdf.v = cdf_values;
+        cdf.p = cdf_probs;
+        cdf.n = cdf_size;
+        for (long i = 0; i < size; ++i)
+            if (mask[i]) data[i] = (float)gauss_inverse((double)cdf.prob(data[i]), 0, 1);
+    }
+    std::vector<float> mv;
+    if (means)
+    {
+        mv.assign(means, means + size);
+        if (use_cdf)
+            for (long i = 0; i < size; ++i) mv[i] = (float)gauss_inverse((double)cdf.prob(means[i]), 0, 1);
+    }
+    const std::vector<Off> tmpl = build_template(f);
+    const bool ordinary = kind == 0 && !means;
+    std::mt19937 gen;
+    gen.seed((std::mt19937::result_type)seed);
+    if (out_status)
+        for (long i = 0; i < size; ++i) out_status[i] = -1;
+    std::vector<int> idx, xs, ys, zs;
+    std::vector<double> w;
+    int node = path.next();
+    for (long counter = 0; counter < size; ++counter, node = path.next())
+    {
+        if (mask[node]) continue;
+        if (sim_mask && sim_mask[node] != 1) continue;
+        int x, y, z;
+        g.coord(node, x, y, z);
+        idx.clear();
+        for (size_t t = 0; t < tmpl.size() && (int)idx.size() < max_nb; ++t)
+        {
+            int q = g.index(x + tmpl[t].dx, y + tmpl[t].dy, z + tmpl[t].dz);
+            if (q >= 0 && mask[q]) idx.push_back(q);
+        }
+        int status = KI_NO_NEIGHBOURS;
+        float est_f = 0.0f;
+        double var = 0.0;
+        if (!idx.empty())
+        {
+            int n = (int)idx.size();
+            xs.resize(n);
+            ys.resize(n);
+            zs.resize(n);
+            for (int i = 0; i < n; ++i) g.coord(idx[i], xs[i], ys[i], zs[i]);
+            if (weights<double>(f, ordinary, x, y, z, xs, ys, zs, w, var))
+            {
+                status = KI_SUCCESS;
+                // combine (combiner.h:10-25): float accumulation around the means
+                float m = means ? mv[node] : 0.0f;
+                est_f = m;
+                for (int i = 0; i < n; ++i)
+                {
+                    float d = data[idx[i]] - (means ? mv[idx[i]] : m);
+                    est_f += (float)(w[i] * d);
+                }
+            }
+            else
+                status = KI_SINGULARITY;
+        }
+        std::uniform_real_distribution<double> dist(0.0, 1.0);
+        double u = dist(gen);
+        double value = status == KI_SUCCESS ? gauss_inverse(u, (double)est_f, var) : gauss_inverse(u, 0, 1);
+        data[node] = (float)value;
+        mask[node] = 1;
+        if (out_status) out_status[node] = status;
+    }
+    if (use_cdf)
+        for (long i = 0; i < size; ++i)
+            if (mask[i]) data[i] = cdf.inverse((float)gauss_cdf((double)data[i], 0, 1));
+    return 0;
+}
+
+// n draws of std::uniform_real_distribution<double>(0, 1) on std::mt19937
+// seeded as mt_random_generator_t::seed does (bs_random_generator.cpp:9-25).
+int ko_mt_draws(long long seed, long long n, double *out)
+{
+    std::mt19937 gen;
+    gen.seed(static_cast<std::mt19937::result_type>((long)seed));
+    for (long long i = 0; i < n; ++i)
+    {
+        std::uniform_real_distribution<double> dist(0.0, 1.0);
+        out[i] = dist(gen);
+    }
+    return 0;
+}
+
+// The first `count` nodes of the SGS path for a grid of `size` nodes.
+int ko_sgs_path(long long size, long long seed, int *out, long long count)
+{
+    PathLcg path;
+    if (!path.init(size, seed)) return -1;
+    for (long long i = 0; i < count; ++i) out[i] = path.next();
+    return 0;
 }
 
 } // extern "C"

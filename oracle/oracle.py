@@ -66,6 +66,10 @@ def load(which: str):
                                           _u8, _u8, _f, C.c_int]
         lib.ko_median_ik_grid.argtypes = [_i, _u8, _u8, C.c_int, _d, _d, C.c_double, C.c_double,
                                           _i, C.c_int, _d, _u8, _u8, _d, _i, C.c_int]
+        lib.ko_sgs.argtypes = [_i, _f, _u8, _u8, _f, _f, C.c_longlong, _f, C.c_int, C.c_int, _d, _d, C.c_double,
+                               C.c_double, _i, C.c_int, C.c_longlong, _i]
+        lib.ko_sgs_path.argtypes = [C.c_longlong, C.c_longlong, _i, C.c_longlong]
+        lib.ko_mt_draws.argtypes = [C.c_longlong, C.c_longlong, _d]
         lib.ko_template.argtypes = [C.c_int, C.c_int, _d, _d, C.c_double, C.c_double, _i, _i,
                                     C.c_int, _i]
         lib.ko_cov.argtypes = [C.c_int, C.c_int, _d, _d, C.c_double, C.c_double, _i, _i, _i]
@@ -260,6 +264,46 @@ def lvm_grid(dims, data, mask, means, cov, radiuses, k, threads=0):
     if rc:
         raise RuntimeError("lvm_grid failed")
     return out_d, out_m, est, var, st
+
+
+def sgs(dims, data, mask, cov, radiuses, k, seed, kind=1, sim_mask=None, cdf=None, means=None):
+    """Sequential Gaussian simulation (port). `cov` carries the sill and nugget
+    the C++ driver receives (geo_bsd's sgs_simulation normalises them by the
+    sill first); `cdf` is (values, probs) or None; `means` makes it LVM SGS.
+    Returns (data, mask, status) with the status of each simulated node."""
+    lib = load("port")
+    data = _arr(data, np.float32).copy()
+    mask = _arr(mask, np.uint8).copy()
+    st = np.zeros(len(data), np.int32)
+    sm = _arr(sim_mask, np.uint8) if sim_mask is not None else None
+    cv = _arr(cdf[0], np.float32) if cdf is not None else None
+    cp = _arr(cdf[1], np.float32) if cdf is not None else None
+    mv = _arr(means, np.float32) if means is not None else None
+    rc = lib.ko_sgs(_ptr(_arr(dims, np.int32), _i), _ptr(data, _f), _ptr(mask, _u8), _ptr(sm, _u8), _ptr(cv, _f),
+                    _ptr(cp, _f), 0 if cv is None else len(cv), _ptr(mv, _f), int(kind), int(cov.cov_type),
+                    _ptr(_arr(cov.ranges, np.float64), _d), _ptr(_arr(cov.angles, np.float64), _d),
+                    float(cov.sill), float(cov.nugget), _ptr(_arr(radiuses, np.int32), _i), int(k), int(seed),
+                    _ptr(st, _i))
+    if rc:
+        raise RuntimeError(f"sgs failed (rc={rc})")
+    return data, mask, st
+
+
+def mt_draws(seed, n):
+    """std::mt19937 + uniform_real_distribution<double>(0, 1) draws (the standard library)."""
+    lib = load("port")
+    out = np.zeros(n, np.float64)
+    lib.ko_mt_draws(int(seed), int(n), _ptr(out, _d))
+    return out
+
+
+def sgs_path(size, seed, count=None):
+    lib = load("port")
+    count = size if count is None else count
+    out = np.zeros(count, np.int32)
+    if lib.ko_sgs_path(int(size), int(seed), _ptr(out, _i), int(count)):
+        raise RuntimeError("sgs_path failed")
+    return out
 
 
 def indicator_grid(dims, data, mask, covs, radiuses, ks, marginals, threads=0):

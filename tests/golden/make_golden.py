@@ -6,6 +6,7 @@ harness libref_harness.so around its own templates):
 
     make -C oracle && python tests/golden/make_golden.py        (all fixtures)
                       python tests/golden/make_golden.py lvm    (lvm.npz only)
+                      python tests/golden/make_golden.py sgs    (sgs.npz only)
 
 Inputs are the seeded workloads of geo_bsd.workloads at reduced scale (the
 conditioning cells are stored in each file, so the fixtures do not depend on
@@ -14,7 +15,8 @@ its own order, the search path taken, the FP64 estimate and variance of
 kriging_interpolation with result_t = double, the float estimate the drivers
 store, and the status code. Whole-grid outputs of the reference's public C API
 (hpgl_ordinary_kriging, hpgl_simple_kriging, hpgl_lvm_kriging,
-hpgl_indicator_kriging, hpgl_median_ik) are stored for the small grids, plus the known-answer cases
+hpgl_indicator_kriging, hpgl_median_ik, hpgl_sgs_simulation,
+hpgl_sgs_lvm_simulation) are stored for the small grids, plus the known-answer cases
 of the reference's test suite (constant field 42, all zeros).
 """
 import ctypes as C
@@ -29,6 +31,8 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, os.path.join(ROOT, "hpgl-reborn_b200"))
 
 import oracle as O  # noqa: E402
+sys.path.insert(0, os.path.dirname(HERE))
+from golden_io import SGS_CASES, sgs_inputs  # noqa: E402
 from geo_bsd import workloads as WL  # noqa: E402  (pure python module)
 
 SAMPLE = 1200
@@ -111,6 +115,56 @@ def api_lvm(lib, dims, data, mask, means, cov, rad, k):
     sh = _shape(dims)
     lib.hpgl_lvm_kriging(data.ctypes.data_as(fp), mask.ctypes.data_as(up), C.byref(sh), means.ctypes.data_as(fp),
                          C.byref(sh), C.byref(p), od.ctypes.data_as(fp), om.ctypes.data_as(up), C.byref(sh))
+    return od, om
+
+
+class SgsP(C.Structure):
+    _fields_ = [("t", C.c_int), ("r", C.c_double * 3), ("a", C.c_double * 3), ("sill", C.c_double),
+                ("nugget", C.c_double), ("rad", C.c_int * 3), ("k", C.c_int), ("kind", C.c_int), ("seed", C.c_long),
+                ("kmin", C.c_int)]
+
+
+class NpCdf(C.Structure):
+    _fields_ = [("values", C.POINTER(C.c_float)), ("probs", C.POINTER(C.c_float)), ("size", C.c_longlong)]
+
+
+class FloatArr(C.Structure):
+    _fields_ = [("data", C.POINTER(C.c_float)), ("shape", Shape)]
+
+
+class UbyteArr(C.Structure):
+    _fields_ = [("data", C.POINTER(C.c_ubyte)), ("shape", Shape)]
+
+
+def api_sgs(lib, dims, data, mask, cov, rad, k, seed, kind=1, sim_mask=None, cdf=None, means=None):
+    """The reference's hpgl_sgs_simulation / hpgl_sgs_lvm_simulation; `cov` holds the
+    sill and nugget as the driver receives them. Returns the output data and mask."""
+    od = np.ascontiguousarray(data, np.float32).copy()
+    om = np.ascontiguousarray(mask, np.uint8).copy()
+    fp = C.POINTER(C.c_float)
+    up = C.POINTER(C.c_ubyte)
+    a = Cont(od.ctypes.data_as(fp), om.ctypes.data_as(up), _shape(dims))
+    p = SgsP(cov.cov_type, (C.c_double * 3)(*cov.ranges), (C.c_double * 3)(*cov.angles), cov.sill, cov.nugget,
+             (C.c_int * 3)(*rad), k, kind, seed, 0)
+    keep = []
+    c = None
+    if cdf is not None:
+        cv = np.ascontiguousarray(cdf[0], np.float32)
+        cp = np.ascontiguousarray(cdf[1], np.float32)
+        keep += [cv, cp]
+        c = C.byref(NpCdf(cv.ctypes.data_as(fp), cp.ctypes.data_as(fp), len(cv)))
+    sm = None
+    if sim_mask is not None:
+        smv = np.ascontiguousarray(sim_mask, np.uint8)
+        keep.append(smv)
+        sm = C.byref(UbyteArr(smv.ctypes.data_as(up), _shape(dims)))
+    if means is None:
+        lib.hpgl_sgs_simulation(C.byref(a), C.byref(p), c, None, sm)
+    else:
+        mv = np.ascontiguousarray(means, np.float32)
+        keep.append(mv)
+        lib.hpgl_sgs_lvm_simulation(C.byref(a), C.byref(p), c, C.byref(FloatArr(mv.ctypes.data_as(fp), _shape(dims))),
+                                    sm)
     return od, om
 
 
@@ -197,12 +251,30 @@ def lvm_cases(lib):
     print("wrote lvm")
 
 
+def sgs_cases(lib):
+    """The reference's hpgl_sgs_simulation / hpgl_sgs_lvm_simulation outputs."""
+    out = {}
+    for name, base, kind, seed, opts in SGS_CASES:
+        g = dict(np.load(os.path.join(HERE, base + ".npz")))
+        x = sgs_inputs(g, opts)
+        od, om = api_sgs(lib, x["dims"], x["data"], x["mask"], x["cov"], x["rad"], x["k"], seed, kind=kind,
+                         sim_mask=x["sim_mask"], cdf=x["cdf"], means=x["means"])
+        out[f"{name}_data"] = od
+        out[f"{name}_mask"] = om
+    np.savez_compressed(os.path.join(HERE, "sgs.npz"), **out)
+    print("wrote sgs")
+
+
 def main(only=None):
     lib = _api()
     if only == "lvm":
         lvm_cases(lib)
         return
+    if only == "sgs":
+        sgs_cases(lib)
+        return
     lvm_cases(lib)
+    sgs_cases(lib)
     cont_case(lib, WL.ok_small(0.3), "ok_small_s030", grid_api=True)
     cont_case(lib, WL.sk_ok_large(0.16), "sk_ok_large_s016")
     cont_case(lib, WL.gauss_cv(0.2), "gauss_cv_s020", grid_api=True)

@@ -34,3 +34,47 @@ def as_workload(g, name="golden", values_key="values", dtype=np.float32, prefix=
     dims, data, mask = grid_inputs(g, values_key, dtype, undefined=-99.0 if dtype == np.float32 else 0)
     cov, rad, k = cov_of(g, prefix)
     return WL.Workload(name, dims, data, mask, cov, rad, k)
+
+
+def empirical_cdf(values):
+    """calc_cdf (cdf.py:8-40) of a set of values: distinct values without the
+    largest, with the running sum of their frequencies."""
+    v, c = np.unique(np.asarray(values, np.float32), return_counts=True)
+    size = v.size - 1 if v.size > 1 else v.size
+    return v[:size].astype(np.float32), np.cumsum(c[:size] / float(len(values))).astype(np.float32)
+
+
+SGS_CASES = [
+    # name, base fixture, kind, seed, options
+    ("sk_plain", "gauss_cv_s020", 1, 1234, {}),
+    ("ok_cdf", "gauss_cv_s020", 0, 7, {"cdf": True}),
+    ("sk_mask", "gauss_cv_s020", 1, 99, {"sim_mask": 0.7}),
+    ("lvm_cdf", "gauss_cv_s020", 1, 5, {"lvm": 0.5, "cdf": True}),
+    ("sk_nohard", "ok_small_s030", 1, 3, {"nohard": True}),
+    ("ok_plain", "ok_small_s030", 0, 11, {}),
+]
+
+
+def sgs_inputs(g, opts):
+    """Inputs of an SGS golden case from its base fixture: data, mask, sim mask,
+    cdf, means (the sill/nugget normalisation of sgs.py:108 applied to cov)."""
+    dims = tuple(int(v) for v in g["dims"])
+    n = dims[0] * dims[1] * dims[2]
+    data = np.full(n, -99.0, np.float32)
+    mask = np.zeros(n, np.uint8)
+    data[g["informed"]] = g["values"]
+    mask[g["informed"]] = 1
+    cov = WL.CovSpec(int(g["cov_type"]), tuple(float(v) for v in g["ranges"]), tuple(float(v) for v in g["angles"]),
+                     1.0, float(g["nugget"]) / float(g["sill"]))
+    out = {"dims": dims, "data": data, "mask": mask, "cov": cov, "rad": tuple(int(v) for v in g["radiuses"]),
+           "k": int(g["k"]), "sim_mask": None, "cdf": None, "means": None}
+    if "sim_mask" in opts:
+        out["sim_mask"] = (np.random.default_rng(3).random(n) < opts["sim_mask"]).astype(np.uint8)
+    if opts.get("cdf"):
+        out["cdf"] = empirical_cdf(g["values"])
+    if "lvm" in opts:
+        out["means"] = (WL.lvm_means(dims) * np.float32(opts["lvm"])).astype(np.float32)
+    if opts.get("nohard"):
+        out["data"] = np.zeros(n, np.float32)
+        out["mask"] = np.zeros(n, np.uint8)
+    return out

@@ -71,6 +71,33 @@ def test_oracle_lvm_matches_reference_per_node(case):
     assert np.abs(r["est_f"][ok] - lv[f"{case}_est_f"][ok]).max() <= 4e-7 * max(np.abs(ref).max(), 1.0)
 
 
+@pytest.mark.parametrize("case", [c[0] for c in G.SGS_CASES])
+def test_oracle_sgs_matches_reference(case):
+    """SGS: the restatement reproduces the reference's hpgl_sgs_simulation output bit for bit."""
+    _, base, kind, seed, opts = next(c for c in G.SGS_CASES if c[0] == case)
+    x = G.sgs_inputs(G.load(base), opts)
+    ref = G.load("sgs")
+    d, m, _ = O.sgs(x["dims"], x["data"], x["mask"], x["cov"], x["rad"], x["k"], seed, kind=kind,
+                    sim_mask=x["sim_mask"], cdf=x["cdf"], means=x["means"])
+    np.testing.assert_array_equal(m, ref[f"{case}_mask"])
+    np.testing.assert_array_equal(d.view(np.uint32), ref[f"{case}_data"].view(np.uint32))
+
+
+@pytest.mark.parametrize("size", [1, 2, 4, 6, 7, 8, 9, 12, 30, 64, 1000, 4096, 12345, 65536])
+def test_sgs_walk_visits_every_node_once(size):
+    """The simulation path (path_random_generator.cpp) is a permutation exactly when
+    its increment (the largest prime <= size/3 not dividing size, else 2) is
+    coprime to the size: every size but a few small ones (2, 4, 6, 8, 12)."""
+    def isprime(q):
+        return q > 1 and all(q % d for d in range(2, int(q ** 0.5) + 1))
+    inc = next((q for q in range(size // 3, 2, -1) if isprime(q) and size % q), 2)
+    for seed in (0, 5, 123456789):
+        p = O.sgs_path(size, seed)
+        assert p[0] == seed % size
+        assert (len(np.unique(p)) == size) == (size % inc != 0 or size == 1)
+    assert (size % inc != 0 or size == 1) == (size not in (2, 4, 6, 8, 12))
+
+
 def test_oracle_indicator_matches_reference():
     g = G.load("indicator_s015")
     dims, data, mask = G.grid_inputs(g, dtype=np.uint8)
