@@ -119,6 +119,24 @@ hb::IkArgs ik_args_from(const hpgl_ik_params_t *p)
     return a;
 }
 
+hb::SgsArgs sgs_args_from(const hpgl_sgs_params_t *p)
+{
+    hb::SgsArgs a{};
+    a.cov_type = p->m_covariance_type;
+    for (int i = 0; i < 3; ++i)
+    {
+        a.ranges[i] = p->m_ranges[i];
+        a.angles[i] = p->m_angles[i];
+        a.radiuses[i] = p->m_radiuses[i];
+    }
+    a.sill = p->m_sill;
+    a.nugget = p->m_nugget;
+    a.max_nb = p->m_max_neighbours;
+    a.kind = p->m_kriging_kind;
+    a.seed = p->m_seed;
+    return a;
+}
+
 hb::Options options_from(const hpgl_b200_options_t *o)
 {
     hb::Options r;
@@ -231,6 +249,46 @@ void hpgl_lvm_kriging(float *input_data, unsigned char *input_mask, hpgl_shape_t
         report_done("LVM Kriging");
 }
 
+void hpgl_sgs_simulation(hpgl_cont_masked_array_t *data, hpgl_sgs_params_t *params, hpgl_non_parametric_cdf_t *cdf,
+                         double *mean, hpgl_ubyte_array_t *simulation_mask)
+{
+    (void)mean; // sequential_gaussian_simulation.cpp:39-41: SK runs around 0 whatever the mean
+    if (!data || !params)
+    {
+        hb::set_error("hpgl_sgs_simulation: null argument");
+        return;
+    }
+    int dims[3];
+    if (!shape_dims(&data->m_shape, dims)) return;
+    hb::CdfTable t;
+    if (cdf) t = {cdf->m_values, cdf->m_probs, cdf->m_size};
+    hb::Options opt;
+    progress("Sequential Gaussian Simulation", 0);
+    if (hb::sgs_simulation(dims, data->m_data, data->m_mask, simulation_mask ? simulation_mask->m_data : nullptr,
+                           cdf ? &t : nullptr, nullptr, sgs_args_from(params), opt) == 0)
+        report_done("Sequential Gaussian Simulation");
+}
+
+void hpgl_sgs_lvm_simulation(hpgl_cont_masked_array_t *data, hpgl_sgs_params_t *params,
+                             hpgl_non_parametric_cdf_t *cdf, hpgl_float_array_t *means,
+                             hpgl_ubyte_array_t *simulation_mask)
+{
+    if (!data || !params || !means || !means->m_data)
+    {
+        hb::set_error("hpgl_sgs_lvm_simulation: null argument");
+        return;
+    }
+    int dims[3];
+    if (!shape_dims(&data->m_shape, dims)) return;
+    hb::CdfTable t;
+    if (cdf) t = {cdf->m_values, cdf->m_probs, cdf->m_size};
+    hb::Options opt;
+    progress("Sequential Gaussian Simulation with Local Varying Mean", 0);
+    if (hb::sgs_simulation(dims, data->m_data, data->m_mask, simulation_mask ? simulation_mask->m_data : nullptr,
+                           cdf ? &t : nullptr, means->m_data, sgs_args_from(params), opt) == 0)
+        report_done("Sequential Gaussian Simulation with Local Varying Mean");
+}
+
 int hpgl_simple_kriging_weights(float *center_coords, float *neighbours_x, float *neighbours_y,
                                 float *neighbours_z, int neighbours_count, hpgl_cov_params_t *params,
                                 float *weights)
@@ -334,6 +392,32 @@ int hpgl_b200_lvm_kriging_ex(const int *dims, const float *in_data, const unsign
                             mean_data);
 }
 
+int hpgl_b200_sgs_draws(long long seed, long long n, double *out)
+{
+    if (n < 0 || (n > 0 && !out))
+    {
+        hb::set_error("hpgl_b200_sgs_draws: bad argument");
+        return HPGL_B200_EINVAL;
+    }
+    hb::sgs_draws((unsigned long long)seed, n, out);
+    return HPGL_B200_OK;
+}
+
+int hpgl_b200_sgs_ex(const int *dims, float *data, unsigned char *mask, const unsigned char *sim_mask,
+                     const hpgl_non_parametric_cdf_t *cdf, const float *means, const hpgl_sgs_params_t *params,
+                     const hpgl_b200_options_t *opt)
+{
+    if (!params)
+    {
+        hb::set_error("hpgl_b200_sgs_ex: bad argument");
+        return HPGL_B200_EINVAL;
+    }
+    hb::CdfTable t;
+    if (cdf) t = {cdf->m_values, cdf->m_probs, cdf->m_size};
+    return hb::sgs_simulation(dims, data, mask, sim_mask, cdf ? &t : nullptr, means, sgs_args_from(params),
+                              options_from(opt));
+}
+
 int hpgl_b200_indicator_kriging_ex(const int *dims, const unsigned char *in_data, const unsigned char *in_mask,
                                    const hpgl_ik_params_t *params, int indicator_count, unsigned char *out_data,
                                    unsigned char *out_mask, const hpgl_b200_options_t *opt)
@@ -400,6 +484,8 @@ int hpgl_b200_last_stats(double *out, int cap)
     v[36] = (double)s.exact_cells;
     v[37] = s.prefilter ? 1.0 : 0.0;
     v[38] = s.plan_ms;
+    v[39] = (double)s.sgs_levels;
+    v[40] = s.draws_ms;
     int n = cap < HPGL_B200_STATS_LEN ? cap : HPGL_B200_STATS_LEN;
     for (int i = 0; i < n; ++i) out[i] = v[i];
     return n;

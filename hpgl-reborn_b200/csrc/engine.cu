@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <exception>
@@ -141,6 +142,20 @@ class Engine
         }
         return stage_;
     }
+    // A second page-locked area (the SGS draws), same rules as staging().
+    unsigned char *staging2(size_t bytes)
+    {
+        if (stage2_cap_ < bytes)
+        {
+            if (stage2_) cudaFreeHost(stage2_);
+            stage2_ = nullptr;
+            stage2_cap_ = 0;
+            const size_t want = bytes + bytes / 4;
+            HB_CK(cudaHostAlloc(reinterpret_cast<void **>(&stage2_), want, cudaHostAllocDefault));
+            stage2_cap_ = want;
+        }
+        return stage2_;
+    }
     int n_sm() const { return n_sm_; }
     int max_smem() const { return max_smem_; }
     cudaStream_t stream(const void *user) const { return user ? (cudaStream_t)user : own_stream_; }
@@ -153,6 +168,8 @@ class Engine
     cudaEvent_t stage_start_;
     int mark_id_[64];
     int n_marks_ = 0;
+    unsigned char *stage2_ = nullptr;
+    size_t stage2_cap_ = 0;
     int device_;
     cudaStream_t own_stream_ = nullptr;
     int n_sm_ = 148;
@@ -926,6 +943,278 @@ int median_ik(const int *dims, const unsigned char *in_data, const unsigned char
         E.stats.solve_ms = a2;
         E.stats.ties = S.ties;
         E.stats.template_cells = S.template_cells;
+        return 0;
+    }
+    catch (const CudaFail &f)
+    {
+        set_error(f.msg);
+        return f.code;
+    }
+    catch (const std::exception &ex)
+    {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+// ------------------------------------------------------------------ SGS
+// The walk of path_random_generator.cpp:24-67: R <- (A R + C) mod size from
+// seed % size, A = 1 + the product of the primes dividing size (doubled when 4
+// divides size), C = the largest prime not above size / 3 that does not divide
+// size, 2 when there is none. Returns false when the walk is not a permutation
+// (C = 2 dividing size: grids of a few cells).
+static bool is_prime_ll(long long p)
+{
+    if (p < 2) return false;
+    for (long long d = 2; d * d <= p; ++d)
+        if (p % d == 0) return false;
+    return true;
+}
+
+static bool sgs_walk(long long size, long long seed, SgsWalk &w)
+{
+    long long A = 1, m = size;
+    for (long long p = 2; p * p <= m; ++p)
+        if (m % p == 0)
+        {
+            A *= p;
+            while (m % p == 0) m /= p;
+        }
+    if (m > 1) A *= m;
+    if (size % 4 == 0) A *= 2;
+    A += 1;
+    long long C = 2;
+    for (long long p = size / 3; p >= 3; --p)
+        if (size % p != 0 && is_prime_ll(p))
+        {
+            C = p;
+            break;
+        }
+    w.A = A;
+    w.C = C;
+    w.M = size;
+    w.R0 = seed % size;
+    return size % C != 0;
+}
+
+int sgs_simulation(const int *dims, float *data, unsigned char *mask, const unsigned char *sim_mask,
+                   const CdfTable *cdf, const float *means, const SgsArgs &a, const Options &opt)
+{
+    std::lock_guard<std::mutex> lk(g_engine_mu);
+    try
+    {
+        if (!dims || !data || !mask) throw CudaFail{-1, "null array argument"};
+        const long long n = check_dims(dims);
+        if (n > 10000000) throw CudaFail{-4, "the simulation path supports at most 10,000,000 cells"};
+        check_model_args(a.cov_type, a.ranges, a.angles, a.sill, a.nugget, a.radiuses, a.max_nb);
+        if (a.max_nb > kSgsBlockMax)
+            throw CudaFail{-4, "simulation supports max_neighbours up to " + std::to_string(kSgsBlockMax)};
+        SgsWalk walk;
+        const bool full_period = sgs_walk(n, a.seed, walk);
+        if (walk.R0 < 0) throw CudaFail{-1, "seed % grid size must not be negative"};
+        const bool use_cdf = cdf && cdf->values && cdf->probs && cdf->size > 0;
+        const bool lvm = means != nullptr;
+        const bool ordinary = !lvm && a.kind == 0;
+        double plan_ms = 0.0;
+        auto plan_f = std::async(std::launch::async, [&]() {
+            const auto t0 = std::chrono::steady_clock::now();
+            Plan p = make_plan(true, a.cov_type, a.ranges, a.angles, a.sill, a.nugget, a.radiuses, a.max_nb, dims);
+            std::vector<Offset> tv = build_template(p.f, p.kt);
+            plan_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            return std::make_pair(std::move(p), std::move(tv));
+        });
+        Engine &E = engine_for_current_device();
+        cudaStream_t st = E.stream(opt.stream);
+        IoPlan io{(opt.flags & 1u) != 0, st};
+        begin_call(E, st);
+
+        // in/out property: data and mask are simulated in place
+        float *d_data = io.device ? data : E.buf<float>("sgs_data", (size_t)n);
+        uint8_t *d_mask = io.device ? mask : E.buf<uint8_t>("sgs_mask", (size_t)n);
+        if (!io.device)
+        {
+            HB_CK(cudaMemcpyAsync(d_data, data, n * 4, cudaMemcpyHostToDevice, st));
+            HB_CK(cudaMemcpyAsync(d_mask, mask, n, cudaMemcpyHostToDevice, st));
+            E.stats.h2d += n * 5;
+        }
+        const uint8_t *d_sim = sim_mask ? to_device(E, "sgs_sim_mask", sim_mask, (size_t)n, io) : nullptr;
+        const float *d_means_in = lvm ? to_device(E, "sgs_means_in", means, (size_t)n, io) : nullptr;
+        float *d_means = lvm ? E.buf<float>("sgs_means", (size_t)n) : nullptr;
+        float *d_cv = nullptr, *d_cp = nullptr;
+        if (use_cdf)
+        {
+            d_cv = E.buf<float>("sgs_cdf_v", (size_t)cdf->size);
+            d_cp = E.buf<float>("sgs_cdf_p", (size_t)cdf->size);
+            HB_CK(cudaMemcpyAsync(d_cv, cdf->values, cdf->size * 4, cudaMemcpyHostToDevice, st));
+            HB_CK(cudaMemcpyAsync(d_cp, cdf->probs, cdf->size * 4, cudaMemcpyHostToDevice, st));
+            HB_CK(cudaStreamSynchronize(st)); // the tables are caller memory, possibly pageable
+        }
+        E.mark(STAGE_UPLOAD, st);
+
+        // the walk -> ranks of the simulated nodes
+        int *rank_of = E.buf<int>("sgs_rank_of", (size_t)n);
+        int *sim_cells = E.buf<int>("sgs_sim_cells", (size_t)n);
+        int n_sim = 0;
+        if (full_period)
+        {
+            int *path_cell = E.buf<int>("sgs_path", (size_t)n);
+            int *flag = E.buf<int>("sgs_flag", (size_t)n);
+            int *tmp = E.buf<int>("scan_tmp", (size_t)scan_tmp_ints(n) + 4);
+            int *total = E.buf<int>("sgs_total", 1);
+            launch_sgs_path(walk, d_mask, d_sim, path_cell, flag, st);
+            int *scan = E.buf<int>("sgs_scan", (size_t)n);
+            HB_CK(cudaMemcpyAsync(scan, flag, n * 4, cudaMemcpyDeviceToDevice, st));
+            exclusive_scan(scan, n, tmp, total, st);
+            launch_sgs_index(n, path_cell, flag, scan, d_mask, rank_of, sim_cells, st);
+            HB_CK(cudaGetLastError());
+            HB_CK(cudaMemcpyAsync(&n_sim, total, sizeof(int), cudaMemcpyDeviceToHost, st));
+            HB_CK(cudaStreamSynchronize(st));
+        }
+        else
+        {
+            // a walk that revisits nodes (grids of a few cells): the first visit of
+            // an uninformed node with simulation mask 1 simulates it
+            std::vector<uint8_t> hm(n), hs(sim_mask ? n : 0), seen(n, 0);
+            std::vector<int> hr(n), hc;
+            HB_CK(cudaMemcpyAsync(hm.data(), d_mask, n, cudaMemcpyDeviceToHost, st));
+            if (d_sim) HB_CK(cudaMemcpyAsync(hs.data(), d_sim, n, cudaMemcpyDeviceToHost, st));
+            HB_CK(cudaStreamSynchronize(st));
+            for (long long i = 0; i < n; ++i) hr[i] = hm[i] ? -1 : INT_MAX;
+            long long R = walk.R0;
+            for (long long p = 0; p < n; ++p)
+            {
+                const int c = (int)R;
+                if (!hm[c] && !seen[c] && (!d_sim || hs[c] == 1))
+                {
+                    seen[c] = 1;
+                    hr[c] = (int)hc.size();
+                    hc.push_back(c);
+                }
+                R = (walk.A * R + walk.C) % walk.M;
+            }
+            n_sim = (int)hc.size();
+            HB_CK(cudaMemcpyAsync(rank_of, hr.data(), n * 4, cudaMemcpyHostToDevice, st));
+            if (n_sim) HB_CK(cudaMemcpyAsync(sim_cells, hc.data(), (size_t)n_sim * 4, cudaMemcpyHostToDevice, st));
+            HB_CK(cudaStreamSynchronize(st));
+        }
+        E.mark(STAGE_COMPACT, st);
+
+        // the draws: one uniform per simulated node in walk order, generated on
+        // the host while the device searches and levels
+        double *h_u = reinterpret_cast<double *>(E.staging2((size_t)std::max(n_sim, 1) * 8));
+        double draws_ms = 0.0;
+        auto draws_f = std::async(std::launch::async, [&, n_sim]() {
+            const auto t0 = std::chrono::steady_clock::now();
+            sgs_draws((unsigned long long)a.seed, n_sim, h_u);
+            draws_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        });
+
+        auto plan_pair = plan_f.get();
+        const Plan &pl = plan_pair.first;
+        const std::vector<Offset> &tv = plan_pair.second;
+        E.stats.plan_ms = plan_ms;
+        const Geom &g = pl.g;
+        const size_t nk = pl.kt.vals.size();
+        double *search_vals = E.buf<double>("search_vals", nk);
+        HB_CK(cudaMemcpyAsync(search_vals, pl.kt.vals.data(), nk * 8, cudaMemcpyHostToDevice, st));
+        const long long pn = (long long)g.pnx * g.pny * (2 * g.phz + 1);
+        double *pair64 = E.buf<double>("pair64", (size_t)pn);
+        float *pair32 = E.buf<float>("pair32", (size_t)pn);
+        launch_build_pair(g, dev_model(pl.f.m), 1, search_vals, pair64, pair32, st);
+        std::vector<int4> t4(tv.size());
+        for (size_t i = 0; i < tv.size(); ++i) t4[i] = make_int4(tv[i].dx, tv[i].dy, tv[i].dz, 0);
+        int4 *tmpl = E.buf<int4>("sgs_tmpl", std::max<size_t>(t4.size(), 1));
+        if (!t4.empty())
+            HB_CK(cudaMemcpyAsync(tmpl, t4.data(), t4.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+        if (use_cdf || lvm)
+            launch_sgs_forward(n, d_data, d_mask, d_means_in, d_means, use_cdf ? d_cv : nullptr, d_cp,
+                               use_cdf ? cdf->size : 0, st);
+        HB_CK(cudaGetLastError());
+        HB_CK(cudaStreamSynchronize(st)); // t4 and the key values are host temporaries
+        E.mark(STAGE_TABLES, st);
+
+        // neighbours of every simulated node
+        const int k = a.max_nb;
+        int *nb = E.buf<int>("sgs_nb", (size_t)std::max(n_sim, 1) * k);
+        int *nb_rank = E.buf<int>("sgs_nb_rank", (size_t)std::max(n_sim, 1) * k);
+        int *nb_cnt = E.buf<int>("sgs_nb_cnt", (size_t)std::max(n_sim, 1));
+        if (n_sim > 0)
+            launch_sgs_search(g, tmpl, (int)t4.size(), sim_cells, n_sim, rank_of, k, nb, nb_rank, nb_cnt, E.n_sm(),
+                              st);
+        HB_CK(cudaGetLastError());
+        E.mark(STAGE_SEARCH, st);
+
+        // dependency levels
+        const int level_cap = 1 << 20;
+        int *levp1 = E.buf<int>("sgs_levp1", (size_t)std::max(n_sim, 1));
+        int *lvl_count = E.buf<int>("sgs_lvl_count", (size_t)level_cap + 1);
+        int *scal = E.buf<int>("sgs_scal", 4); // ticket, max level, error
+        HB_CK(cudaMemsetAsync(levp1, 0, (size_t)std::max(n_sim, 1) * 4, st));
+        HB_CK(cudaMemsetAsync(lvl_count, 0, ((size_t)level_cap + 1) * 4, st));
+        HB_CK(cudaMemsetAsync(scal, 0, 16, st));
+        if (n_sim > 0)
+            launch_sgs_levels(nb_rank, nb_cnt, k, n_sim, levp1, scal + 0, lvl_count, level_cap, scal + 1, scal + 2,
+                              E.n_sm(), st);
+        HB_CK(cudaGetLastError());
+        int hs[4] = {0, 0, 0, 0};
+        HB_CK(cudaMemcpyAsync(hs, scal, 16, cudaMemcpyDeviceToHost, st));
+        HB_CK(cudaStreamSynchronize(st));
+        if (hs[2] == 1) throw CudaFail{-2, "simulation level pass: a dependency wait timed out"};
+        if (hs[2] == 2) throw CudaFail{-4, "simulation needs more than 2^20 dependency levels"};
+        const int n_levels = n_sim > 0 ? hs[1] + 1 : 0;
+        std::vector<int> counts(std::max(n_levels, 1)), offs(std::max(n_levels, 1) + 1, 0);
+        if (n_levels > 0)
+        {
+            HB_CK(cudaMemcpyAsync(counts.data(), lvl_count, (size_t)n_levels * 4, cudaMemcpyDeviceToHost, st));
+            HB_CK(cudaStreamSynchronize(st));
+        }
+        for (int l = 0; l < n_levels; ++l) offs[l + 1] = offs[l] + counts[l];
+        int *order = E.buf<int>("sgs_order", (size_t)std::max(n_sim, 1));
+        int *level_off = E.buf<int>("sgs_level_off", (size_t)n_levels + 1);
+        int *level_fill = E.buf<int>("sgs_level_fill", (size_t)n_levels + 1);
+        if (n_levels > 0)
+        {
+            HB_CK(cudaMemcpyAsync(level_off, offs.data(), ((size_t)n_levels + 1) * 4, cudaMemcpyHostToDevice, st));
+            HB_CK(cudaMemsetAsync(level_fill, 0, ((size_t)n_levels + 1) * 4, st));
+            launch_sgs_level_fill(n_sim, levp1, level_off, level_fill, order, st);
+            HB_CK(cudaGetLastError());
+        }
+        E.stats.sgs_levels = n_levels;
+        E.mark(STAGE_TIES, st);
+
+        // draws in, then one solve launch per level
+        draws_f.get();
+        E.stats.draws_ms = draws_ms;
+        double *d_u = E.buf<double>("sgs_uniforms", (size_t)std::max(n_sim, 1));
+        if (n_sim > 0)
+        {
+            HB_CK(cudaMemcpyAsync(d_u, h_u, (size_t)n_sim * 8, cudaMemcpyHostToDevice, st));
+            E.stats.h2d += (long long)n_sim * 8;
+        }
+        E.mark(STAGE_PREPARE, st);
+        signed char *st_rank = E.buf<signed char>("sgs_st_rank", (size_t)std::max(n_sim, 1));
+        for (int l = 0; l < n_levels; ++l)
+        {
+            HB_CK(launch_sgs_solve(g, order + offs[l], counts[l], sim_cells, nb, nb_cnt, k, pair64, d_data, d_means,
+                                   d_u, st_rank, ordinary, E.n_sm(), st));
+            E.stats.launches += 1;
+        }
+        E.mark(STAGE_SOLVE, st);
+        signed char *d_status =
+            opt.status ? (io.device ? opt.status : E.buf<signed char>("status", (size_t)n)) : nullptr;
+        launch_sgs_finalize(n, d_data, d_mask, rank_of, n_sim, st_rank, d_status, use_cdf ? d_cv : nullptr, d_cp,
+                            use_cdf ? cdf->size : 0, st);
+        HB_CK(cudaGetLastError());
+        E.mark(STAGE_FINALIZE, st);
+        if (!io.device)
+        {
+            to_host(E, data, d_data, (size_t)n, io);
+            to_host(E, mask, d_mask, (size_t)n, io);
+            if (opt.status) to_host(E, opt.status, d_status, (size_t)n, io);
+        }
+        E.mark(STAGE_DOWNLOAD, st);
+        E.stats.kriged = n_sim;
+        end_call(E, st);
         return 0;
     }
     catch (const CudaFail &f)

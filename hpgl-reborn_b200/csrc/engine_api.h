@@ -29,6 +29,26 @@ struct IkArgs
     double marginal;
 };
 
+struct SgsArgs
+{
+    int cov_type;
+    double ranges[3];
+    double angles[3];
+    double sill, nugget;
+    int radiuses[3];
+    int max_nb;
+    int kind; // 0 ordinary, 1 simple (ignored with LVM means)
+    long long seed;
+};
+
+// Non-parametric CDF table (host arrays): ascending values and their probabilities.
+struct CdfTable
+{
+    const float *values = nullptr;
+    const float *probs = nullptr;
+    long long size = 0;
+};
+
 struct Options
 {
     int precision = 0;
@@ -69,6 +89,8 @@ struct Stats
     long long exact_cells = 0; // cells the float prefilter left to the exact rank path
     bool prefilter = false;
     double plan_ms = 0;        // host time building the covariance tables (overlapped with upload/compaction)
+    int sgs_levels = 0;        // SGS: dependency levels (solve launches)
+    double draws_ms = 0;       // SGS: host ms generating the uniform draws (overlapped with the search)
 };
 
 void set_error(const std::string &msg);
@@ -80,6 +102,12 @@ int get_threads();
 // requires; lvm_kriging.cpp:16-39)
 int cont_kriging(int kind, const int *dims, const float *in_data, const unsigned char *in_mask, const SkArgs &a,
                  float *out_data, unsigned char *out_mask, const Options &opt, const float *means = nullptr);
+// Sequential Gaussian simulation in place on data/mask
+// (sequential_gaussian_simulation.cpp:18-131). sim_mask, cdf and means
+// (LVM) are optional; opt.status receives -1 informed, 0 kriged, 1 no
+// neighbours, 2 singular (N(0,1) draw), 3 not simulated.
+int sgs_simulation(const int *dims, float *data, unsigned char *mask, const unsigned char *sim_mask,
+                   const CdfTable *cdf, const float *means, const SgsArgs &a, const Options &opt);
 int indicator_kriging(const int *dims, const unsigned char *in_data, const unsigned char *in_mask,
                       const std::vector<IkArgs> &cats, unsigned char *out_data, unsigned char *out_mask,
                       const Options &opt);

@@ -107,4 +107,9 @@ struct Surrogate
 void build_surrogate(const Flavour &f, const KeyTable &kt, Surrogate &sg);
 
 int clamp_threads(int n);
+// The simulation's uniform draws: n doubles equal to n calls of
+// std::uniform_real_distribution<double>(0, 1) on a std::mt19937 seeded with
+// `seed` (as the standard library seeds it: seed mod 2^32).
+void sgs_draws(unsigned long long seed, long long n, double *out);
+
 } // namespace hb

@@ -125,4 +125,30 @@ void launch_sk_weights(const DevModel &m, const double *pts, int n, double *A, d
                        cudaStream_t st);
 void launch_mik_finalize(long long n_cells, const signed char *status, const double *est64, double marginal1,
                          uint8_t *out_data, uint8_t *out_mask, float *prob_out, cudaStream_t st);
+
+// sequential Gaussian simulation (sgs.cu)
+struct SgsWalk
+{
+    long long A, C, M, R0; // R <- (A R + C) mod M from R0 (a full-period walk)
+};
+constexpr int kSgsBlockMax = 160; // largest max_neighbours of the SGS solve
+void launch_sgs_forward(long long n, float *data, const uint8_t *mask, const float *means_in, float *means_out,
+                        const float *cv, const float *cp, long long cn, cudaStream_t st);
+void launch_sgs_finalize(long long n, float *data, uint8_t *mask, const int *rank_of, int n_sim,
+                         const signed char *st_rank, signed char *status, const float *cv, const float *cp,
+                         long long cn, cudaStream_t st);
+void launch_sgs_path(const SgsWalk &w, const uint8_t *mask, const uint8_t *sim_mask, int *path_cell, int *flag,
+                     cudaStream_t st);
+void launch_sgs_index(long long n, const int *path_cell, const int *flag, const int *scan, const uint8_t *mask,
+                      int *rank_of, int *sim_cells, cudaStream_t st);
+void launch_sgs_search(const Geom &g, const int4 *tmpl, int n_tmpl, const int *sim_cells, int n_sim,
+                       const int *rank_of, int k, int *nb, int *nb_rank, int *nb_cnt, int n_sm, cudaStream_t st);
+void launch_sgs_levels(const int *nb_rank, const int *nb_cnt, int k, int n_sim, int *levp1, int *ticket,
+                       int *level_count, int level_cap, int *max_level, int *err, int n_sm, cudaStream_t st);
+void launch_sgs_level_fill(int n_sim, const int *levp1, const int *level_off, int *level_fill, int *order,
+                           cudaStream_t st);
+size_t sgs_block_smem(int k);
+cudaError_t launch_sgs_solve(const Geom &g, const int *order, int n_items, const int *sim_cells, const int *nb,
+                             const int *nb_cnt, int k, const double *pair64, float *data, const float *means,
+                             const double *uniforms, signed char *st_rank, bool ordinary, int n_sm, cudaStream_t st);
 } // namespace hb

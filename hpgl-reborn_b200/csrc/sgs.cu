@@ -1,0 +1,733 @@
+// Sequential Gaussian simulation on the GPU (sequential_simulation.h:51-118,
+// sequential_gaussian_simulation.cpp:18-131).
+//
+// The reference visits every node in the order of a linear congruential walk
+// and kriges each one that is not yet informed from the first max_nb informed
+// cells of its search template, so the neighbour set of a node depends only on
+// which cells are informed when it is visited: the conditioning cells and the
+// nodes earlier in the walk. With rank(j) = the node's position among the
+// simulated nodes (-1 for conditioning cells, INT_MAX for cells never
+// simulated), "informed when j is visited" is rank(q) < rank(j). Every
+// neighbour set is therefore known before any value is drawn:
+//
+//   k_sgs_path     walk positions -> nodes (the LCG in closed form per chunk)
+//   k_sgs_index    ranks of the simulated nodes (after a scan over the walk)
+//   k_sgs_search   each simulated node's neighbours: the template scanned in
+//                  order with the rank predicate, one warp per node
+//   k_sgs_levels   dependency levels: level(j) = 1 + max level of its simulated
+//                  neighbours; a single pass over the ranks in ticket order
+//   k_sgs_solve_*  one launch per level: every node of a level depends only on
+//                  lower levels, so a level is kriged and drawn in parallel
+//
+// The draws are the reference's: one std::uniform_real_distribution<double>
+// draw of a std::mt19937 per simulated node, in walk order (generated on the
+// host), pushed through the inverse Gaussian CDF with the reference's float
+// mean and double variance.
+#include "engine.cuh"
+#include "kernels.h"
+
+#include <algorithm>
+#include <climits>
+
+namespace hb
+{
+// ------------------------------------------------------------------ scalar maths
+// gaussian_cdf_t (gaussian_distribution.h): Abramowitz & Stegun 26.2.17 and the
+// Odeh & Evans inverse, every operation rounded as the reference's double code
+// rounds it (no contraction); exp and log are CUDA's (within 1 ulp of glibc's).
+__device__ double sgs_gauss_inverse(double pr, double mean, double var)
+{
+    if (pr <= 0.0 || pr >= 1.0) return mean;
+    double p2 = pr > 0.5 ? __dsub_rn(1.0, pr) : pr;
+    if (p2 < 1e-150) p2 = 1e-150;
+    const double y = __dsqrt_rn(log(__ddiv_rn(1.0, __dmul_rn(p2, p2))));
+    double num = __dadd_rn(__dmul_rn(-0.453642210148e-4, y), -0.0204231210245);
+    num = __dadd_rn(__dmul_rn(num, y), -0.342242088547);
+    num = __dadd_rn(__dmul_rn(num, y), -1.0);
+    num = __dadd_rn(__dmul_rn(num, y), -0.322232431088);
+    double den = __dadd_rn(__dmul_rn(0.38560700634e-2, y), 0.103537752850);
+    den = __dadd_rn(__dmul_rn(den, y), 0.531103462366);
+    den = __dadd_rn(__dmul_rn(den, y), 0.588581570495);
+    den = __dadd_rn(__dmul_rn(den, y), 0.0993484626060);
+    double xp = __dadd_rn(y, __ddiv_rn(num, den));
+    if (pr < 0.5) xp = -xp;
+    return __dadd_rn(__dmul_rn(xp, __dsqrt_rn(var)), mean);
+}
+
+// standard normal CDF (mean 0, variance 1: sx = x exactly)
+__device__ double sgs_gauss_cdf(double x)
+{
+    double sx = x;
+    const bool neg = sx < 0;
+    if (neg) sx = -sx;
+    const double t = __ddiv_rn(1.0, __dadd_rn(1.0, __dmul_rn(0.2316419, sx)));
+    const double c = __ddiv_rn(1.0, __dsqrt_rn(__dmul_rn(2.0, 3.14159265358)));
+    const double zx = __dmul_rn(c, exp(__ddiv_rn(__dmul_rn(-sx, sx), 2.0)));
+    double q = __dadd_rn(__dmul_rn(1.330274429, t), -1.821255978);
+    q = __dadd_rn(__dmul_rn(q, t), 1.781477937);
+    q = __dadd_rn(__dmul_rn(q, t), -0.356563782);
+    q = __dadd_rn(__dmul_rn(q, t), 0.319381530);
+    double r = __dsub_rn(1.0, __dmul_rn(__dmul_rn(zx, q), t));
+    if (neg) r = __dsub_rn(1.0, r);
+    return r;
+}
+
+// first index whose value is not less than x (std::lower_bound)
+__device__ __forceinline__ long long lower_bound_f(const float *a, long long n, float x)
+{
+    long long lo = 0, hi = n;
+    while (lo < hi)
+    {
+        const long long mid = lo + (hi - lo) / 2;
+        if (a[mid] < x)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// non_parametric_cdf_2_t::operator() and ::inverse (non_parametric_cdf.h:215-270)
+__device__ float sgs_np_prob(const float *v, const float *p, long long n, float x)
+{
+    const long long i2 = lower_bound_f(v, n, x);
+    if (i2 == n) return p[n - 1];
+    if (i2 == 0) return p[0];
+    const float x1 = v[i2 - 1], x2 = v[i2], y1 = p[i2 - 1], y2 = p[i2];
+    return __fadd_rn(y1, __fmul_rn(__fdiv_rn(__fsub_rn(y2, y1), __fsub_rn(x2, x1)), __fsub_rn(x, x1)));
+}
+
+__device__ float sgs_np_inverse(const float *v, const float *p, long long n, float q)
+{
+    if (n <= 0) return 0.0f;
+    const long long i2 = lower_bound_f(p, n, q);
+    if (i2 == 0) return v[0];
+    if (i2 == n) return v[n - 1];
+    const float x1 = v[i2 - 1], x2 = v[i2], y1 = p[i2 - 1], y2 = p[i2];
+    return __fadd_rn(x1, __fmul_rn(__fdiv_rn(__fsub_rn(x2, x1), __fsub_rn(y2, y1)), __fsub_rn(q, y1)));
+}
+
+// ------------------------------------------------------------------ transforms
+// transform_cdf_p (cdf_utils.h:14-25) into the Gaussian space: informed cells
+// only; LVM means (transform_cdf_ptr) for every cell.
+__global__ void k_sgs_forward(long long n, float *__restrict__ data, const uint8_t *__restrict__ mask,
+                              const float *__restrict__ means_in, float *__restrict__ means_out,
+                              const float *__restrict__ cv, const float *__restrict__ cp, long long cn)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    {
+        if (cv && mask[i])
+            data[i] = __double2float_rn(sgs_gauss_inverse((double)sgs_np_prob(cv, cp, cn, data[i]), 0.0, 1.0));
+        if (means_out)
+            means_out[i] = cv ? __double2float_rn(sgs_gauss_inverse((double)sgs_np_prob(cv, cp, cn, means_in[i]), 0.0,
+                                                                    1.0))
+                              : means_in[i];
+    }
+}
+
+// Marks the simulated cells informed and maps every informed cell back
+// (transform_cdf_p(output, gaussian_cdf_t(), cdf)).
+__global__ void k_sgs_finalize(long long n, float *__restrict__ data, uint8_t *__restrict__ mask,
+                               const int *__restrict__ rank_of, int n_sim, const signed char *__restrict__ st_in,
+                               signed char *__restrict__ status, const float *__restrict__ cv,
+                               const float *__restrict__ cp, long long cn)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    {
+        const int r = rank_of[i];
+        const bool sim = r >= 0 && r < n_sim;
+        if (sim) mask[i] = 1;
+        if (status) status[i] = sim ? st_in[r] : (signed char)(r < 0 ? -1 : 3);
+        if (cv && mask[i]) data[i] = sgs_np_inverse(cv, cp, cn, __double2float_rn(sgs_gauss_cdf((double)data[i])));
+    }
+}
+
+// ------------------------------------------------------------------ the walk
+// R_{p+1} = (A R_p + C) mod M from R_0; f^m(x) = a_m x + c_m (mod M) by squaring.
+struct AffineMod
+{
+    long long a, c;
+};
+__device__ __forceinline__ AffineMod affine_then(AffineMod first, AffineMod second, long long M)
+{
+    // second(first(x)) = a2 (a1 x + c1) + c2
+    return {(second.a * first.a) % M, (second.a * first.c + second.c) % M};
+}
+
+constexpr int kWalkChunk = 64;
+
+// walk position p -> node; flag[p] = 1 when the node is simulated (not
+// informed, simulation mask 1). Requires a full-period walk (a permutation).
+__global__ void k_sgs_path(SgsWalk w, const uint8_t *__restrict__ mask, const uint8_t *__restrict__ sim_mask,
+                           int *__restrict__ path_cell, int *__restrict__ flag)
+{
+    const long long chunks = (w.M + kWalkChunk - 1) / kWalkChunk;
+    for (long long ch = (long long)blockIdx.x * blockDim.x + threadIdx.x; ch < chunks;
+         ch += (long long)gridDim.x * blockDim.x)
+    {
+        const long long p0 = ch * kWalkChunk;
+        // R_{p0} = f^{p0}(R_0)
+        AffineMod acc = {1, 0}, base = {w.A % w.M, w.C % w.M};
+        for (long long e = p0; e > 0; e >>= 1)
+        {
+            if (e & 1) acc = affine_then(acc, base, w.M);
+            base = affine_then(base, base, w.M);
+        }
+        long long R = (acc.a * w.R0 + acc.c) % w.M;
+        const long long p1 = p0 + kWalkChunk < w.M ? p0 + kWalkChunk : w.M;
+        for (long long p = p0; p < p1; ++p)
+        {
+            const int cell = (int)R;
+            path_cell[p] = cell;
+            flag[p] = (!mask[cell] && (!sim_mask || sim_mask[cell] == 1)) ? 1 : 0;
+            R = (w.A * R + w.C) % w.M;
+        }
+    }
+}
+
+// rank_of[cell]: the rank of a simulated cell, -1 for informed cells, INT_MAX
+// for cells never simulated; sim_cells[rank] = cell. `scan` holds the exclusive
+// scan of the flags; `path_cell` and the flags come from k_sgs_path.
+__global__ void k_sgs_index(long long n, const int *__restrict__ path_cell, const int *__restrict__ flag,
+                            const int *__restrict__ scan, const uint8_t *__restrict__ mask, int *__restrict__ rank_of,
+                            int *__restrict__ sim_cells)
+{
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x)
+    {
+        const int cell = path_cell[p];
+        if (flag[p])
+        {
+            rank_of[cell] = scan[p];
+            sim_cells[scan[p]] = cell;
+        }
+        else
+            rank_of[cell] = mask[cell] ? -1 : INT_MAX;
+    }
+}
+
+// ------------------------------------------------------------------ search
+// neighbour_lookup_t::find (sugarbox_neighbour_lookup.h:39-63) with the rank
+// predicate: the first k template offsets, in template order, whose cell lies
+// in the grid and was informed before the node. One warp per node, 32 offsets
+// per step. nb_rank receives each neighbour's rank (-1 for a conditioning
+// cell), which the level pass reads instead of gathering rank_of again.
+__global__ void __launch_bounds__(256) k_sgs_search(const Geom g, const int4 *__restrict__ tmpl, int n_tmpl,
+                                                    const int *__restrict__ sim_cells, int n_sim,
+                                                    const int *__restrict__ rank_of, int k, int *__restrict__ nb,
+                                                    int *__restrict__ nb_rank, int *__restrict__ nb_cnt)
+{
+    const int lane = threadIdx.x & 31;
+    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long r = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < n_sim; r += warps)
+    {
+        const int cell = sim_cells[r];
+        const int x = cell % g.nx, y = (int)((cell / g.nx) % g.ny), z = (int)(cell / ((long long)g.nx * g.ny));
+        int found = 0;
+        int *out = nb + r * (long long)k;
+        int *out_rank = nb_rank + r * (long long)k;
+        for (int base = 0; base < n_tmpl && found < k; base += 32)
+        {
+            const int t = base + lane;
+            bool hit = false;
+            int q = 0, rq = 0;
+            if (t < n_tmpl)
+            {
+                const int4 o = tmpl[t];
+                const int X = x + o.x, Y = y + o.y, Z = z + o.z;
+                if ((unsigned)X < (unsigned)g.nx && (unsigned)Y < (unsigned)g.ny && (unsigned)Z < (unsigned)g.nz)
+                {
+                    q = (int)(((long long)Z * g.ny + Y) * g.nx + X);
+                    rq = rank_of[q];
+                    hit = rq < (int)r;
+                }
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            const int slot = found + __popc(m & ((1u << lane) - 1u));
+            if (hit && slot < k)
+            {
+                out[slot] = q;
+                out_rank[slot] = rq;
+            }
+            found += __popc(m);
+        }
+        if (lane == 0) nb_cnt[r] = found < k ? found : k;
+    }
+}
+
+// ------------------------------------------------------------------ levels
+__device__ __forceinline__ int ld_relaxed_gpu(const int *p)
+{
+    int v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed_gpu(int *p, int v)
+{
+    asm volatile("st.relaxed.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+constexpr unsigned long long kLevelWaitNs = 2000000000ull; // a wait that lasts 2 s is an error
+
+// levp1[r] = level(r) + 1 (0 = not yet known). Warps take batches of 32
+// consecutive ranks in ticket order; a batch waits only on ranks below its
+// first, which belong to earlier tickets, whose warps are running: the waits
+// always end. Dependencies inside a batch are resolved by a sweep over its
+// lanes. Each wait gives up after kLevelWaitNs (err = 1); once err is set,
+// every wait ends at once.
+__global__ void __launch_bounds__(256) k_sgs_levels(const int *__restrict__ nb_rank, const int *__restrict__ nb_cnt,
+                                                    int k, int n_sim, int *levp1, int *ticket, int *level_count,
+                                                    int level_cap, int *max_level, int *err)
+{
+    const int lane = threadIdx.x & 31;
+    for (;;)
+    {
+        int b = 0;
+        if (lane == 0) b = atomicAdd(ticket, 1);
+        b = __shfl_sync(0xffffffffu, b, 0);
+        const long long base = (long long)b * 32;
+        if (base >= n_sim) break;
+        const long long r = base + lane;
+        const bool live = r < n_sim;
+        int L = 0;
+        unsigned intra = 0;
+        if (live)
+        {
+            const int n = nb_cnt[r];
+            const int *row = nb_rank + r * (long long)k;
+            // eight neighbours at a time: their ranks, then every level already
+            // published, issued together; waits only for the missing ones
+            for (int i0 = 0; i0 < n; i0 += 8)
+            {
+                int tq[8], v[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) tq[j] = i0 + j < n ? row[i0 + j] : -1;
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                {
+                    v[j] = -1; // no dependency (conditioning cell, or inside the batch)
+                    if (tq[j] >= base)
+                        intra |= 1u << (tq[j] - (int)base);
+                    else if (tq[j] >= 0)
+                        v[j] = ld_relaxed_gpu(&levp1[tq[j]]);
+                }
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                {
+                    if (v[j] == 0)
+                    {
+                        const unsigned long long t0 = global_ns();
+                        while ((v[j] = ld_relaxed_gpu(&levp1[tq[j]])) == 0)
+                        {
+                            if (ld_relaxed_gpu(err) != 0 || global_ns() - t0 > kLevelWaitNs)
+                            {
+                                atomicExch(err, 1);
+                                v[j] = 1;
+                                break;
+                            }
+                            __nanosleep(64);
+                        }
+                    }
+                    L = max(L, v[j]); // level(dep) + 1
+                }
+            }
+        }
+        // lanes in rank order: lane i's level is final once lanes < i are
+#pragma unroll 1
+        for (int i = 0; i < 32; ++i)
+        {
+            const int li = __shfl_sync(0xffffffffu, L, i);
+            if ((intra >> i) & 1u) L = max(L, li + 1);
+        }
+        if (live)
+        {
+            if (L < level_cap)
+                atomicAdd(&level_count[L], 1);
+            else
+                atomicExch(err, 2);
+            atomicMax(max_level, L);
+            st_relaxed_gpu(&levp1[r], L + 1);
+        }
+    }
+}
+
+// order[level_off[l] + i]: the ranks of level l (any order inside a level)
+__global__ void k_sgs_level_fill(int n_sim, const int *__restrict__ levp1, const int *__restrict__ level_off,
+                                 int *__restrict__ level_fill, int *__restrict__ order)
+{
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n_sim; r += gridDim.x * blockDim.x)
+    {
+        const int l = levp1[r] - 1;
+        const int pos = atomicAdd(&level_fill[l], 1);
+        order[level_off[l] + pos] = r;
+    }
+}
+
+// ------------------------------------------------------------------ solve + draw
+struct SgsNode
+{
+    int status; // 0 kriged, 1 no neighbours, 2 singular
+    float mean; // combine()'s float estimate
+    double var;
+};
+
+// combine (combiner.h:10-25) and the variance sums in the reference's order,
+// through lane shuffles (every lane ends with the result). x: A^-1 b and
+// y: A^-1 1 of row `lane` (lanes < n).
+__device__ __forceinline__ void sgs_combine_warp(int n, bool ordinary, double x, double y, double b, float v, float m,
+                                                 float m_center, double c0, SgsNode &o)
+{
+    // OK: mu = (sum x - 1) / sum y, w = x - mu y (my_kriging_weights.h:198-361)
+    double sx = 0.0, sy = 0.0;
+    if (ordinary)
+    {
+        for (int i = 0; i < n; ++i)
+        {
+            sx = __dadd_rn(sx, __shfl_sync(0xffffffffu, x, i));
+            sy = __dadd_rn(sy, __shfl_sync(0xffffffffu, y, i));
+        }
+    }
+    const bool fail = ordinary && fabs(sy) < 1e-15;
+    const double mu = ordinary && !fail ? __ddiv_rn(__dsub_rn(sx, 1.0), sy) : 0.0;
+    const double w = ordinary ? __dsub_rn(x, __dmul_rn(mu, y)) : x;
+    double var = c0;
+    float est = m_center;
+    for (int i = 0; i < n; ++i)
+    {
+        const double wi = __shfl_sync(0xffffffffu, w, i);
+        const double bi = __shfl_sync(0xffffffffu, b, i);
+        const float vi = __shfl_sync(0xffffffffu, v, i);
+        const float mi = __shfl_sync(0xffffffffu, m, i);
+        var = __dsub_rn(var, __dmul_rn(wi, bi));
+        est = __fadd_rn(est, __double2float_rn(__dmul_rn(wi, (double)__fsub_rn(vi, mi))));
+    }
+    if (ordinary) var = __dsub_rn(var, mu);
+    if (var < 0) var = 0;
+    o.status = fail ? 2 : 0;
+    o.mean = est;
+    o.var = var;
+}
+
+struct SgsSolveArgs
+{
+    Geom g;
+    const int *order;
+    int n_items;
+    const int *sim_cells;
+    const int *nb;
+    const int *nb_cnt;
+    int k;
+    const double *pair64;
+    float *data;
+    const float *means; // LVM (Gaussian-space means) or null
+    const double *uniforms;
+    signed char *st_rank; // status per rank
+    int ordinary;
+};
+
+constexpr int kSgsWarps = 4;
+constexpr int kSgsLD = 33;
+
+// n <= 32: one warp per node, lane r holds row r of A (lower triangle); the
+// second right-hand side (A^-1 1) only for ordinary kriging.
+template <bool ORD>
+__global__ void __launch_bounds__(32 * kSgsWarps) k_sgs_solve_warp(const SgsSolveArgs a)
+{
+    __shared__ double sm_all[kSgsWarps][32 * kSgsLD];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double *Sm = sm_all[warp];
+    const Geom &g = a.g;
+    const long long pc = g.pair_center;
+    for (int it = blockIdx.x * kSgsWarps + warp; it < a.n_items; it += gridDim.x * kSgsWarps)
+    {
+        const int r = a.order[it];
+        const int cell = a.sim_cells[r];
+        const int n = a.nb_cnt[r];
+        const int cx = cell % g.nx, cy = (int)((cell / g.nx) % g.ny), cz = (int)(cell / ((long long)g.nx * g.ny));
+        const bool live = lane < n;
+        int px = 0, py = 0, pz = 0;
+        float v = 0.0f, m = 0.0f;
+        if (live)
+        {
+            const int q = a.nb[(long long)r * a.k + lane];
+            px = q % g.nx;
+            py = (int)((q / g.nx) % g.ny);
+            pz = (int)(q / ((long long)g.nx * g.ny));
+            v = a.data[q];
+            if (a.means) m = a.means[q];
+        }
+        SgsNode o = {1, 0.0f, 0.0};
+        if (n > 0)
+        {
+            double row[32];
+#pragma unroll
+            for (int c = 0; c < 32; ++c)
+            {
+                const int qx = __shfl_sync(0xffffffffu, px, c), qy = __shfl_sync(0xffffffffu, py, c),
+                          qz = __shfl_sync(0xffffffffu, pz, c);
+                double e = 0.0;
+                if (live && c <= lane) e = a.pair64[pc + pair_lin(g, px - qx, py - qy, pz - qz)];
+                if (!live && c == lane) e = 1.0;
+                row[c] = e;
+            }
+            const double b = live ? a.pair64[pc + pair_lin(g, px - cx, py - cy, pz - cz)] : 0.0;
+            bool fail = false;
+            double inv = 0.0;
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+            {
+                Sm[j * kSgsLD + lane] = row[j];
+                __syncwarp();
+                const double d = Sm[j * kSgsLD + j];
+                fail |= !(d > 0.0);
+                const double is = 1.0 / sqrt(d);
+                const double s = row[j] * is * is;
+#pragma unroll
+                for (int c = j + 1; c < 32; ++c) row[c] -= s * Sm[j * kSgsLD + c];
+                row[j] *= is;
+                if (lane == j) inv = is;
+                __syncwarp();
+            }
+            // forward L y = [b, 1], back L^T x = y
+            double acc0 = b, acc1 = live ? 1.0 : 0.0, y0 = 0.0, y1 = 0.0;
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+            {
+                if (lane == j)
+                {
+                    y0 = acc0 * inv;
+                    if (ORD) y1 = acc1 * inv;
+                }
+                const double t0 = __shfl_sync(0xffffffffu, y0, j);
+                const double t1 = ORD ? __shfl_sync(0xffffffffu, y1, j) : 0.0;
+                if (lane > j)
+                {
+                    acc0 -= row[j] * t0;
+                    if (ORD) acc1 -= row[j] * t1;
+                }
+            }
+            double x0 = 0.0, x1 = 0.0;
+            acc0 = y0;
+            acc1 = y1;
+#pragma unroll
+            for (int i = 31; i >= 0; --i)
+            {
+                const double l = Sm[lane * kSgsLD + i] * inv;
+                if (lane == i)
+                {
+                    x0 = acc0 * inv;
+                    if (ORD) x1 = acc1 * inv;
+                }
+                const double t0 = __shfl_sync(0xffffffffu, x0, i);
+                const double t1 = ORD ? __shfl_sync(0xffffffffu, x1, i) : 0.0;
+                if (lane < i)
+                {
+                    acc0 -= l * t0;
+                    if (ORD) acc1 -= l * t1;
+                }
+            }
+            __syncwarp();
+            fail = __any_sync(0xffffffffu, fail && live);
+            const float mc = a.means ? a.means[cell] : 0.0f;
+            sgs_combine_warp(n, ORD, x0, x1, b, v, m, mc, a.pair64[pc], o);
+            if (fail) o.status = 2;
+        }
+        if (lane == 0)
+        {
+            const double u = a.uniforms[r];
+            const double val =
+                o.status == 0 ? sgs_gauss_inverse(u, (double)o.mean, o.var) : sgs_gauss_inverse(u, 0.0, 1.0);
+            a.data[cell] = __double2float_rn(val);
+            a.st_rank[r] = (signed char)o.status;
+        }
+    }
+}
+
+// 32 < n <= kSgsBlockMax: one block per node, the matrix in shared memory.
+constexpr int kSgsBlockThreads = 128;
+
+__global__ void __launch_bounds__(kSgsBlockThreads) k_sgs_solve_block(const SgsSolveArgs a)
+{
+    extern __shared__ double sh[];
+    const int kk = a.k;
+    double *A = sh;                   // kk * kk, row-major
+    double *b = A + (size_t)kk * kk;  // rhs
+    double *x = b + kk;               // A^-1 b
+    double *y = x + kk;               // A^-1 1
+    float *vals = reinterpret_cast<float *>(y + kk);
+    float *ms = vals + kk;
+    __shared__ int s_fail;
+    const Geom &g = a.g;
+    const long long pc = g.pair_center;
+    for (int it = blockIdx.x; it < a.n_items; it += gridDim.x)
+    {
+        const int r = a.order[it];
+        const int cell = a.sim_cells[r];
+        const int n = a.nb_cnt[r];
+        const int cx = cell % g.nx, cy = (int)((cell / g.nx) % g.ny), cz = (int)(cell / ((long long)g.nx * g.ny));
+        const int *row = a.nb + (long long)r * kk;
+        for (int e = threadIdx.x; e < n * n; e += blockDim.x)
+        {
+            const int i = e / n, j = e % n;
+            const int qi = row[i], qj = row[j];
+            const int dx = qi % g.nx - qj % g.nx, dy = (int)((qi / g.nx) % g.ny) - (int)((qj / g.nx) % g.ny),
+                      dz = (int)(qi / ((long long)g.nx * g.ny)) - (int)(qj / ((long long)g.nx * g.ny));
+            A[(size_t)i * n + j] = a.pair64[pc + pair_lin(g, dx, dy, dz)];
+        }
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+        {
+            const int q = row[i];
+            b[i] = a.pair64[pc + pair_lin(g, q % g.nx - cx, (int)((q / g.nx) % g.ny) - cy,
+                                          (int)(q / ((long long)g.nx * g.ny)) - cz)];
+            vals[i] = a.data[q];
+            ms[i] = a.means ? a.means[q] : 0.0f;
+        }
+        if (threadIdx.x == 0) s_fail = 0;
+        __syncthreads();
+        for (int j = 0; j < n; ++j)
+        {
+            const double d = A[(size_t)j * n + j];
+            if (threadIdx.x == 0 && !(d > 0.0)) s_fail = 1;
+            const double ljj = sqrt(d);
+            __syncthreads();
+            for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) A[(size_t)i * n + j] /= ljj;
+            if (threadIdx.x == 0) A[(size_t)j * n + j] = ljj;
+            __syncthreads();
+            const int span = n - j - 1;
+            for (int e = threadIdx.x; e < span * span; e += blockDim.x)
+            {
+                const int i = j + 1 + e / span, c = j + 1 + e % span;
+                if (c <= i) A[(size_t)i * n + c] -= A[(size_t)i * n + j] * A[(size_t)c * n + j];
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x < 2)
+        {
+            double *xv = threadIdx.x == 0 ? x : y;
+            for (int i = 0; i < n; ++i)
+            {
+                double s = threadIdx.x == 0 ? b[i] : 1.0;
+                for (int c = 0; c < i; ++c) s -= A[(size_t)i * n + c] * xv[c];
+                xv[i] = s / A[(size_t)i * n + i];
+            }
+            for (int i = n - 1; i >= 0; --i)
+            {
+                double s = xv[i];
+                for (int c = i + 1; c < n; ++c) s -= A[(size_t)c * n + i] * xv[c];
+                xv[i] = s / A[(size_t)i * n + i];
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            SgsNode o = {1, 0.0f, 0.0};
+            if (n > 0)
+            {
+                const bool ordinary = a.ordinary != 0;
+                double sx = 0.0, sy = 0.0;
+                if (ordinary)
+                    for (int i = 0; i < n; ++i)
+                    {
+                        sx = __dadd_rn(sx, x[i]);
+                        sy = __dadd_rn(sy, y[i]);
+                    }
+                const bool fail = s_fail || (ordinary && fabs(sy) < 1e-15);
+                const double mu = ordinary && !fail ? __ddiv_rn(__dsub_rn(sx, 1.0), sy) : 0.0;
+                double var = a.pair64[pc];
+                float est = a.means ? a.means[cell] : 0.0f;
+                for (int i = 0; i < n; ++i)
+                {
+                    const double w = ordinary ? __dsub_rn(x[i], __dmul_rn(mu, y[i])) : x[i];
+                    var = __dsub_rn(var, __dmul_rn(w, b[i]));
+                    est = __fadd_rn(est, __double2float_rn(__dmul_rn(w, (double)__fsub_rn(vals[i], ms[i]))));
+                }
+                if (ordinary) var = __dsub_rn(var, mu);
+                if (var < 0) var = 0;
+                o.status = fail ? 2 : 0;
+                o.mean = est;
+                o.var = var;
+            }
+            const double u = a.uniforms[r];
+            const double val =
+                o.status == 0 ? sgs_gauss_inverse(u, (double)o.mean, o.var) : sgs_gauss_inverse(u, 0.0, 1.0);
+            a.data[cell] = __double2float_rn(val);
+            a.st_rank[r] = (signed char)o.status;
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------ launchers
+void launch_sgs_forward(long long n, float *data, const uint8_t *mask, const float *means_in, float *means_out,
+                        const float *cv, const float *cp, long long cn, cudaStream_t st)
+{
+    k_sgs_forward<<<1184, 256, 0, st>>>(n, data, mask, means_in, means_out, cv, cp, cn);
+}
+void launch_sgs_finalize(long long n, float *data, uint8_t *mask, const int *rank_of, int n_sim,
+                         const signed char *st_rank, signed char *status, const float *cv, const float *cp,
+                         long long cn, cudaStream_t st)
+{
+    k_sgs_finalize<<<1184, 256, 0, st>>>(n, data, mask, rank_of, n_sim, st_rank, status, cv, cp, cn);
+}
+void launch_sgs_path(const SgsWalk &w, const uint8_t *mask, const uint8_t *sim_mask, int *path_cell, int *flag,
+                     cudaStream_t st)
+{
+    const long long chunks = (w.M + kWalkChunk - 1) / kWalkChunk;
+    const int blocks = (int)std::min<long long>((chunks + 255) / 256, 4736);
+    k_sgs_path<<<blocks, 256, 0, st>>>(w, mask, sim_mask, path_cell, flag);
+}
+void launch_sgs_index(long long n, const int *path_cell, const int *flag, const int *scan, const uint8_t *mask,
+                      int *rank_of, int *sim_cells, cudaStream_t st)
+{
+    k_sgs_index<<<1184, 256, 0, st>>>(n, path_cell, flag, scan, mask, rank_of, sim_cells);
+}
+void launch_sgs_search(const Geom &g, const int4 *tmpl, int n_tmpl, const int *sim_cells, int n_sim,
+                       const int *rank_of, int k, int *nb, int *nb_rank, int *nb_cnt, int n_sm, cudaStream_t st)
+{
+    k_sgs_search<<<n_sm * 8, 256, 0, st>>>(g, tmpl, n_tmpl, sim_cells, n_sim, rank_of, k, nb, nb_rank, nb_cnt);
+}
+void launch_sgs_levels(const int *nb_rank, const int *nb_cnt, int k, int n_sim, int *levp1, int *ticket,
+                       int *level_count, int level_cap, int *max_level, int *err, int n_sm, cudaStream_t st)
+{
+    k_sgs_levels<<<n_sm * 8, 256, 0, st>>>(nb_rank, nb_cnt, k, n_sim, levp1, ticket, level_count, level_cap,
+                                           max_level, err);
+}
+void launch_sgs_level_fill(int n_sim, const int *levp1, const int *level_off, int *level_fill, int *order,
+                           cudaStream_t st)
+{
+    k_sgs_level_fill<<<1184, 256, 0, st>>>(n_sim, levp1, level_off, level_fill, order);
+}
+size_t sgs_block_smem(int k) { return (size_t)k * k * 8 + 3 * (size_t)k * 8 + 2 * (size_t)k * 4; }
+
+cudaError_t launch_sgs_solve(const Geom &g, const int *order, int n_items, const int *sim_cells, const int *nb,
+                             const int *nb_cnt, int k, const double *pair64, float *data, const float *means,
+                             const double *uniforms, signed char *st_rank, bool ordinary, int n_sm, cudaStream_t st)
+{
+    if (n_items <= 0) return cudaSuccess;
+    SgsSolveArgs a{g, order, n_items, sim_cells, nb, nb_cnt, k, pair64, data, means, uniforms, st_rank,
+                   ordinary ? 1 : 0};
+    if (k <= 32)
+    {
+        const int blocks = std::min((n_items + kSgsWarps - 1) / kSgsWarps, n_sm * 16);
+        if (ordinary)
+            k_sgs_solve_warp<true><<<blocks, 32 * kSgsWarps, 0, st>>>(a);
+        else
+            k_sgs_solve_warp<false><<<blocks, 32 * kSgsWarps, 0, st>>>(a);
+    }
+    else
+    {
+        const size_t smem = sgs_block_smem(k);
+        cudaError_t e =
+            cudaFuncSetAttribute(k_sgs_solve_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        const int blocks = std::min(n_items, n_sm * 8);
+        k_sgs_solve_block<<<blocks, kSgsBlockThreads, smem, st>>>(a);
+    }
+    return cudaGetLastError();
+}
+} // namespace hb

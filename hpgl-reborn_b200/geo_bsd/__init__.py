@@ -2,3 +2,5 @@
 from .geo import *  # noqa: F401,F403
 from .geo import __all__  # noqa: F401
 from .hpgl_wrap import last_stats  # noqa: F401
+from .cdf import CdfData, calc_cdf  # noqa: F401
+from .sgs import sgs_simulation  # noqa: F401

@@ -30,6 +30,19 @@ class _HPGL_IND_MASKED_ARRAY(C.Structure):
                 ("indicator_count", C.c_int)]
 
 
+class _HPGL_KRIGING_KIND:
+    ordinary = 0
+    simple = 1
+
+
+class _HPGL_UBYTE_ARRAY(C.Structure):
+    _fields_ = [("data", C.POINTER(C.c_ubyte)), ("shape", _HPGL_SHAPE)]
+
+
+class _HPGL_FLOAT_ARRAY(C.Structure):
+    _fields_ = [("data", C.POINTER(C.c_float)), ("shape", _HPGL_SHAPE)]
+
+
 class _HPGL_OK_PARAMS(C.Structure):
     _fields_ = [("covariance_type", C.c_int), ("ranges", C.c_double * 3), ("angles", C.c_double * 3),
                 ("sill", C.c_double), ("nugget", C.c_double), ("radiuses", C.c_int * 3),
@@ -62,6 +75,20 @@ class __hpgl_cov_params_t(C.Structure):
 _HPGL_COV_PARAMS = __hpgl_cov_params_t
 
 
+class _HPGL_SGS_PARAMS(C.Structure):
+    _fields_ = [("covariance_type", C.c_int), ("ranges", C.c_double * 3), ("angles", C.c_double * 3),
+                ("sill", C.c_double), ("nugget", C.c_double), ("radiuses", C.c_int * 3),
+                ("max_neighbours", C.c_int), ("kriging_kind", C.c_int), ("seed", C.c_long),
+                ("min_neighbours", C.c_int)]
+
+
+class hpgl_non_parametric_cdf_t(C.Structure):
+    _fields_ = [("values", C.POINTER(C.c_float)), ("probs", C.POINTER(C.c_float)), ("size", C.c_longlong)]
+
+
+_HPGL_NON_PARAMETRIC_CDF = hpgl_non_parametric_cdf_t
+
+
 class _HPGL_B200_OPTIONS(C.Structure):
     _fields_ = [("precision", C.c_int), ("refine_steps", C.c_int), ("flags", C.c_uint),
                 ("stream", C.c_void_p), ("estimate64", C.c_void_p), ("variance", C.c_void_p),
@@ -85,7 +112,8 @@ EXPORTS = [
     "hpgl_get_last_exception_message", "hpgl_set_output_handler", "hpgl_set_progress_handler",
     "hpgl_set_thread_num", "hpgl_get_thread_num", "hpgl_ordinary_kriging", "hpgl_simple_kriging",
     "hpgl_simple_kriging_weights", "hpgl_indicator_kriging", "hpgl_median_ik", "hpgl_lvm_kriging",
-    "hpgl_b200_cont_kriging_ex", "hpgl_b200_lvm_kriging_ex", "hpgl_b200_indicator_kriging_ex", "hpgl_b200_median_ik_ex",
+    "hpgl_sgs_simulation", "hpgl_sgs_lvm_simulation",
+    "hpgl_b200_cont_kriging_ex", "hpgl_b200_lvm_kriging_ex", "hpgl_b200_sgs_ex", "hpgl_b200_sgs_draws", "hpgl_b200_indicator_kriging_ex", "hpgl_b200_median_ik_ex",
     "hpgl_b200_find_neighbours", "hpgl_b200_last_stats", "hpgl_b200_host_alloc", "hpgl_b200_host_free",
     "hpgl_b200_transform", "hpgl_b200_template", "hpgl_b200_covariance", "hpgl_b200_version",
     "hpgl_b200_sk_weights_noalloc", "hpgl_b200_loo_ok", "hpgl_b200_loo_ok_adjoint",
@@ -137,6 +165,19 @@ def _load():
     lib.hpgl_b200_lvm_kriging_ex.restype = C.c_int
     lib.hpgl_b200_lvm_kriging_ex.argtypes = [i_p, vp, vp, vp, C.POINTER(_HPGL_OK_PARAMS), vp, vp,
                                              C.POINTER(_HPGL_B200_OPTIONS)]
+    lib.hpgl_sgs_simulation.restype = None
+    lib.hpgl_sgs_simulation.argtypes = [C.POINTER(_HPGL_CONT_MASKED_ARRAY), C.POINTER(_HPGL_SGS_PARAMS),
+                                        C.POINTER(_HPGL_NON_PARAMETRIC_CDF), C.POINTER(C.c_double),
+                                        C.POINTER(_HPGL_UBYTE_ARRAY)]
+    lib.hpgl_sgs_lvm_simulation.restype = None
+    lib.hpgl_sgs_lvm_simulation.argtypes = [C.POINTER(_HPGL_CONT_MASKED_ARRAY), C.POINTER(_HPGL_SGS_PARAMS),
+                                            C.POINTER(_HPGL_NON_PARAMETRIC_CDF), C.POINTER(_HPGL_FLOAT_ARRAY),
+                                            C.POINTER(_HPGL_UBYTE_ARRAY)]
+    lib.hpgl_b200_sgs_ex.restype = C.c_int
+    lib.hpgl_b200_sgs_ex.argtypes = [i_p, vp, vp, vp, C.POINTER(_HPGL_NON_PARAMETRIC_CDF), vp,
+                                     C.POINTER(_HPGL_SGS_PARAMS), C.POINTER(_HPGL_B200_OPTIONS)]
+    lib.hpgl_b200_sgs_draws.restype = C.c_int
+    lib.hpgl_b200_sgs_draws.argtypes = [C.c_longlong, C.c_longlong, vp]
     lib.hpgl_b200_indicator_kriging_ex.restype = C.c_int
     lib.hpgl_b200_indicator_kriging_ex.argtypes = [i_p, vp, vp, C.POINTER(_HPGL_IK_PARAMS), C.c_int, vp, vp,
                                                    C.POINTER(_HPGL_B200_OPTIONS)]
@@ -191,7 +232,7 @@ STATS_KEYS = (["total_ms", "search_ms", "solve_ms", "tie_cells", "template_cells
               + [f"bucket_flops_{i}" for i in range(5)]
               + ["stage_" + s + "_ms" for s in ("upload", "compact", "tables", "bins", "search", "ties", "prepare",
                                               "solve", "finalize", "download")]
-              + ["prefilter_exact_cells", "prefilter_active", "plan_ms"])
+              + ["prefilter_exact_cells", "prefilter_active", "plan_ms", "sgs_levels", "sgs_draws_ms"])
 
 
 def last_stats() -> dict:

@@ -34,6 +34,7 @@ class ValidationConstants:
     MIN_PROBABILITY = 0.0
     MAX_PROBABILITY = 1.0
     MAX_INDICATORS = 256
+    MIN_SEED = 0
 
 
 class ValidationError(Exception):
@@ -150,6 +151,19 @@ class ParameterValidator:
                     validation_logger.warning(
                         f"Angle[{i}] = {a} is outside typical range "
                         f"[{ValidationConstants.MIN_ANGLE}, {ValidationConstants.MAX_ANGLE}]")
+
+    @staticmethod
+    def validate_min_neighbors(min_neighbors: int, max_neighbors: int) -> None:
+        if min_neighbors > max_neighbors:
+            raise CriticalValidationError(
+                f"Min neighbors {min_neighbors} exceeds max neighbors {max_neighbors}", "min_neighbors")
+        if min_neighbors < 0:
+            raise CriticalValidationError(f"Min neighbors {min_neighbors} is negative", "min_neighbors")
+
+    @staticmethod
+    def validate_seed(seed: int) -> None:
+        if seed < ValidationConstants.MIN_SEED:
+            validation_logger.warning(f"Seed value {seed} is negative")
 
     @staticmethod
     def validate_probability(prob: float, name: str = "probability") -> None:

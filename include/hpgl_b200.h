@@ -57,6 +57,19 @@ struct hpgl_ik_params_t {
     int m_radiuses[3]; int m_max_neighbours; double m_marginal_prob;
 };
 
+/* api.h:39-43 */
+struct hpgl_float_array_t { float *m_data; struct hpgl_shape_t m_shape; };
+/* api.h:45-49 */
+struct hpgl_ubyte_array_t { unsigned char *m_data; struct hpgl_shape_t m_shape; };
+/* api.h:84-96 (m_kriging_kind 0 ordinary, 1 simple; m_min_neighbours is unused,
+ * as in the reference) */
+struct hpgl_sgs_params_t {
+    int m_covariance_type; double m_ranges[3]; double m_angles[3]; double m_sill; double m_nugget;
+    int m_radiuses[3]; int m_max_neighbours; int m_kriging_kind; long m_seed; int m_min_neighbours;
+};
+/* api.h:148-153: ascending values with their cumulative probabilities */
+struct hpgl_non_parametric_cdf_t { float *m_values; float *m_probs; long long m_size; };
+
 /* -------------------------------------------------- reference-compatible ABI */
 /* Replaces api.h:159-160 / api.cpp:38-41. */
 char *hpgl_get_last_exception_message(void);
@@ -93,6 +106,22 @@ void hpgl_indicator_kriging(struct hpgl_ind_masked_array_t *in_data, struct hpgl
 /* Replaces api.h:274-277 / api.cpp:552-601 (median_ik.cpp:24-89). */
 void hpgl_median_ik(struct hpgl_ind_masked_array_t *in_data, struct hpgl_median_ik_params_t *params,
                     struct hpgl_ind_masked_array_t *out_data);
+
+/* Replaces api.h:253-258 / api.cpp:484-516 (sequential_gaussian_simulation.cpp:18-77):
+ * simulates, in place, every node of data that is not informed and whose
+ * simulation_mask byte (when given) is 1. cdf (optional) maps the informed
+ * values to the Gaussian space and the result back; `mean` is accepted and, as
+ * in the reference, unused (SK runs around 0). Grids above 10,000,000 cells and
+ * max_neighbours above 160 are rejected. */
+void hpgl_sgs_simulation(struct hpgl_cont_masked_array_t *data, struct hpgl_sgs_params_t *params,
+                         struct hpgl_non_parametric_cdf_t *cdf, double *mean,
+                         struct hpgl_ubyte_array_t *simulation_mask);
+/* Replaces api.h:260-265 / api.cpp:519-550 (sequential_gaussian_simulation.cpp:79-130):
+ * SGS with SK weights around a locally varying mean (one float per cell,
+ * mapped through cdf when given). */
+void hpgl_sgs_lvm_simulation(struct hpgl_cont_masked_array_t *data, struct hpgl_sgs_params_t *params,
+                             struct hpgl_non_parametric_cdf_t *cdf, struct hpgl_float_array_t *means,
+                             struct hpgl_ubyte_array_t *simulation_mask);
 
 /* ------------------------------------------------------------ _ex extensions */
 /* status codes */
@@ -143,6 +172,19 @@ int hpgl_b200_cont_kriging_ex(int kind, const int *dims, const float *in_data, c
 int hpgl_b200_lvm_kriging_ex(const int *dims, const float *in_data, const unsigned char *in_mask,
                              const float *mean_data, const struct hpgl_ok_params_t *params, float *out_data,
                              unsigned char *out_mask, const struct hpgl_b200_options_t *opt);
+/* SGS with options (hpgl_sgs_simulation's rules): data and mask are updated in
+ * place; sim_mask and means (LVM) are optional and, like data and mask, device
+ * pointers under HPGL_B200_DEVICE_POINTERS; the cdf tables are host memory.
+ * opt->status receives per cell -1 informed, 0 kriged, 1 no neighbours,
+ * 2 singular (drawn from N(0,1)), 3 not simulated. */
+int hpgl_b200_sgs_ex(const int *dims, float *data, unsigned char *mask, const unsigned char *sim_mask,
+                     const struct hpgl_non_parametric_cdf_t *cdf, const float *means,
+                     const struct hpgl_sgs_params_t *params, const struct hpgl_b200_options_t *opt);
+/* The simulation's uniform draws (host): out[i] = the i-th call of
+ * std::uniform_real_distribution<double>(0, 1) on a std::mt19937 seeded with
+ * `seed` (bs_random_generator.cpp:9-25), as sgs_simulation consumes them, one
+ * per simulated node in walk order. */
+int hpgl_b200_sgs_draws(long long seed, long long n, double *out);
 /* Full IK (indicator_count > 2 categories, per-category models) or, with one
  * params entry and indicator_count == 2, median IK (median_ik.cpp:24-89). */
 int hpgl_b200_indicator_kriging_ex(const int *dims, const unsigned char *in_data, const unsigned char *in_mask,
@@ -178,8 +220,10 @@ int hpgl_b200_find_neighbours(int kind, const int *dims, const unsigned char *ma
  *   [36] cells whose neighbours the float distance prefilter could not
  *        decide (selected by exact ranks over every candidate instead)
  *   [37] 1 when the float distance prefilter was active in the last search
- *   [38] host ms building the covariance tables (overlapped with the upload) */
-#define HPGL_B200_STATS_LEN 39
+ *   [38] host ms building the covariance tables (overlapped with the upload)
+ *   [39] simulation: dependency levels (one solve launch each)
+ *   [40] simulation: host ms generating the uniform draws (overlapped) */
+#define HPGL_B200_STATS_LEN 41
 int hpgl_b200_last_stats(double *out, int cap);
 
 /* No counterpart in the reference. The same SK weights as

@@ -65,6 +65,38 @@ def engine_lvm(wl, means, precision=0, refine_steps=2, flags=0):
     return {"data": out_d, "mask": out_m, "est": est, "var": var, "status": st, "stats": W.last_stats()}
 
 
+def sgs_params(cov, radiuses, k, kind, seed):
+    return W._HPGL_SGS_PARAMS(covariance_type=cov.cov_type, ranges=tuple(cov.ranges), angles=tuple(cov.angles),
+                              sill=cov.sill, nugget=cov.nugget, radiuses=tuple(int(r) for r in radiuses),
+                              max_neighbours=int(k), kriging_kind=int(kind), seed=int(seed), min_neighbours=0)
+
+
+def engine_sgs(dims, data, mask, cov, radiuses, k, seed, kind=1, sim_mask=None, cdf=None, means=None):
+    """SGS through hpgl_b200_sgs_ex with host buffers; returns data, mask, status, stats."""
+    n = int(np.prod(dims))
+    d = np.ascontiguousarray(data, np.float32).copy()
+    m = np.ascontiguousarray(mask, np.uint8).copy()
+    st = np.zeros(n, np.int8)
+    keep = []
+    c = None
+    if cdf is not None:
+        cv = np.ascontiguousarray(cdf[0], np.float32)
+        cp = np.ascontiguousarray(cdf[1], np.float32)
+        keep += [cv, cp]
+        c = W._HPGL_NON_PARAMETRIC_CDF(values=cv.ctypes.data_as(C.POINTER(C.c_float)),
+                                       probs=cp.ctypes.data_as(C.POINTER(C.c_float)), size=len(cv))
+    sm = np.ascontiguousarray(sim_mask, np.uint8) if sim_mask is not None else None
+    mv = np.ascontiguousarray(means, np.float32) if means is not None else None
+    opt = W._HPGL_B200_OPTIONS(precision=0, refine_steps=0, flags=0, stream=None, estimate64=None, variance=None,
+                               status=st.ctypes.data, ik_probs=None)
+    p = sgs_params(cov, radiuses, k, kind, seed)
+    rc = W._hpgl_so.hpgl_b200_sgs_ex((C.c_int * 3)(*dims), d.ctypes.data, m.ctypes.data,
+                                     sm.ctypes.data if sm is not None else None, C.byref(c) if c is not None else None,
+                                     mv.ctypes.data if mv is not None else None, C.byref(p), C.byref(opt))
+    W.check(rc, "sgs_ex")
+    return {"data": d, "mask": m, "status": st, "stats": W.last_stats()}
+
+
 def engine_neighbours(kind, wl, nodes, cov=None, radiuses=None, k=None, mask=None):
     cov = cov or wl.cov
     radiuses = radiuses or wl.radiuses

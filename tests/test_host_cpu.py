@@ -59,6 +59,12 @@ def test_struct_layouts_match_header():
                                                  "m_radiuses", "m_max_neighbours", "m_marginal_prob"]),
         "hpgl_b200_options_t": (W._HPGL_B200_OPTIONS, ["precision", "refine_steps", "flags", "stream", "estimate64",
                                                        "variance", "status", "ik_probs", "tolerance"]),
+        "hpgl_float_array_t": (W._HPGL_FLOAT_ARRAY, ["m_data", "m_shape"]),
+        "hpgl_ubyte_array_t": (W._HPGL_UBYTE_ARRAY, ["m_data", "m_shape"]),
+        "hpgl_sgs_params_t": (W._HPGL_SGS_PARAMS, ["m_covariance_type", "m_ranges", "m_angles", "m_sill", "m_nugget",
+                                                   "m_radiuses", "m_max_neighbours", "m_kriging_kind", "m_seed",
+                                                   "m_min_neighbours"]),
+        "hpgl_non_parametric_cdf_t": (W._HPGL_NON_PARAMETRIC_CDF, ["m_values", "m_probs", "m_size"]),
     }
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
     for s, (_, fl) in fields.items():
@@ -153,3 +159,58 @@ def test_lvm_entry_argument_checks():
     assert fn(dims, wl.data.ctypes.data, wl.mask.ctypes.data, means.ctypes.data, C.byref(p), out.ctypes.data,
               om.ctypes.data, None) == W.ECUDA
     np.testing.assert_array_equal(out, wl.data)
+
+
+def test_sgs_entry_argument_checks():
+    """SGS limits are checked before any device work: more than 10,000,000 cells
+    and max_neighbours above 160 are ELIMIT, a seed with a negative remainder EINVAL."""
+    dims = (C.c_int * 3)(2000, 2000, 3)
+    p = W._HPGL_SGS_PARAMS(covariance_type=0, ranges=(10.0, 10.0, 10.0), angles=(0.0, 0.0, 0.0), sill=1.0,
+                           nugget=0.0, radiuses=(5, 5, 5), max_neighbours=12, kriging_kind=1, seed=1,
+                           min_neighbours=0)
+    fn = W._hpgl_so.hpgl_b200_sgs_ex
+    assert fn(dims, None, None, None, None, None, C.byref(p), None) == W.EINVAL  # null arrays
+    d = np.zeros(8, np.float32)
+    m = np.zeros(8, np.uint8)
+    assert fn(dims, d.ctypes.data, m.ctypes.data, None, None, None, C.byref(p), None) == W.ELIMIT
+    small = (C.c_int * 3)(2, 2, 2)
+    p.max_neighbours = 161
+    assert fn(small, d.ctypes.data, m.ctypes.data, None, None, None, C.byref(p), None) == W.ELIMIT
+    p.max_neighbours = 12
+    p.seed = -3
+    assert fn(small, d.ctypes.data, m.ctypes.data, None, None, None, C.byref(p), None) == W.EINVAL
+    assert "seed" in W.last_error()
+
+
+def test_calc_cdf_matches_the_reference_loop():
+    """calc_cdf against a loop restatement of cdf.py:8-40 (dict of counts, sorted
+    keys without the largest, running sums)."""
+    import geo_bsd
+    rng = np.random.default_rng(2)
+    data = np.round(rng.normal(size=(6, 5, 4)), 1).astype(np.float32)
+    mask = (rng.random((6, 5, 4)) < 0.6).astype(np.uint8)
+    got = geo_bsd.calc_cdf(geo_bsd.ContProperty(data, mask))
+    counts, full = {}, 0
+    for x in range(6):
+        for y in range(5):
+            for z in range(4):
+                if mask[x, y, z]:
+                    counts[data[x, y, z]] = counts.get(data[x, y, z], 0) + 1
+                    full += 1
+    values = np.sort(list(counts.keys()))[: len(counts) - 1]
+    probs, last = np.zeros(values.shape), 0.0
+    for i in range(values.size):
+        probs[i] = last + counts[values[i]] / float(full)
+        last = probs[i]
+    np.testing.assert_array_equal(got.values, values.astype(np.float32))
+    np.testing.assert_array_equal(got.probs, probs.astype(np.float32))
+
+
+@pytest.mark.parametrize("seed", [0, 1, 42, 4357, 2**31 + 5, 2**32 + 7, -5])
+def test_sgs_draws_equal_the_standard_library(seed):
+    """The simulation's uniform draws (the engine's own MT19937 and canonical
+    double) are bit-identical to std::mt19937 + std::uniform_real_distribution."""
+    n = 5000
+    got = np.zeros(n)
+    assert W._hpgl_so.hpgl_b200_sgs_draws(seed, n, got.ctypes.data) == 0
+    np.testing.assert_array_equal(got.view(np.uint64), O.mt_draws(seed, n).view(np.uint64))
