@@ -18,6 +18,8 @@
 //                  neighbours; a single pass over the ranks in ticket order
 //   k_sgs_solve_*  one launch per level: every node of a level depends only on
 //                  lower levels, so a level is kriged and drawn in parallel
+//                  (FP64: two nodes per warp for up to 32 neighbours, one
+//                  block per node beyond)
 //
 // The draws are the reference's: one std::uniform_real_distribution<double>
 // draw of a std::mt19937 per simulated node, in walk order (generated on the
@@ -275,14 +277,33 @@ __device__ __forceinline__ unsigned long long global_ns()
 constexpr unsigned long long kLevelWaitNs = 2000000000ull; // a wait that lasts 2 s is an error
 
 // levp1[r] = level(r) + 1 (0 = not yet known). Warps take batches of 32
-// consecutive ranks in ticket order; a batch waits only on ranks below its
-// first, which belong to earlier tickets, whose warps are running: the waits
-// always end. Dependencies inside a batch are resolved by a sweep over its
-// lanes. Each wait gives up after kLevelWaitNs (err = 1); once err is set,
-// every wait ends at once.
+// consecutive ranks in ticket order and every lane publishes its own level as
+// soon as its dependencies are known, so a chain of dependencies advances one
+// node at a time rather than one batch at a time. A rank waits only on lower
+// ranks: those of earlier tickets, whose warps are running, and those of lower
+// lanes of its own batch, which independent thread scheduling keeps running
+// while it waits. So every wait ends; each still gives up after kLevelWaitNs
+// (err = 1), and once err is set every wait ends at once.
+__device__ __forceinline__ int sgs_wait_level(const int *levp1, int tq, int *err)
+{
+    int v = ld_relaxed_gpu(&levp1[tq]);
+    if (v != 0) return v;
+    const unsigned long long t0 = global_ns();
+    while ((v = ld_relaxed_gpu(&levp1[tq])) == 0)
+    {
+        if (ld_relaxed_gpu(err) != 0 || global_ns() - t0 > kLevelWaitNs)
+        {
+            atomicExch(err, 1);
+            return 1;
+        }
+        __nanosleep(32);
+    }
+    return v;
+}
+
 __global__ void __launch_bounds__(256) k_sgs_levels(const int *__restrict__ nb_rank, const int *__restrict__ nb_cnt,
-                                                    int k, int n_sim, int *levp1, int *ticket, int *level_count,
-                                                    int level_cap, int *max_level, int *err)
+                                                    int k, int n_sim, int *levp1, int *ticket, int level_cap,
+                                                    int *max_level, int *err)
 {
     const int lane = threadIdx.x & 31;
     for (;;)
@@ -293,67 +314,59 @@ __global__ void __launch_bounds__(256) k_sgs_levels(const int *__restrict__ nb_r
         const long long base = (long long)b * 32;
         if (base >= n_sim) break;
         const long long r = base + lane;
-        const bool live = r < n_sim;
         int L = 0;
-        unsigned intra = 0;
-        if (live)
+        if (r < n_sim)
         {
             const int n = nb_cnt[r];
             const int *row = nb_rank + r * (long long)k;
-            // eight neighbours at a time: their ranks, then every level already
-            // published, issued together; waits only for the missing ones
-            for (int i0 = 0; i0 < n; i0 += 8)
+            // sixteen neighbours at a time: their ranks, then every published level
+            // at once; waits only for the missing ones
+            for (int i0 = 0; i0 < n; i0 += 16)
             {
-                int tq[8], v[8];
+                int tq[16], v[16];
 #pragma unroll
-                for (int j = 0; j < 8; ++j) tq[j] = i0 + j < n ? row[i0 + j] : -1;
+                for (int j = 0; j < 16; ++j) tq[j] = i0 + j < n ? row[i0 + j] : -1;
 #pragma unroll
-                for (int j = 0; j < 8; ++j)
+                for (int j = 0; j < 16; ++j) v[j] = tq[j] >= 0 ? ld_relaxed_gpu(&levp1[tq[j]]) : -1;
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
                 {
-                    v[j] = -1; // no dependency (conditioning cell, or inside the batch)
-                    if (tq[j] >= base)
-                        intra |= 1u << (tq[j] - (int)base);
-                    else if (tq[j] >= 0)
-                        v[j] = ld_relaxed_gpu(&levp1[tq[j]]);
-                }
-#pragma unroll
-                for (int j = 0; j < 8; ++j)
-                {
-                    if (v[j] == 0)
-                    {
-                        const unsigned long long t0 = global_ns();
-                        while ((v[j] = ld_relaxed_gpu(&levp1[tq[j]])) == 0)
-                        {
-                            if (ld_relaxed_gpu(err) != 0 || global_ns() - t0 > kLevelWaitNs)
-                            {
-                                atomicExch(err, 1);
-                                v[j] = 1;
-                                break;
-                            }
-                            __nanosleep(64);
-                        }
-                    }
+                    if (v[j] == 0) v[j] = sgs_wait_level(levp1, tq[j], err);
                     L = max(L, v[j]); // level(dep) + 1
                 }
             }
-        }
-        // lanes in rank order: lane i's level is final once lanes < i are
-#pragma unroll 1
-        for (int i = 0; i < 32; ++i)
-        {
-            const int li = __shfl_sync(0xffffffffu, L, i);
-            if ((intra >> i) & 1u) L = max(L, li + 1);
-        }
-        if (live)
-        {
-            if (L < level_cap)
-                atomicAdd(&level_count[L], 1);
-            else
-                atomicExch(err, 2);
-            atomicMax(max_level, L);
+            if (L >= level_cap) atomicExch(err, 2);
             st_relaxed_gpu(&levp1[r], L + 1);
         }
+        __syncwarp();
+        int m = L;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (lane == 0) atomicMax(max_level, m);
     }
+}
+
+// level_count[l] = number of ranks of level l (a shared-memory histogram of the
+// first kSgsHistLevels levels, global atomics beyond)
+constexpr int kSgsHistLevels = 4096;
+__global__ void __launch_bounds__(256) k_sgs_level_count(int n_sim, const int *__restrict__ levp1, int level_cap,
+                                                         int *__restrict__ level_count)
+{
+    __shared__ int h[kSgsHistLevels];
+    for (int i = threadIdx.x; i < kSgsHistLevels; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n_sim; r += gridDim.x * blockDim.x)
+    {
+        const int l = levp1[r] - 1;
+        if (l < 0 || l >= level_cap) continue; // only after an error, which the host reports
+        if (l < kSgsHistLevels)
+            atomicAdd(&h[l], 1);
+        else
+            atomicAdd(&level_count[l], 1);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kSgsHistLevels; i += blockDim.x)
+        if (h[i]) atomicAdd(&level_count[i], h[i]);
 }
 
 // order[level_off[l] + i]: the ranks of level l (any order inside a level)
@@ -376,43 +389,6 @@ struct SgsNode
     double var;
 };
 
-// combine (combiner.h:10-25) and the variance sums in the reference's order,
-// through lane shuffles (every lane ends with the result). x: A^-1 b and
-// y: A^-1 1 of row `lane` (lanes < n).
-__device__ __forceinline__ void sgs_combine_warp(int n, bool ordinary, double x, double y, double b, float v, float m,
-                                                 float m_center, double c0, SgsNode &o)
-{
-    // OK: mu = (sum x - 1) / sum y, w = x - mu y (my_kriging_weights.h:198-361)
-    double sx = 0.0, sy = 0.0;
-    if (ordinary)
-    {
-        for (int i = 0; i < n; ++i)
-        {
-            sx = __dadd_rn(sx, __shfl_sync(0xffffffffu, x, i));
-            sy = __dadd_rn(sy, __shfl_sync(0xffffffffu, y, i));
-        }
-    }
-    const bool fail = ordinary && fabs(sy) < 1e-15;
-    const double mu = ordinary && !fail ? __ddiv_rn(__dsub_rn(sx, 1.0), sy) : 0.0;
-    const double w = ordinary ? __dsub_rn(x, __dmul_rn(mu, y)) : x;
-    double var = c0;
-    float est = m_center;
-    for (int i = 0; i < n; ++i)
-    {
-        const double wi = __shfl_sync(0xffffffffu, w, i);
-        const double bi = __shfl_sync(0xffffffffu, b, i);
-        const float vi = __shfl_sync(0xffffffffu, v, i);
-        const float mi = __shfl_sync(0xffffffffu, m, i);
-        var = __dsub_rn(var, __dmul_rn(wi, bi));
-        est = __fadd_rn(est, __double2float_rn(__dmul_rn(wi, (double)__fsub_rn(vi, mi))));
-    }
-    if (ordinary) var = __dsub_rn(var, mu);
-    if (var < 0) var = 0;
-    o.status = fail ? 2 : 0;
-    o.mean = est;
-    o.var = var;
-}
-
 struct SgsSolveArgs
 {
     Geom g;
@@ -430,121 +406,265 @@ struct SgsSolveArgs
     int ordinary;
 };
 
-constexpr int kSgsWarps = 4;
-constexpr int kSgsLD = 33;
+// n <= 32: two nodes per warp, sixteen lanes each, lane t holding rows t and
+// 31 - t of A (the folded lower triangle, as the kriging solves lay it out).
+// The right-looking factorisation broadcasts column j through shared memory
+// row j and carries the forward substitution of b (and, for ordinary kriging,
+// of the ones vector); the back substitution reads column i of L from the
+// lane's own shared rows. The weights then go through combine() one by one.
+constexpr int kSgsNP = 32, kSgsG = 16;
+constexpr int kSgsLD = kSgsNP + 2; // 32 entries, then the right-hand sides
+constexpr size_t kSgsSysBytes = ((size_t)kSgsNP * kSgsLD * 8 + kSgsNP * 4 + 127) / 128 * 128 + 16;
+constexpr int kSgsFoldThreads = 256;
 
-// n <= 32: one warp per node, lane r holds row r of A (lower triangle); the
-// second right-hand side (A^-1 1) only for ordinary kriging.
 template <bool ORD>
-__global__ void __launch_bounds__(32 * kSgsWarps) k_sgs_solve_warp(const SgsSolveArgs a)
+__global__ void __launch_bounds__(kSgsFoldThreads, 1) k_sgs_solve_fold(const SgsSolveArgs a)
 {
-    __shared__ double sm_all[kSgsWarps][32 * kSgsLD];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double *Sm = sm_all[warp];
+    constexpr int NP = kSgsNP, G = kSgsG, LD = kSgsLD, QB = ORD ? 2 : 1;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int h = lane / G, t = lane % G, rb = NP - 1 - t;
+    const unsigned gm = 0xFFFFu << (h * G);
+    unsigned char *gb = smem + kSgsSysBytes * (warp * 2 + h);
+    double *M = reinterpret_cast<double *>(gb);
+    int *LIN = reinterpret_cast<int *>(gb + (size_t)NP * LD * 8);
     const Geom &g = a.g;
     const long long pc = g.pair_center;
-    for (int it = blockIdx.x * kSgsWarps + warp; it < a.n_items; it += gridDim.x * kSgsWarps)
+    const double *pair64 = a.pair64;
+    for (int it0 = (blockIdx.x * nwarps + warp) * 2; it0 < a.n_items; it0 += gridDim.x * nwarps * 2)
     {
-        const int r = a.order[it];
-        const int cell = a.sim_cells[r];
-        const int n = a.nb_cnt[r];
+        const int it = it0 + h;
+        const bool valid = it < a.n_items;
+        int r = 0, cell = 0, n = 0;
+        if (valid)
+        {
+            r = a.order[it];
+            cell = a.sim_cells[r];
+            n = a.nb_cnt[r];
+        }
         const int cx = cell % g.nx, cy = (int)((cell / g.nx) % g.ny), cz = (int)(cell / ((long long)g.nx * g.ny));
-        const bool live = lane < n;
-        int px = 0, py = 0, pz = 0;
-        float v = 0.0f, m = 0.0f;
-        if (live)
+        const bool live_a = t < n, live_b = rb < n;
+        int lin_a = 0, lin_b = 0;
+        float va = 0.0f, vb = 0.0f, ma = 0.0f, mb = 0.0f;
+        if (live_a)
         {
-            const int q = a.nb[(long long)r * a.k + lane];
-            px = q % g.nx;
-            py = (int)((q / g.nx) % g.ny);
-            pz = (int)(q / ((long long)g.nx * g.ny));
-            v = a.data[q];
-            if (a.means) m = a.means[q];
+            const int q = a.nb[(long long)r * a.k + t];
+            lin_a = pair_lin(g, q % g.nx - cx, (int)((q / g.nx) % g.ny) - cy, (int)(q / ((long long)g.nx * g.ny)) - cz);
+            va = a.data[q];
+            if (a.means) ma = a.means[q];
         }
-        SgsNode o = {1, 0.0f, 0.0};
-        if (n > 0)
+        if (live_b)
         {
-            double row[32];
-#pragma unroll
-            for (int c = 0; c < 32; ++c)
-            {
-                const int qx = __shfl_sync(0xffffffffu, px, c), qy = __shfl_sync(0xffffffffu, py, c),
-                          qz = __shfl_sync(0xffffffffu, pz, c);
-                double e = 0.0;
-                if (live && c <= lane) e = a.pair64[pc + pair_lin(g, px - qx, py - qy, pz - qz)];
-                if (!live && c == lane) e = 1.0;
-                row[c] = e;
-            }
-            const double b = live ? a.pair64[pc + pair_lin(g, px - cx, py - cy, pz - cz)] : 0.0;
-            bool fail = false;
-            double inv = 0.0;
-#pragma unroll
-            for (int j = 0; j < 32; ++j)
-            {
-                Sm[j * kSgsLD + lane] = row[j];
-                __syncwarp();
-                const double d = Sm[j * kSgsLD + j];
-                fail |= !(d > 0.0);
-                const double is = 1.0 / sqrt(d);
-                const double s = row[j] * is * is;
-#pragma unroll
-                for (int c = j + 1; c < 32; ++c) row[c] -= s * Sm[j * kSgsLD + c];
-                row[j] *= is;
-                if (lane == j) inv = is;
-                __syncwarp();
-            }
-            // forward L y = [b, 1], back L^T x = y
-            double acc0 = b, acc1 = live ? 1.0 : 0.0, y0 = 0.0, y1 = 0.0;
-#pragma unroll
-            for (int j = 0; j < 32; ++j)
-            {
-                if (lane == j)
-                {
-                    y0 = acc0 * inv;
-                    if (ORD) y1 = acc1 * inv;
-                }
-                const double t0 = __shfl_sync(0xffffffffu, y0, j);
-                const double t1 = ORD ? __shfl_sync(0xffffffffu, y1, j) : 0.0;
-                if (lane > j)
-                {
-                    acc0 -= row[j] * t0;
-                    if (ORD) acc1 -= row[j] * t1;
-                }
-            }
-            double x0 = 0.0, x1 = 0.0;
-            acc0 = y0;
-            acc1 = y1;
-#pragma unroll
-            for (int i = 31; i >= 0; --i)
-            {
-                const double l = Sm[lane * kSgsLD + i] * inv;
-                if (lane == i)
-                {
-                    x0 = acc0 * inv;
-                    if (ORD) x1 = acc1 * inv;
-                }
-                const double t0 = __shfl_sync(0xffffffffu, x0, i);
-                const double t1 = ORD ? __shfl_sync(0xffffffffu, x1, i) : 0.0;
-                if (lane < i)
-                {
-                    acc0 -= l * t0;
-                    if (ORD) acc1 -= l * t1;
-                }
-            }
-            __syncwarp();
-            fail = __any_sync(0xffffffffu, fail && live);
-            const float mc = a.means ? a.means[cell] : 0.0f;
-            sgs_combine_warp(n, ORD, x0, x1, b, v, m, mc, a.pair64[pc], o);
-            if (fail) o.status = 2;
+            const int q = a.nb[(long long)r * a.k + rb];
+            lin_b = pair_lin(g, q % g.nx - cx, (int)((q / g.nx) % g.ny) - cy, (int)(q / ((long long)g.nx * g.ny)) - cz);
+            vb = a.data[q];
+            if (a.means) mb = a.means[q];
         }
-        if (lane == 0)
+        LIN[t] = lin_a;
+        LIN[rb] = lin_b;
+        __syncwarp(gm);
+
+        // ---- assembly (lower triangles of rows t and 31 - t; padding rows identity)
+        double ra[G], rbv[NP];
+        const double *base_a = pair64 + pc + lin_a, *base_b = pair64 + pc + lin_b;
+#pragma unroll
+        for (int c = 0; c < G; ++c)
         {
+            double e = 0.0;
+            if (live_a && c <= t) e = __ldg(base_a - LIN[c]);
+            if (!live_a && c == t) e = 1.0;
+            ra[c] = e;
+        }
+#pragma unroll
+        for (int c = 0; c < NP; ++c)
+        {
+            double e = 0.0;
+            if (live_b && c <= rb) e = __ldg(base_b - LIN[c]);
+            if (!live_b && c == rb) e = 1.0;
+            rbv[c] = e;
+        }
+        const double b_a = live_a ? __ldg(base_a) : 0.0;
+        const double b_b = live_b ? __ldg(base_b) : 0.0;
+
+        // ---- factorisation with the forward substitution of b (and 1)
+        double rhs_a[QB], rhs_b[QB], ya[QB], yb[QB];
+        rhs_a[0] = b_a;
+        rhs_b[0] = b_b;
+        if constexpr (ORD)
+        {
+            rhs_a[1] = live_a ? 1.0 : 0.0;
+            rhs_b[1] = live_b ? 1.0 : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < QB; ++q)
+        {
+            ya[q] = 0.0;
+            yb[q] = 0.0;
+        }
+        bool fail = false;
+        double inv_a = 0.0, inv_b = 0.0;
+#pragma unroll
+        for (int j = 0; j < NP; ++j)
+        {
+            if (j < G)
+            {
+                M[j * LD + t] = ra[j];
+                if (t == j)
+                {
+#pragma unroll
+                    for (int q = 0; q < QB; ++q) M[j * LD + NP + q] = rhs_a[q];
+                }
+            }
+            M[j * LD + rb] = rbv[j];
+            if (j >= G && rb == j)
+            {
+#pragma unroll
+                for (int q = 0; q < QB; ++q) M[j * LD + NP + q] = rhs_b[q];
+            }
+            __syncwarp(gm);
+            double mj[LD];
+            const double2 *mv = reinterpret_cast<const double2 *>(M + j * LD);
+#pragma unroll
+            for (int q = j / 2; q < LD / 2; ++q)
+            {
+                const double2 v2 = mv[q];
+                mj[2 * q] = v2.x;
+                mj[2 * q + 1] = v2.y;
+            }
+            const double d = mj[j];
+            fail |= !(d > 0.0);
+            const double inv_s = rsqrt(d);
+            const double inv2 = inv_s * inv_s;
+            if (j < G)
+            {
+                const double sc = ra[j] * inv2;
+#pragma unroll
+                for (int c = j + 1; c < G; ++c) ra[c] -= sc * mj[c];
+                if (t > j)
+                {
+#pragma unroll
+                    for (int q = 0; q < QB; ++q) rhs_a[q] -= sc * mj[NP + q];
+                }
+                ra[j] *= inv_s;
+                if (t == j)
+                {
+                    inv_a = inv_s;
+#pragma unroll
+                    for (int q = 0; q < QB; ++q) ya[q] = rhs_a[q] * inv_s;
+                }
+            }
+            {
+                const double sc = rbv[j] * inv2;
+#pragma unroll
+                for (int c = j + 1; c < NP; ++c) rbv[c] -= sc * mj[c];
+                if (rb > j)
+                {
+#pragma unroll
+                    for (int q = 0; q < QB; ++q) rhs_b[q] -= sc * mj[NP + q];
+                }
+                rbv[j] *= inv_s;
+                if (rb == j)
+                {
+                    inv_b = inv_s;
+#pragma unroll
+                    for (int q = 0; q < QB; ++q) yb[q] = rhs_b[q] * inv_s;
+                }
+            }
+        }
+
+        // ---- back substitution L^T x = y; L[i][row] = M[row][i] / sqrt(d_row)
+        double xa[QB], xb[QB];
+#pragma unroll
+        for (int q = 0; q < QB; ++q)
+        {
+            xa[q] = 0.0;
+            xb[q] = 0.0;
+        }
+#pragma unroll
+        for (int i = NP - 1; i >= 0; --i)
+        {
+            double xi[QB];
+            if (i >= G)
+            {
+                if (rb == i)
+                {
+#pragma unroll
+                    for (int q = 0; q < QB; ++q) xb[q] = yb[q] * inv_b;
+                }
+#pragma unroll
+                for (int q = 0; q < QB; ++q) xi[q] = __shfl_sync(gm, xb[q], NP - 1 - i, G);
+            }
+            else
+            {
+                if (t == i)
+                {
+#pragma unroll
+                    for (int q = 0; q < QB; ++q) xa[q] = ya[q] * inv_a;
+                }
+#pragma unroll
+                for (int q = 0; q < QB; ++q) xi[q] = __shfl_sync(gm, xa[q], i, G);
+            }
+            if (t < i)
+            {
+                const double l = M[t * LD + i] * inv_a;
+#pragma unroll
+                for (int q = 0; q < QB; ++q) ya[q] -= l * xi[q];
+            }
+            if (rb < i)
+            {
+                const double l = M[rb * LD + i] * inv_b;
+#pragma unroll
+                for (int q = 0; q < QB; ++q) yb[q] -= l * xi[q];
+            }
+        }
+
+        // ---- combine() and the variance in the reference's order
+        double sx = 0.0, sy = 0.0;
+        if constexpr (ORD)
+        {
+#pragma unroll
+            for (int i = 0; i < NP; ++i)
+            {
+                const double x0 = __shfl_sync(gm, i < G ? xa[0] : xb[0], i < G ? i : NP - 1 - i, G);
+                const double x1 = __shfl_sync(gm, i < G ? xa[1] : xb[1], i < G ? i : NP - 1 - i, G);
+                if (i < n)
+                {
+                    sx = __dadd_rn(sx, x0);
+                    sy = __dadd_rn(sy, x1);
+                }
+            }
+        }
+        const bool bad_ok = ORD && fabs(sy) < 1e-15;
+        const double mu = ORD && !bad_ok ? __ddiv_rn(__dsub_rn(sx, 1.0), sy) : 0.0;
+        double var = pair64[pc];
+        float est = a.means && valid ? a.means[cell] : 0.0f;
+#pragma unroll
+        for (int i = 0; i < NP; ++i)
+        {
+            const int src = i < G ? i : NP - 1 - i;
+            const double x0 = __shfl_sync(gm, i < G ? xa[0] : xb[0], src, G);
+            const double x1 = ORD ? __shfl_sync(gm, i < G ? xa[QB - 1] : xb[QB - 1], src, G) : 0.0;
+            const double bi = __shfl_sync(gm, i < G ? b_a : b_b, src, G);
+            const float vi = __shfl_sync(gm, i < G ? va : vb, src, G);
+            const float mi = __shfl_sync(gm, i < G ? ma : mb, src, G);
+            if (i < n)
+            {
+                const double w = ORD ? __dsub_rn(x0, __dmul_rn(mu, x1)) : x0;
+                var = __dsub_rn(var, __dmul_rn(w, bi));
+                est = __fadd_rn(est, __double2float_rn(__dmul_rn(w, (double)__fsub_rn(vi, mi))));
+            }
+        }
+        if (ORD) var = __dsub_rn(var, mu);
+        if (var < 0) var = 0;
+        if (valid && t == 0)
+        {
+            const int status = n == 0 ? 1 : ((fail || bad_ok) ? 2 : 0);
             const double u = a.uniforms[r];
-            const double val =
-                o.status == 0 ? sgs_gauss_inverse(u, (double)o.mean, o.var) : sgs_gauss_inverse(u, 0.0, 1.0);
+            const double val = status == 0 ? sgs_gauss_inverse(u, (double)est, var) : sgs_gauss_inverse(u, 0.0, 1.0);
             a.data[cell] = __double2float_rn(val);
-            a.st_rank[r] = (signed char)o.status;
+            a.st_rank[r] = (signed char)status;
         }
+        __syncwarp(gm);
     }
 }
 
@@ -694,8 +814,8 @@ void launch_sgs_search(const Geom &g, const int4 *tmpl, int n_tmpl, const int *s
 void launch_sgs_levels(const int *nb_rank, const int *nb_cnt, int k, int n_sim, int *levp1, int *ticket,
                        int *level_count, int level_cap, int *max_level, int *err, int n_sm, cudaStream_t st)
 {
-    k_sgs_levels<<<n_sm * 8, 256, 0, st>>>(nb_rank, nb_cnt, k, n_sim, levp1, ticket, level_count, level_cap,
-                                           max_level, err);
+    k_sgs_levels<<<n_sm * 8, 256, 0, st>>>(nb_rank, nb_cnt, k, n_sim, levp1, ticket, level_cap, max_level, err);
+    k_sgs_level_count<<<n_sm * 2, 256, 0, st>>>(n_sim, levp1, level_cap, level_count);
 }
 void launch_sgs_level_fill(int n_sim, const int *levp1, const int *level_off, int *level_fill, int *order,
                            cudaStream_t st)
@@ -713,11 +833,12 @@ cudaError_t launch_sgs_solve(const Geom &g, const int *order, int n_items, const
                    ordinary ? 1 : 0};
     if (k <= 32)
     {
-        const int blocks = std::min((n_items + kSgsWarps - 1) / kSgsWarps, n_sm * 16);
-        if (ordinary)
-            k_sgs_solve_warp<true><<<blocks, 32 * kSgsWarps, 0, st>>>(a);
-        else
-            k_sgs_solve_warp<false><<<blocks, 32 * kSgsWarps, 0, st>>>(a);
+        const size_t smem = kSgsSysBytes * (kSgsFoldThreads / kSgsG);
+        const int blocks = std::min((n_items + kSgsFoldThreads / kSgsG - 1) / (kSgsFoldThreads / kSgsG), n_sm);
+        auto kern = ordinary ? k_sgs_solve_fold<true> : k_sgs_solve_fold<false>;
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        kern<<<blocks, kSgsFoldThreads, smem, st>>>(a);
     }
     else
     {
