@@ -486,6 +486,7 @@ int hpgl_b200_last_stats(double *out, int cap)
     v[38] = s.plan_ms;
     v[39] = (double)s.sgs_levels;
     v[40] = s.draws_ms;
+    v[41] = s.sgs_flops;
     int n = cap < HPGL_B200_STATS_LEN ? cap : HPGL_B200_STATS_LEN;
     for (int i = 0; i < n; ++i) out[i] = v[i];
     return n;

@@ -251,7 +251,7 @@ static long long check_dims(const int *dims)
 }
 
 static Plan make_plan(bool truncated, int cov_type, const double *ranges, const double *angles, double sill,
-                      double nugget, const int *radiuses, int k, const int *dims)
+                      double nugget, const int *radiuses, int k, const int *dims, bool surrogate = true)
 {
     check_model_args(cov_type, ranges, angles, sill, nugget, radiuses, k);
     Plan pl;
@@ -261,7 +261,7 @@ static Plan make_plan(bool truncated, int cov_type, const double *ranges, const 
     for (int a = 0; a < 3; ++a) pl.f.r[a] = radiuses[a];
     build_key_table(pl.f, pl.kt, g_threads);
     pl.tmpl_count = template_size(pl.f, pl.kt);
-    if (k <= 64 && pl.kt.n_ranks <= 0xFFFE) build_surrogate(pl.f, pl.kt, pl.sg);
+    if (surrogate && k <= 64 && pl.kt.n_ranks <= 0xFFFE) build_surrogate(pl.f, pl.kt, pl.sg);
     pl.rank_bits = pl.kt.n_ranks > 1 ? bits_for(pl.kt.n_ranks - 1) : 0;
 
     Geom &g = pl.g;
@@ -1018,7 +1018,9 @@ int sgs_simulation(const int *dims, float *data, unsigned char *mask, const unsi
         double plan_ms = 0.0;
         auto plan_f = std::async(std::launch::async, [&]() {
             const auto t0 = std::chrono::steady_clock::now();
-            Plan p = make_plan(true, a.cov_type, a.ranges, a.angles, a.sill, a.nugget, a.radiuses, a.max_nb, dims);
+            // the simulation's search is the template scan alone: no float prefilter tables
+            Plan p = make_plan(true, a.cov_type, a.ranges, a.angles, a.sill, a.nugget, a.radiuses, a.max_nb, dims,
+                               false);
             std::vector<Offset> tv = build_template(p.f, p.kt);
             plan_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
             return std::make_pair(std::move(p), std::move(tv));
@@ -1067,6 +1069,7 @@ int sgs_simulation(const int *dims, float *data, unsigned char *mask, const unsi
             exclusive_scan(scan, n, tmp, total, st);
             launch_sgs_index(n, path_cell, flag, scan, d_mask, rank_of, sim_cells, st);
             HB_CK(cudaGetLastError());
+            E.stats.launches += 2 + scan_kernels(n);
             HB_CK(cudaMemcpyAsync(&n_sim, total, sizeof(int), cudaMemcpyDeviceToHost, st));
             HB_CK(cudaStreamSynchronize(st));
         }
@@ -1121,6 +1124,7 @@ int sgs_simulation(const int *dims, float *data, unsigned char *mask, const unsi
         double *pair64 = E.buf<double>("pair64", (size_t)pn);
         float *pair32 = E.buf<float>("pair32", (size_t)pn);
         launch_build_pair(g, dev_model(pl.f.m), 1, search_vals, pair64, pair32, st);
+        E.stats.launches += 1 + ((use_cdf || lvm) ? 1 : 0) + (n_sim > 0 ? 4 : 0); // + search, moments, levels x2
         std::vector<int4> t4(tv.size());
         for (size_t i = 0; i < tv.size(); ++i) t4[i] = make_int4(tv[i].dx, tv[i].dy, tv[i].dz, 0);
         int4 *tmpl = E.buf<int4>("sgs_tmpl", std::max<size_t>(t4.size(), 1));
@@ -1149,6 +1153,9 @@ int sgs_simulation(const int *dims, float *data, unsigned char *mask, const unsi
         int *levp1 = E.buf<int>("sgs_levp1", (size_t)std::max(n_sim, 1));
         int *lvl_count = E.buf<int>("sgs_lvl_count", (size_t)level_cap + 1);
         int *scal = E.buf<int>("sgs_scal", 4); // ticket, max level, error
+        double *mom = E.buf<double>("sgs_mom", 3);
+        HB_CK(cudaMemsetAsync(mom, 0, 24, st));
+        if (n_sim > 0) launch_sgs_moments(n_sim, nb_cnt, mom, E.n_sm(), st);
         HB_CK(cudaMemsetAsync(levp1, 0, (size_t)std::max(n_sim, 1) * 4, st));
         HB_CK(cudaMemsetAsync(lvl_count, 0, ((size_t)level_cap + 1) * 4, st));
         HB_CK(cudaMemsetAsync(scal, 0, 16, st));
@@ -1157,8 +1164,16 @@ int sgs_simulation(const int *dims, float *data, unsigned char *mask, const unsi
                               E.n_sm(), st);
         HB_CK(cudaGetLastError());
         int hs[4] = {0, 0, 0, 0};
+        double hmom[3] = {0, 0, 0};
         HB_CK(cudaMemcpyAsync(hs, scal, 16, cudaMemcpyDeviceToHost, st));
+        HB_CK(cudaMemcpyAsync(hmom, mom, 24, cudaMemcpyDeviceToHost, st));
         HB_CK(cudaStreamSynchronize(st));
+        {
+            // F(n, r) = n^3/3 + n^2/2 + 2 r n^2 + 30 (n(n+1)/2 + n) + 2 r n, r = 1 (SK) or 2 (OK):
+            // the kriging buckets' count, its triangular solves being here a forward and a back pass
+            const double rhs = ordinary ? 2.0 : 1.0;
+            E.stats.sgs_flops = hmom[2] / 3.0 + hmom[1] * (0.5 + 2.0 * rhs + 15.0) + hmom[0] * (45.0 + 2.0 * rhs);
+        }
         if (hs[2] == 1) throw CudaFail{-2, "simulation level pass: a dependency wait timed out"};
         if (hs[2] == 2) throw CudaFail{-4, "simulation needs more than 2^20 dependency levels"};
         const int n_levels = n_sim > 0 ? hs[1] + 1 : 0;
@@ -1178,6 +1193,7 @@ int sgs_simulation(const int *dims, float *data, unsigned char *mask, const unsi
             HB_CK(cudaMemsetAsync(level_fill, 0, ((size_t)n_levels + 1) * 4, st));
             launch_sgs_level_fill(n_sim, levp1, level_off, level_fill, order, st);
             HB_CK(cudaGetLastError());
+            E.stats.launches += 1;
         }
         E.stats.sgs_levels = n_levels;
         E.mark(STAGE_TIES, st);
@@ -1205,6 +1221,7 @@ int sgs_simulation(const int *dims, float *data, unsigned char *mask, const unsi
         launch_sgs_finalize(n, d_data, d_mask, rank_of, n_sim, st_rank, d_status, use_cdf ? d_cv : nullptr, d_cp,
                             use_cdf ? cdf->size : 0, st);
         HB_CK(cudaGetLastError());
+        E.stats.launches += 1;
         E.mark(STAGE_FINALIZE, st);
         if (!io.device)
         {

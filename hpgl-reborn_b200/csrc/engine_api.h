@@ -91,6 +91,7 @@ struct Stats
     double plan_ms = 0;        // host time building the covariance tables (overlapped with upload/compaction)
     int sgs_levels = 0;        // SGS: dependency levels (solve launches)
     double draws_ms = 0;       // SGS: host ms generating the uniform draws (overlapped with the search)
+    double sgs_flops = 0;      // SGS: algorithmic flops of the kriging solves (same count as the kriging buckets)
 };
 
 void set_error(const std::string &msg);

@@ -34,6 +34,7 @@ struct SolveOut
 // scan / points / bins (search.cu)
 long long scan_tmp_ints(long long n);
 void exclusive_scan(int *v, long long n, int *tmp, int *total, cudaStream_t st);
+int scan_kernels(long long n); // kernels one exclusive_scan of n ints launches
 void launch_flag_informed(const uint8_t *mask, long long n, int *flag, cudaStream_t st);
 // `mean_f` (LVM) centres each continuous value on its own cell's mean, in float
 void launch_emit_points(const uint8_t *mask, const int *pos, const Geom &g, const float *val_f,
@@ -145,6 +146,7 @@ void launch_sgs_search(const Geom &g, const int4 *tmpl, int n_tmpl, const int *s
                        const int *rank_of, int k, int *nb, int *nb_rank, int *nb_cnt, int n_sm, cudaStream_t st);
 void launch_sgs_levels(const int *nb_rank, const int *nb_cnt, int k, int n_sim, int *levp1, int *ticket,
                        int *level_count, int level_cap, int *max_level, int *err, int n_sm, cudaStream_t st);
+void launch_sgs_moments(int n_sim, const int *nb_cnt, double *mom, int n_sm, cudaStream_t st); // mom: 3, zeroed
 void launch_sgs_level_fill(int n_sim, const int *levp1, const int *level_off, int *level_fill, int *order,
                            cudaStream_t st);
 size_t sgs_block_smem(int k);

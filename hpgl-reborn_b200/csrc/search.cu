@@ -95,6 +95,14 @@ long long scan_tmp_ints(long long n)
     return need;
 }
 
+int scan_kernels(long long n)
+{
+    const long long tiles = (n + kScanTile - 1) / kScanTile;
+    if (tiles <= 0) return 0;
+    if (tiles == 1) return 1;
+    return 2 + scan_kernels(tiles);
+}
+
 void exclusive_scan(int *v, long long n, int *tmp, int *total, cudaStream_t st)
 {
     long long tiles = (n + kScanTile - 1) / kScanTile;

@@ -369,6 +369,32 @@ __global__ void __launch_bounds__(256) k_sgs_level_count(int n_sim, const int *_
         if (h[i]) atomicAdd(&level_count[i], h[i]);
 }
 
+// sums of n, n^2, n^3 over the neighbour counts (the solve's algorithmic flops)
+__global__ void __launch_bounds__(256) k_sgs_moments(int n_sim, const int *__restrict__ nb_cnt, double *__restrict__ mom)
+{
+    double s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n_sim; r += gridDim.x * blockDim.x)
+    {
+        const double n = (double)nb_cnt[r];
+        s1 += n;
+        s2 += n * n;
+        s3 += n * n * n;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+        s3 += __shfl_xor_sync(0xffffffffu, s3, o);
+    }
+    if ((threadIdx.x & 31) == 0)
+    {
+        atomicAdd(&mom[0], s1);
+        atomicAdd(&mom[1], s2);
+        atomicAdd(&mom[2], s3);
+    }
+}
+
 // order[level_off[l] + i]: the ranks of level l (any order inside a level)
 __global__ void k_sgs_level_fill(int n_sim, const int *__restrict__ levp1, const int *__restrict__ level_off,
                                  int *__restrict__ level_fill, int *__restrict__ order)
@@ -636,22 +662,25 @@ __global__ void __launch_bounds__(kSgsFoldThreads, 1) k_sgs_solve_fold(const Sgs
         }
         const bool bad_ok = ORD && fabs(sy) < 1e-15;
         const double mu = ORD && !bad_ok ? __ddiv_rn(__dsub_rn(sx, 1.0), sy) : 0.0;
+        // each lane forms its rows' terms; the sums run in row order
+        const double w_a = ORD ? __dsub_rn(xa[0], __dmul_rn(mu, xa[QB - 1])) : xa[0];
+        const double w_b = ORD ? __dsub_rn(xb[0], __dmul_rn(mu, xb[QB - 1])) : xb[0];
+        const double vt_a = __dmul_rn(w_a, b_a), vt_b = __dmul_rn(w_b, b_b);
+        const float et_a = __double2float_rn(__dmul_rn(w_a, (double)__fsub_rn(va, ma)));
+        const float et_b = __double2float_rn(__dmul_rn(w_b, (double)__fsub_rn(vb, mb)));
         double var = pair64[pc];
         float est = a.means && valid ? a.means[cell] : 0.0f;
-#pragma unroll
+#pragma unroll 4
         for (int i = 0; i < NP; ++i)
         {
-            const int src = i < G ? i : NP - 1 - i;
-            const double x0 = __shfl_sync(gm, i < G ? xa[0] : xb[0], src, G);
-            const double x1 = ORD ? __shfl_sync(gm, i < G ? xa[QB - 1] : xb[QB - 1], src, G) : 0.0;
-            const double bi = __shfl_sync(gm, i < G ? b_a : b_b, src, G);
-            const float vi = __shfl_sync(gm, i < G ? va : vb, src, G);
-            const float mi = __shfl_sync(gm, i < G ? ma : mb, src, G);
+            const bool lo = i < G;
+            const int src = lo ? i : NP - 1 - i;
+            const double vt = __shfl_sync(gm, lo ? vt_a : vt_b, src, G);
+            const float et = __shfl_sync(gm, lo ? et_a : et_b, src, G);
             if (i < n)
             {
-                const double w = ORD ? __dsub_rn(x0, __dmul_rn(mu, x1)) : x0;
-                var = __dsub_rn(var, __dmul_rn(w, bi));
-                est = __fadd_rn(est, __double2float_rn(__dmul_rn(w, (double)__fsub_rn(vi, mi))));
+                var = __dsub_rn(var, vt);
+                est = __fadd_rn(est, et);
             }
         }
         if (ORD) var = __dsub_rn(var, mu);
@@ -816,6 +845,10 @@ void launch_sgs_levels(const int *nb_rank, const int *nb_cnt, int k, int n_sim, 
 {
     k_sgs_levels<<<n_sm * 8, 256, 0, st>>>(nb_rank, nb_cnt, k, n_sim, levp1, ticket, level_cap, max_level, err);
     k_sgs_level_count<<<n_sm * 2, 256, 0, st>>>(n_sim, levp1, level_cap, level_count);
+}
+void launch_sgs_moments(int n_sim, const int *nb_cnt, double *mom, int n_sm, cudaStream_t st)
+{
+    k_sgs_moments<<<n_sm * 2, 256, 0, st>>>(n_sim, nb_cnt, mom);
 }
 void launch_sgs_level_fill(int n_sim, const int *levp1, const int *level_off, int *level_fill, int *order,
                            cudaStream_t st)

@@ -232,7 +232,8 @@ STATS_KEYS = (["total_ms", "search_ms", "solve_ms", "tie_cells", "template_cells
               + [f"bucket_flops_{i}" for i in range(5)]
               + ["stage_" + s + "_ms" for s in ("upload", "compact", "tables", "bins", "search", "ties", "prepare",
                                               "solve", "finalize", "download")]
-              + ["prefilter_exact_cells", "prefilter_active", "plan_ms", "sgs_levels", "sgs_draws_ms"])
+              + ["prefilter_exact_cells", "prefilter_active", "plan_ms", "sgs_levels", "sgs_draws_ms",
+                 "sgs_flops"])
 
 
 def last_stats() -> dict:

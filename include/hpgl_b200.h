@@ -222,8 +222,9 @@ int hpgl_b200_find_neighbours(int kind, const int *dims, const unsigned char *ma
  *   [37] 1 when the float distance prefilter was active in the last search
  *   [38] host ms building the covariance tables (overlapped with the upload)
  *   [39] simulation: dependency levels (one solve launch each)
- *   [40] simulation: host ms generating the uniform draws (overlapped) */
-#define HPGL_B200_STATS_LEN 41
+ *   [40] simulation: host ms generating the uniform draws (overlapped)
+ *   [41] simulation: algorithmic flops of its kriging solves */
+#define HPGL_B200_STATS_LEN 42
 int hpgl_b200_last_stats(double *out, int cap);
 
 /* No counterpart in the reference. The same SK weights as

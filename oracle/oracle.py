@@ -289,6 +289,49 @@ def sgs(dims, data, mask, cov, radiuses, k, seed, kind=1, sim_mask=None, cdf=Non
     return data, mask, st
 
 
+class _Shape(C.Structure):
+    _fields_ = [("data", C.c_int * 3), ("strides", C.c_int * 3)]
+
+
+class _Cont(C.Structure):
+    _fields_ = [("data", _f), ("mask", _u8), ("shape", _Shape)]
+
+
+class _SgsP(C.Structure):
+    _fields_ = [("t", C.c_int), ("r", C.c_double * 3), ("a", C.c_double * 3), ("sill", C.c_double),
+                ("nugget", C.c_double), ("rad", C.c_int * 3), ("k", C.c_int), ("kind", C.c_int), ("seed", C.c_long),
+                ("kmin", C.c_int)]
+
+
+def ref_api():
+    """The reference library itself (oracle/_ref/libhpgl.so), its output and
+    progress handlers silenced."""
+    if "api" in _libs:
+        return _libs["api"]
+    lib = C.CDLL(REF_API_PATH)
+    sink = C.CFUNCTYPE(C.c_int, C.c_char_p, C.c_void_p)(lambda s, p: 0)
+    psink = C.CFUNCTYPE(C.c_int, C.c_char_p, C.c_int, C.c_void_p)(lambda s, q, p: 0)
+    lib.hpgl_set_output_handler(sink, None)
+    lib.hpgl_set_progress_handler(psink, None)
+    lib._keep = (sink, psink)
+    _libs["api"] = lib
+    return lib
+
+
+def ref_sgs(dims, data, mask, cov, radiuses, k, seed, kind=1):
+    """The reference's hpgl_sgs_simulation on copies of data/mask (no CDF, no
+    simulation mask); `cov` holds the sill and nugget the driver receives."""
+    lib = ref_api()
+    od = _arr(data, np.float32).copy()
+    om = _arr(mask, np.uint8).copy()
+    sh = _Shape((C.c_int * 3)(*dims), (C.c_int * 3)(1, dims[0], dims[0] * dims[1]))
+    a = _Cont(od.ctypes.data_as(_f), om.ctypes.data_as(_u8), sh)
+    p = _SgsP(int(cov.cov_type), (C.c_double * 3)(*cov.ranges), (C.c_double * 3)(*cov.angles), float(cov.sill),
+              float(cov.nugget), (C.c_int * 3)(*radiuses), int(k), int(kind), int(seed), 0)
+    lib.hpgl_sgs_simulation(C.byref(a), C.byref(p), None, None, None)
+    return od, om
+
+
 def mt_draws(seed, n):
     """std::mt19937 + uniform_real_distribution<double>(0, 1) draws (the standard library)."""
     lib = load("port")
