@@ -457,35 +457,53 @@ __global__ void __launch_bounds__(kSgsFoldThreads, 1) k_sgs_solve_fold(const Sgs
     const Geom &g = a.g;
     const long long pc = g.pair_center;
     const double *pair64 = a.pair64;
-    for (int it0 = (blockIdx.x * nwarps + warp) * 2; it0 < a.n_items; it0 += gridDim.x * nwarps * 2)
+    // The next item's chain of dependent loads (rank, cell and count; its
+    // neighbours; their values) is issued in three stages during the current
+    // item's solve. Its neighbours belong to lower levels, already final.
+    const int stride = gridDim.x * nwarps * 2;
+    int nr = 0, ncell = 0, nn = 0, nqa = 0, nqb = 0;
+    float nva = 0.0f, nvb = 0.0f, nma = 0.0f, nmb = 0.0f;
+    auto stage_a = [&](int itx) {
+        nr = 0;
+        ncell = 0;
+        nn = 0;
+        if (itx < a.n_items)
+        {
+            nr = a.order[itx];
+            ncell = a.sim_cells[nr];
+            nn = a.nb_cnt[nr];
+        }
+    };
+    auto stage_b = [&]() {
+        nqa = t < nn ? a.nb[(long long)nr * a.k + t] : 0;
+        nqb = rb < nn ? a.nb[(long long)nr * a.k + rb] : 0;
+    };
+    auto stage_c = [&]() {
+        nva = t < nn ? a.data[nqa] : 0.0f;
+        nvb = rb < nn ? a.data[nqb] : 0.0f;
+        nma = (a.means && t < nn) ? a.means[nqa] : 0.0f;
+        nmb = (a.means && rb < nn) ? a.means[nqb] : 0.0f;
+    };
+    const int first = (blockIdx.x * nwarps + warp) * 2;
+    stage_a(first + h);
+    stage_b();
+    stage_c();
+    for (int it0 = first; it0 < a.n_items; it0 += stride)
     {
         const int it = it0 + h;
         const bool valid = it < a.n_items;
-        int r = 0, cell = 0, n = 0;
-        if (valid)
-        {
-            r = a.order[it];
-            cell = a.sim_cells[r];
-            n = a.nb_cnt[r];
-        }
+        const int r = nr, cell = ncell, n = nn, qa = nqa, qb = nqb;
+        const float va = nva, vb = nvb, ma = nma, mb = nmb;
+        stage_a(it + stride);
         const int cx = cell % g.nx, cy = (int)((cell / g.nx) % g.ny), cz = (int)(cell / ((long long)g.nx * g.ny));
         const bool live_a = t < n, live_b = rb < n;
         int lin_a = 0, lin_b = 0;
-        float va = 0.0f, vb = 0.0f, ma = 0.0f, mb = 0.0f;
         if (live_a)
-        {
-            const int q = a.nb[(long long)r * a.k + t];
-            lin_a = pair_lin(g, q % g.nx - cx, (int)((q / g.nx) % g.ny) - cy, (int)(q / ((long long)g.nx * g.ny)) - cz);
-            va = a.data[q];
-            if (a.means) ma = a.means[q];
-        }
+            lin_a = pair_lin(g, qa % g.nx - cx, (int)((qa / g.nx) % g.ny) - cy,
+                             (int)(qa / ((long long)g.nx * g.ny)) - cz);
         if (live_b)
-        {
-            const int q = a.nb[(long long)r * a.k + rb];
-            lin_b = pair_lin(g, q % g.nx - cx, (int)((q / g.nx) % g.ny) - cy, (int)(q / ((long long)g.nx * g.ny)) - cz);
-            vb = a.data[q];
-            if (a.means) mb = a.means[q];
-        }
+            lin_b = pair_lin(g, qb % g.nx - cx, (int)((qb / g.nx) % g.ny) - cy,
+                             (int)(qb / ((long long)g.nx * g.ny)) - cz);
         LIN[t] = lin_a;
         LIN[rb] = lin_b;
         __syncwarp(gm);
@@ -511,6 +529,7 @@ __global__ void __launch_bounds__(kSgsFoldThreads, 1) k_sgs_solve_fold(const Sgs
         }
         const double b_a = live_a ? __ldg(base_a) : 0.0;
         const double b_b = live_b ? __ldg(base_b) : 0.0;
+        stage_b();
 
         // ---- factorisation with the forward substitution of b (and 1)
         double rhs_a[QB], rhs_b[QB], ya[QB], yb[QB];
@@ -597,6 +616,8 @@ __global__ void __launch_bounds__(kSgsFoldThreads, 1) k_sgs_solve_fold(const Sgs
                 }
             }
         }
+
+        stage_c();
 
         // ---- back substitution L^T x = y; L[i][row] = M[row][i] / sqrt(d_row)
         double xa[QB], xb[QB];
