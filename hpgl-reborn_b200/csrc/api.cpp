@@ -137,6 +137,80 @@ hb::SgsArgs sgs_args_from(const hpgl_sgs_params_t *p)
     return a;
 }
 
+hb::CovArgs cov_args_from(const hpgl_cov_params_t *p)
+{
+    hb::CovArgs c{};
+    c.cov_type = p->m_covariance_type;
+    for (int i = 0; i < 3; ++i)
+    {
+        c.ranges[i] = p->m_ranges[i];
+        c.angles[i] = p->m_angles[i];
+    }
+    c.sill = p->m_sill;
+    c.nugget = p->m_nugget;
+    return c;
+}
+
+bool cok_args_from(int mark, const hpgl_cokriging_m1_params_t *m1, const hpgl_cokriging_m2_params_t *m2,
+                   hb::CokArgs &a)
+{
+    a = hb::CokArgs{};
+    a.mark = mark;
+    if (mark == 1 && m1)
+    {
+        a.primary.cov_type = m1->m_covariance_type;
+        for (int i = 0; i < 3; ++i)
+        {
+            a.primary.ranges[i] = m1->m_ranges[i];
+            a.primary.angles[i] = m1->m_angles[i];
+            a.radiuses[i] = m1->m_radiuses[i];
+        }
+        a.primary.sill = m1->m_sill;
+        a.primary.nugget = m1->m_nugget;
+        a.secondary = a.primary;
+        a.max_nb = m1->m_max_neighbours;
+        a.primary_mean = m1->m_primary_mean;
+        a.secondary_mean = m1->m_secondary_mean;
+        a.secondary_variance = m1->m_secondary_variance;
+        a.corr = m1->m_correlation_coef;
+        return true;
+    }
+    if (mark == 2 && m2)
+    {
+        a.primary = cov_args_from(&m2->m_primary_cov_params);
+        a.secondary = cov_args_from(&m2->m_secondary_cov_params);
+        for (int i = 0; i < 3; ++i) a.radiuses[i] = m2->m_radiuses[i];
+        a.max_nb = m2->m_max_neighbours;
+        a.primary_mean = m2->m_primary_mean;
+        a.secondary_mean = m2->m_secondary_mean;
+        a.corr = m2->m_correlation_coef;
+        return true;
+    }
+    return false;
+}
+
+// the size checks of api.cpp:690-706
+bool cok_shapes(const char *fn, const hpgl_shape_t *a, const hpgl_shape_t *b, const hpgl_shape_t *c, int *dims)
+{
+    int d2[3], d3[3];
+    if (!shape_dims(a, dims) || !shape_dims(b, d2) || !shape_dims(c, d3)) return false;
+    const long long s1 = (long long)dims[0] * dims[1] * dims[2], s2 = (long long)d2[0] * d2[1] * d2[2],
+                    s3 = (long long)d3[0] * d3[1] * d3[2];
+    if (s1 != s2)
+    {
+        hb::set_error(std::string(fn) + ": Size of secondary data (" + std::to_string(s2) +
+                      ") is different from size of primary data (" + std::to_string(s1) + ")");
+        return false;
+    }
+    if (s1 != s3)
+    {
+        hb::set_error(std::string(fn) + ": Size of output data (" + std::to_string(s3) +
+                      ") is different from size of primary data (" + std::to_string(s1) + ")");
+        return false;
+    }
+    return true;
+}
+
 hb::Options options_from(const hpgl_b200_options_t *o)
 {
     hb::Options r;
@@ -289,6 +363,48 @@ void hpgl_sgs_lvm_simulation(hpgl_cont_masked_array_t *data, hpgl_sgs_params_t *
         report_done("Sequential Gaussian Simulation with Local Varying Mean");
 }
 
+void hpgl_simple_cokriging_mark1(hpgl_cont_masked_array_t *input_data, hpgl_cont_masked_array_t *secondary_data,
+                                 hpgl_cokriging_m1_params_t *params, hpgl_cont_masked_array_t *output_data)
+{
+    if (!input_data || !secondary_data || !params || !output_data)
+    {
+        hb::set_error("hpgl_simple_cokriging_mark1: null argument");
+        return;
+    }
+    int dims[3];
+    if (!cok_shapes("hpgl_simple_cokriging_mark1", &input_data->m_shape, &secondary_data->m_shape,
+                    &output_data->m_shape, dims))
+        return;
+    hb::CokArgs a;
+    cok_args_from(1, params, nullptr, a);
+    hb::Options opt;
+    progress("Simple Colocated Cokriging Markov Model I", 0);
+    if (hb::cokriging(dims, input_data->m_data, input_data->m_mask, secondary_data->m_data, secondary_data->m_mask,
+                      a, output_data->m_data, output_data->m_mask, opt) == 0)
+        report_done("Simple Colocated Cokriging Markov Model I");
+}
+
+void hpgl_simple_cokriging_mark2(hpgl_cont_masked_array_t *primary_data, hpgl_cont_masked_array_t *secondary_data,
+                                 hpgl_cokriging_m2_params_t *params, hpgl_cont_masked_array_t *output_data)
+{
+    if (!primary_data || !secondary_data || !params || !output_data)
+    {
+        hb::set_error("hpgl_simple_cokriging_mark2: null argument");
+        return;
+    }
+    int dims[3];
+    if (!cok_shapes("hpgl_simple_cokriging_mark2", &primary_data->m_shape, &secondary_data->m_shape,
+                    &output_data->m_shape, dims))
+        return;
+    hb::CokArgs a;
+    cok_args_from(2, nullptr, params, a);
+    hb::Options opt;
+    progress("Simple Colocated Cokriging Markov Model II", 0);
+    if (hb::cokriging(dims, primary_data->m_data, primary_data->m_mask, secondary_data->m_data,
+                      secondary_data->m_mask, a, output_data->m_data, output_data->m_mask, opt) == 0)
+        report_done("Simple Colocated Cokriging Markov Model II");
+}
+
 int hpgl_simple_kriging_weights(float *center_coords, float *neighbours_x, float *neighbours_y,
                                 float *neighbours_z, int neighbours_count, hpgl_cov_params_t *params,
                                 float *weights)
@@ -390,6 +506,20 @@ int hpgl_b200_lvm_kriging_ex(const int *dims, const float *in_data, const unsign
     }
     return hb::cont_kriging(2, dims, in_data, in_mask, ok_args_from(params), out_data, out_mask, options_from(opt),
                             mean_data);
+}
+
+int hpgl_b200_cokriging_ex(int mark, const int *dims, const float *pdata, const unsigned char *pmask,
+                           const float *sdata, const unsigned char *smask, const hpgl_cokriging_m1_params_t *m1,
+                           const hpgl_cokriging_m2_params_t *m2, float *out_data, unsigned char *out_mask,
+                           const hpgl_b200_options_t *opt)
+{
+    hb::CokArgs a;
+    if (!cok_args_from(mark, m1, m2, a))
+    {
+        hb::set_error("hpgl_b200_cokriging_ex: mark must be 1 (with m1) or 2 (with m2)");
+        return HPGL_B200_EINVAL;
+    }
+    return hb::cokriging(dims, pdata, pmask, sdata, smask, a, out_data, out_mask, options_from(opt));
 }
 
 int hpgl_b200_sgs_draws(long long seed, long long n, double *out)

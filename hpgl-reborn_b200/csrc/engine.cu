@@ -1246,6 +1246,162 @@ int sgs_simulation(const int *dims, float *data, unsigned char *mask, const unsi
     }
 }
 
+// ------------------------------------------------------------------ cokriging
+int cokriging(const int *dims, const float *pdata, const unsigned char *pmask, const float *sdata,
+              const unsigned char *smask, const CokArgs &a, float *out_data, unsigned char *out_mask,
+              const Options &opt)
+{
+    std::lock_guard<std::mutex> lk(g_engine_mu);
+    try
+    {
+        if (!dims || !pdata || !pmask || !sdata || !smask || !out_data || !out_mask)
+            throw CudaFail{-1, "null array argument"};
+        if (a.mark != 1 && a.mark != 2) throw CudaFail{-1, "cokriging: mark must be 1 or 2"};
+        const long long n = check_dims(dims);
+        const CovArgs &pc = a.primary;
+        check_model_args(pc.cov_type, pc.ranges, pc.angles, pc.sill, pc.nugget, a.radiuses, a.max_nb);
+        if (a.mark == 2)
+            check_model_args(a.secondary.cov_type, a.secondary.ranges, a.secondary.angles, a.secondary.sill,
+                             a.secondary.nugget, a.radiuses, a.max_nb);
+        if (a.max_nb > kSgsBlockMax)
+            throw CudaFail{-4, "cokriging supports max_neighbours up to " + std::to_string(kSgsBlockMax)};
+        if (!std::isfinite(a.primary_mean) || !std::isfinite(a.secondary_mean) ||
+            !std::isfinite(a.secondary_variance) || !std::isfinite(a.corr))
+            throw CudaFail{-1, "cokriging means, variance and correlation must be finite"};
+        // the analytic primary model (the template and A, b), and the cross model
+        double plan_ms = 0.0;
+        auto plan_f = std::async(std::launch::async, [&]() {
+            const auto t0 = std::chrono::steady_clock::now();
+            Plan p = make_plan(false, pc.cov_type, pc.ranges, pc.angles, pc.sill, pc.nugget, a.radiuses, a.max_nb,
+                               dims, false);
+            std::vector<Offset> tv = build_template(p.f, p.kt);
+            plan_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            return std::make_pair(std::move(p), std::move(tv));
+        });
+        Engine &E = engine_for_current_device();
+        cudaStream_t st = E.stream(opt.stream);
+        IoPlan io{(opt.flags & 1u) != 0, st};
+        begin_call(E, st);
+        const float *d_pd = to_device(E, "cok_pdata", pdata, (size_t)n, io);
+        const uint8_t *d_pm = to_device(E, "cok_pmask", pmask, (size_t)n, io);
+        const float *d_sd = to_device(E, "cok_sdata", sdata, (size_t)n, io);
+        const uint8_t *d_sm = to_device(E, "cok_smask", smask, (size_t)n, io);
+        float *d_out = io.device ? out_data : E.buf<float>("out_data", (size_t)n);
+        uint8_t *d_omask = io.device ? out_mask : E.buf<uint8_t>("out_mask", (size_t)n);
+        signed char *d_status =
+            opt.status ? (io.device ? opt.status : E.buf<signed char>("status", (size_t)n)) : nullptr;
+        E.mark(STAGE_UPLOAD, st);
+
+        // targets: the uninformed primary cells in ascending order
+        int *rank_of = E.buf<int>("cok_rank_of", (size_t)n);
+        int *flag = E.buf<int>("cok_flag", (size_t)n);
+        int *pos = E.buf<int>("cok_pos", (size_t)n);
+        int *tmp = E.buf<int>("scan_tmp", (size_t)scan_tmp_ints(n) + 4);
+        int *total = E.buf<int>("cok_total", 1);
+        int *targets = E.buf<int>("cok_targets", (size_t)n);
+        launch_cok_prepare(n, d_pm, rank_of, flag, st);
+        HB_CK(cudaMemcpyAsync(pos, flag, n * 4, cudaMemcpyDeviceToDevice, st));
+        exclusive_scan(pos, n, tmp, total, st);
+        launch_cok_targets(n, flag, pos, targets, st);
+        HB_CK(cudaGetLastError());
+        int n_t = 0;
+        HB_CK(cudaMemcpyAsync(&n_t, total, sizeof(int), cudaMemcpyDeviceToHost, st));
+        HB_CK(cudaStreamSynchronize(st));
+        E.stats.launches += 2 + scan_kernels(n);
+        E.mark(STAGE_COMPACT, st);
+
+        auto plan_pair = plan_f.get();
+        const Plan &pl = plan_pair.first;
+        const std::vector<Offset> &tv = plan_pair.second;
+        E.stats.plan_ms = plan_ms;
+        const Geom &g = pl.g;
+        const size_t nk = pl.kt.vals.size();
+        double *search_vals = E.buf<double>("search_vals", nk);
+        HB_CK(cudaMemcpyAsync(search_vals, pl.kt.vals.data(), nk * 8, cudaMemcpyHostToDevice, st));
+        const long long pn = (long long)g.pnx * g.pny * (2 * g.phz + 1);
+        double *pair64 = E.buf<double>("pair64", (size_t)pn);
+        float *pair32 = E.buf<float>("pair32", (size_t)pn);
+        launch_build_pair(g, dev_model(pl.f.m), 0, search_vals, pair64, pair32, st);
+        // the cross model over the +-radius box and the border's constants
+        // (cross_cov_model_mark_i_t / _mark_ii_t, simple_cokriging_markI.cpp:145-193)
+        Flavour fs = pl.f;
+        if (a.mark == 2)
+        {
+            std::string err;
+            if (!make_model(a.secondary.cov_type, a.secondary.ranges, a.secondary.angles, a.secondary.sill,
+                            a.secondary.nugget, fs.m, err))
+                throw CudaFail{-1, err};
+        }
+        const double c0p = pl.f.c0(), c0s = fs.c0();
+        CokParams cp;
+        if (a.mark == 1)
+        {
+            cp.coef = c0p <= 0 ? 0.0 : a.corr * sqrt(a.secondary_variance) / sqrt(c0p);
+            cp.sec_var = a.secondary_variance;
+        }
+        else
+        {
+            cp.coef = c0s <= 0 ? 0.0 : a.corr * sqrt(c0p / c0s);
+            cp.sec_var = c0s;
+        }
+        cp.b_last = cp.coef * fs.c0();
+        cp.pm = (float)a.primary_mean;
+        cp.sm = (float)a.secondary_mean;
+        const int bx = 2 * g.rx + 1, by = 2 * g.ry + 1, bz = 2 * g.rz + 1;
+        std::vector<double> cross((size_t)bx * by * bz);
+        for (int dz = -g.rz; dz <= g.rz; ++dz)
+            for (int dy = -g.ry; dy <= g.ry; ++dy)
+                for (int dx = -g.rx; dx <= g.rx; ++dx)
+                    cross[((size_t)(dz + g.rz) * by + (dy + g.ry)) * bx + (dx + g.rx)] = fs.at_offset(dx, dy, dz);
+        double *d_cross = E.buf<double>("cok_cross", cross.size());
+        HB_CK(cudaMemcpyAsync(d_cross, cross.data(), cross.size() * 8, cudaMemcpyHostToDevice, st));
+        std::vector<int4> t4(tv.size());
+        for (size_t i = 0; i < tv.size(); ++i) t4[i] = make_int4(tv[i].dx, tv[i].dy, tv[i].dz, 0);
+        int4 *tmpl = E.buf<int4>("sgs_tmpl", std::max<size_t>(t4.size(), 1));
+        if (!t4.empty())
+            HB_CK(cudaMemcpyAsync(tmpl, t4.data(), t4.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+        HB_CK(cudaStreamSynchronize(st)); // host temporaries
+        E.stats.launches += 1;
+        E.mark(STAGE_TABLES, st);
+
+        const int k = a.max_nb;
+        int *nb = E.buf<int>("cok_nb", (size_t)std::max(n_t, 1) * k);
+        int *nb_cnt = E.buf<int>("cok_nb_cnt", (size_t)std::max(n_t, 1));
+        if (n_t > 0)
+        {
+            launch_sgs_search(g, tmpl, (int)t4.size(), targets, n_t, rank_of, k, nb, nullptr, nb_cnt, E.n_sm(), st, 0);
+            E.stats.launches += 1;
+        }
+        HB_CK(cudaGetLastError());
+        E.mark(STAGE_SEARCH, st);
+        HB_CK(launch_cok_solve(g, targets, n_t, nb, nb_cnt, k, pair64, d_cross, d_pd, d_sd, d_sm, cp, d_out, d_omask,
+                               d_status, E.n_sm(), st));
+        if (n_t > 0) E.stats.launches += 1;
+        E.mark(STAGE_SOLVE, st);
+        launch_cok_finalize(n, d_pd, d_pm, d_out, d_omask, d_status, st);
+        HB_CK(cudaGetLastError());
+        E.stats.launches += 1;
+        E.mark(STAGE_FINALIZE, st);
+        to_host(E, out_data, d_out, (size_t)n, io);
+        to_host(E, out_mask, d_omask, (size_t)n, io);
+        if (opt.status) to_host(E, opt.status, d_status, (size_t)n, io);
+        E.mark(STAGE_DOWNLOAD, st);
+        E.stats.kriged = n_t;
+        end_call(E, st);
+        return 0;
+    }
+    catch (const CudaFail &f)
+    {
+        set_error(f.msg);
+        return f.code;
+    }
+    catch (const std::exception &ex)
+    {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
 int find_neighbours(int kind, const int *dims, const unsigned char *mask, const SkArgs &a, const int *nodes,
                     int n_nodes, int *out_idx, int *out_count, unsigned char *out_path)
 {

@@ -29,6 +29,25 @@ struct IkArgs
     double marginal;
 };
 
+struct CovArgs
+{
+    int cov_type;
+    double ranges[3];
+    double angles[3];
+    double sill, nugget;
+};
+
+// Collocated cokriging: mark 1 (one model, the secondary variance given) or
+// mark 2 (primary and secondary models).
+struct CokArgs
+{
+    int mark;
+    CovArgs primary, secondary;
+    int radiuses[3];
+    int max_nb;
+    double primary_mean, secondary_mean, secondary_variance, corr;
+};
+
 struct SgsArgs
 {
     int cov_type;
@@ -109,6 +128,12 @@ int cont_kriging(int kind, const int *dims, const float *in_data, const unsigned
 // neighbours, 2 singular (N(0,1) draw), 3 not simulated.
 int sgs_simulation(const int *dims, float *data, unsigned char *mask, const unsigned char *sim_mask,
                    const CdfTable *cdf, const float *means, const SgsArgs &a, const Options &opt);
+// Simple collocated cokriging (simple_cokriging_markI.cpp:202-330) of every
+// uninformed primary cell; every output cell ends informed. opt.status
+// receives -1 informed, 0 kriged, 1 no neighbours, 2 singular.
+int cokriging(const int *dims, const float *pdata, const unsigned char *pmask, const float *sdata,
+              const unsigned char *smask, const CokArgs &a, float *out_data, unsigned char *out_mask,
+              const Options &opt);
 int indicator_kriging(const int *dims, const unsigned char *in_data, const unsigned char *in_mask,
                       const std::vector<IkArgs> &cats, unsigned char *out_data, unsigned char *out_mask,
                       const Options &opt);

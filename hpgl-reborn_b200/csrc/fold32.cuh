@@ -1,0 +1,195 @@
+// A folded FP64 solve of up to 32 symmetric positive definite systems per
+// warp pair (shared by the simulation and cokriging kernels).
+//
+// Sixteen lanes hold one system: lane t owns rows t and 31 - t of the lower
+// triangle (rows of a system with n < 32 unknowns are padded with the
+// identity). The right-looking Cholesky factorisation broadcasts column j of
+// the updated matrix through shared-memory row j, and carries the forward
+// substitution of QB right-hand sides in the same rows; the back substitution
+// reads column i of L back from the lane's own rows (row r of M holds column r
+// of L times sqrt(d_r)). The matrix entries are covariances read from a pair
+// table: A[r][c] = pair_c[lin_r - lin_c] with lin the pair-table offsets of the
+// unknowns relative to the target.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace hb
+{
+constexpr int kFold32NP = 32, kFold32G = 16;
+constexpr int kFold32LD = kFold32NP + 2; // 32 entries, then up to two right-hand sides
+// per system: M (32 x LD doubles), LIN (32 ints); systems sharing a warp 16 bytes
+// apart modulo 128 so that their broadcast rows fall on different banks
+constexpr size_t kFold32SysBytes = ((size_t)kFold32NP * kFold32LD * 8 + kFold32NP * 4 + 127) / 128 * 128 + 16;
+
+// Solves A [x] = [rhs] for the lane's rows t and 31 - t (QB <= 2 right-hand
+// sides; rows of non-live unknowns carry zeros). `gm` is the system's lane
+// mask; LIN must hold the 32 offsets (0 for non-live rows) and be visible to
+// the system's lanes. after_assembly() and after_factor() run at those points
+// (the callers issue prefetches there). Returns true when a pivot is not
+// positive (or NaN), or, with EPS_PIVOT, below machine epsilon (the test of
+// the reference's Gaussian elimination, gauss_solver.cpp:37-41).
+template <int QB, bool EPS_PIVOT = false, typename F1, typename F2>
+__device__ __forceinline__ bool fold32_solve(const double *pair_c, const int *LIN, double *M, unsigned gm, int t,
+                                             bool live_a, bool live_b, int lin_a, int lin_b,
+                                             const double (&rhs_a_in)[QB], const double (&rhs_b_in)[QB],
+                                             double (&xa)[QB], double (&xb)[QB], F1 after_assembly,
+                                             F2 after_factor)
+{
+    constexpr int NP = kFold32NP, G = kFold32G, LD = kFold32LD;
+    const int rb = NP - 1 - t;
+    // ---- assembly (lower triangles of rows t and 31 - t; padding rows identity)
+    double ra[G], rbv[NP];
+    const double *base_a = pair_c + lin_a, *base_b = pair_c + lin_b;
+#pragma unroll
+    for (int c = 0; c < G; ++c)
+    {
+        double e = 0.0;
+        if (live_a && c <= t) e = __ldg(base_a - LIN[c]);
+        if (!live_a && c == t) e = 1.0;
+        ra[c] = e;
+    }
+#pragma unroll
+    for (int c = 0; c < NP; ++c)
+    {
+        double e = 0.0;
+        if (live_b && c <= rb) e = __ldg(base_b - LIN[c]);
+        if (!live_b && c == rb) e = 1.0;
+        rbv[c] = e;
+    }
+    after_assembly();
+
+    // ---- factorisation with the forward substitution of the right-hand sides
+    double rhs_a[QB], rhs_b[QB], ya[QB], yb[QB];
+#pragma unroll
+    for (int q = 0; q < QB; ++q)
+    {
+        rhs_a[q] = rhs_a_in[q];
+        rhs_b[q] = rhs_b_in[q];
+    }
+#pragma unroll
+    for (int q = 0; q < QB; ++q)
+    {
+        ya[q] = 0.0;
+        yb[q] = 0.0;
+    }
+    bool fail = false;
+    double inv_a = 0.0, inv_b = 0.0;
+#pragma unroll
+    for (int j = 0; j < NP; ++j)
+    {
+        if (j < G)
+        {
+            M[j * LD + t] = ra[j];
+            if (t == j)
+            {
+#pragma unroll
+                for (int q = 0; q < QB; ++q) M[j * LD + NP + q] = rhs_a[q];
+            }
+        }
+        M[j * LD + rb] = rbv[j];
+        if (j >= G && rb == j)
+        {
+#pragma unroll
+            for (int q = 0; q < QB; ++q) M[j * LD + NP + q] = rhs_b[q];
+        }
+        __syncwarp(gm);
+        double mj[LD];
+        const double2 *mv = reinterpret_cast<const double2 *>(M + j * LD);
+#pragma unroll
+        for (int q = j / 2; q < LD / 2; ++q)
+        {
+            const double2 v2 = mv[q];
+            mj[2 * q] = v2.x;
+            mj[2 * q + 1] = v2.y;
+        }
+        const double d = mj[j];
+        fail |= EPS_PIVOT ? !(d >= 2.220446049250313080847e-16) : !(d > 0.0);
+        const double inv_s = rsqrt(d);
+        const double inv2 = inv_s * inv_s;
+        if (j < G)
+        {
+            const double sc = ra[j] * inv2;
+#pragma unroll
+            for (int c = j + 1; c < G; ++c) ra[c] -= sc * mj[c];
+            if (t > j)
+            {
+#pragma unroll
+                for (int q = 0; q < QB; ++q) rhs_a[q] -= sc * mj[NP + q];
+            }
+            ra[j] *= inv_s;
+            if (t == j)
+            {
+                inv_a = inv_s;
+#pragma unroll
+                for (int q = 0; q < QB; ++q) ya[q] = rhs_a[q] * inv_s;
+            }
+        }
+        {
+            const double sc = rbv[j] * inv2;
+#pragma unroll
+            for (int c = j + 1; c < NP; ++c) rbv[c] -= sc * mj[c];
+            if (rb > j)
+            {
+#pragma unroll
+                for (int q = 0; q < QB; ++q) rhs_b[q] -= sc * mj[NP + q];
+            }
+            rbv[j] *= inv_s;
+            if (rb == j)
+            {
+                inv_b = inv_s;
+#pragma unroll
+                for (int q = 0; q < QB; ++q) yb[q] = rhs_b[q] * inv_s;
+            }
+        }
+    }
+
+    after_factor();
+
+    // ---- back substitution L^T x = y; L[i][row] = M[row][i] / sqrt(d_row)
+#pragma unroll
+    for (int q = 0; q < QB; ++q)
+    {
+        xa[q] = 0.0;
+        xb[q] = 0.0;
+    }
+#pragma unroll
+    for (int i = NP - 1; i >= 0; --i)
+    {
+        double xi[QB];
+        if (i >= G)
+        {
+            if (rb == i)
+            {
+#pragma unroll
+                for (int q = 0; q < QB; ++q) xb[q] = yb[q] * inv_b;
+            }
+#pragma unroll
+            for (int q = 0; q < QB; ++q) xi[q] = __shfl_sync(gm, xb[q], NP - 1 - i, G);
+        }
+        else
+        {
+            if (t == i)
+            {
+#pragma unroll
+                for (int q = 0; q < QB; ++q) xa[q] = ya[q] * inv_a;
+            }
+#pragma unroll
+            for (int q = 0; q < QB; ++q) xi[q] = __shfl_sync(gm, xa[q], i, G);
+        }
+        if (t < i)
+        {
+            const double l = M[t * LD + i] * inv_a;
+#pragma unroll
+            for (int q = 0; q < QB; ++q) ya[q] -= l * xi[q];
+        }
+        if (rb < i)
+        {
+            const double l = M[rb * LD + i] * inv_b;
+#pragma unroll
+            for (int q = 0; q < QB; ++q) yb[q] -= l * xi[q];
+        }
+    }
+
+    return fail;
+}
+} // namespace hb

@@ -142,8 +142,11 @@ void launch_sgs_path(const SgsWalk &w, const uint8_t *mask, const uint8_t *sim_m
                      cudaStream_t st);
 void launch_sgs_index(long long n, const int *path_cell, const int *flag, const int *scan, const uint8_t *mask,
                       int *rank_of, int *sim_cells, cudaStream_t st);
+// Template scan with the rank predicate rank_of[q] < rank (or < fixed_rank when
+// fixed_rank >= 0); nb_rank may be null.
 void launch_sgs_search(const Geom &g, const int4 *tmpl, int n_tmpl, const int *sim_cells, int n_sim,
-                       const int *rank_of, int k, int *nb, int *nb_rank, int *nb_cnt, int n_sm, cudaStream_t st);
+                       const int *rank_of, int k, int *nb, int *nb_rank, int *nb_cnt, int n_sm, cudaStream_t st,
+                       int fixed_rank = -1);
 void launch_sgs_levels(const int *nb_rank, const int *nb_cnt, int k, int n_sim, int *levp1, int *ticket,
                        int *level_count, int level_cap, int *max_level, int *err, int n_sm, cudaStream_t st);
 void launch_sgs_moments(int n_sim, const int *nb_cnt, double *mom, int n_sm, cudaStream_t st); // mom: 3, zeroed
@@ -153,4 +156,22 @@ size_t sgs_block_smem(int k);
 cudaError_t launch_sgs_solve(const Geom &g, const int *order, int n_items, const int *sim_cells, const int *nb,
                              const int *nb_cnt, int k, const double *pair64, float *data, const float *means,
                              const double *uniforms, signed char *st_rank, bool ordinary, int n_sm, cudaStream_t st);
+
+// collocated cokriging (cokriging.cu)
+struct CokParams
+{
+    double coef;    // cross covariance = coef * cross_tab (Markov models I and II)
+    double sec_var; // the secondary variance, A[n][n]
+    double b_last;  // coef * C_cross(0), b[n]
+    float pm, sm;   // primary and secondary means (float, as the reference stores them)
+};
+void launch_cok_prepare(long long n, const uint8_t *pmask, int *rank_of, int *flag, cudaStream_t st);
+void launch_cok_targets(long long n, const int *flag, const int *pos, int *targets, cudaStream_t st);
+// cross_tab: the cross model over the +-radius box, x fastest
+cudaError_t launch_cok_solve(const Geom &g, const int *targets, int n_targets, const int *nb, const int *nb_cnt,
+                             int k, const double *pair64, const double *cross_tab, const float *pdata,
+                             const float *sdata, const uint8_t *smask, const CokParams &p, float *out_data,
+                             uint8_t *out_mask, signed char *status, int n_sm, cudaStream_t st);
+void launch_cok_finalize(long long n, const float *pdata, const uint8_t *pmask, float *out_data, uint8_t *out_mask,
+                         signed char *status, cudaStream_t st);
 } // namespace hb

@@ -26,6 +26,7 @@
 // host), pushed through the inverse Gaussian CDF with the reference's float
 // mean and double variance.
 #include "engine.cuh"
+#include "fold32.cuh"
 #include "kernels.h"
 
 #include <algorithm>
@@ -212,11 +213,14 @@ __global__ void k_sgs_index(long long n, const int *__restrict__ path_cell, cons
 // predicate: the first k template offsets, in template order, whose cell lies
 // in the grid and was informed before the node. One warp per node, 32 offsets
 // per step. nb_rank receives each neighbour's rank (-1 for a conditioning
-// cell), which the level pass reads instead of gathering rank_of again.
+// cell), which the level pass reads instead of gathering rank_of again. With
+// fixed_rank >= 0 every node compares against fixed_rank instead of its own
+// rank (cokriging: every target sees the same informed cells).
 __global__ void __launch_bounds__(256) k_sgs_search(const Geom g, const int4 *__restrict__ tmpl, int n_tmpl,
                                                     const int *__restrict__ sim_cells, int n_sim,
-                                                    const int *__restrict__ rank_of, int k, int *__restrict__ nb,
-                                                    int *__restrict__ nb_rank, int *__restrict__ nb_cnt)
+                                                    const int *__restrict__ rank_of, int k, int fixed_rank,
+                                                    int *__restrict__ nb, int *__restrict__ nb_rank,
+                                                    int *__restrict__ nb_cnt)
 {
     const int lane = threadIdx.x & 31;
     const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
@@ -226,7 +230,8 @@ __global__ void __launch_bounds__(256) k_sgs_search(const Geom g, const int4 *__
         const int x = cell % g.nx, y = (int)((cell / g.nx) % g.ny), z = (int)(cell / ((long long)g.nx * g.ny));
         int found = 0;
         int *out = nb + r * (long long)k;
-        int *out_rank = nb_rank + r * (long long)k;
+        int *out_rank = nb_rank ? nb_rank + r * (long long)k : nullptr;
+        const int thr = fixed_rank >= 0 ? fixed_rank : (int)r;
         for (int base = 0; base < n_tmpl && found < k; base += 32)
         {
             const int t = base + lane;
@@ -240,7 +245,7 @@ __global__ void __launch_bounds__(256) k_sgs_search(const Geom g, const int4 *__
                 {
                     q = (int)(((long long)Z * g.ny + Y) * g.nx + X);
                     rq = rank_of[q];
-                    hit = rq < (int)r;
+                    hit = rq < thr;
                 }
             }
             const unsigned m = __ballot_sync(0xffffffffu, hit);
@@ -248,7 +253,7 @@ __global__ void __launch_bounds__(256) k_sgs_search(const Geom g, const int4 *__
             if (hit && slot < k)
             {
                 out[slot] = q;
-                out_rank[slot] = rq;
+                if (out_rank) out_rank[slot] = rq;
             }
             found += __popc(m);
         }
@@ -438,9 +443,9 @@ struct SgsSolveArgs
 // row j and carries the forward substitution of b (and, for ordinary kriging,
 // of the ones vector); the back substitution reads column i of L from the
 // lane's own shared rows. The weights then go through combine() one by one.
-constexpr int kSgsNP = 32, kSgsG = 16;
-constexpr int kSgsLD = kSgsNP + 2; // 32 entries, then the right-hand sides
-constexpr size_t kSgsSysBytes = ((size_t)kSgsNP * kSgsLD * 8 + kSgsNP * 4 + 127) / 128 * 128 + 16;
+constexpr int kSgsNP = kFold32NP, kSgsG = kFold32G;
+constexpr int kSgsLD = kFold32LD;
+constexpr size_t kSgsSysBytes = kFold32SysBytes;
 constexpr int kSgsFoldThreads = 256;
 
 template <bool ORD>
@@ -508,31 +513,9 @@ __global__ void __launch_bounds__(kSgsFoldThreads, 1) k_sgs_solve_fold(const Sgs
         LIN[rb] = lin_b;
         __syncwarp(gm);
 
-        // ---- assembly (lower triangles of rows t and 31 - t; padding rows identity)
-        double ra[G], rbv[NP];
-        const double *base_a = pair64 + pc + lin_a, *base_b = pair64 + pc + lin_b;
-#pragma unroll
-        for (int c = 0; c < G; ++c)
-        {
-            double e = 0.0;
-            if (live_a && c <= t) e = __ldg(base_a - LIN[c]);
-            if (!live_a && c == t) e = 1.0;
-            ra[c] = e;
-        }
-#pragma unroll
-        for (int c = 0; c < NP; ++c)
-        {
-            double e = 0.0;
-            if (live_b && c <= rb) e = __ldg(base_b - LIN[c]);
-            if (!live_b && c == rb) e = 1.0;
-            rbv[c] = e;
-        }
-        const double b_a = live_a ? __ldg(base_a) : 0.0;
-        const double b_b = live_b ? __ldg(base_b) : 0.0;
-        stage_b();
-
-        // ---- factorisation with the forward substitution of b (and 1)
-        double rhs_a[QB], rhs_b[QB], ya[QB], yb[QB];
+        const double b_a = live_a ? __ldg(pair64 + pc + lin_a) : 0.0;
+        const double b_b = live_b ? __ldg(pair64 + pc + lin_b) : 0.0;
+        double rhs_a[QB], rhs_b[QB], xa[QB], xb[QB];
         rhs_a[0] = b_a;
         rhs_b[0] = b_b;
         if constexpr (ORD)
@@ -540,130 +523,8 @@ __global__ void __launch_bounds__(kSgsFoldThreads, 1) k_sgs_solve_fold(const Sgs
             rhs_a[1] = live_a ? 1.0 : 0.0;
             rhs_b[1] = live_b ? 1.0 : 0.0;
         }
-#pragma unroll
-        for (int q = 0; q < QB; ++q)
-        {
-            ya[q] = 0.0;
-            yb[q] = 0.0;
-        }
-        bool fail = false;
-        double inv_a = 0.0, inv_b = 0.0;
-#pragma unroll
-        for (int j = 0; j < NP; ++j)
-        {
-            if (j < G)
-            {
-                M[j * LD + t] = ra[j];
-                if (t == j)
-                {
-#pragma unroll
-                    for (int q = 0; q < QB; ++q) M[j * LD + NP + q] = rhs_a[q];
-                }
-            }
-            M[j * LD + rb] = rbv[j];
-            if (j >= G && rb == j)
-            {
-#pragma unroll
-                for (int q = 0; q < QB; ++q) M[j * LD + NP + q] = rhs_b[q];
-            }
-            __syncwarp(gm);
-            double mj[LD];
-            const double2 *mv = reinterpret_cast<const double2 *>(M + j * LD);
-#pragma unroll
-            for (int q = j / 2; q < LD / 2; ++q)
-            {
-                const double2 v2 = mv[q];
-                mj[2 * q] = v2.x;
-                mj[2 * q + 1] = v2.y;
-            }
-            const double d = mj[j];
-            fail |= !(d > 0.0);
-            const double inv_s = rsqrt(d);
-            const double inv2 = inv_s * inv_s;
-            if (j < G)
-            {
-                const double sc = ra[j] * inv2;
-#pragma unroll
-                for (int c = j + 1; c < G; ++c) ra[c] -= sc * mj[c];
-                if (t > j)
-                {
-#pragma unroll
-                    for (int q = 0; q < QB; ++q) rhs_a[q] -= sc * mj[NP + q];
-                }
-                ra[j] *= inv_s;
-                if (t == j)
-                {
-                    inv_a = inv_s;
-#pragma unroll
-                    for (int q = 0; q < QB; ++q) ya[q] = rhs_a[q] * inv_s;
-                }
-            }
-            {
-                const double sc = rbv[j] * inv2;
-#pragma unroll
-                for (int c = j + 1; c < NP; ++c) rbv[c] -= sc * mj[c];
-                if (rb > j)
-                {
-#pragma unroll
-                    for (int q = 0; q < QB; ++q) rhs_b[q] -= sc * mj[NP + q];
-                }
-                rbv[j] *= inv_s;
-                if (rb == j)
-                {
-                    inv_b = inv_s;
-#pragma unroll
-                    for (int q = 0; q < QB; ++q) yb[q] = rhs_b[q] * inv_s;
-                }
-            }
-        }
-
-        stage_c();
-
-        // ---- back substitution L^T x = y; L[i][row] = M[row][i] / sqrt(d_row)
-        double xa[QB], xb[QB];
-#pragma unroll
-        for (int q = 0; q < QB; ++q)
-        {
-            xa[q] = 0.0;
-            xb[q] = 0.0;
-        }
-#pragma unroll
-        for (int i = NP - 1; i >= 0; --i)
-        {
-            double xi[QB];
-            if (i >= G)
-            {
-                if (rb == i)
-                {
-#pragma unroll
-                    for (int q = 0; q < QB; ++q) xb[q] = yb[q] * inv_b;
-                }
-#pragma unroll
-                for (int q = 0; q < QB; ++q) xi[q] = __shfl_sync(gm, xb[q], NP - 1 - i, G);
-            }
-            else
-            {
-                if (t == i)
-                {
-#pragma unroll
-                    for (int q = 0; q < QB; ++q) xa[q] = ya[q] * inv_a;
-                }
-#pragma unroll
-                for (int q = 0; q < QB; ++q) xi[q] = __shfl_sync(gm, xa[q], i, G);
-            }
-            if (t < i)
-            {
-                const double l = M[t * LD + i] * inv_a;
-#pragma unroll
-                for (int q = 0; q < QB; ++q) ya[q] -= l * xi[q];
-            }
-            if (rb < i)
-            {
-                const double l = M[rb * LD + i] * inv_b;
-#pragma unroll
-                for (int q = 0; q < QB; ++q) yb[q] -= l * xi[q];
-            }
-        }
+        const bool fail = fold32_solve<QB>(pair64 + pc, LIN, M, gm, t, live_a, live_b, lin_a, lin_b, rhs_a, rhs_b,
+                                           xa, xb, stage_b, stage_c);
 
         // ---- combine() and the variance in the reference's order
         double sx = 0.0, sy = 0.0;
@@ -857,9 +718,11 @@ void launch_sgs_index(long long n, const int *path_cell, const int *flag, const 
     k_sgs_index<<<1184, 256, 0, st>>>(n, path_cell, flag, scan, mask, rank_of, sim_cells);
 }
 void launch_sgs_search(const Geom &g, const int4 *tmpl, int n_tmpl, const int *sim_cells, int n_sim,
-                       const int *rank_of, int k, int *nb, int *nb_rank, int *nb_cnt, int n_sm, cudaStream_t st)
+                       const int *rank_of, int k, int *nb, int *nb_rank, int *nb_cnt, int n_sm, cudaStream_t st,
+                       int fixed_rank)
 {
-    k_sgs_search<<<n_sm * 8, 256, 0, st>>>(g, tmpl, n_tmpl, sim_cells, n_sim, rank_of, k, nb, nb_rank, nb_cnt);
+    k_sgs_search<<<n_sm * 8, 256, 0, st>>>(g, tmpl, n_tmpl, sim_cells, n_sim, rank_of, k, fixed_rank, nb, nb_rank,
+                                           nb_cnt);
 }
 void launch_sgs_levels(const int *nb_rank, const int *nb_cnt, int k, int n_sim, int *levp1, int *ticket,
                        int *level_count, int level_cap, int *max_level, int *err, int n_sm, cudaStream_t st)

@@ -2,7 +2,8 @@
 
 Signatures, argument validation and output conventions follow HPGL's
 src/geo_bsd/geo.py: ordinary_kriging (:573-607), simple_kriging (:610-649),
-lvm_kriging (:651-696), median_ik (:699-738), indicator_kriging (:759-801, two categories dispatch to
+lvm_kriging (:651-696), median_ik (:699-738), simple_cokriging_markI (:804-841),
+simple_cokriging_markII (:843-895), indicator_kriging (:759-801, two categories dispatch to
 median IK with data[0]'s model, :785-793), simple_kriging_weights (:897-935),
 the property/grid/model classes (:215-299) and the handler setters (:947-966).
 The output property is a clone of the input that the library fills in place.
@@ -241,6 +242,71 @@ def lvm_kriging(prop, grid, mean_data, radiuses, max_neighbours, cov_model, *, p
     return out_prop
 
 
+def _cokriging_props(prop, secondary):
+    prop = _to_prop(prop)
+    secondary = _to_prop(secondary)
+    if secondary.data.size != prop.data.size:
+        raise RuntimeError("Size of secondary data (%d) is different from size of primary data (%d)"
+                           % (secondary.data.size, prop.data.size))
+    return prop, secondary, _clone_prop(prop)
+
+
+def _cokriging_call(mark, grid, prop, secondary, out_prop, m1, m2):
+    dims = _dims(grid, prop)
+    opt = _options(None, 0)
+    rc = _hpgl_so.hpgl_b200_cokriging_ex(mark, dims, _flat(prop.data).ctypes.data, _flat(prop.mask).ctypes.data,
+                                         _flat(secondary.data).ctypes.data, _flat(secondary.mask).ctypes.data,
+                                         C.byref(m1) if m1 is not None else None,
+                                         C.byref(m2) if m2 is not None else None,
+                                         _flat(out_prop.data).ctypes.data, _flat(out_prop.mask).ctypes.data,
+                                         C.byref(opt))
+    W.check(rc, "simple_cokriging_mark%d" % mark)
+    return out_prop
+
+
+def simple_cokriging_markI(prop, grid, secondary_data, primary_mean, secondary_mean, secondary_variance,
+                           correlation_coef, radiuses, max_neighbours, cov_model):
+    """Simple collocated cokriging, Markov model I: the cross covariance is
+    correlation_coef * sqrt(secondary_variance / C(0)) * C (the primary model)."""
+    GridValidator.validate_grid_dimensions(grid.x, grid.y, grid.z)
+    valid_radiuses = ParameterValidator.validate_radius(radiuses, "radiuses")
+    ParameterValidator.validate_max_neighbors(max_neighbours)
+    ParameterValidator.validate_covariance_parameters(cov_model.sill, cov_model.nugget, cov_model.ranges,
+                                                      cov_model.angles)
+    ParameterValidator.validate_correlation_coef(correlation_coef)
+    ParameterValidator.validate_variance(secondary_variance, "secondary_variance")
+    prop, secondary, out_prop = _cokriging_props(prop, secondary_data)
+    m1 = W._HPGL_COK_M1_PARAMS(covariance_type=cov_model.type, ranges=tuple(cov_model.ranges),
+                               angles=tuple(cov_model.angles), sill=cov_model.sill, nugget=cov_model.nugget,
+                               radiuses=_int_radiuses(valid_radiuses), max_neighbours=max_neighbours,
+                               primary_mean=primary_mean, secondary_mean=secondary_mean,
+                               secondary_variance=secondary_variance, correlation_coef=correlation_coef)
+    return _cokriging_call(1, grid, prop, secondary, out_prop, m1, None)
+
+
+def simple_cokriging_markII(grid, primary_data, secondary_data, correlation_coef, radiuses, max_neighbours):
+    """Simple collocated cokriging, Markov model II: primary_data and
+    secondary_data are dicts with "data" (a property), "mean" and "cov_model";
+    the cross covariance is correlation_coef * sqrt(C1(0) / C2(0)) * C2."""
+    GridValidator.validate_grid_dimensions(grid.x, grid.y, grid.z)
+    valid_radiuses = ParameterValidator.validate_radius(radiuses, "radiuses")
+    ParameterValidator.validate_max_neighbors(max_neighbours)
+    ParameterValidator.validate_correlation_coef(correlation_coef)
+    for d in (primary_data, secondary_data):
+        cm = d["cov_model"]
+        ParameterValidator.validate_covariance_parameters(cm.sill, cm.nugget, cm.ranges, cm.angles)
+    prop, secondary, out_prop = _cokriging_props(primary_data["data"], secondary_data["data"])
+    pcp, scp = primary_data["cov_model"], secondary_data["cov_model"]
+    m2 = W._HPGL_COK_M2_PARAMS(
+        primary_cov_params=W._HPGL_COV_PARAMS(covariance_type=pcp.type, ranges=tuple(pcp.ranges),
+                                              angles=tuple(pcp.angles), sill=pcp.sill, nugget=pcp.nugget),
+        secondary_cov_params=W._HPGL_COV_PARAMS(covariance_type=scp.type, ranges=tuple(scp.ranges),
+                                                angles=tuple(scp.angles), sill=scp.sill, nugget=scp.nugget),
+        radiuses=_int_radiuses(valid_radiuses), max_neighbours=max_neighbours, primary_mean=primary_data["mean"],
+        secondary_mean=secondary_data["mean"], correlation_coef=correlation_coef)
+    return _cokriging_call(2, grid, prop, secondary, out_prop, None, m2)
+
+
 def median_ik(prop, grid, marginal_probs, radiuses, max_neighbours, cov_model, *, precision: Optional[str] = None,
               refine_steps: int = 2):
     prop = _to_prop(prop)
@@ -393,6 +459,7 @@ def find_neighbours(prop, grid, radiuses, max_neighbours, cov_model, nodes, kind
 
 
 __all__ = ["ContProperty", "IndProperty", "SugarboxGrid", "CovarianceModel", "covariance", "ordinary_kriging",
-           "simple_kriging", "lvm_kriging", "median_ik", "indicator_kriging", "simple_kriging_weights", "calc_mean",
+           "simple_kriging", "lvm_kriging", "simple_cokriging_markI",
+           "simple_cokriging_markII", "median_ik", "indicator_kriging", "simple_kriging_weights", "calc_mean",
            "set_thread_num", "get_thread_num", "set_output_handler", "set_progress_handler", "set_precision",
            "find_neighbours", "ValidationError", "CriticalValidationError", "ValidationWarning"]

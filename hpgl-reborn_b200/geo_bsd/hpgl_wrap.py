@@ -75,6 +75,23 @@ class __hpgl_cov_params_t(C.Structure):
 _HPGL_COV_PARAMS = __hpgl_cov_params_t
 
 
+class __hpgl_cockriging_m1_params_t(C.Structure):
+    _fields_ = [("covariance_type", C.c_int), ("ranges", C.c_double * 3), ("angles", C.c_double * 3),
+                ("sill", C.c_double), ("nugget", C.c_double), ("radiuses", C.c_int * 3),
+                ("max_neighbours", C.c_int), ("primary_mean", C.c_double), ("secondary_mean", C.c_double),
+                ("secondary_variance", C.c_double), ("correlation_coef", C.c_double)]
+
+
+class __hpgl_cockriging_m2_params_t(C.Structure):
+    _fields_ = [("primary_cov_params", _HPGL_COV_PARAMS), ("secondary_cov_params", _HPGL_COV_PARAMS),
+                ("radiuses", C.c_int * 3), ("max_neighbours", C.c_int), ("primary_mean", C.c_double),
+                ("secondary_mean", C.c_double), ("correlation_coef", C.c_double)]
+
+
+_HPGL_COK_M1_PARAMS = __hpgl_cockriging_m1_params_t
+_HPGL_COK_M2_PARAMS = __hpgl_cockriging_m2_params_t
+
+
 class _HPGL_SGS_PARAMS(C.Structure):
     _fields_ = [("covariance_type", C.c_int), ("ranges", C.c_double * 3), ("angles", C.c_double * 3),
                 ("sill", C.c_double), ("nugget", C.c_double), ("radiuses", C.c_int * 3),
@@ -112,7 +129,8 @@ EXPORTS = [
     "hpgl_get_last_exception_message", "hpgl_set_output_handler", "hpgl_set_progress_handler",
     "hpgl_set_thread_num", "hpgl_get_thread_num", "hpgl_ordinary_kriging", "hpgl_simple_kriging",
     "hpgl_simple_kriging_weights", "hpgl_indicator_kriging", "hpgl_median_ik", "hpgl_lvm_kriging",
-    "hpgl_sgs_simulation", "hpgl_sgs_lvm_simulation",
+    "hpgl_sgs_simulation", "hpgl_sgs_lvm_simulation", "hpgl_simple_cokriging_mark1", "hpgl_simple_cokriging_mark2",
+    "hpgl_b200_cokriging_ex",
     "hpgl_b200_cont_kriging_ex", "hpgl_b200_lvm_kriging_ex", "hpgl_b200_sgs_ex", "hpgl_b200_sgs_draws", "hpgl_b200_indicator_kriging_ex", "hpgl_b200_median_ik_ex",
     "hpgl_b200_find_neighbours", "hpgl_b200_last_stats", "hpgl_b200_host_alloc", "hpgl_b200_host_free",
     "hpgl_b200_transform", "hpgl_b200_template", "hpgl_b200_covariance", "hpgl_b200_version",
@@ -176,6 +194,14 @@ def _load():
     lib.hpgl_b200_sgs_ex.restype = C.c_int
     lib.hpgl_b200_sgs_ex.argtypes = [i_p, vp, vp, vp, C.POINTER(_HPGL_NON_PARAMETRIC_CDF), vp,
                                      C.POINTER(_HPGL_SGS_PARAMS), C.POINTER(_HPGL_B200_OPTIONS)]
+    cma = C.POINTER(_HPGL_CONT_MASKED_ARRAY)
+    lib.hpgl_simple_cokriging_mark1.restype = None
+    lib.hpgl_simple_cokriging_mark1.argtypes = [cma, cma, C.POINTER(_HPGL_COK_M1_PARAMS), cma]
+    lib.hpgl_simple_cokriging_mark2.restype = None
+    lib.hpgl_simple_cokriging_mark2.argtypes = [cma, cma, C.POINTER(_HPGL_COK_M2_PARAMS), cma]
+    lib.hpgl_b200_cokriging_ex.restype = C.c_int
+    lib.hpgl_b200_cokriging_ex.argtypes = [C.c_int, i_p, vp, vp, vp, vp, C.POINTER(_HPGL_COK_M1_PARAMS),
+                                           C.POINTER(_HPGL_COK_M2_PARAMS), vp, vp, C.POINTER(_HPGL_B200_OPTIONS)]
     lib.hpgl_b200_sgs_draws.restype = C.c_int
     lib.hpgl_b200_sgs_draws.argtypes = [C.c_longlong, C.c_longlong, vp]
     lib.hpgl_b200_indicator_kriging_ex.restype = C.c_int

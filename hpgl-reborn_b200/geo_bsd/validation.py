@@ -161,6 +161,24 @@ class ParameterValidator:
             raise CriticalValidationError(f"Min neighbors {min_neighbors} is negative", "min_neighbors")
 
     @staticmethod
+    def validate_correlation_coef(coef, name: str = "correlation_coef") -> None:
+        if not isinstance(coef, (int, float)):
+            raise CriticalValidationError(f"{name} must be a number, got {type(coef).__name__}", name)
+        if math.isnan(coef) or math.isinf(coef):
+            raise CriticalValidationError(f"{name} must be finite, got {coef}", name)
+        if coef < -1.0 or coef > 1.0:
+            raise CriticalValidationError(f"{name} must be in [-1, 1] range, got {coef}", name)
+
+    @staticmethod
+    def validate_variance(variance, name: str = "variance") -> None:
+        if not isinstance(variance, (int, float)):
+            raise CriticalValidationError(f"{name} must be a number, got {type(variance).__name__}", name)
+        if math.isnan(variance) or math.isinf(variance):
+            raise CriticalValidationError(f"{name} must be finite, got {variance}", name)
+        if variance < 0:
+            raise CriticalValidationError(f"{name} must be non-negative, got {variance}", name)
+
+    @staticmethod
     def validate_seed(seed: int) -> None:
         if seed < ValidationConstants.MIN_SEED:
             validation_logger.warning(f"Seed value {seed} is negative")

@@ -67,6 +67,18 @@ struct hpgl_sgs_params_t {
     int m_covariance_type; double m_ranges[3]; double m_angles[3]; double m_sill; double m_nugget;
     int m_radiuses[3]; int m_max_neighbours; int m_kriging_kind; long m_seed; int m_min_neighbours;
 };
+/* api.h:122-135 */
+struct hpgl_cokriging_m1_params_t {
+    int m_covariance_type; double m_ranges[3]; double m_angles[3]; double m_sill; double m_nugget;
+    int m_radiuses[3]; int m_max_neighbours; double m_primary_mean; double m_secondary_mean;
+    double m_secondary_variance; double m_correlation_coef;
+};
+/* api.h:137-146 */
+struct hpgl_cokriging_m2_params_t {
+    struct hpgl_cov_params_t m_primary_cov_params; struct hpgl_cov_params_t m_secondary_cov_params;
+    int m_radiuses[3]; int m_max_neighbours; double m_primary_mean; double m_secondary_mean;
+    double m_correlation_coef;
+};
 /* api.h:148-153: ascending values with their cumulative probabilities */
 struct hpgl_non_parametric_cdf_t { float *m_values; float *m_probs; long long m_size; };
 
@@ -122,6 +134,20 @@ void hpgl_sgs_simulation(struct hpgl_cont_masked_array_t *data, struct hpgl_sgs_
 void hpgl_sgs_lvm_simulation(struct hpgl_cont_masked_array_t *data, struct hpgl_sgs_params_t *params,
                              struct hpgl_non_parametric_cdf_t *cdf, struct hpgl_float_array_t *means,
                              struct hpgl_ubyte_array_t *simulation_mask);
+
+/* Replaces api.h:297-303 / api.cpp:680-749 (simple_cokriging_markI.cpp:202-265):
+ * simple collocated cokriging, Markov model I, of every uninformed primary
+ * cell; every output cell ends informed (failures take pm + sv - sm). */
+void hpgl_simple_cokriging_mark1(struct hpgl_cont_masked_array_t *input_data,
+                                 struct hpgl_cont_masked_array_t *secondary_data,
+                                 struct hpgl_cokriging_m1_params_t *params,
+                                 struct hpgl_cont_masked_array_t *output_data);
+/* Replaces api.h:304-310 / api.cpp:751-815 (simple_cokriging_markI.cpp:267-330):
+ * Markov model II (the cross covariance from the secondary model). */
+void hpgl_simple_cokriging_mark2(struct hpgl_cont_masked_array_t *primary_data,
+                                 struct hpgl_cont_masked_array_t *secondary_data,
+                                 struct hpgl_cokriging_m2_params_t *params,
+                                 struct hpgl_cont_masked_array_t *output_data);
 
 /* ------------------------------------------------------------ _ex extensions */
 /* status codes */
@@ -180,6 +206,13 @@ int hpgl_b200_lvm_kriging_ex(const int *dims, const float *in_data, const unsign
 int hpgl_b200_sgs_ex(const int *dims, float *data, unsigned char *mask, const unsigned char *sim_mask,
                      const struct hpgl_non_parametric_cdf_t *cdf, const float *means,
                      const struct hpgl_sgs_params_t *params, const struct hpgl_b200_options_t *opt);
+/* Cokriging with options: mark 1 reads m1 (m2 may be NULL), mark 2 reads m2;
+ * arrays of dims' volume (device pointers under HPGL_B200_DEVICE_POINTERS);
+ * opt->status receives -1 informed, 0 kriged, 1 no neighbours, 2 singular. */
+int hpgl_b200_cokriging_ex(int mark, const int *dims, const float *pdata, const unsigned char *pmask,
+                           const float *sdata, const unsigned char *smask,
+                           const struct hpgl_cokriging_m1_params_t *m1, const struct hpgl_cokriging_m2_params_t *m2,
+                           float *out_data, unsigned char *out_mask, const struct hpgl_b200_options_t *opt);
 /* The simulation's uniform draws (host): out[i] = the i-th call of
  * std::uniform_real_distribution<double>(0, 1) on a std::mt19937 seeded with
  * `seed` (bs_random_generator.cpp:9-25), as sgs_simulation consumes them, one

@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <limits>
 #include <random>
 #include <vector>
 #include <omp.h>
@@ -621,6 +622,47 @@ struct NpCdf
         return x1 + (x2 - x1) / (y2 - y1) * (q - y1);
     }
 };
+
+// ---------------------------------------------------------------- cokriging
+// gauss_solve (gauss_solver.cpp:8-70): for column i the first unused row with a
+// non-zero entry is normalised and subtracted from every other unused row; it
+// fails when no row is found or the pivot is below machine epsilon.
+static bool gauss_solve_ref(std::vector<double> &A, std::vector<double> &B, std::vector<double> &X, int size)
+{
+    std::vector<int> flags(size, 0), order(size, 0);
+    for (int i = 0; i < size; ++i)
+    {
+        int row = -1;
+        for (int j = 0; j < size; ++j)
+            if (flags[j] == 0 && A[(size_t)j * size + i] != 0)
+            {
+                row = j;
+                flags[j] = 1;
+                order[i] = j;
+                break;
+            }
+        if (row < 0) return false;
+        double coef = A[(size_t)row * size + i];
+        if (std::abs(coef) < std::numeric_limits<double>::epsilon()) return false;
+        for (int j = i; j < size; ++j) A[(size_t)row * size + j] /= coef;
+        B[row] /= coef;
+        for (int j = 0; j < size; ++j)
+            if (flags[j] == 0)
+            {
+                double c = A[(size_t)j * size + i];
+                for (int k = i; k < size; ++k) A[(size_t)j * size + k] -= c * A[(size_t)row * size + k];
+                B[j] -= c * B[row];
+            }
+    }
+    X.assign(size, 0.0);
+    for (int i = size - 1; i >= 0; --i)
+    {
+        int row = order[i];
+        X[i] = B[row];
+        for (int j = size - 1; j > i; --j) X[i] -= A[(size_t)row * size + j] * X[j];
+    }
+    return true;
+}
 } // namespace ko
 
 using namespace ko;
@@ -1133,6 +1175,107 @@ int ko_sgs_path(long long size, long long seed, int *out, long long count)
     PathLcg path;
     if (!path.init(size, seed)) return -1;
     for (long long i = 0; i < count; ++i) out[i] = path.next();
+    return 0;
+}
+
+// Simple collocated cokriging, Markov models I and II
+// (simple_cokriging_markI.cpp:19-141, 202-330): for every uninformed cell, the
+// first max_nb informed primary cells of the analytic template (the
+// template-only lookup), the bordered system of primary covariances, the
+// collocated cross covariances coef * C(center, x_i) (Mark I: coef = rho
+// sqrt(secondary_variance) / sqrt(C(0)) on the primary model; Mark II: coef =
+// rho sqrt(C1(0) / C2(0)) on the secondary model, secondary variance C2(0)),
+// solved by gauss_solve; the float result accumulated in double per term
+// (combine, :83-106); on failure pm + sv - sm. Informed cells copy the
+// primary value; every output cell is informed. out_status: -1 informed,
+// 0 kriged, 1 no neighbours, 2 singular.
+int ko_cokriging(int mark, const int *dims, const float *pdata, const unsigned char *pmask, const float *sdata,
+                 const unsigned char *smask, int cov_type, const double *ranges, const double *angles, double sill,
+                 double nugget, int cov_type2, const double *ranges2, const double *angles2, double sill2,
+                 double nugget2, const int *radiuses, int max_nb, double primary_mean, double secondary_mean,
+                 double secondary_variance, double corr, float *out_data, unsigned char *out_mask, int *out_status,
+                 int n_threads)
+{
+    Grid g = {dims[0], dims[1], dims[2]};
+    Flavour fp, fs;
+    if (!make_flavour(fp, false, cov_type, ranges, angles, sill, nugget, radiuses)) return -1;
+    if (mark == 2 && !make_flavour(fs, false, cov_type2, ranges2, angles2, sill2, nugget2, radiuses)) return -1;
+    const double c0p = fp.at(0, 0, 0, 0, 0, 0);
+    double coef, sec_var;
+    const Flavour *fc;
+    if (mark == 1)
+    {
+        coef = c0p <= 0 ? 0.0 : corr * sqrt(secondary_variance) / sqrt(c0p);
+        sec_var = secondary_variance;
+        fc = &fp;
+    }
+    else
+    {
+        const double c0s = fs.at(0, 0, 0, 0, 0, 0);
+        coef = c0s <= 0 ? 0.0 : corr * sqrt(c0p / c0s);
+        sec_var = c0s;
+        fc = &fs;
+    }
+    const float pm = (float)primary_mean, sm = (float)secondary_mean; // mean_t is float
+    const std::vector<Off> tmpl = build_template(fp);
+    const long size = g.size();
+    if (n_threads > 0) omp_set_num_threads(n_threads);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (long i = 0; i < size; ++i)
+    {
+        if (pmask[i])
+        {
+            out_data[i] = pdata[i];
+            out_mask[i] = 1;
+            if (out_status) out_status[i] = -1;
+            continue;
+        }
+        const float sv = smask[i] ? sdata[i] : sm;
+        int x, y, z;
+        g.coord((int)i, x, y, z);
+        std::vector<int> idx;
+        for (size_t t = 0; t < tmpl.size() && (int)idx.size() < max_nb; ++t)
+        {
+            int q = g.index(x + tmpl[t].dx, y + tmpl[t].dy, z + tmpl[t].dz);
+            if (q >= 0 && pmask[q]) idx.push_back(q);
+        }
+        int status = 1;
+        float result = 0.0f;
+        if (!idx.empty())
+        {
+            const int n = (int)idx.size(), m = n + 1;
+            std::vector<int> xs(n), ys(n), zs(n);
+            for (int k = 0; k < n; ++k) g.coord(idx[k], xs[k], ys[k], zs[k]);
+            std::vector<double> A((size_t)m * m), B(m), W;
+            for (int a = 0; a < n; ++a)
+                for (int b = a; b < n; ++b)
+                {
+                    A[(size_t)a * m + b] = fp.at(xs[a], ys[a], zs[a], xs[b], ys[b], zs[b]);
+                    A[(size_t)b * m + a] = A[(size_t)a * m + b];
+                }
+            for (int a = 0; a < n; ++a)
+            {
+                A[(size_t)n * m + a] = coef * fc->at(x, y, z, xs[a], ys[a], zs[a]);
+                A[(size_t)a * m + n] = A[(size_t)n * m + a];
+                B[a] = fp.at(xs[a], ys[a], zs[a], x, y, z);
+            }
+            B[n] = coef * fc->at(0, 0, 0, 0, 0, 0);
+            A[(size_t)m * m - 1] = sec_var;
+            if (gauss_solve_ref(A, B, W, m))
+            {
+                status = 0;
+                result = pm;
+                for (int k = 0; k < n; ++k) result += (pdata[idx[k]] - pm) * W[k];
+                result += W[n] * (sv - sm);
+            }
+            else
+                status = 2;
+        }
+        if (status != 0) result = pm + sv - sm;
+        out_data[i] = result;
+        out_mask[i] = 1;
+        if (out_status) out_status[i] = status;
+    }
     return 0;
 }
 

@@ -70,6 +70,9 @@ def load(which: str):
                                C.c_double, _i, C.c_int, C.c_longlong, _i]
         lib.ko_sgs_path.argtypes = [C.c_longlong, C.c_longlong, _i, C.c_longlong]
         lib.ko_mt_draws.argtypes = [C.c_longlong, C.c_longlong, _d]
+        lib.ko_cokriging.argtypes = [C.c_int, _i, _f, _u8, _f, _u8, C.c_int, _d, _d, C.c_double, C.c_double, C.c_int,
+                                     _d, _d, C.c_double, C.c_double, _i, C.c_int, C.c_double, C.c_double,
+                                     C.c_double, C.c_double, _f, _u8, _i, C.c_int]
         lib.ko_template.argtypes = [C.c_int, C.c_int, _d, _d, C.c_double, C.c_double, _i, _i,
                                     C.c_int, _i]
         lib.ko_cov.argtypes = [C.c_int, C.c_int, _d, _d, C.c_double, C.c_double, _i, _i, _i]
@@ -330,6 +333,29 @@ def ref_sgs(dims, data, mask, cov, radiuses, k, seed, kind=1):
               float(cov.nugget), (C.c_int * 3)(*radiuses), int(k), int(kind), int(seed), 0)
     lib.hpgl_sgs_simulation(C.byref(a), C.byref(p), None, None, None)
     return od, om
+
+
+def cokriging(mark, dims, pdata, pmask, sdata, smask, cov, radiuses, k, primary_mean, secondary_mean,
+              secondary_variance=0.0, corr=0.0, cov2=None, threads=0):
+    """Collocated cokriging, Markov model I or II (port). Returns (data, mask, status)."""
+    lib = load("port")
+    n = int(np.prod(dims))
+    od = np.zeros(n, np.float32)
+    om = np.zeros(n, np.uint8)
+    st = np.zeros(n, np.int32)
+    c2 = cov2 if cov2 is not None else cov
+    rc = lib.ko_cokriging(int(mark), _ptr(_arr(dims, np.int32), _i), _ptr(_arr(pdata, np.float32), _f),
+                          _ptr(_arr(pmask, np.uint8), _u8), _ptr(_arr(sdata, np.float32), _f),
+                          _ptr(_arr(smask, np.uint8), _u8), int(cov.cov_type), _ptr(_arr(cov.ranges, np.float64), _d),
+                          _ptr(_arr(cov.angles, np.float64), _d), float(cov.sill), float(cov.nugget),
+                          int(c2.cov_type), _ptr(_arr(c2.ranges, np.float64), _d),
+                          _ptr(_arr(c2.angles, np.float64), _d), float(c2.sill), float(c2.nugget),
+                          _ptr(_arr(radiuses, np.int32), _i), int(k), float(primary_mean), float(secondary_mean),
+                          float(secondary_variance), float(corr), _ptr(od, _f), _ptr(om, _u8), _ptr(st, _i),
+                          int(threads))
+    if rc:
+        raise RuntimeError(f"cokriging failed (rc={rc})")
+    return od, om, st
 
 
 def mt_draws(seed, n):

@@ -7,6 +7,7 @@ harness libref_harness.so around its own templates):
     make -C oracle && python tests/golden/make_golden.py        (all fixtures)
                       python tests/golden/make_golden.py lvm    (lvm.npz only)
                       python tests/golden/make_golden.py sgs    (sgs.npz only)
+                      python tests/golden/make_golden.py cok    (cok.npz only)
 
 Inputs are the seeded workloads of geo_bsd.workloads at reduced scale (the
 conditioning cells are stored in each file, so the fixtures do not depend on
@@ -16,7 +17,7 @@ kriging_interpolation with result_t = double, the float estimate the drivers
 store, and the status code. Whole-grid outputs of the reference's public C API
 (hpgl_ordinary_kriging, hpgl_simple_kriging, hpgl_lvm_kriging,
 hpgl_indicator_kriging, hpgl_median_ik, hpgl_sgs_simulation,
-hpgl_sgs_lvm_simulation) are stored for the small grids, plus the known-answer cases
+hpgl_sgs_lvm_simulation, hpgl_simple_cokriging_mark1/2) are stored for the small grids, plus the known-answer cases
 of the reference's test suite (constant field 42, all zeros).
 """
 import ctypes as C
@@ -32,7 +33,7 @@ sys.path.insert(0, os.path.join(ROOT, "hpgl-reborn_b200"))
 
 import oracle as O  # noqa: E402
 sys.path.insert(0, os.path.dirname(HERE))
-from golden_io import SGS_CASES, sgs_inputs  # noqa: E402
+from golden_io import COK_CASES, SGS_CASES, cok_inputs, sgs_inputs  # noqa: E402
 from geo_bsd import workloads as WL  # noqa: E402  (pure python module)
 
 SAMPLE = 1200
@@ -168,6 +169,49 @@ def api_sgs(lib, dims, data, mask, cov, rad, k, seed, kind=1, sim_mask=None, cdf
     return od, om
 
 
+class CovP(C.Structure):
+    _fields_ = [("t", C.c_int), ("r", C.c_double * 3), ("a", C.c_double * 3), ("sill", C.c_double),
+                ("nugget", C.c_double)]
+
+
+class Cok1P(C.Structure):
+    _fields_ = [("t", C.c_int), ("r", C.c_double * 3), ("a", C.c_double * 3), ("sill", C.c_double),
+                ("nugget", C.c_double), ("rad", C.c_int * 3), ("k", C.c_int), ("pm", C.c_double), ("sm", C.c_double),
+                ("sv", C.c_double), ("corr", C.c_double)]
+
+
+class Cok2P(C.Structure):
+    _fields_ = [("pc", CovP), ("sc", CovP), ("rad", C.c_int * 3), ("k", C.c_int), ("pm", C.c_double),
+                ("sm", C.c_double), ("corr", C.c_double)]
+
+
+def _covp(c):
+    return CovP(c.cov_type, (C.c_double * 3)(*c.ranges), (C.c_double * 3)(*c.angles), c.sill, c.nugget)
+
+
+def api_cokriging(lib, mark, dims, pdata, pmask, sdata, smask, cov, rad, k, pm, sm, sv=0.0, corr=0.0, cov2=None):
+    """The reference's hpgl_simple_cokriging_mark1 / _mark2; returns the output data and mask."""
+    fp = C.POINTER(C.c_float)
+    up = C.POINTER(C.c_ubyte)
+    pd = np.ascontiguousarray(pdata, np.float32)
+    pmk = np.ascontiguousarray(pmask, np.uint8)
+    sd = np.ascontiguousarray(sdata, np.float32)
+    smk = np.ascontiguousarray(smask, np.uint8)
+    od = np.zeros_like(pd)
+    om = np.zeros_like(pmk)
+    a = Cont(pd.ctypes.data_as(fp), pmk.ctypes.data_as(up), _shape(dims))
+    b = Cont(sd.ctypes.data_as(fp), smk.ctypes.data_as(up), _shape(dims))
+    o = Cont(od.ctypes.data_as(fp), om.ctypes.data_as(up), _shape(dims))
+    if mark == 1:
+        p = Cok1P(cov.cov_type, (C.c_double * 3)(*cov.ranges), (C.c_double * 3)(*cov.angles), cov.sill, cov.nugget,
+                  (C.c_int * 3)(*rad), k, pm, sm, sv, corr)
+        lib.hpgl_simple_cokriging_mark1(C.byref(a), C.byref(b), C.byref(p), C.byref(o))
+    else:
+        p = Cok2P(_covp(cov), _covp(cov2), (C.c_int * 3)(*rad), k, pm, sm, corr)
+        lib.hpgl_simple_cokriging_mark2(C.byref(a), C.byref(b), C.byref(p), C.byref(o))
+    return od, om
+
+
 def api_ik(lib, dims, data, mask, covs, rads, ks, marginals):
     data = np.ascontiguousarray(data, np.uint8)
     mask = np.ascontiguousarray(mask, np.uint8)
@@ -265,8 +309,28 @@ def sgs_cases(lib):
     print("wrote sgs")
 
 
+def cok_cases(lib):
+    """The reference's hpgl_simple_cokriging_mark1 / _mark2 outputs, with the
+    secondary fields they were given."""
+    out = {}
+    for name, base, mark in COK_CASES:
+        g = dict(np.load(os.path.join(HERE, base + ".npz")))
+        x = cok_inputs(g, mark)
+        od, om = api_cokriging(lib, mark, x["dims"], x["pdata"], x["pmask"], x["sdata"], x["smask"], x["cov"],
+                               x["rad"], x["k"], x["pm"], x["sm"], sv=x["sv"], corr=x["corr"], cov2=x["cov2"])
+        out[f"{base}_sdata"] = x["sdata"]
+        out[f"{base}_smask"] = x["smask"]
+        out[f"{name}_data"] = od
+        out[f"{name}_mask"] = om
+    np.savez_compressed(os.path.join(HERE, "cok.npz"), **out)
+    print("wrote cok")
+
+
 def main(only=None):
     lib = _api()
+    if only == "cok":
+        cok_cases(lib)
+        return
     if only == "lvm":
         lvm_cases(lib)
         return
@@ -275,6 +339,7 @@ def main(only=None):
         return
     lvm_cases(lib)
     sgs_cases(lib)
+    cok_cases(lib)
     cont_case(lib, WL.ok_small(0.3), "ok_small_s030", grid_api=True)
     cont_case(lib, WL.sk_ok_large(0.16), "sk_ok_large_s016")
     cont_case(lib, WL.gauss_cv(0.2), "gauss_cv_s020", grid_api=True)

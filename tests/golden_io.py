@@ -78,3 +78,32 @@ def sgs_inputs(g, opts):
         out["data"] = np.zeros(n, np.float32)
         out["mask"] = np.zeros(n, np.uint8)
     return out
+
+
+COK_CASES = [
+    # name, base fixture, mark
+    ("m1_gauss", "gauss_cv_s020", 1),
+    ("m2_gauss", "gauss_cv_s020", 2),
+    ("m1_small", "ok_small_s030", 1),
+]
+COK_SECONDARY_COV = WL.CovSpec(WL.EXPONENTIAL, (20.0, 20.0, 5.0), (10.0, 0.0, 0.0), 1.5, 0.1)
+
+
+def cok_inputs(g, mark, secondary=None):
+    """Inputs of a cokriging golden case from its base fixture: the primary
+    data, a secondary field (from the fixture when given, else made: 0.6 times
+    the primary values plus seeded noise, informed on half of the cells) and
+    the parameters (primary mean of the data, secondary mean of the field)."""
+    dims, pdata, pmask = grid_inputs(g)
+    n = len(pdata)
+    if secondary is None:
+        rng = np.random.default_rng(4)
+        sdata = (0.6 * np.where(pmask == 1, pdata, 0) + rng.normal(size=n)).astype(np.float32)
+        smask = (rng.random(n) < 0.5).astype(np.uint8)
+    else:
+        sdata, smask = secondary
+    cov, rad, k = cov_of(g)
+    return {"dims": dims, "pdata": pdata, "pmask": pmask, "sdata": sdata, "smask": smask, "cov": cov, "rad": rad,
+            "k": k, "pm": float(pdata[pmask == 1].astype(np.float64).mean()),
+            "sm": float(sdata[smask == 1].astype(np.float64).mean()), "sv": 0.9, "corr": 0.6,
+            "cov2": COK_SECONDARY_COV if mark == 2 else None}

@@ -65,6 +65,13 @@ def test_struct_layouts_match_header():
                                                    "m_radiuses", "m_max_neighbours", "m_kriging_kind", "m_seed",
                                                    "m_min_neighbours"]),
         "hpgl_non_parametric_cdf_t": (W._HPGL_NON_PARAMETRIC_CDF, ["m_values", "m_probs", "m_size"]),
+        "hpgl_cokriging_m1_params_t": (W._HPGL_COK_M1_PARAMS, ["m_covariance_type", "m_ranges", "m_angles", "m_sill",
+                                                             "m_nugget", "m_radiuses", "m_max_neighbours",
+                                                             "m_primary_mean", "m_secondary_mean",
+                                                             "m_secondary_variance", "m_correlation_coef"]),
+        "hpgl_cokriging_m2_params_t": (W._HPGL_COK_M2_PARAMS, ["m_primary_cov_params", "m_secondary_cov_params",
+                                                             "m_radiuses", "m_max_neighbours", "m_primary_mean",
+                                                             "m_secondary_mean", "m_correlation_coef"]),
     }
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
     for s, (_, fl) in fields.items():
@@ -214,3 +221,16 @@ def test_sgs_draws_equal_the_standard_library(seed):
     got = np.zeros(n)
     assert W._hpgl_so.hpgl_b200_sgs_draws(seed, n, got.ctypes.data) == 0
     np.testing.assert_array_equal(got.view(np.uint64), O.mt_draws(seed, n).view(np.uint64))
+
+
+def test_cokriging_entry_argument_checks():
+    """A mark other than 1 or 2, or one without its parameters, is EINVAL before any device work."""
+    fn = W._hpgl_so.hpgl_b200_cokriging_ex
+    m1 = W._HPGL_COK_M1_PARAMS(covariance_type=0, ranges=(5.0, 5.0, 5.0), angles=(0.0, 0.0, 0.0), sill=1.0,
+                               nugget=0.0, radiuses=(3, 3, 3), max_neighbours=8, primary_mean=0.0, secondary_mean=0.0,
+                               secondary_variance=1.0, correlation_coef=0.5)
+    dims = (C.c_int * 3)(2, 2, 2)
+    assert fn(3, dims, None, None, None, None, C.byref(m1), None, None, None, None) == W.EINVAL
+    assert fn(2, dims, None, None, None, None, C.byref(m1), None, None, None, None) == W.EINVAL
+    assert fn(1, dims, None, None, None, None, C.byref(m1), None, None, None, None) == W.EINVAL  # null arrays
+

@@ -155,3 +155,15 @@ def test_introselect_matches_std_sort_first_k():
             keys = np.sort(keys)[::-1].copy()  # descending runs
         k = int(rng.integers(1, n + 1))
         assert O.select_check(keys, k), (n, k, distinct)
+
+
+@pytest.mark.parametrize("case", [c[0] for c in G.COK_CASES])
+def test_oracle_cokriging_matches_reference(case):
+    """Collocated cokriging: the restatement reproduces hpgl_simple_cokriging_mark1/2 bit for bit."""
+    _, base, mark = next(c for c in G.COK_CASES if c[0] == case)
+    ref = G.load("cok")
+    x = G.cok_inputs(G.load(base), mark, (ref[f"{base}_sdata"], ref[f"{base}_smask"]))
+    d, m, st = O.cokriging(mark, x["dims"], x["pdata"], x["pmask"], x["sdata"], x["smask"], x["cov"], x["rad"], x["k"],
+                           x["pm"], x["sm"], secondary_variance=x["sv"], corr=x["corr"], cov2=x["cov2"], threads=4)
+    np.testing.assert_array_equal(m, ref[f"{case}_mask"])
+    np.testing.assert_array_equal(d.view(np.uint32), ref[f"{case}_data"].view(np.uint32))
