@@ -14,7 +14,10 @@ and mask and the device->host copy of estimate, mask and variance.
 
 `--kind sk|lvm` runs simple kriging or kriging with a locally varying mean
 (a smooth trend, geo_bsd.workloads.lvm_means) on the same grid instead;
-`--kind sgs` times sequential Gaussian simulation (SK, k=32, seed 42) of every
+`--kind cok` times simple collocated cokriging (Markov model I, k=32) of that
+grid with a correlated secondary field informed on half of the cells, against
+the reference's own single-threaded hpgl_simple_cokriging_mark1 on a smaller
+grid of the same generator; `--kind sgs` times sequential Gaussian simulation (SK, k=32, seed 42) of every
 uninformed cell of that grid, against the reference's own single-threaded
 hpgl_sgs_simulation on a smaller grid of the same generator.
 
@@ -49,7 +52,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--workload", default="sk_ok_large")
-    ap.add_argument("--kind", choices=["ok", "sk", "lvm", "sgs"], default="ok")
+    ap.add_argument("--kind", choices=["ok", "sk", "lvm", "sgs", "cok"], default="ok")
     ap.add_argument("--skip-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--profile-case", type=float, default=0.0, metavar="SCALE",
@@ -378,11 +381,191 @@ def bench_sgs(args, rank, world, local):
         dist.destroy_process_group()
 
 
+COK_METRIC = "cokriged cells/s, 1 B200: simple collocated cokriging, Markov model I (k=32)"
+
+
+def cok_workload(scale):
+    """The kriging grid's generator with a secondary field: 0.6 x the primary
+    values plus seeded N(0,1) noise, informed on half of the cells."""
+    from geo_bsd import workloads as WL
+    wl = WL.sk_ok_large(scale)
+    rng = np.random.default_rng(4)
+    sdata = (0.6 * np.where(wl.mask == 1, wl.data, 0) + rng.normal(size=wl.n_cells)).astype(np.float32)
+    smask = (rng.random(wl.n_cells) < 0.5).astype(np.uint8)
+    pm = float(wl.data[wl.mask == 1].astype(np.float64).mean())
+    sm = float(sdata[smask == 1].astype(np.float64).mean())
+    return wl, sdata, smask, pm, sm
+
+
+def cok_reference(target_seconds):
+    """The reference's own cokriging (oracle/_ref/libhpgl.so, single-threaded as
+    it is) on a grid of the same generator sized for about target_seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    def run(scale):
+        wl, sd, smk, pm, sm = cok_workload(scale)
+        t0 = time.perf_counter()
+        O.ref_cokriging_mark1(wl.dims, wl.data, wl.mask, sd, smk, wl.cov, wl.radiuses, wl.max_neighbours, pm, sm,
+                              0.9, 0.6)
+        return wl, time.perf_counter() - t0
+
+    wl, dt = run(0.12)
+    rate = int((wl.mask == 0).sum()) / max(dt, 1e-3)
+    scale = min(1.0, max(0.12, (rate * target_seconds / (256 * 256 * 128)) ** (1.0 / 3.0)))
+    wl, dt = run(scale)
+    cells = int((wl.mask == 0).sum())
+    return cells / dt, {"dims": wl.dims, "cells": cells, "seconds": dt}
+
+
+def bench_cok(args, rank, world, local):
+    import torch
+    if args.impl == "reference":
+        if rank == 0:
+            vals, info = [], None
+            for i in range(args.warmup + args.steps):
+                v, info = cok_reference(min(args.cpu_seconds, 2.0))
+                if i >= args.warmup:
+                    vals.append(v)
+            value = float(np.median(vals))
+            d = "x".join(str(x) for x in info["dims"])
+            print(json.dumps({"impl": "reference", "metric": COK_METRIC, "value": value, "unit": UNIT,
+                              "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                              "data": "synthetic (seeded, geo_bsd.workloads)",
+                              "config": {"workload": f"cokriging Markov I k=32 on a {d} grid of the 256x256x128 "
+                                                     "generator"},
+                              "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                                               "sample": f"whole {d} grid ({info['cells']} cells) per step; the "
+                                                         "reference's cokriging is single-threaded"},
+                              "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist_mod
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+        dist = dist_mod
+    from geo_bsd import hpgl_wrap as W
+    wl, sdata, smask, pm, sm = cok_workload(args.profile_case if args.profile_case > 0 else 1.0)
+    n = wl.n_cells
+    dev = torch.device("cuda", local)
+    arrays = [torch.from_numpy(np.ascontiguousarray(v)).to(dev) for v in (wl.data, wl.mask, sdata, smask)]
+    d_out = torch.empty(n, dtype=torch.float32, device=dev)
+    d_om = torch.empty(n, dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+    dims = (C.c_int * 3)(*wl.dims)
+    c = wl.cov
+    p = W._HPGL_COK_M1_PARAMS(covariance_type=c.cov_type, ranges=c.ranges, angles=c.angles, sill=c.sill,
+                              nugget=c.nugget, radiuses=wl.radiuses, max_neighbours=wl.max_neighbours,
+                              primary_mean=pm, secondary_mean=sm, secondary_variance=0.9, correlation_coef=0.6)
+
+    def call(ptrs, out, om, flags, strm):
+        o = W._HPGL_B200_OPTIONS(precision=0, refine_steps=0, flags=flags, stream=strm, estimate64=None,
+                                 variance=None, status=None, ik_probs=None)
+        rc = W._hpgl_so.hpgl_b200_cokriging_ex(1, dims, *ptrs, C.byref(p), None, out, om, C.byref(o))
+        W.check(rc, "cokriging_ex")
+        return W.last_stats()
+
+    def dev_call():
+        return call([a.data_ptr() for a in arrays], d_out.data_ptr(), d_om.data_ptr(), W.FLAG_DEVICE_POINTERS,
+                    stream.cuda_stream)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    if args.profile_case > 0:
+        st = dev_call()
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_case": wl.dims, "stats": st}), flush=True)
+        return
+    for _ in range(args.warmup):
+        dev_call()
+    times, stats = [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            barrier()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st = dev_call()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+            stats.append(st)
+    barrier()
+    ms = max_over_ranks(float(np.mean(times)))
+    last = stats[-1]
+    value = last["kriged_cells"] * world / (ms / 1e3)
+    # end to end with pinned host buffers
+    lib = W._hpgl_so
+    sizes = (n * 4, n, n * 4, n, n * 4, n)
+    h = [lib.hpgl_b200_host_alloc(sz) for sz in sizes]
+    for ptr, src, sz in zip(h[:4], (wl.data, wl.mask, sdata, smask), sizes[:4]):
+        C.memmove(ptr, np.ascontiguousarray(src).ctypes.data, sz)
+    for _ in range(args.warmup):
+        call(h[:4], h[4], h[5], 0, None)
+    e2e_t = []
+    for _ in range(args.steps):
+        barrier()
+        t0 = time.perf_counter()
+        st = call(h[:4], h[4], h[5], 0, None)
+        e2e_t.append(time.perf_counter() - t0)
+    barrier()
+    e2e_value = st["kriged_cells"] * world / max_over_ranks(float(np.mean(e2e_t)))
+    for ptr in h:
+        lib.hpgl_b200_host_free(ptr)
+    cpu = None
+    if rank == 0 and not args.skip_cpu_baseline:
+        v, info = cok_reference(args.cpu_seconds)
+        d = "x".join(str(x) for x in info["dims"])
+        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "reference",
+               "sample": f"the reference's hpgl_simple_cokriging_mark1 of a {d} grid of the same generator "
+                         f"({info['cells']} cells, {info['seconds']:.1f} s); single-threaded as the reference is"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": COK_METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, geo_bsd.workloads)",
+            "config": {"workload": f"cokriging Markov I {wl.dims[0]}x{wl.dims[1]}x{wl.dims[2]}, 1% lognormal "
+                                   f"conditioning, exponential (30,15,6) az 30, secondary 0.6 x primary + N(0,1) "
+                                   f"on half the cells, rho 0.6, k={wl.max_neighbours}",
+                       "l2": "flushed between timed steps (256 MB write)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "stages_ms": {k[len("stage_"):-len("_ms")]: round(v, 3) for k, v in last.items() if k.startswith("stage_")},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(st["h2d_bytes"]),
+                    "d2h_bytes_per_step": int(st["d2h_bytes"]), "timing": "wall clock per call"},
+            "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
+            "clocks": clk.summary(),
+        }), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
     if args.kind == "sgs":
         bench_sgs(args, rank, world, local)
+        return
+    if args.kind == "cok":
+        bench_cok(args, rank, world, local)
         return
     import torch
 

@@ -358,6 +358,36 @@ def cokriging(mark, dims, pdata, pmask, sdata, smask, cov, radiuses, k, primary_
     return od, om, st
 
 
+class _CovP(C.Structure):
+    _fields_ = [("t", C.c_int), ("r", C.c_double * 3), ("a", C.c_double * 3), ("sill", C.c_double),
+                ("nugget", C.c_double)]
+
+
+class _Cok1P(C.Structure):
+    _fields_ = [("t", C.c_int), ("r", C.c_double * 3), ("a", C.c_double * 3), ("sill", C.c_double),
+                ("nugget", C.c_double), ("rad", C.c_int * 3), ("k", C.c_int), ("pm", C.c_double), ("sm", C.c_double),
+                ("sv", C.c_double), ("corr", C.c_double)]
+
+
+def ref_cokriging_mark1(dims, pdata, pmask, sdata, smask, cov, radiuses, k, pm, sm, sv, corr):
+    """The reference's hpgl_simple_cokriging_mark1; returns (data, mask)."""
+    lib = ref_api()
+    pd = _arr(pdata, np.float32)
+    pmk = _arr(pmask, np.uint8)
+    sd = _arr(sdata, np.float32)
+    smk = _arr(smask, np.uint8)
+    od = np.zeros_like(pd)
+    om = np.zeros_like(pmk)
+    sh = _Shape((C.c_int * 3)(*dims), (C.c_int * 3)(1, dims[0], dims[0] * dims[1]))
+    a = _Cont(pd.ctypes.data_as(_f), pmk.ctypes.data_as(_u8), sh)
+    b = _Cont(sd.ctypes.data_as(_f), smk.ctypes.data_as(_u8), sh)
+    o = _Cont(od.ctypes.data_as(_f), om.ctypes.data_as(_u8), sh)
+    p = _Cok1P(int(cov.cov_type), (C.c_double * 3)(*cov.ranges), (C.c_double * 3)(*cov.angles), float(cov.sill),
+               float(cov.nugget), (C.c_int * 3)(*radiuses), int(k), float(pm), float(sm), float(sv), float(corr))
+    lib.hpgl_simple_cokriging_mark1(C.byref(a), C.byref(b), C.byref(p), C.byref(o))
+    return od, om
+
+
 def mt_draws(seed, n):
     """std::mt19937 + uniform_real_distribution<double>(0, 1) draws (the standard library)."""
     lib = load("port")
