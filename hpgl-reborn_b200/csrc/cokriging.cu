@@ -2,8 +2,8 @@
 // (simple_cokriging_markI.cpp:19-330).
 //
 // Every uninformed cell is kriged from the first max_nb informed primary cells
-// of the analytic search template (the search kernel of the simulation, with a
-// fixed predicate) and the collocated secondary value. The bordered system
+// of the analytic search template (the kriging path's template search over the
+// informed-cell bitmap, run for every bin) and the collocated secondary value. The bordered system
 //   [ A   c ] [w ]   [ b   ]
 //   [ c^T s ] [wn] = [ b_n ]
 // (A, b: primary covariances; c: the cross covariances of the target with the
@@ -22,14 +22,11 @@
 
 namespace hb
 {
-__global__ void k_cok_prepare(long long n, const uint8_t *__restrict__ pmask, int *__restrict__ rank_of,
-                              int *__restrict__ flag)
+// flag[i] = 1 for the targets (uninformed primary cells)
+__global__ void k_cok_prepare(long long n, const uint8_t *__restrict__ pmask, int *__restrict__ flag)
 {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    {
-        rank_of[i] = pmask[i] ? -1 : INT_MAX;
         flag[i] = pmask[i] ? 0 : 1;
-    }
 }
 
 __global__ void k_cok_targets(long long n, const int *__restrict__ flag, const int *__restrict__ pos,
@@ -58,8 +55,8 @@ struct CokArgsDev
     Geom g;
     const int *targets;
     int n_targets;
-    const int *nb;
-    const int *nb_cnt;
+    const int2 *nb_rec; // per cell and slot: {pair-table offset, value bits}
+    const int *nb_n;    // per cell
     int k;
     const double *pair64;
     const double *cross_tab;
@@ -72,8 +69,12 @@ struct CokArgsDev
     signed char *status;
 };
 
-__device__ __forceinline__ int cross_index(const Geom &g, int dx, int dy, int dz)
+// the cross table's entry of a neighbour given by its pair-table offset
+__device__ __forceinline__ int cross_index_of_lin(const Geom &g, int lin)
 {
+    const long long i = g.pair_center + lin;
+    const int dx = (int)(i % g.pnx) - g.phx, dy = (int)((i / g.pnx) % g.pny) - g.phy,
+              dz = (int)(i / ((long long)g.pnx * g.pny)) - g.phz;
     return ((dz + g.rz) * (2 * g.ry + 1) + (dy + g.ry)) * (2 * g.rx + 1) + (dx + g.rx);
 }
 
@@ -107,27 +108,24 @@ __global__ void __launch_bounds__(kCokThreads, 1) k_cok_solve_fold(const CokArgs
         const int it = it0 + h;
         const bool valid = it < a.n_targets;
         const int cell = valid ? a.targets[it] : 0;
-        const int n = valid ? a.nb_cnt[it] : 0;
-        const int cx = cell % g.nx, cy = (int)((cell / g.nx) % g.ny), cz = (int)(cell / ((long long)g.nx * g.ny));
+        const int n = valid ? a.nb_n[cell] : 0;
         const bool live_a = t < n, live_b = rb < n;
         int lin_a = 0, lin_b = 0;
         float va = 0.0f, vb = 0.0f;
         double c_a = 0.0, c_b = 0.0;
         if (live_a)
         {
-            const int q = a.nb[(long long)it * a.k + t];
-            const int dx = q % g.nx - cx, dy = (int)((q / g.nx) % g.ny) - cy, dz = (int)(q / ((long long)g.nx * g.ny)) - cz;
-            lin_a = pair_lin(g, dx, dy, dz);
-            c_a = __dmul_rn(a.p.coef, a.cross_tab[cross_index(g, dx, dy, dz)]);
-            va = a.pdata[q];
+            const int2 rec = a.nb_rec[(long long)cell * a.k + t];
+            lin_a = rec.x;
+            va = __int_as_float(rec.y);
+            c_a = __dmul_rn(a.p.coef, a.cross_tab[cross_index_of_lin(g, lin_a)]);
         }
         if (live_b)
         {
-            const int q = a.nb[(long long)it * a.k + rb];
-            const int dx = q % g.nx - cx, dy = (int)((q / g.nx) % g.ny) - cy, dz = (int)(q / ((long long)g.nx * g.ny)) - cz;
-            lin_b = pair_lin(g, dx, dy, dz);
-            c_b = __dmul_rn(a.p.coef, a.cross_tab[cross_index(g, dx, dy, dz)]);
-            vb = a.pdata[q];
+            const int2 rec = a.nb_rec[(long long)cell * a.k + rb];
+            lin_b = rec.x;
+            vb = __int_as_float(rec.y);
+            c_b = __dmul_rn(a.p.coef, a.cross_tab[cross_index_of_lin(g, lin_b)]);
         }
         const float sv = valid ? (a.smask[cell] ? a.sdata[cell] : a.p.sm) : 0.0f;
         LIN[t] = lin_a;
@@ -185,24 +183,19 @@ __global__ void __launch_bounds__(kCokBlockThreads) k_cok_solve_block(const CokA
     for (int it = blockIdx.x; it < a.n_targets; it += gridDim.x)
     {
         const int cell = a.targets[it];
-        const int n = a.nb_cnt[it];
-        const int cx = cell % g.nx, cy = (int)((cell / g.nx) % g.ny), cz = (int)(cell / ((long long)g.nx * g.ny));
-        const int *row = a.nb + (long long)it * kk;
+        const int n = a.nb_n[cell];
+        const int2 *row = a.nb_rec + (long long)cell * kk;
         for (int e = threadIdx.x; e < n * n; e += blockDim.x)
         {
             const int i = e / n, j = e % n;
-            const int qi = row[i], qj = row[j];
-            const int dx = qi % g.nx - qj % g.nx, dy = (int)((qi / g.nx) % g.ny) - (int)((qj / g.nx) % g.ny),
-                      dz = (int)(qi / ((long long)g.nx * g.ny)) - (int)(qj / ((long long)g.nx * g.ny));
-            A[(size_t)i * n + j] = a.pair64[pc + pair_lin(g, dx, dy, dz)];
+            A[(size_t)i * n + j] = a.pair64[pc + row[i].x - row[j].x];
         }
         for (int i = threadIdx.x; i < n; i += blockDim.x)
         {
-            const int q = row[i];
-            const int dx = q % g.nx - cx, dy = (int)((q / g.nx) % g.ny) - cy, dz = (int)(q / ((long long)g.nx * g.ny)) - cz;
-            b[i] = a.pair64[pc + pair_lin(g, dx, dy, dz)];
-            c[i] = __dmul_rn(a.p.coef, a.cross_tab[cross_index(g, dx, dy, dz)]);
-            vals[i] = a.pdata[q];
+            const int2 rec = row[i];
+            b[i] = a.pair64[pc + rec.x];
+            c[i] = __dmul_rn(a.p.coef, a.cross_tab[cross_index_of_lin(g, rec.x)]);
+            vals[i] = __int_as_float(rec.y);
         }
         if (threadIdx.x == 0) s_fail = 0;
         __syncthreads();
@@ -271,9 +264,9 @@ __global__ void __launch_bounds__(kCokBlockThreads) k_cok_solve_block(const CokA
     }
 }
 
-void launch_cok_prepare(long long n, const uint8_t *pmask, int *rank_of, int *flag, cudaStream_t st)
+void launch_cok_prepare(long long n, const uint8_t *pmask, int *flag, cudaStream_t st)
 {
-    k_cok_prepare<<<1184, 256, 0, st>>>(n, pmask, rank_of, flag);
+    k_cok_prepare<<<1184, 256, 0, st>>>(n, pmask, flag);
 }
 void launch_cok_targets(long long n, const int *flag, const int *pos, int *targets, cudaStream_t st)
 {
@@ -285,13 +278,13 @@ void launch_cok_finalize(long long n, const float *pdata, const uint8_t *pmask, 
     k_cok_finalize<<<1184, 256, 0, st>>>(n, pdata, pmask, out_data, out_mask, status);
 }
 
-cudaError_t launch_cok_solve(const Geom &g, const int *targets, int n_targets, const int *nb, const int *nb_cnt,
+cudaError_t launch_cok_solve(const Geom &g, const int *targets, int n_targets, const int2 *nb_rec, const int *nb_n,
                              int k, const double *pair64, const double *cross_tab, const float *pdata,
                              const float *sdata, const uint8_t *smask, const CokParams &p, float *out_data,
                              uint8_t *out_mask, signed char *status, int n_sm, cudaStream_t st)
 {
     if (n_targets <= 0) return cudaSuccess;
-    CokArgsDev a{g, targets, n_targets, nb, nb_cnt, k, pair64, cross_tab, pdata, sdata, smask, p, out_data, out_mask,
+    CokArgsDev a{g, targets, n_targets, nb_rec, nb_n, k, pair64, cross_tab, pdata, sdata, smask, p, out_data, out_mask,
                  status};
     if (k <= 32)
     {

@@ -1293,13 +1293,12 @@ int cokriging(const int *dims, const float *pdata, const unsigned char *pmask, c
         E.mark(STAGE_UPLOAD, st);
 
         // targets: the uninformed primary cells in ascending order
-        int *rank_of = E.buf<int>("cok_rank_of", (size_t)n);
         int *flag = E.buf<int>("cok_flag", (size_t)n);
         int *pos = E.buf<int>("cok_pos", (size_t)n);
         int *tmp = E.buf<int>("scan_tmp", (size_t)scan_tmp_ints(n) + 4);
         int *total = E.buf<int>("cok_total", 1);
         int *targets = E.buf<int>("cok_targets", (size_t)n);
-        launch_cok_prepare(n, d_pm, rank_of, flag, st);
+        launch_cok_prepare(n, d_pm, flag, st);
         HB_CK(cudaMemcpyAsync(pos, flag, n * 4, cudaMemcpyDeviceToDevice, st));
         exclusive_scan(pos, n, tmp, total, st);
         launch_cok_targets(n, flag, pos, targets, st);
@@ -1355,26 +1354,42 @@ int cokriging(const int *dims, const float *pdata, const unsigned char *pmask, c
                     cross[((size_t)(dz + g.rz) * by + (dy + g.ry)) * bx + (dx + g.rx)] = fs.at_offset(dx, dy, dz);
         double *d_cross = E.buf<double>("cok_cross", cross.size());
         HB_CK(cudaMemcpyAsync(d_cross, cross.data(), cross.size() * 8, cudaMemcpyHostToDevice, st));
+        // the template search over the informed-cell bitmap of the grid padded by
+        // the radiuses, for every bin (the reference's lookup here is the template
+        // scan alone); its linear offsets are 32-bit
+        const long long PX = g.nx + 2LL * g.rx, PY = g.ny + 2LL * g.ry;
+        if ((long long)g.rz * PY * PX + (long long)g.ry * PX + g.rx > 2147483647LL)
+            throw CudaFail{-4, "grid too large for the template search at these radiuses"};
         std::vector<int4> t4(tv.size());
-        for (size_t i = 0; i < tv.size(); ++i) t4[i] = make_int4(tv[i].dx, tv[i].dy, tv[i].dz, 0);
-        int4 *tmpl = E.buf<int4>("sgs_tmpl", std::max<size_t>(t4.size(), 1));
+        for (size_t i = 0; i < tv.size(); ++i)
+            t4[i] = make_int4(tv[i].dx, tv[i].dy, tv[i].dz, template_padded_offset(g, tv[i].dx, tv[i].dy, tv[i].dz));
+        int4 *tmpl = E.buf<int4>("tmpl", std::max<size_t>(t4.size(), 1));
         if (!t4.empty())
             HB_CK(cudaMemcpyAsync(tmpl, t4.data(), t4.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+        std::vector<int> all_bins(g.n_bins);
+        for (int b = 0; b < g.n_bins; ++b) all_bins[b] = b;
+        int *tmpl_bins = E.buf<int>("tmpl_bins", (size_t)g.n_bins);
+        HB_CK(cudaMemcpyAsync(tmpl_bins, all_bins.data(), (size_t)g.n_bins * 4, cudaMemcpyHostToDevice, st));
         HB_CK(cudaStreamSynchronize(st)); // host temporaries
         E.stats.launches += 1;
         E.mark(STAGE_TABLES, st);
 
         const int k = a.max_nb;
-        int *nb = E.buf<int>("cok_nb", (size_t)std::max(n_t, 1) * k);
-        int *nb_cnt = E.buf<int>("cok_nb_cnt", (size_t)std::max(n_t, 1));
+        DevPoints P = compact_points(E, grid_geom(dims), d_pm, d_pd, nullptr, st);
+        E.stats.launches += 2 + scan_kernels(n);
+        int2 *nb_rec = E.buf<int2>("nb_rec", (size_t)n * k);
+        int *nb_n = E.buf<int>("nb_n", (size_t)n);
+        int *tcount = E.buf<int>("cok_tcount", 1);
+        HB_CK(cudaMemsetAsync(tcount, 0, 4, st));
         if (n_t > 0)
         {
-            launch_sgs_search(g, tmpl, (int)t4.size(), targets, n_t, rank_of, k, nb, nullptr, nb_cnt, E.n_sm(), st, 0);
-            E.stats.launches += 1;
+            HB_CK(launch_search_template(g, d_pm, E.buf<uint32_t>("mask_bits", (size_t)(template_padded_cells(g) + 31) / 32),
+                                         0, tmpl_bins, g.n_bins, P.pts_val, tmpl, (int)t4.size(), P.pid_of_node,
+                                         nullptr, nb_rec, nb_n, tcount, E.n_sm(), st));
+            E.stats.launches += 2;
         }
-        HB_CK(cudaGetLastError());
         E.mark(STAGE_SEARCH, st);
-        HB_CK(launch_cok_solve(g, targets, n_t, nb, nb_cnt, k, pair64, d_cross, d_pd, d_sd, d_sm, cp, d_out, d_omask,
+        HB_CK(launch_cok_solve(g, targets, n_t, nb_rec, nb_n, k, pair64, d_cross, d_pd, d_sd, d_sm, cp, d_out, d_omask,
                                d_status, E.n_sm(), st));
         if (n_t > 0) E.stats.launches += 1;
         E.mark(STAGE_SOLVE, st);

@@ -165,10 +165,11 @@ struct CokParams
     double b_last;  // coef * C_cross(0), b[n]
     float pm, sm;   // primary and secondary means (float, as the reference stores them)
 };
-void launch_cok_prepare(long long n, const uint8_t *pmask, int *rank_of, int *flag, cudaStream_t st);
+void launch_cok_prepare(long long n, const uint8_t *pmask, int *flag, cudaStream_t st);
 void launch_cok_targets(long long n, const int *flag, const int *pos, int *targets, cudaStream_t st);
 // cross_tab: the cross model over the +-radius box, x fastest
-cudaError_t launch_cok_solve(const Geom &g, const int *targets, int n_targets, const int *nb, const int *nb_cnt,
+// nb_rec / nb_n: the kriging search's per-cell neighbour records and counts
+cudaError_t launch_cok_solve(const Geom &g, const int *targets, int n_targets, const int2 *nb_rec, const int *nb_n,
                              int k, const double *pair64, const double *cross_tab, const float *pdata,
                              const float *sdata, const uint8_t *smask, const CokParams &p, float *out_data,
                              uint8_t *out_mask, signed char *status, int n_sm, cudaStream_t st);
