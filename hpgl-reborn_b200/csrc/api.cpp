@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -211,6 +212,29 @@ bool cok_shapes(const char *fn, const hpgl_shape_t *a, const hpgl_shape_t *b, co
     return true;
 }
 
+// init_remap_table (api.cpp:143-167): the given values when there is one per
+// indicator (the first indicator_count of more, with a warning), else 0, 1, 2 ...
+std::vector<unsigned char> remap_table(const unsigned char *values, int values_count, int indicator_count)
+{
+    std::vector<unsigned char> t;
+    if (values_count == indicator_count)
+        t.assign(values, values + values_count);
+    else if (values_count > indicator_count)
+    {
+        emit("Given " + std::to_string(values_count) + " values for " + std::to_string(indicator_count) +
+             " indicators. Ignoring extra values.\n");
+        t.assign(values, values + indicator_count);
+    }
+    else
+    {
+        if (values_count > 0)
+            emit("Warning: Given " + std::to_string(values_count) + " values for " + std::to_string(indicator_count) +
+                 " indicators. Ignoring values. Using [0, 1, 2 ..]\n");
+        for (int i = 0; i < indicator_count; ++i) t.push_back((unsigned char)i);
+    }
+    return t;
+}
+
 hb::Options options_from(const hpgl_b200_options_t *o)
 {
     hb::Options r;
@@ -403,6 +427,125 @@ void hpgl_simple_cokriging_mark2(hpgl_cont_masked_array_t *primary_data, hpgl_co
     if (hb::cokriging(dims, primary_data->m_data, primary_data->m_mask, secondary_data->m_data,
                       secondary_data->m_mask, a, output_data->m_data, output_data->m_mask, opt) == 0)
         report_done("Simple Colocated Cokriging Markov Model II");
+}
+
+int hpgl_read_inc_file_float(char *filename, float undefined_value, int size, float *data, unsigned char *mask)
+{
+    try
+    {
+        if (!filename || !data || size < 0) throw std::runtime_error("hpgl_read_inc_file_float: bad argument");
+        hb::read_inc_float(filename, undefined_value, size, data, mask);
+        return 0;
+    }
+    catch (const std::exception &ex)
+    {
+        hb::set_error(ex.what());
+        return -1;
+    }
+}
+
+int hpgl_read_inc_file_byte(char *filename, int undefined_value, int size, unsigned char *data, unsigned char *mask,
+                            unsigned char *values, int values_count)
+{
+    try
+    {
+        if (!filename || !data || !mask || size < 0 || (values_count > 0 && !values))
+            throw std::runtime_error("hpgl_read_inc_file_byte: bad argument");
+        hb::read_inc_byte(filename, undefined_value, size, data, mask);
+        // values -> category indices (api.cpp:95-108): the first matching entry
+        for (int i = 0; i < size; ++i)
+            if (mask[i] != 0)
+                for (int j = 0; j < values_count; ++j)
+                    if (data[i] == values[j])
+                    {
+                        data[i] = (unsigned char)j;
+                        break;
+                    }
+        return 0;
+    }
+    catch (const std::exception &ex)
+    {
+        hb::set_error(ex.what());
+        return -1;
+    }
+}
+
+int hpgl_write_inc_file_float(char *filename, hpgl_cont_masked_array_t *arr, float undefined_value, char *name)
+{
+    try
+    {
+        if (!filename || !arr || !name) throw std::runtime_error("hpgl_write_inc_file_float: bad argument");
+        int dims[3];
+        if (!shape_dims(&arr->m_shape, dims)) return -1;
+        hb::write_inc_float(filename, name, arr->m_data, arr->m_mask, (long long)dims[0] * dims[1] * dims[2],
+                            undefined_value, false);
+        return 0;
+    }
+    catch (const std::exception &ex)
+    {
+        hb::set_error(ex.what());
+        return -1;
+    }
+}
+
+int hpgl_write_inc_file_byte(char *filename, hpgl_ind_masked_array_t *arr, int undefined_value, char *name,
+                             unsigned char *values, int values_count)
+{
+    try
+    {
+        if (!filename || !arr || !name) throw std::runtime_error("hpgl_write_inc_file_byte: bad argument");
+        int dims[3];
+        if (!shape_dims(&arr->m_shape, dims)) return -1;
+        hb::write_inc_byte(filename, name, arr->m_data, arr->m_mask, (long long)dims[0] * dims[1] * dims[2],
+                           (unsigned char)undefined_value, remap_table(values, values_count, arr->m_indicator_count),
+                           false);
+        return 0;
+    }
+    catch (const std::exception &ex)
+    {
+        hb::set_error(ex.what());
+        return -1;
+    }
+}
+
+int hpgl_write_gslib_cont_property(hpgl_cont_masked_array_t *data, const char *filename, const char *name,
+                                   double undefined_value)
+{
+    try
+    {
+        if (!filename || !data || !name) throw std::runtime_error("hpgl_write_gslib_cont_property: bad argument");
+        int dims[3];
+        if (!shape_dims(&data->m_shape, dims)) return -1;
+        // the undefined value passes through cont_value_t (float), property_writer.cpp:95-99
+        hb::write_inc_float(filename, name, data->m_data, data->m_mask, (long long)dims[0] * dims[1] * dims[2],
+                            (float)undefined_value, true);
+        return 0;
+    }
+    catch (const std::exception &ex)
+    {
+        hb::set_error(ex.what());
+        return -1;
+    }
+}
+
+int hpgl_write_gslib_byte_property(hpgl_ind_masked_array_t *data, const char *filename, const char *name,
+                                   double undefined_value, unsigned char *values, int values_count)
+{
+    try
+    {
+        if (!filename || !data || !name) throw std::runtime_error("hpgl_write_gslib_byte_property: bad argument");
+        int dims[3];
+        if (!shape_dims(&data->m_shape, dims)) return -1;
+        hb::write_inc_byte(filename, name, data->m_data, data->m_mask, (long long)dims[0] * dims[1] * dims[2],
+                           (unsigned char)undefined_value, remap_table(values, values_count, data->m_indicator_count),
+                           true);
+        return 0;
+    }
+    catch (const std::exception &ex)
+    {
+        hb::set_error(ex.what());
+        return -1;
+    }
 }
 
 int hpgl_simple_kriging_weights(float *center_coords, float *neighbours_x, float *neighbours_y,

@@ -148,6 +148,16 @@ double host_covariance(int kind, int cov_type, const double *ranges, const doubl
                        double nugget, const int *radiuses, const int *a, const int *b);
 int sk_weights(const double *center, const double *xs, const double *ys, const double *zs, int n, int cov_type,
                const double *ranges, const double *angles, double sill, double nugget, double *out_w);
+// Property files (inc_io.cpp): INC (read_inc_file.cpp, property_writer.cpp)
+// and GSLIB (property_writer.cpp:87-140). Failures throw std::runtime_error
+// with the reference's messages.
+void read_inc_float(const char *path, float undefined_value, long long size, float *data, unsigned char *mask);
+void read_inc_byte(const char *path, int undefined_value, long long size, unsigned char *data, unsigned char *mask);
+void write_inc_float(const char *path, const char *name, const float *data, const unsigned char *mask,
+                     long long size, float undefined_value, bool gslib);
+void write_inc_byte(const char *path, const char *name, const unsigned char *data, const unsigned char *mask,
+                    long long size, unsigned char undefined_value, const std::vector<unsigned char> &remap,
+                    bool gslib);
 void *host_alloc(size_t bytes);
 void host_free(void *p);
 } // namespace hb

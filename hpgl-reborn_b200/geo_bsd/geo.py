@@ -22,7 +22,7 @@ from typing import Optional
 import numpy
 
 from . import hpgl_wrap as W
-from .validation import (CriticalValidationError, GridValidator, ParameterValidator, ValidationError,
+from .validation import (CriticalValidationError, GridValidator, ParameterValidator, PathValidator, ValidationError,
                          ValidationWarning)
 
 _hpgl_so = W._hpgl_so
@@ -397,6 +397,145 @@ def simple_kriging_weights(center_point, n_x, n_y, n_z, ranges=(100000, 100000, 
     return weights
 
 
+# ------------------------------------------------------------------ property files
+# write_property / write_gslib_property / load_cont_property / read_inc_file_float /
+# read_inc_file_byte / load_ind_property: geo.py:418-570 of the reference.
+def _shape_of(prop):
+    if prop.data.ndim == 3:
+        return W._HPGL_SHAPE(data=prop.data.shape, strides=(1, prop.data.shape[0],
+                                                           prop.data.shape[0] * prop.data.shape[1]))
+    return W._HPGL_SHAPE(data=(prop.data.size, 1, 1), strides=(1, prop.data.size, prop.data.size))
+
+
+def _io_check(rc, what):
+    if rc != 0:
+        raise RuntimeError(what + " failed: " + W.last_error())
+
+
+def write_property(prop, filename, prop_name, undefined_value, indicator_values=None):
+    safe_path = PathValidator.validate_filepath(filename)
+    prop = _to_prop(prop)
+    if indicator_values is None:
+        indicator_values = []
+    sh = _shape_of(prop)
+    if isinstance(prop, ContProperty):
+        marr = W._HPGL_CONT_MASKED_ARRAY(data=prop.data.ctypes.data_as(C.POINTER(C.c_float)),
+                                         mask=prop.mask.ctypes.data_as(C.POINTER(C.c_ubyte)), shape=sh)
+        rc = _hpgl_so.hpgl_write_inc_file_float(safe_path.encode("utf-8"), C.byref(marr), undefined_value,
+                                                prop_name.encode("utf-8"))
+    else:
+        ind_arr = numpy.array(indicator_values, dtype="uint8")
+        marr = W._HPGL_IND_MASKED_ARRAY(data=prop.data.ctypes.data_as(C.POINTER(C.c_ubyte)),
+                                        mask=prop.mask.ctypes.data_as(C.POINTER(C.c_ubyte)), shape=sh,
+                                        indicator_count=prop.indicator_count)
+        rc = _hpgl_so.hpgl_write_inc_file_byte(safe_path.encode("utf-8"), C.byref(marr), int(undefined_value),
+                                               prop_name.encode("utf-8"),
+                                               ind_arr.ctypes.data_as(C.POINTER(C.c_ubyte)), len(indicator_values))
+    _io_check(rc, "write_property")
+
+
+def write_gslib_property(prop, filename, prop_name, undefined_value, indicator_values=None):
+    safe_path = PathValidator.validate_filepath(filename)
+    prop = _to_prop(prop)
+    if indicator_values is None:
+        indicator_values = []
+    sh = _shape_of(prop)
+    if isinstance(prop, ContProperty):
+        marr = W._HPGL_CONT_MASKED_ARRAY(data=prop.data.ctypes.data_as(C.POINTER(C.c_float)),
+                                         mask=prop.mask.ctypes.data_as(C.POINTER(C.c_ubyte)), shape=sh)
+        rc = _hpgl_so.hpgl_write_gslib_cont_property(C.byref(marr), safe_path.encode("utf-8"),
+                                                     prop_name.encode("utf-8"), undefined_value)
+    else:
+        ind_arr = (C.c_ubyte * max(len(indicator_values), 1))(*indicator_values)
+        marr = W._HPGL_IND_MASKED_ARRAY(data=prop.data.ctypes.data_as(C.POINTER(C.c_ubyte)),
+                                        mask=prop.mask.ctypes.data_as(C.POINTER(C.c_ubyte)), shape=sh,
+                                        indicator_count=prop.indicator_count)
+        rc = _hpgl_so.hpgl_write_gslib_byte_property(C.byref(marr), safe_path.encode("utf-8"),
+                                                     prop_name.encode("utf-8"), undefined_value, ind_arr,
+                                                     len(indicator_values))
+    _io_check(rc, "write_gslib_property")
+
+
+def _load_prop_cont_slow(filename, undefined_value):
+    values, mask = [], []
+    with open(PathValidator.validate_filepath(filename), "r", encoding="utf-8") as f:
+        for line in f:
+            if line.strip().startswith("--"):
+                continue
+            for part in line.split():
+                try:
+                    val = float(part.strip())
+                except (ValueError, TypeError):
+                    continue
+                values.append(val)
+                mask.append(0 if val == undefined_value else 1)
+    return ContProperty(numpy.array(values, dtype="float32"), numpy.array(mask, dtype="uint8"))
+
+
+def _load_prop_ind_slow(filename, undefined_value, ind_values):
+    dict_map = {v: i for i, v in enumerate(ind_values)}
+    values, mask = [], []
+    with open(PathValidator.validate_filepath(filename), "r", encoding="utf-8") as f:
+        for line in f:
+            if line.strip().startswith("--"):
+                continue
+            for part in line.split():
+                try:
+                    val = int(part.strip())
+                except (ValueError, TypeError):
+                    continue
+                if val == undefined_value:
+                    values.append(255)
+                    mask.append(0)
+                else:
+                    values.append(dict_map[val])
+                    mask.append(1)
+    return IndProperty(numpy.array(values, dtype="uint8"), numpy.array(mask, dtype="uint8"), len(ind_values))
+
+
+def _total(size):
+    if isinstance(size, tuple) and len(size) == 3:
+        GridValidator.validate_grid_dimensions(size[0], size[1], size[2])
+        return size[0] * size[1] * size[2]
+    return size
+
+
+def read_inc_file_float(filename, undefined_value, size):
+    safe_path = PathValidator.validate_filepath(filename, must_exist=True)
+    total = _total(size)
+    data = numpy.zeros(total, dtype="float32", order="F")
+    mask = numpy.zeros(total, dtype="uint8", order="F")
+    _io_check(_hpgl_so.hpgl_read_inc_file_float(safe_path.encode("utf-8"), undefined_value, total, data, mask),
+              "read_inc_file_float")
+    return ContProperty(data, mask)
+
+
+def read_inc_file_byte(filename, undefined_value, size, indicator_values):
+    safe_path = PathValidator.validate_filepath(filename, must_exist=True)
+    total = _total(size)
+    data = numpy.zeros(total, dtype="uint8", order="F")
+    mask = numpy.zeros(total, dtype="uint8", order="F")
+    vals = numpy.array(indicator_values, dtype="uint8")
+    _io_check(_hpgl_so.hpgl_read_inc_file_byte(safe_path.encode("utf-8"), int(undefined_value), total, data, mask,
+                                               vals, len(indicator_values)), "read_inc_file_byte")
+    return IndProperty(data, mask, len(indicator_values))
+
+
+def load_cont_property(filename, undefined_value, size=None):
+    safe_path = PathValidator.validate_filepath(filename, must_exist=True)
+    if size is None:
+        print("[WARNING]. load_cont_property: Size is not specified. Using slow and ineficcient method.")
+        return _load_prop_cont_slow(safe_path, undefined_value)
+    return read_inc_file_float(safe_path, undefined_value, size)
+
+
+def load_ind_property(filename, undefined_value, indicator_values, size=None):
+    if size is None:
+        print("[WARNING]. load_ind_property: Size is not specified. Using slow and ineficcient method.")
+        return _load_prop_ind_slow(filename, undefined_value, indicator_values)
+    return read_inc_file_byte(filename, undefined_value, size, indicator_values)
+
+
 def calc_mean(prop):
     prop = _to_prop(prop)
     sel = prop.mask.reshape(-1) == 1
@@ -461,5 +600,7 @@ def find_neighbours(prop, grid, radiuses, max_neighbours, cov_model, nodes, kind
 __all__ = ["ContProperty", "IndProperty", "SugarboxGrid", "CovarianceModel", "covariance", "ordinary_kriging",
            "simple_kriging", "lvm_kriging", "simple_cokriging_markI",
            "simple_cokriging_markII", "median_ik", "indicator_kriging", "simple_kriging_weights", "calc_mean",
-           "set_thread_num", "get_thread_num", "set_output_handler", "set_progress_handler", "set_precision",
+           "set_thread_num", "get_thread_num", "write_property",
+           "write_gslib_property", "load_cont_property", "load_ind_property", "read_inc_file_float",
+           "read_inc_file_byte", "set_output_handler", "set_progress_handler", "set_precision",
            "find_neighbours", "ValidationError", "CriticalValidationError", "ValidationWarning"]

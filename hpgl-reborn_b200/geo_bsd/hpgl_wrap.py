@@ -130,7 +130,8 @@ EXPORTS = [
     "hpgl_set_thread_num", "hpgl_get_thread_num", "hpgl_ordinary_kriging", "hpgl_simple_kriging",
     "hpgl_simple_kriging_weights", "hpgl_indicator_kriging", "hpgl_median_ik", "hpgl_lvm_kriging",
     "hpgl_sgs_simulation", "hpgl_sgs_lvm_simulation", "hpgl_simple_cokriging_mark1", "hpgl_simple_cokriging_mark2",
-    "hpgl_b200_cokriging_ex",
+    "hpgl_b200_cokriging_ex", "hpgl_read_inc_file_float", "hpgl_read_inc_file_byte", "hpgl_write_inc_file_float",
+    "hpgl_write_inc_file_byte", "hpgl_write_gslib_cont_property", "hpgl_write_gslib_byte_property",
     "hpgl_b200_cont_kriging_ex", "hpgl_b200_lvm_kriging_ex", "hpgl_b200_sgs_ex", "hpgl_b200_sgs_draws", "hpgl_b200_indicator_kriging_ex", "hpgl_b200_median_ik_ex",
     "hpgl_b200_find_neighbours", "hpgl_b200_last_stats", "hpgl_b200_host_alloc", "hpgl_b200_host_free",
     "hpgl_b200_transform", "hpgl_b200_template", "hpgl_b200_covariance", "hpgl_b200_version",
@@ -202,6 +203,21 @@ def _load():
     lib.hpgl_b200_cokriging_ex.restype = C.c_int
     lib.hpgl_b200_cokriging_ex.argtypes = [C.c_int, i_p, vp, vp, vp, vp, C.POINTER(_HPGL_COK_M1_PARAMS),
                                            C.POINTER(_HPGL_COK_M2_PARAMS), vp, vp, C.POINTER(_HPGL_B200_OPTIONS)]
+    lib.hpgl_read_inc_file_float.restype = C.c_int
+    lib.hpgl_read_inc_file_float.argtypes = [C.c_char_p, C.c_float, C.c_int, _f32F, _u8F]
+    lib.hpgl_read_inc_file_byte.restype = C.c_int
+    lib.hpgl_read_inc_file_byte.argtypes = [C.c_char_p, C.c_int, C.c_int, _u8F, _u8F, _u8, C.c_int]
+    lib.hpgl_write_inc_file_float.restype = C.c_int
+    lib.hpgl_write_inc_file_float.argtypes = [C.c_char_p, C.POINTER(_HPGL_CONT_MASKED_ARRAY), C.c_float, C.c_char_p]
+    lib.hpgl_write_inc_file_byte.restype = C.c_int
+    lib.hpgl_write_inc_file_byte.argtypes = [C.c_char_p, C.POINTER(_HPGL_IND_MASKED_ARRAY), C.c_int, C.c_char_p,
+                                             C.POINTER(C.c_ubyte), C.c_int]
+    lib.hpgl_write_gslib_cont_property.restype = C.c_int
+    lib.hpgl_write_gslib_cont_property.argtypes = [C.POINTER(_HPGL_CONT_MASKED_ARRAY), C.c_char_p, C.c_char_p,
+                                                   C.c_double]
+    lib.hpgl_write_gslib_byte_property.restype = C.c_int
+    lib.hpgl_write_gslib_byte_property.argtypes = [C.POINTER(_HPGL_IND_MASKED_ARRAY), C.c_char_p, C.c_char_p,
+                                                   C.c_double, C.POINTER(C.c_ubyte), C.c_int]
     lib.hpgl_b200_sgs_draws.restype = C.c_int
     lib.hpgl_b200_sgs_draws.argtypes = [C.c_longlong, C.c_longlong, vp]
     lib.hpgl_b200_indicator_kriging_ex.restype = C.c_int

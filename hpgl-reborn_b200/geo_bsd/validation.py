@@ -59,6 +59,28 @@ def _bad(x) -> bool:
     return math.isnan(x) or math.isinf(x)
 
 
+class PathValidator:
+    """File-path checks of the property readers and writers (validation.py:96-170)."""
+
+    @staticmethod
+    def validate_filepath(filename, must_exist: bool = False) -> str:
+        import os
+        import pathlib
+        if not filename:
+            raise CriticalValidationError("Filename cannot be empty", "filename")
+        path_str = os.path.normpath(str(filename))
+        if ".." in path_str.split(os.sep) or "../" in str(filename) or "..\\" in str(filename):
+            raise CriticalValidationError(f"Path traversal detected in filename: {filename}", "filename")
+        path = pathlib.Path(filename)
+        try:
+            resolved = path.resolve(strict=must_exist)
+        except (OSError, RuntimeError) as e:
+            raise CriticalValidationError(f"File does not exist: {filename}", "filename") from e
+        if must_exist and not resolved.is_file():
+            raise CriticalValidationError(f"Not a file: {filename}", "filename")
+        return str(resolved)
+
+
 class GridValidator:
     @staticmethod
     def validate_grid_dimensions(x: int, y: int, z: int) -> None:

@@ -149,6 +149,25 @@ void hpgl_simple_cokriging_mark2(struct hpgl_cont_masked_array_t *primary_data,
                                  struct hpgl_cokriging_m2_params_t *params,
                                  struct hpgl_cont_masked_array_t *output_data);
 
+/* Property files. Replace api.h:171-214 / api.cpp:53-252 (read_inc_file.cpp,
+ * property_writer.cpp): the INC text format (a property-name line, then
+ * whitespace-separated values, "--" comments to the end of a line, a "/"
+ * terminator) and the GSLIB format. Readers return 0, or -1 with the message
+ * in hpgl_get_last_exception_message (a "/" or a bad token among the first
+ * `size` values, or a file with fewer values); the mask marks values other
+ * than undefined_value. The byte reader maps values[j] to category j. */
+int hpgl_read_inc_file_float(char *filename, float undefined_value, int size, float *data, unsigned char *mask);
+int hpgl_read_inc_file_byte(char *filename, int undefined_value, int size, unsigned char *data, unsigned char *mask,
+                            unsigned char *values, int values_count);
+int hpgl_write_inc_file_float(char *filename, struct hpgl_cont_masked_array_t *arr, float undefined_value,
+                              char *name);
+int hpgl_write_inc_file_byte(char *filename, struct hpgl_ind_masked_array_t *arr, int undefined_value, char *name,
+                             unsigned char *values, int values_count);
+int hpgl_write_gslib_cont_property(struct hpgl_cont_masked_array_t *data, const char *filename, const char *name,
+                                   double undefined_value);
+int hpgl_write_gslib_byte_property(struct hpgl_ind_masked_array_t *data, const char *filename, const char *name,
+                                   double undefined_value, unsigned char *values, int values_count);
+
 /* ------------------------------------------------------------ _ex extensions */
 /* status codes */
 #define HPGL_B200_OK 0
