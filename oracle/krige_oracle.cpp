@@ -1279,4 +1279,114 @@ int ko_cokriging(int mark, const int *dims, const float *pdata, const unsigned c
     return 0;
 }
 
+// Sequential indicator simulation (sequential_indicator_simulation.cpp:24-185):
+// the walk of the simulation; per visited node that is not informed and whose
+// simulation mask is 1, for every category c (only c = 0 with two categories,
+// the other probability being 1 - p) the SK estimate of the indicator
+// (category == c) from the first max_nb[c] informed cells of category c's
+// truncated template, around float(marginal[c]) or the LVM means of category
+// c, accumulated in double (the marginal / mean on failure); then one
+// std::uniform_real_distribution draw u picks the first category whose running
+// sum of probabilities exceeds u times their sum (sample.cpp:8-21). `params`:
+// per category cov_type, ranges[3], angles[3], sill, nugget; radiuses (3 per
+// category), max_nb, marginal. means: per category a float per cell, or null.
+// Returns 0, -1 on bad arguments, -3 when the walk does not visit every node
+// (the reference throws at the end of such a path).
+int ko_sis(const int *dims, unsigned char *data, unsigned char *mask, const unsigned char *sim_mask, int ncat,
+           const int *cov_types, const double *ranges, const double *angles, const double *sills,
+           const double *nuggets, const int *radiuses, const int *max_nb, const double *marginals,
+           const float *const *means, long long seed, int *out_status)
+{
+    Grid g = {dims[0], dims[1], dims[2]};
+    const long size = g.size();
+    if (size > 10000000 || ncat < 2) return -1;
+    std::vector<Flavour> f(ncat);
+    std::vector<std::vector<Off>> tmpl(ncat);
+    const int kcat = ncat == 2 ? 1 : ncat;
+    for (int c = 0; c < kcat; ++c)
+    {
+        if (!make_flavour(f[c], true, cov_types[c], ranges + 3 * c, angles + 3 * c, sills[c], nuggets[c],
+                          radiuses + 3 * c))
+            return -1;
+        tmpl[c] = build_template(f[c]);
+    }
+    PathLcg path;
+    if (!path.init(size, (int)seed)) return -1;
+    std::mt19937 gen;
+    gen.seed((std::mt19937::result_type)(long)(int)seed);
+    if (out_status)
+        for (long i = 0; i < size; ++i) out_status[i] = -1;
+    std::vector<int> idx, xs, ys, zs;
+    std::vector<double> w, probs(ncat);
+    const long first = path.R;
+    for (long counter = 0; counter < size; ++counter)
+    {
+        const int node = path.next();
+        if (mask[node]) continue;
+        if (sim_mask && sim_mask[node] != 1) continue;
+        int x, y, z;
+        g.coord(node, x, y, z);
+        int st_all = 0;
+        for (int c = 0; c < kcat; ++c)
+        {
+            idx.clear();
+            for (size_t t = 0; t < tmpl[c].size() && (int)idx.size() < max_nb[c]; ++t)
+            {
+                int q = g.index(x + tmpl[c][t].dx, y + tmpl[c][t].dy, z + tmpl[c][t].dz);
+                if (q >= 0 && mask[q]) idx.push_back(q);
+            }
+            const float mc = means ? means[c][node] : (float)marginals[c];
+            // the failure value: the mean provider at the node (double)
+            double prob = means ? (double)means[c][node] : (double)(float)marginals[c];
+            int status = KI_NO_NEIGHBOURS;
+            if (!idx.empty())
+            {
+                const int n = (int)idx.size();
+                xs.resize(n);
+                ys.resize(n);
+                zs.resize(n);
+                for (int i = 0; i < n; ++i) g.coord(idx[i], xs[i], ys[i], zs[i]);
+                double var;
+                if (weights<double>(f[c], false, x, y, z, xs, ys, zs, w, var))
+                {
+                    status = KI_SUCCESS;
+                    double r = (double)mc;
+                    for (int i = 0; i < n; ++i)
+                    {
+                        const unsigned char v = data[idx[i]] == c ? 1 : 0;
+                        const float mi = means ? means[c][idx[i]] : mc;
+                        r += w[i] * (v - mi);
+                    }
+                    prob = r;
+                }
+                else
+                    status = KI_SINGULARITY;
+            }
+            probs[c] = prob;
+            if (status > st_all) st_all = status;
+        }
+        if (ncat == 2) probs[1] = 1 - probs[0];
+        double sum = 0.0;
+        for (int c = 0; c < ncat; ++c) sum += probs[c];
+        std::uniform_real_distribution<double> dist(0.0, 1.0);
+        const double s = dist(gen) * sum;
+        double p = 0;
+        int pick = ncat - 1;
+        for (int c = 0; c < ncat; ++c)
+        {
+            p += probs[c];
+            if (s < p)
+            {
+                pick = c;
+                break;
+            }
+        }
+        data[node] = (unsigned char)pick;
+        mask[node] = 1;
+        if (out_status) out_status[node] = st_all;
+    }
+    if (path.R != first) return -3;
+    return 0;
+}
+
 } // extern "C"

@@ -70,6 +70,8 @@ def load(which: str):
                                C.c_double, _i, C.c_int, C.c_longlong, _i]
         lib.ko_sgs_path.argtypes = [C.c_longlong, C.c_longlong, _i, C.c_longlong]
         lib.ko_mt_draws.argtypes = [C.c_longlong, C.c_longlong, _d]
+        lib.ko_sis.argtypes = [_i, _u8, _u8, _u8, C.c_int, _i, _d, _d, _d, _d, _i, _i, _d, C.c_void_p,
+                               C.c_longlong, _i]
         lib.ko_cokriging.argtypes = [C.c_int, _i, _f, _u8, _f, _u8, C.c_int, _d, _d, C.c_double, C.c_double, C.c_int,
                                      _d, _d, C.c_double, C.c_double, _i, C.c_int, C.c_double, C.c_double,
                                      C.c_double, C.c_double, _f, _u8, _i, C.c_int]
@@ -386,6 +388,36 @@ def ref_cokriging_mark1(dims, pdata, pmask, sdata, smask, cov, radiuses, k, pm, 
                float(cov.nugget), (C.c_int * 3)(*radiuses), int(k), float(pm), float(sm), float(sv), float(corr))
     lib.hpgl_simple_cokriging_mark1(C.byref(a), C.byref(b), C.byref(p), C.byref(o))
     return od, om
+
+
+def sis(dims, data, mask, covs, radiuses, ks, marginals, seed, sim_mask=None, means=None):
+    """Sequential indicator simulation (port): covs / radiuses / ks / marginals per
+    category; means (LVM) a list of per-cell float arrays. Returns (data, mask, status)."""
+    lib = load("port")
+    ncat = len(covs)
+    data = _arr(data, np.uint8).copy()
+    mask = _arr(mask, np.uint8).copy()
+    st = np.zeros(len(data), np.int32)
+    ct = _arr([c.cov_type for c in covs], np.int32)
+    rg = _arr([r for c in covs for r in c.ranges], np.float64)
+    an = _arr([a for c in covs for a in c.angles], np.float64)
+    si = _arr([c.sill for c in covs], np.float64)
+    nu = _arr([c.nugget for c in covs], np.float64)
+    rd = _arr([r for rr in radiuses for r in rr], np.int32)
+    kk = _arr(ks, np.int32)
+    mg = _arr(marginals, np.float64)
+    sm = _arr(sim_mask, np.uint8) if sim_mask is not None else None
+    mp = None
+    keep = []
+    if means is not None:
+        keep = [_arr(m, np.float32) for m in means]
+        mp = (_f * ncat)(*[k.ctypes.data_as(_f) for k in keep])
+    rc = lib.ko_sis(_ptr(_arr(dims, np.int32), _i), _ptr(data, _u8), _ptr(mask, _u8), _ptr(sm, _u8), ncat,
+                    _ptr(ct, _i), _ptr(rg, _d), _ptr(an, _d), _ptr(si, _d), _ptr(nu, _d), _ptr(rd, _i),
+                    _ptr(kk, _i), _ptr(mg, _d), mp, int(seed), _ptr(st, _i))
+    if rc:
+        raise RuntimeError(f"sis failed (rc={rc})")
+    return data, mask, st
 
 
 def mt_draws(seed, n):

@@ -8,6 +8,7 @@ harness libref_harness.so around its own templates):
                       python tests/golden/make_golden.py lvm    (lvm.npz only)
                       python tests/golden/make_golden.py sgs    (sgs.npz only)
                       python tests/golden/make_golden.py cok    (cok.npz only)
+                      python tests/golden/make_golden.py sis    (sis.npz only)
 
 Inputs are the seeded workloads of geo_bsd.workloads at reduced scale (the
 conditioning cells are stored in each file, so the fixtures do not depend on
@@ -17,7 +18,7 @@ kriging_interpolation with result_t = double, the float estimate the drivers
 store, and the status code. Whole-grid outputs of the reference's public C API
 (hpgl_ordinary_kriging, hpgl_simple_kriging, hpgl_lvm_kriging,
 hpgl_indicator_kriging, hpgl_median_ik, hpgl_sgs_simulation,
-hpgl_sgs_lvm_simulation, hpgl_simple_cokriging_mark1/2) are stored for the small grids, plus the known-answer cases
+hpgl_sgs_lvm_simulation, hpgl_simple_cokriging_mark1/2, hpgl_sis_simulation(_lvm)) are stored for the small grids, plus the known-answer cases
 of the reference's test suite (constant field 42, all zeros).
 """
 import ctypes as C
@@ -33,7 +34,7 @@ sys.path.insert(0, os.path.join(ROOT, "hpgl-reborn_b200"))
 
 import oracle as O  # noqa: E402
 sys.path.insert(0, os.path.dirname(HERE))
-from golden_io import COK_CASES, SGS_CASES, cok_inputs, sgs_inputs  # noqa: E402
+from golden_io import COK_CASES, SGS_CASES, SIS_CASES, cok_inputs, sgs_inputs, sis_inputs  # noqa: E402
 from geo_bsd import workloads as WL  # noqa: E402  (pure python module)
 
 SAMPLE = 1200
@@ -212,6 +213,36 @@ def api_cokriging(lib, mark, dims, pdata, pmask, sdata, smask, cov, rad, k, pm, 
     return od, om
 
 
+def api_sis(lib, dims, data, mask, covs, rads, ks, marginals, seed, sim_mask=None, means=None):
+    """The reference's hpgl_sis_simulation / hpgl_sis_simulation_lvm (no correlograms);
+    returns the output data and mask."""
+    od = np.ascontiguousarray(data, np.uint8).copy()
+    om = np.ascontiguousarray(mask, np.uint8).copy()
+    up = C.POINTER(C.c_ubyte)
+    m = len(covs)
+    arr = (IkP * m)()
+    for i, c in enumerate(covs):
+        arr[i] = IkP(c.cov_type, (C.c_double * 3)(*c.ranges), (C.c_double * 3)(*c.angles), c.sill, c.nugget,
+                     (C.c_int * 3)(*rads[i]), ks[i], marginals[i])
+    a = Ind(od.ctypes.data_as(up), om.ctypes.data_as(up), _shape(dims), m)
+    keep = []
+    sm = None
+    if sim_mask is not None:
+        smv = np.ascontiguousarray(sim_mask, np.uint8)
+        keep.append(smv)
+        sm = C.byref(UbyteArr(smv.ctypes.data_as(up), _shape(dims)))
+    if means is None:
+        lib.hpgl_sis_simulation(C.byref(a), arr, m, seed, sm)
+    else:
+        fa = (FloatArr * m)()
+        for i, mv in enumerate(means):
+            mv = np.ascontiguousarray(mv, np.float32)
+            keep.append(mv)
+            fa[i] = FloatArr(mv.ctypes.data_as(C.POINTER(C.c_float)), _shape(dims))
+        lib.hpgl_sis_simulation_lvm(C.byref(a), arr, fa, m, seed, sm, 0)
+    return od, om
+
+
 def api_ik(lib, dims, data, mask, covs, rads, ks, marginals):
     data = np.ascontiguousarray(data, np.uint8)
     mask = np.ascontiguousarray(mask, np.uint8)
@@ -326,8 +357,24 @@ def cok_cases(lib):
     print("wrote cok")
 
 
+def sis_cases(lib):
+    """The reference's SIS outputs (inputs: the indicator fixture; see golden_io.sis_inputs)."""
+    out = {}
+    for name, opts in SIS_CASES:
+        x = sis_inputs(dict(np.load(os.path.join(HERE, "indicator_s015.npz"))), opts)
+        od, om = api_sis(lib, x["dims"], x["data"], x["mask"], x["covs"], x["rads"], x["ks"], x["marginals"],
+                         x["seed"], sim_mask=x["sim_mask"], means=x["means"])
+        out[f"{name}_data"] = od
+        out[f"{name}_mask"] = om
+    np.savez_compressed(os.path.join(HERE, "sis.npz"), **out)
+    print("wrote sis")
+
+
 def main(only=None):
     lib = _api()
+    if only == "sis":
+        sis_cases(lib)
+        return
     if only == "cok":
         cok_cases(lib)
         return
@@ -340,6 +387,7 @@ def main(only=None):
     lvm_cases(lib)
     sgs_cases(lib)
     cok_cases(lib)
+    sis_cases(lib)
     cont_case(lib, WL.ok_small(0.3), "ok_small_s030", grid_api=True)
     cont_case(lib, WL.sk_ok_large(0.16), "sk_ok_large_s016")
     cont_case(lib, WL.gauss_cv(0.2), "gauss_cv_s020", grid_api=True)

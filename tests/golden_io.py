@@ -107,3 +107,42 @@ def cok_inputs(g, mark, secondary=None):
             "k": k, "pm": float(pdata[pmask == 1].astype(np.float64).mean()),
             "sm": float(sdata[smask == 1].astype(np.float64).mean()), "sv": 0.9, "corr": 0.6,
             "cov2": COK_SECONDARY_COV if mark == 2 else None}
+
+
+SIS_CASES = [
+    # name, options: seed, categories (5 = the fixture's, 2 = median SIS on category >= 2), mask, LVM
+    ("sis5", {"seed": 17}),
+    ("sis5_mask", {"seed": 5, "sim_mask": 0.6}),
+    ("sis2_median", {"seed": 9, "two": True}),
+    ("sis5_lvm", {"seed": 23, "lvm": True}),
+]
+
+
+def sis_inputs(g, opts):
+    """Inputs of a SIS golden case from the indicator fixture: its categories,
+    per-category models, radiuses and marginals (k = 12 per category); a
+    seeded simulation mask; LVM means from a smooth trend per category."""
+    dims, data, mask = grid_inputs(g, dtype=np.uint8)
+    n = len(data)
+    data = np.where(mask == 1, data, 0).astype(np.uint8)
+    covs, rads = [], []
+    for c in range(5):
+        cov, rad, _ = cov_of(g, f"c{c}_")
+        covs.append(cov)
+        rads.append(rad)
+    marg = [float(v) for v in g["marginals"]]
+    if opts.get("two"):
+        data = (data >= 2).astype(np.uint8) * mask
+        covs, rads = covs[2:4], rads[2:4]
+        marg = [0.6, 0.4]
+    ks = [12] * len(covs)
+    x = {"dims": dims, "data": data, "mask": mask.copy(), "covs": covs, "rads": rads, "ks": ks, "marginals": marg,
+         "seed": opts["seed"], "sim_mask": None, "means": None}
+    if "sim_mask" in opts:
+        x["sim_mask"] = (np.random.default_rng(6).random(n) < opts["sim_mask"]).astype(np.uint8)
+    if opts.get("lvm"):
+        t = WL.lvm_means(dims)
+        t = (t - t.min()) / max(float(t.max() - t.min()), 1e-6)
+        base = np.array(marg, np.float64)
+        x["means"] = [((0.5 * base[c] + 0.5 * base[c] * (0.5 + t)) / 1.0).astype(np.float32) for c in range(5)]
+    return x

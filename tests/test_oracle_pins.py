@@ -167,3 +167,15 @@ def test_oracle_cokriging_matches_reference(case):
                            x["pm"], x["sm"], secondary_variance=x["sv"], corr=x["corr"], cov2=x["cov2"], threads=4)
     np.testing.assert_array_equal(m, ref[f"{case}_mask"])
     np.testing.assert_array_equal(d.view(np.uint32), ref[f"{case}_data"].view(np.uint32))
+
+
+@pytest.mark.parametrize("case", [c[0] for c in G.SIS_CASES])
+def test_oracle_sis_matches_reference(case):
+    """SIS: the restatement reproduces the reference's hpgl_sis_simulation(_lvm) output exactly."""
+    opts = next(c[1] for c in G.SIS_CASES if c[0] == case)
+    x = G.sis_inputs(G.load("indicator_s015"), opts)
+    ref = G.load("sis")
+    d, m, _ = O.sis(x["dims"], x["data"], x["mask"], x["covs"], x["rads"], x["ks"], x["marginals"], x["seed"],
+                    sim_mask=x["sim_mask"], means=x["means"])
+    np.testing.assert_array_equal(m, ref[f"{case}_mask"])
+    np.testing.assert_array_equal(d, ref[f"{case}_data"])
