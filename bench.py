@@ -19,7 +19,10 @@ grid with a correlated secondary field informed on half of the cells, against
 the reference's own single-threaded hpgl_simple_cokriging_mark1 on a smaller
 grid of the same generator; `--kind sgs` times sequential Gaussian simulation (SK, k=32, seed 42) of every
 uninformed cell of that grid, against the reference's own single-threaded
-hpgl_sgs_simulation on a smaller grid of the same generator.
+hpgl_sgs_simulation on a smaller grid of the same generator; `--kind sis` times
+sequential indicator simulation (5 categories, k=24, seed 42) of the 200x200x100
+indicator grid (geo_bsd.workloads.indicator) against the reference's own
+single-threaded hpgl_sis_simulation on a smaller grid of that generator.
 
 Usage:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 For N > 1 the driver runs it under torchrun; every rank runs its own replica
@@ -52,7 +55,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--workload", default="sk_ok_large")
-    ap.add_argument("--kind", choices=["ok", "sk", "lvm", "sgs", "cok"], default="ok")
+    ap.add_argument("--kind", choices=["ok", "sk", "lvm", "sgs", "cok", "sis"], default="ok")
     ap.add_argument("--skip-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--profile-case", type=float, default=0.0, metavar="SCALE",
@@ -381,6 +384,209 @@ def bench_sgs(args, rank, world, local):
         dist.destroy_process_group()
 
 
+SIS_METRIC = "simulated cells/s, 1 B200: sequential indicator simulation (5 categories, k=24)"
+SIS_SEED = 42
+
+
+def sis_workload(scale):
+    from geo_bsd import workloads as WL
+    wl = WL.indicator(scale)
+    data = np.where(wl.mask == 1, wl.data, 0).astype(np.uint8)
+    return wl, data
+
+
+def sis_reference(target_seconds):
+    """The reference's own SIS (oracle/_ref/libhpgl.so, single-threaded as it is)
+    on a grid of the same generator sized for about target_seconds; returns
+    (cells/s, info)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    def run(scale):
+        wl, data = sis_workload(scale)
+        ks = [wl.max_neighbours] * wl.categories
+        t0 = time.perf_counter()
+        O.ref_sis(wl.dims, data, wl.mask, wl.cat_covs, wl.cat_radiuses, ks, wl.marginals, SIS_SEED)
+        return wl, time.perf_counter() - t0
+
+    wl, dt = run(0.2)
+    rate = int((wl.mask == 0).sum()) / max(dt, 1e-3)
+    scale = min(1.0, max(0.2, (rate * target_seconds / (200 * 200 * 100)) ** (1.0 / 3.0)))
+    wl, dt = run(scale)
+    cells = int((wl.mask == 0).sum())
+    return cells / dt, {"dims": wl.dims, "cells": cells, "seconds": dt}
+
+
+def bench_sis(args, rank, world, local):
+    import torch
+    if args.impl == "reference":
+        if rank == 0:
+            vals, info = [], None
+            for i in range(args.warmup + args.steps):
+                v, info = sis_reference(min(args.cpu_seconds, 2.0))
+                if i >= args.warmup:
+                    vals.append(v)
+            value = float(np.median(vals))
+            d = "x".join(str(x) for x in info["dims"])
+            print(json.dumps({"impl": "reference", "metric": SIS_METRIC, "value": value, "unit": UNIT,
+                              "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                              "data": "synthetic (seeded, geo_bsd.workloads)",
+                              "config": {"workload": f"SIS 5 categories k=24 seed {SIS_SEED}, grid {d} of the "
+                                                     "200x200x100 indicator generator (1.5% conditioning)"},
+                              "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                                               "sample": f"whole simulation of a {d} grid ({info['cells']} cells) "
+                                                         "per step; the reference's SIS is single-threaded"},
+                              "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist_mod
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+        dist = dist_mod
+    from geo_bsd import hpgl_wrap as W
+    wl, data = sis_workload(args.profile_case if args.profile_case > 0 else 1.0)
+    n = wl.n_cells
+    m = wl.categories
+    dev = torch.device("cuda", local)
+    d_data0 = torch.from_numpy(np.ascontiguousarray(data)).to(dev)
+    d_mask0 = torch.from_numpy(np.ascontiguousarray(wl.mask)).to(dev)
+    d_data = d_data0.clone()
+    d_mask = d_mask0.clone()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+    dims = (C.c_int * 3)(*wl.dims)
+    params = (W._HPGL_IK_PARAMS * m)()
+    for i, c in enumerate(wl.cat_covs):
+        params[i] = W._HPGL_IK_PARAMS(covariance_type=c.cov_type, ranges=c.ranges, angles=c.angles, sill=c.sill,
+                                      nugget=c.nugget, radiuses=wl.cat_radiuses[i], max_neighbours=wl.max_neighbours,
+                                      marginal_prob=wl.marginals[i])
+
+    def dev_call():
+        o = W._HPGL_B200_OPTIONS(precision=0, refine_steps=0, flags=W.FLAG_DEVICE_POINTERS, stream=stream.cuda_stream,
+                                 estimate64=None, variance=None, status=None, ik_probs=None)
+        rc = W._hpgl_so.hpgl_b200_sis_ex(dims, d_data.data_ptr(), d_mask.data_ptr(), None, params, m, None, SIS_SEED,
+                                         0, C.byref(o))
+        W.check(rc, "sis_ex")
+        return W.last_stats()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def restore():
+        d_data.copy_(d_data0)
+        d_mask.copy_(d_mask0)
+
+    if args.profile_case > 0:
+        st = dev_call()
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_case": wl.dims, "stats": st}), flush=True)
+        return
+    for _ in range(args.warmup):
+        restore()
+        dev_call()
+    times, stats = [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            restore()
+            flush.zero_()  # L2 flush between steps (outside the timed region)
+            barrier()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st = dev_call()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+            stats.append(st)
+    barrier()
+    ms = max_over_ranks(float(np.mean(times)))
+    last = stats[-1]
+    cells = last["kriged_cells"]
+    value = cells * world / (ms / 1e3)
+    pk = peak_table()
+    solve_ms = float(np.mean([s["stage_solve_ms"] for s in stats]))
+    achieved = last["sgs_flops"] / (solve_ms / 1e3) / 1e12
+    roofline = {"bound": "fp64", "kernel": "k_sis_solve_fold (FP64, two nodes per warp, one launch per category "
+                                            "and level) + k_sis_sample",
+                "achieved": achieved, "peak": pk["fp64"], "unit": "TFLOP/s", "frac": achieved / pk["fp64"],
+                "traffic": None, "peak_source": f"CUDA-core FP64 peak 148 SM x 64 lanes x 2 x {pk['source']}",
+                "algorithmic_flops_per_call": last["sgs_flops"], "solve_stage_ms": solve_ms,
+                "levels": last["sgs_levels"]}
+
+    # end to end with pinned host buffers (categories and mask in, simulated categories and mask out)
+    lib = W._hpgl_so
+    h_data = lib.hpgl_b200_host_alloc(n)
+    h_mask = lib.hpgl_b200_host_alloc(n)
+    src_d = np.ascontiguousarray(data)
+    src_m = np.ascontiguousarray(wl.mask)
+
+    def host_call():
+        C.memmove(h_data, src_d.ctypes.data, n)
+        C.memmove(h_mask, src_m.ctypes.data, n)
+        o = W._HPGL_B200_OPTIONS(precision=0, refine_steps=0, flags=0, stream=None, estimate64=None, variance=None,
+                                 status=None, ik_probs=None)
+        t0 = time.perf_counter()
+        rc = lib.hpgl_b200_sis_ex(dims, h_data, h_mask, None, params, m, None, SIS_SEED, 0, C.byref(o))
+        dt = time.perf_counter() - t0
+        W.check(rc, "sis_ex (host)")
+        return dt, W.last_stats()
+
+    for _ in range(args.warmup):
+        host_call()
+    e2e_t = []
+    for _ in range(args.steps):
+        barrier()
+        dt, st = host_call()
+        e2e_t.append(dt)
+    barrier()
+    e2e_s = max_over_ranks(float(np.mean(e2e_t)))
+    e2e_value = st["kriged_cells"] * world / e2e_s
+    lib.hpgl_b200_host_free(h_data)
+    lib.hpgl_b200_host_free(h_mask)
+    cpu = None
+    if rank == 0 and not args.skip_cpu_baseline:
+        v, info = sis_reference(args.cpu_seconds)
+        d = "x".join(str(x) for x in info["dims"])
+        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "reference",
+               "sample": f"the reference's hpgl_sis_simulation of a {d} grid of the same generator "
+                         f"({info['cells']} cells, {info['seconds']:.1f} s); single-threaded as the reference is"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": SIS_METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, geo_bsd.workloads)",
+            "config": {"workload": f"SIS {wl.dims[0]}x{wl.dims[1]}x{wl.dims[2]}, 1.5% conditioning, 5 categories "
+                                   f"(spherical, ranges 12-25), k={wl.max_neighbours} per category, seed {SIS_SEED}",
+                       "l2": "flushed between timed steps (256 MB write)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "stages_ms": {k[len("stage_"):-len("_ms")]: round(v, 3) for k, v in last.items() if k.startswith("stage_")},
+            "host_draws_ms": last["sgs_draws_ms"],
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(st["h2d_bytes"]),
+                    "d2h_bytes_per_step": int(st["d2h_bytes"]), "timing": "wall clock per call"},
+            "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
+            "clocks": clk.summary(),
+        }), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 COK_METRIC = "cokriged cells/s, 1 B200: simple collocated cokriging, Markov model I (k=32)"
 
 
@@ -564,6 +770,8 @@ def main():
     if args.kind == "sgs":
         bench_sgs(args, rank, world, local)
         return
+    if args.kind == "sis":
+        return bench_sis(args, rank, world, local)
     if args.kind == "cok":
         bench_cok(args, rank, world, local)
         return

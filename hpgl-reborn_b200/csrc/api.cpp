@@ -548,6 +548,50 @@ int hpgl_write_gslib_byte_property(hpgl_ind_masked_array_t *data, const char *fi
     }
 }
 
+void hpgl_sis_simulation(hpgl_ind_masked_array_t *data, hpgl_ik_params_t *params, int indicator_count, int seed,
+                         hpgl_ubyte_array_t *simulation_mask)
+{
+    if (!data || !params || indicator_count <= 0)
+    {
+        hb::set_error("hpgl_sis_simulation: bad argument");
+        return;
+    }
+    int dims[3];
+    if (!shape_dims(&data->m_shape, dims)) return;
+    std::vector<hb::IkArgs> cats;
+    for (int i = 0; i < indicator_count; ++i) cats.push_back(ik_args_from(params + i));
+    hb::Options opt;
+    progress("Sequential Indicator Simulation", 0);
+    if (hb::sis_simulation(dims, data->m_data, data->m_mask, simulation_mask ? simulation_mask->m_data : nullptr,
+                           cats, nullptr, seed, opt) == 0)
+        report_done("Sequential Indicator Simulation");
+}
+
+void hpgl_sis_simulation_lvm(hpgl_ind_masked_array_t *data, hpgl_ik_params_t *params, hpgl_float_array_t *mean_data,
+                             int indicator_count, int seed, hpgl_ubyte_array_t *simulation_mask,
+                             int use_correlograms)
+{
+    if (!data || !params || !mean_data || indicator_count <= 0)
+    {
+        hb::set_error("hpgl_sis_simulation_lvm: bad argument");
+        return;
+    }
+    int dims[3];
+    if (!shape_dims(&data->m_shape, dims)) return;
+    std::vector<hb::IkArgs> cats;
+    std::vector<const float *> means;
+    for (int i = 0; i < indicator_count; ++i)
+    {
+        cats.push_back(ik_args_from(params + i));
+        means.push_back(mean_data[i].m_data);
+    }
+    hb::Options opt;
+    progress("Sequential Indicator Simulation", 0);
+    if (hb::sis_simulation(dims, data->m_data, data->m_mask, simulation_mask ? simulation_mask->m_data : nullptr,
+                           cats, means.data(), seed, opt, use_correlograms != 0) == 0)
+        report_done("Sequential Indicator Simulation");
+}
+
 int hpgl_simple_kriging_weights(float *center_coords, float *neighbours_x, float *neighbours_y,
                                 float *neighbours_z, int neighbours_count, hpgl_cov_params_t *params,
                                 float *weights)
@@ -663,6 +707,20 @@ int hpgl_b200_cokriging_ex(int mark, const int *dims, const float *pdata, const 
         return HPGL_B200_EINVAL;
     }
     return hb::cokriging(dims, pdata, pmask, sdata, smask, a, out_data, out_mask, options_from(opt));
+}
+
+int hpgl_b200_sis_ex(const int *dims, unsigned char *data, unsigned char *mask, const unsigned char *sim_mask,
+                     const hpgl_ik_params_t *params, int indicator_count, const float *const *means, int seed,
+                     int use_correlograms, const hpgl_b200_options_t *opt)
+{
+    if (!params || indicator_count <= 0)
+    {
+        hb::set_error("hpgl_b200_sis_ex: bad argument");
+        return HPGL_B200_EINVAL;
+    }
+    std::vector<hb::IkArgs> cats;
+    for (int i = 0; i < indicator_count; ++i) cats.push_back(ik_args_from(params + i));
+    return hb::sis_simulation(dims, data, mask, sim_mask, cats, means, seed, options_from(opt), use_correlograms != 0);
 }
 
 int hpgl_b200_sgs_draws(long long seed, long long n, double *out)

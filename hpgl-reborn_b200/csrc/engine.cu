@@ -1246,6 +1246,252 @@ int sgs_simulation(const int *dims, float *data, unsigned char *mask, const unsi
     }
 }
 
+// ------------------------------------------------------------------ SIS
+int sis_simulation(const int *dims, unsigned char *data, unsigned char *mask, const unsigned char *sim_mask,
+                   const std::vector<IkArgs> &cats, const float *const *means, long long seed, const Options &opt,
+                   bool correlogram)
+{
+    std::lock_guard<std::mutex> lk(g_engine_mu);
+    try
+    {
+        if (!dims || !data || !mask) throw CudaFail{-1, "null array argument"};
+        const long long n = check_dims(dims);
+        if (n > 10000000) throw CudaFail{-4, "the simulation path supports at most 10,000,000 cells"};
+        const int ncat = (int)cats.size();
+        if (ncat < 2) throw CudaFail{-1, "indicator simulation needs at least two categories"};
+        if (ncat > kSisMaxCat)
+            throw CudaFail{-4, "indicator simulation supports up to " + std::to_string(kSisMaxCat) + " categories"};
+        // median SIS (two categories) krige the first only
+        const int kcat = ncat == 2 ? 1 : ncat;
+        for (int c = 0; c < kcat; ++c)
+        {
+            const IkArgs &a = cats[c];
+            check_model_args(a.cov_type, a.ranges, a.angles, a.sill, a.nugget, a.radiuses, a.max_nb);
+            if (a.max_nb > 32) throw CudaFail{-4, "indicator simulation supports max_neighbours up to 32"};
+        }
+        SgsWalk walk;
+        if (!sgs_walk(n, seed, walk))
+            throw CudaFail{-1, "the simulation path does not visit every node of a grid of this size"};
+        if (walk.R0 < 0) throw CudaFail{-1, "seed % grid size must not be negative"};
+        double plan_ms = 0.0;
+        auto plan_f = std::async(std::launch::async, [&]() {
+            const auto t0 = std::chrono::steady_clock::now();
+            std::vector<std::pair<Plan, std::vector<Offset>>> v;
+            for (int c = 0; c < kcat; ++c)
+            {
+                const IkArgs &a = cats[c];
+                Plan p = make_plan(true, a.cov_type, a.ranges, a.angles, a.sill, a.nugget, a.radiuses, a.max_nb, dims,
+                                   false);
+                std::vector<Offset> tv = build_template(p.f, p.kt);
+                v.emplace_back(std::move(p), std::move(tv));
+            }
+            plan_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            return v;
+        });
+        Engine &E = engine_for_current_device();
+        cudaStream_t st = E.stream(opt.stream);
+        IoPlan io{(opt.flags & 1u) != 0, st};
+        begin_call(E, st);
+        uint8_t *d_data = io.device ? data : E.buf<uint8_t>("sis_data", (size_t)n);
+        uint8_t *d_mask = io.device ? mask : E.buf<uint8_t>("sis_mask", (size_t)n);
+        if (!io.device)
+        {
+            HB_CK(cudaMemcpyAsync(d_data, data, n, cudaMemcpyHostToDevice, st));
+            HB_CK(cudaMemcpyAsync(d_mask, mask, n, cudaMemcpyHostToDevice, st));
+            E.stats.h2d += n * 2;
+        }
+        const uint8_t *d_sim = sim_mask ? to_device(E, "sgs_sim_mask", sim_mask, (size_t)n, io) : nullptr;
+        std::vector<const float *> d_means(kcat, nullptr);
+        if (means)
+            for (int c = 0; c < kcat; ++c)
+            {
+                if (!means[c]) throw CudaFail{-1, "LVM indicator simulation needs a mean array per category"};
+                const std::string slot = "sis_means_" + std::to_string(c);
+                d_means[c] = to_device(E, slot.c_str(), means[c], (size_t)n, io);
+            }
+        E.mark(STAGE_UPLOAD, st);
+
+        // the walk -> ranks (the same walk as the Gaussian simulation's)
+        int *rank_of = E.buf<int>("sgs_rank_of", (size_t)n);
+        int *sim_cells = E.buf<int>("sgs_sim_cells", (size_t)n);
+        int n_sim = 0;
+        {
+            int *path_cell = E.buf<int>("sgs_path", (size_t)n);
+            int *flag = E.buf<int>("sgs_flag", (size_t)n);
+            int *tmp = E.buf<int>("scan_tmp", (size_t)scan_tmp_ints(n) + 4);
+            int *total = E.buf<int>("sgs_total", 1);
+            int *scan = E.buf<int>("sgs_scan", (size_t)n);
+            launch_sgs_path(walk, d_mask, d_sim, path_cell, flag, st);
+            HB_CK(cudaMemcpyAsync(scan, flag, n * 4, cudaMemcpyDeviceToDevice, st));
+            exclusive_scan(scan, n, tmp, total, st);
+            launch_sgs_index(n, path_cell, flag, scan, d_mask, rank_of, sim_cells, st);
+            HB_CK(cudaGetLastError());
+            HB_CK(cudaMemcpyAsync(&n_sim, total, sizeof(int), cudaMemcpyDeviceToHost, st));
+            HB_CK(cudaStreamSynchronize(st));
+            E.stats.launches += 2 + scan_kernels(n);
+        }
+        E.mark(STAGE_COMPACT, st);
+        double *h_u = reinterpret_cast<double *>(E.staging2((size_t)std::max(n_sim, 1) * 8));
+        double draws_ms = 0.0;
+        auto draws_f = std::async(std::launch::async, [&, n_sim]() {
+            const auto t0 = std::chrono::steady_clock::now();
+            sgs_draws((unsigned long long)seed, n_sim, h_u);
+            draws_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        });
+
+        // per category: pair table, template, search (ranks into one merged row per node)
+        auto plans = plan_f.get();
+        E.stats.plan_ms = plan_ms;
+        int ktot = 0;
+        std::vector<int> koff(kcat);
+        for (int c = 0; c < kcat; ++c)
+        {
+            koff[c] = ktot;
+            ktot += cats[c].max_nb;
+        }
+        const size_t ns = (size_t)std::max(n_sim, 1);
+        int *nb_rank = E.buf<int>("sis_nb_rank", ns * ktot);
+        HB_CK(cudaMemsetAsync(nb_rank, 0xFF, ns * ktot * 4, st)); // -1: no neighbour
+        std::vector<double *> pair64(kcat);
+        std::vector<int *> nb(kcat), nb_cnt(kcat);
+        for (int c = 0; c < kcat; ++c)
+        {
+            const Plan &pl = plans[c].first;
+            const std::vector<Offset> &tv = plans[c].second;
+            const Geom &g = pl.g;
+            const std::string sfx = std::to_string(c);
+            const size_t nk = pl.kt.vals.size();
+            double *sv = E.buf<double>(("sis_vals_" + sfx).c_str(), nk);
+            HB_CK(cudaMemcpyAsync(sv, pl.kt.vals.data(), nk * 8, cudaMemcpyHostToDevice, st));
+            const long long pn = (long long)g.pnx * g.pny * (2 * g.phz + 1);
+            pair64[c] = E.buf<double>(("sis_pair64_" + sfx).c_str(), (size_t)pn);
+            float *p32 = E.buf<float>(("sis_pair32_" + sfx).c_str(), (size_t)pn);
+            launch_build_pair(g, dev_model(pl.f.m), 1, sv, pair64[c], p32, st);
+            std::vector<int4> t4(tv.size());
+            for (size_t i = 0; i < tv.size(); ++i) t4[i] = make_int4(tv[i].dx, tv[i].dy, tv[i].dz, 0);
+            int4 *tmpl = E.buf<int4>(("sis_tmpl_" + sfx).c_str(), std::max<size_t>(t4.size(), 1));
+            if (!t4.empty())
+                HB_CK(cudaMemcpyAsync(tmpl, t4.data(), t4.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+            nb[c] = E.buf<int>(("sis_nb_" + sfx).c_str(), ns * cats[c].max_nb);
+            nb_cnt[c] = E.buf<int>(("sis_nb_cnt_" + sfx).c_str(), ns);
+            if (n_sim > 0)
+                launch_sgs_search(g, tmpl, (int)t4.size(), sim_cells, n_sim, rank_of, cats[c].max_nb, nb[c],
+                                  nb_rank + koff[c], nb_cnt[c], E.n_sm(), st, -1, ktot);
+            HB_CK(cudaGetLastError());
+            HB_CK(cudaStreamSynchronize(st)); // the host tables of this category
+            E.stats.launches += 1 + (n_sim > 0 ? 1 : 0);
+        }
+        E.mark(STAGE_SEARCH, st);
+
+        // the solves' size moments over every category's systems
+        double *mom = E.buf<double>("sgs_mom", 3);
+        HB_CK(cudaMemsetAsync(mom, 0, 24, st));
+        if (n_sim > 0)
+        {
+            for (int c = 0; c < kcat; ++c) launch_sgs_moments(n_sim, nb_cnt[c], mom, E.n_sm(), st);
+            E.stats.launches += kcat;
+        }
+        // dependency levels over the union of the categories' neighbours
+        const int level_cap = 1 << 20;
+        int *levp1 = E.buf<int>("sgs_levp1", ns);
+        int *lvl_count = E.buf<int>("sgs_lvl_count", (size_t)level_cap + 1);
+        int *scal = E.buf<int>("sgs_scal", 4);
+        HB_CK(cudaMemsetAsync(levp1, 0, ns * 4, st));
+        HB_CK(cudaMemsetAsync(lvl_count, 0, ((size_t)level_cap + 1) * 4, st));
+        HB_CK(cudaMemsetAsync(scal, 0, 16, st));
+        if (n_sim > 0)
+        {
+            launch_sgs_levels(nb_rank, nullptr, ktot, n_sim, levp1, scal + 0, lvl_count, level_cap, scal + 1,
+                              scal + 2, E.n_sm(), st);
+            E.stats.launches += 2;
+        }
+        HB_CK(cudaGetLastError());
+        int hs[4] = {0, 0, 0, 0};
+        double hmom[3] = {0, 0, 0};
+        HB_CK(cudaMemcpyAsync(hs, scal, 16, cudaMemcpyDeviceToHost, st));
+        HB_CK(cudaMemcpyAsync(hmom, mom, 24, cudaMemcpyDeviceToHost, st));
+        HB_CK(cudaStreamSynchronize(st));
+        // the simple-kriging count F(n, 1) of the Gaussian simulation, per category system
+        E.stats.sgs_flops = hmom[2] / 3.0 + hmom[1] * (0.5 + 2.0 + 15.0) + hmom[0] * (45.0 + 2.0);
+        if (hs[2] == 1) throw CudaFail{-2, "simulation level pass: a dependency wait timed out"};
+        if (hs[2] == 2) throw CudaFail{-4, "simulation needs more than 2^20 dependency levels"};
+        const int n_levels = n_sim > 0 ? hs[1] + 1 : 0;
+        std::vector<int> counts(std::max(n_levels, 1)), offs(std::max(n_levels, 1) + 1, 0);
+        if (n_levels > 0)
+        {
+            HB_CK(cudaMemcpyAsync(counts.data(), lvl_count, (size_t)n_levels * 4, cudaMemcpyDeviceToHost, st));
+            HB_CK(cudaStreamSynchronize(st));
+        }
+        for (int l = 0; l < n_levels; ++l) offs[l + 1] = offs[l] + counts[l];
+        int *order = E.buf<int>("sgs_order", ns);
+        int *level_off = E.buf<int>("sgs_level_off", (size_t)n_levels + 1);
+        int *level_fill = E.buf<int>("sgs_level_fill", (size_t)n_levels + 1);
+        if (n_levels > 0)
+        {
+            HB_CK(cudaMemcpyAsync(level_off, offs.data(), ((size_t)n_levels + 1) * 4, cudaMemcpyHostToDevice, st));
+            HB_CK(cudaMemsetAsync(level_fill, 0, ((size_t)n_levels + 1) * 4, st));
+            launch_sgs_level_fill(n_sim, levp1, level_off, level_fill, order, st);
+            HB_CK(cudaGetLastError());
+            E.stats.launches += 1;
+        }
+        E.stats.sgs_levels = n_levels;
+        E.mark(STAGE_TIES, st);
+
+        draws_f.get();
+        E.stats.draws_ms = draws_ms;
+        double *d_u = E.buf<double>("sgs_uniforms", ns);
+        if (n_sim > 0)
+        {
+            HB_CK(cudaMemcpyAsync(d_u, h_u, (size_t)n_sim * 8, cudaMemcpyHostToDevice, st));
+            E.stats.h2d += (long long)n_sim * 8;
+        }
+        E.mark(STAGE_PREPARE, st);
+        double *probs = E.buf<double>("sis_probs", ns * ncat);
+        signed char *st_rank = E.buf<signed char>("sgs_st_rank", ns);
+        for (int l = 0; l < n_levels; ++l)
+        {
+            for (int c = 0; c < kcat; ++c)
+            {
+                SisSolveArgs sa{plans[c].first.g, order + offs[l], counts[l], sim_cells, nb[c], nb_cnt[c],
+                                cats[c].max_nb, pair64[c], d_data, c, ncat, (float)cats[c].marginal, d_means[c],
+                                probs, st_rank, correlogram && means ? 1 : 0};
+                HB_CK(launch_sis_solve(sa, E.n_sm(), st));
+            }
+            launch_sis_sample(order + offs[l], counts[l], sim_cells, probs, ncat, d_u, d_data, st);
+            E.stats.launches += kcat + 1;
+        }
+        HB_CK(cudaGetLastError());
+        E.mark(STAGE_SOLVE, st);
+        signed char *d_status =
+            opt.status ? (io.device ? opt.status : E.buf<signed char>("status", (size_t)n)) : nullptr;
+        // masks and status (no transform): the simulation's finalize on an empty CDF
+        launch_sgs_finalize(n, nullptr, d_mask, rank_of, n_sim, st_rank, d_status, nullptr, nullptr, 0, st);
+        HB_CK(cudaGetLastError());
+        E.stats.launches += 1;
+        E.mark(STAGE_FINALIZE, st);
+        if (!io.device)
+        {
+            to_host(E, data, d_data, (size_t)n, io);
+            to_host(E, mask, d_mask, (size_t)n, io);
+            if (opt.status) to_host(E, opt.status, d_status, (size_t)n, io);
+        }
+        E.mark(STAGE_DOWNLOAD, st);
+        E.stats.kriged = n_sim;
+        end_call(E, st);
+        return 0;
+    }
+    catch (const CudaFail &f)
+    {
+        set_error(f.msg);
+        return f.code;
+    }
+    catch (const std::exception &ex)
+    {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
 // ------------------------------------------------------------------ cokriging
 int cokriging(const int *dims, const float *pdata, const unsigned char *pmask, const float *sdata,
               const unsigned char *smask, const CokArgs &a, float *out_data, unsigned char *out_mask,

@@ -134,6 +134,13 @@ int sgs_simulation(const int *dims, float *data, unsigned char *mask, const unsi
 int cokriging(const int *dims, const float *pdata, const unsigned char *pmask, const float *sdata,
               const unsigned char *smask, const CokArgs &a, float *out_data, unsigned char *out_mask,
               const Options &opt);
+// Sequential indicator simulation in place on data (categories) / mask
+// (sequential_indicator_simulation.cpp:24-185): cats per category; means (LVM)
+// one float array per category or null, with `correlogram` the correlogram
+// weights (my_kriging_weights.h:363-505); opt.status as for the simulation.
+int sis_simulation(const int *dims, unsigned char *data, unsigned char *mask, const unsigned char *sim_mask,
+                   const std::vector<IkArgs> &cats, const float *const *means, long long seed, const Options &opt,
+                   bool correlogram = false);
 int indicator_kriging(const int *dims, const unsigned char *in_data, const unsigned char *in_mask,
                       const std::vector<IkArgs> &cats, unsigned char *out_data, unsigned char *out_mask,
                       const Options &opt);

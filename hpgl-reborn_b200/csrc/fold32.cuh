@@ -27,13 +27,16 @@ constexpr size_t kFold32SysBytes = ((size_t)kFold32NP * kFold32LD * 8 + kFold32N
 // the system's lanes. after_assembly() and after_factor() run at those points
 // (the callers issue prefetches there). Returns true when a pivot is not
 // positive (or NaN), or, with EPS_PIVOT, below machine epsilon (the test of
-// the reference's Gaussian elimination, gauss_solver.cpp:37-41).
-template <int QB, bool EPS_PIVOT = false, typename F1, typename F2>
+// the reference's Gaussian elimination, gauss_solver.cpp:37-41). With SCALE,
+// A[r][c] = pair * (sig_r * sig_c), SIG holding the 32 row scales (visible to
+// the system's lanes) and sig_a / sig_b the lane's own.
+template <int QB, bool EPS_PIVOT = false, bool SCALE = false, typename F1, typename F2>
 __device__ __forceinline__ bool fold32_solve(const double *pair_c, const int *LIN, double *M, unsigned gm, int t,
                                              bool live_a, bool live_b, int lin_a, int lin_b,
                                              const double (&rhs_a_in)[QB], const double (&rhs_b_in)[QB],
                                              double (&xa)[QB], double (&xb)[QB], F1 after_assembly,
-                                             F2 after_factor)
+                                             F2 after_factor, const double *SIG = nullptr, double sig_a = 1.0,
+                                             double sig_b = 1.0)
 {
     constexpr int NP = kFold32NP, G = kFold32G, LD = kFold32LD;
     const int rb = NP - 1 - t;
@@ -44,7 +47,11 @@ __device__ __forceinline__ bool fold32_solve(const double *pair_c, const int *LI
     for (int c = 0; c < G; ++c)
     {
         double e = 0.0;
-        if (live_a && c <= t) e = __ldg(base_a - LIN[c]);
+        if (live_a && c <= t)
+        {
+            e = __ldg(base_a - LIN[c]);
+            if (SCALE) e = __dmul_rn(e, __dmul_rn(sig_a, SIG[c]));
+        }
         if (!live_a && c == t) e = 1.0;
         ra[c] = e;
     }
@@ -52,7 +59,11 @@ __device__ __forceinline__ bool fold32_solve(const double *pair_c, const int *LI
     for (int c = 0; c < NP; ++c)
     {
         double e = 0.0;
-        if (live_b && c <= rb) e = __ldg(base_b - LIN[c]);
+        if (live_b && c <= rb)
+        {
+            e = __ldg(base_b - LIN[c]);
+            if (SCALE) e = __dmul_rn(e, __dmul_rn(sig_b, SIG[c]));
+        }
         if (!live_b && c == rb) e = 1.0;
         rbv[c] = e;
     }

@@ -146,7 +146,31 @@ void launch_sgs_index(long long n, const int *path_cell, const int *flag, const 
 // fixed_rank >= 0); nb_rank may be null.
 void launch_sgs_search(const Geom &g, const int4 *tmpl, int n_tmpl, const int *sim_cells, int n_sim,
                        const int *rank_of, int k, int *nb, int *nb_rank, int *nb_cnt, int n_sm, cudaStream_t st,
-                       int fixed_rank = -1);
+                       int fixed_rank = -1, int rank_stride = 0);
+// SIS (sgs.cu): one category's indicator SK probabilities of a level, then the draws
+constexpr int kSisMaxCat = 16;
+struct SisSolveArgs
+{
+    Geom g;
+    const int *order;
+    int n_items;
+    const int *sim_cells;
+    const int *nb; // this category's neighbour cells, k per rank
+    const int *nb_cnt;
+    int k;
+    const double *pair64;
+    const uint8_t *data; // categories of the informed cells
+    int category;
+    int ncat;
+    float marginal;    // the category's mean (float, as the reference stores it)
+    const float *means; // LVM: the category's mean per cell, or null
+    double *probs;      // per rank, ncat entries
+    signed char *st_rank;
+    int correlogram;    // LVM correlogram weights (corellogramed_weights_3)
+};
+cudaError_t launch_sis_solve(const SisSolveArgs &a, int n_sm, cudaStream_t st);
+void launch_sis_sample(const int *order, int n_items, const int *sim_cells, const double *probs, int ncat,
+                       const double *uniforms, uint8_t *data, cudaStream_t st);
 void launch_sgs_levels(const int *nb_rank, const int *nb_cnt, int k, int n_sim, int *levp1, int *ticket,
                        int *level_count, int level_cap, int *max_level, int *err, int n_sm, cudaStream_t st);
 void launch_sgs_moments(int n_sim, const int *nb_cnt, double *mom, int n_sm, cudaStream_t st); // mom: 3, zeroed

@@ -219,7 +219,7 @@ __global__ void k_sgs_index(long long n, const int *__restrict__ path_cell, cons
 __global__ void __launch_bounds__(256) k_sgs_search(const Geom g, const int4 *__restrict__ tmpl, int n_tmpl,
                                                     const int *__restrict__ sim_cells, int n_sim,
                                                     const int *__restrict__ rank_of, int k, int fixed_rank,
-                                                    int *__restrict__ nb, int *__restrict__ nb_rank,
+                                                    int *__restrict__ nb, int *__restrict__ nb_rank, int rank_stride,
                                                     int *__restrict__ nb_cnt)
 {
     const int lane = threadIdx.x & 31;
@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(256) k_sgs_search(const Geom g, const int4 *__
         const int x = cell % g.nx, y = (int)((cell / g.nx) % g.ny), z = (int)(cell / ((long long)g.nx * g.ny));
         int found = 0;
         int *out = nb + r * (long long)k;
-        int *out_rank = nb_rank ? nb_rank + r * (long long)k : nullptr;
+        int *out_rank = nb_rank ? nb_rank + r * (long long)rank_stride : nullptr;
         const int thr = fixed_rank >= 0 ? fixed_rank : (int)r;
         for (int base = 0; base < n_tmpl && found < k; base += 32)
         {
@@ -322,7 +322,7 @@ __global__ void __launch_bounds__(256) k_sgs_levels(const int *__restrict__ nb_r
         int L = 0;
         if (r < n_sim)
         {
-            const int n = nb_cnt[r];
+            const int n = nb_cnt ? nb_cnt[r] : k; // without counts: k slots, -1 where empty
             const int *row = nb_rank + r * (long long)k;
             // sixteen neighbours at a time: their ranks, then every published level
             // at once; waits only for the missing ones
@@ -693,6 +693,138 @@ __global__ void __launch_bounds__(kSgsBlockThreads) k_sgs_solve_block(const SgsS
     }
 }
 
+// ------------------------------------------------------------------ SIS
+// One category's probability for the nodes of a level (sequential_indicator_
+// simulation.cpp:77-108): the SK estimate of the indicator (category == c)
+// from the category's neighbours, accumulated in double around the float
+// mean (combine for a double result); the mean where kriging fails. The
+// status of a rank is the largest over its categories.
+constexpr int kSisFoldThreads = 256;
+constexpr size_t kSisSysBytes = kFold32SysBytes + kFold32NP * 8; // plus the 32 row scales
+
+// the correlogram scale of a mean (corellogramed_weights_3, my_kriging_weights.h:407-438)
+__device__ __forceinline__ double sis_sigma(float mean)
+{
+    double m = (double)mean;
+    if (m == 0) m = __dadd_rn(m, 0.00001);
+    if (m == 1) m = __dsub_rn(m, 0.00001);
+    return __dsqrt_rn(__dmul_rn(m, __dsub_rn(1.0, m)));
+}
+
+// CORR: correlogram weights (LVM): A_ij = C_ij (s_i s_j), b_i = C_ic (s_i s_c)
+template <bool CORR>
+__global__ void __launch_bounds__(kSisFoldThreads, 1) k_sis_solve_fold(const SisSolveArgs a)
+{
+    constexpr int NP = kFold32NP, G = kFold32G;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int h = lane / G, t = lane % G, rb = NP - 1 - t;
+    const unsigned gm = 0xFFFFu << (h * G);
+    unsigned char *gb = smem + kSisSysBytes * (warp * 2 + h);
+    double *M = reinterpret_cast<double *>(gb);
+    int *LIN = reinterpret_cast<int *>(gb + (size_t)NP * kFold32LD * 8);
+    double *SIG = reinterpret_cast<double *>(gb + kFold32SysBytes); // the system's row scales
+    const Geom &g = a.g;
+    const long long pc = g.pair_center;
+    const int stride = gridDim.x * nwarps * 2;
+    for (int it0 = (blockIdx.x * nwarps + warp) * 2; it0 < a.n_items; it0 += stride)
+    {
+        const int it = it0 + h;
+        const bool valid = it < a.n_items;
+        const int r = valid ? a.order[it] : 0;
+        const int cell = valid ? a.sim_cells[r] : 0;
+        const int n = valid ? a.nb_cnt[r] : 0;
+        const int cx = cell % g.nx, cy = (int)((cell / g.nx) % g.ny), cz = (int)(cell / ((long long)g.nx * g.ny));
+        const bool live_a = t < n, live_b = rb < n;
+        int lin_a = 0, lin_b = 0;
+        float da = 0.0f, db = 0.0f; // indicator - mean, in float
+        double sa = 1.0, sb = 1.0;
+        const float mc = a.means ? (valid ? a.means[cell] : 0.0f) : a.marginal;
+        if (live_a)
+        {
+            const int q = a.nb[(long long)r * a.k + t];
+            lin_a = pair_lin(g, q % g.nx - cx, (int)((q / g.nx) % g.ny) - cy, (int)(q / ((long long)g.nx * g.ny)) - cz);
+            const float mq = a.means ? a.means[q] : mc;
+            da = __fsub_rn(a.data[q] == a.category ? 1.0f : 0.0f, mq);
+            if (CORR) sa = sis_sigma(mq);
+        }
+        if (live_b)
+        {
+            const int q = a.nb[(long long)r * a.k + rb];
+            lin_b = pair_lin(g, q % g.nx - cx, (int)((q / g.nx) % g.ny) - cy, (int)(q / ((long long)g.nx * g.ny)) - cz);
+            const float mq = a.means ? a.means[q] : mc;
+            db = __fsub_rn(a.data[q] == a.category ? 1.0f : 0.0f, mq);
+            if (CORR) sb = sis_sigma(mq);
+        }
+        LIN[t] = lin_a;
+        LIN[rb] = lin_b;
+        if (CORR)
+        {
+            SIG[t] = sa;
+            SIG[rb] = sb;
+        }
+        __syncwarp(gm);
+        const double sc = CORR ? sis_sigma(mc) : 1.0;
+        double rhs_a[1] = {live_a ? __ldg(a.pair64 + pc + lin_a) : 0.0};
+        double rhs_b[1] = {live_b ? __ldg(a.pair64 + pc + lin_b) : 0.0};
+        if (CORR)
+        {
+            rhs_a[0] = __dmul_rn(rhs_a[0], __dmul_rn(sa, sc));
+            rhs_b[0] = __dmul_rn(rhs_b[0], __dmul_rn(sb, sc));
+        }
+        double xa[1], xb[1];
+        const bool fail = fold32_solve<1, false, CORR>(a.pair64 + pc, LIN, M, gm, t, live_a, live_b, lin_a, lin_b,
+                                                       rhs_a, rhs_b, xa, xb, [] {}, [] {}, SIG, sa, sb);
+        const double ta = __dmul_rn(xa[0], (double)da), tb = __dmul_rn(xb[0], (double)db);
+        double prob = (double)mc;
+#pragma unroll 4
+        for (int i = 0; i < NP; ++i)
+        {
+            const bool lo = i < G;
+            const double ti = __shfl_sync(gm, lo ? ta : tb, lo ? i : NP - 1 - i, G);
+            if (i < n) prob = __dadd_rn(prob, ti);
+        }
+        if (valid && t == 0)
+        {
+            const int status = n == 0 ? 1 : (fail ? 2 : 0);
+            a.probs[(long long)r * a.ncat + a.category] = status == 0 ? prob : (double)mc;
+            if (a.category == 0 || status > a.st_rank[r]) a.st_rank[r] = (signed char)status;
+        }
+        __syncwarp(gm);
+    }
+}
+
+// sample (sample.cpp:8-21): the first category whose running sum exceeds
+// u times the sum; with two categories p1 = 1 - p0 (median SIS)
+__global__ void k_sis_sample(const int *__restrict__ order, int n_items, const int *__restrict__ sim_cells,
+                             const double *__restrict__ probs, int ncat, const double *__restrict__ uniforms,
+                             uint8_t *__restrict__ data)
+{
+    for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < n_items; it += gridDim.x * blockDim.x)
+    {
+        const int r = order[it];
+        const double *p = probs + (long long)r * ncat;
+        double pr[kSisMaxCat];
+        for (int c = 0; c < ncat; ++c) pr[c] = p[c];
+        if (ncat == 2) pr[1] = __dsub_rn(1.0, pr[0]);
+        double sum = 0.0;
+        for (int c = 0; c < ncat; ++c) sum = __dadd_rn(sum, pr[c]);
+        const double s = __dmul_rn(uniforms[r], sum);
+        double acc = 0.0;
+        int pick = ncat - 1;
+        for (int c = 0; c < ncat; ++c)
+        {
+            acc = __dadd_rn(acc, pr[c]);
+            if (s < acc)
+            {
+                pick = c;
+                break;
+            }
+        }
+        data[sim_cells[r]] = (uint8_t)pick;
+    }
+}
+
 // ------------------------------------------------------------------ launchers
 void launch_sgs_forward(long long n, float *data, const uint8_t *mask, const float *means_in, float *means_out,
                         const float *cv, const float *cp, long long cn, cudaStream_t st)
@@ -719,10 +851,10 @@ void launch_sgs_index(long long n, const int *path_cell, const int *flag, const 
 }
 void launch_sgs_search(const Geom &g, const int4 *tmpl, int n_tmpl, const int *sim_cells, int n_sim,
                        const int *rank_of, int k, int *nb, int *nb_rank, int *nb_cnt, int n_sm, cudaStream_t st,
-                       int fixed_rank)
+                       int fixed_rank, int rank_stride)
 {
     k_sgs_search<<<n_sm * 8, 256, 0, st>>>(g, tmpl, n_tmpl, sim_cells, n_sim, rank_of, k, fixed_rank, nb, nb_rank,
-                                           nb_cnt);
+                                           rank_stride > 0 ? rank_stride : k, nb_cnt);
 }
 void launch_sgs_levels(const int *nb_rank, const int *nb_cnt, int k, int n_sim, int *levp1, int *ticket,
                        int *level_count, int level_cap, int *max_level, int *err, int n_sm, cudaStream_t st)
@@ -738,6 +870,25 @@ void launch_sgs_level_fill(int n_sim, const int *levp1, const int *level_off, in
                            cudaStream_t st)
 {
     k_sgs_level_fill<<<1184, 256, 0, st>>>(n_sim, levp1, level_off, level_fill, order);
+}
+cudaError_t launch_sis_solve(const SisSolveArgs &a, int n_sm, cudaStream_t st)
+{
+    if (a.n_items <= 0) return cudaSuccess;
+    const int spb = kSisFoldThreads / kFold32G;
+    const size_t smem = kSisSysBytes * spb;
+    auto kern = a.correlogram ? k_sis_solve_fold<true> : k_sis_solve_fold<false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int blocks = std::min((a.n_items + spb - 1) / spb, n_sm);
+    kern<<<blocks, kSisFoldThreads, smem, st>>>(a);
+    return cudaGetLastError();
+}
+void launch_sis_sample(const int *order, int n_items, const int *sim_cells, const double *probs, int ncat,
+                       const double *uniforms, uint8_t *data, cudaStream_t st)
+{
+    if (n_items <= 0) return;
+    k_sis_sample<<<std::min((n_items + 255) / 256, 1184), 256, 0, st>>>(order, n_items, sim_cells, probs, ncat,
+                                                                       uniforms, data);
 }
 size_t sgs_block_smem(int k) { return (size_t)k * k * 8 + 3 * (size_t)k * 8 + 2 * (size_t)k * 4; }
 

@@ -4,3 +4,4 @@ from .geo import __all__  # noqa: F401
 from .hpgl_wrap import last_stats  # noqa: F401
 from .cdf import CdfData, calc_cdf  # noqa: F401
 from .sgs import sgs_simulation  # noqa: F401
+from .sis import sis_simulation  # noqa: F401

@@ -135,6 +135,17 @@ def _clone_prop(prop):
     return ContProperty(data2, mask2)
 
 
+def _empty_clone(prop):
+    """A property of the same shape with every value 0 and every cell uninformed."""
+    data2 = prop.data.copy("F")
+    data2.fill(0)
+    mask2 = prop.mask.copy("F")
+    mask2.fill(0)
+    if isinstance(prop, IndProperty):
+        return IndProperty(data2, mask2, prop.indicator_count)
+    return ContProperty(data2, mask2)
+
+
 def _dims(grid, prop):
     n = grid.x * grid.y * grid.z
     if prop.data.size != n:

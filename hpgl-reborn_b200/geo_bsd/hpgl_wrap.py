@@ -130,7 +130,8 @@ EXPORTS = [
     "hpgl_set_thread_num", "hpgl_get_thread_num", "hpgl_ordinary_kriging", "hpgl_simple_kriging",
     "hpgl_simple_kriging_weights", "hpgl_indicator_kriging", "hpgl_median_ik", "hpgl_lvm_kriging",
     "hpgl_sgs_simulation", "hpgl_sgs_lvm_simulation", "hpgl_simple_cokriging_mark1", "hpgl_simple_cokriging_mark2",
-    "hpgl_b200_cokriging_ex", "hpgl_read_inc_file_float", "hpgl_read_inc_file_byte", "hpgl_write_inc_file_float",
+    "hpgl_b200_cokriging_ex", "hpgl_sis_simulation", "hpgl_sis_simulation_lvm", "hpgl_b200_sis_ex",
+    "hpgl_read_inc_file_float", "hpgl_read_inc_file_byte", "hpgl_write_inc_file_float",
     "hpgl_write_inc_file_byte", "hpgl_write_gslib_cont_property", "hpgl_write_gslib_byte_property",
     "hpgl_b200_cont_kriging_ex", "hpgl_b200_lvm_kriging_ex", "hpgl_b200_sgs_ex", "hpgl_b200_sgs_draws", "hpgl_b200_indicator_kriging_ex", "hpgl_b200_median_ik_ex",
     "hpgl_b200_find_neighbours", "hpgl_b200_last_stats", "hpgl_b200_host_alloc", "hpgl_b200_host_free",
@@ -218,6 +219,15 @@ def _load():
     lib.hpgl_write_gslib_byte_property.restype = C.c_int
     lib.hpgl_write_gslib_byte_property.argtypes = [C.POINTER(_HPGL_IND_MASKED_ARRAY), C.c_char_p, C.c_char_p,
                                                    C.c_double, C.POINTER(C.c_ubyte), C.c_int]
+    ima = C.POINTER(_HPGL_IND_MASKED_ARRAY)
+    lib.hpgl_sis_simulation.restype = None
+    lib.hpgl_sis_simulation.argtypes = [ima, C.POINTER(_HPGL_IK_PARAMS), C.c_int, C.c_int, C.POINTER(_HPGL_UBYTE_ARRAY)]
+    lib.hpgl_sis_simulation_lvm.restype = None
+    lib.hpgl_sis_simulation_lvm.argtypes = [ima, C.POINTER(_HPGL_IK_PARAMS), C.POINTER(_HPGL_FLOAT_ARRAY), C.c_int,
+                                            C.c_int, C.POINTER(_HPGL_UBYTE_ARRAY), C.c_int]
+    lib.hpgl_b200_sis_ex.restype = C.c_int
+    lib.hpgl_b200_sis_ex.argtypes = [i_p, vp, vp, vp, C.POINTER(_HPGL_IK_PARAMS), C.c_int, vp, C.c_int, C.c_int,
+                                     C.POINTER(_HPGL_B200_OPTIONS)]
     lib.hpgl_b200_sgs_draws.restype = C.c_int
     lib.hpgl_b200_sgs_draws.argtypes = [C.c_longlong, C.c_longlong, vp]
     lib.hpgl_b200_indicator_kriging_ex.restype = C.c_int

@@ -15,18 +15,10 @@ import numpy
 
 from . import hpgl_wrap as W
 from .cdf import CdfData
-from .geo import CovarianceModel, _clone_prop, _to_prop
+from .geo import CovarianceModel, _clone_prop, _empty_clone, _to_prop
 from .validation import GridValidator, ParameterValidator
 
 __all__ = ["sgs_simulation"]
-
-
-def _empty_clone(prop):
-    data = prop.data.copy("F")
-    data.fill(0)
-    mask = prop.mask.copy("F")
-    mask.fill(0)
-    return type(prop)(data, mask)
 
 
 def normed_cov_model(cov_model):

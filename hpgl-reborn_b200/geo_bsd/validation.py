@@ -35,6 +35,7 @@ class ValidationConstants:
     MAX_PROBABILITY = 1.0
     MAX_INDICATORS = 256
     MIN_SEED = 0
+    PROBABILITY_SUM_TOLERANCE = 0.01
 
 
 class ValidationError(Exception):
@@ -213,6 +214,17 @@ class ParameterValidator:
             raise CriticalValidationError(
                 f"{name} = {prob} outside valid range "
                 f"[{ValidationConstants.MIN_PROBABILITY}, {ValidationConstants.MAX_PROBABILITY}]", name)
+
+    @staticmethod
+    def validate_probability_sum(probs) -> None:
+        """The probabilities must sum to 1 within PROBABILITY_SUM_TOLERANCE (validation.py:522-543)."""
+        prob_sum = sum(probs)
+        if _bad(prob_sum):
+            raise CriticalValidationError("Probability sum is NaN or infinite", "probabilities")
+        diff = abs(prob_sum - 1.0)
+        if diff > ValidationConstants.PROBABILITY_SUM_TOLERANCE:
+            raise CriticalValidationError(
+                f"Probabilities sum to {prob_sum}, expected 1.0 (difference: {diff})", "probabilities")
 
     @staticmethod
     def validate_indicator_count(count: int) -> None:

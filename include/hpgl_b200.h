@@ -149,6 +149,23 @@ void hpgl_simple_cokriging_mark2(struct hpgl_cont_masked_array_t *primary_data,
                                  struct hpgl_cokriging_m2_params_t *params,
                                  struct hpgl_cont_masked_array_t *output_data);
 
+/* Replaces api.h:279-286 / api.cpp:603-635 (sequential_indicator_simulation.cpp:24-145):
+ * sequential indicator simulation, in place, of every node of data that is not
+ * informed and whose simulation_mask byte (when given) is 1; params: one entry
+ * per category (two categories: median SIS, the first kriged). Grids whose
+ * walk does not visit every node (2, 4, 6, 8, 12 cells), more than 16
+ * categories and max_neighbours above 32 are rejected. */
+void hpgl_sis_simulation(struct hpgl_ind_masked_array_t *data, struct hpgl_ik_params_t *params, int indicator_count,
+                         int seed, struct hpgl_ubyte_array_t *simulation_mask);
+/* Replaces api.h:288-296 / api.cpp:637-677 (sequential_indicator_simulation.cpp:147-183):
+ * SIS around a locally varying mean per category (mean_data: indicator_count
+ * arrays); use_correlograms != 0 selects the correlogram weights
+ * (corellogramed_weights_3, my_kriging_weights.h:363-505: the SK system scaled
+ * by sqrt(m (1 - m)) of each cell's mean). */
+void hpgl_sis_simulation_lvm(struct hpgl_ind_masked_array_t *data, struct hpgl_ik_params_t *params,
+                             struct hpgl_float_array_t *mean_data, int indicator_count, int seed,
+                             struct hpgl_ubyte_array_t *simulation_mask, int use_correlograms);
+
 /* Property files. Replace api.h:171-214 / api.cpp:53-252 (read_inc_file.cpp,
  * property_writer.cpp): the INC text format (a property-name line, then
  * whitespace-separated values, "--" comments to the end of a line, a "/"
@@ -232,6 +249,14 @@ int hpgl_b200_cokriging_ex(int mark, const int *dims, const float *pdata, const 
                            const float *sdata, const unsigned char *smask,
                            const struct hpgl_cokriging_m1_params_t *m1, const struct hpgl_cokriging_m2_params_t *m2,
                            float *out_data, unsigned char *out_mask, const struct hpgl_b200_options_t *opt);
+/* SIS with options (hpgl_sis_simulation's rules): means, when not NULL, holds
+ * indicator_count per-cell arrays (LVM, use_correlograms as for
+ * hpgl_sis_simulation_lvm); arrays on the device under
+ * HPGL_B200_DEVICE_POINTERS; opt->status as for hpgl_b200_sgs_ex (the largest
+ * status over the node's categories). */
+int hpgl_b200_sis_ex(const int *dims, unsigned char *data, unsigned char *mask, const unsigned char *sim_mask,
+                     const struct hpgl_ik_params_t *params, int indicator_count, const float *const *means, int seed,
+                     int use_correlograms, const struct hpgl_b200_options_t *opt);
 /* The simulation's uniform draws (host): out[i] = the i-th call of
  * std::uniform_real_distribution<double>(0, 1) on a std::mt19937 seeded with
  * `seed` (bs_random_generator.cpp:9-25), as sgs_simulation consumes them, one

@@ -1279,6 +1279,39 @@ int ko_cokriging(int mark, const int *dims, const float *pdata, const unsigned c
     return 0;
 }
 
+// The correlogram scale of an indicator mean (my_kriging_weights.h:407-436):
+// sqrt(m (1 - m)) with 0 and 1 moved inside by 1e-5.
+static double corr_sigma(double m)
+{
+    if (m == 0) m += 0.00001;
+    if (m == 1) m -= 0.00001;
+    return std::sqrt(m * (1 - m));
+}
+
+// corellogramed_weights_3 (my_kriging_weights.h:363-505): the SK system with
+// A_ij = C_ij (s_i s_j) and b_i = C_ic (s_i s_c), solved by Cholesky; the
+// weights are used as they come out (no rescaling).
+static bool corr_weights(const Flavour &f, int cx, int cy, int cz, double mean_c, const std::vector<int> &xs,
+                         const std::vector<int> &ys, const std::vector<int> &zs, const std::vector<double> &means,
+                         std::vector<double> &w)
+{
+    const int n = (int)xs.size();
+    if (n <= 0) return false;
+    const double sc = corr_sigma(mean_c);
+    std::vector<double> sg(n), A((size_t)n * n);
+    for (int i = 0; i < n; ++i) sg[i] = corr_sigma(means[i]);
+    w.assign(n, 0.0);
+    for (int i = 0; i < n; ++i)
+    {
+        for (int j = 0; j < n; ++j)
+            A[(size_t)i * n + j] = f.at(xs[i], ys[i], zs[i], xs[j], ys[j], zs[j]) * (sg[i] * sg[j]);
+        w[i] = f.at(xs[i], ys[i], zs[i], cx, cy, cz) * (sg[i] * sc);
+    }
+    if (!cholesky(A, n)) return false;
+    chol_solve(A, n, w);
+    return true;
+}
+
 // Sequential indicator simulation (sequential_indicator_simulation.cpp:24-185):
 // the walk of the simulation; per visited node that is not informed and whose
 // simulation mask is 1, for every category c (only c = 0 with two categories,
@@ -1289,13 +1322,14 @@ int ko_cokriging(int mark, const int *dims, const float *pdata, const unsigned c
 // std::uniform_real_distribution draw u picks the first category whose running
 // sum of probabilities exceeds u times their sum (sample.cpp:8-21). `params`:
 // per category cov_type, ranges[3], angles[3], sill, nugget; radiuses (3 per
-// category), max_nb, marginal. means: per category a float per cell, or null.
+// category), max_nb, marginal. means: per category a float per cell, or null;
+// with means, `corr` selects the correlogram weights (corellogram_weight_calculator_t).
 // Returns 0, -1 on bad arguments, -3 when the walk does not visit every node
 // (the reference throws at the end of such a path).
 int ko_sis(const int *dims, unsigned char *data, unsigned char *mask, const unsigned char *sim_mask, int ncat,
            const int *cov_types, const double *ranges, const double *angles, const double *sills,
            const double *nuggets, const int *radiuses, const int *max_nb, const double *marginals,
-           const float *const *means, long long seed, int *out_status)
+           const float *const *means, long long seed, int *out_status, int corr)
 {
     Grid g = {dims[0], dims[1], dims[2]};
     const long size = g.size();
@@ -1317,7 +1351,7 @@ int ko_sis(const int *dims, unsigned char *data, unsigned char *mask, const unsi
     if (out_status)
         for (long i = 0; i < size; ++i) out_status[i] = -1;
     std::vector<int> idx, xs, ys, zs;
-    std::vector<double> w, probs(ncat);
+    std::vector<double> w, probs(ncat), nbm;
     const long first = path.R;
     for (long counter = 0; counter < size; ++counter)
     {
@@ -1347,7 +1381,16 @@ int ko_sis(const int *dims, unsigned char *data, unsigned char *mask, const unsi
                 zs.resize(n);
                 for (int i = 0; i < n; ++i) g.coord(idx[i], xs[i], ys[i], zs[i]);
                 double var;
-                if (weights<double>(f[c], false, x, y, z, xs, ys, zs, w, var))
+                bool ok;
+                if (corr && means)
+                {
+                    nbm.resize(n);
+                    for (int i = 0; i < n; ++i) nbm[i] = (double)means[c][idx[i]];
+                    ok = corr_weights(f[c], x, y, z, (double)mc, xs, ys, zs, nbm, w);
+                }
+                else
+                    ok = weights<double>(f[c], false, x, y, z, xs, ys, zs, w, var);
+                if (ok)
                 {
                     status = KI_SUCCESS;
                     double r = (double)mc;

@@ -71,7 +71,7 @@ def load(which: str):
         lib.ko_sgs_path.argtypes = [C.c_longlong, C.c_longlong, _i, C.c_longlong]
         lib.ko_mt_draws.argtypes = [C.c_longlong, C.c_longlong, _d]
         lib.ko_sis.argtypes = [_i, _u8, _u8, _u8, C.c_int, _i, _d, _d, _d, _d, _i, _i, _d, C.c_void_p,
-                               C.c_longlong, _i]
+                               C.c_longlong, _i, C.c_int]
         lib.ko_cokriging.argtypes = [C.c_int, _i, _f, _u8, _f, _u8, C.c_int, _d, _d, C.c_double, C.c_double, C.c_int,
                                      _d, _d, C.c_double, C.c_double, _i, C.c_int, C.c_double, C.c_double,
                                      C.c_double, C.c_double, _f, _u8, _i, C.c_int]
@@ -360,6 +360,31 @@ def cokriging(mark, dims, pdata, pmask, sdata, smask, cov, radiuses, k, primary_
     return od, om, st
 
 
+class _Ind(C.Structure):
+    _fields_ = [("data", _u8), ("mask", _u8), ("shape", _Shape), ("indicator_count", C.c_int)]
+
+
+class _IkP(C.Structure):
+    _fields_ = [("t", C.c_int), ("r", C.c_double * 3), ("a", C.c_double * 3), ("sill", C.c_double),
+                ("nugget", C.c_double), ("rad", C.c_int * 3), ("k", C.c_int), ("marginal", C.c_double)]
+
+
+def ref_sis(dims, data, mask, covs, radiuses, ks, marginals, seed):
+    """The reference's hpgl_sis_simulation on copies of data/mask (no
+    simulation mask); returns the simulated categories and mask."""
+    lib = ref_api()
+    od = _arr(data, np.uint8).copy()
+    om = _arr(mask, np.uint8).copy()
+    sh = _Shape((C.c_int * 3)(*dims), (C.c_int * 3)(1, dims[0], dims[0] * dims[1]))
+    m = len(covs)
+    a = _Ind(od.ctypes.data_as(_u8), om.ctypes.data_as(_u8), sh, m)
+    p = (_IkP * m)(*[_IkP(int(c.cov_type), (C.c_double * 3)(*c.ranges), (C.c_double * 3)(*c.angles),
+                          float(c.sill), float(c.nugget), (C.c_int * 3)(*radiuses[i]), int(ks[i]),
+                          float(marginals[i])) for i, c in enumerate(covs)])
+    lib.hpgl_sis_simulation(C.byref(a), p, m, int(seed), None)
+    return od, om
+
+
 class _CovP(C.Structure):
     _fields_ = [("t", C.c_int), ("r", C.c_double * 3), ("a", C.c_double * 3), ("sill", C.c_double),
                 ("nugget", C.c_double)]
@@ -390,9 +415,10 @@ def ref_cokriging_mark1(dims, pdata, pmask, sdata, smask, cov, radiuses, k, pm, 
     return od, om
 
 
-def sis(dims, data, mask, covs, radiuses, ks, marginals, seed, sim_mask=None, means=None):
+def sis(dims, data, mask, covs, radiuses, ks, marginals, seed, sim_mask=None, means=None, correlogram=False):
     """Sequential indicator simulation (port): covs / radiuses / ks / marginals per
-    category; means (LVM) a list of per-cell float arrays. Returns (data, mask, status)."""
+    category; means (LVM) a list of per-cell float arrays, with `correlogram` the
+    correlogram weights. Returns (data, mask, status)."""
     lib = load("port")
     ncat = len(covs)
     data = _arr(data, np.uint8).copy()
@@ -414,7 +440,8 @@ def sis(dims, data, mask, covs, radiuses, ks, marginals, seed, sim_mask=None, me
         mp = (_f * ncat)(*[k.ctypes.data_as(_f) for k in keep])
     rc = lib.ko_sis(_ptr(_arr(dims, np.int32), _i), _ptr(data, _u8), _ptr(mask, _u8), _ptr(sm, _u8), ncat,
                     _ptr(ct, _i), _ptr(rg, _d), _ptr(an, _d), _ptr(si, _d), _ptr(nu, _d), _ptr(rd, _i),
-                    _ptr(kk, _i), _ptr(mg, _d), mp, int(seed), _ptr(st, _i))
+                    _ptr(kk, _i), _ptr(mg, _d), mp, int(seed), _ptr(st, _i),
+                    int(bool(correlogram)))
     if rc:
         raise RuntimeError(f"sis failed (rc={rc})")
     return data, mask, st

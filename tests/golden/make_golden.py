@@ -213,9 +213,9 @@ def api_cokriging(lib, mark, dims, pdata, pmask, sdata, smask, cov, rad, k, pm, 
     return od, om
 
 
-def api_sis(lib, dims, data, mask, covs, rads, ks, marginals, seed, sim_mask=None, means=None):
-    """The reference's hpgl_sis_simulation / hpgl_sis_simulation_lvm (no correlograms);
-    returns the output data and mask."""
+def api_sis(lib, dims, data, mask, covs, rads, ks, marginals, seed, sim_mask=None, means=None, corr=False):
+    """The reference's hpgl_sis_simulation / hpgl_sis_simulation_lvm (correlogram
+    weights with `corr`); returns the output data and mask."""
     od = np.ascontiguousarray(data, np.uint8).copy()
     om = np.ascontiguousarray(mask, np.uint8).copy()
     up = C.POINTER(C.c_ubyte)
@@ -239,7 +239,7 @@ def api_sis(lib, dims, data, mask, covs, rads, ks, marginals, seed, sim_mask=Non
             mv = np.ascontiguousarray(mv, np.float32)
             keep.append(mv)
             fa[i] = FloatArr(mv.ctypes.data_as(C.POINTER(C.c_float)), _shape(dims))
-        lib.hpgl_sis_simulation_lvm(C.byref(a), arr, fa, m, seed, sm, 0)
+        lib.hpgl_sis_simulation_lvm(C.byref(a), arr, fa, m, seed, sm, int(bool(corr)))
     return od, om
 
 
@@ -363,7 +363,7 @@ def sis_cases(lib):
     for name, opts in SIS_CASES:
         x = sis_inputs(dict(np.load(os.path.join(HERE, "indicator_s015.npz"))), opts)
         od, om = api_sis(lib, x["dims"], x["data"], x["mask"], x["covs"], x["rads"], x["ks"], x["marginals"],
-                         x["seed"], sim_mask=x["sim_mask"], means=x["means"])
+                         x["seed"], sim_mask=x["sim_mask"], means=x["means"], corr=x["corr"])
         out[f"{name}_data"] = od
         out[f"{name}_mask"] = om
     np.savez_compressed(os.path.join(HERE, "sis.npz"), **out)

@@ -110,11 +110,13 @@ def cok_inputs(g, mark, secondary=None):
 
 
 SIS_CASES = [
-    # name, options: seed, categories (5 = the fixture's, 2 = median SIS on category >= 2), mask, LVM
+    # name, options: seed, categories (5 = the fixture's, 2 = median SIS on category >= 2), mask, LVM,
+    # correlogram weights (LVM)
     ("sis5", {"seed": 17}),
     ("sis5_mask", {"seed": 5, "sim_mask": 0.6}),
     ("sis2_median", {"seed": 9, "two": True}),
     ("sis5_lvm", {"seed": 23, "lvm": True}),
+    ("sis5_lvm_corr", {"seed": 31, "lvm": True, "corr": True}),
 ]
 
 
@@ -137,7 +139,7 @@ def sis_inputs(g, opts):
         marg = [0.6, 0.4]
     ks = [12] * len(covs)
     x = {"dims": dims, "data": data, "mask": mask.copy(), "covs": covs, "rads": rads, "ks": ks, "marginals": marg,
-         "seed": opts["seed"], "sim_mask": None, "means": None}
+         "seed": opts["seed"], "sim_mask": None, "means": None, "corr": bool(opts.get("corr"))}
     if "sim_mask" in opts:
         x["sim_mask"] = (np.random.default_rng(6).random(n) < opts["sim_mask"]).astype(np.uint8)
     if opts.get("lvm"):

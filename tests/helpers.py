@@ -169,3 +169,26 @@ def rel_err(a, ref):
     if a.size == 0:
         return 0.0
     return float(np.max(np.abs(a - ref)) / max(np.max(np.abs(ref)), 1e-300))
+
+
+def engine_sis(dims, data, mask, covs, radiuses, ks, marginals, seed, sim_mask=None, means=None, corr=False):
+    """SIS through hpgl_b200_sis_ex with host buffers; returns data, mask, status, stats."""
+    n = int(np.prod(dims))
+    d = np.ascontiguousarray(data, np.uint8).copy()
+    m = np.ascontiguousarray(mask, np.uint8).copy()
+    st = np.zeros(n, np.int8)
+    sm = np.ascontiguousarray(sim_mask, np.uint8) if sim_mask is not None else None
+    keep = []
+    mp = None
+    if means is not None:
+        keep = [np.ascontiguousarray(v, np.float32) for v in means]
+        mp = (C.c_void_p * len(keep))(*[v.ctypes.data for v in keep])
+    opt = W._HPGL_B200_OPTIONS(precision=0, refine_steps=0, flags=0, stream=None, estimate64=None, variance=None,
+                               status=st.ctypes.data, ik_probs=None)
+    arr = ik_params(covs, radiuses, ks, marginals)
+    rc = W._hpgl_so.hpgl_b200_sis_ex((C.c_int * 3)(*dims), d.ctypes.data, m.ctypes.data,
+                                     sm.ctypes.data if sm is not None else None, arr, len(covs),
+                                     C.cast(mp, C.c_void_p) if mp is not None else None, int(seed), int(bool(corr)),
+                                     C.byref(opt))
+    W.check(rc, "sis_ex")
+    return {"data": d, "mask": m, "status": st, "stats": W.last_stats()}

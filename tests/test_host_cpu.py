@@ -234,3 +234,52 @@ def test_cokriging_entry_argument_checks():
     assert fn(2, dims, None, None, None, None, C.byref(m1), None, None, None, None) == W.EINVAL
     assert fn(1, dims, None, None, None, None, C.byref(m1), None, None, None, None) == W.EINVAL  # null arrays
 
+
+
+def _sis_params(m, k=8):
+    arr = (W._HPGL_IK_PARAMS * m)()
+    for i in range(m):
+        arr[i] = W._HPGL_IK_PARAMS(covariance_type=0, ranges=(4.0, 4.0, 4.0), angles=(0.0, 0.0, 0.0), sill=1.0,
+                                   nugget=0.1, radiuses=(3, 3, 3), max_neighbours=k, marginal_prob=1.0 / m)
+    return arr
+
+
+def test_sis_entry_argument_checks():
+    """SIS limits are checked before any device work: null arrays and fewer than
+    two categories are EINVAL, more than 16 categories, more than 32 neighbours
+    and more than 10,000,000 cells ELIMIT, a walk that misses nodes EINVAL."""
+    fn = W._hpgl_so.hpgl_b200_sis_ex
+    dims = (C.c_int * 3)(6, 5, 4)
+    d = np.zeros(120, np.uint8)
+    m = np.zeros(120, np.uint8)
+    assert fn(dims, None, None, None, _sis_params(3), 3, None, 1, 0, None) == W.EINVAL
+    assert fn(dims, d.ctypes.data, m.ctypes.data, None, _sis_params(1), 1, None, 1, 0, None) == W.EINVAL
+    assert fn(dims, d.ctypes.data, m.ctypes.data, None, _sis_params(17), 17, None, 1, 0, None) == W.ELIMIT
+    assert fn(dims, d.ctypes.data, m.ctypes.data, None, _sis_params(3, 33), 3, None, 1, 0, None) == W.ELIMIT
+    big = (C.c_int * 3)(2000, 2000, 3)
+    assert fn(big, d.ctypes.data, m.ctypes.data, None, _sis_params(3), 3, None, 1, 0, None) == W.ELIMIT
+    four = (C.c_int * 3)(2, 2, 1)
+    assert fn(four, d.ctypes.data, m.ctypes.data, None, _sis_params(3), 3, None, 1, 0, None) == W.EINVAL
+    assert "visit" in W.last_error()
+
+
+def test_geo_sis_simulation_validation():
+    """geo_bsd.sis_simulation validates as the reference's sis.py does before calling the library."""
+    import geo_bsd
+    from geo_bsd.validation import CriticalValidationError, ParameterValidator
+    ParameterValidator.validate_probability_sum([0.3, 0.3, 0.405])
+    with pytest.raises(CriticalValidationError):
+        ParameterValidator.validate_probability_sum([0.3, 0.3, 0.3])
+    with pytest.raises(CriticalValidationError):
+        ParameterValidator.validate_probability_sum([0.5, float("nan")])
+    grid = geo_bsd.SugarboxGrid(4, 4, 2)
+    prop = geo_bsd.IndProperty(np.zeros((4, 4, 2), np.uint8, order="F"), np.zeros((4, 4, 2), np.uint8, order="F"), 2)
+    cm = geo_bsd.CovarianceModel(type=0, ranges=(4.0, 4.0, 4.0), sill=1.0)
+    data = [{"cov_model": cm, "radiuses": (3, 3, 3), "max_neighbours": 8} for _ in range(2)]
+    with pytest.raises(CriticalValidationError):
+        geo_bsd.sis_simulation(prop, grid, data, 1, [0.2, 0.2])
+    with pytest.raises(CriticalValidationError):
+        geo_bsd.sis_simulation(prop, grid, data, 1, [1.2, -0.2])
+    cont = geo_bsd.ContProperty(np.zeros((4, 4, 2), np.float32, order="F"), np.zeros((4, 4, 2), np.uint8, order="F"))
+    with pytest.raises(TypeError):
+        geo_bsd.sis_simulation(cont, grid, data, 1, [0.5, 0.5])

@@ -176,6 +176,6 @@ def test_oracle_sis_matches_reference(case):
     x = G.sis_inputs(G.load("indicator_s015"), opts)
     ref = G.load("sis")
     d, m, _ = O.sis(x["dims"], x["data"], x["mask"], x["covs"], x["rads"], x["ks"], x["marginals"], x["seed"],
-                    sim_mask=x["sim_mask"], means=x["means"])
+                    sim_mask=x["sim_mask"], means=x["means"], correlogram=x["corr"])
     np.testing.assert_array_equal(m, ref[f"{case}_mask"])
     np.testing.assert_array_equal(d, ref[f"{case}_data"])
