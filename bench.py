@@ -520,8 +520,8 @@ def bench_sis(args, rank, world, local):
     pk = peak_table()
     solve_ms = float(np.mean([s["stage_solve_ms"] for s in stats]))
     achieved = last["sgs_flops"] / (solve_ms / 1e3) / 1e12
-    roofline = {"bound": "fp64", "kernel": "k_sis_solve_fold (FP64, two nodes per warp, one launch per category "
-                                            "and level) + k_sis_sample",
+    roofline = {"bound": "fp64", "kernel": "k_sis_level (FP64, two systems per warp, every category of a level "
+                                            "in one launch, the node's last system draws)",
                 "achieved": achieved, "peak": pk["fp64"], "unit": "TFLOP/s", "frac": achieved / pk["fp64"],
                 "traffic": None, "peak_source": f"CUDA-core FP64 peak 148 SM x 64 lanes x 2 x {pk['source']}",
                 "algorithmic_flops_per_call": last["sgs_flops"], "solve_stage_ms": solve_ms,

@@ -1446,19 +1446,26 @@ int sis_simulation(const int *dims, unsigned char *data, unsigned char *mask, co
             E.stats.h2d += (long long)n_sim * 8;
         }
         E.mark(STAGE_PREPARE, st);
-        double *probs = E.buf<double>("sis_probs", ns * ncat);
+        double *probs = E.buf<double>("sis_probs", ns * kcat);
+        signed char *st_cat = E.buf<signed char>("sis_st_cat", ns * kcat);
+        int *done = E.buf<int>("sis_done", ns);
         signed char *st_rank = E.buf<signed char>("sgs_st_rank", ns);
+        std::vector<SisCat> hc(kcat);
+        for (int c = 0; c < kcat; ++c)
+        {
+            const Geom &g = plans[c].first.g;
+            hc[c] = SisCat{pair64[c], nb[c], nb_cnt[c], d_means[c], g.pair_center, g.pnx, g.pny, cats[c].max_nb,
+                           (float)cats[c].marginal};
+        }
+        SisCat *d_cats = E.buf<SisCat>("sis_cats", kSisMaxCat);
+        HB_CK(cudaMemcpyAsync(d_cats, hc.data(), kcat * sizeof(SisCat), cudaMemcpyHostToDevice, st));
+        HB_CK(cudaMemsetAsync(done, 0, ns * 4, st));
         for (int l = 0; l < n_levels; ++l)
         {
-            for (int c = 0; c < kcat; ++c)
-            {
-                SisSolveArgs sa{plans[c].first.g, order + offs[l], counts[l], sim_cells, nb[c], nb_cnt[c],
-                                cats[c].max_nb, pair64[c], d_data, c, ncat, (float)cats[c].marginal, d_means[c],
-                                probs, st_rank, correlogram && means ? 1 : 0};
-                HB_CK(launch_sis_solve(sa, E.n_sm(), st));
-            }
-            launch_sis_sample(order + offs[l], counts[l], sim_cells, probs, ncat, d_u, d_data, st);
-            E.stats.launches += kcat + 1;
+            SisLevelArgs la{d_cats, dims[0], dims[1], order + offs[l], counts[l], kcat, ncat, sim_cells, d_data,
+                            probs, st_cat, done, d_u, st_rank, correlogram && means ? 1 : 0};
+            HB_CK(launch_sis_level(la, E.n_sm(), st));
+            E.stats.launches += 1;
         }
         HB_CK(cudaGetLastError());
         E.mark(STAGE_SOLVE, st);

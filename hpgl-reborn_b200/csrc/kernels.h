@@ -147,30 +147,37 @@ void launch_sgs_index(long long n, const int *path_cell, const int *flag, const 
 void launch_sgs_search(const Geom &g, const int4 *tmpl, int n_tmpl, const int *sim_cells, int n_sim,
                        const int *rank_of, int k, int *nb, int *nb_rank, int *nb_cnt, int n_sm, cudaStream_t st,
                        int fixed_rank = -1, int rank_stride = 0);
-// SIS (sgs.cu): one category's indicator SK probabilities of a level, then the draws
+// SIS (sgs.cu): one launch per level solves every (node, kriged category)
+// system and draws each node's category when its last system is done
 constexpr int kSisMaxCat = 16;
-struct SisSolveArgs
+struct SisCat
 {
-    Geom g;
-    const int *order;
-    int n_items;
-    const int *sim_cells;
-    const int *nb; // this category's neighbour cells, k per rank
+    const double *pair64; // the category's pair table
+    const int *nb;        // its neighbour cells, k per rank
     const int *nb_cnt;
+    const float *means;   // LVM: the category's mean per cell, or null
+    long long pair_center;
+    int pnx, pny;
     int k;
-    const double *pair64;
-    const uint8_t *data; // categories of the informed cells
-    int category;
-    int ncat;
-    float marginal;    // the category's mean (float, as the reference stores it)
-    const float *means; // LVM: the category's mean per cell, or null
-    double *probs;      // per rank, ncat entries
-    signed char *st_rank;
-    int correlogram;    // LVM correlogram weights (corellogramed_weights_3)
+    float marginal;       // the category's mean (float, as the reference stores it)
 };
-cudaError_t launch_sis_solve(const SisSolveArgs &a, int n_sm, cudaStream_t st);
-void launch_sis_sample(const int *order, int n_items, const int *sim_cells, const double *probs, int ncat,
-                       const double *uniforms, uint8_t *data, cudaStream_t st);
+struct SisLevelArgs
+{
+    const SisCat *cats;  // kcat entries (device)
+    int nx, ny;
+    const int *order;    // the level's ranks
+    int n_nodes;
+    int kcat, ncat;
+    const int *sim_cells;
+    uint8_t *data;       // categories (the draws are written here)
+    double *probs;       // per rank, kcat entries
+    signed char *st_cat; // per rank, kcat entries
+    int *done;           // per rank: systems finished (zeroed per call)
+    const double *uniforms;
+    signed char *st_rank;
+    int correlogram;     // LVM correlogram weights (corellogramed_weights_3)
+};
+cudaError_t launch_sis_level(const SisLevelArgs &a, int n_sm, cudaStream_t st);
 void launch_sgs_levels(const int *nb_rank, const int *nb_cnt, int k, int n_sim, int *levp1, int *ticket,
                        int *level_count, int level_cap, int *max_level, int *err, int n_sm, cudaStream_t st);
 void launch_sgs_moments(int n_sim, const int *nb_cnt, double *mom, int n_sm, cudaStream_t st); // mom: 3, zeroed

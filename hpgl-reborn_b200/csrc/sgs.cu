@@ -29,6 +29,8 @@
 #include "fold32.cuh"
 #include "kernels.h"
 
+#include <cuda/atomic>
+
 #include <algorithm>
 #include <climits>
 
@@ -694,11 +696,13 @@ __global__ void __launch_bounds__(kSgsBlockThreads) k_sgs_solve_block(const SgsS
 }
 
 // ------------------------------------------------------------------ SIS
-// One category's probability for the nodes of a level (sequential_indicator_
-// simulation.cpp:77-108): the SK estimate of the indicator (category == c)
-// from the category's neighbours, accumulated in double around the float
-// mean (combine for a double result); the mean where kriging fails. The
-// status of a rank is the largest over its categories.
+// One launch per level: every (node, kriged category) system of the level
+// (sequential_indicator_simulation.cpp:77-108): the SK estimate of the
+// indicator (category == c) from the category's neighbours, accumulated in
+// double around the float mean (combine for a double result); the mean where
+// kriging fails. The last system of a node to finish draws its category
+// (sample.cpp:8-21): the first category whose running sum exceeds u times the
+// sum, p1 = 1 - p0 with two categories (median SIS).
 constexpr int kSisFoldThreads = 256;
 constexpr size_t kSisSysBytes = kFold32SysBytes + kFold32NP * 8; // plus the 32 row scales
 
@@ -711,9 +715,39 @@ __device__ __forceinline__ double sis_sigma(float mean)
     return __dsqrt_rn(__dmul_rn(m, __dsub_rn(1.0, m)));
 }
 
+// the draw of rank r once every category's probability is stored (read
+// through L2: other SMs wrote them); two passes, the sum then the running sum
+__device__ __forceinline__ void sis_draw(const double *probs, const signed char *st_cat, int kcat, int ncat,
+                                         double u, uint8_t *data_cell, signed char *st_out)
+{
+    const double p0 = __ldcg(probs);
+    double sum = 0.0;
+    int stv = 0;
+    for (int c = 0; c < kcat; ++c)
+    {
+        sum = __dadd_rn(sum, __ldcg(probs + c));
+        stv = max(stv, (int)__ldcg(reinterpret_cast<const unsigned char *>(st_cat) + c));
+    }
+    if (ncat == 2) sum = __dadd_rn(sum, __dsub_rn(1.0, p0)); // median SIS: p1 = 1 - p0
+    const double s = __dmul_rn(u, sum);
+    double acc = 0.0;
+    int pick = ncat - 1;
+    for (int c = 0; c < ncat; ++c)
+    {
+        acc = __dadd_rn(acc, ncat == 2 && c == 1 ? __dsub_rn(1.0, p0) : __ldcg(probs + c));
+        if (s < acc)
+        {
+            pick = c;
+            break;
+        }
+    }
+    *data_cell = (uint8_t)pick;
+    *st_out = (signed char)stv;
+}
+
 // CORR: correlogram weights (LVM): A_ij = C_ij (s_i s_j), b_i = C_ic (s_i s_c)
 template <bool CORR>
-__global__ void __launch_bounds__(kSisFoldThreads, 1) k_sis_solve_fold(const SisSolveArgs a)
+__global__ void __launch_bounds__(kSisFoldThreads, 1) k_sis_level(const SisLevelArgs a)
 {
     constexpr int NP = kFold32NP, G = kFold32G;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -724,36 +758,45 @@ __global__ void __launch_bounds__(kSisFoldThreads, 1) k_sis_solve_fold(const Sis
     double *M = reinterpret_cast<double *>(gb);
     int *LIN = reinterpret_cast<int *>(gb + (size_t)NP * kFold32LD * 8);
     double *SIG = reinterpret_cast<double *>(gb + kFold32SysBytes); // the system's row scales
-    const Geom &g = a.g;
-    const long long pc = g.pair_center;
+    const int n_sys = a.n_nodes * a.kcat;
     const int stride = gridDim.x * nwarps * 2;
-    for (int it0 = (blockIdx.x * nwarps + warp) * 2; it0 < a.n_items; it0 += stride)
+    for (int it0 = (blockIdx.x * nwarps + warp) * 2; it0 < n_sys; it0 += stride)
     {
         const int it = it0 + h;
-        const bool valid = it < a.n_items;
-        const int r = valid ? a.order[it] : 0;
+        const bool valid = it < n_sys;
+        // category-major: the SMs of a moment share one category's pair table
+        const int cat = valid ? it / a.n_nodes : 0;
+        const int node = valid ? it - cat * a.n_nodes : 0;
+        const SisCat &C = a.cats[cat];
+        const int r = valid ? a.order[node] : 0;
         const int cell = valid ? a.sim_cells[r] : 0;
-        const int n = valid ? a.nb_cnt[r] : 0;
-        const int cx = cell % g.nx, cy = (int)((cell / g.nx) % g.ny), cz = (int)(cell / ((long long)g.nx * g.ny));
+        const int n = valid ? __ldg(C.nb_cnt + r) : 0;
+        const int k = C.k;
+        const int pnx = C.pnx, pny = C.pny;
+        const double *pair_c = C.pair64 + C.pair_center;
+        const float *means = C.means;
+        const int cx = cell % a.nx, cy = (int)((cell / a.nx) % a.ny), cz = (int)(cell / ((long long)a.nx * a.ny));
         const bool live_a = t < n, live_b = rb < n;
         int lin_a = 0, lin_b = 0;
         float da = 0.0f, db = 0.0f; // indicator - mean, in float
         double sa = 1.0, sb = 1.0;
-        const float mc = a.means ? (valid ? a.means[cell] : 0.0f) : a.marginal;
+        const float mc = means ? (valid ? means[cell] : 0.0f) : C.marginal;
         if (live_a)
         {
-            const int q = a.nb[(long long)r * a.k + t];
-            lin_a = pair_lin(g, q % g.nx - cx, (int)((q / g.nx) % g.ny) - cy, (int)(q / ((long long)g.nx * g.ny)) - cz);
-            const float mq = a.means ? a.means[q] : mc;
-            da = __fsub_rn(a.data[q] == a.category ? 1.0f : 0.0f, mq);
+            const int q = __ldg(C.nb + (long long)r * k + t);
+            const int qz = (int)(q / ((long long)a.nx * a.ny)), qy = (int)((q / a.nx) % a.ny), qx = q % a.nx;
+            lin_a = ((qz - cz) * pny + (qy - cy)) * pnx + (qx - cx);
+            const float mq = means ? means[q] : mc;
+            da = __fsub_rn(a.data[q] == cat ? 1.0f : 0.0f, mq);
             if (CORR) sa = sis_sigma(mq);
         }
         if (live_b)
         {
-            const int q = a.nb[(long long)r * a.k + rb];
-            lin_b = pair_lin(g, q % g.nx - cx, (int)((q / g.nx) % g.ny) - cy, (int)(q / ((long long)g.nx * g.ny)) - cz);
-            const float mq = a.means ? a.means[q] : mc;
-            db = __fsub_rn(a.data[q] == a.category ? 1.0f : 0.0f, mq);
+            const int q = __ldg(C.nb + (long long)r * k + rb);
+            const int qz = (int)(q / ((long long)a.nx * a.ny)), qy = (int)((q / a.nx) % a.ny), qx = q % a.nx;
+            lin_b = ((qz - cz) * pny + (qy - cy)) * pnx + (qx - cx);
+            const float mq = means ? means[q] : mc;
+            db = __fsub_rn(a.data[q] == cat ? 1.0f : 0.0f, mq);
             if (CORR) sb = sis_sigma(mq);
         }
         LIN[t] = lin_a;
@@ -765,16 +808,16 @@ __global__ void __launch_bounds__(kSisFoldThreads, 1) k_sis_solve_fold(const Sis
         }
         __syncwarp(gm);
         const double sc = CORR ? sis_sigma(mc) : 1.0;
-        double rhs_a[1] = {live_a ? __ldg(a.pair64 + pc + lin_a) : 0.0};
-        double rhs_b[1] = {live_b ? __ldg(a.pair64 + pc + lin_b) : 0.0};
+        double rhs_a[1] = {live_a ? __ldg(pair_c + lin_a) : 0.0};
+        double rhs_b[1] = {live_b ? __ldg(pair_c + lin_b) : 0.0};
         if (CORR)
         {
             rhs_a[0] = __dmul_rn(rhs_a[0], __dmul_rn(sa, sc));
             rhs_b[0] = __dmul_rn(rhs_b[0], __dmul_rn(sb, sc));
         }
         double xa[1], xb[1];
-        const bool fail = fold32_solve<1, false, CORR>(a.pair64 + pc, LIN, M, gm, t, live_a, live_b, lin_a, lin_b,
-                                                       rhs_a, rhs_b, xa, xb, [] {}, [] {}, SIG, sa, sb);
+        const bool fail = fold32_solve<1, false, CORR>(pair_c, LIN, M, gm, t, live_a, live_b, lin_a, lin_b, rhs_a,
+                                                       rhs_b, xa, xb, [] {}, [] {}, SIG, sa, sb);
         const double ta = __dmul_rn(xa[0], (double)da), tb = __dmul_rn(xb[0], (double)db);
         double prob = (double)mc;
 #pragma unroll 4
@@ -787,41 +830,17 @@ __global__ void __launch_bounds__(kSisFoldThreads, 1) k_sis_solve_fold(const Sis
         if (valid && t == 0)
         {
             const int status = n == 0 ? 1 : (fail ? 2 : 0);
-            a.probs[(long long)r * a.ncat + a.category] = status == 0 ? prob : (double)mc;
-            if (a.category == 0 || status > a.st_rank[r]) a.st_rank[r] = (signed char)status;
-        }
-        __syncwarp(gm);
-    }
-}
-
-// sample (sample.cpp:8-21): the first category whose running sum exceeds
-// u times the sum; with two categories p1 = 1 - p0 (median SIS)
-__global__ void k_sis_sample(const int *__restrict__ order, int n_items, const int *__restrict__ sim_cells,
-                             const double *__restrict__ probs, int ncat, const double *__restrict__ uniforms,
-                             uint8_t *__restrict__ data)
-{
-    for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < n_items; it += gridDim.x * blockDim.x)
-    {
-        const int r = order[it];
-        const double *p = probs + (long long)r * ncat;
-        double pr[kSisMaxCat];
-        for (int c = 0; c < ncat; ++c) pr[c] = p[c];
-        if (ncat == 2) pr[1] = __dsub_rn(1.0, pr[0]);
-        double sum = 0.0;
-        for (int c = 0; c < ncat; ++c) sum = __dadd_rn(sum, pr[c]);
-        const double s = __dmul_rn(uniforms[r], sum);
-        double acc = 0.0;
-        int pick = ncat - 1;
-        for (int c = 0; c < ncat; ++c)
-        {
-            acc = __dadd_rn(acc, pr[c]);
-            if (s < acc)
+            a.probs[(long long)r * a.kcat + cat] = status == 0 ? prob : (double)mc;
+            a.st_cat[(long long)r * a.kcat + cat] = (signed char)status;
+            // release this system's probability; the last system of the node acquires the others'
+            cuda::atomic_ref<int, cuda::thread_scope_device> done(a.done[r]);
+            if (done.fetch_add(1, cuda::memory_order_acq_rel) == a.kcat - 1)
             {
-                pick = c;
-                break;
+                sis_draw(a.probs + (long long)r * a.kcat, a.st_cat + (long long)r * a.kcat, a.kcat, a.ncat,
+                         a.uniforms[r], a.data + cell, a.st_rank + r);
             }
         }
-        data[sim_cells[r]] = (uint8_t)pick;
+        __syncwarp(gm);
     }
 }
 
@@ -871,24 +890,18 @@ void launch_sgs_level_fill(int n_sim, const int *levp1, const int *level_off, in
 {
     k_sgs_level_fill<<<1184, 256, 0, st>>>(n_sim, levp1, level_off, level_fill, order);
 }
-cudaError_t launch_sis_solve(const SisSolveArgs &a, int n_sm, cudaStream_t st)
+cudaError_t launch_sis_level(const SisLevelArgs &a, int n_sm, cudaStream_t st)
 {
-    if (a.n_items <= 0) return cudaSuccess;
+    const int n_sys = a.n_nodes * a.kcat;
+    if (n_sys <= 0) return cudaSuccess;
     const int spb = kSisFoldThreads / kFold32G;
     const size_t smem = kSisSysBytes * spb;
-    auto kern = a.correlogram ? k_sis_solve_fold<true> : k_sis_solve_fold<false>;
+    auto kern = a.correlogram ? k_sis_level<true> : k_sis_level<false>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    const int blocks = std::min((a.n_items + spb - 1) / spb, n_sm);
+    const int blocks = std::min((n_sys + spb - 1) / spb, n_sm);
     kern<<<blocks, kSisFoldThreads, smem, st>>>(a);
     return cudaGetLastError();
-}
-void launch_sis_sample(const int *order, int n_items, const int *sim_cells, const double *probs, int ncat,
-                       const double *uniforms, uint8_t *data, cudaStream_t st)
-{
-    if (n_items <= 0) return;
-    k_sis_sample<<<std::min((n_items + 255) / 256, 1184), 256, 0, st>>>(order, n_items, sim_cells, probs, ncat,
-                                                                       uniforms, data);
 }
 size_t sgs_block_smem(int k) { return (size_t)k * k * 8 + 3 * (size_t)k * 8 + 2 * (size_t)k * 4; }
 
