@@ -90,6 +90,8 @@ __device__ __forceinline__ void cok_write(const CokArgsDev &a, int cell, int sta
 // n <= 32: two targets per warp in the folded layout
 constexpr int kCokThreads = 256;
 
+// BOUND (k < 32): the factorisation stops at the warp's largest system
+template <bool BOUND>
 __global__ void __launch_bounds__(kCokThreads, 1) k_cok_solve_fold(const CokArgsDev a)
 {
     constexpr int NP = kFold32NP, G = kFold32G;
@@ -131,11 +133,18 @@ __global__ void __launch_bounds__(kCokThreads, 1) k_cok_solve_fold(const CokArgs
         LIN[t] = lin_a;
         LIN[rb] = lin_b;
         __syncwarp(gm);
-        const double b_a = live_a ? __ldg(a.pair64 + pc + lin_a) : 0.0;
-        const double b_b = live_b ? __ldg(a.pair64 + pc + lin_b) : 0.0;
-        double rhs_a[2] = {b_a, c_a}, rhs_b[2] = {b_b, c_b}, xa[2], xb[2];
-        const bool fail = fold32_solve<2, true>(a.pair64 + pc, LIN, M, gm, t, live_a, live_b, lin_a, lin_b, rhs_a, rhs_b,
-                                          xa, xb, [] {}, [] {});
+        double b_a = 0.0, b_b = 0.0, xa[2], xb[2];
+        auto load_rhs = [&](double(&rhs_a)[2], double(&rhs_b)[2]) {
+            b_a = live_a ? __ldg(a.pair64 + pc + lin_a) : 0.0;
+            b_b = live_b ? __ldg(a.pair64 + pc + lin_b) : 0.0;
+            rhs_a[0] = b_a;
+            rhs_a[1] = c_a;
+            rhs_b[0] = b_b;
+            rhs_b[1] = c_b;
+        };
+        const int nmax = BOUND ? __reduce_max_sync(0xffffffffu, n) : NP; // both targets of the warp
+        const bool fail = fold32_solve<2, true>(a.pair64 + pc, LIN, M, gm, t, live_a, live_b, lin_a, lin_b, load_rhs,
+                                                xa, xb, [] {}, [] {}, nullptr, 1.0, 1.0, nmax);
         // the border: wn = (b_n - c.x) / (s - c.y)
         double cx_ = c_a * xa[0] + c_b * xb[0], cy_ = c_a * xa[1] + c_b * xb[1];
 #pragma unroll
@@ -290,10 +299,11 @@ cudaError_t launch_cok_solve(const Geom &g, const int *targets, int n_targets, c
     {
         const int spb = kCokThreads / kFold32G;
         const size_t smem = kFold32SysBytes * spb;
-        cudaError_t e = cudaFuncSetAttribute(k_cok_solve_fold, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        auto kern = k < 32 ? k_cok_solve_fold<true> : k_cok_solve_fold<false>;
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         const int blocks = std::min((n_targets + spb - 1) / spb, n_sm);
-        k_cok_solve_fold<<<blocks, kCokThreads, smem, st>>>(a);
+        kern<<<blocks, kCokThreads, smem, st>>>(a);
     }
     else
     {

@@ -1457,13 +1457,15 @@ int sis_simulation(const int *dims, unsigned char *data, unsigned char *mask, co
             hc[c] = SisCat{pair64[c], nb[c], nb_cnt[c], d_means[c], g.pair_center, g.pnx, g.pny, cats[c].max_nb,
                            (float)cats[c].marginal};
         }
+        int kmax = 0;
+        for (int c = 0; c < kcat; ++c) kmax = std::max(kmax, cats[c].max_nb);
         SisCat *d_cats = E.buf<SisCat>("sis_cats", kSisMaxCat);
         HB_CK(cudaMemcpyAsync(d_cats, hc.data(), kcat * sizeof(SisCat), cudaMemcpyHostToDevice, st));
         HB_CK(cudaMemsetAsync(done, 0, ns * 4, st));
         for (int l = 0; l < n_levels; ++l)
         {
             SisLevelArgs la{d_cats, dims[0], dims[1], order + offs[l], counts[l], kcat, ncat, sim_cells, d_data,
-                            probs, st_cat, done, d_u, st_rank, correlogram && means ? 1 : 0};
+                            probs, st_cat, done, d_u, st_rank, correlogram && means ? 1 : 0, kmax};
             HB_CK(launch_sis_level(la, E.n_sm(), st));
             E.stats.launches += 1;
         }

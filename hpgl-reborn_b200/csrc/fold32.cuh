@@ -24,19 +24,24 @@ constexpr size_t kFold32SysBytes = ((size_t)kFold32NP * kFold32LD * 8 + kFold32N
 // Solves A [x] = [rhs] for the lane's rows t and 31 - t (QB <= 2 right-hand
 // sides; rows of non-live unknowns carry zeros). `gm` is the system's lane
 // mask; LIN must hold the 32 offsets (0 for non-live rows) and be visible to
-// the system's lanes. after_assembly() and after_factor() run at those points
-// (the callers issue prefetches there). Returns true when a pivot is not
+// the system's lanes. load_rhs(rhs_a, rhs_b) fills the lane's right-hand sides
+// once the matrix loads are issued (their loads then queue behind those);
+// after_assembly() and after_factor() run at those points (the callers issue
+// prefetches there). Returns true when a pivot is not
 // positive (or NaN), or, with EPS_PIVOT, below machine epsilon (the test of
 // the reference's Gaussian elimination, gauss_solver.cpp:37-41). With SCALE,
 // A[r][c] = pair * (sig_r * sig_c), SIG holding the 32 row scales (visible to
-// the system's lanes) and sig_a / sig_b the lane's own.
-template <int QB, bool EPS_PIVOT = false, bool SCALE = false, typename F1, typename F2>
+// the system's lanes) and sig_a / sig_b the lane's own. nmax, the same on every
+// lane of the warp, bounds the live unknowns of both its systems: the steps of
+// the padding rows beyond it change no live row and are skipped (a uniform
+// bound keeps the warp's two systems in step; rows of M beyond it are never
+// written nor read).
+template <int QB, bool EPS_PIVOT = false, bool SCALE = false, typename F0, typename F1, typename F2>
 __device__ __forceinline__ bool fold32_solve(const double *pair_c, const int *LIN, double *M, unsigned gm, int t,
-                                             bool live_a, bool live_b, int lin_a, int lin_b,
-                                             const double (&rhs_a_in)[QB], const double (&rhs_b_in)[QB],
+                                             bool live_a, bool live_b, int lin_a, int lin_b, F0 load_rhs,
                                              double (&xa)[QB], double (&xb)[QB], F1 after_assembly,
                                              F2 after_factor, const double *SIG = nullptr, double sig_a = 1.0,
-                                             double sig_b = 1.0)
+                                             double sig_b = 1.0, int nmax = kFold32NP)
 {
     constexpr int NP = kFold32NP, G = kFold32G, LD = kFold32LD;
     const int rb = NP - 1 - t;
@@ -67,16 +72,11 @@ __device__ __forceinline__ bool fold32_solve(const double *pair_c, const int *LI
         if (!live_b && c == rb) e = 1.0;
         rbv[c] = e;
     }
+    double rhs_a[QB], rhs_b[QB], ya[QB], yb[QB];
+    load_rhs(rhs_a, rhs_b);
     after_assembly();
 
     // ---- factorisation with the forward substitution of the right-hand sides
-    double rhs_a[QB], rhs_b[QB], ya[QB], yb[QB];
-#pragma unroll
-    for (int q = 0; q < QB; ++q)
-    {
-        rhs_a[q] = rhs_a_in[q];
-        rhs_b[q] = rhs_b_in[q];
-    }
 #pragma unroll
     for (int q = 0; q < QB; ++q)
     {
@@ -88,6 +88,7 @@ __device__ __forceinline__ bool fold32_solve(const double *pair_c, const int *LI
 #pragma unroll
     for (int j = 0; j < NP; ++j)
     {
+        if (j >= nmax) break;
         if (j < G)
         {
             M[j * LD + t] = ra[j];
@@ -166,6 +167,7 @@ __device__ __forceinline__ bool fold32_solve(const double *pair_c, const int *LI
 #pragma unroll
     for (int i = NP - 1; i >= 0; --i)
     {
+        if (i >= nmax) continue;
         double xi[QB];
         if (i >= G)
         {

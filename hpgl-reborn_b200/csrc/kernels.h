@@ -176,6 +176,7 @@ struct SisLevelArgs
     const double *uniforms;
     signed char *st_rank;
     int correlogram;     // LVM correlogram weights (corellogramed_weights_3)
+    int kmax;            // the largest k of the categories
 };
 cudaError_t launch_sis_level(const SisLevelArgs &a, int n_sm, cudaStream_t st);
 void launch_sgs_levels(const int *nb_rank, const int *nb_cnt, int k, int n_sim, int *levp1, int *ticket,
