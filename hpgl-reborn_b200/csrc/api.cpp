@@ -734,6 +734,11 @@ int hpgl_b200_sgs_draws(long long seed, long long n, double *out)
     return HPGL_B200_OK;
 }
 
+int hpgl_b200_sim_levels(long long n_sim, int k, const int *nb_rank, int *levels)
+{
+    return hb::sim_levels(n_sim, k, nb_rank, levels);
+}
+
 int hpgl_b200_sgs_ex(const int *dims, float *data, unsigned char *mask, const unsigned char *sim_mask,
                      const hpgl_non_parametric_cdf_t *cdf, const float *means, const hpgl_sgs_params_t *params,
                      const hpgl_b200_options_t *opt)

@@ -1246,6 +1246,57 @@ int sgs_simulation(const int *dims, float *data, unsigned char *mask, const unsi
     }
 }
 
+// ------------------------------------------------------------------ levels
+int sim_levels(long long n_sim, int k, const int *nb_rank, int *levels)
+{
+    std::lock_guard<std::mutex> lk(g_engine_mu);
+    try
+    {
+        if (n_sim < 0 || n_sim > 10000000 || k <= 0 || k > 4096 || (n_sim > 0 && (!nb_rank || !levels)))
+            throw CudaFail{-1, "bad argument"};
+        // every listed rank is read by the pass: it must name a rank or be -1
+        for (long long i = 0; i < n_sim * k; ++i)
+            if (nb_rank[i] < -1 || nb_rank[i] >= n_sim) throw CudaFail{-1, "neighbour rank out of range"};
+        if (n_sim == 0) return 0;
+        Engine &E = engine_for_current_device();
+        cudaStream_t st = E.stream(nullptr);
+        begin_call(E, st);
+        const size_t ns = (size_t)n_sim;
+        int *d_rank = E.buf<int>("lv_nb_rank", ns * k);
+        HB_CK(cudaMemcpyAsync(d_rank, nb_rank, ns * k * 4, cudaMemcpyHostToDevice, st));
+        const int level_cap = 1 << 20;
+        int *levp1 = E.buf<int>("sgs_levp1", ns);
+        int *lvl_count = E.buf<int>("sgs_lvl_count", (size_t)level_cap + 1);
+        int *scal = E.buf<int>("sgs_scal", 4);
+        HB_CK(cudaMemsetAsync(levp1, 0, ns * 4, st));
+        HB_CK(cudaMemsetAsync(lvl_count, 0, ((size_t)level_cap + 1) * 4, st));
+        HB_CK(cudaMemsetAsync(scal, 0, 16, st));
+        launch_sgs_levels(d_rank, nullptr, k, (int)n_sim, levp1, scal + 0, lvl_count, level_cap, scal + 1, scal + 2,
+                          E.n_sm(), st);
+        HB_CK(cudaGetLastError());
+        E.stats.launches += 2;
+        int hs[4] = {0, 0, 0, 0};
+        HB_CK(cudaMemcpyAsync(hs, scal, 16, cudaMemcpyDeviceToHost, st));
+        HB_CK(cudaMemcpyAsync(levels, levp1, ns * 4, cudaMemcpyDeviceToHost, st));
+        end_call(E, st);
+        if (hs[2] == 1) throw CudaFail{-2, "simulation level pass: a dependency wait timed out"};
+        if (hs[2] == 2) throw CudaFail{-4, "simulation needs more than 2^20 dependency levels"};
+        for (size_t i = 0; i < ns; ++i) levels[i] -= 1;
+        E.stats.sgs_levels = hs[1] + 1;
+        return 0;
+    }
+    catch (const CudaFail &f)
+    {
+        set_error(f.msg);
+        return f.code;
+    }
+    catch (const std::exception &ex)
+    {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
 // ------------------------------------------------------------------ SIS
 int sis_simulation(const int *dims, unsigned char *data, unsigned char *mask, const unsigned char *sim_mask,
                    const std::vector<IkArgs> &cats, const float *const *means, long long seed, const Options &opt,

@@ -134,6 +134,10 @@ int sgs_simulation(const int *dims, float *data, unsigned char *mask, const unsi
 int cokriging(const int *dims, const float *pdata, const unsigned char *pmask, const float *sdata,
               const unsigned char *smask, const CokArgs &a, float *out_data, unsigned char *out_mask,
               const Options &opt);
+// The simulations' dependency levels: level(r) = 1 + the largest level of the
+// ranks listed for r (k per rank, -1 for none; each below r in a simulation),
+// 0 with none listed.
+int sim_levels(long long n_sim, int k, const int *nb_rank, int *levels);
 // Sequential indicator simulation in place on data (categories) / mask
 // (sequential_indicator_simulation.cpp:24-185): cats per category; means (LVM)
 // one float array per category or null, with `correlogram` the correlogram

@@ -290,20 +290,22 @@ constexpr unsigned long long kLevelWaitNs = 2000000000ull; // a wait that lasts 
 // ranks: those of earlier tickets, whose warps are running, and those of lower
 // lanes of its own batch, which independent thread scheduling keeps running
 // while it waits. So every wait ends; each still gives up after kLevelWaitNs
-// (err = 1), and once err is set every wait ends at once.
+// (err = 1), and once err is set every wait ends at once. The spin reads the
+// timer and the error flag every 64 polls and does not sleep (sleeping between
+// polls doubled the pass).
 __device__ __forceinline__ int sgs_wait_level(const int *levp1, int tq, int *err)
 {
     int v = ld_relaxed_gpu(&levp1[tq]);
     if (v != 0) return v;
     const unsigned long long t0 = global_ns();
+    unsigned polls = 0;
     while ((v = ld_relaxed_gpu(&levp1[tq])) == 0)
     {
-        if (ld_relaxed_gpu(err) != 0 || global_ns() - t0 > kLevelWaitNs)
+        if ((++polls & 63u) == 0 && (ld_relaxed_gpu(err) != 0 || global_ns() - t0 > kLevelWaitNs))
         {
             atomicExch(err, 1);
             return 1;
         }
-        __nanosleep(32);
     }
     return v;
 }

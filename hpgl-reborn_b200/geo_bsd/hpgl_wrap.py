@@ -131,6 +131,7 @@ EXPORTS = [
     "hpgl_simple_kriging_weights", "hpgl_indicator_kriging", "hpgl_median_ik", "hpgl_lvm_kriging",
     "hpgl_sgs_simulation", "hpgl_sgs_lvm_simulation", "hpgl_simple_cokriging_mark1", "hpgl_simple_cokriging_mark2",
     "hpgl_b200_cokriging_ex", "hpgl_sis_simulation", "hpgl_sis_simulation_lvm", "hpgl_b200_sis_ex",
+    "hpgl_b200_sim_levels",
     "hpgl_read_inc_file_float", "hpgl_read_inc_file_byte", "hpgl_write_inc_file_float",
     "hpgl_write_inc_file_byte", "hpgl_write_gslib_cont_property", "hpgl_write_gslib_byte_property",
     "hpgl_b200_cont_kriging_ex", "hpgl_b200_lvm_kriging_ex", "hpgl_b200_sgs_ex", "hpgl_b200_sgs_draws", "hpgl_b200_indicator_kriging_ex", "hpgl_b200_median_ik_ex",
@@ -228,6 +229,8 @@ def _load():
     lib.hpgl_b200_sis_ex.restype = C.c_int
     lib.hpgl_b200_sis_ex.argtypes = [i_p, vp, vp, vp, C.POINTER(_HPGL_IK_PARAMS), C.c_int, vp, C.c_int, C.c_int,
                                      C.POINTER(_HPGL_B200_OPTIONS)]
+    lib.hpgl_b200_sim_levels.restype = C.c_int
+    lib.hpgl_b200_sim_levels.argtypes = [C.c_longlong, C.c_int, vp, vp]
     lib.hpgl_b200_sgs_draws.restype = C.c_int
     lib.hpgl_b200_sgs_draws.argtypes = [C.c_longlong, C.c_longlong, vp]
     lib.hpgl_b200_indicator_kriging_ex.restype = C.c_int

@@ -262,6 +262,13 @@ int hpgl_b200_sis_ex(const int *dims, unsigned char *data, unsigned char *mask, 
  * `seed` (bs_random_generator.cpp:9-25), as sgs_simulation consumes them, one
  * per simulated node in walk order. */
 int hpgl_b200_sgs_draws(long long seed, long long n, double *out);
+/* The dependency levels the simulations schedule by (no counterpart in HPGL):
+ * for ranks r = 0 .. n_sim-1 with k listed ranks each (nb_rank, host, -1 for
+ * none, every other entry in [0, n_sim)), levels[r] = 1 + the largest level of
+ * its listed ranks, 0 with none. In a simulation each listed rank is below r;
+ * a rank that lists itself or a later rank in a cycle waits, and after 2 s the
+ * call returns HPGL_B200_ECUDA ("timed out") with the device still usable. */
+int hpgl_b200_sim_levels(long long n_sim, int k, const int *nb_rank, int *levels);
 /* Full IK (indicator_count > 2 categories, per-category models) or, with one
  * params entry and indicator_count == 2, median IK (median_ik.cpp:24-89). */
 int hpgl_b200_indicator_kriging_ex(const int *dims, const unsigned char *in_data, const unsigned char *in_mask,

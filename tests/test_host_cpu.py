@@ -283,3 +283,17 @@ def test_geo_sis_simulation_validation():
     cont = geo_bsd.ContProperty(np.zeros((4, 4, 2), np.float32, order="F"), np.zeros((4, 4, 2), np.uint8, order="F"))
     with pytest.raises(TypeError):
         geo_bsd.sis_simulation(cont, grid, data, 1, [0.5, 0.5])
+
+
+def test_sim_levels_argument_checks():
+    """Ranks outside [-1, n_sim) and bad sizes are EINVAL before any device work; no ranks is OK."""
+    fn = W._hpgl_so.hpgl_b200_sim_levels
+    out = np.zeros(4, np.int32)
+    bad = np.array([[-1], [0], [4], [1]], np.int32)
+    assert fn(4, 1, bad.ctypes.data, out.ctypes.data) == W.EINVAL
+    assert "range" in W.last_error()
+    low = np.array([[-1], [-2], [0], [1]], np.int32)
+    assert fn(4, 1, low.ctypes.data, out.ctypes.data) == W.EINVAL
+    assert fn(4, 0, low.ctypes.data, out.ctypes.data) == W.EINVAL
+    assert fn(4, 1, None, out.ctypes.data) == W.EINVAL
+    assert fn(0, 1, None, None) == W.OK
