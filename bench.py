@@ -753,6 +753,7 @@ def bench_cok(args, rank, world, local):
                        "l2": "flushed between timed steps (256 MB write)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "stages_ms": {k[len("stage_"):-len("_ms")]: round(v, 3) for k, v in last.items() if k.startswith("stage_")},
+            "search": {"prefilter": bool(last["prefilter_active"]), "exact_cells": int(last["prefilter_exact_cells"])},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(st["h2d_bytes"]),
                     "d2h_bytes_per_step": int(st["d2h_bytes"]), "timing": "wall clock per call"},

@@ -1616,17 +1616,11 @@ int cokriging(const int *dims, const float *pdata, const unsigned char *pmask, c
         E.mark(STAGE_COMPACT, st);
 
         auto plan_pair = plan_f.get();
-        const Plan &pl = plan_pair.first;
+        Plan &pl = plan_pair.first;
         const std::vector<Offset> &tv = plan_pair.second;
         E.stats.plan_ms = plan_ms;
         const Geom &g = pl.g;
-        const size_t nk = pl.kt.vals.size();
-        double *search_vals = E.buf<double>("search_vals", nk);
-        HB_CK(cudaMemcpyAsync(search_vals, pl.kt.vals.data(), nk * 8, cudaMemcpyHostToDevice, st));
-        const long long pn = (long long)g.pnx * g.pny * (2 * g.phz + 1);
-        double *pair64 = E.buf<double>("pair64", (size_t)pn);
-        float *pair32 = E.buf<float>("pair32", (size_t)pn);
-        launch_build_pair(g, dev_model(pl.f.m), 0, search_vals, pair64, pair32, st);
+        const int k = a.max_nb;
         // the cross model over the +-radius box and the border's constants
         // (cross_cov_model_mark_i_t / _mark_ii_t, simple_cokriging_markI.cpp:145-193)
         Flavour fs = pl.f;
@@ -1660,39 +1654,84 @@ int cokriging(const int *dims, const float *pdata, const unsigned char *pmask, c
                     cross[((size_t)(dz + g.rz) * by + (dy + g.ry)) * bx + (dx + g.rx)] = fs.at_offset(dx, dy, dz);
         double *d_cross = E.buf<double>("cok_cross", cross.size());
         HB_CK(cudaMemcpyAsync(d_cross, cross.data(), cross.size() * 8, cudaMemcpyHostToDevice, st));
-        // the template search over the informed-cell bitmap of the grid padded by
-        // the radiuses, for every bin (the reference's lookup here is the template
-        // scan alone); its linear offsets are 32-bit
-        const long long PX = g.nx + 2LL * g.rx, PY = g.ny + 2LL * g.ry;
-        if ((long long)g.rz * PY * PX + (long long)g.ry * PX + g.rx > 2147483647LL)
-            throw CudaFail{-4, "grid too large for the template search at these radiuses"};
-        std::vector<int4> t4(tv.size());
-        for (size_t i = 0; i < tv.size(); ++i)
-            t4[i] = make_int4(tv[i].dx, tv[i].dy, tv[i].dz, template_padded_offset(g, tv[i].dx, tv[i].dy, tv[i].dz));
-        int4 *tmpl = E.buf<int4>("tmpl", std::max<size_t>(t4.size(), 1));
-        if (!t4.empty())
-            HB_CK(cudaMemcpyAsync(tmpl, t4.data(), t4.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
-        std::vector<int> all_bins(g.n_bins);
-        for (int b = 0; b < g.n_bins; ++b) all_bins[b] = b;
-        int *tmpl_bins = E.buf<int>("tmpl_bins", (size_t)g.n_bins);
-        HB_CK(cudaMemcpyAsync(tmpl_bins, all_bins.data(), (size_t)g.n_bins * 4, cudaMemcpyHostToDevice, st));
         HB_CK(cudaStreamSynchronize(st)); // host temporaries
-        E.stats.launches += 1;
         E.mark(STAGE_TABLES, st);
 
-        const int k = a.max_nb;
         DevPoints P = compact_points(E, grid_geom(dims), d_pm, d_pd, nullptr, st);
         E.stats.launches += 2 + scan_kernels(n);
-        int2 *nb_rec = E.buf<int2>("nb_rec", (size_t)n * k);
-        int *nb_n = E.buf<int>("nb_n", (size_t)n);
-        int *tcount = E.buf<int>("cok_tcount", 1);
-        HB_CK(cudaMemsetAsync(tcount, 0, 4, st));
-        if (n_t > 0)
+        // The reference's lookup here is the template scan alone
+        // (sugarbox_neighbour_lookup.h:39-63): the first k informed cells in
+        // template order. As a selection: every informed cell of the 27 bins
+        // around a cell keyed by its offset's position in the sorted template
+        // (unique keys, so the k smallest are those cells, in that order), through
+        // the kriging path's binned search with every bin selecting. The scan of
+        // the template over the informed-cell bitmap remains for configurations
+        // the selection does not take (k > 64, templates past 65534 offsets,
+        // candidate lists past shared memory).
+        int2 *nb_rec = nullptr;
+        int *nb_n = nullptr;
+        double *pair64 = nullptr;
+        bool selected = false;
+        if (k <= 64 && tv.size() <= 0xFFFE)
         {
-            HB_CK(launch_search_template(g, d_pm, E.buf<uint32_t>("mask_bits", (size_t)(template_padded_cells(g) + 31) / 32),
-                                         0, tmpl_bins, g.n_bins, P.pts_val, tmpl, (int)t4.size(), P.pid_of_node,
-                                         nullptr, nb_rec, nb_n, tcount, E.n_sm(), st));
-            E.stats.launches += 2;
+            std::fill(pl.kt.rank.begin(), pl.kt.rank.end(), KEY_EXCLUDED);
+            for (size_t i = 0; i < tv.size(); ++i) pl.kt.rank[key_index(g, tv[i].dx, tv[i].dy, tv[i].dz)] = (uint32_t)i;
+            pl.kt.n_ranks = (uint32_t)tv.size();
+            pl.rank_bits = pl.kt.n_ranks > 1 ? bits_for(pl.kt.n_ranks - 1) : 0;
+            pl.sg = Surrogate();
+            build_surrogate(pl.f, pl.kt, pl.sg, true);
+            pl.g.limit = INT_MAX; // no bin takes the template path
+            try
+            {
+                DevSearch S = run_search(E, pl, P, d_pm, 0, st);
+                if (S.ties != 0) throw CudaFail{-2, "cokriging search: equal template keys"};
+                nb_rec = S.nb_rec;
+                nb_n = S.nb_n;
+                pair64 = S.pair64;
+                selected = true;
+            }
+            catch (const CudaFail &f)
+            {
+                if (f.code != -4) throw;
+            }
+        }
+        if (!selected)
+        {
+            const size_t nk = pl.kt.vals.size();
+            double *search_vals = E.buf<double>("search_vals", nk);
+            HB_CK(cudaMemcpyAsync(search_vals, pl.kt.vals.data(), nk * 8, cudaMemcpyHostToDevice, st));
+            const long long pn = (long long)g.pnx * g.pny * (2 * g.phz + 1);
+            pair64 = E.buf<double>("pair64", (size_t)pn);
+            float *pair32 = E.buf<float>("pair32", (size_t)pn);
+            launch_build_pair(g, dev_model(pl.f.m), 0, search_vals, pair64, pair32, st);
+            // the template over the informed-cell bitmap of the grid padded by
+            // the radiuses, for every bin; its linear offsets are 32-bit
+            const long long PX = g.nx + 2LL * g.rx, PY = g.ny + 2LL * g.ry;
+            if ((long long)g.rz * PY * PX + (long long)g.ry * PX + g.rx > 2147483647LL)
+                throw CudaFail{-4, "grid too large for the template search at these radiuses"};
+            std::vector<int4> t4(tv.size());
+            for (size_t i = 0; i < tv.size(); ++i)
+                t4[i] = make_int4(tv[i].dx, tv[i].dy, tv[i].dz, template_padded_offset(g, tv[i].dx, tv[i].dy, tv[i].dz));
+            int4 *tmpl = E.buf<int4>("tmpl", std::max<size_t>(t4.size(), 1));
+            if (!t4.empty())
+                HB_CK(cudaMemcpyAsync(tmpl, t4.data(), t4.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+            std::vector<int> all_bins(g.n_bins);
+            for (int b = 0; b < g.n_bins; ++b) all_bins[b] = b;
+            int *tmpl_bins = E.buf<int>("tmpl_bins", (size_t)g.n_bins);
+            HB_CK(cudaMemcpyAsync(tmpl_bins, all_bins.data(), (size_t)g.n_bins * 4, cudaMemcpyHostToDevice, st));
+            HB_CK(cudaStreamSynchronize(st)); // host temporaries
+            E.stats.launches += 1;
+            nb_rec = E.buf<int2>("nb_rec", (size_t)n * k);
+            nb_n = E.buf<int>("nb_n", (size_t)n);
+            int *tcount = E.buf<int>("cok_tcount", 1);
+            HB_CK(cudaMemsetAsync(tcount, 0, 4, st));
+            if (n_t > 0)
+            {
+                HB_CK(launch_search_template(g, d_pm, E.buf<uint32_t>("mask_bits", (size_t)(template_padded_cells(g) + 31) / 32),
+                                             0, tmpl_bins, g.n_bins, P.pts_val, tmpl, (int)t4.size(), P.pid_of_node,
+                                             nullptr, nb_rec, nb_n, tcount, E.n_sm(), st));
+                E.stats.launches += 2;
+            }
         }
         E.mark(STAGE_SEARCH, st);
         HB_CK(launch_cok_solve(g, targets, n_t, nb_rec, nb_n, k, pair64, d_cross, d_pd, d_sd, d_sm, cp, d_out, d_omask,

@@ -256,7 +256,7 @@ long template_size(const Flavour &f, const KeyTable &kt)
     return n;
 }
 
-void build_surrogate(const Flavour &f, const KeyTable &kt, Surrogate &sg)
+void build_surrogate(const Flavour &f, const KeyTable &kt, Surrogate &sg, bool running_max)
 {
     sg.ok = false;
     sg.h2_rank.clear();
@@ -286,9 +286,16 @@ void build_surrogate(const Flavour &f, const KeyTable &kt, Surrogate &sg)
                 lo[rk] = std::min(lo[rk], acc);
                 hi[rk] = std::max(hi[rk], acc);
             }
-    // ranks increase with h2: every h2 of rank r lies below every h2 of rank r + 1
-    for (uint32_t r = 0; r + 1 < kt.n_ranks; ++r)
-        if (!(hi[r] < lo[r + 1])) return;
+    if (running_max)
+    {
+        for (uint32_t r = 1; r < kt.n_ranks; ++r) hi[r] = std::max(hi[r], hi[r - 1]);
+    }
+    else
+    {
+        // ranks increase with h2: every h2 of rank r lies below every h2 of rank r + 1
+        for (uint32_t r = 0; r + 1 < kt.n_ranks; ++r)
+            if (!(hi[r] < lo[r + 1])) return;
+    }
     sg.h2_rank = hi;
     sg.h2_cut = hi[kt.n_ranks - 1];
     // A transformed coordinate is formed in float as fma(T2, z, fma(T1, y, T0 * x))

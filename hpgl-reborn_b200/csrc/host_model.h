@@ -94,7 +94,10 @@ long template_size(const Flavour &f, const KeyTable &kt);
 // largest h2 carrying it; when the check holds (ok == true) any candidate whose
 // true h2 exceeds that value for the k-th selected rank ranks strictly after
 // it, so a float h2 with a bounded error can discard far candidates without
-// reading their ranks.
+// reading their ranks. With `running_max` the ranks need not follow h2:
+// h2_rank[r] is then the largest h2 of any rank <= r, which bounds every rank
+// the selection keeps ahead of r all the same (keys that are positions in the
+// sorted template, where offsets of one covariance sit in the sort's order).
 struct Surrogate
 {
     bool ok = false;
@@ -104,7 +107,7 @@ struct Surrogate
     float step[3] = {0, 0, 0};  // ||T e_a||: a bound on how far the k-th distance moves per unit step
     std::vector<double> h2_rank; // largest h2 of each rank
 };
-void build_surrogate(const Flavour &f, const KeyTable &kt, Surrogate &sg);
+void build_surrogate(const Flavour &f, const KeyTable &kt, Surrogate &sg, bool running_max = false);
 
 int clamp_threads(int n);
 // The simulation's uniform draws: n doubles equal to n calls of

@@ -118,6 +118,19 @@ def test_cokriging_against_oracle(name, scale, mark):
     np.testing.assert_array_equal(out[failed], fb[failed])
 
 
+@pytest.mark.parametrize("k", [80, 24])
+def test_template_scan_and_selection_paths(k):
+    """k > 64 takes the template scan over the informed-cell bitmap, k <= 64 the
+    binned selection keyed by template position; both give the oracle's cells."""
+    x = _scaled("gauss_cv", 0.3, 1)
+    x = dict(x, k=k)
+    od, om, ost = _oracle(x, 1)
+    out, mk, st = _run_ex(x, 1)
+    np.testing.assert_array_equal(mk, om)
+    np.testing.assert_array_equal(st, ost.astype(np.int8))
+    _close(out, od, f"k={k}")
+
+
 def test_device_pointers_match_host_buffers():
     x = _scaled("gauss_cv", 0.35, 1)
     host, hm, hs = _run_ex(x, 1)
