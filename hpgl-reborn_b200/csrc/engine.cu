@@ -438,7 +438,8 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
     S.bin_flag = E.buf<uint8_t>("bin_flag", g.n_bins);
     int *bin_pts = E.buf<int>("bin_pts", std::max(P.m, 1));
     int *tmpl_bins = E.buf<int>("tmpl_bins", g.n_bins);
-    int *scal = E.buf<int>("scalars", 8); // 0 total, 1 max_cand, 2 tmpl bins, 3 ties, 4 tmpl cells, 5 exact cells
+    // 0 total, 1 max_cand, 2 tmpl bins, 3 ties, 4 tmpl cells, 5 exact cells, 6 max_cand of the template bins
+    int *scal = E.buf<int>("scalars", 8);
     int *tmp = E.buf<int>("scan_tmp2", (size_t)scan_tmp_ints(g.n_bins) + 4);
     HB_CK(cudaMemsetAsync(bin_cnt, 0, sizeof(int) * g.n_bins, st));
     HB_CK(cudaMemsetAsync(bin_fill, 0, sizeof(int) * g.n_bins, st));
@@ -448,7 +449,7 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
     exclusive_scan(bin_start, g.n_bins, tmp, scal + 0, st);
     launch_bin_fill(P.pts_xyz, P.n_pts, g, bin_start, bin_fill, bin_pts, st);
     launch_bin_sort(g, bin_start, bin_cnt, bin_pts, S.bin_flag, st);
-    launch_bin_region(g, S.bin_flag, bin_cnt, scal + 1, scal + 2, tmpl_bins, st);
+    launch_bin_region(g, S.bin_flag, bin_cnt, scal + 1, scal + 2, tmpl_bins, scal + 6, st);
     HB_CK(cudaGetLastError());
     int host_scal[8];
     HB_CK(cudaMemcpyAsync(host_scal, scal, sizeof(host_scal), cudaMemcpyDeviceToHost, st));
@@ -456,23 +457,59 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
     E.mark(STAGE_BINS, st);
     int max_cand = host_scal[1];
     const int n_tmpl_bins = host_scal[2];
-    // the sorted template, only when some bin takes the template path
+    const int max_cand_tmpl = host_scal[6];
+    // Template-path bins (sugarbox_neighbour_lookup.h:171-197: the first k informed
+    // cells of the sorted template, in its order) as a selection: the informed
+    // cells of the 27 bins around a cell keyed by their offset's position in the
+    // template, unique keys whose k smallest are those cells, through the fast
+    // search; the template scan over the informed-cell bitmap beyond its limits.
     int n_tmpl = 0;
     int4 *tmpl = E.buf<int4>("tmpl", std::max<long>(pl.tmpl_count, 1));
-    if (host_scal[2] > 0 && pl.tmpl_count > 0)
+    bool tmpl_select = false;
+    uint16_t *keypos16 = nullptr;
+    SurrDev sdp = {};
+    int cand_cap_t = 0, warps_t = 8;
+    if (n_tmpl_bins > 0 && pl.tmpl_count > 0)
     {
-        // the template probes a bitmap of the grid padded by the radiuses; its
-        // linear offsets are 32-bit
-        const long long PX = g.nx + 2LL * g.rx, PY = g.ny + 2LL * g.ry;
-        if ((long long)g.rz * PY * PX + (long long)g.ry * PX + g.rx > 2147483647LL)
-            throw CudaFail{-4, "grid too large for the template search path at these radiuses"};
         const std::vector<Offset> tv = build_template(pl.f, pl.kt);
-        std::vector<int4> t4(tv.size());
-        for (size_t i = 0; i < tv.size(); ++i)
-            t4[i] = make_int4(tv[i].dx, tv[i].dy, tv[i].dz, template_padded_offset(g, tv[i].dx, tv[i].dy, tv[i].dz));
-        HB_CK(cudaMemcpyAsync(tmpl, t4.data(), t4.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
-        HB_CK(cudaStreamSynchronize(st)); // t4 is a temporary
-        n_tmpl = (int)tv.size();
+        if (g.k <= 64 && tv.size() <= 0xFFFE)
+        {
+            cand_cap_t = std::max(4, (max_cand_tmpl + 3) / 4 * 4);
+            while (warps_t > 1 && search_fast_smem_bytes(cand_cap_t, g.k, warps_t) > (size_t)E.max_smem()) --warps_t;
+            tmpl_select = cand_cap_t <= 65536 && search_fast_smem_bytes(cand_cap_t, g.k, warps_t) <= (size_t)E.max_smem();
+        }
+        if (tmpl_select)
+        {
+            std::vector<uint16_t> kp(nk, (uint16_t)0xFFFF);
+            for (size_t i = 0; i < tv.size(); ++i) kp[key_index(g, tv[i].dx, tv[i].dy, tv[i].dz)] = (uint16_t)i;
+            keypos16 = E.buf<uint16_t>("keypos16", nk);
+            HB_CK(cudaMemcpyAsync(keypos16, kp.data(), nk * 2, cudaMemcpyHostToDevice, st));
+            Surrogate sgp;
+            build_surrogate_template(pl.f, tv, sgp);
+            double *h2p = E.buf<double>("h2_pos", sgp.h2_rank.size());
+            HB_CK(cudaMemcpyAsync(h2p, sgp.h2_rank.data(), sgp.h2_rank.size() * 8, cudaMemcpyHostToDevice, st));
+            sdp.on = sgp.ok && !exact_search ? 1 : 0;
+            for (int i = 0; i < 9; ++i) sdp.T[i] = sgp.T[i];
+            for (int a = 0; a < 3; ++a) sdp.step[a] = sgp.step[a];
+            sdp.e3 = sgp.e3;
+            sdp.h2_cut = sgp.h2_cut;
+            sdp.h2_rank = h2p;
+            HB_CK(cudaStreamSynchronize(st)); // kp and sgp are temporaries
+        }
+        else
+        {
+            // the template probes a bitmap of the grid padded by the radiuses; its
+            // linear offsets are 32-bit
+            const long long PX = g.nx + 2LL * g.rx, PY = g.ny + 2LL * g.ry;
+            if ((long long)g.rz * PY * PX + (long long)g.ry * PX + g.rx > 2147483647LL)
+                throw CudaFail{-4, "grid too large for the template search path at these radiuses"};
+            std::vector<int4> t4(tv.size());
+            for (size_t i = 0; i < tv.size(); ++i)
+                t4[i] = make_int4(tv[i].dx, tv[i].dy, tv[i].dz, template_padded_offset(g, tv[i].dx, tv[i].dy, tv[i].dz));
+            HB_CK(cudaMemcpyAsync(tmpl, t4.data(), t4.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+            HB_CK(cudaStreamSynchronize(st)); // t4 is a temporary
+            n_tmpl = (int)tv.size();
+        }
     }
 
     // search
@@ -494,13 +531,17 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
     HB_CK(cudaEventRecord(E.ev_[8], st));
     if (fast)
         HB_CK(launch_search_fast(g, d_mask, all_cells, bin_start, bin_cnt, S.bin_flag, bin_pts, P.pts_xyz, P.pts_val,
-                                 keytab16, sd, tmpl, n_tmpl, P.pid_of_node, cand_cap, warps, S.nb_pid,
+                                 keytab16, sd, 0, P.pid_of_node, cand_cap, warps, S.nb_pid,
                                  S.nb_rec, S.nb_n, tie_cells, scal + 3, scal + 4, scal + 5, st));
     else
         HB_CK(launch_search(g, d_mask, all_cells, bin_start, bin_cnt, S.bin_flag, bin_pts, P.pts_xyz, P.pts_val,
                             keytab(), pl.rank_bits, tmpl, n_tmpl, P.pid_of_node, cand_cap, warps,
                             S.nb_pid, S.nb_rec, S.nb_n, tie_cells, scal + 3, scal + 4, st));
-    if (n_tmpl_bins > 0)
+    if (n_tmpl_bins > 0 && tmpl_select)
+        HB_CK(launch_search_fast(g, d_mask, all_cells, bin_start, bin_cnt, S.bin_flag, bin_pts, P.pts_xyz, P.pts_val,
+                                 keypos16, sdp, 1, P.pid_of_node, cand_cap_t, warps_t, S.nb_pid, S.nb_rec, S.nb_n,
+                                 tie_cells, scal + 3, scal + 4, scal + 5, st));
+    else if (n_tmpl_bins > 0)
         HB_CK(launch_search_template(g, d_mask, E.buf<uint32_t>("mask_bits", (size_t)(template_padded_cells(g) + 31) / 32), all_cells,
                                      tmpl_bins, n_tmpl_bins, P.pts_val, tmpl, n_tmpl, P.pid_of_node, S.nb_pid,
                                      S.nb_rec, S.nb_n, scal + 4, E.n_sm(), st));
@@ -518,7 +559,7 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
         E.stats.search_kernel_ms += ms;
     }
     // flag, scan tiles (+add), emit, pair table, bin count, bin scan, fill, sort, region, search
-    E.stats.launches += 10 + (g.n_cells > 1024 ? 2 : 0) + (n_tmpl_bins > 0 ? 2 : 0);
+    E.stats.launches += 10 + (g.n_cells > 1024 ? 2 : 0) + (n_tmpl_bins > 0 ? (tmpl_select ? 1 : 2) : 0);
 
     // tie groups straddling the k-th slot: std::sort's choice, replayed
     if (S.ties > 0)

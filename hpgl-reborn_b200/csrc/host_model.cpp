@@ -256,48 +256,27 @@ long template_size(const Flavour &f, const KeyTable &kt)
     return n;
 }
 
-void build_surrogate(const Flavour &f, const KeyTable &kt, Surrogate &sg, bool running_max)
+namespace
 {
-    sg.ok = false;
-    sg.h2_rank.clear();
-    for (int i = 0; i < 9; ++i) sg.T[i] = (float)f.m.T[i];
-    if (kt.n_ranks == 0) return;
-    // per rank the smallest and largest h2 carrying it (offsets whose h2 agree
-    // mathematically can differ in the last bit and still share a covariance)
-    std::vector<double> lo(kt.n_ranks, 1e308), hi(kt.n_ranks, -1.0);
-    for (int iz = 0; iz < kt.n[2]; ++iz)
-        for (int iy = 0; iy < kt.n[1]; ++iy)
-            for (int ix = 0; ix < kt.n[0]; ++ix)
-            {
-                const long i = ((long)iz * kt.n[1] + iy) * kt.n[0] + ix;
-                const uint32_t rk = kt.rank[i];
-                if (rk == KEY_EXCLUDED) continue;
-                const double v[3] = {(double)(0 - (ix - kt.half[0])), (double)(0 - (iy - kt.half[1])),
-                                     (double)(0 - (iz - kt.half[2]))};
-                double acc = 0.0;
-                for (int r = 0; r < 3; ++r)
-                {
-                    double d = 0.0;
-                    d += v[0] * f.m.T[3 * r + 0];
-                    d += v[1] * f.m.T[3 * r + 1];
-                    d += v[2] * f.m.T[3 * r + 2];
-                    acc += d * d;
-                }
-                lo[rk] = std::min(lo[rk], acc);
-                hi[rk] = std::max(hi[rk], acc);
-            }
-    if (running_max)
+// h2 = ||T v||^2 in double, v the negated offset (as the key block stores it)
+double offset_h2(const Flavour &f, int dx, int dy, int dz)
+{
+    const double v[3] = {(double)(0 - dx), (double)(0 - dy), (double)(0 - dz)};
+    double acc = 0.0;
+    for (int r = 0; r < 3; ++r)
     {
-        for (uint32_t r = 1; r < kt.n_ranks; ++r) hi[r] = std::max(hi[r], hi[r - 1]);
+        double d = 0.0;
+        d += v[0] * f.m.T[3 * r + 0];
+        d += v[1] * f.m.T[3 * r + 1];
+        d += v[2] * f.m.T[3 * r + 2];
+        acc += d * d;
     }
-    else
-    {
-        // ranks increase with h2: every h2 of rank r lies below every h2 of rank r + 1
-        for (uint32_t r = 0; r + 1 < kt.n_ranks; ++r)
-            if (!(hi[r] < lo[r + 1])) return;
-    }
-    sg.h2_rank = hi;
-    sg.h2_cut = hi[kt.n_ranks - 1];
+    return acc;
+}
+
+// The bounds of the float evaluation, which do not depend on the keys.
+void surrogate_geometry(const Flavour &f, Surrogate &sg)
+{
     // A transformed coordinate is formed in float as fma(T2, z, fma(T1, y, T0 * x))
     // for the cell and for the candidate, both relative to the bin corner, then
     // subtracted: with |T' - T| <= u |T| and four roundings, each component is off
@@ -318,6 +297,60 @@ void build_surrogate(const Flavour &f, const KeyTable &kt, Surrogate &sg, bool r
         for (int r = 0; r < 3; ++r) s += f.m.T[3 * r + a] * f.m.T[3 * r + a];
         sg.step[a] = (float)(std::sqrt(s) * (1.0 + 1e-6));
     }
+}
+} // namespace
+
+void build_surrogate(const Flavour &f, const KeyTable &kt, Surrogate &sg, bool running_max)
+{
+    sg.ok = false;
+    sg.h2_rank.clear();
+    for (int i = 0; i < 9; ++i) sg.T[i] = (float)f.m.T[i];
+    if (kt.n_ranks == 0) return;
+    // per rank the smallest and largest h2 carrying it (offsets whose h2 agree
+    // mathematically can differ in the last bit and still share a covariance)
+    std::vector<double> lo(kt.n_ranks, 1e308), hi(kt.n_ranks, -1.0);
+    for (int iz = 0; iz < kt.n[2]; ++iz)
+        for (int iy = 0; iy < kt.n[1]; ++iy)
+            for (int ix = 0; ix < kt.n[0]; ++ix)
+            {
+                const long i = ((long)iz * kt.n[1] + iy) * kt.n[0] + ix;
+                const uint32_t rk = kt.rank[i];
+                if (rk == KEY_EXCLUDED) continue;
+                const double acc = offset_h2(f, ix - kt.half[0], iy - kt.half[1], iz - kt.half[2]);
+                lo[rk] = std::min(lo[rk], acc);
+                hi[rk] = std::max(hi[rk], acc);
+            }
+    if (running_max)
+    {
+        for (uint32_t r = 1; r < kt.n_ranks; ++r) hi[r] = std::max(hi[r], hi[r - 1]);
+    }
+    else
+    {
+        // ranks increase with h2: every h2 of rank r lies below every h2 of rank r + 1
+        for (uint32_t r = 0; r + 1 < kt.n_ranks; ++r)
+            if (!(hi[r] < lo[r + 1])) return;
+    }
+    sg.h2_rank = hi;
+    sg.h2_cut = hi[kt.n_ranks - 1];
+    surrogate_geometry(f, sg);
+    sg.ok = true;
+}
+
+void build_surrogate_template(const Flavour &f, const std::vector<Offset> &tmpl, Surrogate &sg)
+{
+    sg.ok = false;
+    sg.h2_rank.clear();
+    for (int i = 0; i < 9; ++i) sg.T[i] = (float)f.m.T[i];
+    if (tmpl.empty()) return;
+    sg.h2_rank.resize(tmpl.size());
+    double run = -1.0;
+    for (size_t i = 0; i < tmpl.size(); ++i)
+    {
+        run = std::max(run, offset_h2(f, tmpl[i].dx, tmpl[i].dy, tmpl[i].dz));
+        sg.h2_rank[i] = run;
+    }
+    sg.h2_cut = run;
+    surrogate_geometry(f, sg);
     sg.ok = true;
 }
 } // namespace hb

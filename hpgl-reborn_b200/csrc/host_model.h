@@ -108,6 +108,9 @@ struct Surrogate
     std::vector<double> h2_rank; // largest h2 of each rank
 };
 void build_surrogate(const Flavour &f, const KeyTable &kt, Surrogate &sg, bool running_max = false);
+// The same for keys that are positions in the sorted template `tmpl` (the
+// running maximum of h2 along it).
+void build_surrogate_template(const Flavour &f, const std::vector<Offset> &tmpl, Surrogate &sg);
 
 int clamp_threads(int n);
 // The simulation's uniform draws: n doubles equal to n calls of

@@ -46,8 +46,10 @@ void launch_bin_fill(const unsigned long long *pts_xyz, const int *n_pts, const 
                      int *bin_fill, int *bin_pts, cudaStream_t st);
 void launch_bin_sort(const Geom &g, const int *bin_start, const int *bin_cnt, int *bin_pts, uint8_t *bin_flag,
                      cudaStream_t st);
+// max_cand / max_cand_tmpl: the largest 27-bin candidate count of the cluster-
+// path / template-path bins
 void launch_bin_region(const Geom &g, uint8_t *bin_flag, const int *bin_cnt, int *max_cand, int *n_tmpl_bins,
-                       int *tmpl_bins, cudaStream_t st);
+                       int *tmpl_bins, int *max_cand_tmpl, cudaStream_t st);
 // Template-path search over a bitmap of the grid padded by the radiuses:
 // `bits` is scratch of (template_padded_cells + 31) / 32 words; template entries
 // carry template_padded_offset(dx, dy, dz) in .w.
@@ -77,11 +79,13 @@ struct SurrDev
 };
 
 size_t search_fast_smem_bytes(int cand_cap, int k, int warps);
-// exact_cells (may be null) counts cells the float prefilter left to the exact path
+// exact_cells (may be null) counts cells the float prefilter left to the exact
+// path. template_bins = 0 searches the cluster-path bins; 1 the template-path
+// bins, keytab16 then holding template positions (n_template_cells counts them)
 cudaError_t launch_search_fast(const Geom &g, const uint8_t *mask, int all_cells, const int *bin_start,
                                const int *bin_cnt, const uint8_t *bin_flag, const int *bin_pts,
                                const unsigned long long *pts_xyz, const float *pts_vf, const uint16_t *keytab16,
-                               const SurrDev &sd, const int4 *tmpl, int n_tmpl, const int *pid_of_node, int cand_cap,
+                               const SurrDev &sd, int template_bins, const int *pid_of_node, int cand_cap,
                                int warps, int *nb_pid, int2 *nb_rec, int *nb_n, int *tie_cells, int *tie_count,
                                int *n_template_cells, int *exact_cells, cudaStream_t st);
 void launch_resolve_ties(const Geom &g, const int *tie_cells, const int *tie_count, int first, int chunk,

@@ -224,7 +224,7 @@ __global__ void k_bin_sort(Geom g, const int *__restrict__ bin_start, const int 
 // bit 1: the cells of this bin take the template path
 __global__ void k_bin_region(Geom g, uint8_t *__restrict__ bin_flag, const int *__restrict__ bin_cnt,
                              int *__restrict__ max_cand, int *__restrict__ n_template_bins,
-                             int *__restrict__ template_bins)
+                             int *__restrict__ template_bins, int *__restrict__ max_cand_tmpl)
 {
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < g.n_bins; b += gridDim.x * blockDim.x)
     {
@@ -244,6 +244,7 @@ __global__ void k_bin_region(Geom g, uint8_t *__restrict__ bin_flag, const int *
         {
             bin_flag[b] |= 2;
             template_bins[atomicAdd(n_template_bins, 1)] = b;
+            atomicMax(max_cand_tmpl, cand);
         }
         else
             atomicMax(max_cand, cand);
@@ -864,7 +865,7 @@ __global__ void __launch_bounds__(256) k_search_fast(
     const Geom g, const uint8_t *__restrict__ mask, int all_cells, const int *__restrict__ bin_start,
     const int *__restrict__ bin_cnt, const uint8_t *__restrict__ bin_flag, const int *__restrict__ bin_pts,
     const unsigned long long *__restrict__ pts_xyz, const float *__restrict__ pts_vf,
-    const uint16_t *__restrict__ keytab16, const SurrDev sd, const int4 *__restrict__ tmpl, int n_tmpl,
+    const uint16_t *__restrict__ keytab16, const SurrDev sd, int template_bins,
     const int *__restrict__ pid_of_node, int cand_cap, int *__restrict__ nb_pid, int2 *__restrict__ nb_rec,
     int *__restrict__ nb_n, int *__restrict__ tie_cells, int *__restrict__ tie_count,
     int *__restrict__ n_template_cells, int *__restrict__ exact_cells)
@@ -880,7 +881,9 @@ __global__ void __launch_bounds__(256) k_search_fast(
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const int k = g.k;
 
-    if (bin_flag[b] & 2) return; // k_search_template
+    // the cluster-path bins, or (template_bins) the template-path bins with
+    // template positions as keys
+    if (((bin_flag[b] >> 1) & 1) != template_bins) return;
 
     float4 *ctp = reinterpret_cast<float4 *>(smem);
     int *cklin = reinterpret_cast<int *>(ctp + cand_cap);
@@ -940,7 +943,7 @@ __global__ void __launch_bounds__(256) k_search_fast(
     bool have_h = false;
     double h_prev = 0.0;
     float path = 0.0f;
-    int n_exact = 0;
+    int n_exact = 0, n_done = 0;
     // Chunks of kChunk consecutive cells share a sublist of the candidates within
     // R of the chunk's centre (transformed coordinates), kept in `keys`. A cell scans
     // it instead of all C when sqrt(Tg) + |cell - centre| + slack <= R: every
@@ -1053,6 +1056,7 @@ __global__ void __launch_bounds__(256) k_search_fast(
             have_h = n != 0;
         h_prev = h;
         path = 0.0f;
+        ++n_done;
         if (lane == 0)
         {
             if (n < 0)
@@ -1066,6 +1070,7 @@ __global__ void __launch_bounds__(256) k_search_fast(
         }
     }
     if (exact_cells && lane == 0 && n_exact) atomicAdd(exact_cells, n_exact);
+    if (template_bins && n_template_cells && lane == 0 && n_done) atomicAdd(n_template_cells, n_done);
 }
 
 size_t search_fast_smem_bytes(int cand_cap, int k, int warps)
@@ -1077,7 +1082,7 @@ size_t search_fast_smem_bytes(int cand_cap, int k, int warps)
 cudaError_t launch_search_fast(const Geom &g, const uint8_t *mask, int all_cells, const int *bin_start,
                                const int *bin_cnt, const uint8_t *bin_flag, const int *bin_pts,
                                const unsigned long long *pts_xyz, const float *pts_vf, const uint16_t *keytab16,
-                               const SurrDev &sd, const int4 *tmpl, int n_tmpl, const int *pid_of_node, int cand_cap,
+                               const SurrDev &sd, int template_bins, const int *pid_of_node, int cand_cap,
                                int warps, int *nb_pid, int2 *nb_rec, int *nb_n, int *tie_cells, int *tie_count,
                                int *n_template_cells, int *exact_cells, cudaStream_t st)
 {
@@ -1087,7 +1092,7 @@ cudaError_t launch_search_fast(const Geom &g, const uint8_t *mask, int all_cells
         cudaError_t e = cudaFuncSetAttribute(k_search_fast<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         k_search_fast<2><<<g.n_bins, warps * 32, smem, st>>>(g, mask, all_cells, bin_start, bin_cnt, bin_flag, bin_pts,
-                                                            pts_xyz, pts_vf, keytab16, sd, tmpl, n_tmpl, pid_of_node,
+                                                            pts_xyz, pts_vf, keytab16, sd, template_bins, pid_of_node,
                                                             cand_cap, nb_pid, nb_rec, nb_n, tie_cells, tie_count,
                                                             n_template_cells, exact_cells);
     }
@@ -1096,7 +1101,7 @@ cudaError_t launch_search_fast(const Geom &g, const uint8_t *mask, int all_cells
         cudaError_t e = cudaFuncSetAttribute(k_search_fast<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         k_search_fast<4><<<g.n_bins, warps * 32, smem, st>>>(g, mask, all_cells, bin_start, bin_cnt, bin_flag, bin_pts,
-                                                            pts_xyz, pts_vf, keytab16, sd, tmpl, n_tmpl, pid_of_node,
+                                                            pts_xyz, pts_vf, keytab16, sd, template_bins, pid_of_node,
                                                             cand_cap, nb_pid, nb_rec, nb_n, tie_cells, tie_count,
                                                             n_template_cells, exact_cells);
     }
@@ -1405,10 +1410,10 @@ void launch_bin_sort(const Geom &g, const int *bin_start, const int *bin_cnt, in
     k_bin_sort<<<blocks, 256, 0, st>>>(g, bin_start, bin_cnt, bin_pts, bin_flag);
 }
 void launch_bin_region(const Geom &g, uint8_t *bin_flag, const int *bin_cnt, int *max_cand, int *n_tmpl_bins,
-                       int *tmpl_bins, cudaStream_t st)
+                       int *tmpl_bins, int *max_cand_tmpl, cudaStream_t st)
 {
     int blocks = (g.n_bins + 255) / 256;
-    k_bin_region<<<blocks, 256, 0, st>>>(g, bin_flag, bin_cnt, max_cand, n_tmpl_bins, tmpl_bins);
+    k_bin_region<<<blocks, 256, 0, st>>>(g, bin_flag, bin_cnt, max_cand, n_tmpl_bins, tmpl_bins, max_cand_tmpl);
 }
 
 // Template-path cells (k_search and k_search_fast leave their bins alone): a
