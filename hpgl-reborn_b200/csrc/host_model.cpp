@@ -204,14 +204,21 @@ void build_key_table(const Flavour &f, KeyTable &kt, int n_threads)
     // are sorted by the value's bit pattern, which orders positive doubles like
     // their values (least-significant-digit radix sort, 11-bit digits, digits
     // that every key shares skipped), then ranked walking down from the top.
+    // The block is symmetric (index total-1-i holds -d) and so are the values
+    // (cov(-d) is formed from the same squares as cov(d)), so the first half and
+    // the centre are ranked and the mirrors take their ranks.
     struct KI
     {
         uint64_t key;
         uint32_t idx;
     };
     std::vector<KI> a, b;
-    a.reserve(total / 4);
-    for (long i = 0; i < total; ++i)
+    a.reserve(total / 8 + 1);
+    const long half = (total - 1) / 2; // the centre's index
+    bool symmetric = true;
+    for (long i = 0; i <= half && symmetric; ++i) symmetric = kt.vals[i] == kt.vals[total - 1 - i];
+    const long last = symmetric ? half : total - 1;
+    for (long i = 0; i <= last; ++i)
         if (kt.vals[i] > thr)
         {
             uint64_t bits;
@@ -239,6 +246,7 @@ void build_key_table(const Flavour &f, KeyTable &kt, int n_threads)
     {
         if (j + 1 < a.size() && a[j].key != a[j + 1].key) ++r;
         kt.rank[a[j].idx] = r;
+        if (symmetric) kt.rank[total - 1 - a[j].idx] = r;
     }
     kt.n_ranks = a.empty() ? 0 : r + 1;
 }
