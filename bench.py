@@ -26,7 +26,8 @@ single-threaded hpgl_sis_simulation on a smaller grid of that generator.
 
 Usage:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 For N > 1 the driver runs it under torchrun; every rank runs its own replica
-(the path needs no collective) and rank 0 prints one JSON line.
+(cells are independent given the conditioning data, so no collective is on the
+data path) and rank 0 prints one JSON line.
 """
 from __future__ import annotations
 
