@@ -669,16 +669,78 @@ __global__ void __launch_bounds__(256, 1)
 // two rows. The arithmetic (right-looking Cholesky with the forward
 // substitution fused in, FP32 back substitution, dual-weighted FP64 residual
 // correction, classic refinement and FP64 escalation) is that of solve_one.
+//
+// M is stored packed: row j is read and written only from column 4*(j/4) on
+// (its first 16-byte chunk holding a column >= j) through the right-hand sides,
+// so row j keeps LD/4 - j/4 chunks. Row j's column c sits at float
+// 4*row[j] + c; the rows follow one another in order, and each row's start
+// is moved forward by whole chunks until the 16-byte chunk index of column 0,
+// modulo 8, differs from that of every earlier row of its group of 8 rows.
+// The back substitution's 16-byte loads (lanes t..t+7 reading rows t..t+7, or
+// NP-1-t down) then keep to distinct banks as in a square layout, at 68%
+// (NP = 32) or 60% (NP = 64) of its footprint, which leaves the L1 cache
+// the shared memory gives up for the pair-table gathers.
+template <int NP>
+struct FoldRows
+{
+    int row[NP]; // chunk index of column 0 of each row
+    int chunks;  // 16-byte chunks of the packed matrix
+};
+
+template <int NP>
+constexpr FoldRows<NP> make_fold_rows()
+{
+    FoldRows<NP> f{};
+    constexpr int C = (NP + 4) / 4; // chunks of a full row
+    int end = 0;
+    unsigned used = 0;
+    for (int j = 0; j < NP; ++j)
+    {
+        if (j % 8 == 0) used = 0;
+        const int a = j / 4;
+        int p = end;
+        while (used & (1u << ((p - a) & 7))) ++p;
+        used |= 1u << ((p - a) & 7);
+        f.row[j] = p - a;
+        end = p + C - a;
+    }
+    f.chunks = end;
+    return f;
+}
+
+__device__ constexpr FoldRows<8> d_fold_rows8 = make_fold_rows<8>();
+__device__ constexpr FoldRows<16> d_fold_rows16 = make_fold_rows<16>();
+__device__ constexpr FoldRows<32> d_fold_rows32 = make_fold_rows<32>();
+__device__ constexpr FoldRows<64> d_fold_rows64 = make_fold_rows<64>();
+
+// Float offset of column 0 of row j of the packed matrix: the tables are
+// constant with known contents, so with j known after unrolling the offset
+// folds into the shared-memory instruction; a lane's own rows (t, NP-1-t) are
+// read once per call.
+template <int NP>
+__device__ __forceinline__ int fold_row(int j)
+{
+    if constexpr (NP == 8)
+        return 4 * d_fold_rows8.row[j];
+    else if constexpr (NP == 16)
+        return 4 * d_fold_rows16.row[j];
+    else if constexpr (NP == 32)
+        return 4 * d_fold_rows32.row[j];
+    else
+        return 4 * d_fold_rows64.row[j];
+}
+
 template <int NP, int R>
 struct FoldSmem
 {
     static constexpr int LD = NP + 4; // NP entries, then up to 4 right-hand sides
-    static constexpr size_t m_bytes = (size_t)NP * LD * sizeof(float);
+    static constexpr size_t m_bytes = (size_t)make_fold_rows<NP>().chunks * 16;
     static constexpr size_t lin_off = m_bytes;
     static constexpr size_t x_off = (lin_off + NP * sizeof(int) + 15) / 16 * 16;
+    static constexpr size_t raw = x_off + (size_t)R * NP * sizeof(double);
     // Systems sharing a warp sit 4 G bytes apart modulo 128, so the G words each
     // writes per step, and the rows they broadcast, fall on disjoint banks.
-    static constexpr size_t bytes = (x_off + (size_t)R * NP * sizeof(double) + 127) / 128 * 128 + 4 * (NP / 2);
+    static constexpr size_t bytes = raw + (size_t)((4 * (NP / 2) - (int)(raw % 128) + 128) % 128);
 };
 
 template <int G>
@@ -714,7 +776,7 @@ __device__ __forceinline__ void fold_back(const FoldGrp<NP / 2> &fg, const float
                                           const float (&yb)[Q], float inv_a, float inv_b, float (&xa)[Q],
                                           float (&xb)[Q])
 {
-    constexpr int G = NP / 2, LD = FoldSmem<NP, 3>::LD;
+    constexpr int G = NP / 2;
     const int rb = NP - 1 - t;
     float acc_a[Q], acc_b[Q];
 #pragma unroll
@@ -725,8 +787,8 @@ __device__ __forceinline__ void fold_back(const FoldGrp<NP / 2> &fg, const float
         xa[q] = 0.0f;
         xb[q] = 0.0f;
     }
-    const float4 *Ma = reinterpret_cast<const float4 *>(M + t * LD);
-    const float4 *Mb = reinterpret_cast<const float4 *>(M + rb * LD);
+    const float4 *Ma = reinterpret_cast<const float4 *>(M + fold_row<NP>(t));
+    const float4 *Mb = reinterpret_cast<const float4 *>(M + fold_row<NP>(rb));
     float4 ma = make_float4(0, 0, 0, 0), mb = ma;
 #pragma unroll
     for (int i = NP - 1; i >= 0; --i)
@@ -780,7 +842,7 @@ template <int NP, int Q>
 __device__ __forceinline__ void fold_forward(const FoldGrp<NP / 2> &fg, const float *M, int t, const float (&ra)[Q],
                                              const float (&rb_rhs)[Q], float (&ya)[Q], float (&yb)[Q])
 {
-    constexpr int G = NP / 2, LD = FoldSmem<NP, 3>::LD;
+    constexpr int G = NP / 2;
     const int rb = NP - 1 - t;
     float acc_a[Q], acc_b[Q];
 #pragma unroll
@@ -794,7 +856,8 @@ __device__ __forceinline__ void fold_forward(const FoldGrp<NP / 2> &fg, const fl
 #pragma unroll
     for (int j = 0; j < NP; ++j)
     {
-        const float inv_j = rsqrtf(M[j * LD + j]);
+        const float *Mj = M + fold_row<NP>(j);
+        const float inv_j = rsqrtf(Mj[j]);
         float yj[Q];
         if (j < G)
         {
@@ -818,13 +881,13 @@ __device__ __forceinline__ void fold_forward(const FoldGrp<NP / 2> &fg, const fl
         }
         if (j < G && t > j)
         {
-            const float l = M[j * LD + t] * inv_j;
+            const float l = Mj[t] * inv_j;
 #pragma unroll
             for (int q = 0; q < Q; ++q) acc_a[q] -= l * yj[q];
         }
         if (rb > j)
         {
-            const float l = M[j * LD + rb] * inv_j;
+            const float l = Mj[rb] * inv_j;
 #pragma unroll
             for (int q = 0; q < Q; ++q) acc_b[q] -= l * yj[q];
         }
@@ -1066,24 +1129,26 @@ __global__ void __launch_bounds__(fold_threads<NP>(), fold_min_blocks<NP>())
 #pragma unroll
         for (int j = 0; j < NP; ++j)
         {
+            // row j of the packed matrix holds columns 4*(j/4) on
+            float *Mj = M + fold_row<NP>(j);
             if (j < G)
             {
-                M[j * LD + t] = ra[j];
+                if (t >= (j & ~3)) Mj[t] = ra[j];
                 if (t == j)
                 {
 #pragma unroll
-                    for (int q = 0; q < R; ++q) M[j * LD + NP + q] = rhs_a[q];
+                    for (int q = 0; q < R; ++q) Mj[NP + q] = rhs_a[q];
                 }
             }
-            M[j * LD + rb] = rbv[j];
+            if (rb >= (j & ~3)) Mj[rb] = rbv[j];
             if (j >= G && rb == j)
             {
 #pragma unroll
-                for (int q = 0; q < R; ++q) M[j * LD + NP + q] = rhs_b[q];
+                for (int q = 0; q < R; ++q) Mj[NP + q] = rhs_b[q];
             }
             fg.sync();
             float mj[LD];
-            const float4 *mv = reinterpret_cast<const float4 *>(M + j * LD);
+            const float4 *mv = reinterpret_cast<const float4 *>(Mj);
 #pragma unroll
             for (int q = j / 4; q < LD / 4; ++q)
             {
@@ -1534,6 +1599,23 @@ static cudaError_t launch_kernel(K kern, int threads, size_t smem, int max_items
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
+    // The smallest shared-memory carveout that holds per_sm blocks: the rest of
+    // the SM's unified L1 / shared storage stays L1 for the pair-table gathers.
+    {
+        int dev = 0, smem_sm = 0, reserved = 0;
+        cudaFuncAttributes fa{};
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) == cudaSuccess &&
+            cudaFuncGetAttributes(&fa, kern) == cudaSuccess && smem_sm > 0)
+        {
+            const long long need = (long long)per_sm * ((long long)smem + (long long)fa.sharedSizeBytes + reserved);
+            int pct = (int)((need * 100 + smem_sm - 1) / smem_sm);
+            pct = pct < 1 ? 1 : (pct > 100 ? 100 : pct);
+            e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+            if (e != cudaSuccess) return e;
+        }
+    }
     long long want = ((long long)max_items + gpb - 1) / gpb;
     long long blocks = (long long)n_sm * per_sm;
     if (want < blocks) blocks = want;
