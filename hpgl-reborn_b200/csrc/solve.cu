@@ -1373,7 +1373,10 @@ template <int NP>
 struct Fold64Smem
 {
     static constexpr int LD = NP + 4; // doubles: NP entries, then up to 4 right-hand sides
-    static constexpr size_t m_bytes = (size_t)NP * LD * sizeof(double);
+    // Row j is read only at step j (no back substitution), so two rows in turn
+    // suffice: the step's warp synchronisation orders the writes of row j + 2
+    // after every lane's reads of row j.
+    static constexpr size_t m_bytes = (size_t)2 * LD * sizeof(double);
     static constexpr size_t lin_off = m_bytes;
     // systems sharing a warp 16 bytes apart modulo 128: their broadcast rows on different banks
     static constexpr size_t bytes = (lin_off + NP * sizeof(int) + 127) / 128 * 128 + 16;
@@ -1477,24 +1480,25 @@ __global__ void __launch_bounds__(HB_FOLD64_THREADS, 1)
 #pragma unroll
         for (int j = 0; j < NP; ++j)
         {
+            double *Mj = M + (j & 1) * LD;
             if (j < G)
             {
-                M[j * LD + t] = ra[j];
+                Mj[t] = ra[j];
                 if (t == j)
                 {
 #pragma unroll
-                    for (int q = 0; q < R; ++q) M[j * LD + NP + q] = rhs_a[q];
+                    for (int q = 0; q < R; ++q) Mj[NP + q] = rhs_a[q];
                 }
             }
-            M[j * LD + rb] = rbv[j];
+            Mj[rb] = rbv[j];
             if (j >= G && rb == j)
             {
 #pragma unroll
-                for (int q = 0; q < R; ++q) M[j * LD + NP + q] = rhs_b[q];
+                for (int q = 0; q < R; ++q) Mj[NP + q] = rhs_b[q];
             }
             fg.sync();
             double mj[LD];
-            const double2 *mv = reinterpret_cast<const double2 *>(M + j * LD);
+            const double2 *mv = reinterpret_cast<const double2 *>(Mj);
 #pragma unroll
             for (int q = j / 2; q < LD / 2; ++q)
             {
