@@ -942,25 +942,28 @@ def main():
     C.memmove(h_out, h_data, nbytes)
     C.memmove(h_omask, h_mask, n)
 
-    def host_call():
-        o = W._HPGL_B200_OPTIONS(precision=1, refine_steps=3, flags=W.FLAG_OUT_IS_CLONE, stream=None,
+    def host_call(precision):
+        o = W._HPGL_B200_OPTIONS(precision=precision, refine_steps=3, flags=W.FLAG_OUT_IS_CLONE, stream=None,
                                  estimate64=None, variance=h_var, status=None, ik_probs=None)
         rc = krige(h_data, h_mask, h_mean if lvm else None, h_out, h_omask, o)
         W.check(rc, "kriging_ex (host)")
         return W.last_stats()
 
-    for _ in range(args.warmup):
-        host_call()
-    e2e_t = []
-    st = None
-    for _ in range(args.steps):
+    def timed_host(precision):
+        for _ in range(args.warmup):
+            host_call(precision)
+        times = []
+        stats = None
+        for _ in range(args.steps):
+            barrier()
+            t0 = time.perf_counter()
+            stats = host_call(precision)
+            times.append(time.perf_counter() - t0)
         barrier()
-        t0 = time.perf_counter()
-        st = host_call()
-        e2e_t.append(time.perf_counter() - t0)
-    barrier()
-    e2e_s = max_over_ranks(float(np.mean(e2e_t)))
-    e2e_value = st["kriged_cells"] * world / e2e_s
+        return stats, stats["kriged_cells"] * world / max_over_ranks(float(np.mean(times)))
+
+    st, e2e_value = timed_host(1)
+    _, e2e_value64 = timed_host(0)
     for ptr in h_ptrs:
         lib.hpgl_b200_host_free(ptr)
 
@@ -984,7 +987,7 @@ def main():
                        "l2": "flushed between timed steps (256 MB write)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "fp64_plain": {"value": value64, "ms_per_step": ms64, "kernel_tflops": fp64_kernel_tflops,
-                           "kernel_frac_of_fp64_peak": fp64_kernel_tflops / pk["fp64"]},
+                           "kernel_frac_of_fp64_peak": fp64_kernel_tflops / pk["fp64"], "e2e_value": e2e_value64},
             "fp32_refined_over_fp64_plain": value / value64,
             "rel_err_fp32_refined_vs_fp64": rel_err,
             "escalated_cells": last["escalated_cells"],
