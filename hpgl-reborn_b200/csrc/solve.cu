@@ -1382,9 +1382,13 @@ struct Fold64Smem
     static constexpr size_t bytes = (lin_off + NP * sizeof(int) + 127) / 128 * 128 + 16;
 };
 
-// Threads per block of the FP64 folded kernel (one block per SM).
+// Threads per block of the FP64 folded kernel (one block per SM): 384 threads
+// cap registers at 168, which the step's row read 16 bytes at a time fits with
+// almost no spills, and give each scheduler three warps to cover the FP64
+// dependency latency (256 threads: 198M cells/s; 320: 173M; 512, spilling: 196M;
+// 384: 211M on the 256x256x128 benchmark).
 #ifndef HB_FOLD64_THREADS
-#define HB_FOLD64_THREADS 256
+#define HB_FOLD64_THREADS 384
 #endif
 
 template <int NP, bool ORDINARY>
@@ -1497,29 +1501,38 @@ __global__ void __launch_bounds__(HB_FOLD64_THREADS, 1)
                 for (int q = 0; q < R; ++q) Mj[NP + q] = rhs_b[q];
             }
             fg.sync();
-            double mj[LD];
-            const double2 *mv = reinterpret_cast<const double2 *>(Mj);
-#pragma unroll
-            for (int q = j / 2; q < LD / 2; ++q)
-            {
-                const double2 v2 = mv[q];
-                mj[2 * q] = v2.x;
-                mj[2 * q + 1] = v2.y;
-            }
-            const double d = mj[j];
+            // row j is applied as it is read, 16 bytes at a time, so it never
+            // sits in registers whole
+            const double d = Mj[j];
             fail |= !(d > 0.0);
             const double inv_s = rsqrt(d);
             const double inv2 = inv_s * inv_s;
+            const double s_a = j < G ? ra[j] * inv2 : 0.0;
+            const double s_b = rbv[j] * inv2;
+            const double2 *mv = reinterpret_cast<const double2 *>(Mj);
+#pragma unroll
+            for (int q2 = j / 2; q2 < LD / 2; ++q2)
+            {
+                const double2 v2 = mv[q2];
+#pragma unroll
+                for (int e = 0; e < 2; ++e)
+                {
+                    const int c = 2 * q2 + e;
+                    const double m = e == 0 ? v2.x : v2.y;
+                    if (c > j && c < NP)
+                    {
+                        if (j < G && c < G) ra[c] -= s_a * m;
+                        rbv[c] -= s_b * m;
+                    }
+                    else if (c >= NP && c < NP + R)
+                    {
+                        if (j < G && t > j) rhs_a[c - NP] -= s_a * m;
+                        if (rb > j) rhs_b[c - NP] -= s_b * m;
+                    }
+                }
+            }
             if (j < G)
             {
-                const double s = ra[j] * inv2;
-#pragma unroll
-                for (int c = j + 1; c < G; ++c) ra[c] -= s * mj[c];
-                if (t > j)
-                {
-#pragma unroll
-                    for (int q = 0; q < R; ++q) rhs_a[q] -= s * mj[NP + q];
-                }
                 ra[j] *= inv_s;
                 if (t == j)
                 {
@@ -1527,21 +1540,11 @@ __global__ void __launch_bounds__(HB_FOLD64_THREADS, 1)
                     for (int q = 0; q < R; ++q) ya[q] = rhs_a[q] * inv_s;
                 }
             }
+            rbv[j] *= inv_s;
+            if (rb == j)
             {
-                const double s = rbv[j] * inv2;
 #pragma unroll
-                for (int c = j + 1; c < NP; ++c) rbv[c] -= s * mj[c];
-                if (rb > j)
-                {
-#pragma unroll
-                    for (int q = 0; q < R; ++q) rhs_b[q] -= s * mj[NP + q];
-                }
-                rbv[j] *= inv_s;
-                if (rb == j)
-                {
-#pragma unroll
-                    for (int q = 0; q < R; ++q) yb[q] = rhs_b[q] * inv_s;
-                }
+                for (int q = 0; q < R; ++q) yb[q] = rhs_b[q] * inv_s;
             }
         }
 
