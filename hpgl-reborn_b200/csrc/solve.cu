@@ -1363,7 +1363,7 @@ __global__ void __launch_bounds__(fold_threads<NP>(), fold_min_blocks<NP>())
     }
 }
 
-// FP64-plain systems of up to 32 neighbours, folded like k_solve_fold (G = NP/2
+// FP64-plain systems of up to 64 neighbours, folded like k_solve_fold (G = NP/2
 // lanes per system, lane t owning rows t and NP-1-t). FP64 plain needs only the
 // forward substitution: every kriging quantity is a bilinear form
 // u^T A^-1 w = (L^-1 u) . (L^-1 w) of b, (OK) the ones vector and v - mean, so the
@@ -1391,8 +1391,16 @@ struct Fold64Smem
 #define HB_FOLD64_THREADS 384
 #endif
 
+// Systems of 33 to 64 neighbours fold onto one warp each (rows t and 63 - t:
+// 96 doubles a lane), in 256-thread blocks with up to 255 registers.
+template <int NP>
+constexpr int fold64_threads()
+{
+    return NP <= 32 ? HB_FOLD64_THREADS : 256;
+}
+
 template <int NP, bool ORDINARY>
-__global__ void __launch_bounds__(HB_FOLD64_THREADS, 1)
+__global__ void __launch_bounds__(fold64_threads<NP>(), 1)
     k_solve_fold64(const Geom g, const int2 *__restrict__ cells, const int *__restrict__ n_items_ptr,
                    const int2 *__restrict__ nb_rec, int ind_value, SolveParams P)
 {
@@ -1649,9 +1657,9 @@ static cudaError_t launch_one(const Geom &g, const int2 *cells, const int *n_ite
         if (e != cudaSuccess) return e;
         kern<<<(unsigned)blocks, fthreads, smem, st>>>(g, cells, n_items, nb_rec, ind_value, pair32, P);
     }
-    else if constexpr (!REF && NP <= 32)
+    else if constexpr (!REF)
     {
-        constexpr int fthreads = HB_FOLD64_THREADS;
+        constexpr int fthreads = fold64_threads<NP>();
         constexpr int spb = fthreads / (NP / 2); // systems per block
         const size_t smem = Fold64Smem<NP>::bytes * spb;
         auto kern = k_solve_fold64<NP, ORD>;
