@@ -8,34 +8,34 @@
 // SK: w = x, variance C(0) - w.b. The estimate is mean + sum w_i (v_i - mean)
 // (combiner.h:10-25; mean 0 for OK).
 //
-// Layout: one "group" of NP threads per system (NP in {8, 16, 32, 64}); thread r
-// owns row r of the (padded) matrix in registers. Rows past the neighbour count
-// n are identity rows with zero right-hand sides, which leaves the solution of
-// the first n unknowns unchanged. The search stage hands over, per neighbour,
-// its pair-table offset lin(o_i) (o_i = neighbour - centre) and its value, so
+// Layout: one system per G = NP / 2 lanes (NP in {8, 16, 32, 64}), lane t
+// owning rows t and NP - 1 - t of the (padded) matrix in registers ("folded":
+// see the folded kernels below). Rows past the neighbour count n are identity
+// rows with zero right-hand sides, which leaves the solution of the first n
+// unknowns unchanged. The search stage hands over, per neighbour, its
+// pair-table offset lin(o_i) (o_i = neighbour - centre) and its value, so
 // cov(c_i, c_j) = pair[centre + lin_i - lin_j] and cov(c_i, centre) =
 // pair[centre + lin_i]: assembly is one subtraction and one gather per entry.
 //
 // Factorisation: right-looking Cholesky with the forward substitution fused in.
-// Step j: every thread stores its current A[r][j] in row j of the group's shared
-// matrix M and thread j appends its current right-hand sides; the row is read
-// back with 16-byte broadcast loads, and each thread r > j updates
-// A[r][c] -= A[r][j] * M[j][c] / M[j][j] (c > j) and rhs_r -= A[r][j] * rhs_j /
-// M[j][j]; thread j scales its row by 1/sqrt(M[j][j]) and keeps y_j = rhs_j /
-// sqrt(M[j][j]), the forward solution. Afterwards thread r holds row r of L in
-// registers and row r of M holds column r of L (times sqrt(M[r][r])), which the
-// back substitution reads with 16-byte loads of the thread's own row.
+// Step j: the owner of column j of each row stores its current A[r][j] in row
+// j of the system's shared matrix M and the owner of row j appends its current
+// right-hand sides; the row is read back with 16-byte broadcast loads, every
+// row r > j is updated A[r][c] -= A[r][j] * M[j][c] / M[j][j] (c > j) and
+// rhs_r -= A[r][j] * rhs_j / M[j][j]; row j is scaled by 1/sqrt(M[j][j]) and
+// keeps y_j = rhs_j / sqrt(M[j][j]), the forward solution. Afterwards row r
+// of M holds column r of L (times sqrt(M[r][r])), which the back substitution
+// reads with 16-byte loads of the lane's own rows.
 //
 // Precision modes:
 //   FP64 plain   : T = double throughout. Every kriging quantity is a bilinear
 //                  form u^T A^-1 w = (L^-1 u) . (L^-1 w), so the forward
 //                  solutions of b, (OK) the ones vector and v - mean suffice:
 //                  no back substitution.
-//   FP32 refined : the matrix is gathered once from the double pair table and
-//                  kept in shared memory (packed lower triangle, groups of up to
-//                  32 threads; larger groups gather it again); its float
-//                  rounding is factored and solved in float for b, (OK) the
-//                  ones vector and the centred values v - mean. Each bilinear
+//   FP32 refined : the matrix is gathered from the float pair table (the
+//                  rounding of the double one), factored and solved in float
+//                  for b, (OK) the ones vector and the centred values
+//                  v - mean. Each bilinear
 //                  form is corrected with one FP64 residual,
 //                    u^T A^-1 w = u^T x_w + x_u^T (w - A64 x_w) + O(|e_u| |e_w|),
 //                  (x_w = A32^-1 w), so one residual pass in double gives
@@ -54,253 +54,6 @@
 
 namespace hb
 {
-template <int NP>
-struct Grp
-{
-    int r;         // thread index inside the group
-    unsigned mask; // lanes of the group inside its warp (NP <= 32)
-    int bar;       // named barrier id (NP == 64)
-
-    __device__ __forceinline__ void sync() const
-    {
-        if constexpr (NP <= 32)
-            __syncwarp(mask);
-        else
-            asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(NP) : "memory");
-    }
-};
-
-template <int NP, typename T>
-__device__ __forceinline__ T group_sum(const Grp<NP> &g, T v, T *scratch)
-{
-    if constexpr (NP <= 32)
-    {
-#pragma unroll
-        for (int o = NP / 2; o > 0; o >>= 1) v += __shfl_xor_sync(g.mask, v, o, NP);
-        return v;
-    }
-    else
-    {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if ((g.r & 31) == 0) scratch[g.r >> 5] = v;
-        g.sync();
-        T s = scratch[0] + scratch[1];
-        g.sync();
-        return s;
-    }
-}
-
-template <int NP, typename T>
-__device__ __forceinline__ T group_max(const Grp<NP> &g, T v, T *scratch)
-{
-    if constexpr (NP <= 32)
-    {
-#pragma unroll
-        for (int o = NP / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(g.mask, v, o, NP));
-        return v;
-    }
-    else
-    {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-        if ((g.r & 31) == 0) scratch[g.r >> 5] = v;
-        g.sync();
-        T s = fmax(scratch[0], scratch[1]);
-        g.sync();
-        return s;
-    }
-}
-
-// value of `v` held by group thread `src`
-template <int NP, typename T>
-__device__ __forceinline__ T group_bcast(const Grp<NP> &g, T v, int src, T *slot)
-{
-    if constexpr (NP <= 32)
-    {
-        return __shfl_sync(g.mask, v, src, NP);
-    }
-    else
-    {
-        if (g.r == src) *slot = v;
-        g.sync();
-        return *slot;
-    }
-}
-
-template <typename T>
-__device__ __forceinline__ T rsqrt_t(T d);
-template <>
-__device__ __forceinline__ float rsqrt_t<float>(float d) { return rsqrtf(d); }
-template <>
-__device__ __forceinline__ double rsqrt_t<double>(double d) { return rsqrt(d); }
-
-template <typename T>
-__device__ __forceinline__ T pair_get(const float *p32, const double *p64, long long i);
-template <>
-__device__ __forceinline__ float pair_get<float>(const float *p32, const double *, long long i) { return __ldg(p32 + i); }
-template <>
-__device__ __forceinline__ double pair_get<double>(const float *, const double *p64, long long i) { return __ldg(p64 + i); }
-
-// 16-byte vectors of T
-template <typename T>
-struct Vec;
-template <>
-struct Vec<float>
-{
-    typedef float4 type;
-    static constexpr int n = 4;
-    static __device__ __forceinline__ void unpack(const float4 &v, float *o)
-    {
-        o[0] = v.x;
-        o[1] = v.y;
-        o[2] = v.z;
-        o[3] = v.w;
-    }
-};
-template <>
-struct Vec<double>
-{
-    typedef double2 type;
-    static constexpr int n = 2;
-    static __device__ __forceinline__ void unpack(const double2 &v, double *o)
-    {
-        o[0] = v.x;
-        o[1] = v.y;
-    }
-};
-
-// Forward substitution L y = rhs for R right-hand sides (row-oriented).
-template <int NP, typename T, int R>
-__device__ __forceinline__ void forward_solve(const Grp<NP> &g, const T (&row)[NP], T (&acc)[R], T my_inv,
-                                              T *slots, T (&y)[R])
-{
-#pragma unroll
-    for (int q = 0; q < R; ++q) y[q] = 0;
-#pragma unroll
-    for (int j = 0; j < NP; ++j)
-    {
-        if (g.r == j)
-        {
-#pragma unroll
-            for (int q = 0; q < R; ++q) y[q] = acc[q] * my_inv;
-        }
-        T yj[R];
-#pragma unroll
-        for (int q = 0; q < R; ++q) yj[q] = group_bcast<NP, T>(g, y[q], j, slots + (NP <= 32 ? 0 : (q * NP + j)));
-        if (g.r > j)
-        {
-#pragma unroll
-            for (int q = 0; q < R; ++q) acc[q] -= row[j] * yj[q];
-        }
-    }
-    if constexpr (NP > 32) g.sync(); // slots are reused by the next solve
-}
-
-// Back substitution L^T x = y; row r of M holds column r of L times
-// sqrt(M[r][r]). Thread r reads its own row four (float) or two (double)
-// entries at a time; with rows NP + V entries apart the 16-byte loads of eight
-// consecutive threads fall on distinct bank groups.
-template <int NP, typename T, int R, int LD>
-__device__ __forceinline__ void back_solve(const Grp<NP> &g, const T *M, T (&yv)[R], T my_inv, T *slots,
-                                           T (&x)[R])
-{
-    typedef typename Vec<T>::type VT;
-    constexpr int V = Vec<T>::n;
-    T acc[R];
-#pragma unroll
-    for (int q = 0; q < R; ++q)
-    {
-        acc[q] = yv[q];
-        x[q] = 0;
-    }
-    const VT *Mr = reinterpret_cast<const VT *>(M + g.r * LD);
-    T mc[V];
-#pragma unroll
-    for (int i = NP - 1; i >= 0; --i)
-    {
-        if (i % V == V - 1) Vec<T>::unpack(Mr[i / V], mc);
-        if (g.r == i)
-        {
-#pragma unroll
-            for (int q = 0; q < R; ++q) x[q] = acc[q] * my_inv;
-        }
-        T xi[R];
-#pragma unroll
-        for (int q = 0; q < R; ++q) xi[q] = group_bcast<NP, T>(g, x[q], i, slots + (NP <= 32 ? 0 : (q * NP + i)));
-        if (g.r < i)
-        {
-            const T l = mc[i % V] * my_inv;
-#pragma unroll
-            for (int q = 0; q < R; ++q) acc[q] -= l * xi[q];
-        }
-    }
-    if constexpr (NP > 32) g.sync();
-}
-
-// Per-group shared memory of k_solve. M: NP rows of NP matrix entries plus RP
-// right-hand side slots (R padded to 16 bytes).
-template <int NP, typename TF, bool REFINE, int R>
-struct SolveSmem
-{
-    static constexpr int V = 16 / (int)sizeof(TF);
-    static constexpr int RP = (R + V - 1) / V * V;
-    static constexpr int LD = NP + RP;
-    static constexpr size_t m_bytes = (size_t)NP * LD * sizeof(TF);
-    static constexpr size_t lin_off = (m_bytes + 15) / 16 * 16;
-    static constexpr size_t x_off = (lin_off + NP * sizeof(int) + 15) / 16 * 16;
-    static constexpr size_t x_bytes = REFINE ? 2 * NP * sizeof(double) : 0;
-    static constexpr size_t slot_off = x_off + x_bytes;
-    static constexpr size_t slot_bytes = NP > 32 ? 3 * NP * sizeof(TF) : 0;
-    static constexpr size_t scr_off = (slot_off + slot_bytes + 15) / 16 * 16;
-    static constexpr size_t bytes = (scr_off + 4 * sizeof(double) + 15) / 16 * 16;
-};
-
-// Residuals res[q] = rhs[q] - A64 x[q] for the first Q right-hand sides, FP64,
-// A64 row r gathered from the double pair table; X holds the solutions.
-template <int NP, int Q, int RX>
-__device__ __forceinline__ void residuals_fp64(const Grp<NP> &grp, const double *__restrict__ pair64, long long pc,
-                                               int lin, const int *LIN, double *X, int n, bool live,
-                                               const double (&x)[RX], const double (&rhs)[Q], double (&res)[Q])
-{
-    const int r = grp.r;
-#pragma unroll
-    for (int q = 0; q < Q; ++q) X[q * NP + r] = x[q];
-    grp.sync();
-#pragma unroll
-    for (int q = 0; q < Q; ++q) res[q] = rhs[q];
-    if (live)
-    {
-#pragma unroll
-        for (int c = 0; c < NP; ++c)
-        {
-            if (c < n)
-            {
-                const double a = __ldg(pair64 + pc + lin - LIN[c]);
-#pragma unroll
-                for (int q = 0; q < Q; ++q) res[q] -= a * X[q * NP + c];
-            }
-        }
-    }
-    else
-    {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) res[q] = -x[q];
-    }
-    grp.sync();
-}
-
-// Per-group view of the shared memory and the launch-wide parameters.
-template <int NP, typename TF>
-struct GroupMem
-{
-    TF *M;
-    int *LIN;
-    double *X;
-    TF *slots;
-    double *scr;
-};
-
 struct SolveParams
 {
     const double *pair64;
@@ -314,348 +67,12 @@ struct SolveParams
     int *esc_count;
 };
 
-// Factorisation, solves, FP64 correction and outputs of one system whose
-// (float or double) matrix row r is in `row` (lower triangle, padding rows
-// identity) and whose b_r is b64.
-template <int NP, typename TF, bool ORDINARY, bool REFINE>
-__device__ __forceinline__ void solve_one(const Grp<NP> &grp, const GroupMem<NP, TF> &gm, const SolveParams &P,
-                                          TF (&row)[NP], double b64, double vc, bool live, int lin, int my_cell,
-                                          int my_n)
-{
-    constexpr int QB = ORDINARY ? 2 : 1; // b and 1: the systems the weights come from
-    constexpr int R = QB + 1;            // plus v: the adjoint system of the estimate
-    typedef SolveSmem<NP, TF, REFINE, R> SM;
-    constexpr int LD = SM::LD;
-    constexpr int V = SM::V;
-    typedef typename Vec<TF>::type VT;
-    const int r = grp.r;
-    TF *M = gm.M;
-    double *scr = gm.scr;
-
-    // ---- factorisation with the forward substitution of b, 1 and v - mean
-    TF rhs[R], yv[R];
-    rhs[0] = live ? (TF)b64 : (TF)0;
-    if constexpr (ORDINARY) rhs[1] = live ? (TF)1 : (TF)0;
-    rhs[R - 1] = (TF)vc;
-#pragma unroll
-    for (int q = 0; q < R; ++q) yv[q] = (TF)0;
-    bool fail = false;
-    TF my_inv = 0;
-#pragma unroll
-    for (int j = 0; j < NP; ++j)
-    {
-        M[j * LD + r] = row[j];
-        if (r == j)
-        {
-#pragma unroll
-            for (int q = 0; q < R; ++q) M[j * LD + NP + q] = rhs[q];
-        }
-        grp.sync();
-        TF mj[LD];
-        const VT *mv = reinterpret_cast<const VT *>(M + j * LD);
-#pragma unroll
-        for (int q = j / V; q < LD / V; ++q) Vec<TF>::unpack(mv[q], mj + q * V);
-        const TF d = mj[j];
-        fail |= !(d > (TF)0);
-        const TF inv_s = rsqrt_t<TF>(d);
-        const TF s = row[j] * (inv_s * inv_s);
-#pragma unroll
-        for (int c = j + 1; c < NP; ++c) row[c] -= s * mj[c];
-        if (r > j)
-        {
-#pragma unroll
-            for (int q = 0; q < R; ++q) rhs[q] -= s * mj[NP + q];
-        }
-        row[j] *= inv_s;
-        if (r == j)
-        {
-            my_inv = inv_s;
-#pragma unroll
-            for (int q = 0; q < R; ++q) yv[q] = rhs[q] * inv_s;
-        }
-    }
-    const double one = live ? 1.0 : 0.0;
-
-    // Bilinear forms u^T A^-1 w of the estimate and variance.
-    double f_vb, f_bb, f_1b = 0.0, f_v1 = 0.0, f_11 = 0.0;
-    bool escalate = false;
-    double x[R];
-    double corr_vb = 0.0, corr_bb = 0.0;
-    if constexpr (!REFINE)
-    {
-        // (L^-1 u) . (L^-1 w): the forward solutions are all that is needed
-        const double yb = (double)yv[0], yvv = (double)yv[R - 1];
-        f_vb = yvv * yb;
-        f_bb = yb * yb;
-        if constexpr (ORDINARY)
-        {
-            const double y1 = (double)yv[1];
-            f_1b = y1 * yb;
-            f_v1 = yvv * y1;
-            f_11 = y1 * y1;
-        }
-    }
-    else
-    {
-        TF xs[R];
-        back_solve<NP, TF, R, LD>(grp, M, yv, my_inv, gm.slots, xs);
-#pragma unroll
-        for (int q = 0; q < R; ++q) x[q] = (double)xs[q];
-        // With FP32 solutions each form gets the dual-weighted residual correction
-        //   u^T A^-1 w = u^T x_w + x_u^T (w - A64 x_w) + O(|e_u| |e_w|),
-        // x_w = A32^-1 w, x_u = A32^-1 u, the residual in FP64.
-        f_vb = vc * x[0];
-        f_bb = b64 * x[0];
-        if constexpr (ORDINARY)
-        {
-            f_1b = one * x[0];
-            f_v1 = vc * x[1];
-            f_11 = one * x[1];
-        }
-        escalate = fail;
-        double rhs64[QB], res[QB];
-        rhs64[0] = b64;
-        if constexpr (ORDINARY) rhs64[1] = one;
-        residuals_fp64<NP, QB, R>(grp, P.pair64, P.pc, lin, gm.LIN, gm.X, my_n, live, x, rhs64, res);
-        corr_vb = x[R - 1] * res[0];
-        corr_bb = x[0] * res[0];
-        f_vb += corr_vb;
-        f_bb += corr_bb;
-        if constexpr (ORDINARY)
-        {
-            f_1b += x[1] * res[0];
-            f_v1 += x[R - 1] * res[1];
-            f_11 += x[1] * res[1];
-        }
-    }
-    double s_vb = group_sum<NP, double>(grp, f_vb, scr);
-    double s_bb = group_sum<NP, double>(grp, f_bb, scr);
-    double s_1b = 0.0, s_v1 = 0.0, s_11 = 0.0;
-    if constexpr (ORDINARY)
-    {
-        s_1b = group_sum<NP, double>(grp, f_1b, scr);
-        s_v1 = group_sum<NP, double>(grp, f_v1, scr);
-        s_11 = group_sum<NP, double>(grp, f_11, scr);
-    }
-    if constexpr (REFINE)
-    {
-        // a-posteriori check: the first-order correction of each form relative
-        // to the form's scale; what remains after it is about its square
-        const double abs_vb = group_sum<NP, double>(grp, fabs(vc * x[0]), scr) + 1e-300;
-        const double abs_bb = group_sum<NP, double>(grp, fabs(b64 * x[0]), scr) + 1e-300;
-        const double c1 = fabs(group_sum<NP, double>(grp, corr_vb, scr)) / abs_vb;
-        const double c2 = fabs(group_sum<NP, double>(grp, corr_bb, scr)) / abs_bb;
-        const double d = fmax(c1, c2);
-        if (!(d * d <= P.tol)) escalate = true;
-        if (!(s_vb == s_vb) || !(s_bb == s_bb)) escalate = true;
-        if (escalate && P.steps > 0 && !fail)
-        {
-            // classic refinement of x (and y): x += A32^-1 (b - A64 x) until the
-            // correction stops mattering, then the forms without correction
-            double prev = 0.0;
-            bool done = false;
-            for (int it = 0; it < P.steps && !done; ++it)
-            {
-                double rq[QB], rr64[QB], xq[QB];
-#pragma unroll
-                for (int q = 0; q < QB; ++q)
-                {
-                    rq[q] = q == 0 ? b64 : one;
-                    xq[q] = x[q];
-                }
-                residuals_fp64<NP, QB, QB>(grp, P.pair64, P.pc, lin, gm.LIN, gm.X, my_n, live, xq, rq, rr64);
-                TF rr[QB], yy[QB], dd[QB];
-#pragma unroll
-                for (int q = 0; q < QB; ++q) rr[q] = (TF)rr64[q];
-                forward_solve<NP, TF, QB>(grp, row, rr, my_inv, gm.slots, yy);
-                back_solve<NP, TF, QB, LD>(grp, M, yy, my_inv, gm.slots, dd);
-                double dmax = 0.0, xmax = 0.0;
-#pragma unroll
-                for (int q = 0; q < QB; ++q)
-                {
-                    x[q] += (double)dd[q];
-                    dmax = fmax(dmax, fabs((double)dd[q]));
-                    xmax = fmax(xmax, fabs(x[q]));
-                }
-                dmax = group_max<NP, double>(grp, dmax, scr);
-                xmax = group_max<NP, double>(grp, xmax, scr);
-                const double delta = xmax > 0.0 ? dmax / xmax : 0.0;
-                double err;
-                if (it == 0)
-                    err = delta * delta;
-                else
-                {
-                    const double rho = prev > 0.0 ? delta / prev : 0.0;
-                    err = rho < 0.5 ? delta * rho / (1.0 - rho) : 1.0;
-                }
-                if (!(delta == delta)) err = 1.0;
-                prev = delta;
-                done = err <= P.tol;
-            }
-            if (done)
-            {
-                escalate = false;
-                s_vb = group_sum<NP, double>(grp, vc * x[0], scr);
-                s_bb = group_sum<NP, double>(grp, b64 * x[0], scr);
-                if constexpr (ORDINARY)
-                {
-                    s_1b = group_sum<NP, double>(grp, one * x[0], scr);
-                    s_v1 = group_sum<NP, double>(grp, vc * x[1], scr);
-                    s_11 = group_sum<NP, double>(grp, one * x[1], scr);
-                }
-            }
-        }
-    }
-
-    if (escalate)
-    {
-        if (r == 0)
-        {
-            int slot = atomicAdd(P.esc_count, 1);
-            P.esc_cells[slot] = make_int2(my_cell, my_n);
-            if (P.out.status) P.out.status[my_cell] = 4;
-        }
-        grp.sync();
-        return;
-    }
-
-    // ---- estimate and variance from the forms
-    //   SK: est = mean + (v-m)^T A^-1 b,        var = C0 - b^T A^-1 b
-    //   OK: mu = (1^T A^-1 b - 1) / 1^T A^-1 1,  est = v^T A^-1 b - mu v^T A^-1 1,
-    //       var = C0 - b^T A^-1 b + mu 1^T A^-1 b - mu   (my_kriging_weights.h:312-357)
-    double est, var;
-    if constexpr (ORDINARY)
-    {
-        if (fabs(s_11) < 1e-15) fail = true;
-        const double mu = (s_1b - 1.0) / s_11;
-        est = s_vb - mu * s_v1;
-        var = P.c0 - s_bb + mu * s_1b - mu;
-    }
-    else
-    {
-        est = (double)(P.out.cell_mean ? P.out.cell_mean[my_cell] : P.mf) + s_vb;
-        var = P.c0 - s_bb;
-    }
-    if (var < 0) var = 0;
-    if (r == 0)
-    {
-        const SolveOut &out = P.out;
-        if (!fail)
-        {
-            if (out.write_cont)
-            {
-                out.out_data[my_cell] = (float)est;
-                out.out_mask[my_cell] = 1;
-            }
-            if (out.prob) out.prob[(long long)my_cell * out.prob_stride] = (float)est;
-            if (out.est64) out.est64[my_cell] = est;
-            if (out.var) out.var[my_cell] = var;
-            if (out.status) out.status[my_cell] = 0;
-        }
-        else if (out.status)
-            out.status[my_cell] = 2;
-    }
-    grp.sync();
-}
-
-// Work items are {cell, n}, listed in ascending cell order. Each block takes a
-// contiguous run of them and its groups interleave inside it, so the systems a
-// block has in flight belong to neighbouring cells, which share most of their
-// neighbour pairs: their pair-table gathers hit the same lines.
-struct WorkRun
-{
-    int first, end, stride;
-};
-__device__ __forceinline__ WorkRun work_run(int n_items, int groups_per_block, int gi)
-{
-    const int per_block = (n_items + gridDim.x - 1) / gridDim.x;
-    WorkRun w;
-    w.first = blockIdx.x * per_block + gi;
-    w.end = min(n_items, (blockIdx.x + 1) * per_block);
-    w.stride = groups_per_block;
-    return w;
-}
-
 // neighbour value centred on the (float) mean as combine() does (combiner.h:19-24)
 __device__ __forceinline__ double centred_value(bool live, float vraw, int ind_value, float mf)
 {
     float v = 0.0f;
     if (live) v = ind_value >= 0 ? (vraw == (float)ind_value ? 1.0f : 0.0f) : vraw;
     return live ? (double)(v - mf) : 0.0;
-}
-
-template <int NP>
-__device__ __forceinline__ Grp<NP> make_group(int gi)
-{
-    Grp<NP> grp;
-    grp.r = threadIdx.x % NP;
-    if constexpr (NP <= 32)
-    {
-        int lane0 = (threadIdx.x & 31) / NP * NP;
-        grp.mask = (NP == 32) ? 0xffffffffu : (((1u << NP) - 1u) << lane0);
-    }
-    else
-        grp.mask = 0xffffffffu;
-    grp.bar = 1 + gi;
-    return grp;
-}
-
-// One system per group of NP threads, thread r owning row r (the FP64 kernel
-// and FP32-refined systems of 33 to 64 neighbours).
-template <int NP, typename TF, bool ORDINARY, bool REFINE>
-__global__ void __launch_bounds__(256, 1)
-    k_solve(const Geom g, const int2 *__restrict__ cells, const int *__restrict__ n_items_ptr,
-            const int2 *__restrict__ nb_rec, int ind_value, const float *__restrict__ pair32, SolveParams P)
-{
-    constexpr int R = (ORDINARY ? 2 : 1) + 1;
-    typedef SolveSmem<NP, TF, REFINE, R> SM;
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int groups_per_block = blockDim.x / NP;
-    const int gi = threadIdx.x / NP;
-    const Grp<NP> grp = make_group<NP>(gi);
-    const int r = grp.r;
-    unsigned char *gb = smem + SM::bytes * gi;
-    GroupMem<NP, TF> gm;
-    gm.M = reinterpret_cast<TF *>(gb);
-    gm.LIN = reinterpret_cast<int *>(gb + SM::lin_off);
-    gm.X = reinterpret_cast<double *>(gb + SM::x_off);
-    gm.slots = reinterpret_cast<TF *>(gb + SM::slot_off);
-    gm.scr = reinterpret_cast<double *>(gb + SM::scr_off);
-    const long long pc = P.pc;
-
-    // The record of item i+1 and the work entry of item i+2 are loaded while
-    // item i is solved.
-    const WorkRun wr = work_run(*n_items_ptr, groups_per_block, gi);
-    const int stride = wr.stride, run_end = wr.end;
-    int item = wr.first;
-    int2 w_cur = item < run_end ? cells[item] : make_int2(0, 0);
-    int2 w_nxt = item + stride < run_end ? cells[item + stride] : make_int2(0, 0);
-    int2 rec = (item < run_end && r < w_cur.y) ? nb_rec[(long long)w_cur.x * g.k + r] : make_int2(0, 0);
-    for (; item < run_end; item += stride)
-    {
-        const int my_cell = w_cur.x, my_n = w_cur.y;
-        const int lin = rec.x;
-        const bool live = r < my_n;
-        const double vc = centred_value(live, __int_as_float(rec.y), ind_value, P.mf);
-        rec = (item + stride < run_end && r < w_nxt.y) ? nb_rec[(long long)w_nxt.x * g.k + r] : make_int2(0, 0);
-        w_cur = w_nxt;
-        w_nxt = item + 2 * stride < run_end ? cells[item + 2 * stride] : make_int2(0, 0);
-        gm.LIN[r] = live ? lin : 0;
-        grp.sync();
-
-        // ---- assembly (lower triangle of row r; padding rows are identity)
-        TF row[NP];
-#pragma unroll
-        for (int c = 0; c < NP; ++c)
-        {
-            TF a = (TF)0;
-            if (live && c <= r) a = pair_get<TF>(pair32, P.pair64, pc + lin - gm.LIN[c]);
-            if (!live && c == r) a = (TF)1;
-            row[c] = a;
-        }
-        const double b64 = live ? __ldg(P.pair64 + pc + lin) : 0.0;
-        solve_one<NP, TF, ORDINARY, REFINE>(grp, gm, P, row, b64, vc, live, lin, my_cell, my_n);
-    }
 }
 
 // ------------------------------------------------------------------ folded
@@ -668,7 +85,8 @@ __global__ void __launch_bounds__(256, 1)
 // shared-memory broadcast, the rsqrt and the synchronisation of a step serving
 // two rows. The arithmetic (right-looking Cholesky with the forward
 // substitution fused in, FP32 back substitution, dual-weighted FP64 residual
-// correction, classic refinement and FP64 escalation) is that of solve_one.
+// correction, classic refinement and FP64 escalation) is described at the top
+// of this file.
 //
 // M is stored packed: row j is read and written only from column 4*(j/4) on
 // (its first 16-byte chunk holding a column >= j) through the right-hand sides,
@@ -1643,11 +1061,8 @@ template <int NP, typename TF, bool ORD, bool REF>
 static cudaError_t launch_one(const Geom &g, const int2 *cells, const int *n_items, int max_items, const int2 *nb_rec,
                               int ind_value, const float *pair32, const SolveParams &P, int n_sm, cudaStream_t st)
 {
-    constexpr int threads = 256;
-    constexpr int gpb = threads / NP;
-    constexpr bool FOLD = REF;
     int blocks = 0;
-    if constexpr (FOLD)
+    if constexpr (REF)
     {
         constexpr int fthreads = fold_threads<NP>();
         constexpr int spb = fthreads / (NP / 2); // systems per block
@@ -1657,7 +1072,7 @@ static cudaError_t launch_one(const Geom &g, const int2 *cells, const int *n_ite
         if (e != cudaSuccess) return e;
         kern<<<(unsigned)blocks, fthreads, smem, st>>>(g, cells, n_items, nb_rec, ind_value, pair32, P);
     }
-    else if constexpr (!REF)
+    else
     {
         constexpr int fthreads = fold64_threads<NP>();
         constexpr int spb = fthreads / (NP / 2); // systems per block
@@ -1666,14 +1081,6 @@ static cudaError_t launch_one(const Geom &g, const int2 *cells, const int *n_ite
         cudaError_t e = launch_kernel(kern, fthreads, smem, max_items, spb, n_sm, blocks);
         if (e != cudaSuccess) return e;
         kern<<<(unsigned)blocks, fthreads, smem, st>>>(g, cells, n_items, nb_rec, ind_value, P);
-    }
-    else
-    {
-        const size_t smem = SolveSmem<NP, TF, REF, ORD ? 3 : 2>::bytes * gpb;
-        auto kern = k_solve<NP, TF, ORD, REF>;
-        cudaError_t e = launch_kernel(kern, threads, smem, max_items, gpb, n_sm, blocks);
-        if (e != cudaSuccess) return e;
-        kern<<<(unsigned)blocks, threads, smem, st>>>(g, cells, n_items, nb_rec, ind_value, pair32, P);
     }
     return cudaGetLastError();
 }
