@@ -300,7 +300,8 @@ cudaError_t launch_cok_solve(const Geom &g, const int *targets, int n_targets, c
         const int spb = kCokThreads / kFold32G;
         const size_t smem = kFold32SysBytes * spb;
         auto kern = k < 32 ? k_cok_solve_fold<true> : k_cok_solve_fold<false>;
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int per_sm = 0;
+        cudaError_t e = set_smem_min_carveout(kern, kCokThreads, smem, per_sm);
         if (e != cudaSuccess) return e;
         const int blocks = std::min((n_targets + spb - 1) / spb, n_sm);
         kern<<<blocks, kCokThreads, smem, st>>>(a);

@@ -63,4 +63,32 @@ __host__ __device__ __forceinline__ int pair_lin(const Geom &g, int dx, int dy, 
 {
     return (dz * g.pny + dy) * g.pnx + dx;
 }
+// Dynamic shared memory of `smem` bytes per block for `kern`, then the
+// smallest shared-memory carveout that holds the blocks an SM keeps resident
+// at that size (per_sm, returned): the rest of the SM's unified L1 / shared
+// storage stays L1 for the kernels' pair-table gathers.
+template <typename K>
+inline cudaError_t set_smem_min_carveout(K kern, int threads, size_t smem, int &per_sm)
+{
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    int dev = 0, smem_sm = 0, reserved = 0;
+    cudaFuncAttributes fa{};
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) == cudaSuccess &&
+        cudaFuncGetAttributes(&fa, kern) == cudaSuccess && smem_sm > 0)
+    {
+        const long long need = (long long)per_sm * ((long long)smem + (long long)fa.sharedSizeBytes + reserved);
+        int pct = (int)((need * 100 + smem_sm - 1) / smem_sm);
+        pct = pct < 1 ? 1 : (pct > 100 ? 100 : pct);
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
 } // namespace hb

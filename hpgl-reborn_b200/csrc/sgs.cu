@@ -1077,7 +1077,8 @@ cudaError_t launch_sis_level(const SisLevelArgs &a, int n_sm, cudaStream_t st)
     const size_t smem = kSisSysBytes * spb;
     auto kern = a.correlogram ? (a.kmax < 32 ? k_sis_level<true, true> : k_sis_level<true, false>)
                               : (a.kmax < 32 ? k_sis_level<false, true> : k_sis_level<false, false>);
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 0;
+    cudaError_t e = set_smem_min_carveout(kern, kSisFoldThreads, smem, per_sm);
     if (e != cudaSuccess) return e;
     const int blocks = std::min((n_sys + spb - 1) / spb, n_sm);
     kern<<<blocks, kSisFoldThreads, smem, st>>>(a);
@@ -1098,7 +1099,8 @@ cudaError_t launch_sgs_solve(const Geom &g, const int *order, int n_items, const
         const int blocks = std::min((n_items + kSgsFoldThreads / kSgsG - 1) / (kSgsFoldThreads / kSgsG), n_sm);
         auto kern = ordinary ? (k < 32 ? k_sgs_solve_fold<true, true> : k_sgs_solve_fold<true, false>)
                              : (k < 32 ? k_sgs_solve_fold<false, true> : k_sgs_solve_fold<false, false>);
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int per_sm = 0;
+        cudaError_t e = set_smem_min_carveout(kern, kSgsFoldThreads, smem, per_sm);
         if (e != cudaSuccess) return e;
         kern<<<blocks, kSgsFoldThreads, smem, st>>>(a);
     }

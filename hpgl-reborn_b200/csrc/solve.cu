@@ -1026,29 +1026,9 @@ __global__ void __launch_bounds__(fold64_threads<NP>(), 1)
 template <typename K>
 static cudaError_t launch_kernel(K kern, int threads, size_t smem, int max_items, int gpb, int n_sm, int &blocks_out)
 {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+    cudaError_t e = set_smem_min_carveout(kern, threads, smem, per_sm);
     if (e != cudaSuccess) return e;
-    if (per_sm < 1) per_sm = 1;
-    // The smallest shared-memory carveout that holds per_sm blocks: the rest of
-    // the SM's unified L1 / shared storage stays L1 for the pair-table gathers.
-    {
-        int dev = 0, smem_sm = 0, reserved = 0;
-        cudaFuncAttributes fa{};
-        if (cudaGetDevice(&dev) == cudaSuccess &&
-            cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) == cudaSuccess &&
-            cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) == cudaSuccess &&
-            cudaFuncGetAttributes(&fa, kern) == cudaSuccess && smem_sm > 0)
-        {
-            const long long need = (long long)per_sm * ((long long)smem + (long long)fa.sharedSizeBytes + reserved);
-            int pct = (int)((need * 100 + smem_sm - 1) / smem_sm);
-            pct = pct < 1 ? 1 : (pct > 100 ? 100 : pct);
-            e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
-            if (e != cudaSuccess) return e;
-        }
-    }
     long long want = ((long long)max_items + gpb - 1) / gpb;
     long long blocks = (long long)n_sm * per_sm;
     if (want < blocks) blocks = want;
