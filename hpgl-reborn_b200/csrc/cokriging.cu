@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(kCokThreads, 1) k_cok_solve_fold(const CokArgs
     const unsigned gm = 0xFFFFu << (h * G);
     unsigned char *gb = smem + kFold32SysBytes * (warp * 2 + h);
     double *M = reinterpret_cast<double *>(gb);
-    int *LIN = reinterpret_cast<int *>(gb + (size_t)NP * kFold32LD * 8);
+    int *LIN = reinterpret_cast<int *>(gb + kFold32MBytes);
     const Geom &g = a.g;
     const long long pc = g.pair_center;
     const int stride = gridDim.x * nwarps * 2;

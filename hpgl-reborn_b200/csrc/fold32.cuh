@@ -17,9 +17,42 @@ namespace hb
 {
 constexpr int kFold32NP = 32, kFold32G = 16;
 constexpr int kFold32LD = kFold32NP + 2; // 32 entries, then up to two right-hand sides
-// per system: M (32 x LD doubles), LIN (32 ints); systems sharing a warp 16 bytes
+
+// M is stored packed: row j is read and written only from column 2*(j/2) on
+// (its first 16-byte pair holding a column >= j), so it keeps LD - 2*(j/2)
+// doubles. Row j's column c sits at double row[j] + c; the rows follow one
+// another, each start moved forward until row[j] is even (16-byte pairs) and
+// its residue modulo 16 is used by at most one earlier row of its group of 16
+// (rows t and 31 - t of the lanes), so the back substitution's 8-byte column
+// reads keep the two-way bank conflicts of the square layout at 74% of its
+// footprint; the L1 cache gets what the shared memory gives up.
+struct Fold32Rows
+{
+    int row[kFold32NP];
+    int doubles;
+};
+constexpr Fold32Rows make_fold32_rows()
+{
+    Fold32Rows f{};
+    int end = 0;
+    int cnt[2][16] = {};
+    for (int j = 0; j < kFold32NP; ++j)
+    {
+        const int a = 2 * (j / 2), grp = j / 16;
+        int p = end;
+        while ((p - a) % 2 != 0 || cnt[grp][(p - a) % 16] >= 2) ++p;
+        cnt[grp][(p - a) % 16] += 1;
+        f.row[j] = p - a;
+        end = p + kFold32LD - a;
+    }
+    f.doubles = end;
+    return f;
+}
+__device__ constexpr Fold32Rows d_fold32_rows = make_fold32_rows();
+constexpr size_t kFold32MBytes = (size_t)make_fold32_rows().doubles * 8;
+// per system: packed M, then LIN (32 ints); systems sharing a warp 16 bytes
 // apart modulo 128 so that their broadcast rows fall on different banks
-constexpr size_t kFold32SysBytes = ((size_t)kFold32NP * kFold32LD * 8 + kFold32NP * 4 + 127) / 128 * 128 + 16;
+constexpr size_t kFold32SysBytes = (kFold32MBytes + kFold32NP * 4 + 127) / 128 * 128 + 16;
 
 // Solves A [x] = [rhs] for the lane's rows t and 31 - t (QB <= 2 right-hand
 // sides; rows of non-live unknowns carry zeros). `gm` is the system's lane
@@ -45,6 +78,7 @@ __device__ __forceinline__ bool fold32_solve(const double *pair_c, const int *LI
 {
     constexpr int NP = kFold32NP, G = kFold32G, LD = kFold32LD;
     const int rb = NP - 1 - t;
+    const int row_a = d_fold32_rows.row[t], row_b = d_fold32_rows.row[rb]; // the lane's rows in M
     // ---- assembly (lower triangles of rows t and 31 - t; padding rows identity)
     double ra[G], rbv[NP];
     const double *base_a = pair_c + lin_a, *base_b = pair_c + lin_b;
@@ -89,24 +123,26 @@ __device__ __forceinline__ bool fold32_solve(const double *pair_c, const int *LI
     for (int j = 0; j < NP; ++j)
     {
         if (j >= nmax) break;
+        // row j of the packed matrix holds columns 2*(j/2) on
+        double *Mj = M + d_fold32_rows.row[j];
         if (j < G)
         {
-            M[j * LD + t] = ra[j];
+            if (t >= (j & ~1)) Mj[t] = ra[j];
             if (t == j)
             {
 #pragma unroll
-                for (int q = 0; q < QB; ++q) M[j * LD + NP + q] = rhs_a[q];
+                for (int q = 0; q < QB; ++q) Mj[NP + q] = rhs_a[q];
             }
         }
-        M[j * LD + rb] = rbv[j];
+        if (rb >= (j & ~1)) Mj[rb] = rbv[j];
         if (j >= G && rb == j)
         {
 #pragma unroll
-            for (int q = 0; q < QB; ++q) M[j * LD + NP + q] = rhs_b[q];
+            for (int q = 0; q < QB; ++q) Mj[NP + q] = rhs_b[q];
         }
         __syncwarp(gm);
         double mj[LD];
-        const double2 *mv = reinterpret_cast<const double2 *>(M + j * LD);
+        const double2 *mv = reinterpret_cast<const double2 *>(Mj);
 #pragma unroll
         for (int q = j / 2; q < LD / 2; ++q)
         {
@@ -191,13 +227,13 @@ __device__ __forceinline__ bool fold32_solve(const double *pair_c, const int *LI
         }
         if (t < i)
         {
-            const double l = M[t * LD + i] * inv_a;
+            const double l = M[row_a + i] * inv_a;
 #pragma unroll
             for (int q = 0; q < QB; ++q) ya[q] -= l * xi[q];
         }
         if (rb < i)
         {
-            const double l = M[rb * LD + i] * inv_b;
+            const double l = M[row_b + i] * inv_b;
 #pragma unroll
             for (int q = 0; q < QB; ++q) yb[q] -= l * xi[q];
         }

@@ -451,41 +451,7 @@ constexpr int kSgsNP = kFold32NP, kSgsG = kFold32G;
 constexpr int kSgsLD = kFold32LD;
 constexpr int kSgsFoldThreads = 256;
 
-// M is stored packed: row j is read and written only from column 2*(j/2) on
-// (its first 16-byte pair holding a column >= j), so it keeps LD - 2*(j/2)
-// doubles. Row j's column c sits at double row[j] + c; the rows follow one
-// another, each start moved forward until row[j] is even (16-byte pairs) and
-// its residue modulo 16 is used by at most one earlier row of its group of 16
-// (rows t and 31 - t of the lanes), so the back substitution's 8-byte column
-// reads keep the two-way bank conflicts of the square layout at 74% of its
-// footprint.
-struct SgsRows
-{
-    int row[kSgsNP];
-    int doubles;
-};
-constexpr SgsRows make_sgs_rows()
-{
-    SgsRows f{};
-    int end = 0;
-    int cnt[2][16] = {};
-    for (int j = 0; j < kSgsNP; ++j)
-    {
-        const int a = 2 * (j / 2), grp = j / 16;
-        int p = end;
-        while ((p - a) % 2 != 0 || cnt[grp][(p - a) % 16] >= 2) ++p;
-        cnt[grp][(p - a) % 16] += 1;
-        f.row[j] = p - a;
-        end = p + kSgsLD - a;
-    }
-    f.doubles = end;
-    return f;
-}
-__device__ constexpr SgsRows d_sgs_rows = make_sgs_rows();
-constexpr size_t kSgsMBytes = (size_t)make_sgs_rows().doubles * 8;
-// per system: packed M, then LIN (32 ints); systems sharing a warp 16 bytes
-// apart modulo 128 so that their broadcast rows fall on different banks
-constexpr size_t kSgsSysBytes = (kSgsMBytes + kSgsNP * 4 + 127) / 128 * 128 + 16;
+constexpr size_t kSgsSysBytes = kFold32SysBytes;
 
 // BOUND (k < 32): the factorisation stops at the warp's largest system
 template <bool ORD, bool BOUND>
@@ -498,8 +464,8 @@ __global__ void __launch_bounds__(kSgsFoldThreads, 1) k_sgs_solve_fold(const Sgs
     const unsigned gm = 0xFFFFu << (h * G);
     unsigned char *gb = smem + kSgsSysBytes * (warp * 2 + h);
     double *M = reinterpret_cast<double *>(gb);
-    int *LIN = reinterpret_cast<int *>(gb + kSgsMBytes);
-    const int row_a = d_sgs_rows.row[t], row_b = d_sgs_rows.row[rb]; // the lane's rows in M
+    int *LIN = reinterpret_cast<int *>(gb + kFold32MBytes);
+    const int row_a = d_fold32_rows.row[t], row_b = d_fold32_rows.row[rb]; // the lane's rows in M
     const Geom &g = a.g;
     const long long pc = g.pair_center;
     const double *pair64 = a.pair64;
@@ -604,7 +570,7 @@ __global__ void __launch_bounds__(kSgsFoldThreads, 1) k_sgs_solve_fold(const Sgs
         {
             if (BOUND && j >= nmax) break;
             // row j of the packed matrix holds columns 2*(j/2) on
-            double *Mj = M + d_sgs_rows.row[j];
+            double *Mj = M + d_fold32_rows.row[j];
             if (j < G)
             {
                 if (t >= (j & ~1)) Mj[t] = ra[j];
@@ -949,7 +915,7 @@ __global__ void __launch_bounds__(kSisFoldThreads, 1) k_sis_level(const SisLevel
     const unsigned gm = 0xFFFFu << (h * G);
     unsigned char *gb = smem + kSisSysBytes * (warp * 2 + h);
     double *M = reinterpret_cast<double *>(gb);
-    int *LIN = reinterpret_cast<int *>(gb + (size_t)NP * kFold32LD * 8);
+    int *LIN = reinterpret_cast<int *>(gb + kFold32MBytes);
     double *SIG = reinterpret_cast<double *>(gb + kFold32SysBytes); // the system's row scales
     const int n_sys = a.n_nodes * a.kcat;
     const int stride = gridDim.x * nwarps * 2;
