@@ -823,9 +823,26 @@ int hpgl_b200_last_stats(double *out, int cap)
     v[39] = (double)s.sgs_levels;
     v[40] = s.draws_ms;
     v[41] = s.sgs_flops;
+    v[42] = (double)s.refined;
     int n = cap < HPGL_B200_STATS_LEN ? cap : HPGL_B200_STATS_LEN;
     for (int i = 0; i < n; ++i) out[i] = v[i];
     return n;
+}
+
+int hpgl_b200_solve_variant(int bucket_np, int cov_type, int precision, int variant)
+{
+    const int prev = hb::set_solve_variant(bucket_np, cov_type, precision, variant);
+    if (prev < 0)
+    {
+        hb::set_error("hpgl_b200_solve_variant: invalid key or variant");
+        return HPGL_B200_EINVAL;
+    }
+    return prev;
+}
+
+int hpgl_b200_solve_variant_get(int bucket_np, int cov_type, int precision)
+{
+    return hb::solve_variant(bucket_np, cov_type, precision);
 }
 
 void *hpgl_b200_host_alloc(size_t bytes) { return hb::host_alloc(bytes); }

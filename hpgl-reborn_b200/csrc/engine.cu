@@ -606,11 +606,24 @@ static void run_solves(Engine &E, const Plan &pl, const DevPoints &P, const DevS
     unsigned long long *tile_mom = E.buf<unsigned long long>("tile_mom", n_tiles * kBuckets * 3);
     int2 *cells = E.buf<int2>("cells", (size_t)g.n_cells);
     unsigned long long *moments = E.buf<unsigned long long>("moments", kBuckets * 3);
-    int *esc_cnt = E.buf<int>("esc_cnt", kBuckets);
+    // FP32-refined systems that fail the four-rows-per-lane kernel's check go
+    // first to the two-rows-per-lane kernel (classic refinement), and what
+    // that does not converge to the FP64 kernel
+    int *esc_cnt = E.buf<int>("esc_cnt", 2 * kBuckets);
+    int *ref_cnt = esc_cnt + kBuckets;
     int2 *esc_cells = precision ? E.buf<int2>("esc_cells", (size_t)g.n_cells) : nullptr;
+    int2 *ref_cells = nullptr;
+    int variant[kBuckets];
+    bool any_quad = false;
+    for (int b = 0; b < kBuckets; ++b)
+    {
+        variant[b] = b < 4 ? solve_variant(kBucketNP[b], pl.f.m.type, precision) : kVariantFold;
+        any_quad = any_quad || (precision && b < 4 && kBucketNP[b] <= 32 && variant[b] == kVariantQuad);
+    }
+    if (any_quad) ref_cells = E.buf<int2>("ref_cells", (size_t)g.n_cells);
     launch_prepare(g, d_mask, all_cells, S.nb_n, d_status, bucket_cnt, bucket_off, tile_cnt, tile_mom, cells, moments,
                    st);
-    HB_CK(cudaMemsetAsync(esc_cnt, 0, sizeof(int) * kBuckets, st));
+    HB_CK(cudaMemsetAsync(esc_cnt, 0, sizeof(int) * 2 * kBuckets, st));
     HB_CK(cudaGetLastError());
     E.stats.launches += 3;
     int cnt[kBuckets];
@@ -629,12 +642,14 @@ static void run_solves(Engine &E, const Plan &pl, const DevPoints &P, const DevS
         if (cnt[b] > 0)
         {
             const int2 *bcells = cells + off;
+            const bool quad = precision && b < 4 && kBucketNP[b] <= 32 && variant[b] == kVariantQuad;
             HB_CK(cudaEventRecord(E.ev_[10 + 2 * b], st));
             if (b < 4)
             {
-                HB_CK(launch_solve_bucket(kBucketNP[b], precision, ordinary, g, bcells, bucket_cnt + b, cnt[b],
-                                          S.nb_rec, S.nb_n, ind_value, S.pair64, S.pair32, mean, c0, steps, tol, out,
-                                          esc_cells ? esc_cells + off : nullptr, esc_cnt + b, E.n_sm(), st));
+                int2 *first_esc = quad ? ref_cells + off : (esc_cells ? esc_cells + off : nullptr);
+                HB_CK(launch_solve_bucket(kBucketNP[b], precision, variant[b], ordinary, g, bcells, bucket_cnt + b,
+                                          cnt[b], S.nb_rec, S.nb_n, ind_value, S.pair64, S.pair32, mean, c0, steps,
+                                          tol, out, first_esc, quad ? ref_cnt + b : esc_cnt + b, E.n_sm(), st));
             }
             else
             {
@@ -655,19 +670,33 @@ static void run_solves(Engine &E, const Plan &pl, const DevPoints &P, const DevS
     }
     if (precision)
     {
+        // classic refinement of what the four-rows-per-lane kernel queued
+        for (int b = 0; b < 4; ++b)
+        {
+            if (cnt[b] == 0 || !(kBucketNP[b] <= 32 && variant[b] == kVariantQuad)) continue;
+            HB_CK(launch_solve_bucket(kBucketNP[b], 1, kVariantFold, ordinary, g, ref_cells + esc_off[b], ref_cnt + b,
+                                      std::min(cnt[b], E.n_sm() * 8), S.nb_rec, S.nb_n, ind_value, S.pair64,
+                                      S.pair32, mean, c0, steps, tol, out, esc_cells + esc_off[b], esc_cnt + b,
+                                      E.n_sm(), st));
+            E.stats.launches += 1;
+        }
         // FP64 re-solve of escalated systems, one persistent launch per bucket
         for (int b = 0; b < 4; ++b)
         {
             if (cnt[b] == 0) continue;
-            HB_CK(launch_solve_bucket(kBucketNP[b], 0, ordinary, g, esc_cells + esc_off[b], esc_cnt + b,
-                                      std::min(cnt[b], E.n_sm() * 8), S.nb_rec, S.nb_n, ind_value, S.pair64,
-                                      S.pair32, mean, c0, 0, tol, out, nullptr, nullptr, E.n_sm(), st));
+            HB_CK(launch_solve_bucket(kBucketNP[b], 0, kVariantDefault, ordinary, g, esc_cells + esc_off[b],
+                                      esc_cnt + b, std::min(cnt[b], E.n_sm() * 8), S.nb_rec, S.nb_n, ind_value,
+                                      S.pair64, S.pair32, mean, c0, 0, tol, out, nullptr, nullptr, E.n_sm(), st));
             E.stats.launches += 1;
         }
-        int esc[kBuckets];
+        int esc[2 * kBuckets];
         HB_CK(cudaMemcpyAsync(esc, esc_cnt, sizeof(esc), cudaMemcpyDeviceToHost, st));
         HB_CK(cudaStreamSynchronize(st));
-        for (int b = 0; b < kBuckets; ++b) E.stats.escalated += esc[b];
+        for (int b = 0; b < kBuckets; ++b)
+        {
+            E.stats.escalated += esc[b];
+            E.stats.refined += esc[kBuckets + b];
+        }
     }
     else
         HB_CK(cudaStreamSynchronize(st));

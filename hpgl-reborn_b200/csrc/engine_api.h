@@ -102,6 +102,7 @@ struct Stats
     double total_ms = 0, search_ms = 0, solve_ms = 0, search_kernel_ms = 0;
     long long ties = 0, template_cells = 0, kriged = 0, launches = 0;
     long long h2d = 0, d2h = 0, escalated = 0;
+    long long refined = 0; // FP32 systems the four-rows-per-lane check passed on to classic refinement
     long long bucket_items[5] = {0, 0, 0, 0, 0};
     double bucket_ms[5] = {0, 0, 0, 0, 0};
     double bucket_flops[5] = {0, 0, 0, 0, 0};
@@ -117,6 +118,11 @@ void set_error(const std::string &msg);
 const char *last_error();
 void set_threads(int n);
 int get_threads();
+// the solve-kernel tuning table (tune.cpp): the variant a (bucket, covariance
+// type, precision) key runs, and an override returning the previous setting
+// (-1 for an invalid key or variant)
+int solve_variant(int np, int cov_type, int precision);
+int set_solve_variant(int np, int cov_type, int precision, int variant);
 
 // kind 0 OK, 1 SK, 2 LVM (SK weights around the per-cell `means`, which kind 2
 // requires; lvm_kriging.cpp:16-39)

@@ -100,7 +100,24 @@ cudaError_t launch_resolve_ties_fast(const Geom &g, const int *tie_cells, const 
                                      int cap, int *nb_pid, int2 *nb_rec, int n_sm, cudaStream_t st);
 
 // solves (solve.cu, misc.cu)
-cudaError_t launch_solve_bucket(int np, int precision, bool ordinary, const Geom &g, const int2 *cells,
+// Solve-kernel variants (the launch shapes the tuning table chooses between,
+// tune.cpp). FP32-refined, n <= 32: kVariantQuad (four rows per lane,
+// solve_quad.cu) or kVariantFold (two rows per lane with in-kernel classic
+// refinement, solve.cu); n 33-64 and FP64 have one variant each.
+enum SolveVariant : int
+{
+    kVariantDefault = 0,
+    kVariantFold = 1,
+    kVariantQuad = 2,
+};
+constexpr int kVariantCount = 3;
+// the variant that runs for a (bucket, covariance type, precision) key
+int solve_variant(int np, int cov_type, int precision);
+// whether `variant` can run the key (kVariantDefault always can)
+bool solve_variant_valid(int np, int precision, int variant);
+// overrides one key; returns its previous setting, or -1 for an invalid key or variant
+int set_solve_variant(int np, int cov_type, int precision, int variant);
+cudaError_t launch_solve_bucket(int np, int precision, int variant, bool ordinary, const Geom &g, const int2 *cells,
                                 const int *n_items, int max_items, const int2 *nb_rec, const int *nb_n, int ind_value,
                                 const double *pair64, const float *pair32, double mean, double c0, int steps,
                                 double tol, const SolveOut &out, int2 *esc_cells, int *esc_count, int n_sm,

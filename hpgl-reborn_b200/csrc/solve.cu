@@ -49,32 +49,12 @@
 //                  reported singular.
 #include "engine.cuh"
 #include "kernels.h"
+#include "solve_common.cuh"
 
 #include <cstdint>
 
 namespace hb
 {
-struct SolveParams
-{
-    const double *pair64;
-    long long pc;
-    float mf;
-    double c0;
-    int steps;
-    double tol;
-    SolveOut out;
-    int2 *esc_cells;
-    int *esc_count;
-};
-
-// neighbour value centred on the (float) mean as combine() does (combiner.h:19-24)
-__device__ __forceinline__ double centred_value(bool live, float vraw, int ind_value, float mf)
-{
-    float v = 0.0f;
-    if (live) v = ind_value >= 0 ? (vraw == (float)ind_value ? 1.0f : 0.0f) : vraw;
-    return live ? (double)(v - mf) : 0.0;
-}
-
 // ------------------------------------------------------------------ folded
 // FP32-refined systems of up to 64 neighbours, folded: a system is solved by
 // G = NP / 2 lanes and lane t owns rows t ("row a", columns 0..t) and
@@ -1023,20 +1003,6 @@ __global__ void __launch_bounds__(fold64_threads<NP>(), 1)
     }
 }
 
-template <typename K>
-static cudaError_t launch_kernel(K kern, int threads, size_t smem, int max_items, int gpb, int n_sm, int &blocks_out)
-{
-    int per_sm = 0;
-    cudaError_t e = set_smem_min_carveout(kern, threads, smem, per_sm);
-    if (e != cudaSuccess) return e;
-    long long want = ((long long)max_items + gpb - 1) / gpb;
-    long long blocks = (long long)n_sm * per_sm;
-    if (want < blocks) blocks = want;
-    if (blocks < 1) blocks = 1;
-    blocks_out = (int)blocks;
-    return cudaSuccess;
-}
-
 template <int NP, typename TF, bool ORD, bool REF>
 static cudaError_t launch_one(const Geom &g, const int2 *cells, const int *n_items, int max_items, const int2 *nb_rec,
                               int ind_value, const float *pair32, const SolveParams &P, int n_sm, cudaStream_t st)
@@ -1066,18 +1032,29 @@ static cudaError_t launch_one(const Geom &g, const int2 *cells, const int *n_ite
 }
 
 template <int NP>
-static cudaError_t launch_np(int precision, bool ordinary, const Geom &g, const int2 *cells, const int *n_items,
-                             int max_items, const int2 *nb_rec, int ind_value, const float *pair32,
+static cudaError_t launch_np(int precision, int variant, bool ordinary, const Geom &g, const int2 *cells,
+                             const int *n_items, int max_items, const int2 *nb_rec, int ind_value, const float *pair32,
                              const SolveParams &P, int n_sm, cudaStream_t st)
 {
 #define HB_ARGS g, cells, n_items, max_items, nb_rec, ind_value, pair32, P, n_sm, st
     if (precision == 0)
         return ordinary ? launch_one<NP, double, true, false>(HB_ARGS) : launch_one<NP, double, false, false>(HB_ARGS);
+    if constexpr (NP <= 32)
+    {
+        if (variant != kVariantFold) return launch_solve_quad(NP, ordinary, HB_ARGS);
+    }
     return ordinary ? launch_one<NP, float, true, true>(HB_ARGS) : launch_one<NP, float, false, true>(HB_ARGS);
 #undef HB_ARGS
 }
 
-cudaError_t launch_solve_bucket(int np, int precision, bool ordinary, const Geom &g, const int2 *cells,
+bool solve_variant_valid(int np, int precision, int variant)
+{
+    if (variant == kVariantDefault) return true;
+    if (precision == 1 && np <= 32) return variant == kVariantFold || variant == kVariantQuad;
+    return variant == kVariantFold;
+}
+
+cudaError_t launch_solve_bucket(int np, int precision, int variant, bool ordinary, const Geom &g, const int2 *cells,
                                 const int *n_items, int max_items, const int2 *nb_rec, const int *nb_n, int ind_value,
                                 const double *pair64, const float *pair32, double mean, double c0, int steps,
                                 double tol, const SolveOut &out, int2 *esc_cells, int *esc_count, int n_sm,
@@ -1094,18 +1071,20 @@ cudaError_t launch_solve_bucket(int np, int precision, bool ordinary, const Geom
     P.out = out;
     P.esc_cells = esc_cells;
     P.esc_count = esc_count;
+#define HB_NARGS precision, variant, ordinary, g, cells, n_items, max_items, nb_rec, ind_value, pair32, P, n_sm, st
     switch (np)
     {
     case 8:
-        return launch_np<8>(precision, ordinary, g, cells, n_items, max_items, nb_rec, ind_value, pair32, P, n_sm, st);
+        return launch_np<8>(HB_NARGS);
     case 16:
-        return launch_np<16>(precision, ordinary, g, cells, n_items, max_items, nb_rec, ind_value, pair32, P, n_sm, st);
+        return launch_np<16>(HB_NARGS);
     case 32:
-        return launch_np<32>(precision, ordinary, g, cells, n_items, max_items, nb_rec, ind_value, pair32, P, n_sm, st);
+        return launch_np<32>(HB_NARGS);
     case 64:
-        return launch_np<64>(precision, ordinary, g, cells, n_items, max_items, nb_rec, ind_value, pair32, P, n_sm, st);
+        return launch_np<64>(HB_NARGS);
     default:
         return cudaErrorInvalidValue;
     }
+#undef HB_NARGS
 }
 } // namespace hb

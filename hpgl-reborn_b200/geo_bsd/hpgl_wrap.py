@@ -138,6 +138,7 @@ EXPORTS = [
     "hpgl_b200_find_neighbours", "hpgl_b200_last_stats", "hpgl_b200_host_alloc", "hpgl_b200_host_free",
     "hpgl_b200_transform", "hpgl_b200_template", "hpgl_b200_covariance", "hpgl_b200_version",
     "hpgl_b200_sk_weights_noalloc", "hpgl_b200_loo_ok", "hpgl_b200_loo_ok_adjoint",
+    "hpgl_b200_solve_variant", "hpgl_b200_solve_variant_get",
 ]
 
 
@@ -244,6 +245,10 @@ def _load():
                                               vp]
     lib.hpgl_b200_last_stats.restype = C.c_int
     lib.hpgl_b200_last_stats.argtypes = [C.POINTER(C.c_double), C.c_int]
+    lib.hpgl_b200_solve_variant.restype = C.c_int
+    lib.hpgl_b200_solve_variant.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int]
+    lib.hpgl_b200_solve_variant_get.restype = C.c_int
+    lib.hpgl_b200_solve_variant_get.argtypes = [C.c_int, C.c_int, C.c_int]
     lib.hpgl_b200_host_alloc.restype = C.c_void_p
     lib.hpgl_b200_host_alloc.argtypes = [C.c_size_t]
     lib.hpgl_b200_host_free.restype = None
@@ -288,7 +293,23 @@ STATS_KEYS = (["total_ms", "search_ms", "solve_ms", "tie_cells", "template_cells
               + ["stage_" + s + "_ms" for s in ("upload", "compact", "tables", "bins", "search", "ties", "prepare",
                                               "solve", "finalize", "download")]
               + ["prefilter_exact_cells", "prefilter_active", "plan_ms", "sgs_levels", "sgs_draws_ms",
-                 "sgs_flops"])
+                 "sgs_flops", "refined_cells"])
+
+
+VARIANT_DEFAULT, VARIANT_FOLD, VARIANT_QUAD = 0, 1, 2
+
+
+def solve_variant(bucket_np: int, cov_type: int, precision: int, variant: int = None) -> int:
+    """The solve-kernel variant of one (bucket, covariance type, precision) key
+    (hpgl_b200_solve_variant_get); with `variant`, set it and return the
+    previous setting (hpgl_b200_solve_variant)."""
+    if variant is None:
+        return int(_hpgl_so.hpgl_b200_solve_variant_get(bucket_np, cov_type, precision))
+    prev = int(_hpgl_so.hpgl_b200_solve_variant(bucket_np, cov_type, precision, variant))
+    if prev < 0:
+        raise ValueError(f"invalid solve variant {variant} for bucket {bucket_np}, cov type {cov_type}, "
+                         f"precision {precision}")
+    return prev
 
 
 def last_stats() -> dict:

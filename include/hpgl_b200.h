@@ -307,9 +307,32 @@ int hpgl_b200_find_neighbours(int kind, const int *dims, const unsigned char *ma
  *   [38] host ms building the covariance tables (overlapped with the upload)
  *   [39] simulation: dependency levels (one solve launch each)
  *   [40] simulation: host ms generating the uniform draws (overlapped)
- *   [41] simulation: algorithmic flops of its kriging solves */
-#define HPGL_B200_STATS_LEN 42
+ *   [41] simulation: algorithmic flops of its kriging solves
+ *   [42] FP32_REFINED systems whose first-order check failed in the
+ *        four-rows-per-lane kernel and went to classic refinement */
+#define HPGL_B200_STATS_LEN 43
 int hpgl_b200_last_stats(double *out, int cap);
+
+/* Solve-kernel variants (no counterpart in the reference: HPGL makes one
+ * LAPACK call per node). Each (bucket, covariance type, precision) key runs
+ * one launch shape: bucket_np 8, 16, 32 or 64 (neighbour counts up to it),
+ * cov_type 0 spherical / 1 exponential / 2 Gaussian, precision
+ * HPGL_B200_FP64_PLAIN or HPGL_B200_FP32_REFINED. Variants:
+ *   HPGL_B200_VARIANT_DEFAULT  the built-in pick of the key
+ *   HPGL_B200_VARIANT_FOLD     two rows per lane (FP32: 512-thread blocks,
+ *                              classic refinement in the kernel)
+ *   HPGL_B200_VARIANT_QUAD     FP32_REFINED, bucket_np <= 32: four rows per
+ *                              lane, 384-thread blocks; failing systems go on
+ *                              to FOLD's refinement, then to FP64
+ * hpgl_b200_solve_variant sets a key and returns its previous setting, or
+ * HPGL_B200_EINVAL for an invalid key or a variant the key cannot run;
+ * hpgl_b200_solve_variant_get returns the variant a key runs now. Results of
+ * every variant meet the precision's error bound; they differ in rounding. */
+#define HPGL_B200_VARIANT_DEFAULT 0
+#define HPGL_B200_VARIANT_FOLD 1
+#define HPGL_B200_VARIANT_QUAD 2
+int hpgl_b200_solve_variant(int bucket_np, int cov_type, int precision, int variant);
+int hpgl_b200_solve_variant_get(int bucket_np, int cov_type, int precision);
 
 /* No counterpart in the reference. The same SK weights as
  * hpgl_simple_kriging_weights for callers that cannot allocate device memory
@@ -320,7 +343,11 @@ int hpgl_b200_last_stats(double *out, int cap);
  * (HPGL_B200_ELIMIT beyond). Calls share the array: calls that overlap on the
  * GPU race and must be serialised by the caller. The first call on a device
  * looks the array's address up (cudaGetSymbolAddress); make it before any
- * stream capture. Host pointers; `stream` may be NULL (the legacy stream).
+ * stream capture. With lazy module loading (CUDA's default) that first call
+ * is also when the device takes the array's memory, so it can fail on a full
+ * device: make it before reserving a memory pool; later calls allocate
+ * nothing. The call waits on `stream` for its own work before it returns.
+ * Host pointers; `stream` may be NULL (the legacy stream).
  * Returns 0, or a negative HPGL_B200_E* code with the message kept for
  * hpgl_get_last_exception_message. */
 int hpgl_b200_sk_weights_noalloc(const float *center_coords, const float *neighbours_x, const float *neighbours_y,
