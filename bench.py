@@ -74,20 +74,96 @@ def dist_env():
     return rank, world, local
 
 
+def workloads_module():
+    """geo_bsd/workloads.py loaded by file path: the seeded generators without
+    importing the geo_bsd package (whose import loads the engine library), so
+    the reference arm never maps the product library."""
+    name = "hb_bench_workloads"
+    if name in sys.modules:
+        return sys.modules[name]
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, "hpgl-reborn_b200", "geo_bsd",
+                                                                     "workloads.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def load_workload(name):
-    from geo_bsd import workloads as WL
-    return WL.ALL[name](1.0)
+    return workloads_module().ALL[name](1.0)
 
 
 def lvm_means(wl):
-    from geo_bsd import workloads as WL
-    return WL.lvm_means(wl.dims)
+    return workloads_module().lvm_means(wl.dims)
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 KIND_NAMES = {"ok": "ordinary kriging", "sk": "simple kriging", "lvm": "LVM kriging (smooth trend mean)"}
 
 
 # ---------------------------------------------------------------- CPU baseline
+def z_slab(wl, z0, nz):
+    """Layers z0 .. z0+nz-1 of a workload as a grid of their own (the slab's
+    own conditioning cells; x fastest, so a slab is a contiguous range)."""
+    nx, ny, _ = wl.dims
+    a, b = nx * ny * z0, nx * ny * (z0 + nz)
+    return (nx, ny, nz), np.ascontiguousarray(wl.data[a:b]), np.ascontiguousarray(wl.mask[a:b])
+
+
+def ref_api_slab(wl, kind, nz, threads):
+    """One whole call of the reference library's own public entry point
+    (hpgl_ordinary_kriging / hpgl_simple_kriging from oracle/_ref/libhpgl.so,
+    built from the reference's sources: the call geo.ordinary_kriging /
+    simple_kriging make), lookup construction included, on the middle nz
+    layers of the workload at `threads` OpenMP threads. Returns (kriged
+    cells/s, info)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    z0 = max(0, wl.dims[2] // 2 - nz // 2)
+    dims, data, mask = z_slab(wl, z0, nz)
+    t0 = time.perf_counter()
+    _, om = O.ref_cont_api(0 if kind == "ok" else 1, dims, data, mask, wl.cov, wl.radiuses, wl.max_neighbours,
+                           threads=threads)
+    dt = time.perf_counter() - t0
+    kriged = int(((om == 1) & (mask == 0)).sum())
+    return kriged / dt, {"slab": f"layers {z0}..{z0 + nz - 1} of z as a {dims[0]}x{dims[1]}x{nz} grid",
+                         "kriged_cells": kriged, "seconds": dt, "threads": threads}
+
+
+def slab_layers(wl, kind, target_seconds, threads):
+    """Layers of a slab that one reference call finishes in about
+    `target_seconds` (from a 2-layer probe)."""
+    rate, _ = ref_api_slab(wl, kind, 2, threads)
+    per_layer = wl.dims[0] * wl.dims[1]
+    return int(max(2, min(wl.dims[2], round(rate * target_seconds / per_layer))))
+
+
+def cpu_baseline_api(wl, kind, target_seconds):
+    """cpu_baseline of the reference library's own entry point: all host
+    threads on a slab of about `target_seconds`, and one thread on 2 layers."""
+    threads = os.cpu_count() or 1
+    nz = slab_layers(wl, kind, target_seconds, threads)
+    v, info = ref_api_slab(wl, kind, nz, threads)
+    v1, info1 = ref_api_slab(wl, kind, 2, 1)
+    return {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"one whole hpgl_{'ordinary' if kind == 'ok' else 'simple'}_kriging call of the reference "
+                      f"library ({info['slab']}, {info['kriged_cells']} kriged cells, {info['seconds']:.2f} s, "
+                      f"lookup construction included)",
+            "value_1_thread": v1, "sample_1_thread": f"{info1['slab']}, {info1['seconds']:.2f} s",
+            "cpu_model": cpu_model()}
+
+
 def cpu_reference(wl, kind, target_seconds, threads):
     """Reference CPU path (oracle/_ref, the reference's own code) on a sample of
     uninformed cells; falls back to the CPU restatement if the reference build
@@ -194,7 +270,7 @@ SGS_SEED = 42
 
 
 def sgs_workload(scale):
-    from geo_bsd import workloads as WL
+    WL = workloads_module()
     wl = WL.sk_ok_large(scale)
     cov = WL.CovSpec(wl.cov.cov_type, wl.cov.ranges, wl.cov.angles, 1.0, wl.cov.nugget / wl.cov.sill)
     return wl, cov
@@ -390,7 +466,7 @@ SIS_SEED = 42
 
 
 def sis_workload(scale):
-    from geo_bsd import workloads as WL
+    WL = workloads_module()
     wl = WL.indicator(scale)
     data = np.where(wl.mask == 1, wl.data, 0).astype(np.uint8)
     return wl, data
@@ -594,7 +670,7 @@ COK_METRIC = "cokriged cells/s, 1 B200: simple collocated cokriging, Markov mode
 def cok_workload(scale):
     """The kriging grid's generator with a secondary field: 0.6 x the primary
     values plus seeded N(0,1) noise, informed on half of the cells."""
-    from geo_bsd import workloads as WL
+    WL = workloads_module()
     wl = WL.sk_ok_large(scale)
     rng = np.random.default_rng(4)
     sdata = (0.6 * np.where(wl.mask == 1, wl.data, 0) + rng.normal(size=wl.n_cells)).astype(np.float32)
@@ -780,24 +856,41 @@ def main():
     import torch
 
     if args.impl == "reference":
+        # The reference's own CPU implementation (no GPU, none of this
+        # repository's engine: the package is not imported). ok / sk: each
+        # step is one whole call of the reference library's public entry point
+        # on a z-slab of the workload; lvm: its per-node code on sampled cells.
         if rank == 0:
             wl = load_workload(args.workload)
             threads = os.cpu_count() or 1
-            vals = []
-            info = None
-            for i in range(args.warmup + args.steps):
-                v, info = cpu_reference(wl, args.kind, min(args.cpu_seconds, 8.0), threads)
-                if i >= args.warmup:
-                    vals.append(v)
+            vals, info = [], None
+            if args.kind in ("ok", "sk"):
+                nz = slab_layers(wl, args.kind, 3.0, threads)
+                for i in range(args.warmup + args.steps):
+                    v, info = ref_api_slab(wl, args.kind, nz, threads)
+                    if i >= args.warmup:
+                        vals.append(v)
+                sample = (f"one whole hpgl_{'ordinary' if args.kind == 'ok' else 'simple'}_kriging call of the "
+                          f"reference library per step ({info['slab']}, {info['kriged_cells']} kriged cells, lookup "
+                          f"construction included)")
+                v1, info1 = ref_api_slab(wl, args.kind, 2, 1)
+                extra = {"value_1_thread": v1, "sample_1_thread": f"{info1['slab']}, {info1['seconds']:.2f} s"}
+            else:
+                for i in range(args.warmup + args.steps):
+                    v, info = cpu_reference(wl, args.kind, min(args.cpu_seconds, 8.0), threads)
+                    if i >= args.warmup:
+                        vals.append(v)
+                sample = f"{info['sample_cells']} random uninformed cells per step, lookup built once"
+                extra = {}
             value = float(np.median(vals))
+            d = wl.dims
             line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
                     "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
                     "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, geo_bsd.workloads)",
-                    "config": {"workload": f"{args.workload} {args.kind.upper()} (256x256x128, k=32)",
-                               "sample": f"{info['sample_cells']} random uninformed cells per step"},
-                    "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
-                                     "kind": "reference" if info["which"] == "ref" else "port",
-                                     "sample": f"{info['sample_cells']} random uninformed cells, lookup built once"},
+                    "config": {"workload": f"{KIND_NAMES[args.kind]} {d[0]}x{d[1]}x{d[2]}, k={wl.max_neighbours}",
+                               "sample": sample},
+                    "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                                     "sample": sample, "cpu_model": cpu_model(), **extra},
                     "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
             print(json.dumps(line), flush=True)
         return
@@ -813,7 +906,7 @@ def main():
     from geo_bsd import hpgl_wrap as W
 
     if args.profile_case > 0:
-        from geo_bsd import workloads as WL
+        WL = workloads_module()
         wl = WL.ALL[args.workload](args.profile_case)
     else:
         wl = load_workload(args.workload)
@@ -968,13 +1061,16 @@ def main():
         lib.hpgl_b200_host_free(ptr)
 
     cpu = None
-    if rank == 0 and not args.skip_cpu_baseline:
-        threads = os.cpu_count() or 1
-        v, info = cpu_reference(wl, args.kind, args.cpu_seconds, threads)
-        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "reference" if info["which"] == "ref" else "port",
-               "sample": f"{info['sample_cells']} random uninformed cells of the same grid; the reference's own "
-                         f"per-node code (kriging_interpolation) over OpenMP, lookup construction excluded "
-                         f"({info['setup_seconds']:.2f}s)"}
+    if rank == 0 and world == 1 and not args.skip_cpu_baseline:
+        if args.kind in ("ok", "sk"):
+            cpu = cpu_baseline_api(wl, args.kind, args.cpu_seconds)
+        else:
+            threads = os.cpu_count() or 1
+            v, info = cpu_reference(wl, args.kind, args.cpu_seconds, threads)
+            cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "reference" if info["which"] == "ref" else "port",
+                   "sample": f"{info['sample_cells']} random uninformed cells of the same grid; the reference's own "
+                             f"per-node code (kriging_interpolation) over OpenMP, lookup construction excluded "
+                             f"({info['setup_seconds']:.2f}s)", "cpu_model": cpu_model()}
 
     if rank == 0:
         line = {

@@ -323,6 +323,43 @@ def ref_api():
     return lib
 
 
+class _OkP(C.Structure):
+    _fields_ = [("t", C.c_int), ("r", C.c_double * 3), ("a", C.c_double * 3), ("sill", C.c_double),
+                ("nugget", C.c_double), ("rad", C.c_int * 3), ("k", C.c_int)]
+
+
+class _SkP(C.Structure):
+    _fields_ = _OkP._fields_ + [("auto", C.c_ubyte), ("mean", C.c_double)]
+
+
+def ref_cont_api(kind, dims, data, mask, cov, radiuses, k, mean=None, threads=0):
+    """The reference library's public kriging entry points on copies of
+    data/mask: hpgl_ordinary_kriging (kind 0, api.cpp:253-293) or
+    hpgl_simple_kriging (kind 1, automatic mean when `mean` is None,
+    api.cpp:323-354), the whole call as geo.ordinary_kriging / simple_kriging
+    make it (neighbour lookup construction, per-node kriging under OpenMP).
+    `threads` > 0 sets the reference's thread count first (hpgl_set_thread_num).
+    Returns (out_data, out_mask)."""
+    lib = ref_api()
+    if threads > 0:
+        lib.hpgl_set_thread_num(int(threads))
+    data = _arr(data, np.float32)
+    mask = _arr(mask, np.uint8)
+    od, om = data.copy(), mask.copy()
+    sh = _Shape((C.c_int * 3)(*dims), (C.c_int * 3)(1, dims[0], dims[0] * dims[1]))
+    base = (int(cov.cov_type), (C.c_double * 3)(*cov.ranges), (C.c_double * 3)(*cov.angles), float(cov.sill),
+            float(cov.nugget), (C.c_int * 3)(*[int(r) for r in radiuses]), int(k))
+    if kind == 0:
+        a = _Cont(data.ctypes.data_as(_f), mask.ctypes.data_as(_u8), sh)
+        b = _Cont(od.ctypes.data_as(_f), om.ctypes.data_as(_u8), sh)
+        lib.hpgl_ordinary_kriging(C.byref(a), C.byref(_OkP(*base)), C.byref(b))
+    else:
+        p = _SkP(*base, 1 if mean is None else 0, 0.0 if mean is None else float(mean))
+        lib.hpgl_simple_kriging(data.ctypes.data_as(_f), mask.ctypes.data_as(_u8), C.byref(sh), C.byref(p),
+                                od.ctypes.data_as(_f), om.ctypes.data_as(_u8), C.byref(sh))
+    return od, om
+
+
 def ref_sgs(dims, data, mask, cov, radiuses, k, seed, kind=1):
     """The reference's hpgl_sgs_simulation on copies of data/mask (no CDF, no
     simulation mask); `cov` holds the sill and nugget the driver receives."""
