@@ -3,6 +3,7 @@
 // neighbour counts above 64.
 #include "engine.cuh"
 #include "kernels.h"
+#include "sk_single.cuh"
 
 #include <cstdint>
 
@@ -544,75 +545,12 @@ cudaError_t launch_solve_large(const Geom &g, const int2 *cells, const int *n_it
 namespace hb
 {
 // ------------------------------------------------------------- single system
-// SK weights for arbitrary real coordinates with the analytic model
-// (simple_kriging.cpp:67-87 via sk_kriging_weights_3 on real_location_t):
-// one CTA, matrix in global memory, FP64. status[0] = 1 on success.
-__device__ double cov_real_dev(const DevModel &m, double v0, double v1, double v2)
-{
-    double acc = 0.0;
-    for (int i = 0; i < 3; ++i)
-    {
-        double d = 0.0;
-        d = __dadd_rn(d, __dmul_rn(v0, m.T[3 * i + 0]));
-        d = __dadd_rn(d, __dmul_rn(v1, m.T[3 * i + 1]));
-        d = __dadd_rn(d, __dmul_rn(v2, m.T[3 * i + 2]));
-        acc = __dadd_rn(acc, __dmul_rn(d, d));
-    }
-    double h = sqrt(acc);
-    if (h < 0.0001) return m.sill;
-    double u = h / m.r0;
-    if (m.type == 2) return (m.sill - m.nugget) * exp(-3.0 * (u * u));
-    if (m.type == 1) return (m.sill - m.nugget) * exp((-3.0 * h) / m.r0);
-    if (h > m.r0) return 0.0;
-    return (m.sill - m.nugget) * (1.0 - (1.5 * h) / m.r0 + 0.5 * (u * u * u));
-}
-
+// SK weights for arbitrary real coordinates (sk_single.cuh); status[0] = 1 on success.
 __global__ void k_sk_weights(DevModel m, const double *__restrict__ pts, int n, double *__restrict__ A,
                              double *__restrict__ w, int *__restrict__ status)
 {
-    const double cx = pts[0], cy = pts[1], cz = pts[2];
-    const double *xs = pts + 3, *ys = xs + n, *zs = ys + n;
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x)
-    {
-        int i = e / n, j = e % n;
-        A[e] = cov_real_dev(m, xs[i] - xs[j], ys[i] - ys[j], zs[i] - zs[j]);
-    }
-    for (int i = threadIdx.x; i < n; i += blockDim.x) w[i] = cov_real_dev(m, xs[i] - cx, ys[i] - cy, zs[i] - cz);
-    __syncthreads();
-    bool fail = false;
-    for (int j = 0; j < n; ++j)
-    {
-        double d = A[(size_t)j * n + j];
-        if (!(d > 0.0)) fail = true;
-        double ljj = sqrt(d);
-        __syncthreads();
-        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) A[(size_t)i * n + j] /= ljj;
-        if (threadIdx.x == 0) A[(size_t)j * n + j] = ljj;
-        __syncthreads();
-        int span = n - j - 1;
-        for (int e = threadIdx.x; e < span * span; e += blockDim.x)
-        {
-            int i = j + 1 + e / span, c = j + 1 + e % span;
-            if (c <= i) A[(size_t)i * n + c] -= A[(size_t)i * n + j] * A[(size_t)c * n + j];
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0)
-    {
-        for (int i = 0; i < n; ++i)
-        {
-            double s = w[i];
-            for (int c = 0; c < i; ++c) s -= A[(size_t)i * n + c] * w[c];
-            w[i] = s / A[(size_t)i * n + i];
-        }
-        for (int i = n - 1; i >= 0; --i)
-        {
-            double s = w[i];
-            for (int c = i + 1; c < n; ++c) s -= A[(size_t)c * n + i] * w[c];
-            w[i] = s / A[(size_t)i * n + i];
-        }
-        status[0] = fail ? 0 : 1;
-    }
+    const bool fail = sk_single_solve(m, pts, n, A, w);
+    if (threadIdx.x == 0) status[0] = fail ? 0 : 1;
 }
 
 void launch_sk_weights(const DevModel &m, const double *pts, int n, double *A, double *w, int *status,

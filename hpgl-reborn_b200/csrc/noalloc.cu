@@ -20,10 +20,19 @@
 //     between calls;
 //   * the first call on a device looks the array's device address up
 //     (cudaGetSymbolAddress) with that device current and caches it; make that
-//     first call before any stream capture.
+//     first call before any stream capture;
+//   * with lazy module loading (CUDA's default since 12.2) the device holds
+//     the array only from the moment this file's device code is loaded onto
+//     it, which the first call's set-up forces (cudaFuncGetAttributes on the
+//     kernel). That first call can therefore allocate the array's memory and
+//     fail when the device is already full: make it before the caller reserves
+//     its memory pool. Later calls allocate nothing;
+//   * the call waits on `stream` for its own copies and kernel before it
+//     returns the weights.
 #include "../../include/hpgl_b200.h"
 #include "engine_api.h"
 #include "host_model.h"
+#include "sk_single.cuh"
 
 #include <cuda_runtime.h>
 
@@ -37,99 +46,34 @@ constexpr int kMaxDevices = 64;
 // layout in doubles: centre (3) | x, y, z (3 n) | A (n n) | w (n) | status (1)
 constexpr size_t kScratchDoubles = 3 + 3 * kNoAllocMaxN + (size_t)kNoAllocMaxN * kNoAllocMaxN + kNoAllocMaxN + 1;
 
-struct NoAllocModel
-{
-    int type;
-    double r0, sill, nugget;
-    double T[9];
-};
-
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
-// the analytic model of cov_model.h:146-183 on a real displacement
-__device__ double noalloc_cov(const NoAllocModel &m, double v0, double v1, double v2)
-{
-    double acc = 0.0;
-    for (int i = 0; i < 3; ++i)
-    {
-        double d = 0.0;
-        d = __dadd_rn(d, __dmul_rn(v0, m.T[3 * i + 0]));
-        d = __dadd_rn(d, __dmul_rn(v1, m.T[3 * i + 1]));
-        d = __dadd_rn(d, __dmul_rn(v2, m.T[3 * i + 2]));
-        acc = __dadd_rn(acc, __dmul_rn(d, d));
-    }
-    const double h = sqrt(acc);
-    if (h < 0.0001) return m.sill;
-    const double u = h / m.r0;
-    if (m.type == 2) return (m.sill - m.nugget) * exp(-3.0 * (u * u));
-    if (m.type == 1) return (m.sill - m.nugget) * exp((-3.0 * h) / m.r0);
-    if (h > m.r0) return 0.0;
-    return (m.sill - m.nugget) * (1.0 - (1.5 * h) / m.r0 + 0.5 * (u * u * u));
-}
-
 // One CTA solves the system held in `s` (the static array's address): builds A
-// and b, factors A = L L^T and solves for the weights, all in FP64.
-__global__ void k_sk_weights_noalloc(NoAllocModel m, double *__restrict__ s, int n)
+// and b, factors A = L L^T and solves for the weights, all in FP64, with the
+// same device code as the regular entry point (sk_single.cuh).
+__global__ void k_sk_weights_noalloc(hb::DevModel m, double *__restrict__ s, int n)
 {
-    const double cx = s[0], cy = s[1], cz = s[2];
-    const double *xs = s + 3, *ys = xs + n, *zs = ys + n;
     double *A = s + 3 + 3 * kNoAllocMaxN;
     double *w = A + (size_t)kNoAllocMaxN * kNoAllocMaxN;
-    double *status = w + kNoAllocMaxN;
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x)
-    {
-        const int i = e / n, j = e % n;
-        A[e] = noalloc_cov(m, xs[i] - xs[j], ys[i] - ys[j], zs[i] - zs[j]);
-    }
-    for (int i = threadIdx.x; i < n; i += blockDim.x) w[i] = noalloc_cov(m, xs[i] - cx, ys[i] - cy, zs[i] - cz);
-    __syncthreads();
-    bool fail = false;
-    for (int j = 0; j < n; ++j)
-    {
-        const double d = A[(size_t)j * n + j];
-        if (!(d > 0.0)) fail = true;
-        const double ljj = sqrt(d);
-        __syncthreads();
-        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) A[(size_t)i * n + j] /= ljj;
-        if (threadIdx.x == 0) A[(size_t)j * n + j] = ljj;
-        __syncthreads();
-        const int span = n - j - 1;
-        for (int e = threadIdx.x; e < span * span; e += blockDim.x)
-        {
-            const int i = j + 1 + e / span, c = j + 1 + e % span;
-            if (c <= i) A[(size_t)i * n + c] -= A[(size_t)i * n + j] * A[(size_t)c * n + j];
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0)
-    {
-        for (int i = 0; i < n; ++i)
-        {
-            double acc = w[i];
-            for (int c = 0; c < i; ++c) acc -= A[(size_t)i * n + c] * w[c];
-            w[i] = acc / A[(size_t)i * n + i];
-        }
-        for (int i = n - 1; i >= 0; --i)
-        {
-            double acc = w[i];
-            for (int c = i + 1; c < n; ++c) acc -= A[(size_t)c * n + i] * w[c];
-            w[i] = acc / A[(size_t)i * n + i];
-        }
-        status[0] = fail ? 0.0 : 1.0;
-    }
+    const bool fail = hb::sk_single_solve(m, s, n, A, w);
+    if (threadIdx.x == 0) w[kNoAllocMaxN] = fail ? 0.0 : 1.0;
 }
 
 std::mutex g_setup_mu;
 double *g_scratch_ptr[kMaxDevices] = {nullptr};
 
-// Device address of the static array on the current device, looked up once.
+// Device address of the static array on the current device, looked up once;
+// the kernel's module (and with it the array) is loaded onto the device here.
 cudaError_t scratch_address(int dev, double **out)
 {
     std::lock_guard<std::mutex> lk(g_setup_mu);
     if (!g_scratch_ptr[dev])
     {
+        cudaFuncAttributes fa{};
+        cudaError_t e = cudaFuncGetAttributes(&fa, k_sk_weights_noalloc);
+        if (e != cudaSuccess) return e;
         void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return e;
         g_scratch_ptr[dev] = static_cast<double *>(p);
     }
@@ -163,7 +107,7 @@ extern "C" int hpgl_b200_sk_weights_noalloc(const float *center_coords, const fl
         hb::set_error("hpgl_b200_sk_weights_noalloc: " + err);
         return HPGL_B200_EINVAL;
     }
-    NoAllocModel m;
+    hb::DevModel m;
     m.type = cm.type;
     m.r0 = cm.ranges[0];
     m.sill = cm.sill;
