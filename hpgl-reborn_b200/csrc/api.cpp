@@ -845,6 +845,39 @@ int hpgl_b200_solve_variant_get(int bucket_np, int cov_type, int precision)
     return hb::solve_variant(bucket_np, cov_type, precision);
 }
 
+int hpgl_b200_tune_mode(int on)
+{
+    const int prev = hb::tune_mode();
+    hb::set_tune_mode(on);
+    return prev;
+}
+
+int hpgl_b200_tune_load(const char *path)
+{
+    std::string err;
+    const int n = path ? hb::tune_load(path, err) : -1;
+    if (n < 0)
+    {
+        hb::set_error("hpgl_b200_tune_load: " + (path ? err : std::string("null path")));
+        return HPGL_B200_EINVAL;
+    }
+    return n;
+}
+
+int hpgl_b200_tune_save(const char *path)
+{
+    std::string err;
+    const int n = path ? hb::tune_save(path, err) : -1;
+    if (n < 0)
+    {
+        hb::set_error("hpgl_b200_tune_save: " + (path ? err : std::string("null path")));
+        return HPGL_B200_EINVAL;
+    }
+    return n;
+}
+
+void hpgl_b200_tune_reset(void) { hb::tune_reset(); }
+
 void *hpgl_b200_host_alloc(size_t bytes) { return hb::host_alloc(bytes); }
 void hpgl_b200_host_free(void *p) { hb::host_free(p); }
 

@@ -618,7 +618,8 @@ static void run_solves(Engine &E, const Plan &pl, const DevPoints &P, const DevS
     for (int b = 0; b < kBuckets; ++b)
     {
         variant[b] = b < 4 ? solve_variant(kBucketNP[b], pl.f.m.type, precision) : kVariantFold;
-        any_quad = any_quad || (precision && b < 4 && kBucketNP[b] <= 32 && variant[b] == kVariantQuad);
+        any_quad = any_quad || (precision && b < 4 && kBucketNP[b] <= 32 &&
+                                (is_quad_variant(variant[b]) || tune_wanted(kBucketNP[b], pl.f.m.type, precision)));
     }
     if (any_quad) ref_cells = E.buf<int2>("ref_cells", (size_t)g.n_cells);
     launch_prepare(g, d_mask, all_cells, S.nb_n, d_status, bucket_cnt, bucket_off, tile_cnt, tile_mom, cells, moments,
@@ -636,13 +637,44 @@ static void run_solves(Engine &E, const Plan &pl, const DevPoints &P, const DevS
     const double c0 = pl.f.c0();
     const double rhs = ordinary ? 2.0 : 1.0;
     int esc_off[kBuckets];
+    // Tuning mode: the first large bucket of a key without a setting runs
+    // every variant the key can run once, timed, and the fastest becomes the
+    // key's setting (and runs below, leaving this call's outputs).
+    auto tune_bucket = [&](int b, const int2 *bcells, int first) {
+        const int np = kBucketNP[b];
+        double ms[kVariantCount] = {0};
+        for (int v = 1; v < kVariantCount; ++v)
+        {
+            if (!solve_variant_valid(np, precision, v)) continue;
+            const bool quad = precision && is_quad_variant(v);
+            HB_CK(cudaMemsetAsync(esc_cnt + b, 0, sizeof(int), st));
+            HB_CK(cudaMemsetAsync(ref_cnt + b, 0, sizeof(int), st));
+            HB_CK(cudaEventRecord(E.ev_[10 + 2 * b], st));
+            HB_CK(launch_solve_bucket(np, precision, v, ordinary, g, bcells, bucket_cnt + b, cnt[b], S.nb_rec,
+                                      S.nb_n, ind_value, S.pair64, S.pair32, mean, c0, steps, tol, out,
+                                      quad ? ref_cells + first : (esc_cells ? esc_cells + first : nullptr),
+                                      quad ? ref_cnt + b : esc_cnt + b, E.n_sm(), st));
+            HB_CK(cudaEventRecord(E.ev_[11 + 2 * b], st));
+            HB_CK(cudaEventSynchronize(E.ev_[11 + 2 * b]));
+            float t = 0.0f;
+            HB_CK(cudaEventElapsedTime(&t, E.ev_[10 + 2 * b], E.ev_[11 + 2 * b]));
+            ms[v] = t * 1e6 / (double)cnt[b];
+            E.stats.launches += 1;
+        }
+        tune_record(np, pl.f.m.type, precision, ms);
+        HB_CK(cudaMemsetAsync(esc_cnt + b, 0, sizeof(int), st));
+        HB_CK(cudaMemsetAsync(ref_cnt + b, 0, sizeof(int), st));
+        variant[b] = solve_variant(np, pl.f.m.type, precision);
+    };
     for (int b = 0; b < kBuckets; ++b)
     {
         esc_off[b] = off;
         if (cnt[b] > 0)
         {
             const int2 *bcells = cells + off;
-            const bool quad = precision && b < 4 && kBucketNP[b] <= 32 && variant[b] == kVariantQuad;
+            if (b < 4 && cnt[b] >= kTuneMinItems && tune_wanted(kBucketNP[b], pl.f.m.type, precision))
+                tune_bucket(b, bcells, off);
+            const bool quad = precision && b < 4 && kBucketNP[b] <= 32 && is_quad_variant(variant[b]);
             HB_CK(cudaEventRecord(E.ev_[10 + 2 * b], st));
             if (b < 4)
             {
@@ -673,7 +705,7 @@ static void run_solves(Engine &E, const Plan &pl, const DevPoints &P, const DevS
         // classic refinement of what the four-rows-per-lane kernel queued
         for (int b = 0; b < 4; ++b)
         {
-            if (cnt[b] == 0 || !(kBucketNP[b] <= 32 && variant[b] == kVariantQuad)) continue;
+            if (cnt[b] == 0 || !(kBucketNP[b] <= 32 && is_quad_variant(variant[b]))) continue;
             HB_CK(launch_solve_bucket(kBucketNP[b], 1, kVariantFold, ordinary, g, ref_cells + esc_off[b], ref_cnt + b,
                                       std::min(cnt[b], E.n_sm() * 8), S.nb_rec, S.nb_n, ind_value, S.pair64,
                                       S.pair32, mean, c0, steps, tol, out, esc_cells + esc_off[b], esc_cnt + b,

@@ -123,6 +123,13 @@ int get_threads();
 // (-1 for an invalid key or variant)
 int solve_variant(int np, int cov_type, int precision);
 int set_solve_variant(int np, int cov_type, int precision, int variant);
+// tuning mode on / off; the tuning cache (JSON) read and written, returning
+// the number of keys or -1 with `err`; every key back to its built-in pick
+int tune_mode();
+void set_tune_mode(int on);
+int tune_load(const char *path, std::string &err);
+int tune_save(const char *path, std::string &err);
+void tune_reset();
 
 // kind 0 OK, 1 SK, 2 LVM (SK weights around the per-cell `means`, which kind 2
 // requires; lvm_kriging.cpp:16-39)

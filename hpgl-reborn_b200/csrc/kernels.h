@@ -101,22 +101,35 @@ cudaError_t launch_resolve_ties_fast(const Geom &g, const int *tie_cells, const 
 
 // solves (solve.cu, misc.cu)
 // Solve-kernel variants (the launch shapes the tuning table chooses between,
-// tune.cpp). FP32-refined, n <= 32: kVariantQuad (four rows per lane,
-// solve_quad.cu) or kVariantFold (two rows per lane with in-kernel classic
-// refinement, solve.cu); n 33-64 and FP64 have one variant each.
+// tune.cpp). n <= 32: kVariantFold (two rows per lane: FP32-refined 512-thread
+// blocks with in-kernel classic refinement, FP64 384-thread blocks),
+// kVariantFoldNarrow (the same with 256-thread blocks and up to 255
+// registers); FP32-refined also kVariantQuad (four rows per lane, 384-thread
+// blocks, solve_quad.cu) and kVariantQuadNarrow (256-thread blocks). n 33-64
+// has one variant (kVariantFold: one warp per system, 256-thread blocks).
 enum SolveVariant : int
 {
     kVariantDefault = 0,
     kVariantFold = 1,
     kVariantQuad = 2,
+    kVariantFoldNarrow = 3,
+    kVariantQuadNarrow = 4,
 };
-constexpr int kVariantCount = 3;
+constexpr int kVariantCount = 5;
+// the four-rows-per-lane FP32 kernels queue failing systems for classic refinement
+inline bool is_quad_variant(int v) { return v == kVariantQuad || v == kVariantQuadNarrow; }
 // the variant that runs for a (bucket, covariance type, precision) key
 int solve_variant(int np, int cov_type, int precision);
 // whether `variant` can run the key (kVariantDefault always can)
 bool solve_variant_valid(int np, int precision, int variant);
 // overrides one key; returns its previous setting, or -1 for an invalid key or variant
 int set_solve_variant(int np, int cov_type, int precision, int variant);
+// tuning mode (tune.cpp): a key without a setting is timed on its first bucket
+// of at least kTuneMinItems systems; tune_record takes the ms per 1M systems
+// of each variant (<= 0: not run) and sets the fastest
+constexpr int kTuneMinItems = 20000;
+bool tune_wanted(int np, int cov_type, int precision);
+void tune_record(int np, int cov_type, int precision, const double *ms_per_variant);
 cudaError_t launch_solve_bucket(int np, int precision, int variant, bool ordinary, const Geom &g, const int2 *cells,
                                 const int *n_items, int max_items, const int2 *nb_rec, const int *nb_n, int ind_value,
                                 const double *pair64, const float *pair32, double mean, double c0, int steps,

@@ -409,28 +409,19 @@ __device__ __forceinline__ void fold_bilinear(const FoldGrp<NP / 2> &fg, const d
     fg.sync();
 }
 
-// Threads per block of the folded kernel: one block of 512 per SM (registers
+// Threads per block of the folded kernel (one block per SM): 512 (registers
 // capped at 128), so all the systems in flight on an SM come from one run of
-// neighbouring cells.
-#ifndef HB_FOLD_THREADS
-#define HB_FOLD_THREADS 512
-#endif
-
-// Systems of 33 to 64 neighbours fold onto one warp each (two rows of up to 64
-// entries per lane): 256-thread blocks, up to 255 registers.
+// neighbouring cells; the narrow variant (kVariantFoldNarrow) runs 256 with up
+// to 255 registers. Systems of 33 to 64 neighbours fold onto one warp each (two
+// rows of up to 64 entries per lane): 256-thread blocks.
 template <int NP>
 constexpr int fold_threads()
 {
-    return NP <= 32 ? HB_FOLD_THREADS : 256;
-}
-template <int NP>
-constexpr int fold_min_blocks()
-{
-    return NP <= 32 ? 512 / HB_FOLD_THREADS : 1;
+    return NP <= 32 ? 512 : 256;
 }
 
-template <int NP, bool ORDINARY>
-__global__ void __launch_bounds__(fold_threads<NP>(), fold_min_blocks<NP>())
+template <int NP, bool ORDINARY, int TH>
+__global__ void __launch_bounds__(TH, 1)
     k_solve_fold(const Geom g, const int2 *__restrict__ cells, const int *__restrict__ n_items_ptr,
                  const int2 *__restrict__ nb_rec, int ind_value, const float *__restrict__ pair32, SolveParams P)
 {
@@ -784,21 +775,17 @@ struct Fold64Smem
 // cap registers at 168, which the step's row read 16 bytes at a time fits with
 // almost no spills, and give each scheduler three warps to cover the FP64
 // dependency latency (256 threads: 198M cells/s; 320: 173M; 512, spilling: 196M;
-// 384: 211M on the 256x256x128 benchmark).
-#ifndef HB_FOLD64_THREADS
-#define HB_FOLD64_THREADS 384
-#endif
-
-// Systems of 33 to 64 neighbours fold onto one warp each (rows t and 63 - t:
-// 96 doubles a lane), in 256-thread blocks with up to 255 registers.
+// 384: 211M on the 256x256x128 benchmark); the narrow variant runs 256. Systems
+// of 33 to 64 neighbours fold onto one warp each (rows t and 63 - t: 96
+// doubles a lane), in 256-thread blocks with up to 255 registers.
 template <int NP>
 constexpr int fold64_threads()
 {
-    return NP <= 32 ? HB_FOLD64_THREADS : 256;
+    return NP <= 32 ? 384 : 256;
 }
 
-template <int NP, bool ORDINARY>
-__global__ void __launch_bounds__(fold64_threads<NP>(), 1)
+template <int NP, bool ORDINARY, int TH>
+__global__ void __launch_bounds__(TH, 1)
     k_solve_fold64(const Geom g, const int2 *__restrict__ cells, const int *__restrict__ n_items_ptr,
                    const int2 *__restrict__ nb_rec, int ind_value, SolveParams P)
 {
@@ -1003,27 +990,27 @@ __global__ void __launch_bounds__(fold64_threads<NP>(), 1)
     }
 }
 
-template <int NP, typename TF, bool ORD, bool REF>
+template <int NP, typename TF, bool ORD, bool REF, int TH>
 static cudaError_t launch_one(const Geom &g, const int2 *cells, const int *n_items, int max_items, const int2 *nb_rec,
                               int ind_value, const float *pair32, const SolveParams &P, int n_sm, cudaStream_t st)
 {
     int blocks = 0;
     if constexpr (REF)
     {
-        constexpr int fthreads = fold_threads<NP>();
+        constexpr int fthreads = TH;
         constexpr int spb = fthreads / (NP / 2); // systems per block
         const size_t smem = FoldSmem<NP, ORD ? 3 : 2>::bytes * spb;
-        auto kern = k_solve_fold<NP, ORD>;
+        auto kern = k_solve_fold<NP, ORD, TH>;
         cudaError_t e = launch_kernel(kern, fthreads, smem, max_items, spb, n_sm, blocks);
         if (e != cudaSuccess) return e;
         kern<<<(unsigned)blocks, fthreads, smem, st>>>(g, cells, n_items, nb_rec, ind_value, pair32, P);
     }
     else
     {
-        constexpr int fthreads = fold64_threads<NP>();
+        constexpr int fthreads = TH;
         constexpr int spb = fthreads / (NP / 2); // systems per block
         const size_t smem = Fold64Smem<NP>::bytes * spb;
-        auto kern = k_solve_fold64<NP, ORD>;
+        auto kern = k_solve_fold64<NP, ORD, TH>;
         cudaError_t e = launch_kernel(kern, fthreads, smem, max_items, spb, n_sm, blocks);
         if (e != cudaSuccess) return e;
         kern<<<(unsigned)blocks, fthreads, smem, st>>>(g, cells, n_items, nb_rec, ind_value, P);
@@ -1037,21 +1024,42 @@ static cudaError_t launch_np(int precision, int variant, bool ordinary, const Ge
                              const SolveParams &P, int n_sm, cudaStream_t st)
 {
 #define HB_ARGS g, cells, n_items, max_items, nb_rec, ind_value, pair32, P, n_sm, st
-    if (precision == 0)
-        return ordinary ? launch_one<NP, double, true, false>(HB_ARGS) : launch_one<NP, double, false, false>(HB_ARGS);
     if constexpr (NP <= 32)
     {
-        if (variant != kVariantFold) return launch_solve_quad(NP, ordinary, HB_ARGS);
+        if (precision == 0)
+        {
+            if (variant == kVariantFoldNarrow)
+                return ordinary ? launch_one<NP, double, true, false, 256>(HB_ARGS)
+                                : launch_one<NP, double, false, false, 256>(HB_ARGS);
+            return ordinary ? launch_one<NP, double, true, false, 384>(HB_ARGS)
+                            : launch_one<NP, double, false, false, 384>(HB_ARGS);
+        }
+        if (variant == kVariantQuad || variant == kVariantQuadNarrow || variant == kVariantDefault)
+            return launch_solve_quad(NP, ordinary, variant == kVariantQuadNarrow ? 256 : 384, HB_ARGS);
+        if (variant == kVariantFoldNarrow)
+            return ordinary ? launch_one<NP, float, true, true, 256>(HB_ARGS)
+                            : launch_one<NP, float, false, true, 256>(HB_ARGS);
+        return ordinary ? launch_one<NP, float, true, true, 512>(HB_ARGS)
+                        : launch_one<NP, float, false, true, 512>(HB_ARGS);
     }
-    return ordinary ? launch_one<NP, float, true, true>(HB_ARGS) : launch_one<NP, float, false, true>(HB_ARGS);
+    else
+    {
+        (void)variant;
+        if (precision == 0)
+            return ordinary ? launch_one<NP, double, true, false, 256>(HB_ARGS)
+                            : launch_one<NP, double, false, false, 256>(HB_ARGS);
+        return ordinary ? launch_one<NP, float, true, true, 256>(HB_ARGS)
+                        : launch_one<NP, float, false, true, 256>(HB_ARGS);
+    }
 #undef HB_ARGS
 }
 
 bool solve_variant_valid(int np, int precision, int variant)
 {
     if (variant == kVariantDefault) return true;
-    if (precision == 1 && np <= 32) return variant == kVariantFold || variant == kVariantQuad;
-    return variant == kVariantFold;
+    if (np > 32) return variant == kVariantFold;
+    if (precision == 1) return variant >= kVariantFold && variant <= kVariantQuadNarrow;
+    return variant == kVariantFold || variant == kVariantFoldNarrow;
 }
 
 cudaError_t launch_solve_bucket(int np, int precision, int variant, bool ordinary, const Geom &g, const int2 *cells,

@@ -89,7 +89,8 @@ static cudaError_t launch_kernel(K kern, int threads, size_t smem, int max_items
 namespace hb
 {
 // FP32-refined solves of up to 32 neighbours, four rows per lane (solve_quad.cu)
-cudaError_t launch_solve_quad(int np, bool ordinary, const Geom &g, const int2 *cells, const int *n_items,
-                              int max_items, const int2 *nb_rec, int ind_value, const float *pair32,
-                              const SolveParams &P, int n_sm, cudaStream_t st);
+// (threads per block: 384 or 256)
+cudaError_t launch_solve_quad(int np, bool ordinary, int threads, const Geom &g, const int2 *cells,
+                              const int *n_items, int max_items, const int2 *nb_rec, int ind_value,
+                              const float *pair32, const SolveParams &P, int n_sm, cudaStream_t st);
 } // namespace hb

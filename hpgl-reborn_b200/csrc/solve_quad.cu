@@ -108,10 +108,6 @@ struct QuadSmem
     static constexpr size_t bytes = raw + (size_t)((shift - (int)(raw % 128) + 128) % 128);
 };
 
-#ifndef HB_QUAD_THREADS
-#define HB_QUAD_THREADS 384
-#endif
-
 template <int NP>
 __device__ __forceinline__ float q_get(const float2 (&A)[5 * NP / 4], int k, int c)
 {
@@ -308,8 +304,10 @@ __device__ __forceinline__ bool q_factor(float2 (&A)[5 * NP / 4], float (&rhs)[4
     return fail;
 }
 
-template <int NP, bool ORDINARY>
-__global__ void __launch_bounds__(HB_QUAD_THREADS, 1)
+// Threads per block TH: 384 (168 registers, twelve warps) or 256 (255
+// registers, eight warps), one block per SM.
+template <int NP, bool ORDINARY, int TH>
+__global__ void __launch_bounds__(TH, 1)
     k_solve_quad(const Geom g, const int2 *__restrict__ cells, const int *__restrict__ n_items_ptr,
                  const int2 *__restrict__ nb_rec, int ind_value, const float *__restrict__ pair32, SolveParams P)
 {
@@ -495,35 +493,44 @@ __global__ void __launch_bounds__(HB_QUAD_THREADS, 1)
     q_cp_async_wait_all();
 }
 
-template <int NP, bool ORD>
+template <int NP, bool ORD, int TH>
 static cudaError_t launch_quad_one(const Geom &g, const int2 *cells, const int *n_items, int max_items,
                                    const int2 *nb_rec, int ind_value, const float *pair32, const SolveParams &P,
                                    int n_sm, cudaStream_t st)
 {
-    constexpr int threads = HB_QUAD_THREADS;
-    constexpr int spb = threads / 32 * (32 / (NP / 4));
+    constexpr int spb = TH / 32 * (32 / (NP / 4));
     const size_t smem = QuadSmem<NP, ORD ? 3 : 2>::bytes * spb;
-    auto kern = k_solve_quad<NP, ORD>;
+    auto kern = k_solve_quad<NP, ORD, TH>;
     int blocks = 0;
-    cudaError_t e = launch_kernel(kern, threads, smem, max_items, spb, n_sm, blocks);
+    cudaError_t e = launch_kernel(kern, TH, smem, max_items, spb, n_sm, blocks);
     if (e != cudaSuccess) return e;
-    kern<<<(unsigned)blocks, threads, smem, st>>>(g, cells, n_items, nb_rec, ind_value, pair32, P);
+    kern<<<(unsigned)blocks, TH, smem, st>>>(g, cells, n_items, nb_rec, ind_value, pair32, P);
     return cudaGetLastError();
 }
 
-cudaError_t launch_solve_quad(int np, bool ordinary, const Geom &g, const int2 *cells, const int *n_items,
-                              int max_items, const int2 *nb_rec, int ind_value, const float *pair32,
-                              const SolveParams &P, int n_sm, cudaStream_t st)
+template <int NP, bool ORD>
+static cudaError_t launch_quad_th(int threads, const Geom &g, const int2 *cells, const int *n_items, int max_items,
+                                  const int2 *nb_rec, int ind_value, const float *pair32, const SolveParams &P,
+                                  int n_sm, cudaStream_t st)
 {
-#define HB_QARGS g, cells, n_items, max_items, nb_rec, ind_value, pair32, P, n_sm, st
+    if (threads == 256)
+        return launch_quad_one<NP, ORD, 256>(g, cells, n_items, max_items, nb_rec, ind_value, pair32, P, n_sm, st);
+    return launch_quad_one<NP, ORD, 384>(g, cells, n_items, max_items, nb_rec, ind_value, pair32, P, n_sm, st);
+}
+
+cudaError_t launch_solve_quad(int np, bool ordinary, int threads, const Geom &g, const int2 *cells,
+                              const int *n_items, int max_items, const int2 *nb_rec, int ind_value,
+                              const float *pair32, const SolveParams &P, int n_sm, cudaStream_t st)
+{
+#define HB_QARGS threads, g, cells, n_items, max_items, nb_rec, ind_value, pair32, P, n_sm, st
     switch (np)
     {
     case 8:
-        return ordinary ? launch_quad_one<8, true>(HB_QARGS) : launch_quad_one<8, false>(HB_QARGS);
+        return ordinary ? launch_quad_th<8, true>(HB_QARGS) : launch_quad_th<8, false>(HB_QARGS);
     case 16:
-        return ordinary ? launch_quad_one<16, true>(HB_QARGS) : launch_quad_one<16, false>(HB_QARGS);
+        return ordinary ? launch_quad_th<16, true>(HB_QARGS) : launch_quad_th<16, false>(HB_QARGS);
     case 32:
-        return ordinary ? launch_quad_one<32, true>(HB_QARGS) : launch_quad_one<32, false>(HB_QARGS);
+        return ordinary ? launch_quad_th<32, true>(HB_QARGS) : launch_quad_th<32, false>(HB_QARGS);
     default:
         return cudaErrorInvalidValue;
     }

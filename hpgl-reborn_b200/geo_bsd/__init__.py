@@ -5,3 +5,6 @@ from .hpgl_wrap import last_stats  # noqa: F401
 from .cdf import CdfData, calc_cdf  # noqa: F401
 from .sgs import sgs_simulation  # noqa: F401
 from .sis import sis_simulation  # noqa: F401
+from . import tune as _tune
+
+_tune._load_default()  # the solve-kernel tuning cache (geo_bsd/tune_cache.json)

@@ -138,7 +138,8 @@ EXPORTS = [
     "hpgl_b200_find_neighbours", "hpgl_b200_last_stats", "hpgl_b200_host_alloc", "hpgl_b200_host_free",
     "hpgl_b200_transform", "hpgl_b200_template", "hpgl_b200_covariance", "hpgl_b200_version",
     "hpgl_b200_sk_weights_noalloc", "hpgl_b200_loo_ok", "hpgl_b200_loo_ok_adjoint",
-    "hpgl_b200_solve_variant", "hpgl_b200_solve_variant_get",
+    "hpgl_b200_solve_variant", "hpgl_b200_solve_variant_get", "hpgl_b200_tune_mode", "hpgl_b200_tune_load",
+    "hpgl_b200_tune_save", "hpgl_b200_tune_reset",
 ]
 
 
@@ -249,6 +250,14 @@ def _load():
     lib.hpgl_b200_solve_variant.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int]
     lib.hpgl_b200_solve_variant_get.restype = C.c_int
     lib.hpgl_b200_solve_variant_get.argtypes = [C.c_int, C.c_int, C.c_int]
+    lib.hpgl_b200_tune_mode.restype = C.c_int
+    lib.hpgl_b200_tune_mode.argtypes = [C.c_int]
+    lib.hpgl_b200_tune_load.restype = C.c_int
+    lib.hpgl_b200_tune_load.argtypes = [C.c_char_p]
+    lib.hpgl_b200_tune_save.restype = C.c_int
+    lib.hpgl_b200_tune_save.argtypes = [C.c_char_p]
+    lib.hpgl_b200_tune_reset.restype = None
+    lib.hpgl_b200_tune_reset.argtypes = []
     lib.hpgl_b200_host_alloc.restype = C.c_void_p
     lib.hpgl_b200_host_alloc.argtypes = [C.c_size_t]
     lib.hpgl_b200_host_free.restype = None
@@ -296,7 +305,9 @@ STATS_KEYS = (["total_ms", "search_ms", "solve_ms", "tie_cells", "template_cells
                  "sgs_flops", "refined_cells"])
 
 
-VARIANT_DEFAULT, VARIANT_FOLD, VARIANT_QUAD = 0, 1, 2
+VARIANT_DEFAULT, VARIANT_FOLD, VARIANT_QUAD, VARIANT_FOLD_NARROW, VARIANT_QUAD_NARROW = 0, 1, 2, 3, 4
+VARIANT_NAMES = {VARIANT_DEFAULT: "default", VARIANT_FOLD: "fold", VARIANT_QUAD: "quad",
+                 VARIANT_FOLD_NARROW: "fold_narrow", VARIANT_QUAD_NARROW: "quad_narrow"}
 
 
 def solve_variant(bucket_np: int, cov_type: int, precision: int, variant: int = None) -> int:

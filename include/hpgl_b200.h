@@ -318,12 +318,17 @@ int hpgl_b200_last_stats(double *out, int cap);
  * one launch shape: bucket_np 8, 16, 32 or 64 (neighbour counts up to it),
  * cov_type 0 spherical / 1 exponential / 2 Gaussian, precision
  * HPGL_B200_FP64_PLAIN or HPGL_B200_FP32_REFINED. Variants:
- *   HPGL_B200_VARIANT_DEFAULT  the built-in pick of the key
- *   HPGL_B200_VARIANT_FOLD     two rows per lane (FP32: 512-thread blocks,
- *                              classic refinement in the kernel)
- *   HPGL_B200_VARIANT_QUAD     FP32_REFINED, bucket_np <= 32: four rows per
- *                              lane, 384-thread blocks; failing systems go on
- *                              to FOLD's refinement, then to FP64
+ *   HPGL_B200_VARIANT_DEFAULT      the built-in pick of the key
+ *   HPGL_B200_VARIANT_FOLD         two rows per lane (FP32: 512-thread blocks,
+ *                                  classic refinement in the kernel; FP64:
+ *                                  384-thread blocks; bucket 64: one warp per
+ *                                  system, 256-thread blocks)
+ *   HPGL_B200_VARIANT_FOLD_NARROW  bucket_np <= 32: FOLD in 256-thread blocks
+ *                                  (up to 255 registers a thread)
+ *   HPGL_B200_VARIANT_QUAD         FP32_REFINED, bucket_np <= 32: four rows
+ *                                  per lane, 384-thread blocks; failing systems
+ *                                  go on to FOLD's refinement, then to FP64
+ *   HPGL_B200_VARIANT_QUAD_NARROW  QUAD in 256-thread blocks
  * hpgl_b200_solve_variant sets a key and returns its previous setting, or
  * HPGL_B200_EINVAL for an invalid key or a variant the key cannot run;
  * hpgl_b200_solve_variant_get returns the variant a key runs now. Results of
@@ -331,8 +336,26 @@ int hpgl_b200_last_stats(double *out, int cap);
 #define HPGL_B200_VARIANT_DEFAULT 0
 #define HPGL_B200_VARIANT_FOLD 1
 #define HPGL_B200_VARIANT_QUAD 2
+#define HPGL_B200_VARIANT_FOLD_NARROW 3
+#define HPGL_B200_VARIANT_QUAD_NARROW 4
 int hpgl_b200_solve_variant(int bucket_np, int cov_type, int precision, int variant);
 int hpgl_b200_solve_variant_get(int bucket_np, int cov_type, int precision);
+/* The tuner behind those keys (no counterpart in the reference).
+ * hpgl_b200_tune_mode(1): a key without a setting is timed the first time a
+ * call meets a bucket of at least 20000 of its systems: that bucket runs once
+ * with every variant the key can run, the fastest becomes the key's setting
+ * and produces the call's outputs; mode 0 (the default) uses the settings as
+ * they are. Returns the previous mode.
+ * hpgl_b200_tune_load / hpgl_b200_tune_save read / write the settings as a
+ * JSON list of {"np", "cov_type", "precision", "variant", "ms_per_million"}
+ * objects (the timings, ms per million systems, are written for keys this
+ * process timed); they return the number of keys, or HPGL_B200_EINVAL with
+ * the message kept for hpgl_get_last_exception_message.
+ * hpgl_b200_tune_reset puts every key back to its built-in pick. */
+int hpgl_b200_tune_mode(int on);
+int hpgl_b200_tune_load(const char *path);
+int hpgl_b200_tune_save(const char *path);
+void hpgl_b200_tune_reset(void);
 
 /* No counterpart in the reference. The same SK weights as
  * hpgl_simple_kriging_weights for callers that cannot allocate device memory

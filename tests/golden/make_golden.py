@@ -4,7 +4,7 @@ Run here, where the reference sources are present and oracle/Makefile has built
 oracle/_ref/ (the reference's unmodified library, libhpgl.so, and the white-box
 harness libref_harness.so around its own templates):
 
-    make -C oracle && python tests/golden/make_golden.py        (all fixtures)
+    make -C oracle REF=<reference checkout> && python tests/golden/make_golden.py   (all fixtures)
                       python tests/golden/make_golden.py lvm    (lvm.npz only)
                       python tests/golden/make_golden.py sgs    (sgs.npz only)
                       python tests/golden/make_golden.py cok    (cok.npz only)
