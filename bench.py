@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--workload", default="sk_ok_large")
     ap.add_argument("--kind", choices=["ok", "sk", "lvm", "sgs", "cok", "sis"], default="ok")
     ap.add_argument("--skip-cpu-baseline", action="store_true")
+    ap.add_argument("--skip-configs", action="store_true",
+                    help="leave out the other benchmark configurations (100x100x50, clustered 512x512x64, "
+                         "indicator 200x200x100, leave-one-out 200x200x50)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--profile-case", type=float, default=0.0, metavar="SCALE",
                     help="run one device call on the workload shrunk by SCALE and exit "
@@ -842,6 +845,211 @@ def bench_cok(args, rank, world, local):
         dist.destroy_process_group()
 
 
+def bucket_kernel(W, b, cov_type, precision, ordinary):
+    """Name of the solve kernel that ran bucket b (0..4) for this key."""
+    if b == 4:
+        return "k_solve_large (n > 64, one block per system, FP64)"
+    np_ = [8, 16, 32, 64][b]
+    v = W.solve_variant(np_, cov_type, precision) if hasattr(W, "solve_variant") else 1
+    kind = "ordinary" if ordinary else "simple"
+    if np_ == 64 and v in (getattr(W, "VARIANT_WIDE", -1), W.VARIANT_DEFAULT):
+        th, pr = (256, "FP64 plain") if precision == 0 else (384, "FP32 refined")
+        return f"k_solve_wide{64 if precision == 0 else 32}<{kind}, {th}> ({pr}, one warp per system, rolled phases)"
+    if precision == 0:
+        th = 384 if (np_ <= 32 and v == W.VARIANT_FOLD) else 256
+        return f"k_solve_fold64<NP={np_}, {kind}, {th}> (FP64 plain, NP/2 lanes per system)"
+    if np_ == 32 and v in (getattr(W, "VARIANT_TILE", -1), getattr(W, "VARIANT_TILE_NARROW", -1)):
+        th = 384 if v == W.VARIANT_TILE else 192
+        return f"k_solve_tile<NP=32, {kind}, {th}> (FP32 refined, union tiles of {th // 8} systems, NP/4 lanes per system)"
+    if np_ <= 32 and v in (W.VARIANT_QUAD, W.VARIANT_QUAD_NARROW):
+        th = 384 if v == W.VARIANT_QUAD else 256
+        return f"k_solve_quad<NP={np_}, {kind}, {th}> (FP32 refined, NP/4 lanes per system)"
+    th = 512 if (np_ <= 32 and v == W.VARIANT_FOLD) else 256
+    return f"k_solve_fold<NP={np_}, {kind}, {th}> (FP32 refined, NP/2 lanes per system)"
+
+
+def solve_roofline(W, stats_list, cov_type, precision, ordinary, pk):
+    """Dominant solve kernel of a run (the bucket with the largest time) and its
+    algorithmic rate against the derived CUDA-core peak of the precision."""
+    last = stats_list[-1]
+    b = int(np.argmax([last[f"bucket_ms_{i}"] for i in range(5)]))
+    ms = float(np.mean([s[f"bucket_ms_{b}"] for s in stats_list]))
+    flops = last[f"bucket_flops_{b}"]
+    tf = flops / (ms / 1e3) / 1e12 if ms > 0 else 0.0
+    peak = pk["fp32"] if precision else pk["fp64"]
+    return {"kernel": bucket_kernel(W, b, cov_type, precision, ordinary), "kernel_ms": ms,
+            "algorithmic_flops": flops, "achieved_tflops": tf, "peak_tflops": peak, "frac": tf / peak,
+            "bound": "fp32" if precision else "fp64"}
+
+
+def bench_other_configs(args, W, dev, stream, pk):
+    """The benchmark's other configurations at one GPU (device pointers, CUDA
+    events on the launching stream, inputs resident in HBM): FP64-plain and
+    FP32-refined OK of the 100x100x50 grid (k = 12) and of the clustered
+    512x512x64 grid (k = 64, nugget 1e-3, with the error of both against the
+    FP64 oracle on sampled cells), full and median IK of the 200x200x100
+    five-category grid (k = 24), and the leave-one-out forward and adjoint
+    kernels on the 200x200x50 Gaussian-field grid (k = 24)."""
+    import torch
+    WL = workloads_module()
+    steps = max(1, min(args.steps, 3))
+    out = {}
+
+    def timed(fn, n):
+        fn()
+        torch.cuda.synchronize()
+        times, stats = [], []
+        for _ in range(n):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st = fn()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+            stats.append(st)
+        return float(np.mean(times)), stats
+
+    def cont_case(wl, n_steps, kind=0):
+        d_data = torch.from_numpy(np.ascontiguousarray(wl.data)).to(dev)
+        d_mask = torch.from_numpy(np.ascontiguousarray(wl.mask)).to(dev)
+        d_out, d_om = d_data.clone(), d_mask.clone()
+        d_est = torch.empty(wl.n_cells, dtype=torch.float64, device=dev)
+        dims = (C.c_int * 3)(*wl.dims)
+        p = W._HPGL_SK_PARAMS(covariance_type=wl.cov.cov_type, ranges=wl.cov.ranges, angles=wl.cov.angles,
+                              sill=wl.cov.sill, nugget=wl.cov.nugget, radiuses=wl.radiuses,
+                              max_neighbours=wl.max_neighbours, automatic_mean=1, mean=0.0)
+        res, ests = {}, {}
+        for prec, name in ((0, "fp64_plain"), (1, "fp32_refined")):
+            def call():
+                o = W._HPGL_B200_OPTIONS(precision=prec, refine_steps=2,
+                                         flags=W.FLAG_DEVICE_POINTERS | W.FLAG_OUT_IS_CLONE,
+                                         stream=stream.cuda_stream, estimate64=d_est.data_ptr(), variance=None,
+                                         status=None, ik_probs=None)
+                rc = W._hpgl_so.hpgl_b200_cont_kriging_ex(kind, dims, d_data.data_ptr(), d_mask.data_ptr(),
+                                                          C.byref(p), d_out.data_ptr(), d_om.data_ptr(), C.byref(o))
+                W.check(rc, "cont_kriging_ex")
+                return W.last_stats()
+            ms, stats = timed(call, n_steps)
+            cells = stats[-1]["kriged_cells"]
+            res[name] = {"value": cells / (ms / 1e3), "unit": "kriged cells/s", "ms_per_call": ms,
+                         "kriged_cells": cells, "escalated_cells": stats[-1]["escalated_cells"],
+                         "roofline": solve_roofline(W, stats, wl.cov.cov_type, prec, kind == 0, pk)}
+            ests[name] = d_est.cpu().numpy()
+        res["fp32_refined_over_fp64_plain"] = res["fp32_refined"]["value"] / res["fp64_plain"]["value"]
+        ok = np.isfinite(ests["fp64_plain"]) & (wl.mask == 0)
+        res["rel_err_fp32_refined_vs_fp64_plain"] = float(
+            np.abs(ests["fp32_refined"][ok] - ests["fp64_plain"][ok]).max() / np.abs(ests["fp64_plain"][ok]).max())
+        return res, ests
+
+    # 100x100x50, spherical, k = 12
+    wl = WL.ok_small()
+    out["ok_100x100x50_k12"], _ = cont_case(wl, max(steps, 3))
+
+    # clustered 512x512x64, Gaussian nugget 1e-3, k = 64; error against the FP64 oracle on sampled cells
+    wl = WL.clustered()
+    res, ests = cont_case(wl, 2)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    which = "ref" if O.available("ref") else "port"
+    rng = np.random.default_rng(55)
+    cand = np.flatnonzero((wl.mask == 0) & np.isfinite(ests["fp64_plain"]))
+    nodes = np.sort(rng.choice(cand, min(2000, len(cand)), replace=False)).astype(np.int32)
+    r = O.krige_nodes(which, 0, wl.dims, wl.data, wl.mask, wl.cov, wl.radiuses, wl.max_neighbours, nodes=nodes,
+                      want_idx=False)
+    okn = r["status"] == 0
+    ref = r["est"][okn]
+    scale = np.abs(ref).max()
+    for name in ("fp64_plain", "fp32_refined"):
+        e = ests[name][nodes][okn]
+        per = np.abs(e - ref) / np.maximum(np.abs(ref), 1e-300)
+        res[name]["error_vs_fp64_oracle"] = {"normwise": float(np.abs(e - ref).max() / scale),
+                                             "per_cell_p999": float(np.quantile(per, 0.999)),
+                                             "sampled_cells": int(okn.sum()), "oracle": which}
+    out["clustered_512x512x64_k64"] = res
+
+    # 200x200x100, five categories, k = 24: full IK and median IK
+    wl = WL.indicator()
+    m = len(wl.cat_covs)
+    d_data = torch.from_numpy(np.ascontiguousarray(wl.data)).to(dev)
+    d_mask = torch.from_numpy(np.ascontiguousarray(wl.mask)).to(dev)
+    d_out, d_om = d_data.clone(), d_mask.clone()
+    dims = (C.c_int * 3)(*wl.dims)
+    arr = (W._HPGL_IK_PARAMS * m)()
+    for i in range(m):
+        c = wl.cat_covs[i]
+        arr[i] = W._HPGL_IK_PARAMS(covariance_type=c.cov_type, ranges=tuple(c.ranges), angles=tuple(c.angles),
+                                   sill=c.sill, nugget=c.nugget, radiuses=tuple(wl.cat_radiuses[i]),
+                                   max_neighbours=wl.max_neighbours, marginal_prob=float(wl.marginals[i]))
+    d_mik = (d_data >= 2).to(torch.uint8)
+    c2 = wl.cat_covs[2]
+    mp = (1.0 - float(sum(wl.marginals[2:])), float(sum(wl.marginals[2:])))
+    pm = W._HPGL_MEDIAN_IK_PARAMS(covariance_type=c2.cov_type, ranges=tuple(c2.ranges), angles=tuple(c2.angles),
+                                  sill=c2.sill, nugget=c2.nugget, radiuses=tuple(wl.cat_radiuses[2]),
+                                  max_neighbours=wl.max_neighbours, marginal_probs=mp)
+    ik = {}
+    for prec, name in ((0, "fp64_plain"), (1, "fp32_refined")):
+        def ik_call():
+            o = W._HPGL_B200_OPTIONS(precision=prec, refine_steps=2, flags=W.FLAG_DEVICE_POINTERS | W.FLAG_OUT_IS_CLONE,
+                                     stream=stream.cuda_stream, estimate64=None, variance=None, status=None,
+                                     ik_probs=None)
+            rc = W._hpgl_so.hpgl_b200_indicator_kriging_ex(dims, d_data.data_ptr(), d_mask.data_ptr(), arr, m,
+                                                           d_out.data_ptr(), d_om.data_ptr(), C.byref(o))
+            W.check(rc, "indicator_kriging_ex")
+            return W.last_stats()
+
+        def mik_call():
+            o = W._HPGL_B200_OPTIONS(precision=prec, refine_steps=2, flags=W.FLAG_DEVICE_POINTERS | W.FLAG_OUT_IS_CLONE,
+                                     stream=stream.cuda_stream, estimate64=None, variance=None, status=None,
+                                     ik_probs=None)
+            rc = W._hpgl_so.hpgl_b200_median_ik_ex(dims, d_mik.data_ptr(), d_mask.data_ptr(), C.byref(pm),
+                                                   d_out.data_ptr(), d_om.data_ptr(), C.byref(o))
+            W.check(rc, "median_ik_ex")
+            return W.last_stats()
+        ms, stats = timed(ik_call, steps)
+        ik[f"ik_{name}"] = {"value": wl.n_cells * m / (ms / 1e3), "unit": "category-cells/s", "ms_per_call": ms,
+                            "cells_per_s": wl.n_cells / (ms / 1e3),
+                            "roofline": solve_roofline(W, stats, c2.cov_type, prec, False, pk)}
+        ms, stats = timed(mik_call, steps)
+        ik[f"median_ik_{name}"] = {"value": wl.n_cells / (ms / 1e3), "unit": "cells/s", "ms_per_call": ms,
+                                   "roofline": solve_roofline(W, stats, c2.cov_type, prec, False, pk)}
+    out["indicator_200x200x100_k24"] = ik
+
+    # 200x200x50 Gaussian field, k = 24: leave-one-out forward and adjoint kernels
+    wl = WL.gauss_cv()
+    from geo_bsd import geo as GEO
+    from geo_bsd import loo as LOO
+    prop = GEO.ContProperty(wl.data.reshape(wl.dims, order="F"), wl.mask.reshape(wl.dims, order="F"))
+    grid = GEO.SugarboxGrid(*wl.dims)
+    cm = GEO.CovarianceModel(type=wl.cov.cov_type, ranges=wl.cov.ranges, angles=wl.cov.angles, sill=wl.cov.sill,
+                             nugget=wl.cov.nugget)
+    geom = LOO.loo_geometry(prop, grid, wl.radiuses, wl.max_neighbours, cm)
+    ranges = torch.tensor(wl.cov.ranges, dtype=torch.float64, requires_grad=True)
+    sill = torch.tensor(wl.cov.sill, dtype=torch.float64, requires_grad=True)
+    nug = torch.tensor(wl.cov.nugget, dtype=torch.float64, requires_grad=True)
+    vals = geom.values.clone().requires_grad_(True)
+    fwd_ms, _ = timed(lambda: LOO.loo_estimates(geom, ranges, wl.cov.angles, sill, nug, vals), steps)
+    loss = None
+
+    def both():
+        nonlocal loss
+        loss = LOO.loo_cv_mse(geom, ranges, wl.cov.angles, sill, nug, vals)
+        loss.backward()
+    both_ms, _ = timed(both, steps)
+    t = int(geom.targets.numel())
+    k = wl.max_neighbours
+    f_sys = k ** 3 / 3 + k ** 2 / 2 + 2 * 2 * k ** 2 + 30 * (k * (k + 1) / 2 + k) + 2 * 2 * k  # F(k, 2)
+    out["loo_200x200x50_k24"] = {"targets": t, "forward_ms": fwd_ms, "forward_and_adjoint_ms": both_ms,
+                                 "adjoint_ms": both_ms - fwd_ms, "targets_per_s_forward": t / (fwd_ms / 1e3),
+                                 "forward_roofline": {"kernel": "k_loo_forward (FP64, one warp per target)",
+                                                      "algorithmic_flops": t * f_sys,
+                                                      "achieved_tflops": t * f_sys / (fwd_ms / 1e3) / 1e12,
+                                                      "peak_tflops": pk["fp64"],
+                                                      "frac": t * f_sys / (fwd_ms / 1e3) / 1e12 / pk["fp64"],
+                                                      "note": "forward call time includes the torch layer"}}
+    return out
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -1011,9 +1219,7 @@ def main():
     b_flops = last[f"bucket_flops_{b}"]
     achieved = b_flops / (b_ms / 1e3) / 1e12
     tpc = traffic_per_cell()
-    ordn = "ordinary" if kind == 0 and not lvm else "simple"
-    kname = (f"k_solve_fold<NP={[8, 16, 32][b]}, {ordn}> (FP32 refined, NP/2 lanes per system)" if b < 3
-             else f"k_solve_fold<NP=64, {ordn}> (FP32 refined)" if b == 3 else "k_solve_large")
+    kname = bucket_kernel(W, b, wl.cov.cov_type, 1, kind == 0 and not lvm)
     roofline = {"bound": "fp32", "kernel": kname,
                 "achieved": achieved, "peak": pk["fp32"], "unit": "TFLOP/s", "frac": achieved / pk["fp32"],
                 "traffic": (tpc * last[f"bucket_items_{b}"]) if tpc else None,
@@ -1060,6 +1266,33 @@ def main():
     for ptr in h_ptrs:
         lib.hpgl_b200_host_free(ptr)
 
+    # end to end through the public Python API (geo_bsd.ordinary_kriging / simple_kriging) with
+    # pageable numpy arrays: validation, the output clone and the copies included
+    e2e_api = None
+    if not lvm:
+        from geo_bsd import geo as GEO
+        prop = GEO.ContProperty(wl.data.reshape(wl.dims, order="F"), wl.mask.reshape(wl.dims, order="F"))
+        grid = GEO.SugarboxGrid(*wl.dims)
+        cm = GEO.CovarianceModel(type=wl.cov.cov_type, ranges=wl.cov.ranges, angles=wl.cov.angles,
+                                 sill=wl.cov.sill, nugget=wl.cov.nugget)
+        api_fn = GEO.ordinary_kriging if kind == 0 else GEO.simple_kriging
+        times = []
+        for i in range(2 + min(args.steps, 3)):
+            barrier()
+            t0 = time.perf_counter()
+            api_fn(prop, grid, wl.radiuses, wl.max_neighbours, cm, precision="fp32_refined")
+            if i >= 2:
+                times.append(time.perf_counter() - t0)
+        barrier()
+        api_cells = W.last_stats()["kriged_cells"]
+        e2e_api = {"value": api_cells * world / max_over_ranks(float(np.mean(times))), "unit": UNIT,
+                   "path": f"geo_bsd.{api_fn.__name__}(..., precision='fp32_refined'), pageable numpy inputs, "
+                           "wall clock per call"}
+
+    configs = None
+    if world == 1 and args.kind == "ok" and not args.skip_configs:
+        configs = bench_other_configs(args, W, dev, stream, peak_table())
+
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu_baseline:
         if args.kind in ("ok", "sk"):
@@ -1094,6 +1327,8 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(st["h2d_bytes"]),
                     "d2h_bytes_per_step": int(st["d2h_bytes"]), "timing": "wall clock per call (host tables, "
                                                                          "copies and kernels)"},
+            "e2e_api": e2e_api,
+            "configs": configs,
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }

@@ -638,8 +638,9 @@ static void run_solves(Engine &E, const Plan &pl, const DevPoints &P, const DevS
     const double rhs = ordinary ? 2.0 : 1.0;
     int esc_off[kBuckets];
     // Tuning mode: the first large bucket of a key without a setting runs
-    // every variant the key can run once, timed, and the fastest becomes the
-    // key's setting (and runs below, leaving this call's outputs).
+    // every variant the key can run twice, the second run timed (the first
+    // loads the kernel), and the fastest becomes the key's setting (and runs
+    // below, leaving this call's outputs).
     auto tune_bucket = [&](int b, const int2 *bcells, int first) {
         const int np = kBucketNP[b];
         double ms[kVariantCount] = {0};
@@ -647,19 +648,22 @@ static void run_solves(Engine &E, const Plan &pl, const DevPoints &P, const DevS
         {
             if (!solve_variant_valid(np, precision, v)) continue;
             const bool quad = precision && is_quad_variant(v);
-            HB_CK(cudaMemsetAsync(esc_cnt + b, 0, sizeof(int), st));
-            HB_CK(cudaMemsetAsync(ref_cnt + b, 0, sizeof(int), st));
-            HB_CK(cudaEventRecord(E.ev_[10 + 2 * b], st));
-            HB_CK(launch_solve_bucket(np, precision, v, ordinary, g, bcells, bucket_cnt + b, cnt[b], S.nb_rec,
-                                      S.nb_n, ind_value, S.pair64, S.pair32, mean, c0, steps, tol, out,
-                                      quad ? ref_cells + first : (esc_cells ? esc_cells + first : nullptr),
-                                      quad ? ref_cnt + b : esc_cnt + b, E.n_sm(), st));
-            HB_CK(cudaEventRecord(E.ev_[11 + 2 * b], st));
+            for (int rep = 0; rep < 2; ++rep)
+            {
+                HB_CK(cudaMemsetAsync(esc_cnt + b, 0, sizeof(int), st));
+                HB_CK(cudaMemsetAsync(ref_cnt + b, 0, sizeof(int), st));
+                HB_CK(cudaEventRecord(E.ev_[10 + 2 * b], st));
+                HB_CK(launch_solve_bucket(np, precision, v, ordinary, g, bcells, bucket_cnt + b, cnt[b], S.nb_rec,
+                                          S.nb_n, ind_value, S.pair64, S.pair32, mean, c0, steps, tol, out,
+                                          quad ? ref_cells + first : (esc_cells ? esc_cells + first : nullptr),
+                                          quad ? ref_cnt + b : esc_cnt + b, E.n_sm(), st));
+                HB_CK(cudaEventRecord(E.ev_[11 + 2 * b], st));
+                E.stats.launches += 1;
+            }
             HB_CK(cudaEventSynchronize(E.ev_[11 + 2 * b]));
             float t = 0.0f;
             HB_CK(cudaEventElapsedTime(&t, E.ev_[10 + 2 * b], E.ev_[11 + 2 * b]));
             ms[v] = t * 1e6 / (double)cnt[b];
-            E.stats.launches += 1;
         }
         tune_record(np, pl.f.m.type, precision, ms);
         HB_CK(cudaMemsetAsync(esc_cnt + b, 0, sizeof(int), st));

@@ -105,8 +105,12 @@ cudaError_t launch_resolve_ties_fast(const Geom &g, const int *tie_cells, const 
 // blocks with in-kernel classic refinement, FP64 384-thread blocks),
 // kVariantFoldNarrow (the same with 256-thread blocks and up to 255
 // registers); FP32-refined also kVariantQuad (four rows per lane, 384-thread
-// blocks, solve_quad.cu) and kVariantQuadNarrow (256-thread blocks). n 33-64
-// has one variant (kVariantFold: one warp per system, 256-thread blocks).
+// blocks, solve_quad.cu) and kVariantQuadNarrow (256-thread blocks), and for
+// n 17-32 kVariantTile (four rows per lane reading a union matrix the block
+// shares, solve_tile.cu; 384-thread blocks, one per SM) and kVariantTileNarrow
+// (192-thread blocks, two per SM). n 33-64: kVariantWide (one warp per system,
+// rows shifted in registers, rolled factorisation phases, solve_wide.cu) and
+// kVariantFold (one warp per system, fully unrolled, 256-thread blocks).
 enum SolveVariant : int
 {
     kVariantDefault = 0,
@@ -114,10 +118,16 @@ enum SolveVariant : int
     kVariantQuad = 2,
     kVariantFoldNarrow = 3,
     kVariantQuadNarrow = 4,
+    kVariantTile = 5,
+    kVariantTileNarrow = 6,
+    kVariantWide = 7,
 };
-constexpr int kVariantCount = 5;
+constexpr int kVariantCount = 8;
 // the four-rows-per-lane FP32 kernels queue failing systems for classic refinement
-inline bool is_quad_variant(int v) { return v == kVariantQuad || v == kVariantQuadNarrow; }
+inline bool is_quad_variant(int v)
+{
+    return v == kVariantQuad || v == kVariantQuadNarrow || v == kVariantTile || v == kVariantTileNarrow;
+}
 // the variant that runs for a (bucket, covariance type, precision) key
 int solve_variant(int np, int cov_type, int precision);
 // whether `variant` can run the key (kVariantDefault always can)

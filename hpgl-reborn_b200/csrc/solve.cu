@@ -50,6 +50,7 @@
 #include "engine.cuh"
 #include "kernels.h"
 #include "solve_common.cuh"
+#include "solve_quad.cuh" // static_for
 
 #include <cstdint>
 
@@ -188,9 +189,8 @@ __device__ __forceinline__ void fold_back(const FoldGrp<NP / 2> &fg, const float
     const float4 *Ma = reinterpret_cast<const float4 *>(M + fold_row<NP>(t));
     const float4 *Mb = reinterpret_cast<const float4 *>(M + fold_row<NP>(rb));
     float4 ma = make_float4(0, 0, 0, 0), mb = ma;
-#pragma unroll
-    for (int i = NP - 1; i >= 0; --i)
-    {
+    static_for<0, NP>([&](auto IC) {
+        constexpr int i = NP - 1 - decltype(IC)::value;
         if (i % 4 == 3)
         {
             ma = Ma[i / 4];
@@ -231,7 +231,7 @@ __device__ __forceinline__ void fold_back(const FoldGrp<NP / 2> &fg, const float
 #pragma unroll
             for (int q = 0; q < Q; ++q) acc_b[q] -= l * xi[q];
         }
-    }
+    });
 }
 
 // Forward substitution L y = rhs from the factor kept in M (the refinement
@@ -251,9 +251,8 @@ __device__ __forceinline__ void fold_forward(const FoldGrp<NP / 2> &fg, const fl
         ya[q] = 0.0f;
         yb[q] = 0.0f;
     }
-#pragma unroll
-    for (int j = 0; j < NP; ++j)
-    {
+    static_for<0, NP>([&](auto JC) {
+        constexpr int j = decltype(JC)::value;
         const float *Mj = M + fold_row<NP>(j);
         const float inv_j = rsqrtf(Mj[j]);
         float yj[Q];
@@ -289,7 +288,7 @@ __device__ __forceinline__ void fold_forward(const FoldGrp<NP / 2> &fg, const fl
 #pragma unroll
             for (int q = 0; q < Q; ++q) acc_b[q] -= l * yj[q];
         }
-    }
+    });
 }
 
 // FP64 residuals of both rows: res = rhs - A64 x, A64 rows gathered from the
@@ -515,9 +514,8 @@ __global__ void __launch_bounds__(TH, 1)
         }
         bool fail = false;
         float inv_a = 0.0f, inv_b = 0.0f;
-#pragma unroll
-        for (int j = 0; j < NP; ++j)
-        {
+        static_for<0, NP>([&](auto JC) {
+            constexpr int j = decltype(JC)::value;
             // row j of the packed matrix holds columns 4*(j/4) on
             float *Mj = M + fold_row<NP>(j);
             if (j < G)
@@ -586,7 +584,7 @@ __global__ void __launch_bounds__(TH, 1)
                     for (int q = 0; q < R; ++q) yb[q] = rhs_b[q] * inv_s;
                 }
             }
-        }
+        });
 
         // ---- back substitution and the dual-weighted FP64 correction of the forms
         float xsa[R], xsb[R];
@@ -874,9 +872,8 @@ __global__ void __launch_bounds__(TH, 1)
             yb[q] = 0.0;
         }
         bool fail = false;
-#pragma unroll
-        for (int j = 0; j < NP; ++j)
-        {
+        static_for<0, NP>([&](auto JC) {
+            constexpr int j = decltype(JC)::value;
             double *Mj = M + (j & 1) * LD;
             if (j < G)
             {
@@ -939,7 +936,7 @@ __global__ void __launch_bounds__(TH, 1)
 #pragma unroll
                 for (int q = 0; q < R; ++q) yb[q] = rhs_b[q] * inv_s;
             }
-        }
+        });
 
         // ---- forms (L^-1 u) . (L^-1 w); q: 0 = b, 1 = ones (OK), R-1 = v - mean
         constexpr int V = R - 1;
@@ -1034,6 +1031,11 @@ static cudaError_t launch_np(int precision, int variant, bool ordinary, const Ge
             return ordinary ? launch_one<NP, double, true, false, 384>(HB_ARGS)
                             : launch_one<NP, double, false, false, 384>(HB_ARGS);
         }
+        if constexpr (NP == 32)
+        {
+            if (variant == kVariantTile || variant == kVariantTileNarrow)
+                return launch_solve_tile(NP, ordinary, variant == kVariantTile ? 384 : 192, HB_ARGS);
+        }
         if (variant == kVariantQuad || variant == kVariantQuadNarrow || variant == kVariantDefault)
             return launch_solve_quad(NP, ordinary, variant == kVariantQuadNarrow ? 256 : 384, HB_ARGS);
         if (variant == kVariantFoldNarrow)
@@ -1044,7 +1046,7 @@ static cudaError_t launch_np(int precision, int variant, bool ordinary, const Ge
     }
     else
     {
-        (void)variant;
+        if (variant != kVariantFold) return launch_solve_wide(precision, ordinary, HB_ARGS);
         if (precision == 0)
             return ordinary ? launch_one<NP, double, true, false, 256>(HB_ARGS)
                             : launch_one<NP, double, false, false, 256>(HB_ARGS);
@@ -1057,8 +1059,10 @@ static cudaError_t launch_np(int precision, int variant, bool ordinary, const Ge
 bool solve_variant_valid(int np, int precision, int variant)
 {
     if (variant == kVariantDefault) return true;
-    if (np > 32) return variant == kVariantFold;
-    if (precision == 1) return variant >= kVariantFold && variant <= kVariantQuadNarrow;
+    if (np > 32) return variant == kVariantFold || variant == kVariantWide;
+    if (precision == 1)
+        return (variant >= kVariantFold && variant <= kVariantQuadNarrow) ||
+               ((variant == kVariantTile || variant == kVariantTileNarrow) && np == 32);
     return variant == kVariantFold || variant == kVariantFoldNarrow;
 }
 

@@ -89,6 +89,16 @@ static cudaError_t launch_kernel(K kern, int threads, size_t smem, int max_items
 namespace hb
 {
 // FP32-refined solves of up to 32 neighbours, four rows per lane (solve_quad.cu)
+// FP32-refined solves of 17 to 32 neighbours from a union matrix shared by
+// the block (solve_tile.cu; threads per block: 384 or 192)
+cudaError_t launch_solve_tile(int np, bool ordinary, int threads, const Geom &g, const int2 *cells, const int *n_items,
+                              int max_items, const int2 *nb_rec, int ind_value, const float *pair32,
+                              const SolveParams &P, int n_sm, cudaStream_t st);
+// FP32-refined (precision 1) and FP64-plain solves of 33 to 64 neighbours,
+// one warp per system (solve_wide.cu)
+cudaError_t launch_solve_wide(int precision, bool ordinary, const Geom &g, const int2 *cells, const int *n_items,
+                              int max_items, const int2 *nb_rec, int ind_value, const float *pair32,
+                              const SolveParams &P, int n_sm, cudaStream_t st);
 // (threads per block: 384 or 256)
 cudaError_t launch_solve_quad(int np, bool ordinary, int threads, const Geom &g, const int2 *cells,
                               const int *n_items, int max_items, const int2 *nb_rec, int ind_value,

@@ -49,7 +49,8 @@ int bucket_index(int np)
 // the built-in pick of each key
 int builtin_variant(int np, int precision)
 {
-    if (precision == 1 && np <= 32) return kVariantQuad;
+    if (np > 32) return kVariantWide;
+    if (precision == 1) return kVariantQuad;
     return kVariantFold;
 }
 
@@ -58,7 +59,8 @@ bool key_ok(int b, int cov_type, int precision)
     return b >= 0 && precision >= 0 && precision <= 1 && cov_type >= 0 && cov_type < kCovTypes;
 }
 
-const char *kVariantNames[kVariantCount] = {"default", "fold", "quad", "fold_narrow", "quad_narrow"};
+const char *kVariantNames[kVariantCount] = {"default", "fold", "quad", "fold_narrow", "quad_narrow", "tile",
+                                            "tile_narrow", "wide"};
 } // namespace
 
 int solve_variant(int np, int cov_type, int precision)

@@ -305,9 +305,11 @@ STATS_KEYS = (["total_ms", "search_ms", "solve_ms", "tie_cells", "template_cells
                  "sgs_flops", "refined_cells"])
 
 
-VARIANT_DEFAULT, VARIANT_FOLD, VARIANT_QUAD, VARIANT_FOLD_NARROW, VARIANT_QUAD_NARROW = 0, 1, 2, 3, 4
+VARIANT_DEFAULT, VARIANT_FOLD, VARIANT_QUAD, VARIANT_FOLD_NARROW, VARIANT_QUAD_NARROW, VARIANT_TILE = 0, 1, 2, 3, 4, 5
+VARIANT_TILE_NARROW, VARIANT_WIDE = 6, 7
 VARIANT_NAMES = {VARIANT_DEFAULT: "default", VARIANT_FOLD: "fold", VARIANT_QUAD: "quad",
-                 VARIANT_FOLD_NARROW: "fold_narrow", VARIANT_QUAD_NARROW: "quad_narrow"}
+                 VARIANT_FOLD_NARROW: "fold_narrow", VARIANT_QUAD_NARROW: "quad_narrow", VARIANT_TILE: "tile",
+                 VARIANT_TILE_NARROW: "tile_narrow", VARIANT_WIDE: "wide"}
 
 
 def solve_variant(bucket_np: int, cov_type: int, precision: int, variant: int = None) -> int:

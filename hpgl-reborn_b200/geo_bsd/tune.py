@@ -10,8 +10,9 @@ starts from built-in picks; this module
   ``save_cache``; the package loads ``tune_cache.json`` beside this file at
   import, or the file named by ``HPGL_B200_TUNE_CACHE``, ``none`` for none);
 * switches the engine's tuning mode (``mode``), in which the first bucket of
-  at least 20000 systems of a key without a setting runs once with every
-  variant the key can run and the fastest becomes its setting;
+  at least 20000 systems of a key without a setting runs with every variant
+  the key can run (each twice, the second run timed) and the fastest becomes
+  its setting;
 * rebuilds the cache (``autotune``): one synthetic ordinary-kriging grid per
   bucket and covariance type, run in tuning mode for each precision.
 

@@ -329,6 +329,17 @@ int hpgl_b200_last_stats(double *out, int cap);
  *                                  per lane, 384-thread blocks; failing systems
  *                                  go on to FOLD's refinement, then to FP64
  *   HPGL_B200_VARIANT_QUAD_NARROW  QUAD in 256-thread blocks
+ *   HPGL_B200_VARIANT_TILE         FP32_REFINED, bucket_np == 32: QUAD reading
+ *                                  the covariances from a union matrix that the
+ *                                  block builds in shared memory for the 48
+ *                                  consecutive cells it solves at once
+ *   HPGL_B200_VARIANT_TILE_NARROW  TILE in 192-thread blocks, two a
+ *                                  multiprocessor, 24 cells at once
+ *   HPGL_B200_VARIANT_WIDE         bucket_np == 64 (the built-in pick): one
+ *                                  warp per system, the factorisation's steps
+ *                                  rolled in phases of eight over rows kept
+ *                                  shifted in registers (FOLD is the same
+ *                                  layout fully unrolled)
  * hpgl_b200_solve_variant sets a key and returns its previous setting, or
  * HPGL_B200_EINVAL for an invalid key or a variant the key cannot run;
  * hpgl_b200_solve_variant_get returns the variant a key runs now. Results of
@@ -338,12 +349,16 @@ int hpgl_b200_last_stats(double *out, int cap);
 #define HPGL_B200_VARIANT_QUAD 2
 #define HPGL_B200_VARIANT_FOLD_NARROW 3
 #define HPGL_B200_VARIANT_QUAD_NARROW 4
+#define HPGL_B200_VARIANT_TILE 5
+#define HPGL_B200_VARIANT_TILE_NARROW 6
+#define HPGL_B200_VARIANT_WIDE 7
 int hpgl_b200_solve_variant(int bucket_np, int cov_type, int precision, int variant);
 int hpgl_b200_solve_variant_get(int bucket_np, int cov_type, int precision);
 /* The tuner behind those keys (no counterpart in the reference).
  * hpgl_b200_tune_mode(1): a key without a setting is timed the first time a
- * call meets a bucket of at least 20000 of its systems: that bucket runs once
- * with every variant the key can run, the fastest becomes the key's setting
+ * call meets a bucket of at least 20000 of its systems: that bucket runs with
+ * every variant the key can run (twice each, the second run timed), the
+ * fastest becomes the key's setting
  * and produces the call's outputs; mode 0 (the default) uses the settings as
  * they are. Returns the previous mode.
  * hpgl_b200_tune_load / hpgl_b200_tune_save read / write the settings as a

@@ -6,7 +6,8 @@
   oracle's statuses and within the precision's error bound).
 * Every variant the table can pick gives the same statuses and meets the
   error bound (FP32-refined 1e-6, FP64 plain 1e-10 against the FP64 plain
-  built-in pick).
+  built-in pick), for the buckets up to 32 on the benchmark's model and for
+  the 33-64 bucket on the clustered grid.
 * The picks of the committed cache are not slower than the built-in picks
   on the benchmark's model (the bucket's kernel time, median of five calls,
   within 5 % for timing noise).
@@ -56,7 +57,7 @@ def test_tuning_mode_sets_the_key_and_keeps_correct_outputs(precision):
     assert H.rel_err(e["var"][ok], ref["var"][ok]) <= tol
 
 
-@pytest.mark.parametrize("precision,variants", [(1, (1, 2, 3, 4)), (0, (1, 3))])
+@pytest.mark.parametrize("precision,variants", [(1, (1, 2, 3, 4, 5, 6)), (0, (1, 3))])
 def test_every_variant_meets_the_bound(precision, variants):
     wl = WL.sk_ok_large(0.3)
     ref = H.engine_cont(0, wl, precision=0)
@@ -64,7 +65,8 @@ def test_every_variant_meets_the_bound(precision, variants):
     tol = 1e-10 if precision == 0 else 1e-6
     for v in variants:
         for b in (8, 16, 32):
-            W.solve_variant(b, wl.cov.cov_type, precision, v)
+            if b == 32 or v not in (W.VARIANT_TILE, W.VARIANT_TILE_NARROW):
+                W.solve_variant(b, wl.cov.cov_type, precision, v)
         for kind in (0, 1):
             r = ref if kind == 0 else H.engine_cont(1, wl, precision=0)
             e = H.engine_cont(kind, wl, precision=precision)
@@ -73,6 +75,31 @@ def test_every_variant_meets_the_bound(precision, variants):
             assert H.rel_err(e["est"][okk], r["est"][okk]) <= tol, (v, kind)
             assert H.rel_err(e["var"][okk], r["var"][okk]) <= tol, (v, kind)
     assert ok.any()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_bucket64_variants_meet_the_bound(precision):
+    """The 33-64 bucket's two variants (WIDE, the built-in pick, and FOLD) on
+    the clustered Gaussian grid with nugget 1e-3 (k = 64): statuses identical
+    and estimates / variances within the precision's bound of the FP64
+    built-in pick; escalated FP32 systems are re-solved in FP64."""
+    wl = WL.clustered(0.25)
+    cov = wl.cov.cov_type
+    assert W.solve_variant(64, cov, precision) == W.VARIANT_WIDE
+    ref = H.engine_cont(0, wl, precision=0)
+    assert ref["stats"]["bucket_items_3"] > 1000
+    ok = ref["status"] == 0
+    assert ok.any()
+    tol = 1e-10 if precision == 0 else 1e-6
+    for v in (W.VARIANT_WIDE, W.VARIANT_FOLD):
+        W.solve_variant(64, cov, precision, v)
+        for kind in (0, 1):
+            r = ref if kind == 0 else H.engine_cont(1, wl, precision=0)
+            e = H.engine_cont(kind, wl, precision=precision)
+            np.testing.assert_array_equal(e["status"], r["status"])
+            okk = r["status"] == 0
+            assert H.rel_err(e["est"][okk], r["est"][okk]) <= tol, (v, kind)
+            assert H.rel_err(e["var"][okk], r["var"][okk]) <= tol, (v, kind)
 
 
 @pytest.mark.parametrize("precision", [0, 1])

@@ -25,7 +25,8 @@ def _restore_table():
 
 def test_builtin_picks_and_overrides():
     assert W.solve_variant(32, 1, W.FP32_REFINED) == W.VARIANT_QUAD
-    assert W.solve_variant(64, 1, W.FP32_REFINED) == W.VARIANT_FOLD
+    assert W.solve_variant(64, 1, W.FP32_REFINED) == W.VARIANT_WIDE
+    assert W.solve_variant(64, 1, W.FP64_PLAIN) == W.VARIANT_WIDE
     assert W.solve_variant(32, 1, W.FP64_PLAIN) == W.VARIANT_FOLD
     assert W.solve_variant(16, 2, W.FP64_PLAIN, W.VARIANT_FOLD_NARROW) == W.VARIANT_DEFAULT
     assert W.solve_variant(16, 2, W.FP64_PLAIN) == W.VARIANT_FOLD_NARROW
@@ -33,7 +34,10 @@ def test_builtin_picks_and_overrides():
     with pytest.raises(ValueError):
         W.solve_variant(32, 1, W.FP64_PLAIN, W.VARIANT_QUAD)  # four rows per lane is FP32 only
     with pytest.raises(ValueError):
-        W.solve_variant(64, 1, W.FP32_REFINED, W.VARIANT_QUAD_NARROW)  # bucket 64 has one variant
+        W.solve_variant(64, 1, W.FP32_REFINED, W.VARIANT_QUAD_NARROW)  # bucket 64: WIDE and FOLD only
+    assert W.solve_variant(64, 1, W.FP32_REFINED) == W.VARIANT_WIDE
+    with pytest.raises(ValueError):
+        W.solve_variant(32, 1, W.FP32_REFINED, W.VARIANT_WIDE)
     with pytest.raises(ValueError):
         W.solve_variant(24, 1, W.FP32_REFINED, W.VARIANT_FOLD)  # not a bucket
     with pytest.raises(ValueError):
