@@ -20,7 +20,9 @@
 // as long as on anything else.
 //
 // k_solve_wide64: FP64 plain, forward substitution only (the forms are
-// (L^-1 u) . (L^-1 w)). k_solve_wide32: FP32 factorisation and substitutions,
+// (L^-1 u) . (L^-1 w)). k_solve_wide32: FP32 factorisation (two steps a body
+// as a rank-2 update, the rows as float2 pairs shifted by two, so that the
+// update runs as packed FP32x2 FMAs) and substitutions,
 // the bilinear forms corrected with the FP64 dual-weighted residual from the
 // lower triangle (as the other FP32-refined kernels do); a system whose check
 // fails is queued for the FP64 kernel.
@@ -54,7 +56,8 @@ template <typename T, int R, bool BACK>
 struct WideSmem
 {
     static constexpr int LDW = wide_ldw<T, R>();
-    static constexpr size_t w_bytes = (size_t)2 * LDW * sizeof(T);
+    // two broadcast buffers in turn; FP32 (BACK) broadcasts two columns a body
+    static constexpr size_t w_bytes = (size_t)(BACK ? 4 : 2) * LDW * sizeof(T);
     static constexpr size_t lin_off = w_bytes;
     // (FP32) the factor's columns before scaling, for the back substitution
     static constexpr size_t lc_off = lin_off + kWideNP * sizeof(int);
@@ -187,6 +190,195 @@ __device__ __forceinline__ bool wide_factor(T (&ra)[32], T (&rbv)[kWideNP], T (&
 #pragma unroll
                 for (int q = 0; q < R; ++q) yb[q] = rhs_b[q] * inv_s;
             }
+        }
+    });
+    return fail;
+}
+
+// FP32: r[m] = r[m + 1] - s0 (V[2m + 2], V[2m + 3]) - s1 (U[2m + 2], U[2m + 3])
+// for pairs m < L - 1 (L <= N): two steps' updates of the lane's row, shifted
+// by two entries, as packed FP32x2 FMAs on aligned register pairs.
+template <int L, int N>
+__device__ __forceinline__ void wide_shift2(float2 (&r)[N], float s0, float s1, const float *V, const float *U)
+{
+    if constexpr (L > 1)
+    {
+        const float2 n0 = make_float2(-s0, -s0), n1 = make_float2(-s1, -s1);
+        static_for<0, L / 2 + 1>([&](auto KC) {
+            constexpr int k = decltype(KC)::value; // 16-byte chunk k holds pairs 2k, 2k + 1
+            constexpr bool lo = 2 * k - 1 >= 0 && 2 * k - 1 < L - 1, hi = 2 * k < L - 1;
+            if constexpr (lo || hi)
+            {
+                const float4 v = reinterpret_cast<const float4 *>(V)[k];
+                const float4 u = reinterpret_cast<const float4 *>(U)[k];
+                if constexpr (lo)
+                {
+                    constexpr int m = 2 * k - 1;
+                    r[m] = __ffma2_rn(n1, make_float2(u.x, u.y), __ffma2_rn(n0, make_float2(v.x, v.y), r[m + 1]));
+                }
+                if constexpr (hi)
+                {
+                    constexpr int m = 2 * k;
+                    r[m] = __ffma2_rn(n1, make_float2(u.z, u.w), __ffma2_rn(n0, make_float2(v.z, v.w), r[m + 1]));
+                }
+            }
+        });
+    }
+}
+
+// The FP32 factorisation two steps at a time (a rank-2 update), rows held as
+// float2 pairs shifted by two per body, so both updates run as packed FP32x2
+// FMAs on aligned pairs. Column j is broadcast from row j on (V[i] = A(j + i,
+// j), the diagonal at V[0]) and column j + 1, after step j's update, from row
+// j on as well (U[i] = A'(j + i, j + 1), its diagonal at U[1]): the entries a
+// pair of rows needs then sit in aligned pairs of both buffers. Results,
+// outputs and the kept columns in LC are those of wide_factor<float, R, true>
+// (the same FMAs in the same order).
+template <int R, int PH>
+__device__ __forceinline__ bool wide_factor2(float2 (&ra)[16], float2 (&rb)[32], float (&rhs_a)[R],
+                                             float (&rhs_b)[R], float (&ya)[R], float (&yb)[R], float &inv_a,
+                                             float &inv_b, int t, float *Wbuf, float *LC)
+{
+    constexpr int NP = kWideNP;
+    constexpr int LDW = wide_ldw<float, R>();
+    const int b = NP - 1 - t;
+    bool fail = false;
+    static_for<0, NP / PH>([&](auto PC) {
+        constexpr int p = decltype(PC)::value;
+        constexpr int LA = 32 - PH * p > 0 ? (32 - PH * p) / 2 : 0; // pairs
+        constexpr int LB = (NP - PH * p) / 2;
+#pragma unroll 1
+        for (int jj = 0; jj < PH; jj += 2)
+        {
+            const int j = PH * p + jj;
+            float *V = Wbuf + ((j >> 1) & 1) * 2 * LDW;
+            float *U = V + LDW;
+            // ---- step j
+            if constexpr (LA > 0)
+            {
+                if (t >= j)
+                {
+                    V[t - j] = ra[0].x;
+                    LC[wide_col(j) + t - j] = ra[0].x;
+                }
+                if (t == j)
+                {
+#pragma unroll
+                    for (int q = 0; q < R; ++q) V[NP + q] = rhs_a[q];
+                }
+            }
+            if (b >= j)
+            {
+                V[b - j] = rb[0].x;
+                LC[wide_col(j) + b - j] = rb[0].x;
+            }
+            if (b == j)
+            {
+#pragma unroll
+                for (int q = 0; q < R; ++q) V[NP + q] = rhs_b[q];
+            }
+            __syncwarp();
+            const float d0 = V[0];
+            fail |= !(d0 > 0.0f);
+            const float i0 = rsqrtf(d0);
+            const float i0s = i0 * i0;
+            const float v1 = V[1];
+            float vr[R];
+#pragma unroll
+            for (int q = 0; q < R; ++q) vr[q] = V[NP + q];
+            const float sb0 = rb[0].x * i0s;
+            const float cb = rb[0].y - sb0 * v1; // A'(b, j + 1)
+            if (b > j)
+            {
+#pragma unroll
+                for (int q = 0; q < R; ++q) rhs_b[q] -= sb0 * vr[q];
+            }
+            if (b == j)
+            {
+                inv_b = i0;
+#pragma unroll
+                for (int q = 0; q < R; ++q) yb[q] = rhs_b[q] * i0;
+            }
+            float sa0 = 0.0f, ca = 0.0f;
+            if constexpr (LA > 0)
+            {
+                sa0 = ra[0].x * i0s;
+                ca = ra[0].y - sa0 * v1;
+                if (t > j)
+                {
+#pragma unroll
+                    for (int q = 0; q < R; ++q) rhs_a[q] -= sa0 * vr[q];
+                }
+                if (t == j)
+                {
+                    inv_a = i0;
+#pragma unroll
+                    for (int q = 0; q < R; ++q) ya[q] = rhs_a[q] * i0;
+                }
+            }
+            // ---- step j + 1: column j + 1 after step j
+            if constexpr (LA > 0)
+            {
+                if (t > j)
+                {
+                    U[t - j] = ca;
+                    LC[wide_col(j + 1) + t - j - 1] = ca;
+                }
+                if (t == j + 1)
+                {
+#pragma unroll
+                    for (int q = 0; q < R; ++q) U[NP + q] = rhs_a[q];
+                }
+            }
+            if (b > j)
+            {
+                U[b - j] = cb;
+                LC[wide_col(j + 1) + b - j - 1] = cb;
+            }
+            if (b == j + 1)
+            {
+#pragma unroll
+                for (int q = 0; q < R; ++q) U[NP + q] = rhs_b[q];
+            }
+            __syncwarp();
+            const float d1 = U[1];
+            fail |= !(d1 > 0.0f);
+            const float i1 = rsqrtf(d1);
+            const float i1s = i1 * i1;
+            float ur[R];
+#pragma unroll
+            for (int q = 0; q < R; ++q) ur[q] = U[NP + q];
+            const float sb1 = cb * i1s;
+            if (b > j + 1)
+            {
+#pragma unroll
+                for (int q = 0; q < R; ++q) rhs_b[q] -= sb1 * ur[q];
+            }
+            if (b == j + 1)
+            {
+                inv_b = i1;
+#pragma unroll
+                for (int q = 0; q < R; ++q) yb[q] = rhs_b[q] * i1;
+            }
+            float sa1 = 0.0f;
+            if constexpr (LA > 0)
+            {
+                sa1 = ca * i1s;
+                if (t > j + 1)
+                {
+#pragma unroll
+                    for (int q = 0; q < R; ++q) rhs_a[q] -= sa1 * ur[q];
+                }
+                if (t == j + 1)
+                {
+                    inv_a = i1;
+#pragma unroll
+                    for (int q = 0; q < R; ++q) ya[q] = rhs_a[q] * i1;
+                }
+            }
+            // ---- both updates, the rows shifted by two
+            wide_shift2<LB>(rb, sb0, sb1, V, U);
+            if constexpr (LA > 0) wide_shift2<LA>(ra, sa0, sa1, V, U);
         }
     });
     return fail;
@@ -350,14 +542,17 @@ __global__ void __launch_bounds__(TH, 1)
         __syncwarp();
 
         // ---- assembly from the float pair table
-        float ra[32], rbv[NP];
+        float2 ra[16], rbv[NP / 2];
 #pragma unroll
         for (int c = 0; c < 32; ++c)
         {
             float a = 0.0f;
             if (live_a && c <= t) a = __ldg(p32c + lin_a - LIN[c]);
             if (!live_a && c == t) a = 1.0f;
-            ra[c] = a;
+            if (c & 1)
+                ra[c >> 1].y = a;
+            else
+                ra[c >> 1].x = a;
         }
 #pragma unroll
         for (int c = 0; c < NP; ++c)
@@ -365,7 +560,10 @@ __global__ void __launch_bounds__(TH, 1)
             float a = 0.0f;
             if (live_b && c <= b) a = __ldg(p32c + lin_b - LIN[c]);
             if (!live_b && c == b) a = 1.0f;
-            rbv[c] = a;
+            if (c & 1)
+                rbv[c >> 1].y = a;
+            else
+                rbv[c >> 1].x = a;
         }
         const double b64_a = live_a ? __ldg(p64c + lin_a) : 0.0;
         const double b64_b = live_b ? __ldg(p64c + lin_b) : 0.0;
@@ -382,7 +580,7 @@ __global__ void __launch_bounds__(TH, 1)
 #pragma unroll
         for (int q = 0; q < R; ++q) ya[q] = yb[q] = 0.0f;
         float inv_a = 0.0f, inv_b = 0.0f;
-        const bool fail = wide_factor<float, R, true>(ra, rbv, rhs_a, rhs_b, ya, yb, inv_a, inv_b, t, Wbuf, LC);
+        const bool fail = wide_factor2<R, kWidePhase>(ra, rbv, rhs_a, rhs_b, ya, yb, inv_a, inv_b, t, Wbuf, LC);
         __syncwarp();
 
         // ---- back substitution L^T x = y from the kept columns: lane t reads
@@ -455,21 +653,30 @@ __global__ void __launch_bounds__(TH, 1)
 #pragma unroll
         for (int q = 0; q < R; ++q) Pa[q] = Pb[q] = 0.0;
         const double *base_a = p64c + lin_a, *base_b = p64c + lin_b;
-#pragma unroll 4
-        for (int c = 0; c < NP; ++c)
+        // (eight columns a batch: the batch's sixteen gathers in flight together;
+        // every LIN and X entry of the 64 rows is set, padding rows to zero)
+        constexpr int PB = 8;
+#pragma unroll 1
+        for (int c0 = 0; c0 < my_n; c0 += PB)
         {
-            if (c < my_n)
+            double pa[PB], pb[PB];
+#pragma unroll
+            for (int e = 0; e < PB; ++e)
             {
+                const int c = c0 + e;
                 const int l = LIN[c];
-                const bool ga = live_a && c < t, gbb = live_b && c < b;
-                const double pa = ga ? __ldg(base_a - l) : 0.0;
-                const double pb = gbb ? __ldg(base_b - l) : 0.0;
+                pa[e] = live_a && c < t ? __ldg(base_a - l) : 0.0;
+                pb[e] = live_b && c < b ? __ldg(base_b - l) : 0.0;
+            }
+#pragma unroll
+            for (int e = 0; e < PB; ++e)
+            {
 #pragma unroll
                 for (int q = 0; q < R; ++q)
                 {
-                    const double xc = X[q * NP + c];
-                    Pa[q] = fma(pa, xc, Pa[q]);
-                    Pb[q] = fma(pb, xc, Pb[q]);
+                    const double xc = X[q * NP + c0 + e];
+                    Pa[q] = fma(pa[e], xc, Pa[q]);
+                    Pb[q] = fma(pb[e], xc, Pb[q]);
                 }
             }
         }
