@@ -142,6 +142,21 @@ struct FoldSmem
     static constexpr size_t bytes = raw + (size_t)((4 * (NP / 2) - (int)(raw % 128) + 128) % 128);
 };
 
+// The step loops of the folded kernels: unrolled by the compiler up to 32
+// rows; at 64, where its unroller gives up (and the rows would go to local
+// memory), instantiated step by step.
+template <int NP, typename F>
+__device__ __forceinline__ void fold_steps(F &&f)
+{
+    if constexpr (NP > 32)
+        static_for<0, NP>([&](auto JC) { f(decltype(JC)::value); });
+    else
+    {
+#pragma unroll
+        for (int j = 0; j < NP; ++j) f(j);
+    }
+}
+
 template <int G>
 struct FoldGrp
 {
@@ -189,8 +204,8 @@ __device__ __forceinline__ void fold_back(const FoldGrp<NP / 2> &fg, const float
     const float4 *Ma = reinterpret_cast<const float4 *>(M + fold_row<NP>(t));
     const float4 *Mb = reinterpret_cast<const float4 *>(M + fold_row<NP>(rb));
     float4 ma = make_float4(0, 0, 0, 0), mb = ma;
-    static_for<0, NP>([&](auto IC) {
-        constexpr int i = NP - 1 - decltype(IC)::value;
+    fold_steps<NP>([&](const int ic) {
+        const int i = NP - 1 - ic;
         if (i % 4 == 3)
         {
             ma = Ma[i / 4];
@@ -251,8 +266,7 @@ __device__ __forceinline__ void fold_forward(const FoldGrp<NP / 2> &fg, const fl
         ya[q] = 0.0f;
         yb[q] = 0.0f;
     }
-    static_for<0, NP>([&](auto JC) {
-        constexpr int j = decltype(JC)::value;
+    fold_steps<NP>([&](const int j) {
         const float *Mj = M + fold_row<NP>(j);
         const float inv_j = rsqrtf(Mj[j]);
         float yj[Q];
@@ -514,8 +528,7 @@ __global__ void __launch_bounds__(TH, 1)
         }
         bool fail = false;
         float inv_a = 0.0f, inv_b = 0.0f;
-        static_for<0, NP>([&](auto JC) {
-            constexpr int j = decltype(JC)::value;
+        fold_steps<NP>([&](const int j) {
             // row j of the packed matrix holds columns 4*(j/4) on
             float *Mj = M + fold_row<NP>(j);
             if (j < G)
@@ -872,8 +885,7 @@ __global__ void __launch_bounds__(TH, 1)
             yb[q] = 0.0;
         }
         bool fail = false;
-        static_for<0, NP>([&](auto JC) {
-            constexpr int j = decltype(JC)::value;
+        fold_steps<NP>([&](const int j) {
             double *Mj = M + (j & 1) * LD;
             if (j < G)
             {
