@@ -853,7 +853,7 @@ def bucket_kernel(W, b, cov_type, precision, ordinary):
     v = W.solve_variant(np_, cov_type, precision) if hasattr(W, "solve_variant") else 1
     kind = "ordinary" if ordinary else "simple"
     if np_ == 64 and v in (getattr(W, "VARIANT_WIDE", -1), W.VARIANT_DEFAULT):
-        th, pr = (256, "FP64 plain") if precision == 0 else (384, "FP32 refined")
+        th, pr = (256, "FP64 plain") if precision == 0 else (256, "FP32 refined")
         return f"k_solve_wide{64 if precision == 0 else 32}<{kind}, {th}> ({pr}, one warp per system, rolled phases)"
     if precision == 0:
         th = 384 if (np_ <= 32 and v == W.VARIANT_FOLD) else 256

@@ -720,15 +720,16 @@ __global__ void __launch_bounds__(TH, 1)
     }
 }
 
-// Threads per block: FP64 256 (up to 255 registers: the rows take 192), FP32
-// 384 (up to 168).
+// Threads per block: 256 (up to 255 registers; the FP64 rows take 192). FP32
+// in 384-thread blocks (168 registers) spilled in the factorisation's body and
+// ran 6 % slower (213 against 200 ms on the clustered 512x512x64 grid).
 template <bool ORD, bool F64>
 static cudaError_t launch_wide_one(const Geom &g, const int2 *cells, const int *n_items, int max_items,
                                    const int2 *nb_rec, int ind_value, const float *pair32, const SolveParams &P,
                                    int n_sm, cudaStream_t st)
 {
     constexpr int R = ORD ? 3 : 2;
-    constexpr int TH = F64 ? 256 : 384;
+    constexpr int TH = 256;
     const size_t smem = (F64 ? WideSmem<double, R, false>::bytes : WideSmem<float, R, true>::bytes) * (TH / 32);
     int blocks = 0;
     if constexpr (F64)
