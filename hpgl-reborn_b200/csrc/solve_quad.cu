@@ -54,8 +54,7 @@ struct QuadSmem
     static constexpr int G = NP / 4;
     static constexpr int LDB = NP + 4; // floats per broadcast row: NP entries, then 4 right-hand sides
     static constexpr size_t lin_off = (size_t)2 * LDB * sizeof(float);
-    static constexpr size_t x_off = (lin_off + NP * sizeof(int) + 15) / 16 * 16;
-    static constexpr size_t rec_off = x_off + (size_t)R * NP * sizeof(double);
+    static constexpr size_t rec_off = (lin_off + NP * sizeof(int) + 15) / 16 * 16;
     static constexpr size_t raw = rec_off + (size_t)2 * NP * sizeof(int2);
     // Systems of one warp sit 4 G bytes (at least 16) apart modulo 128, so the
     // rows their lanes write at each step fall on distinct banks.
@@ -84,7 +83,6 @@ __global__ void __launch_bounds__(TH, 1)
     unsigned char *sb = smem + SM::bytes * (warp * SPW + h);
     float *B = reinterpret_cast<float *>(sb);
     int *LIN = reinterpret_cast<int *>(sb + SM::lin_off);
-    double *X = reinterpret_cast<double *>(sb + SM::x_off);
     int2 *REC = reinterpret_cast<int2 *>(sb + SM::rec_off); // two sets of NP records, in turn
     const int rows[4] = {t, H - 1 - t, H + t, NP - 1 - t};
     const long long pc = P.pc;
@@ -144,57 +142,33 @@ __global__ void __launch_bounds__(TH, 1)
         float inv[4] = {0.0f, 0.0f, 0.0f, 0.0f};
         const bool fail = q_factor<NP, R>(A, rhs, inv, rows, t, B);
         __syncwarp();
-        q_back<NP, R>(A, rows, inv, t, B, rhs);
-
-        // ---- the dual-weighted FP64 correction of the bilinear forms
+        // ---- back substitution with the correction's FP64 row sums
+        // x_u^T A x_w = sum_r ( A_rr u_r w_r + u_r P_w(r) + w_r P_u(r) ), P_w(r) = sum_{c<r} A_rc w_c
         bool live[4];
         int lin[4];
-        double b64[4], vc[4], one[4], x[4][R];
 #pragma unroll
         for (int k = 0; k < 4; ++k)
         {
             live[k] = rows[k] < my_n;
             lin[k] = LIN[rows[k]];
-            b64[k] = live[k] ? __ldg(p64c + lin[k]) : 0.0;
-            vc[k] = centred_value(live[k], __int_as_float(rec[rows[k]].y), ind_value, P.mf);
-            one[k] = live[k] ? 1.0 : 0.0;
-#pragma unroll
-            for (int q = 0; q < R; ++q)
-            {
-                x[k][q] = (double)rhs[k][q];
-                X[q * NP + rows[k]] = x[k][q];
-            }
         }
-        __syncwarp();
-        // x_u^T A x_w = sum_r ( A_rr u_r w_r + u_r P_w(r) + w_r P_u(r) ), P_w(r) = sum_{c<r} A_rc w_c
         double Pk[4][R];
 #pragma unroll
         for (int k = 0; k < 4; ++k)
 #pragma unroll
             for (int q = 0; q < R; ++q) Pk[k][q] = 0.0;
+        q_back_p<NP, R, 2>(A, rows, inv, t, B, rhs, p64c, lin, LIN, live, Pk);
+
+        // ---- the dual-weighted FP64 correction of the bilinear forms
+        double b64[4], vc[4], one[4], x[4][R];
 #pragma unroll
-        for (int c2 = 0; c2 < NP / 2; ++c2)
+        for (int k = 0; k < 4; ++k)
         {
-            double2 xc2[R];
+            b64[k] = live[k] ? __ldg(p64c + lin[k]) : 0.0;
+            vc[k] = centred_value(live[k], __int_as_float(rec[rows[k]].y), ind_value, P.mf);
+            one[k] = live[k] ? 1.0 : 0.0;
 #pragma unroll
-            for (int q = 0; q < R; ++q) xc2[q] = reinterpret_cast<const double2 *>(X + q * NP)[c2];
-            const int2 l2 = reinterpret_cast<const int2 *>(LIN)[c2];
-#pragma unroll
-            for (int e = 0; e < 2; ++e)
-            {
-                const int c = 2 * c2 + e;
-                const int l = e == 0 ? l2.x : l2.y;
-#pragma unroll
-                for (int k = 0; k < 4; ++k)
-                {
-                    if (c < q_hi<NP>(k) && live[k] && c < rows[k])
-                    {
-                        const double a = __ldg(p64c + lin[k] - l);
-#pragma unroll
-                        for (int q = 0; q < R; ++q) Pk[k][q] = fma(a, e == 0 ? xc2[q].x : xc2[q].y, Pk[k][q]);
-                    }
-                }
-            }
+            for (int q = 0; q < R; ++q) x[k][q] = (double)rhs[k][q];
         }
         auto bil = [&](int u, int w) {
             double sacc = 0.0;

@@ -101,7 +101,7 @@ __device__ __forceinline__ void decode_lin(const Geom &g, int lin, int &dx, int 
     dz = z;
 }
 
-// Back substitution L^T x = y (q_back of solve_quad.cuh) with the correction's
+// Back substitution L^T x = y (q_back_p of solve_quad.cuh) with the correction's
 // FP64 row sums P_k = sum_{c < r_k} A64[r_k][c] x_c accumulated as each x_c
 // is shuffled: A64[r_k][c] = um[rb[k] + u_c], u_c the union index of row c.
 template <int NP, int Q>
