@@ -19,8 +19,7 @@
 //     kernel reads is written earlier in the same call, so nothing carries over
 //     between calls;
 //   * the first call on a device looks the array's device address up
-//     (cudaGetSymbolAddress) with that device current and caches it; make that
-//     first call before any stream capture;
+//     (cudaGetSymbolAddress) with that device current and caches it;
 //   * with lazy module loading (CUDA's default since 12.2) the device holds
 //     the array only from the moment this file's device code is loaded onto
 //     it, which the first call's set-up forces (cudaFuncGetAttributes on the

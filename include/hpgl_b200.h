@@ -380,8 +380,8 @@ void hpgl_b200_tune_reset(void);
  * call never allocates or frees device memory. At most 128 neighbours
  * (HPGL_B200_ELIMIT beyond). Calls share the array: calls that overlap on the
  * GPU race and must be serialised by the caller. The first call on a device
- * looks the array's address up (cudaGetSymbolAddress); make it before any
- * stream capture. With lazy module loading (CUDA's default) that first call
+ * looks the array's address up (cudaGetSymbolAddress). With lazy module
+ * loading (CUDA's default) that first call
  * is also when the device takes the array's memory, so it can fail on a full
  * device: make it before reserving a memory pool; later calls allocate
  * nothing. The call waits on `stream` for its own work before it returns.
