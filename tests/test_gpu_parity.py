@@ -183,6 +183,27 @@ def test_indicator_probabilities_match_reference(precision):
 
 
 @pytest.mark.parametrize("precision", [0, 1])
+def test_indicator_kriging_wide_systems_against_oracle(precision):
+    """IK with 40 to 64 neighbours per category (the 33-64 bucket's one-warp
+    kernels writing per-category probabilities): corrected probabilities
+    within 1e-5 of the CPU oracle's and categories identical wherever the
+    oracle's largest probability is not within that of the runner-up."""
+    wl = WL.indicator(0.3)
+    covs, rads = wl.cat_covs, wl.cat_radiuses
+    ks = [40, 48, 56, 64, 48]
+    od, om, op = O.indicator_grid(wl.dims, wl.data, wl.mask, covs, rads, ks, wl.marginals)
+    out_d, out_m, probs = H.engine_indicator(wl, covs, rads, ks, wl.marginals, precision=precision)
+    np.testing.assert_array_equal(out_m, om)
+    assert np.abs(probs - op).max() <= 1e-5
+    top2 = np.sort(op, axis=1)[:, -2:]
+    clear = (top2[:, 1] - top2[:, 0]) > 1e-5
+    np.testing.assert_array_equal(out_d[clear], od[clear])
+    _, cnt, _ = H.engine_neighbours(1, wl, np.flatnonzero(wl.mask == 0)[::97], cov=covs[3], radiuses=rads[3],
+                                    k=ks[3])
+    assert (cnt > 32).mean() > 0.5  # the wide kernels carry most systems
+
+
+@pytest.mark.parametrize("precision", [0, 1])
 def test_indicator_kriging_matches_reference(precision):
     g = G.load("indicator_s015")
     dims, data, mask = G.grid_inputs(g, dtype=np.uint8)
