@@ -49,6 +49,25 @@ METRIC = "kriged cells/s, 1 B200: FP32-refined vs FP64 plain at <=1e-6 rel err"
 UNIT = "cells/s"
 
 
+def rank_max(dist, x, device):
+    """Maximum of x over all ranks (x itself without a process group): a
+    step's device time is the slowest rank's."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank, world, ms):
+    """Units per second of the whole job: every rank processes
+    units_per_rank (independent replicas) and the job takes the slowest
+    rank's ms."""
+    return units_per_rank * world / (ms / 1e3)
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -358,11 +377,7 @@ def bench_sgs(args, rank, world, local):
             dist.barrier()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return rank_max(dist, x, dev)
 
     def restore():
         d_data.copy_(d_data0)
@@ -560,11 +575,7 @@ def bench_sis(args, rank, world, local):
             dist.barrier()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return rank_max(dist, x, dev)
 
     def restore():
         d_data.copy_(d_data0)
@@ -767,11 +778,7 @@ def bench_cok(args, rank, world, local):
             dist.barrier()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return rank_max(dist, x, dev)
 
     if args.profile_case > 0:
         st = dev_call()
@@ -1162,11 +1169,7 @@ def main():
             dist.barrier()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return rank_max(dist, x, dev)
 
     def timed_device(precision):
         for _ in range(args.warmup):
@@ -1207,8 +1210,8 @@ def main():
     ms32 = max_over_ranks(float(np.mean(t32)))
     ms64 = max_over_ranks(float(np.mean(t64)))
     cells = s32[-1]["kriged_cells"]
-    value = cells * world / (ms32 / 1e3)
-    value64 = s64[-1]["kriged_cells"] * world / (ms64 / 1e3)
+    value = whole_job_rate(cells, world, ms32)
+    value64 = whole_job_rate(s64[-1]["kriged_cells"], world, ms64)
     launches = int(sum(s["kernel_launches"] for s in s32))
 
     # roofline of the dominant kernel (the solve bucket with the largest time)
