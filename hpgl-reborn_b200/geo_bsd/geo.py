@@ -135,6 +135,17 @@ def _clone_prop(prop):
     return ContProperty(data2, mask2)
 
 
+def _output_like(prop):
+    """Output arrays for an engine call that writes every cell of its outputs
+    (values and mask, the informed cells copied on the device): the input's
+    shapes and types, not initialised on the host."""
+    data2 = numpy.empty_like(prop.data, order="F")
+    mask2 = numpy.empty_like(prop.mask, order="F")
+    if isinstance(prop, IndProperty):
+        return IndProperty(data2, mask2, prop.indicator_count)
+    return ContProperty(data2, mask2)
+
+
 def _empty_clone(prop):
     """A property of the same shape with every value 0 and every cell uninformed."""
     data2 = prop.data.copy("F")
@@ -182,7 +193,7 @@ def _cont_kriging(kind, prop, grid, radiuses, max_neighbours, cov_model, mean, p
     ParameterValidator.validate_max_neighbors(max_neighbours)
     ParameterValidator.validate_covariance_parameters(cov_model.sill, cov_model.nugget, cov_model.ranges,
                                                       cov_model.angles)
-    out_prop = _clone_prop(prop)
+    out_prop = _output_like(prop)
     dims = _dims(grid, prop)
     p = W._HPGL_SK_PARAMS(covariance_type=cov_model.type, ranges=tuple(cov_model.ranges),
                           angles=tuple(cov_model.angles), sill=cov_model.sill, nugget=cov_model.nugget,
@@ -230,7 +241,7 @@ def lvm_kriging(prop, grid, mean_data, radiuses, max_neighbours, cov_model, *, p
         raise ValueError("lvm_kriging: mean_data must be a numpy array")
     if mean_data.dtype != numpy.float32:
         mean_data = numpy.require(mean_data, dtype="float32")
-    out_prop = _clone_prop(prop)
+    out_prop = _output_like(prop)
     dims = _dims(grid, prop)
     if mean_data.size != prop.data.size:
         raise RuntimeError("lvm_kriging: mean_data has %d values, the grid %d" % (mean_data.size, prop.data.size))
