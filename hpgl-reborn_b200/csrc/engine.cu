@@ -789,7 +789,9 @@ struct IoPlan
 // call time.
 constexpr size_t kStageMin = 4u << 20;
 
-static bool host_locked(const void *p)
+// true for ordinary pageable host memory (not page-locked, registered, device
+// or managed memory: those go to cudaMemcpyAsync as they are)
+static bool host_pageable(const void *p)
 {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess)
@@ -797,7 +799,7 @@ static bool host_locked(const void *p)
         cudaGetLastError();
         return false;
     }
-    return a.type == cudaMemoryTypeHost;
+    return a.type == cudaMemoryTypeUnregistered;
 }
 
 // memcpy split over up to eight host threads (4 MB at least each)
@@ -828,7 +830,7 @@ static T *to_device(Engine &E, const char *slot, const T *src, size_t n, const I
     if (io.device) return const_cast<T *>(src);
     T *d = E.buf<T>(slot, n);
     const size_t bytes = n * sizeof(T);
-    if (bytes < kStageMin || host_locked(src))
+    if (bytes < kStageMin || !host_pageable(src))
         HB_CK(cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, io.st));
     else
     {
@@ -845,7 +847,7 @@ static void to_host(Engine &E, T *dst, const T *dsrc, size_t n, const IoPlan &io
 {
     if (io.device || dst == dsrc) return;
     const size_t bytes = n * sizeof(T);
-    if (bytes < kStageMin || host_locked(dst))
+    if (bytes < kStageMin || !host_pageable(dst))
         HB_CK(cudaMemcpyAsync(dst, dsrc, bytes, cudaMemcpyDeviceToHost, io.st));
     else
     {

@@ -160,6 +160,53 @@ def test_device_pointers_on_a_caller_stream_and_determinism():
     np.testing.assert_array_equal(outs[0][0], host["data"])
 
 
+def test_pageable_pinned_and_device_buffers_agree():
+    """Inputs and outputs above the staging threshold (4 MB) in pageable numpy
+    arrays (copied through page-locked areas by host threads), in page-locked
+    buffers from hpgl_b200_host_alloc (copied directly) and on the device give
+    bit-identical outputs; a second pageable call into fresh arrays too."""
+    import torch
+    wl = WL.sk_ok_large(0.55)
+    n = wl.n_cells
+    assert n * 4 >= 4 << 20
+    a = H.engine_cont(0, wl, precision=1)
+    b = H.engine_cont(0, wl, precision=1)
+    np.testing.assert_array_equal(a["data"], b["data"])
+    np.testing.assert_array_equal(a["var"], b["var"])
+    lib = W._hpgl_so
+    sizes = (n * 4, n, n * 4, n, n * 8)
+    ptrs = [lib.hpgl_b200_host_alloc(sz) for sz in sizes]
+    try:
+        hd, hm, ho, hom, hv = ptrs
+        C.memmove(hd, np.ascontiguousarray(wl.data, np.float32).ctypes.data, n * 4)
+        C.memmove(hm, np.ascontiguousarray(wl.mask, np.uint8).ctypes.data, n)
+        o = W._HPGL_B200_OPTIONS(precision=1, refine_steps=2, flags=W.FLAG_OUT_IS_CLONE, stream=None,
+                                 estimate64=None, variance=hv, status=None, ik_probs=None)
+        p = H.sk_params(wl.cov, wl.radiuses, wl.max_neighbours)
+        rc = lib.hpgl_b200_cont_kriging_ex(0, (C.c_int * 3)(*wl.dims), hd, hm, C.byref(p), ho, hom, C.byref(o))
+        W.check(rc, "pinned call")
+        out = np.ctypeslib.as_array((C.c_float * n).from_address(ho)).copy()
+        omask = np.ctypeslib.as_array((C.c_ubyte * n).from_address(hom)).copy()
+        var = np.ctypeslib.as_array((C.c_double * n).from_address(hv)).copy()
+    finally:
+        for q in ptrs:
+            lib.hpgl_b200_host_free(q)
+    np.testing.assert_array_equal(out, a["data"])
+    np.testing.assert_array_equal(omask, a["mask"])
+    np.testing.assert_array_equal(var, a["var"])
+    dev = torch.device("cuda", 0)
+    d = torch.from_numpy(np.ascontiguousarray(wl.data)).to(dev)
+    m = torch.from_numpy(np.ascontiguousarray(wl.mask)).to(dev)
+    od, om = d.clone(), m.clone()
+    o = W._HPGL_B200_OPTIONS(precision=1, refine_steps=2, flags=W.FLAG_DEVICE_POINTERS | W.FLAG_OUT_IS_CLONE,
+                             stream=None, estimate64=None, variance=None, status=None, ik_probs=None)
+    rc = lib.hpgl_b200_cont_kriging_ex(0, (C.c_int * 3)(*wl.dims), d.data_ptr(), m.data_ptr(), C.byref(p),
+                                       od.data_ptr(), om.data_ptr(), C.byref(o))
+    W.check(rc, "device call")
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(od.cpu().numpy(), a["data"])
+
+
 def test_full_size_benchmark_grid_properties():
     """256x256x128 OK, k=32: FP32-refined agrees with FP64 plain to 1e-6, variances are
     non-negative, every uninformed cell is kriged, and repeated runs are bit-identical."""
