@@ -593,7 +593,7 @@ static DevSearch run_search(Engine &E, const Plan &pl, const DevPoints &P, const
     if (S.ties > 0)
     {
         int cap = std::max(max_cand, 1);
-        if (fast && resolve_ties_fast_smem(cap, 4) <= (size_t)E.max_smem())
+        if (fast && cap <= 65535 && resolve_ties_fast_smem(cap, 1) <= (size_t)E.max_smem())
         {
             HB_CK(launch_resolve_ties_fast(g, tie_cells, scal + 3, S.ties, bin_start, bin_cnt, bin_pts, P.pts_xyz,
                                            P.pts_val, keytab16, cap, S.nb_pid, S.nb_rec, E.n_sm(), st));

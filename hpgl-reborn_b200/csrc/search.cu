@@ -1188,9 +1188,11 @@ struct RankLess
 // The serial loop swaps a[L[m]] and a[R[m]] while L[m] < R[m]; every such L
 // lies below every such R, so the swaps are disjoint and independent, and the
 // loop returns min(L[M], R[M-1]) for the first M with L[M] >= R[M] (an exhausted
-// L counts as +inf, R[-1] as +inf). lstop / rstop hold hi - lo ints each.
+// L counts as +inf, R[-1] as +inf). lstop / rstop hold hi - lo positions each
+// (16-bit: candidate lists stay below 65,536 entries).
 template <typename Less>
-__device__ int warp_partition_around_front(uint32_t *a, int lo, int hi, Less less, int *lstop, int *rstop, int lane)
+__device__ int warp_partition_around_front(uint32_t *a, int lo, int hi, Less less, uint16_t *lstop, uint16_t *rstop,
+                                           int lane)
 {
     const uint32_t pivot = a[lo];
     int nr = 0;
@@ -1199,7 +1201,7 @@ __device__ int warp_partition_around_front(uint32_t *a, int lo, int hi, Less les
         const int j = top - lane;
         const bool st = j >= lo && !less(pivot, a[j]);
         const unsigned bl = __ballot_sync(0xffffffffu, st);
-        if (st) rstop[nr + __popc(bl & lanemask_lt())] = j;
+        if (st) rstop[nr + __popc(bl & lanemask_lt())] = (uint16_t)j;
         nr += __popc(bl);
     }
     __syncwarp();
@@ -1211,7 +1213,7 @@ __device__ int warp_partition_around_front(uint32_t *a, int lo, int hi, Less les
         const unsigned bl = __ballot_sync(0xffffffffu, st);
         const int m = nl + __popc(bl & lanemask_lt());
         const bool cross = st && (m >= nr || i >= rstop[m]);
-        if (st && !cross) lstop[m] = i;
+        if (st && !cross) lstop[m] = (uint16_t)i;
         const unsigned cb = __ballot_sync(0xffffffffu, cross);
         if (cb)
         {
@@ -1240,7 +1242,8 @@ __device__ int warp_partition_around_front(uint32_t *a, int lo, int hi, Less les
 // heapsort fallback and the final short insertion sort by lane 0): the same
 // first-k set std::sort leaves in front.
 template <typename Less>
-__device__ void warp_select_first_k(uint32_t *a, int n, int k, Less less, int *lstop, int *rstop, int lane)
+__device__ void warp_select_first_k(uint32_t *a, int n, int k, Less less, uint16_t *lstop, uint16_t *rstop,
+                                    int lane)
 {
     const int kThreshold = 16;
     if (n <= 0 || k <= 0 || k >= n) return;
@@ -1269,6 +1272,10 @@ __device__ void warp_select_first_k(uint32_t *a, int n, int k, Less less, int *l
     __syncwarp();
 }
 
+// shared memory of one warp: the list (key and slot), the point ids, the two
+// stop lists
+__host__ __device__ inline size_t ties_warp_bytes(int cap) { return ((size_t)cap * 12 + 15) / 16 * 16; }
+
 template <int E>
 __global__ void __launch_bounds__(128) k_resolve_ties_fast(
     const Geom g, const int *__restrict__ tie_cells, const int *__restrict__ tie_count,
@@ -1278,9 +1285,9 @@ __global__ void __launch_bounds__(128) k_resolve_ties_fast(
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    uint32_t *arr = reinterpret_cast<uint32_t *>(smem) + (size_t)warp * 4 * cap;
+    uint32_t *arr = reinterpret_cast<uint32_t *>(smem + (size_t)warp * ties_warp_bytes(cap));
     int *pid = reinterpret_cast<int *>(arr + cap);
-    int *lstop = pid + cap, *rstop = lstop + cap;
+    uint16_t *lstop = reinterpret_cast<uint16_t *>(pid + cap), *rstop = lstop + cap;
     const int n_ties = *tie_count;
     for (int t = blockIdx.x * nwarps + warp; t < n_ties; t += gridDim.x * nwarps)
     {
@@ -1352,17 +1359,25 @@ __global__ void __launch_bounds__(128) k_resolve_ties_fast(
     }
 }
 
-size_t resolve_ties_fast_smem(int cap, int warps) { return (size_t)warps * 4 * cap * 4; }
+size_t resolve_ties_fast_smem(int cap, int warps) { return (size_t)warps * ties_warp_bytes(cap); }
 
 cudaError_t launch_resolve_ties_fast(const Geom &g, const int *tie_cells, const int *tie_count, int n_ties,
                                      const int *bin_start, const int *bin_cnt, const int *bin_pts,
                                      const unsigned long long *pts_xyz, const float *pts_vf, const uint16_t *keytab16,
                                      int cap, int *nb_pid, int2 *nb_rec, int n_sm, cudaStream_t st)
 {
-    const int warps = 4;
+    // Four warps a block while that keeps as many warps resident as one-warp
+    // blocks would (the candidate lists of clustered data fill shared memory:
+    // 31 KB a warp at 2,580 candidates, seven warps an SM in one-warp blocks,
+    // four in four-warp blocks).
+    constexpr size_t kSmemSM = 227u * 1024u;
+    const size_t pw = ties_warp_bytes(cap);
+    const long r1 = std::min<long>(32, (long)(kSmemSM / pw));
+    const long r4 = 4 * (long)(kSmemSM / (4 * pw));
+    const int warps = r4 >= r1 ? 4 : 1;
     const size_t smem = resolve_ties_fast_smem(cap, warps);
     int blocks = (n_ties + warps - 1) / warps;
-    if (blocks > n_sm * 16) blocks = n_sm * 16;
+    if (blocks > n_sm * 64 / warps) blocks = n_sm * 64 / warps;
     if (blocks < 1) blocks = 1;
     if (g.k <= 32)
     {
