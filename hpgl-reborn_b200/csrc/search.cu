@@ -1272,9 +1272,13 @@ __device__ void warp_select_first_k(uint32_t *a, int n, int k, Less less, uint16
     __syncwarp();
 }
 
-// shared memory of one warp: the list (key and slot), the point ids, the two
-// stop lists
-__host__ __device__ inline size_t ties_warp_bytes(int cap) { return ((size_t)cap * 12 + 15) / 16 * 16; }
+// shared memory of one warp: the 27 bins' list offsets and starts, the list
+// (key and slot), the point ids, the two stop lists
+__host__ __device__ inline size_t ties_warp_bytes(int cap) { return 256 + ((size_t)cap * 12 + 15) / 16 * 16; }
+
+// chunks of 32 candidates whose loads a warp has in flight at once while it
+// builds a cell's list
+constexpr int kTieChunks = 4;
 
 template <int E>
 __global__ void __launch_bounds__(128) k_resolve_ties_fast(
@@ -1285,7 +1289,9 @@ __global__ void __launch_bounds__(128) k_resolve_ties_fast(
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    uint32_t *arr = reinterpret_cast<uint32_t *>(smem + (size_t)warp * ties_warp_bytes(cap));
+    int *bpre = reinterpret_cast<int *>(smem + (size_t)warp * ties_warp_bytes(cap)); // 28: list offsets
+    int *bst = bpre + 32;                                                                // 27: bin starts
+    uint32_t *arr = reinterpret_cast<uint32_t *>(bpre + 64);
     int *pid = reinterpret_cast<int *>(arr + cap);
     uint16_t *lstop = reinterpret_cast<uint16_t *>(pid + cap), *rstop = lstop + cap;
     const int n_ties = *tie_count;
@@ -1294,37 +1300,84 @@ __global__ void __launch_bounds__(128) k_resolve_ties_fast(
         const int cell = tie_cells[t];
         const int x = cell % g.nx, y = cell % (g.nx * g.ny) / g.nx, z = cell / (g.nx * g.ny);
         const int bxi = x / g.rx, byi = y / g.ry, bzi = z / g.rz;
+        // the 27 bins (z, y, x nested) as one list: lane q < 27 holds bin q's
+        // start and count, the prefix sums give each bin's offset in the list
+        int bs = 0, bc = 0;
+        if (lane < 27)
+        {
+            const int kk = bzi - 1 + lane / 9, jj = byi - 1 + (lane / 3) % 3, ii = bxi - 1 + lane % 3;
+            if (ii >= 0 && jj >= 0 && kk >= 0 && ii < g.bx && jj < g.by && kk < g.bz)
+            {
+                const int nb = (kk * g.by + jj) * g.bx + ii;
+                bs = bin_start[nb];
+                bc = bin_cnt[nb];
+            }
+        }
+        int incl = bc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const int tv = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += tv;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 26);
+        __syncwarp(); // the previous cell's reads of bpre / bst are done
+        if (lane < 27)
+        {
+            bpre[lane] = incl - bc;
+            bst[lane] = bs;
+        }
+        __syncwarp();
+        // kTieChunks chunks of 32 list entries at a time: their three dependent
+        // loads (point, coordinates, key) in flight together, then the chunks
+        // compacted in list order
         int n = 0;
-        for (int kk = bzi - 1; kk <= bzi + 1; ++kk)
-            for (int jj = byi - 1; jj <= byi + 1; ++jj)
-                for (int ii = bxi - 1; ii <= bxi + 1; ++ii)
+        for (int base = 0; base < total; base += 32 * kTieChunks)
+        {
+            int p[kTieChunks];
+            unsigned long long q[kTieChunks];
+            uint32_t key[kTieChunks];
+#pragma unroll
+            for (int u = 0; u < kTieChunks; ++u)
+            {
+                const int gi = base + 32 * u + lane;
+                p[u] = -1;
+                if (gi < total)
                 {
-                    if (ii < 0 || jj < 0 || kk < 0 || ii >= g.bx || jj >= g.by || kk >= g.bz) continue;
-                    const int nb = (kk * g.by + jj) * g.bx + ii;
-                    const int s = bin_start[nb], cnt = bin_cnt[nb];
-                    for (int base = 0; base < cnt; base += 32)
-                    {
-                        const int i = base + lane;
-                        uint32_t key = 0xFFFFu;
-                        int p = 0;
-                        if (i < cnt)
-                        {
-                            p = bin_pts[s + i];
-                            int px, py, pz;
-                            unpack_xyz(pts_xyz[p], px, py, pz);
-                            key = keytab[key_index(g, px - x, py - y, pz - z)];
-                        }
-                        const bool keep = key != 0xFFFFu;
-                        const unsigned bl = __ballot_sync(0xffffffffu, keep);
-                        const int slot = n + __popc(bl & lanemask_lt());
-                        if (keep && slot < cap)
-                        {
-                            arr[slot] = (key << 16) | (uint32_t)slot;
-                            pid[slot] = p;
-                        }
-                        n += __popc(bl);
-                    }
+                    int b = 0; // the last bin whose offset is <= gi
+#pragma unroll
+                    for (int st = 16; st > 0; st >>= 1)
+                        if (b + st <= 26 && bpre[b + st] <= gi) b += st;
+                    p[u] = bin_pts[bst[b] + gi - bpre[b]];
                 }
+            }
+#pragma unroll
+            for (int u = 0; u < kTieChunks; ++u) q[u] = p[u] >= 0 ? pts_xyz[p[u]] : 0ull;
+#pragma unroll
+            for (int u = 0; u < kTieChunks; ++u)
+            {
+                key[u] = 0xFFFFu;
+                if (p[u] >= 0)
+                {
+                    int px, py, pz;
+                    unpack_xyz(q[u], px, py, pz);
+                    key[u] = keytab[key_index(g, px - x, py - y, pz - z)];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kTieChunks; ++u)
+            {
+                const bool keep = key[u] != 0xFFFFu;
+                const unsigned bl = __ballot_sync(0xffffffffu, keep);
+                const int slot = n + __popc(bl & lanemask_lt());
+                if (keep && slot < cap)
+                {
+                    arr[slot] = (key[u] << 16) | (uint32_t)slot;
+                    pid[slot] = p[u];
+                }
+                n += __popc(bl);
+            }
+        }
         if (n > cap) n = cap; // cannot happen: cap bounds every candidate list
         __syncwarp();
         warp_select_first_k(arr, n, g.k, RankLess(), lstop, rstop, lane);
