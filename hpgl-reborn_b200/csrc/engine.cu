@@ -1875,6 +1875,8 @@ int cokriging(const int *dims, const float *pdata, const unsigned char *pmask, c
             std::fill(pl.kt.rank.begin(), pl.kt.rank.end(), KEY_EXCLUDED);
             for (size_t i = 0; i < tv.size(); ++i) pl.kt.rank[key_index(g, tv[i].dx, tv[i].dy, tv[i].dz)] = (uint32_t)i;
             pl.kt.n_ranks = (uint32_t)tv.size();
+            pl.kt.h2_lo.clear(); // the key table's h2 ranges belong to its own ranks
+            pl.kt.h2_hi.clear();
             pl.rank_bits = pl.kt.n_ranks > 1 ? bits_for(pl.kt.n_ranks - 1) : 0;
             pl.sg = Surrogate();
             build_surrogate(pl.f, pl.kt, pl.sg, true);

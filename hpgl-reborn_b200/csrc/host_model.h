@@ -79,6 +79,10 @@ struct KeyTable
     std::vector<double> vals;
     std::vector<uint32_t> rank;
     uint32_t n_ranks = 0; // distinct kept values
+    // per rank the smallest and largest squared anisotropic distance h2 carrying
+    // it (||T v||^2 over the offsets of that rank), for the ranks build_key_table
+    // assigns; code that assigns other ranks clears them
+    std::vector<double> h2_lo, h2_hi;
 };
 void build_key_table(const Flavour &f, KeyTable &kt, int n_threads);
 // The same template as build_template(f), its covariances read from kt.
