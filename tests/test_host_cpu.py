@@ -105,14 +105,22 @@ def test_transform_template_and_covariance_bit_identical(mi):
     assert lib.hpgl_b200_transform((C.c_double * 3)(*cov.ranges), (C.c_double * 3)(*cov.angles), t) == 0
     np.testing.assert_array_equal(np.array(list(t)), O.transform("port", cov.ranges, cov.angles))
     cap = (2 * rad[0] + 1) * (2 * rad[1] + 1) * (2 * rad[2] + 1)
-    for kind in (0, 1):
-        out = np.zeros((cap, 3), np.int32)
-        lim = C.c_int(0)
-        n = lib.hpgl_b200_template(kind, C.byref(_covp(cov)), (C.c_int * 3)(*rad), out.ctypes.data, cap,
-                                   C.byref(lim))
-        ref, rlim = O.template("port", kind, cov, rad)
-        assert n == len(ref) and lim.value == rlim
-        np.testing.assert_array_equal(out[:n], ref)
+    # the key table behind the template is built by a team of host threads (the
+    # first half of the block evaluated, the mirrors copied): the same at any size
+    saved = lib.hpgl_get_thread_num()
+    try:
+        for threads in (1, 3, 16):
+            lib.hpgl_set_thread_num(threads)
+            for kind in (0, 1):
+                out = np.zeros((cap, 3), np.int32)
+                lim = C.c_int(0)
+                n = lib.hpgl_b200_template(kind, C.byref(_covp(cov)), (C.c_int * 3)(*rad), out.ctypes.data, cap,
+                                           C.byref(lim))
+                ref, rlim = O.template("port", kind, cov, rad)
+                assert n == len(ref) and lim.value == rlim
+                np.testing.assert_array_equal(out[:n], ref)
+    finally:
+        lib.hpgl_set_thread_num(saved)
     rng = np.random.default_rng(mi)
     for _ in range(300):
         a = rng.integers(0, 60, 3).astype(np.int32)
