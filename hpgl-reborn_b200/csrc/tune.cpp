@@ -16,6 +16,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 namespace hb
 {
@@ -170,7 +171,13 @@ int tune_load(const char *path, std::string &err)
     size_t got;
     while ((got = std::fread(buf, 1, sizeof buf, f)) > 0) text.append(buf, got);
     std::fclose(f);
-    int n = 0;
+    // every entry is checked before any is applied: a file that fails leaves
+    // the table as it was
+    struct Entry
+    {
+        int prec, b, cov, var;
+    };
+    std::vector<Entry> entries;
     size_t pos = 0;
     while (true)
     {
@@ -179,9 +186,10 @@ int tune_load(const char *path, std::string &err)
         if (open == std::string::npos) break;
         const size_t lb = text.rfind('{', open);
         size_t rb = text.find('}', open);
-        // skip a nested timing object
+        // skip a nested timing object: the entry closes at the brace after the
+        // one that closes it (rb is then that inner brace, the first after open)
         const size_t nested = text.find('{', open);
-        if (nested != std::string::npos && nested < rb) rb = text.find('}', text.find('}', nested) + 1);
+        if (rb != std::string::npos && nested != std::string::npos && nested < rb) rb = text.find('}', rb + 1);
         if (lb == std::string::npos || rb == std::string::npos)
         {
             err = "malformed tuning cache";
@@ -202,12 +210,15 @@ int tune_load(const char *path, std::string &err)
             err = "tuning cache entry with an invalid key or variant";
             return -1;
         }
-        g_table[prec][b][cov].store(var, std::memory_order_relaxed);
-        std::lock_guard<std::mutex> lk(g_ms_mu);
-        g_source[prec][b][cov] = 2;
-        ++n;
+        entries.push_back({prec, b, cov, var});
     }
-    return n;
+    std::lock_guard<std::mutex> lk(g_ms_mu);
+    for (const Entry &e : entries)
+    {
+        g_table[e.prec][e.b][e.cov].store(e.var, std::memory_order_relaxed);
+        g_source[e.prec][e.b][e.cov] = 2;
+    }
+    return (int)entries.size();
 }
 
 int tune_save(const char *path, std::string &err)

@@ -87,6 +87,21 @@ def test_cache_reader_rejects_invalid_entries(tmp_path, entry):
     assert "tune_load" in W.last_error()
 
 
+@pytest.mark.timeout(60)
+def test_truncated_cache_is_an_error_and_changes_nothing(tmp_path):
+    """A file cut inside an entry's timing object, after a complete entry: an
+    error (not a scan that restarts before the cut), and no entry applied."""
+    good = {"np": 8, "cov_type": 0, "precision": 0, "variant": "fold_narrow"}
+    cut = '{"np": 32, "cov_type": 1, "precision": 1, "variant": "quad", "ms_per_million": {"fold": 4.8'
+    path = tmp_path / "cut.json"
+    path.write_text("[" + json.dumps(good) + ", " + cut)
+    before = W.solve_variant(8, 0, W.FP64_PLAIN)
+    with pytest.raises(RuntimeError):
+        T.load_cache(str(path))
+    assert "tune_load" in W.last_error()
+    assert W.solve_variant(8, 0, W.FP64_PLAIN) == before
+
+
 def test_missing_cache_file_is_an_error(tmp_path):
     with pytest.raises(RuntimeError):
         T.load_cache(str(tmp_path / "absent.json"))
