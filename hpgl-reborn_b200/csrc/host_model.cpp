@@ -98,7 +98,9 @@ class Workers
 // A team of n host threads running one body (on the workers above). sync() is
 // a reusable barrier for the whole team (spin, then yield: the phases between
 // barriers are tens of microseconds, so sleeping would cost more than the
-// work). Every member must reach every sync() of the body, in the same order.
+// work). Every member must reach every sync() of the body, in the same order,
+// and the body must not throw (a member that left would hold the others at
+// their next barrier): it allocates nothing.
 class Team
 {
   public:
@@ -365,6 +367,8 @@ void build_key_table(const Flavour &f, KeyTable &kt, int n_threads)
     std::vector<uint32_t> bstart(kKeyBuckets + 1);        // bucket starts in the scattered list
     std::vector<uint32_t> part(nt);                        // keys per member's bucket range
     std::vector<Edge> edges(2 * (size_t)nt);
+    kt.h2_lo.reserve(n_half); // at most one rank per kept entry: sized in the body without allocating
+    kt.h2_hi.reserve(n_half);
     long n_kept = 0, n_changes = 0;
     team.run([&](int t) {
         uint32_t own_hist[kKeyBuckets], acc[kKeyBuckets];
