@@ -131,6 +131,81 @@ def test_transform_template_and_covariance_bit_identical(mi):
             assert v == O.cov_point("port", kind, cov, rad, a, b)
 
 
+def _template(lib, mi, kind=0):
+    cov, rad = MODELS[mi], RADII[mi]
+    cap = (2 * rad[0] + 1) * (2 * rad[1] + 1) * (2 * rad[2] + 1)
+    out = np.zeros((cap, 3), np.int32)
+    lim = C.c_int(0)
+    n = lib.hpgl_b200_template(kind, C.byref(_covp(cov)), (C.c_int * 3)(*rad), out.ctypes.data, cap, C.byref(lim))
+    return out[:n].copy(), lim.value
+
+
+@pytest.mark.timeout(300)
+def test_key_tables_built_from_several_threads_at_once():
+    """The key table's host workers serve one build at a time; builds that find
+    them busy start threads of their own. Concurrent builds from six Python
+    threads (ctypes calls release the GIL) all equal the oracle's template."""
+    import threading
+
+    lib = W._hpgl_so
+    want = {mi: O.template("port", 0, MODELS[mi], RADII[mi]) for mi in range(len(MODELS))}
+    errors = []
+
+    def worker(seed):
+        rng = np.random.default_rng(seed)
+        for mi in rng.integers(0, len(MODELS), 8):
+            got, lim = _template(lib, int(mi))
+            ref, rlim = want[int(mi)]
+            if lim != rlim or not np.array_equal(got, ref):
+                errors.append(int(mi))
+
+    saved = lib.hpgl_get_thread_num()
+    lib.hpgl_set_thread_num(4)
+    try:
+        ts = [threading.Thread(target=worker, args=(s,)) for s in range(6)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+    finally:
+        lib.hpgl_set_thread_num(saved)
+    assert not errors, errors
+
+
+@pytest.mark.timeout(300)
+@pytest.mark.filterwarnings("ignore:This process .* is multi-threaded:DeprecationWarning")
+def test_key_table_in_a_forked_child():
+    """A child forked after the workers started builds with workers of its own
+    (the library's own locks are free at the fork; the wait for the child is
+    bounded all the same)."""
+    import time
+
+    lib = W._hpgl_so
+    ref, rlim = O.template("port", 0, MODELS[1], RADII[1])
+    got, lim = _template(lib, 1)  # the workers exist in this process now
+    assert lim == rlim and np.array_equal(got, ref)
+    pid = os.fork()
+    if pid == 0:
+        code = 1
+        try:
+            g, l = _template(lib, 1)
+            code = 0 if (l == rlim and np.array_equal(g, ref)) else 2
+        finally:
+            os._exit(code)
+    deadline = time.time() + 120
+    status = None
+    while time.time() < deadline:
+        done, status = os.waitpid(pid, os.WNOHANG)
+        if done:
+            break
+        time.sleep(0.05)
+    else:
+        os.kill(pid, 9)
+        os.waitpid(pid, 0)
+        pytest.fail("the forked child did not finish its key table")
+    assert os.WIFEXITED(status) and os.WEXITSTATUS(status) == 0, status
+
+
 def test_zero_range_is_an_error_not_an_abort():
     lib = W._hpgl_so
     out = (C.c_double * 9)()
